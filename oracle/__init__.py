@@ -1,0 +1,357 @@
+"""CPU ORACLE -- test infrastructure, never the product.
+
+A C restatement (``oracle/csrc``) of the reference's (PyRITE v0.36.2) transport
+and emission-scoring arithmetic, plus this thin ctypes wrapper. Only the tests,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline use it, as the
+checker or as the timed CPU reference; ``pyrite_b200`` never imports it.
+
+Parity status: pinned against golden vectors produced by running the reference
+itself (``tests/golden/make_golden.py`` through ``oracle.ref_harness``):
+transport rows bit for bit, the CXR line chain and its reductions and the
+Bethe-Heitler spectrum to FP64 rounding.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+
+RNG_SPLITMIX = 0
+RNG_PHILOX = 1
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.is_file():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+_I32 = C.POINTER(C.c_int)
+_I16 = C.POINTER(C.c_int16)
+_I8 = C.POINTER(C.c_int8)
+_U8 = C.POINTER(C.c_uint8)
+
+
+class _Layers(C.Structure):
+    _fields_ = [
+        ("n_layers", C.c_int),
+        ("max_el", C.c_int),
+        ("z_top", _D),
+        ("z_bot", _D),
+        ("n_el", _I32),
+        ("J", _D),
+        ("k", _D),
+        ("coeff", _D),
+        ("E_cross", _D),
+        ("sr_rate_numer", _D),
+        ("sr_joy_numer", _D),
+    ]
+
+
+class _Rows(C.Structure):
+    _fields_ = [
+        ("r_mid", _D),
+        ("v_hat", _D),
+        ("L", _D),
+        ("E_start", _D),
+        ("E_end", _D),
+        ("t_start", _D),
+        ("t_end", _D),
+        ("elec_id", _I64),
+        ("layer", _I16),
+        ("flight", _I64),
+        ("event", _I8),
+    ]
+
+
+class _CxrTables(C.Structure):
+    _fields_ = [
+        ("n_g", C.c_int),
+        ("G", _D),
+        ("ES", _D),
+        ("EP", _D),
+        ("WM", _D),
+        ("row_table", _I32),
+        ("n_tab", C.c_int),
+        ("E_tab", _D),
+        ("chi_re", _D),
+        ("chi_im", _D),
+        ("u_re", _D),
+        ("u_im", _D),
+        ("n_mu", C.c_int),
+        ("log_mu", _D),
+        ("delta", _D),
+        ("lo_keep", C.c_double),
+        ("hi_keep", C.c_double),
+    ]
+
+
+class _CxrGeom(C.Structure):
+    _fields_ = [("n_hat", C.c_double * 3), ("thickness", C.c_double)]
+
+
+def _declare(L):
+    L.or_splitmix64.restype = C.c_uint64
+    L.or_splitmix64.argtypes = [C.c_uint64]
+    L.or_stream_key.restype = C.c_uint64
+    L.or_stream_key.argtypes = [C.c_uint64, C.c_uint64]
+    L.or_stream_uniform.restype = C.c_double
+    L.or_stream_uniform.argtypes = [C.c_uint64, C.c_uint64]
+    L.or_philox_uniform.restype = C.c_double
+    L.or_philox_uniform.argtypes = [C.c_uint64, C.c_uint64]
+    L.or_philox4x32_10.restype = None
+    L.or_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.or_dEds_spliced.restype = C.c_double
+    L.or_dEds_spliced.argtypes = [C.POINTER(_Layers), C.c_int, C.c_double]
+    L.or_sr_rate.restype = C.c_double
+    L.or_sr_rate.argtypes = [C.c_double, C.c_double, C.c_double]
+    L.or_transport.restype = None
+    L.or_transport.argtypes = [
+        C.POINTER(_Layers), C.c_int, C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_int64,
+        C.c_int64, _D, _D, _D, _D, C.POINTER(_Rows), _I64, _I8, C.c_int,
+    ]
+    L.or_cxr_lines.restype = None
+    L.or_cxr_lines.argtypes = [
+        C.POINTER(_CxrTables), C.POINTER(_CxrGeom), C.c_int64, _D, _D, _D, _D, _I64, C.c_int64,
+        _D, _D, _D, _U8, C.c_int,
+    ]
+    L.or_reduce_node.restype = None
+    L.or_reduce_node.argtypes = [C.c_int64, _D, _D, _D, C.c_int64, _D, _D, C.c_int]
+    L.or_reduce_binmean.restype = None
+    L.or_reduce_binmean.argtypes = [C.c_int64, _D, _D, _D, C.c_int64, _D, _D, C.c_int]
+    L.or_sincsq_tail.restype = C.c_double
+    L.or_sincsq_tail.argtypes = [C.c_double]
+    L.or_mean_transmission.restype = C.c_double
+    L.or_mean_transmission.argtypes = [C.c_double, C.c_double]
+    L.or_quantum_line_factors.restype = None
+    L.or_quantum_line_factors.argtypes = [C.c_double] * 10 + [_D, _D]
+    L.or_brem_spectrum.restype = None
+    L.or_brem_spectrum.argtypes = [
+        C.c_int64, _D, _D, _D, _D, C.c_int, _D, _D, C.c_double, _D, C.c_int64, _D, _D, _D,
+        C.c_int,
+    ]
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(ctype)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---------------------------------------------------------------------------
+# RNG
+# ---------------------------------------------------------------------------
+def splitmix64(x: int) -> int:
+    return int(lib().or_splitmix64(C.c_uint64(int(x))))
+
+
+def stream_key(seed: int, elec: int) -> int:
+    return int(lib().or_stream_key(C.c_uint64(int(seed) % 2**64), C.c_uint64(int(elec))))
+
+
+def stream_uniform(key: int, counter: int) -> float:
+    return float(lib().or_stream_uniform(C.c_uint64(int(key)), C.c_uint64(int(counter))))
+
+
+def philox_uniform(key: int, draw: int) -> float:
+    return float(lib().or_philox_uniform(C.c_uint64(int(key)), C.c_uint64(int(draw))))
+
+
+def philox4x32_10(ctr, key):
+    c = (C.c_uint32 * 4)(*[int(v) for v in ctr])
+    k = (C.c_uint32 * 2)(*[int(v) for v in key])
+    lib().or_philox4x32_10(c, k)
+    return [int(v) for v in c]
+
+
+# ---------------------------------------------------------------------------
+# Layer tables (src/pyrite/montecarlo/transport/layer_tables.py:52-114)
+# ---------------------------------------------------------------------------
+class LayerTables:
+    """Per-layer element coefficients, as ``build_layer_tables`` hoists them."""
+
+    def __init__(self, z_top, z_bot, n_el, Z, J, N, E_cross):
+        self.z_top = _f64(z_top)
+        self.z_bot = _f64(z_bot)
+        self.n_el = np.ascontiguousarray(n_el, dtype=np.int32)
+        Z = _f64(Z)
+        self.Z = Z
+        self.J = _f64(J)
+        N = _f64(N)
+        safe_Z = np.where(Z > 0, Z, 1.0)
+        self.k = np.where(Z > 0, 0.731 + 0.0688 * np.log10(safe_Z), 0.0)
+        self.coeff = (N / 0.602214076) * Z
+        self.E_cross = _f64(E_cross)
+        self.sr_rate_numer = 5.21e-21 * Z * Z * np.float64(4.0) * np.float64(np.pi) * (N * 1e24)
+        self.sr_joy_numer = np.where(Z > 0, np.float64(3.4e-3) * safe_Z ** np.float64(0.67), 0.0)
+        for name in ("k", "coeff", "sr_rate_numer", "sr_joy_numer"):
+            setattr(self, name, _f64(getattr(self, name)))
+        self.struct = _Layers(
+            len(self.z_top), Z.shape[1], _p(self.z_top, _D), _p(self.z_bot, _D),
+            _p(self.n_el, _I32), _p(self.J, _D), _p(self.k, _D), _p(self.coeff, _D),
+            _p(self.E_cross, _D), _p(self.sr_rate_numer, _D), _p(self.sr_joy_numer, _D),
+        )
+
+    def dEds(self, L, E):
+        return float(lib().or_dEds_spliced(C.byref(self.struct), int(L), float(E)))
+
+
+def transport(layers: LayerTables, pos, direction, E, *, seed, E_cut, rng=RNG_SPLITMIX,
+              e_start=0, max_steps=400_000, cap=4096, keep_rows=True, clock=None):
+    """Per-electron transport of ``len(E)`` histories; returns a dict of rows and finals."""
+    n = int(np.asarray(E).size)
+    pos = _f64(pos).reshape(n, 3).copy()
+    direction = _f64(direction).reshape(n, 3).copy()
+    E = _f64(E).copy()
+    clock = np.zeros(n) if clock is None else _f64(clock).copy()
+    seg_count = np.zeros(n, dtype=np.int64)
+    exit_code = np.zeros(n, dtype=np.int8)
+    rows = None
+    holders = None
+    if keep_rows:
+        m = n * cap
+        holders = dict(
+            r_mid=np.zeros((m, 3)), v_hat=np.zeros((m, 3)), L=np.zeros(m), E_start=np.zeros(m),
+            E_end=np.zeros(m), t_start=np.zeros(m), t_end=np.zeros(m),
+            elec_id=np.zeros(m, dtype=np.int64), layer=np.zeros(m, dtype=np.int16),
+            flight=np.zeros(m, dtype=np.int64), event=np.zeros(m, dtype=np.int8),
+        )
+        h = holders
+        rows = _Rows(
+            _p(h["r_mid"], _D), _p(h["v_hat"], _D), _p(h["L"], _D), _p(h["E_start"], _D),
+            _p(h["E_end"], _D), _p(h["t_start"], _D), _p(h["t_end"], _D), _p(h["elec_id"], _I64),
+            _p(h["layer"], _I16), _p(h["flight"], _I64), _p(h["event"], _I8),
+        )
+    lib().or_transport(
+        C.byref(layers.struct), int(rng), C.c_uint64(int(seed) % 2**64), int(e_start), n,
+        float(E_cut), int(max_steps), int(cap), _p(pos, _D), _p(direction, _D), _p(E, _D),
+        _p(clock, _D), C.byref(rows) if rows is not None else None, _p(seg_count, _I64),
+        _p(exit_code, _I8), 1,
+    )
+    out = dict(pos=pos, dir=direction, E=E, clock=clock, seg_count=seg_count, exit_code=exit_code)
+    if holders is not None:
+        stored = np.minimum(seg_count, cap)
+        mask = (np.arange(cap)[None, :] < stored[:, None]).reshape(-1)
+        for k, v in holders.items():
+            out[k] = v[mask]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CXR line chain and reductions
+# ---------------------------------------------------------------------------
+def cxr_lines(tables: dict, n_hat, thickness, seg: dict, Ne):
+    """Line (E_res, a_width, weight, good) per (segment, row), segment-major."""
+    G = _f64(tables["G"])
+    ES, EP, WM = _f64(tables["ES"]), _f64(tables["EP"]), _f64(tables["WM"])
+    row_table = np.ascontiguousarray(tables["row_table"], dtype=np.int32)
+    E_tab = _f64(tables["E_tab"])
+    chi_re, chi_im = _f64(tables["chi_re"]), _f64(tables["chi_im"])
+    u_re, u_im = _f64(tables["u_re"]), _f64(tables["u_im"])
+    log_mu = _f64(np.atleast_2d(tables["log_mu"]))
+    delta = _f64(tables["delta"])
+    t = _CxrTables(
+        int(G.shape[0]), _p(G, _D), _p(ES, _D), _p(EP, _D), _p(WM, _D), _p(row_table, _I32),
+        int(E_tab.size), _p(E_tab, _D), _p(chi_re, _D), _p(chi_im, _D), _p(u_re, _D),
+        _p(u_im, _D), int(log_mu.shape[0]), _p(log_mu, _D), _p(delta, _D),
+        float(tables["lo_keep"]), float(tables["hi_keep"]),
+    )
+    geo = _CxrGeom((C.c_double * 3)(*[float(v) for v in n_hat]), float(thickness))
+    v_hat = _f64(seg["v_hat"])
+    E = _f64(seg["E_keV"])
+    L = _f64(seg["L_ang"])
+    r = _f64(seg["r_mid"])
+    eid = np.ascontiguousarray(seg["elec_id"], dtype=np.int64)
+    n = int(E.size)
+    m = n * int(G.shape[0])
+    E_res = np.empty(m)
+    aw = np.empty(m)
+    w = np.empty(m)
+    good = np.empty(m, dtype=np.uint8)
+    lib().or_cxr_lines(
+        C.byref(t), C.byref(geo), n, _p(v_hat, _D), _p(E, _D), _p(L, _D), _p(r, _D),
+        _p(eid, _I64), int(Ne), _p(E_res, _D), _p(aw, _D), _p(w, _D), _p(good, _U8), 1,
+    )
+    return E_res, aw, w, good.astype(bool)
+
+
+def reduce_node(E_res, a_width, weight, E_grid):
+    E_res, a_width, weight, E_grid = (_f64(x) for x in (E_res, a_width, weight, E_grid))
+    spec = np.zeros(E_grid.size)
+    lib().or_reduce_node(E_res.size, _p(E_res, _D), _p(a_width, _D), _p(weight, _D), E_grid.size,
+                         _p(E_grid, _D), _p(spec, _D), 1)
+    return spec
+
+
+def reduce_binmean(E_res, a_width, weight, edges):
+    E_res, a_width, weight, edges = (_f64(x) for x in (E_res, a_width, weight, edges))
+    spec = np.zeros(edges.size - 1)
+    lib().or_reduce_binmean(E_res.size, _p(E_res, _D), _p(a_width, _D), _p(weight, _D),
+                            edges.size - 1, _p(edges, _D), _p(spec, _D), 1)
+    return spec
+
+
+def sincsq_tail(x):
+    return np.array([lib().or_sincsq_tail(float(v)) for v in np.ravel(x)]).reshape(np.shape(x))
+
+
+def mean_transmission(t0, t1):
+    return float(lib().or_mean_transmission(float(t0), float(t1)))
+
+
+def quantum_line_factors(h, gamma, vdg, k_dot_v, k_dot_g, g2, k2, v_dot_e, g_dot_e, k_dot_e):
+    a, b = C.c_double(), C.c_double()
+    lib().or_quantum_line_factors(
+        *[float(v) for v in (h, gamma, vdg, k_dot_v, k_dot_g, g2, k2, v_dot_e, g_dot_e, k_dot_e)],
+        C.byref(a), C.byref(b),
+    )
+    return a.value, b.value
+
+
+def energy_bin_edges(E_grid):
+    """Bin edges of the bin-mean routes (spectrum/characteristic.py:621-646)."""
+    grid = np.asarray(E_grid, dtype=float)
+    edges = np.empty(grid.size + 1)
+    edges[1:-1] = 0.5 * (grid[:-1] + grid[1:])
+    edges[0] = max(0.0, grid[0] - 0.5 * (grid[1] - grid[0]))
+    edges[-1] = grid[-1] + 0.5 * (grid[-1] - grid[-2])
+    return edges
+
+
+def brem_spectrum(seg: dict, Z, n_ang3, thickness, n_hat, E_grid, mu_grid, Ne):
+    """BH + Elwert track-length spectrum [photons/eV/sr/electron] (brem.py:829-1239)."""
+    E = _f64(seg["E_keV"])
+    L = _f64(seg["L_ang"])
+    r = _f64(seg["r_mid"])
+    v = _f64(seg["v_hat"])
+    Z = _f64(Z)
+    n_ang3 = _f64(n_ang3)
+    nh = _f64(n_hat)
+    E_grid = _f64(E_grid)
+    mu_grid = _f64(mu_grid)
+    spec = np.zeros(E_grid.size)
+    lib().or_brem_spectrum(E.size, _p(E, _D), _p(L, _D), _p(r, _D), _p(v, _D), int(Z.size),
+                           _p(Z, _D), _p(n_ang3, _D), float(thickness), _p(nh, _D), E_grid.size,
+                           _p(E_grid, _D), _p(mu_grid, _D), _p(spec, _D), 1)
+    return spec / (4.0 * np.pi) / Ne

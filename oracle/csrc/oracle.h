@@ -1,0 +1,148 @@
+/*
+ * CPU ORACLE -- test infrastructure, never the product.
+ *
+ * C restatement of the reference's transport and emission-scoring arithmetic
+ * (PyRITE v0.36.2). Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline call into it, always as the checker or the timed CPU reference,
+ * never as the product path.
+ */
+#ifndef PYRITE_ORACLE_H
+#define PYRITE_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OR_RNG_SPLITMIX = 0, OR_RNG_PHILOX = 1 };
+
+/* Exit codes: src/pyrite/montecarlo/transport/cores.py:88-93 */
+enum {
+    OR_EXIT_CUTOFF = 0,
+    OR_EXIT_BACKSCATTERED = 1,
+    OR_EXIT_TRANSMITTED = 2,
+    OR_EXIT_SIDE = 3,
+    OR_EXIT_STEP_LIMITED = 4,
+    OR_EXIT_NOT_ENTERED = 5
+};
+
+/* Row events: src/pyrite/montecarlo/transport/events.py:35-42 */
+enum {
+    OR_EVENT_ELASTIC = 0,
+    OR_EVENT_LAYER_BOUNDARY = 2,
+    OR_EVENT_EXIT_TOP = 4,
+    OR_EVENT_EXIT_BOTTOM = 5,
+    OR_EVENT_CUTOFF = 7
+};
+
+/* Padded per-layer element tables: batching.py:33-105 (pack_layer_tables). */
+typedef struct {
+    int n_layers;
+    int max_el;
+    const double *z_top;         /* [n_layers] Angstrom */
+    const double *z_bot;         /* [n_layers] */
+    const int *n_el;             /* [n_layers] */
+    const double *J;             /* [n_layers*max_el] keV */
+    const double *k;             /* Joy-Luo k */
+    const double *coeff;         /* (n_i / 0.602214076) Z */
+    const double *E_cross;       /* Joy-Luo / Berger-Seltzer crossover, keV */
+    const double *sr_rate_numer; /* 5.21e-21 Z^2 4 pi n_cm3 */
+    const double *sr_joy_numer;  /* 3.4e-3 Z^0.67 */
+} or_layers;
+
+/* Segment rows, slot i*cap + s (cores.py:911-935). */
+typedef struct {
+    double *r_mid;   /* [rows*3] */
+    double *v_hat;   /* [rows*3] */
+    double *L;
+    double *E_start;
+    double *E_end;
+    double *t_start;
+    double *t_end;
+    int64_t *elec_id;
+    int16_t *layer;
+    int64_t *flight;
+    int8_t *event;
+} or_rows;
+
+uint64_t or_splitmix64(uint64_t x);
+uint64_t or_stream_key(uint64_t seed, uint64_t elec);
+double or_stream_uniform(uint64_t key, uint64_t counter);
+void or_philox4x32_10(uint32_t ctr[4], uint32_t key[2]);
+double or_philox_uniform(uint64_t key, uint64_t draw);
+
+double or_beta_from_keV(double E);
+double or_dEds_spliced(const or_layers *ly, int L, double E);
+double or_sr_rate(double E, double sr_rate_numer, double sr_joy_numer);
+double or_cos_theta_sr(double alpha, double R);
+void or_rotate(double *dx, double *dy, double *dz, double cos_t, double phi);
+
+void or_transport(const or_layers *ly, int rng_kind, uint64_t seed, int64_t e_start, int64_t n,
+                  double E_cut, int64_t max_steps, int64_t cap, double *pos, double *dir, double *E,
+                  double *clock, or_rows *rows, int64_t *seg_count, int8_t *exit_code,
+                  int n_threads);
+
+/* ---- CXR line chain (PXR + CBS, incoherent, single slab) ---------------- */
+typedef struct {
+    int n_g;           /* reflection x orientation rows */
+    const double *G;   /* [n_g*3] sample-frame reciprocal vectors, 1/Angstrom */
+    const double *ES;  /* [n_g*3] sigma polarization */
+    const double *EP;  /* [n_g*3] pi polarization */
+    const double *WM;  /* [n_g] mosaic weight */
+    const int *row_table; /* [n_g] coupling-table row */
+    int n_tab;
+    const double *E_tab;  /* [n_tab] eV */
+    const double *chi_re; /* [n_hkl*n_tab] */
+    const double *chi_im;
+    const double *u_re;   /* U_g / m_e c^2 */
+    const double *u_im;
+    int n_mu;
+    const double *log_mu; /* [n_mu*n_tab] log(1/Angstrom) per absorber element */
+    const double *delta;  /* [n_tab] 1 - Re n */
+    double lo_keep, hi_keep;
+} or_cxr_tables;
+
+typedef struct {
+    double n_hat[3];
+    double thickness;  /* Angstrom; slab 0 <= z <= thickness */
+} or_cxr_geom;
+
+/* One line per (segment, row): E_res [eV], a_width [1/eV], weight; good = 0
+ * when the pair is dropped. Arrays are [n_seg*n_g], segment-major. */
+void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
+                  const double *v_hat, const double *E_keV, const double *L_ang,
+                  const double *r_mid, const int64_t *elec_id, int64_t Ne, double *E_res,
+                  double *a_width, double *weight, uint8_t *good, int n_threads);
+
+/* spec[e] += sum_j w_j sinc^2(a_j (E_e - E_j)/pi) (cxr/_cpu_reduce.py:26-50) */
+void or_reduce_node(int64_t n_lines, const double *E_res, const double *a_width,
+                    const double *weight, int64_t n_e, const double *E_grid, double *spec,
+                    int n_threads);
+
+/* spec[b] += sum_j w_j (1/width_b) int_bin sinc^2 (exact, Si based) */
+void or_reduce_binmean(int64_t n_lines, const double *E_res, const double *a_width,
+                       const double *weight, int64_t n_bins, const double *edges, double *spec,
+                       int n_threads);
+
+double or_sincsq_tail(double x);
+double or_si_minus_half_pi(double t);
+
+/* mean of exp(-tau) between linear end depths (segment_escape.py:276-289) */
+double or_mean_transmission(double tau0, double tau1);
+
+/* exact second-order PXR numerator and CBS factor (cxr/_recoil.py:35-76) */
+void or_quantum_line_factors(double h, double gamma, double vdg, double k_dot_v, double k_dot_g,
+                             double g2, double k2, double v_dot_e, double g_dot_e, double k_dot_e,
+                             double *pxr_num, double *f_cbs);
+
+/* ---- Bethe-Heitler + Elwert bremsstrahlung (spectrum/brem.py:431-505) --- */
+void or_brem_spectrum(int64_t n_seg, const double *E_keV, const double *L_ang,
+                      const double *r_mid, const double *v_hat, int n_el, const double *Z,
+                      const double *n_cm3, double thickness, const double n_hat[3], int64_t n_e,
+                      const double *E_grid, const double *mu_grid, double *spec, int n_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

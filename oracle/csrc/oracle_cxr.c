@@ -1,0 +1,380 @@
+/*
+ * CPU ORACLE -- test infrastructure, never the product.
+ *
+ * C restatement of the reference's incoherent PXR + CBS line chain for a
+ * fixed segment list on a single slab (the batched route,
+ * src/pyrite/montecarlo/spectrum/cxr/_batched.py:461-931), its two line
+ * reductions (node sampling, cxr/_cpu_reduce.py:26-50; exact bin means,
+ * cxr/_bin_quadrature.py:280-520) and the Bethe-Heitler + Elwert
+ * bremsstrahlung track-length estimator (spectrum/brem.py:396-505,1196-1239).
+ * Evaluation order follows the reference expression by expression, so FP64
+ * results agree with it to rounding (pinned by tests/golden/cxr_*.npz and
+ * brem_*.npz).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+
+#include "oracle.h"
+
+#define HBARC_EV_ANG 1973.269804
+#define M_E_EV 510998.95
+#define ALPHA_FS (1.0 / 137.035999)
+#define RESONANCE_ROOT_RTOL 1e-3
+
+/* cxr/_kernels.py:328-349: bracket index against an ascending grid. */
+static void interp_index(double x, const double *grid, int n, int *idx, double *frac, int *below,
+                         int *above) {
+    int i;
+    if (isnan(x)) {
+        i = n; /* NaN sorts last in searchsorted */
+    } else {
+        int lo = 0, hi = n; /* searchsorted side="left" */
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (grid[mid] < x) lo = mid + 1; else hi = mid;
+        }
+        i = lo;
+    }
+    if (i < 1) i = 1;
+    if (i > n - 1) i = n - 1;
+    *idx = i;
+    *frac = (x - grid[i - 1]) / (grid[i] - grid[i - 1]);
+    *below = x <= grid[0];
+    *above = x >= grid[n - 1];
+}
+
+/* cxr/_kernels.py:495-506 */
+static double gather1(const double *f, int n, int idx, double frac, int below, int above) {
+    double f0 = f[idx - 1];
+    double y = f0 + frac * (f[idx] - f0);
+    if (below) y = f[0];
+    if (above) y = f[n - 1];
+    return y;
+}
+
+/* cxr/_kernels.py:352-366 */
+static double log_interp_fraction(double x, const double *grid, int idx) {
+    double x0 = grid[idx - 1], x1 = grid[idx];
+    double bx = fmin(fmax(x, x0), x1);
+    if (isnan(x)) bx = x;
+    return log1p((bx - x0) / x0) / log1p((x1 - x0) / x0);
+}
+
+/* segment_escape.py:276-289 */
+double or_mean_transmission(double t0, double t1) {
+    double lo = fmin(t0, t1);
+    if (isnan(t0) || isnan(t1)) lo = NAN;
+    double d = fabs(t1 - t0);
+    double safe = d > 1.0e-4 ? d : 1.0;
+    double ratio = d > 1.0e-4 ? -expm1(-safe) / safe : 1.0 - 0.5 * d + d * d / 6.0;
+    return exp(-lo) * ratio;
+}
+
+/* cxr/_recoil.py:35-76 */
+void or_quantum_line_factors(double h, double gamma, double vdg, double k_dot_v, double k_dot_g,
+                             double g2, double k2, double v_dot_e, double g_dot_e, double k_dot_e,
+                             double *pxr_num, double *f_cbs) {
+    double gg = gamma * gamma;
+    double n_1 = h * g2 - 2.0 * gamma * vdg;
+    double n_2 = n_1 + 2.0 * h * k_dot_g;
+    double n_f = h * (g2 + 2.0 * k_dot_g + k2) - 2.0 * gamma * (vdg + k_dot_v);
+    double e_1 = sqrt(gg + h * n_1);
+    double e_2 = sqrt(gg + h * (h * k2 - 2.0 * gamma * k_dot_v));
+    double e_f = sqrt(gg + h * n_f);
+    double s_if = gamma + e_f;
+    double ge_ke = g_dot_e + k_dot_e;
+    *pxr_num = (-n_f * ge_ke - k2 * (2.0 * gamma * v_dot_e - h * ge_ke)) / s_if;
+    double s_1 = e_1 + gamma;
+    double s_3 = e_1 + e_f;
+    double s_4 = gamma + e_2;
+    double x = 2.0 * gamma * v_dot_e - h * k_dot_e;
+    double sigma = s_if + e_1 + e_2;
+    *f_cbs = 2.0 * g_dot_e * s_1 / (s_3 * n_1) +
+             x * (n_1 * (n_f / s_if) * sigma - 2.0 * s_1 * s_4 * k_dot_g) / (s_3 * s_4 * n_1 * n_2);
+}
+
+/* segment_escape.py:50-75: slab escape path [Angstrom] from depth z along n. */
+static double slab_path(double z, double thickness, double nz) {
+    double inv_nz = 1.0 / fmax(fabs(nz), 1.0e-12);
+    double depth = fmin(fmax(z, 0.0), thickness);
+    return nz < 0 ? depth * inv_nz : (thickness - depth) * inv_nz;
+}
+
+void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
+                  const double *v_hat, const double *E_keV, const double *L_ang,
+                  const double *r_mid, const int64_t *elec_id, int64_t Ne, double *E_res_out,
+                  double *a_width_out, double *weight_out, uint8_t *good_out, int n_threads) {
+    const double nx = geo->n_hat[0], ny = geo->n_hat[1], nz = geo->n_hat[2];
+    const double T = geo->thickness;
+    const double h = HBARC_EV_ANG / M_E_EV;              /* cxr/_recoil.py:27-32 */
+    const double pref_c1 = 4.0 * (M_PI * M_PI) * HBARC_EV_ANG; /* cxr/_kernels.py:325 */
+    const double mec2_kev = M_E_EV / 1e3;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads > 0 ? n_threads : 1)
+    for (int64_t s = 0; s < n_seg; ++s) {
+        const double E = E_keV[s];
+        const double vhx = v_hat[3 * s], vhy = v_hat[3 * s + 1], vhz = v_hat[3 * s + 2];
+        /* cxr/_setup.py:945-1005 */
+        const double beta = or_beta_from_keV(E);
+        const double vx = beta * vhx, vy = beta * vhy, vz = beta * vhz;
+        /* cxr/_kernels.py:678-699 (_vacuum_doppler) */
+        const double gamma = 1.0 + E / mec2_kev;
+        const double one_minus_beta = 1.0 / (gamma * gamma * (1.0 + beta));
+        const double dvx = vhx - nx, dvy = vhy - ny, dvz = vhz - nz;
+        const double omc = 0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
+        const double denom_row = one_minus_beta + beta * omc;
+        const double t_L = L_ang[s] / beta;
+        /* segment_escape.py:239-270 (one linear piece on a single slab) */
+        const double half = 0.5 * L_ang[s];
+        const double z_mid = r_mid[3 * s + 2];
+        const double path0 = slab_path(z_mid - half * vhz, T, nz);
+        const double path1 = slab_path(z_mid + half * vhz, T, nz);
+        /* segment_escape.py:95-131: grad L = -z_hat / (z_hat . n), zero outside */
+        double gx = -0.0 / nz, gy = -0.0 / nz, gz = -1.0 / nz;
+        if (z_mid < 0.0 || z_mid > T) { gx = 0.0; gy = 0.0; gz = 0.0; }
+        const double grad2 = gx * gx + gy * gy + gz * gz;
+        const double v_dot_grad = vx * gx + vy * gy + vz * gz;
+        const int cxr_electron = elec_id[s] < Ne;
+        const double inv_E = HBARC_EV_ANG / (gamma * M_E_EV); /* cxr/_recoil.py:19-24 */
+        for (int g = 0; g < t->n_g; ++g) {
+            const int64_t o = s * t->n_g + g;
+            const double Gx = t->G[3 * g], Gy = t->G[3 * g + 1], Gz = t->G[3 * g + 2];
+            const double g2 = Gx * Gx + Gy * Gy + Gz * Gz;
+            const double n_dot_g = Gx * nx + Gy * ny + Gz * nz;
+            /* cxr/_block_prologue.py:18-38 + cxr/_recoil.py:79-97 */
+            const double r_num = 0.5 * g2 * inv_E;
+            const double r_den = n_dot_g * inv_E;
+            const double v_dot_g_exact = (vx * Gx + vy * Gy + vz * Gz) - r_num;
+            const double denom_vac = denom_row + r_den;
+            /* cxr/_kernels.py:702-765: three fixed-point Snell passes */
+            double denom = denom_vac, previous = denom, delta = NAN;
+            for (int pass = 0; pass < 3; ++pass) {
+                double Er = HBARC_EV_ANG * (v_dot_g_exact / denom);
+                int ix, bl, ab;
+                double fr;
+                interp_index(Er, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+                delta = gather1(t->delta, t->n_tab, ix, fr, bl, ab);
+                previous = denom;
+                denom = denom_vac - delta * v_dot_grad;
+            }
+            int settled = fabs(denom - previous) <= RESONANCE_ROOT_RTOL * fabs(denom);
+            settled = settled && (2.0 * fabs(delta) * grad2 < 1.0);
+            if (!settled) denom = NAN;
+            /* cxr/_block_prologue.py:41-50 */
+            const double n_dot_g_blk = n_dot_g + delta * (gx * Gx + gy * Gy + gz * Gz);
+            /* cxr/_kernels.py:624-655 (_cxr_kin_core) */
+            const double v_dot_g = vx * Gx + vy * Gy + vz * Gz;
+            const double omega = (v_dot_g - r_num) / denom;
+            const double k_dot_v = omega * ((1.0 - denom) + r_den);
+            const double k_dot_g = omega * n_dot_g_blk;
+            const double detuning = g2 + 2.0 * k_dot_g;
+            /* cxr/_batched.py:435-458 (_line_bracket) */
+            const double k_mag =
+                omega * sqrt(grad2 == 0.0 ? 1.0 : 1.0 - 2.0 * delta + delta * delta * grad2);
+            const double E_res = HBARC_EV_ANG * omega;
+            int keep = cxr_electron && (E_res > t->lo_keep) && (E_res > 10.0) && (E_res < t->hi_keep);
+            int ix, bl, ab;
+            double fr;
+            interp_index(E_res, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+            const double lfr = log_interp_fraction(E_res, t->E_tab, ix);
+            /* cxr/_block_prologue.py:53-62 + cxr/_recoil.py:100-118 */
+            const double slope = denom * (1.0 / (1.0 - omega * inv_E));
+            keep = keep && (denom > 0) && (omega * inv_E <= 1.0 - 1.0 / gamma);
+            /* cxr/_kernels.py:482-506,369-388: couplings and attenuation */
+            const int row = t->row_table[g];
+            const double *cr = t->chi_re + (int64_t)row * t->n_tab;
+            const double *ci = t->chi_im + (int64_t)row * t->n_tab;
+            const double *ur = t->u_re + (int64_t)row * t->n_tab;
+            const double *ui = t->u_im + (int64_t)row * t->n_tab;
+            const double chi_re = gather1(cr, t->n_tab, ix, fr, bl, ab);
+            const double chi_im = gather1(ci, t->n_tab, ix, fr, bl, ab);
+            const double u_re = gather1(ur, t->n_tab, ix, fr, bl, ab);
+            const double u_im = gather1(ui, t->n_tab, ix, fr, bl, ab);
+            double mu = 0.0;
+            for (int el = 0; el < t->n_mu; ++el) {
+                const double *lm = t->log_mu + (int64_t)el * t->n_tab;
+                double f0 = lm[ix - 1];
+                double v = exp(f0 + lfr * (lm[ix] - f0));
+                if (bl) v = exp(lm[0]);
+                if (ab) v = exp(lm[t->n_tab - 1]);
+                mu += v;
+            }
+            /* cxr/_batched.py:789-826 + cxr/_line_amplitude.py:14-37 */
+            double A2 = 0.0;
+            for (int pol = 0; pol < 2; ++pol) {
+                const double *Ev = pol == 0 ? t->ES + 3 * g : t->EP + 3 * g;
+                const double ex = Ev[0], ey = Ev[1], ez = Ev[2];
+                const double g_dot_e = Gx * ex + Gy * ey + Gz * ez;
+                const double v_dot_e = vx * ex + vy * ey + vz * ez;
+                const double k_dot_e = omega * delta * (gx * ex + gy * ey + gz * ez);
+                double pxr_num, f_cbs;
+                or_quantum_line_factors(h, gamma, v_dot_g, k_dot_v, k_dot_g, g2, k_mag * k_mag,
+                                        v_dot_e, g_dot_e, k_dot_e, &pxr_num, &f_cbs);
+                const double f_pxr = pxr_num / detuning;
+                const double re = chi_re * f_pxr + u_re * f_cbs;
+                const double im = chi_im * f_pxr + u_im * f_cbs;
+                const double a2 = re * re + im * im;
+                A2 = pol == 0 ? a2 : A2 + a2;
+            }
+            /* cxr/_batched.py:702-730 + cxr/_kernels.py:658-668 */
+            const double T_abs = or_mean_transmission(path0 * mu, path1 * mu);
+            const double pref = ALPHA_FS * omega / pref_c1 * (t_L * t_L) * T_abs;
+            const double a_width = slope * t_L / (2.0 * HBARC_EV_ANG) * 1.0;
+            const double weight = pref * A2 * t->WM[g];
+            const int good = keep && isfinite(weight) && (weight > 0);
+            E_res_out[o] = E_res;
+            a_width_out[o] = a_width;
+            weight_out[o] = weight;
+            good_out[o] = (uint8_t)good;
+        }
+    }
+}
+
+/* ---- line reductions ---------------------------------------------------- */
+
+void or_reduce_node(int64_t n_lines, const double *E_res, const double *a_width,
+                    const double *weight, int64_t n_e, const double *E_grid, double *spec,
+                    int n_threads) {
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : 1)
+    for (int64_t e = 0; e < n_e; ++e) {
+        const double E = E_grid[e];
+        double acc = 0.0;
+        for (int64_t j = 0; j < n_lines; ++j) {
+            double x = a_width[j] * (E - E_res[j]) / M_PI;
+            if (x == 0.0) x = 1.0e-20;
+            double y = M_PI * x;
+            double s = sin(y) / y;
+            acc += weight[j] * (s * s);
+        }
+        spec[e] += acc;
+    }
+}
+
+/* Si(t) - pi/2 for t >= 0: power series below t = 4, else the continued
+ * fraction of E1(i t) evaluated by the modified Lentz method (Numerical
+ * Recipes, "cisi"), with E1(i t) = -Ci(t) + i (Si(t) - pi/2). */
+double or_si_minus_half_pi(double t) {
+    if (t <= 4.0) {
+        double t2 = t * t, term = t, sum = t;
+        for (int k = 1; k < 40; ++k) {
+            term *= -t2 / ((2.0 * k) * (2.0 * k + 1.0));
+            double add = term / (2.0 * k + 1.0);
+            sum += add;
+            if (fabs(add) < 1e-18 * fabs(sum)) break;
+        }
+        return sum - 0.5 * M_PI;
+    }
+    /* b = 1 + i t; h = 1/b; c = big; d = 1/b */
+    double br = 1.0, bi = t;
+    double den = br * br + bi * bi;
+    double dr = br / den, di = -bi / den;
+    double hr = dr, hi = di;
+    double cr = 1e300, ci = 0.0;
+    for (int i = 2; i < 400; ++i) {
+        double a = -(double)(i - 1) * (double)(i - 1);
+        br += 2.0;
+        /* d = 1 / (a d + b) */
+        double xr = a * dr + br, xi = a * di + bi;
+        den = xr * xr + xi * xi;
+        dr = xr / den;
+        di = -xi / den;
+        /* c = b + a / c */
+        den = cr * cr + ci * ci;
+        double qr = a * cr / den, qi = -a * ci / den;
+        cr = br + qr;
+        ci = bi + qi;
+        double delr = cr * dr - ci * di, deli = cr * di + ci * dr;
+        double nhr = hr * delr - hi * deli, nhi = hr * deli + hi * delr;
+        hr = nhr;
+        hi = nhi;
+        if (fabs(delr - 1.0) + fabs(deli) < 1e-16) break;
+    }
+    /* E1(i t) = (cos t - i sin t) h */
+    double c = cos(t), s = sin(t);
+    double e_im = c * hi - s * hr;
+    return e_im;
+}
+
+/* R(x) = F(x) - sign(x)/2 with F(x) = Si(2 pi x)/pi - x sinc^2(x), the
+ * integral of sinc^2 from 0 (cxr/_bin_quadrature.py:351-375). */
+double or_sincsq_tail(double x) {
+    double u = fabs(x);
+    double t = 2.0 * M_PI * u;
+    double s = u == 0.0 ? 1.0 : sin(M_PI * u) / (M_PI * u);
+    double r = or_si_minus_half_pi(t) / M_PI - u * s * s;
+    return x >= 0.0 ? r : -r;
+}
+
+void or_reduce_binmean(int64_t n_lines, const double *E_res, const double *a_width,
+                       const double *weight, int64_t n_bins, const double *edges, double *spec,
+                       int n_threads) {
+    double *partial = (double *)calloc((size_t)n_bins, sizeof(double));
+#pragma omp parallel num_threads(n_threads > 0 ? n_threads : 1)
+    {
+        double *local = (double *)calloc((size_t)n_bins, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t j = 0; j < n_lines; ++j) {
+            const double a = a_width[j], Er = E_res[j], w = weight[j];
+            double x_lo = a * (edges[0] - Er) / M_PI;
+            double r_lo = or_sincsq_tail(x_lo);
+            for (int64_t b = 0; b < n_bins; ++b) {
+                double x_hi = a * (edges[b + 1] - Er) / M_PI;
+                double r_hi = or_sincsq_tail(x_hi);
+                double mass = r_hi - r_lo + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
+                double mean = mass * (M_PI / a) / (edges[b + 1] - edges[b]);
+                local[b] += w * mean;
+                x_lo = x_hi;
+                r_lo = r_hi;
+            }
+        }
+#pragma omp critical
+        for (int64_t b = 0; b < n_bins; ++b) partial[b] += local[b];
+        free(local);
+    }
+    for (int64_t b = 0; b < n_bins; ++b) spec[b] += partial[b];
+    free(partial);
+}
+
+/* ---- Bethe-Heitler + Elwert (spectrum/brem.py:431-479) ------------------ */
+#define R_E_CM2 7.9407877e-26
+#define BREM_MC2_KEV 510.99895
+
+static double brem_dsigma_dk(double T_i, double k_keV, double Z) {
+    double mc2 = BREM_MC2_KEV;
+    double T_f = T_i - k_keV;
+    int ok = (T_f > 1e-6) && (k_keV > 0.0);
+    if (!ok) return 0.0;
+    double p_i = sqrt(T_i * (T_i + 2.0 * mc2)) / mc2;
+    double p_f = sqrt(T_f * (T_f + 2.0 * mc2)) / mc2;
+    double beta_i = p_i / (1.0 + T_i / mc2);
+    double beta_f = p_f / (1.0 + T_f / mc2);
+    double born_log = log((p_i + p_f) / fmax(p_i - p_f, 1e-30));
+    double elwert = beta_i / beta_f * (1.0 - exp(-2.0 * M_PI * Z * ALPHA_FS / beta_i)) /
+                    (1.0 - exp(-2.0 * M_PI * Z * ALPHA_FS / beta_f));
+    return 16.0 / 3.0 * ALPHA_FS * R_E_CM2 * (Z * Z) / fmax(k_keV * 1e3, 1e-30) / (p_i * p_i) *
+           born_log * elwert;
+}
+
+void or_brem_spectrum(int64_t n_seg, const double *E_keV, const double *L_ang,
+                      const double *r_mid, const double *v_hat, int n_el, const double *Z,
+                      const double *n_ang3, double thickness, const double n_hat[3], int64_t n_e,
+                      const double *E_grid, const double *mu_grid, double *spec, int n_threads) {
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : 1)
+    for (int64_t e = 0; e < n_e; ++e) {
+        const double k = E_grid[e] / 1e3;
+        double acc = 0.0;
+        for (int64_t s = 0; s < n_seg; ++s) {
+            const double half = 0.5 * L_ang[s];
+            const double z = r_mid[3 * s + 2];
+            const double p0 = slab_path(z - half * v_hat[3 * s + 2], thickness, n_hat[2]);
+            const double p1 = slab_path(z + half * v_hat[3 * s + 2], thickness, n_hat[2]);
+            const double T_abs = or_mean_transmission(p0 * mu_grid[e], p1 * mu_grid[e]);
+            const double path_cm = L_ang[s] * 1e-8;
+            for (int el = 0; el < n_el; ++el) {
+                double d = brem_dsigma_dk(E_keV[s], k, Z[el]);
+                acc += (n_ang3[el] * 1e24 * 1.0 * path_cm) * (d * T_abs);
+            }
+        }
+        spec[e] += acc;
+    }
+}

@@ -1,0 +1,301 @@
+/*
+ * CPU ORACLE -- test infrastructure, never the product.
+ *
+ * Plain-C restatement of the reference's per-electron transport core with the
+ * data-free physics set (screened-Rutherford elastic, spliced Joy-Luo /
+ * Berger-Seltzer stopping, midpoint energy rule, no straggling, no
+ * substeps), used by the tests as the checker for the CUDA transport kernel
+ * and by bench.py as the timed CPU baseline. Each block cites the reference
+ * lines it follows (paths relative to the reference project root).
+ *
+ * Parity: pinned bit for bit against rows produced by the reference itself
+ * (tests/golden/transport_*.npz, made by tests/golden/make_golden.py).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "oracle.h"
+
+/* ---- counter RNGs ------------------------------------------------------ */
+
+/* SplitMix64 finalizer: src/pyrite/montecarlo/transport/kinematics.py:205-211 */
+uint64_t or_splitmix64(uint64_t x) {
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+
+/* kinematics.py:219-222: key_e = sm64(seed + phi (e + 1)) */
+uint64_t or_stream_key(uint64_t seed, uint64_t elec) {
+    return or_splitmix64(seed + 0x9E3779B97F4A7C15ULL * (elec + 1ULL));
+}
+
+/* kinematics.py:225-229: u = (sm64(key + phi (c + 1)) >> 11) 2^-53 */
+double or_stream_uniform(uint64_t key, uint64_t counter) {
+    uint64_t z = or_splitmix64(key + 0x9E3779B97F4A7C15ULL * (counter + 1ULL));
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Random123 Philox4x32-10 (Salmon et al., SC11), round mapping as in
+ * src/pyrite/montecarlo/channeling/_axial_cuda_rng.py:17-43. */
+void or_philox4x32_10(uint32_t ctr[4], uint32_t key[2]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = 0xD2511F53ULL * (uint64_t)c0;
+        uint64_t p1 = 0xCD9E8D57ULL * (uint64_t)c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+        k0 += 0x9E3779B9U;
+        k1 += 0xBB67AE85U;
+    }
+    ctr[0] = c0; ctr[1] = c1; ctr[2] = c2; ctr[3] = c3;
+}
+
+/* Draw ``draw`` of the Philox stream with 64-bit key ``key``: block draw/2 is
+ * the counter, even draws use words (0,1), odd draws (2,3), 53-bit mantissa. */
+double or_philox_uniform(uint64_t key, uint64_t draw) {
+    uint64_t block = draw >> 1;
+    uint32_t ctr[4] = {(uint32_t)block, (uint32_t)(block >> 32), 0u, 0u};
+    uint32_t k[2] = {(uint32_t)key, (uint32_t)(key >> 32)};
+    or_philox4x32_10(ctr, k);
+    uint32_t a = (draw & 1ULL) ? ctr[2] : ctr[0];
+    uint32_t b = (draw & 1ULL) ? ctr[3] : ctr[1];
+    return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) / 9007199254740992.0;
+}
+
+static double draw_uniform(int rng_kind, uint64_t key, uint64_t counter) {
+    return rng_kind == OR_RNG_PHILOX ? or_philox_uniform(key, counter)
+                                     : or_stream_uniform(key, counter);
+}
+
+/* ---- physics leaves ------------------------------------------------------ */
+
+#define MC2_KEV 510.99895
+#define LN2 0.6931471805599453
+#define BS_PREFACTOR 1.535e-6
+
+/* kinematics.py:162-166 */
+double or_beta_from_keV(double E) {
+    double g = 1.0 + E / 510.99895;
+    double gis = 1.0 / (g * g);
+    return sqrt(1.0 - gis);
+}
+
+/* stopping.py:384-410, _dEds_spliced_packed_scalar (delta = 0) */
+double or_dEds_spliced(const or_layers *ly, int L, double E) {
+    double tau = E / MC2_KEV;
+    double gamma = 1.0 + tau;
+    double beta_sq = 1.0 - 1.0 / (gamma * gamma);
+    double f_minus = 1.0 - beta_sq + (tau * tau / 8.0 - (2.0 * tau + 1.0) * LN2) / (gamma * gamma);
+    double jl = 0.0, bs = 0.0;
+    int n_el = ly->n_el[L];
+    for (int i = 0; i < n_el; ++i) {
+        int ix = L * ly->max_el + i;
+        double J = ly->J[ix], coeff = ly->coeff[ix];
+        if (E < ly->E_cross[ix]) {
+            jl += coeff * log(1.166 * (E + ly->k[ix] * J) / J);
+        } else {
+            double I_rel = J / MC2_KEV;
+            bs += coeff * (log(tau * tau * (tau + 2.0) / (2.0 * I_rel * I_rel)) + f_minus - 0.0);
+        }
+    }
+    return -7.85e-4 / E * jl - BS_PREFACTOR / beta_sq * bs;
+}
+
+/* scattering.py:208-218, _scatter_rates_sr_scalar [1/cm] */
+double or_sr_rate(double E, double sr_rate_numer, double sr_joy_numer) {
+    double a = sr_joy_numer / E;
+    double p511 = E + 511.0;
+    double p1024 = E + 1024.0;
+    double r = p511 / p1024;
+    return sr_rate_numer / (E * E) / (a * (1.0 + a)) * (r * r);
+}
+
+/* scattering.py:234-236 */
+double or_cos_theta_sr(double alpha, double R) { return 1.0 - 2.0 * alpha * R / (1.0 + alpha - R); }
+
+/* core_geometry.py:16-35, _rotate_direction_scalar */
+void or_rotate(double *dx, double *dy, double *dz, double cos_t, double phi) {
+    double st2 = 1.0 - cos_t * cos_t;
+    double sin_t = sqrt(st2 > 0.0 ? st2 : 0.0);
+    double cp = cos(phi), sp = sin(phi);
+    double refx, refy;
+    if (fabs(*dx) < 0.9) { refx = 1.0; refy = 0.0; } else { refx = 0.0; refy = 1.0; }
+    double ux = -(*dz) * refy, uy = (*dz) * refx, uz = (*dx) * refy - (*dy) * refx;
+    double um = sqrt(ux * ux + uy * uy + uz * uz);
+    ux /= um; uy /= um; uz /= um;
+    double wx = (*dy) * uz - (*dz) * uy, wy = (*dz) * ux - (*dx) * uz, wz = (*dx) * uy - (*dy) * ux;
+    double a = sin_t * cp, b = sin_t * sp;
+    double ox = cos_t * (*dx) + a * ux + b * wx;
+    double oy = cos_t * (*dy) + a * uy + b * wy;
+    double oz = cos_t * (*dz) + a * uz + b * wz;
+    double m = sqrt(ox * ox + oy * oy + oz * oz);
+    *dx = ox / m; *dy = oy / m; *dz = oz / m;
+}
+
+/* core_geometry.py:78-86, searchsorted(side="right") over the internal bounds */
+static int layer_of(const or_layers *ly, double z) {
+    int n = ly->n_layers - 1, lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (ly->z_top[mid + 1] <= z) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+/* ---- the per-electron event loop ----------------------------------------
+ * cores.py:379-1230 with per_electron=True, lut=False, grooved=False,
+ * inelastic=False, radiative=False, mixed=False, cone_split=False,
+ * elastic_model_code=0 (SR), energy_model_code=1 (midpoint), straggling off,
+ * max_dE_frac=0, infinite lateral footprint. With spliced stopping the lazy
+ * cutoff bound is never armed (_jit_cutoff_bound.py:47-56), so the midpoint
+ * cutoff solve always runs.
+ */
+void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t elec, double E_cut,
+                      int64_t max_steps, int64_t cap, double *pos, double *dir, double *E_io,
+                      double *clock_io, or_rows *rows, int64_t row_base, int64_t *seg_count,
+                      int8_t *exit_code) {
+    double px = pos[0], py = pos[1], pz = pos[2];
+    double dx = dir[0], dy = dir[1], dz = dir[2];
+    double E = *E_io, clk = *clock_io;
+    double tau_left = -1.0;
+    uint64_t draws = 0;
+    int64_t nseg = 0, flight = 0, steps = 0;
+    int8_t code = OR_EXIT_STEP_LIMITED;
+    const double EPS = 1e-6;
+    double z_total = ly->z_bot[ly->n_layers - 1];
+    while (steps < max_steps) {
+        int L = ly->n_layers == 1 ? 0 : layer_of(ly, pz);
+        int n_el = ly->n_el[L];
+        double z_top = ly->z_top[L], z_bot = ly->z_bot[L];
+        const double E_j = E;
+        double total_rate = 0.0;
+        for (int i = 0; i < n_el; ++i) {
+            int ix = L * ly->max_el + i;
+            total_rate += or_sr_rate(E_j, ly->sr_rate_numer[ix], ly->sr_joy_numer[ix]);
+        }
+        double lam = 1e8 / total_rate;
+        if (tau_left < 0.0) {
+            tau_left = -log(draw_uniform(rng_kind, key, draws));
+            draws += 1;
+        }
+        double step = tau_left * lam;
+        int cross_up = 0, cross_dn = 0;
+        if (dz < 0.0) {
+            double sb = (pz - z_top) / (-dz);
+            if (step > sb) { step = sb; cross_up = 1; }
+        } else if (dz > 0.0) {
+            double sb = (z_bot - pz) / dz;
+            if (step > sb) { step = sb; cross_dn = 1; }
+        }
+        int exit_top = cross_up && z_top <= 0.0;
+        int exit_bot = cross_dn && z_bot >= z_total;
+        double dEds = or_dEds_spliced(ly, L, E_j);
+        int geometry_event = cross_up || cross_dn;
+        int cutoff = 0;
+        /* cores.py:734-776: midpoint cutoff distance */
+        double cutoff_rate = or_dEds_spliced(ly, L, 0.5 * (E_j + E_cut));
+        double cutoff_distance = (E_cut - E_j) / cutoff_rate;
+        if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
+            step = cutoff_distance;
+            cutoff = 1;
+            cross_up = cross_dn = exit_top = exit_bot = 0;
+        }
+        /* cores.py:783-809: midpoint (RK2) end energy and clock */
+        double E_end;
+        if (cutoff) {
+            E_end = E_cut;
+        } else {
+            double E_pred = E_j + dEds * step;
+            double E_mid = 0.5 * (E_j + E_pred);
+            E_end = E_j + step * or_dEds_spliced(ly, L, E_mid);
+        }
+        double t_end = clk + step / or_beta_from_keV(0.5 * (E_j + E_end));
+        int8_t event;
+        if (cutoff) event = OR_EVENT_CUTOFF;
+        else if (exit_top) event = OR_EVENT_EXIT_TOP;
+        else if (exit_bot) event = OR_EVENT_EXIT_BOTTOM;
+        else if (cross_up || cross_dn) event = OR_EVENT_LAYER_BOUNDARY;
+        else event = OR_EVENT_ELASTIC;
+        /* cores.py:911-935: row written to slot i*cap + s while it fits */
+        if (rows && nseg < cap) {
+            int64_t s = row_base + nseg;
+            rows->v_hat[3 * s + 0] = dx; rows->v_hat[3 * s + 1] = dy; rows->v_hat[3 * s + 2] = dz;
+            rows->r_mid[3 * s + 0] = px + 0.5 * step * dx;
+            rows->r_mid[3 * s + 1] = py + 0.5 * step * dy;
+            rows->r_mid[3 * s + 2] = pz + 0.5 * step * dz;
+            rows->L[s] = step;
+            rows->E_start[s] = E_j;
+            rows->E_end[s] = E_end;
+            rows->t_start[s] = clk;
+            rows->t_end[s] = t_end;
+            rows->elec_id[s] = elec;
+            rows->layer[s] = (int16_t)L;
+            rows->flight[s] = flight;
+            rows->event[s] = event;
+        }
+        nseg += 1;
+        px = px + step * dx; py = py + step * dy; pz = pz + step * dz;
+        E = E_end;
+        clk = t_end;
+        tau_left -= step / lam;
+        if (tau_left < 0.0) tau_left = 0.0;
+        /* cores.py:1060-1066: every row closes the flight and resets tau */
+        flight += 1;
+        tau_left = -1.0;
+        if (exit_top || exit_bot || cutoff) {
+            code = exit_top ? OR_EXIT_BACKSCATTERED : exit_bot ? OR_EXIT_TRANSMITTED : OR_EXIT_CUTOFF;
+            break;
+        }
+        if (cross_up || cross_dn) {
+            pz += (dz > 0.0 ? 1.0 : -1.0) * EPS;
+            steps += 1;
+            continue;
+        }
+        /* cores.py:1082-1141: element by partial rate at the row-start energy,
+         * SR screening at the post-step energy, then two angle draws. */
+        int i_el = 0;
+        if (n_el > 1) {
+            double u = draw_uniform(rng_kind, key, draws) * total_rate;
+            draws += 1;
+            double cum = 0.0;
+            i_el = n_el - 1;
+            for (int k = 0; k < n_el; ++k) {
+                int ix = L * ly->max_el + k;
+                cum += or_sr_rate(E_j, ly->sr_rate_numer[ix], ly->sr_joy_numer[ix]);
+                if (cum > u) { i_el = k; break; }
+            }
+        }
+        double alpha = ly->sr_joy_numer[L * ly->max_el + i_el] / E;
+        double cos_u = draw_uniform(rng_kind, key, draws);
+        draws += 1;
+        double phi_u = draw_uniform(rng_kind, key, draws);
+        draws += 1;
+        double cos_t = or_cos_theta_sr(alpha, cos_u);
+        or_rotate(&dx, &dy, &dz, cos_t, 2.0 * M_PI * phi_u);
+        steps += 1;
+    }
+    pos[0] = px; pos[1] = py; pos[2] = pz;
+    dir[0] = dx; dir[1] = dy; dir[2] = dz;
+    *E_io = E;
+    *clock_io = clk;
+    *seg_count = nseg;
+    *exit_code = code;
+}
+
+void or_transport(const or_layers *ly, int rng_kind, uint64_t seed, int64_t e_start, int64_t n,
+                  double E_cut, int64_t max_steps, int64_t cap, double *pos, double *dir, double *E,
+                  double *clock, or_rows *rows, int64_t *seg_count, int8_t *exit_code, int n_threads) {
+#pragma omp parallel for schedule(dynamic, 16) num_threads(n_threads > 0 ? n_threads : 1)
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t key = or_stream_key(seed, (uint64_t)(e_start + i));
+        or_transport_one(ly, rng_kind, key, e_start + i, E_cut, max_steps, cap, pos + 3 * i,
+                         dir + 3 * i, E + i, clock + i, rows, i * cap, seg_count + i, exit_code + i);
+    }
+}

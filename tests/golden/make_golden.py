@@ -1,0 +1,311 @@
+"""Generate the golden vectors the oracle is pinned against, by running the reference.
+
+Run from the repository root, in a container that holds the reference tree::
+
+    python tests/golden/make_golden.py [--only NAME ...]
+
+It imports PyRITE v0.36.2 through ``oracle.ref_harness`` (stand-ins for the
+absent third-party packages; ``PYRITE_MC_BACKEND=cpu``) and calls the
+reference's own CPU functions on seeded inputs. Every fixture stores the
+inputs it was made from next to the reference's outputs, so the tests never
+need the reference at run time. Data the reference would read from absent
+tables (EPDL attenuation, Chantler refraction, the CXR tabulation mesh) is
+injected through the reference's own module seams with the smooth analytic
+tables of ``synthetic_tables`` below; the arithmetic that consumes them is
+the reference's.
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from oracle.ref_harness import import_reference  # noqa: E402
+
+import_reference()
+
+from pyrite.montecarlo import geometry as ref_geometry  # noqa: E402
+from pyrite.montecarlo.transport import TransportLUTConfig, _simulate_trajectories  # noqa: E402
+from pyrite.montecarlo.transport import kinematics as ref_kin  # noqa: E402
+from pyrite.montecarlo.transport import scattering as ref_scat  # noqa: E402
+from pyrite.montecarlo.transport import stopping as ref_stop  # noqa: E402
+
+
+def _save(name, **arrays):
+    path = OUT / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path.relative_to(ROOT)} ({path.stat().st_size / 1024:.1f} KiB)")
+
+
+# ---------------------------------------------------------------------------
+# RNG: SplitMix64 counter stream (pyrite/montecarlo/transport/kinematics.py:205-246)
+# and the Philox4x32-10 published vector quoted by the reference's tests.
+# ---------------------------------------------------------------------------
+def gen_rng():
+    xs = np.array([0, 1, 2, 3, 2**32 - 1, 2**63 + 7, 2**64 - 1], dtype=np.uint64)
+    sm = np.array([int(ref_kin._splitmix64(np.uint64(x))) for x in xs], dtype=np.uint64)
+    keys = ref_kin.stream_keys(7, 64)
+    keys_block = ref_kin.stream_keys(7, 16, start=100)
+    pairs = []
+    for elec in (0, 1, 4095, 123456789):
+        key = int(ref_kin._stream_key_scalar(3, elec))
+        for counter in (0, 1, 2, 997, 10**6):
+            u = ref_kin._stream_uniform_scalar(np.uint64(key), np.uint64(counter))
+            pairs.append((elec, counter, key, u))
+    pairs = np.array(pairs, dtype=object)
+    cu = ref_kin.counter_uniforms(np.uint64(2**40 + 5), 8, 3, start=11)
+    # Random123 Philox4x32-10, counter = key = 0 (tests/montecarlo/quantum/
+    # test_channeling_axial_cuda.py:129).
+    philox_words = np.array([0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8], dtype=np.uint32)
+    _save(
+        "rng",
+        splitmix_in=xs,
+        splitmix_out=sm,
+        stream_keys_seed7=keys,
+        stream_keys_seed7_start100=keys_block,
+        uniform_elec=pairs[:, 0].astype(np.int64),
+        uniform_counter=pairs[:, 1].astype(np.int64),
+        uniform_key=np.array([int(k) for k in pairs[:, 2]], dtype=np.uint64),
+        uniform_value=pairs[:, 3].astype(np.float64),
+        counter_uniforms_root=np.uint64(2**40 + 5),
+        counter_uniforms_out=cu,
+        philox_zero_words=philox_words,
+    )
+
+
+# ---------------------------------------------------------------------------
+# Transport physics leaves (scattering.py:208,114,234; stopping.py:384)
+# ---------------------------------------------------------------------------
+def _layer_coefficients(composition):
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+
+    rows = []
+    for el, n in composition:
+        p = TRANSPORT_ELEMENTS[el]
+        Z, A, J = float(p["Z"]), float(p["A"]), float(p["J_keV"])
+        rows.append(
+            dict(
+                el=el,
+                Z=Z,
+                A=A,
+                J=J,
+                n=n,
+                k=0.731 + 0.0688 * np.log10(Z),
+                coeff=(n / 0.602214076) * Z,
+                E_cross=ref_stop._element_crossover_keV(el, Z, A, J),
+                sr_rate_numer=5.21e-21 * Z * Z * 4.0 * np.pi * (n * 1e24),
+                sr_joy_numer=3.4e-3 * Z**0.67,
+            )
+        )
+    return rows
+
+
+def gen_physics_leaves():
+    comps = {
+        "C": [("C", 0.1133)],
+        "Si": [("Si", 0.04994)],
+        "W": [("W", 0.0632)],
+        "SiO2": [("Si", 0.0227), ("O", 0.0454)],
+    }
+    E = np.geomspace(5.0, 1.2e5, 97)
+    out = {"E_keV": E}
+    for name, comp in comps.items():
+        rows = _layer_coefficients(comp)
+        J = np.array([r["J"] for r in rows])
+        k = np.array([r["k"] for r in rows])
+        coeff = np.array([r["coeff"] for r in rows])
+        Ec = np.array([r["E_cross"] for r in rows])
+        srn = np.array([r["sr_rate_numer"] for r in rows])
+        sjn = np.array([r["sr_joy_numer"] for r in rows])
+        out[f"{name}_Z"] = np.array([r["Z"] for r in rows])
+        out[f"{name}_A"] = np.array([r["A"] for r in rows])
+        out[f"{name}_J"] = J
+        out[f"{name}_n"] = np.array([r["n"] for r in rows])
+        out[f"{name}_E_cross"] = Ec
+        out[f"{name}_dEds"] = np.array(
+            [ref_stop._dEds_spliced_compound_scalar(J, k, coeff, Ec, 0.0, e) for e in E]
+        )
+        rates = np.array(
+            [[ref_scat._scatter_rates_sr_scalar(e, srn[i], sjn[i]) for i in range(len(rows))] for e in E]
+        )
+        out[f"{name}_sr_rates"] = rates
+        out[f"{name}_alpha"] = np.array([[sjn[i] / e for i in range(len(rows))] for e in E])
+    R = np.linspace(0.0, 0.999, 11)
+    alphas = np.array([1e-7, 1e-4, 0.3])
+    out["cos_R"] = R
+    out["cos_alpha"] = alphas
+    out["cos_theta"] = np.array(
+        [[ref_scat._sample_cos_theta_from_alpha(a, r) for r in R] for a in alphas]
+    )
+    _save("physics_leaves", **out)
+
+
+# ---------------------------------------------------------------------------
+# Transport, per-electron core (pyrite/montecarlo/transport/cores.py:96-1230)
+# ---------------------------------------------------------------------------
+ROW_KEYS = (
+    "r_mid",
+    "v_hat",
+    "L_ang",
+    "E_keV",
+    "E_end_keV",
+    "E_repr_keV",
+    "t_ang",
+    "t_end_ang",
+    "elec_id",
+    "layer",
+    "flight_id",
+    "event_kind",
+)
+COUNT_KEYS = (
+    "n_backscattered",
+    "n_transmitted",
+    "n_side_exited",
+    "n_cutoff_stopped",
+    "n_step_limited",
+    "n_missed",
+)
+
+TRANSPORT_CASES = {
+    # HOPG-density carbon, 20 MeV, 100 um, 45 deg tilt, 1 mm FWHM spot.
+    "c20mev": dict(
+        E0_keV=20000.0, Ne=48, layers=[(0.0, 1.0e6, [("C", 0.1133)])], seed=0,
+        tilt_deg=45.0, theta_obs_deg=90.0, beam_fwhm_mm=1.1774,
+    ),
+    # Si 50 MeV, 500 um, 10 deg tilt.
+    "si50mev": dict(
+        E0_keV=50000.0, Ne=24, layers=[(0.0, 5.0e6, [("Si", 0.04994)])], seed=3,
+        tilt_deg=10.0, theta_obs_deg=20.0, beam_fwhm_mm=2.3548,
+    ),
+    # Three-layer stack C / Si / W at 10 MeV.
+    "stack10mev": dict(
+        E0_keV=10000.0, Ne=12,
+        layers=[
+            (0.0, 2.0e5, [("C", 0.1133)]),
+            (2.0e5, 2.2e6, [("Si", 0.04994)]),
+            (2.2e6, 2.4e6, [("W", 0.0632)]),
+        ],
+        seed=5, tilt_deg=0.0, theta_obs_deg=20.0, beam_fwhm_mm=None,
+    ),
+    # Low-energy Si: backscatter and cutoff exits (the reference test BASE_CASE).
+    "si30kev": dict(
+        E0_keV=30.0, Ne=16, layers=[(0.0, 5.0e4, [("Si", 0.04996)])], seed=11,
+        tilt_deg=0.0, theta_obs_deg=119.0, beam_fwhm_mm=None,
+    ),
+    # Two-element compound: element choice by partial rate.
+    "sio2_300kev": dict(
+        E0_keV=300.0, Ne=16, layers=[(0.0, 2.0e5, [("Si", 0.0227), ("O", 0.0454)])], seed=2,
+        tilt_deg=30.0, theta_obs_deg=90.0, beam_fwhm_mm=0.5,
+    ),
+}
+
+
+def run_reference_transport(case, lut=False):
+    layers = case["layers"]
+    tp = np.deg2rad(case["tilt_deg"])
+    beam_dir, n_hat = ref_geometry.tilted_geometry(np.deg2rad(case["theta_obs_deg"]), tp, 0.0)
+    kwargs = dict(
+        E0_keV=case["E0_keV"],
+        Ne=case["Ne"],
+        thickness_ang=layers[-1][1],
+        seed=case["seed"],
+        elastic_model="sr",
+        transport_core="per-electron",
+        radiative_model="uncoupled",
+        beam_dir=beam_dir,
+        tilt_polar_rad=tp,
+        beam_fwhm_mm=case["beam_fwhm_mm"],
+        transport_lut_config=TransportLUTConfig(enabled=bool(lut)),
+    )
+    if len(layers) == 1:
+        kwargs["composition"] = layers[0][2]
+    else:
+        kwargs["layers"] = layers
+    out = _simulate_trajectories(**kwargs)
+    return out, beam_dir, n_hat
+
+
+def _pack_layers(layers):
+    z_top = np.array([l[0] for l in layers])
+    z_bot = np.array([l[1] for l in layers])
+    n_el = np.array([len(l[2]) for l in layers], dtype=np.int32)
+    syms = [[el for el, _ in l[2]] for l in layers]
+    dens = [[n for _, n in l[2]] for l in layers]
+    width = int(n_el.max())
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+
+    Z = np.zeros((len(layers), width))
+    A = np.zeros((len(layers), width))
+    J = np.zeros((len(layers), width))
+    N = np.zeros((len(layers), width))
+    for i, (ss, dd) in enumerate(zip(syms, dens)):
+        for j, (s, d) in enumerate(zip(ss, dd)):
+            p = TRANSPORT_ELEMENTS[s]
+            Z[i, j], A[i, j], J[i, j], N[i, j] = p["Z"], p["A"], p["J_keV"], d
+    return z_top, z_bot, n_el, Z, A, J, N
+
+
+def gen_transport():
+    for name, case in TRANSPORT_CASES.items():
+        out, beam_dir, n_hat = run_reference_transport(case)
+        z_top, z_bot, n_el, Z, A, J, N = _pack_layers(case["layers"])
+        E_cross = np.zeros_like(Z)
+        from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+
+        for i, layer in enumerate(case["layers"]):
+            for j, (s, _d) in enumerate(layer[2]):
+                p = TRANSPORT_ELEMENTS[s]
+                E_cross[i, j] = ref_stop._element_crossover_keV(s, float(p["Z"]), float(p["A"]), float(p["J_keV"]))
+        arrays = {k: np.asarray(out[k]) for k in ROW_KEYS}
+        counts = np.array([int(out[k]) for k in COUNT_KEYS], dtype=np.int64)
+        _save(
+            f"transport_{name}",
+            E0_keV=case["E0_keV"],
+            E_cut_keV=5.0,
+            seed=case["seed"],
+            Ne=case["Ne"],
+            beam_dir=beam_dir,
+            n_hat=n_hat,
+            z_top=z_top,
+            z_bot=z_bot,
+            n_el=n_el,
+            Z=Z,
+            A=A,
+            J=J,
+            N=N,
+            E_cross=E_cross,
+            initial_r=out["initial_r_ang"],
+            initial_v=out["initial_v_hat"],
+            initial_E=out["initial_E_keV"],
+            count_names=np.array(COUNT_KEYS),
+            counts=counts,
+            **arrays,
+        )
+
+
+GENERATORS = {
+    "rng": gen_rng,
+    "physics_leaves": gen_physics_leaves,
+    "transport": gen_transport,
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*", default=None)
+    args = ap.parse_args(argv)
+    for name, fn in GENERATORS.items():
+        if args.only and name not in args.only:
+            continue
+        fn()
+
+
+if __name__ == "__main__":
+    main()
