@@ -290,10 +290,223 @@ def gen_transport():
         )
 
 
+# ---------------------------------------------------------------------------
+# Synthetic data tables injected into the reference's CXR/brem data seams.
+# Smooth, positive, analytic; stand-ins for the absent Chantler/EPDL data.
+# ---------------------------------------------------------------------------
+def synthetic_E_tab(E_grid):
+    pad = 0.2 * (float(E_grid[-1]) - float(E_grid[0]))
+    lo, hi = max(float(E_grid[0]) - pad, 1.0), float(E_grid[-1]) + pad
+    return np.geomspace(lo, hi, 700)
+
+
+def synthetic_delta(E):
+    E = np.asarray(E, dtype=float)
+    return 4.5e-6 * (1.0e4 / (E + 500.0)) ** 2
+
+
+def synthetic_log_mu(composition, E):
+    E = np.asarray(E, dtype=float)
+    rows = []
+    for i, (el, n) in enumerate(composition):
+        scale = (1.0 + 0.7 * i) * n / 0.05
+        rows.append(np.log(scale * (2.0e-4 * (1.0e4 / E) ** 2.8 + 3.0e-7)))
+    return np.stack(rows, axis=0)
+
+
+def synthetic_mu_total(composition, E):
+    return np.exp(synthetic_log_mu(composition, E)).sum(axis=0)
+
+
+def synthetic_couplings(g_mags, E_tab):
+    E = np.asarray(E_tab, dtype=float)[None, :]
+    g = np.asarray(g_mags, dtype=float)[:, None]
+    lam2 = (1.0e4 / E) ** 2
+    chi_re = -2.5e-6 * lam2 * np.exp(-0.012 * g * g) * (1.0 + 0.05 * np.cos(3.0 * g))
+    chi_im = 0.03 * chi_re * (1.0e4 / (E + 2.0e3)) + 1.0e-9 * np.sin(g)
+    u_re = 3.0e-6 * np.exp(-0.006 * g * g) / (1.0 + 0.08 * g * g) + 0.0 * E
+    u_im = 2.0e-8 * np.cos(g) + 0.0 * E
+    return chi_re, chi_im, u_re, u_im
+
+
+CXR_CASES = {
+    # HOPG-density carbon rows at 20 MeV, 45 deg tilt, 90 deg detector,
+    # fibre (00l) rows, Gauss-Hermite mosaic; grid 1-40 keV in 50 eV steps.
+    "hopg20": dict(
+        transport="c20mev", crystal="hopg", absorber="C", surface_hkl=(0, 0, 1),
+        hkl=[(0, 0, l) for l in range(-8, 9) if l != 0],
+        mosaic_fwhm_deg=0.4 * 2.3548200450309493, mosaic_nodes=3,
+        E_grid=np.arange(1000.0, 40000.0 + 1e-6, 50.0),
+    ),
+    # Si rows at 50 MeV, (220) cut, 10 deg tilt, 20 deg detector, perfect
+    # crystal; grid 1-60 keV in 2048 nodes.
+    "si50": dict(
+        transport="si50mev", crystal="silicon", absorber="Si", surface_hkl=(2, 2, 0),
+        hkl="diamond<=4", mosaic_fwhm_deg=None, mosaic_nodes=1,
+        E_grid=np.linspace(1000.0, 60000.0, 2048),
+    ),
+}
+
+
+def _diamond_hkls(hmax):
+    out = []
+    r = range(-hmax, hmax + 1)
+    for h in r:
+        for k in r:
+            for l in r:
+                if (h, k, l) == (0, 0, 0):
+                    continue
+                odd = h % 2 and k % 2 and l % 2
+                even = (h % 2 == 0) and (k % 2 == 0) and (l % 2 == 0) and (h + k + l) % 4 == 0
+                if odd or even:
+                    out.append((h, k, l))
+    return out
+
+
+def gen_cxr():
+    from pyrite.materials.crystal import CRYSTALS, reciprocal_g_vector
+    from pyrite.montecarlo.spectrum.cxr import _batched, _setup
+    from pyrite.montecarlo.spectrum.cxr._spectrum import mc_cxr_spectrum
+
+    for name, case in CXR_CASES.items():
+        tr = np.load(OUT / f"transport_{case['transport']}.npz")
+        seg = {
+            "r_mid": tr["r_mid"], "v_hat": tr["v_hat"], "L_ang": tr["L_ang"],
+            "E_keV": tr["E_keV"], "E_repr_keV": tr["E_repr_keV"], "elec_id": tr["elec_id"],
+            "Ne": int(tr["Ne"]), "thickness_ang": float(tr["z_bot"][-1]),
+        }
+        info = CRYSTALS[case["crystal"]]
+        hkl = _diamond_hkls(4) if case["hkl"] == "diamond<=4" else case["hkl"]
+        g_mags = np.array([reciprocal_g_vector(h, info["lattice"])[1] for h in hkl])
+        E_grid = case["E_grid"]
+        E_tab = synthetic_E_tab(E_grid)
+        n_atoms = len(info["basis"]) / info["V_cell"]
+        comp = [(case["absorber"], n_atoms)]
+        tables = synthetic_couplings(g_mags, E_tab)
+        captured = {}
+        orig_brt = _batched._batched_reflection_tables
+
+        def capture(st, _orig=orig_brt):
+            out = _orig(st)
+            captured["rows"] = out
+            return out
+
+        patches = [
+            (_setup, "_line_tabulation_grid", lambda *a, **k: E_tab),
+            (_setup, "_elemental_log_mu_table", lambda c, E: synthetic_log_mu(c, E)),
+            (_setup, "refractive_index", lambda cr, E, uh=True: (1.0 - synthetic_delta(E)) + 0j),
+            (_batched, "_reflection_tables", lambda *a, **k: tuple(np.array(t) for t in tables)),
+            (_batched, "_batched_reflection_tables", capture),
+        ]
+        saved = [(m, n, getattr(m, n)) for m, n, _ in patches]
+        for m, n, f in patches:
+            setattr(m, n, f)
+        try:
+            common = dict(
+                crystal=case["crystal"], hkl_list=[tuple(h) for h in hkl],
+                B_ang2=float(info.get("B_ang2", 0.0) or 0.0), absorber_element=case["absorber"],
+                n_hat=tr["n_hat"], surface_hkl=case["surface_hkl"],
+                mosaic_fwhm_rad=None if case["mosaic_fwhm_deg"] is None else np.deg2rad(case["mosaic_fwhm_deg"]),
+                mosaic_nodes=case["mosaic_nodes"], node_support_cutoff=None,
+            )
+            spec_node = np.asarray(mc_cxr_spectrum(seg, E_grid, line_quadrature="node", **common))
+            spec_bin = np.asarray(mc_cxr_spectrum(seg, E_grid, line_quadrature="bin-mean", **common))
+        finally:
+            for m, n, f in saved:
+                setattr(m, n, f)
+        G, ES, EP, WM, _cr, _ci, _ur, _ui, ROW_TABLE = captured["rows"][:9]
+        _save(
+            f"cxr_{name}",
+            transport=case["transport"], crystal=case["crystal"], hkl=np.array(hkl, dtype=np.int64),
+            g_mags=g_mags, lattice_a=float(info["lattice"]["a"]),
+            n_hat=tr["n_hat"], thickness=seg["thickness_ang"], Ne=seg["Ne"],
+            surface_hkl=np.array(case["surface_hkl"]),
+            mosaic_fwhm_rad=np.nan if case["mosaic_fwhm_deg"] is None else np.deg2rad(case["mosaic_fwhm_deg"]),
+            mosaic_nodes=case["mosaic_nodes"],
+            E_grid=E_grid, E_tab=E_tab, delta=synthetic_delta(E_tab),
+            log_mu=synthetic_log_mu(comp, E_tab), absorber_n=n_atoms,
+            chi_re=tables[0], chi_im=tables[1], u_re=tables[2], u_im=tables[3],
+            G=np.asarray(G), ES=np.asarray(ES), EP=np.asarray(EP), WM=np.asarray(WM).reshape(-1),
+            row_table=np.asarray(ROW_TABLE), spec_node=spec_node, spec_binmean=spec_bin,
+        )
+
+
+def gen_brem():
+    from pyrite.montecarlo.spectrum import brem as ref_brem
+
+    for name, tname, comp_el in (("c20", "c20mev", "C"), ("sio2", "sio2_300kev", None)):
+        tr = np.load(OUT / f"transport_{tname}.npz")
+        seg = {
+            "r_mid": tr["r_mid"], "v_hat": tr["v_hat"], "L_ang": tr["L_ang"],
+            "E_keV": tr["E_keV"], "E_repr_keV": tr["E_repr_keV"], "elec_id": tr["elec_id"],
+            "Ne": int(tr["Ne"]), "thickness_ang": float(tr["z_bot"][-1]),
+        }
+        n_el = int(tr["n_el"][0])
+        comp = [(["C", "Si", "O", "W"][[6, 14, 8, 74].index(int(z))], float(n)) for z, n in zip(tr["Z"][0][:n_el], tr["N"][0][:n_el])]
+        E_grid = np.linspace(1000.0, 40000.0, 391) if comp_el else np.linspace(1000.0, 250000.0, 300)
+        saved = ref_brem._mu_total_inv_ang
+        ref_brem._mu_total_inv_ang = lambda c, E: synthetic_mu_total(c, np.asarray(E, dtype=float))
+        try:
+            spec = np.asarray(ref_brem.mc_brem_spectrum(
+                seg, E_grid, composition=comp, n_hat=tr["n_hat"],
+                cross_section_model="bethe-heitler",
+            ))
+        finally:
+            ref_brem._mu_total_inv_ang = saved
+        from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+
+        _save(
+            f"brem_{name}", transport=tname, E_grid=E_grid,
+            Z=np.array([float(TRANSPORT_ELEMENTS[e]["Z"]) for e, _ in comp]),
+            n_ang3=np.array([n for _, n in comp]),
+            mu_grid=synthetic_mu_total(comp, E_grid), n_hat=tr["n_hat"],
+            thickness=seg["thickness_ang"], Ne=seg["Ne"], spec=spec,
+        )
+
+
+def gen_cxr_leaves():
+    from pyrite.montecarlo.spectrum.cxr._bin_quadrature import sincsq_bin_masses, sincsq_tail
+    from pyrite.montecarlo.spectrum.cxr._recoil import _quantum_line_factors
+    from pyrite.montecarlo.spectrum.segment_escape import mean_transmission
+
+    rng = np.random.default_rng(344)
+    n = 64
+    args = dict(
+        h=np.full(n, 1973.269804 / 510998.95),
+        gamma=rng.uniform(10.0, 200.0, n),
+        vdg=rng.uniform(0.2, 4.0, n),
+        k_dot_v=rng.uniform(0.5, 30.0, n),
+        k_dot_g=rng.uniform(-3.0, 3.0, n),
+        g2=rng.uniform(1.0, 40.0, n),
+        k2=rng.uniform(1.0, 900.0, n),
+        v_dot_e=rng.uniform(-0.5, 0.5, n),
+        g_dot_e=rng.uniform(-3.0, 3.0, n),
+        k_dot_e=rng.uniform(-1e-3, 1e-3, n),
+    )
+    pxr, cbs = _quantum_line_factors(*args.values())
+    x = np.concatenate([np.linspace(-30.0, 30.0, 241), [1e-9, -1e-9, 0.0, 3.7e3, -8.1e4, 2.5e6]])
+    tails = sincsq_tail(x)
+    a_w = rng.uniform(0.002, 3.0, 40)
+    e_r = rng.uniform(900.0, 41000.0, 40)
+    edges = np.linspace(975.0, 40025.0, 782)
+    masses = sincsq_bin_masses(a_w, e_r, edges)
+    t0 = np.concatenate([rng.uniform(0, 5, 50), [0.3, 0.3, 2.0]])
+    t1 = np.concatenate([rng.uniform(0, 5, 50), [0.3 + 5e-5, 0.3, 2.0 + 2e-4]])
+    mt = mean_transmission(t0, t1)
+    _save(
+        "cxr_leaves", **{f"qlf_{k}": v for k, v in args.items()}, qlf_pxr=pxr, qlf_cbs=cbs,
+        tail_x=x, tail=tails, bm_a=a_w, bm_E=e_r, bm_edges=edges, bm_mass=masses,
+        mt_t0=t0, mt_t1=t1, mt=mt,
+    )
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
     "transport": gen_transport,
+    "cxr": gen_cxr,
+    "brem": gen_brem,
+    "cxr_leaves": gen_cxr_leaves,
 }
 
 
