@@ -83,6 +83,24 @@ class _Rows(C.Structure):
     ]
 
 
+class _Lut(C.Structure):
+    _fields_ = [
+        ("n_layers", C.c_int),
+        ("max_el", C.c_int),
+        ("n_energy", C.c_int),
+        ("log_E_min", C.c_double),
+        ("inv_dlogE", C.c_double),
+        ("z_top", _D),
+        ("z_bot", _D),
+        ("n_el", _I32),
+        ("total_rate", _D),
+        ("dEds", _D),
+        ("inv_beta", _D),
+        ("cdf", _D),
+        ("alpha", _D),
+    ]
+
+
 class _CxrTables(C.Structure):
     _fields_ = [
         ("n_g", C.c_int),
@@ -128,6 +146,11 @@ def _declare(L):
     L.or_transport.argtypes = [
         C.POINTER(_Layers), C.c_int, C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_int64,
         C.c_int64, _D, _D, _D, _D, C.POINTER(_Rows), _I64, _I8, C.c_int,
+    ]
+    L.or_transport_lut.restype = None
+    L.or_transport_lut.argtypes = [
+        C.POINTER(_Lut), C.c_int, C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_int64,
+        C.c_int64, _D, _D, _D, _D, C.POINTER(_Rows), _I64, _I8,
     ]
     L.or_cxr_lines.restype = None
     L.or_cxr_lines.argtypes = [
@@ -217,9 +240,30 @@ class LayerTables:
         return float(lib().or_dEds_spliced(C.byref(self.struct), int(L), float(E)))
 
 
-def transport(layers: LayerTables, pos, direction, E, *, seed, E_cut, rng=RNG_SPLITMIX,
+class LutTables:
+    """A transport LUT as ``build_transport_energy_lut`` returns it (lut.py:283-437)."""
+
+    def __init__(self, z_top, z_bot, n_el, log_E_min, inv_dlogE, total_rate, dEds, inv_beta, cdf,
+                 alpha):
+        self.z_top, self.z_bot = _f64(z_top), _f64(z_bot)
+        self.n_el = np.ascontiguousarray(n_el, dtype=np.int32)
+        self.total_rate, self.dEds = _f64(total_rate), _f64(dEds)
+        self.inv_beta, self.cdf, self.alpha = _f64(inv_beta), _f64(cdf), _f64(alpha)
+        n_layers, max_el, n_energy = self.cdf.shape
+        self.struct = _Lut(
+            n_layers, max_el, n_energy, float(log_E_min), float(inv_dlogE), _p(self.z_top, _D),
+            _p(self.z_bot, _D), _p(self.n_el, _I32), _p(self.total_rate, _D), _p(self.dEds, _D),
+            _p(self.inv_beta, _D), _p(self.cdf, _D), _p(self.alpha, _D),
+        )
+
+
+def transport(layers, pos, direction, E, *, seed, E_cut, rng=RNG_SPLITMIX,
               e_start=0, max_steps=400_000, cap=4096, keep_rows=True, clock=None):
-    """Per-electron transport of ``len(E)`` histories; returns a dict of rows and finals."""
+    """Per-electron transport of ``len(E)`` histories; returns a dict of rows and finals.
+
+    ``layers`` is a :class:`LayerTables` (the exact analytic core) or a
+    :class:`LutTables` (the reference's default LUT core).
+    """
     n = int(np.asarray(E).size)
     pos = _f64(pos).reshape(n, 3).copy()
     direction = _f64(direction).reshape(n, 3).copy()
@@ -243,12 +287,16 @@ def transport(layers: LayerTables, pos, direction, E, *, seed, E_cut, rng=RNG_SP
             _p(h["E_end"], _D), _p(h["t_start"], _D), _p(h["t_end"], _D), _p(h["elec_id"], _I64),
             _p(h["layer"], _I16), _p(h["flight"], _I64), _p(h["event"], _I8),
         )
-    lib().or_transport(
+    args = (
         C.byref(layers.struct), int(rng), C.c_uint64(int(seed) % 2**64), int(e_start), n,
         float(E_cut), int(max_steps), int(cap), _p(pos, _D), _p(direction, _D), _p(E, _D),
         _p(clock, _D), C.byref(rows) if rows is not None else None, _p(seg_count, _I64),
-        _p(exit_code, _I8), 1,
+        _p(exit_code, _I8),
     )
+    if isinstance(layers, LutTables):
+        lib().or_transport_lut(*args)
+    else:
+        lib().or_transport(*args, 1)
     out = dict(pos=pos, dir=direction, E=E, clock=clock, seg_count=seg_count, exit_code=exit_code)
     if holders is not None:
         stored = np.minimum(seg_count, cap)

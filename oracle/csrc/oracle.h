@@ -83,6 +83,28 @@ void or_transport(const or_layers *ly, int rng_kind, uint64_t seed, int64_t e_st
                   double *clock, or_rows *rows, int64_t *seg_count, int8_t *exit_code,
                   int n_threads);
 
+/* Uniform-log-energy transport LUT (src/pyrite/montecarlo/transport/lut.py:64-283). */
+typedef struct {
+    int n_layers;
+    int max_el;
+    int n_energy;
+    double log_E_min;
+    double inv_dlogE;
+    const double *z_top;      /* [n_layers] */
+    const double *z_bot;
+    const int *n_el;
+    const double *total_rate; /* [n_layers*n_energy] 1/cm */
+    const double *dEds;       /* [n_layers*n_energy] keV/Angstrom */
+    const double *inv_beta;   /* [n_energy] */
+    const double *cdf;        /* [n_layers*max_el*n_energy] */
+    const double *alpha;      /* [n_layers*max_el*n_energy] */
+} or_lut;
+
+void or_transport_lut(const or_lut *t, int rng_kind, uint64_t seed, int64_t e_start, int64_t n,
+                      double E_cut, int64_t max_steps, int64_t cap, double *pos, double *dir,
+                      double *E, double *clock, or_rows *rows, int64_t *seg_count,
+                      int8_t *exit_code);
+
 /* ---- CXR line chain (PXR + CBS, incoherent, single slab) ---------------- */
 typedef struct {
     int n_g;           /* reflection x orientation rows */

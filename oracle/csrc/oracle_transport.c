@@ -299,3 +299,172 @@ void or_transport(const or_layers *ly, int rng_kind, uint64_t seed, int64_t e_st
                          dir + 3 * i, E + i, clock + i, rows, i * cap, seg_count + i, exit_code + i);
     }
 }
+
+/* ---- the LUT core (the reference's default exact-physics path) -----------
+ * cores.py:379-1230 with lut=True: one uniform-log-energy table per layer for
+ * the total elastic rate, the stopping power and the element CDF / screening,
+ * one shared 1/beta table (lut.py:64-283), read by the closed-form index of
+ * lut.py:118-137 and linear interpolation.
+ */
+static void lut_index(const or_lut *t, double E, int *i, double *f) {
+    double x = (log(E) - t->log_E_min) * t->inv_dlogE;
+    int last = t->n_energy - 1;
+    if (x >= last) { *i = last - 1; *f = 1.0; return; }
+    if (x > 0.0) { int ii = (int)x; *i = ii; *f = x - ii; return; }
+    *i = 0; *f = 0.0;
+}
+
+static double lerp(const double *row, int i, double f) { return row[i] + f * (row[i + 1] - row[i]); }
+
+void or_transport_lut_one(const or_lut *t, int rng_kind, uint64_t key, int64_t elec, double E_cut,
+                          int64_t max_steps, int64_t cap, double *pos, double *dir, double *E_io,
+                          double *clock_io, or_rows *rows, int64_t row_base, int64_t *seg_count,
+                          int8_t *exit_code) {
+    double px = pos[0], py = pos[1], pz = pos[2];
+    double dx = dir[0], dy = dir[1], dz = dir[2];
+    double E = *E_io, clk = *clock_io;
+    double tau_left = -1.0;
+    uint64_t draws = 0;
+    int64_t nseg = 0, flight = 0, steps = 0;
+    int8_t code = OR_EXIT_STEP_LIMITED;
+    const double EPS = 1e-6;
+    const int ne = t->n_energy;
+    double z_total = t->z_bot[t->n_layers - 1];
+    while (steps < max_steps) {
+        int L = 0;
+        if (t->n_layers > 1) {
+            int n = t->n_layers - 1, lo = 0, hi = n;
+            while (lo < hi) {
+                int mid = (lo + hi) / 2;
+                if (t->z_top[mid + 1] <= pz) lo = mid + 1; else hi = mid;
+            }
+            L = lo;
+        }
+        int n_el = t->n_el[L];
+        double z_top = t->z_top[L], z_bot = t->z_bot[L];
+        const double E_j = E;
+        const double *rate_row = t->total_rate + (int64_t)L * ne;
+        const double *dEds_row = t->dEds + (int64_t)L * ne;
+        int li;
+        double lf;
+        lut_index(t, E_j, &li, &lf);
+        double total_rate = lerp(rate_row, li, lf);
+        double lam = 1e8 / total_rate;
+        if (tau_left < 0.0) {
+            tau_left = -log(draw_uniform(rng_kind, key, draws));
+            draws += 1;
+        }
+        double step = tau_left * lam;
+        int cross_up = 0, cross_dn = 0;
+        if (dz < 0.0) {
+            double sb = (pz - z_top) / (-dz);
+            if (step > sb) { step = sb; cross_up = 1; }
+        } else if (dz > 0.0) {
+            double sb = (z_bot - pz) / dz;
+            if (step > sb) { step = sb; cross_dn = 1; }
+        }
+        int exit_top = cross_up && z_top <= 0.0;
+        int exit_bot = cross_dn && z_bot >= z_total;
+        double dEds = lerp(dEds_row, li, lf);
+        int geometry_event = cross_up || cross_dn;
+        int cutoff = 0;
+        int ci;
+        double cf;
+        lut_index(t, 0.5 * (E_j + E_cut), &ci, &cf);
+        double cutoff_distance = (E_cut - E_j) / lerp(dEds_row, ci, cf);
+        if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
+            step = cutoff_distance;
+            cutoff = 1;
+            cross_up = cross_dn = exit_top = exit_bot = 0;
+        }
+        double E_end;
+        if (cutoff) {
+            E_end = E_cut;
+        } else {
+            double E_pred = E_j + dEds * step;
+            int mi;
+            double mf;
+            lut_index(t, 0.5 * (E_j + E_pred), &mi, &mf);
+            E_end = E_j + step * lerp(dEds_row, mi, mf);
+        }
+        int ki;
+        double kf;
+        lut_index(t, 0.5 * (E_j + E_end), &ki, &kf);
+        double t_end = clk + step * lerp(t->inv_beta, ki, kf);
+        int8_t event;
+        if (cutoff) event = OR_EVENT_CUTOFF;
+        else if (exit_top) event = OR_EVENT_EXIT_TOP;
+        else if (exit_bot) event = OR_EVENT_EXIT_BOTTOM;
+        else if (cross_up || cross_dn) event = OR_EVENT_LAYER_BOUNDARY;
+        else event = OR_EVENT_ELASTIC;
+        if (rows && nseg < cap) {
+            int64_t s = row_base + nseg;
+            rows->v_hat[3 * s + 0] = dx; rows->v_hat[3 * s + 1] = dy; rows->v_hat[3 * s + 2] = dz;
+            rows->r_mid[3 * s + 0] = px + 0.5 * step * dx;
+            rows->r_mid[3 * s + 1] = py + 0.5 * step * dy;
+            rows->r_mid[3 * s + 2] = pz + 0.5 * step * dz;
+            rows->L[s] = step;
+            rows->E_start[s] = E_j;
+            rows->E_end[s] = E_end;
+            rows->t_start[s] = clk;
+            rows->t_end[s] = t_end;
+            rows->elec_id[s] = elec;
+            rows->layer[s] = (int16_t)L;
+            rows->flight[s] = flight;
+            rows->event[s] = event;
+        }
+        nseg += 1;
+        px = px + step * dx; py = py + step * dy; pz = pz + step * dz;
+        E = E_end;
+        clk = t_end;
+        flight += 1;
+        tau_left = -1.0;
+        if (exit_top || exit_bot || cutoff) {
+            code = exit_top ? OR_EXIT_BACKSCATTERED : exit_bot ? OR_EXIT_TRANSMITTED : OR_EXIT_CUTOFF;
+            break;
+        }
+        if (cross_up || cross_dn) {
+            pz += (dz > 0.0 ? 1.0 : -1.0) * EPS;
+            steps += 1;
+            continue;
+        }
+        int i_el = 0;
+        if (n_el > 1) {
+            double u = draw_uniform(rng_kind, key, draws);
+            draws += 1;
+            i_el = n_el - 1;
+            for (int k = 0; k < n_el; ++k) {
+                const double *cdf = t->cdf + ((int64_t)L * t->max_el + k) * ne;
+                if (lerp(cdf, li, lf) > u) { i_el = k; break; }
+            }
+        }
+        int ai;
+        double af;
+        lut_index(t, E, &ai, &af);
+        double alpha = lerp(t->alpha + ((int64_t)L * t->max_el + i_el) * ne, ai, af);
+        double cos_u = draw_uniform(rng_kind, key, draws);
+        draws += 1;
+        double phi_u = draw_uniform(rng_kind, key, draws);
+        draws += 1;
+        or_rotate(&dx, &dy, &dz, or_cos_theta_sr(alpha, cos_u), 2.0 * M_PI * phi_u);
+        steps += 1;
+    }
+    pos[0] = px; pos[1] = py; pos[2] = pz;
+    dir[0] = dx; dir[1] = dy; dir[2] = dz;
+    *E_io = E;
+    *clock_io = clk;
+    *seg_count = nseg;
+    *exit_code = code;
+}
+
+void or_transport_lut(const or_lut *t, int rng_kind, uint64_t seed, int64_t e_start, int64_t n,
+                      double E_cut, int64_t max_steps, int64_t cap, double *pos, double *dir,
+                      double *E, double *clock, or_rows *rows, int64_t *seg_count,
+                      int8_t *exit_code) {
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t key = or_stream_key(seed, (uint64_t)(e_start + i));
+        or_transport_lut_one(t, rng_kind, key, e_start + i, E_cut, max_steps, cap, pos + 3 * i,
+                             dir + 3 * i, E + i, clock + i, rows, i * cap, seg_count + i,
+                             exit_code + i);
+    }
+}

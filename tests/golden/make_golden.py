@@ -500,10 +500,45 @@ def gen_cxr_leaves():
     )
 
 
+def gen_transport_lut():
+    """Same cases through the reference's default LUT core (lut.py, cores.py lut=True)."""
+    from pyrite.montecarlo.transport import host_pass
+
+    for name in ("c20mev", "stack10mev", "si30kev", "sio2_300kev"):
+        case = TRANSPORT_CASES[name]
+        captured = {}
+        orig = host_pass.build_transport_energy_lut
+
+        def wrapped(*a, _orig=orig, **k):
+            out = _orig(*a, **k)
+            captured["lut"] = out
+            return out
+
+        host_pass.build_transport_energy_lut = wrapped
+        try:
+            out, beam_dir, n_hat = run_reference_transport(case, lut=True)
+        finally:
+            host_pass.build_transport_energy_lut = orig
+        lut = captured["lut"]
+        arrays = {k: np.asarray(out[k]) for k in ROW_KEYS}
+        counts = np.array([int(out[k]) for k in COUNT_KEYS], dtype=np.int64)
+        _save(
+            f"transport_lut_{name}",
+            log_E_min=np.float64(lut.log_E_min), inv_dlogE=np.float64(lut.inv_dlogE),
+            n_energy=int(lut.n_energy), lut_n_el=np.asarray(lut.n_el),
+            lut_total_rate=lut.total_rate, lut_dEds=lut.dEds, lut_inv_beta=lut.inv_beta,
+            lut_cdf=lut.cdf, lut_alpha=lut.alpha, E_min_keV=np.float64(lut.E_min_keV),
+            E_max_keV=np.float64(lut.E_max_keV), initial_r=out["initial_r_ang"],
+            initial_v=out["initial_v_hat"], initial_E=out["initial_E_keV"],
+            counts=counts, **arrays,
+        )
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
     "transport": gen_transport,
+    "transport_lut": gen_transport_lut,
     "cxr": gen_cxr,
     "brem": gen_brem,
     "cxr_leaves": gen_cxr_leaves,
