@@ -1,0 +1,274 @@
+/*
+ * pyrite_b200 -- C ABI of the B200 (sm_100a) electron-transport and
+ * radiation-scoring hot path of PyRITE.
+ *
+ * Every entry point takes plain C types: device pointers the caller owns,
+ * sizes, and a CUDA stream passed as ``void *`` (NULL = the legacy default
+ * stream). Calls are stream-ordered and return an int status (PB_OK = 0);
+ * pb_last_error() returns the message of the calling thread's last failure.
+ * Device-side conditions (a step limit reached, a queue overflow, a bounded
+ * wait that gave up) are reported through the ``status`` word each call
+ * writes, never by trapping. Nothing here allocates device memory unless
+ * the function says so; workspace sizes are queried first.
+ *
+ * Reference interfaces replaced (paths relative to the PyRITE v0.36.2 tree):
+ *   pb_transport      -- the per-electron transport core call
+ *                        core((e_start, m, cap, keys), *core_args, scratch,
+ *                        (seg_count, exit_code), ...)
+ *                        src/pyrite/montecarlo/transport/batching.py:547-554,
+ *                        kernels src/pyrite/montecarlo/transport/cores.py:96
+ *                        (exact core) and lut.py:283 (LUT core); entry
+ *                        sampling transport/beam_entry.py:23 and
+ *                        transverse.py:197.
+ *   pb_cxr_score      -- the incoherent PXR+CBS line scorer for a fixed
+ *                        segment list, mc_cxr_spectrum
+ *                        src/pyrite/montecarlo/spectrum/cxr/_spectrum.py:25,
+ *                        batched route cxr/_batched.py:461-931.
+ *   pb_brem_score     -- mc_brem_spectrum, Bethe-Heitler + Elwert
+ *                        src/pyrite/montecarlo/spectrum/brem.py:829.
+ *   pb_char_yields    -- the characteristic-line chunk kernel
+ *                        src/pyrite/montecarlo/spectrum/_characteristic_chunk_kernel.py:120.
+ *   pb_mlp_*          -- BF16 MLP surrogate of the reflection sum (no
+ *                        counterpart in the reference).
+ */
+#ifndef PYRITE_B200_H
+#define PYRITE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_ABI_VERSION 1
+
+enum pb_status {
+    PB_OK = 0,
+    PB_ERR_INVALID = 1,   /* bad argument (size, pointer, enum) */
+    PB_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    PB_ERR_UNSUPPORTED = 3,
+    PB_ERR_CAPACITY = 4   /* an output buffer was too small (replay with more) */
+};
+
+/* Device status word bits (written by kernels, read by the host). */
+enum pb_device_status {
+    PB_DEV_STEP_LIMIT = 1u,      /* some history reached max_steps */
+    PB_DEV_ROW_OVERFLOW = 2u,    /* rows beyond cap were counted, not stored */
+    PB_DEV_QUEUE_OVERFLOW = 4u,  /* segment stream capacity exceeded */
+    PB_DEV_WAIT_TIMEOUT = 8u,    /* a bounded wait gave up */
+    PB_DEV_BAD_INPUT = 16u
+};
+
+enum pb_rng { PB_RNG_SPLITMIX = 0, PB_RNG_PHILOX = 1 };
+enum pb_precision { PB_FP64 = 0, PB_MIXED = 1 };
+enum pb_beam_mode { PB_BEAM_EXPLICIT = 0, PB_BEAM_SPOT = 1, PB_BEAM_TWISS = 2 };
+enum pb_quadrature { PB_QUAD_NODE = 0, PB_QUAD_BINMEAN = 1 };
+
+/* Exact analytic physics, padded per-layer element rows
+ * (transport/batching.py:33-105). Device pointers. */
+typedef struct pb_layers {
+    int32_t n_layers;
+    int32_t max_el;
+    const double *z_top;         /* [n_layers] Angstrom */
+    const double *z_bot;         /* [n_layers] */
+    const int32_t *n_el;         /* [n_layers] */
+    const double *J;             /* [n_layers*max_el] keV */
+    const double *k;
+    const double *coeff;
+    const double *E_cross;
+    const double *sr_rate_numer;
+    const double *sr_joy_numer;
+} pb_layers;
+
+/* Uniform-log-energy LUT (transport/lut.py:64-283), packed by the host into
+ * one 16-byte-aligned device buffer of ``elem_bytes``-sized values (8 for
+ * FP64, 4 for the mixed path): [total_rate L x ne | dEds L x ne |
+ * inv_beta ne | cdf L x max_el x ne | alpha L x max_el x ne], each block
+ * starting at ``off_*`` values from ``base``. */
+typedef struct pb_lut {
+    int32_t n_energy;
+    int32_t elem_bytes;
+    double log_E_min;
+    double inv_dlogE;
+    const void *base;
+    int64_t total_bytes;
+    int64_t off_total_rate, off_dEds, off_inv_beta, off_cdf, off_alpha;
+} pb_lut;
+
+/* Entrance state (transport/beam_entry.py:23-160, transverse.py:197-226,
+ * geometry.py:330-420). */
+typedef struct pb_beam {
+    int32_t mode;              /* pb_beam_mode */
+    int32_t tilted;            /* nonzero: project spot onto the tilted face */
+    double E0_keV;
+    double beam_dir[3];        /* sample frame, unit */
+    double e_x[3], e_y[3];     /* sample-frame lab spot axes */
+    double basis[9];           /* beam frame basis, row-major, columns are axes */
+    double sigma_x_ang, sigma_y_ang;  /* PB_BEAM_SPOT */
+    double twiss_x[3], twiss_y[3];    /* PB_BEAM_TWISS: eps [mm rad], beta [mm/rad], alpha */
+    uint64_t root;             /* counter-stream root of the entry draws */
+    const double *pos0;        /* PB_BEAM_EXPLICIT: [n*3], [n*3], [n] device */
+    const double *dir0;
+    const double *E0;
+} pb_beam;
+
+/* Segment rows, slot i*cap + s, exactly as the reference core writes them. */
+typedef struct pb_rows {
+    double *r_mid;
+    double *v_hat;
+    double *L;
+    double *E_start;
+    double *E_end;
+    double *t_start;
+    double *t_end;
+    int64_t *elec_id;
+    int16_t *layer;
+    int64_t *flight;
+    int8_t *event;
+} pb_rows;
+
+/* Compact segment list: the scorers' input. SoA, device. */
+typedef struct pb_segments {
+    int64_t capacity;
+    unsigned long long *count;  /* device counter (appended by pb_transport) */
+    double *r_mid;    /* [capacity*3] */
+    double *v_hat;    /* [capacity*3] */
+    double *L;
+    double *E_repr;   /* midpoint energy, keV */
+    int64_t *elec_id;
+    int32_t *layer;
+} pb_segments;
+
+/* Fused exit tallies (trajectory_summary.py:147-260): escaped primaries'
+ * exit energy and polar exit angle to sample +z, uniform bins with explicit
+ * underflow (index 0) and overflow (index n+1) slots, np.histogram edges. */
+typedef struct pb_tallies {
+    unsigned long long *fates;   /* [6] histories per exit code */
+    unsigned long long *exit_E;  /* [n_E+2] */
+    int32_t n_E;
+    double E_lo, E_hi;
+    unsigned long long *exit_theta;  /* [n_theta+2] */
+    int32_t n_theta;
+    double theta_lo, theta_hi;
+    double *deposit;             /* [n_layers] keV lost continuously, per layer */
+} pb_tallies;
+
+typedef struct pb_transport_args {
+    int32_t rng;        /* pb_rng */
+    int32_t precision;  /* pb_precision */
+    int32_t use_lut;
+    int32_t block_threads;  /* 0 = tuned default */
+    uint64_t seed;
+    int64_t e_start;    /* first global history index */
+    int64_t n;          /* histories */
+    double E_cut_keV;
+    int64_t max_steps;
+    pb_layers layers;
+    pb_lut lut;
+    pb_beam beam;
+    int64_t cap;            /* rows per history when rows.L != NULL */
+    pb_rows rows;
+    int64_t *seg_count;     /* [n] true row count (may exceed cap) */
+    int8_t *exit_code;      /* [n] */
+    double *final_pos;      /* [n*3] optional */
+    double *final_dir;      /* [n*3] optional */
+    double *final_E;        /* [n] optional */
+    pb_segments seg;        /* optional compact stream */
+    pb_tallies tallies;     /* optional (NULL pointers skip) */
+    unsigned long long *work_counter;  /* device scratch, 1 word; zeroed by the call */
+    unsigned int *status;   /* device status word (pb_device_status bits), OR-ed */
+} pb_transport_args;
+
+/* CXR reflection rows and coupling tables (cxr/_batched.py:232-331). */
+typedef struct pb_cxr_tables {
+    int32_t n_g;
+    const double *G;        /* [n_g*3] 1/Angstrom, sample frame */
+    const double *ES;       /* [n_g*3] */
+    const double *EP;       /* [n_g*3] */
+    const double *WM;       /* [n_g] */
+    const int32_t *row_table;  /* [n_g] */
+    int32_t n_tab;
+    const double *E_tab;    /* [n_tab] eV, ascending */
+    const double *chi_re;   /* [n_hkl*n_tab] */
+    const double *chi_im;
+    const double *u_re;
+    const double *u_im;
+    int32_t n_mu;
+    const double *log_mu;   /* [n_mu*n_tab] */
+    const double *delta;    /* [n_tab] */
+    double lo_keep, hi_keep;
+} pb_cxr_tables;
+
+typedef struct pb_cxr_args {
+    int32_t precision;      /* pb_precision */
+    int32_t quadrature;     /* pb_quadrature; PB_QUAD_NODE needs the line buffer */
+    int32_t n_dir;          /* detector directions (angular tiles) */
+    const double *n_hat;    /* [n_dir*3] device */
+    double thickness;
+    int64_t Ne;             /* electrons counted (elec_id < Ne radiate) */
+    int64_t n_seg;
+    const double *r_mid, *v_hat, *L, *E_keV;  /* segment list (device) */
+    const int64_t *elec_id;
+    const unsigned long long *n_seg_device;  /* optional: read n_seg on device */
+    pb_cxr_tables tables;
+    int32_t n_E;            /* output nodes (node) or bins (bin-mean) */
+    const double *E_grid;   /* [n_E] nodes */
+    const double *edges;    /* [n_E+1] bin edges (bin-mean) */
+    double exact_widths;    /* bin-mean: exact within this many widths; <=0: all exact */
+    int32_t far_pad;        /* bin-mean, uniform axis: virtual centre bins each side
+                               covering the keep window; -1 disables the far field */
+    double *spec;           /* [n_dir*n_E] accumulated (+=), FP64, not normalised */
+    double *far_moments;    /* workspace [n_dir*(n_E+2*far_pad)*3], zeroed by the call */
+    /* Line buffer (node quadrature, and optional output of every kept line):
+     * [line_capacity] each; direction index in line_dir. */
+    int64_t line_capacity;
+    unsigned long long *line_count;  /* device counter, zeroed by the call */
+    double *line_E;
+    double *line_a;
+    double *line_w;
+    int32_t *line_dir;
+    /* Optional per-pair output for parity checks: [n_dir*n_seg*n_g] each. */
+    double *pair_E;
+    double *pair_a;
+    double *pair_w;
+    uint8_t *pair_good;
+    unsigned int *status;
+} pb_cxr_args;
+
+typedef struct pb_brem_args {
+    int32_t precision;
+    int32_t n_dir;
+    const double *n_hat;    /* [n_dir*3] */
+    double thickness;
+    int64_t Ne;
+    int64_t n_seg;
+    const double *r_mid, *v_hat, *L, *E_keV;
+    const int64_t *elec_id;
+    const unsigned long long *n_seg_device;
+    int32_t n_el;
+    const double *Z;        /* [n_el] */
+    const double *n_ang3;   /* [n_el] atoms / Angstrom^3 */
+    int32_t n_E;
+    const double *E_grid;   /* [n_E] eV */
+    const double *mu;       /* [n_E] 1/Angstrom attenuation at the grid */
+    double *spec;           /* [n_dir*n_E] accumulated (+=), not normalised */
+    unsigned int *status;
+} pb_brem_args;
+
+int pb_abi_version(void);
+const char *pb_last_error(void);
+int pb_device_count(int *count);
+
+/* Transport: rows (parity replay), compact segments and/or fused tallies. */
+int pb_transport(const pb_transport_args *args, void *stream);
+
+/* Incoherent PXR + CBS lines of a segment list, reduced onto spectra. */
+int pb_cxr_score(const pb_cxr_args *args, void *stream);
+
+/* Bethe-Heitler + Elwert track-length bremsstrahlung of a segment list. */
+int pb_brem_score(const pb_brem_args *args, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,25 @@
+"""pyrite_b200: PyRITE's electron-transport and radiation-scoring hot path on B200.
+
+Hand-written sm_100a CUDA behind a C ABI (``include/pyrite_b200.h``), loaded
+with ctypes; this package holds the host-side mirror of the reference's calls
+and the tables they need. There is no CPU fallback.
+"""
+
+from .api import (  # noqa: F401
+    BeamSpec,
+    LineTables,
+    mc_brem_spectrum,
+    mc_cxr_spectrum,
+    simulate_trajectories,
+)
+from ._lib import PyriteB200Error, load  # noqa: F401
+
+__all__ = [
+    "BeamSpec",
+    "LineTables",
+    "PyriteB200Error",
+    "load",
+    "mc_brem_spectrum",
+    "mc_cxr_spectrum",
+    "simulate_trajectories",
+]

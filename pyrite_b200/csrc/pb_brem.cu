@@ -1,0 +1,157 @@
+// Bethe-Heitler + Elwert track-length bremsstrahlung of a segment list
+// (sm_100a). spec[d][e] += sum_seg sum_el n_el L dsigma/dk(Z_el, T, k_e)
+// * <exp(-mu(k_e) path)>_segment, the estimator of
+// src/pyrite/montecarlo/spectrum/brem.py:431-479,1196-1239 before its
+// 1/(4 pi Ne) normalisation.
+//
+// Work split: a block owns 256 photon-energy nodes (one per thread), a chunk
+// of segments staged in shared memory with their energy-independent parts
+// (incident momentum, beta, Elwert incident factor, escape end paths), and
+// one detector direction. Each thread sums its node over the chunk in a
+// register; one global atomic per node per block publishes it.
+//
+// The mixed path forms p_i - p_f without cancellation,
+// (p_i^2 - p_f^2)/(p_i + p_f) = k (T_i + T_f + 2 m c^2)/((m c^2)^2 (p_i + p_f)),
+// which float needs for MeV electrons and keV photons; FP64 keeps the
+// reference's direct difference.
+#include <cstdint>
+
+#include "pb_common.cuh"
+#include "pb_internal.h"
+
+namespace pb {
+
+constexpr int kBremThreads = 256;
+constexpr int kBremChunk = 256;
+constexpr int kBremMaxEl = 4;
+
+template <class Real>
+struct BremSeg {
+    Real T;       // keV
+    Real p_i;     // momentum / (m c)
+    Real beta_i;
+    Real path0, path1;
+    Real nL[kBremMaxEl];     // n_el * 1e24 * L * 1e-8  [1/cm^2]
+    Real den_i[kBremMaxEl];  // 1 - exp(-2 pi Z alpha / beta_i)
+};
+
+__device__ __forceinline__ double b_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float b_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double b_exp(double x) { return exp(x); }
+__device__ __forceinline__ float b_exp(float x) { return expf(x); }
+__device__ __forceinline__ double b_log(double x) { return log(x); }
+__device__ __forceinline__ float b_log(float x) { return logf(x); }
+__device__ __forceinline__ double b_expm1(double x) { return expm1(x); }
+__device__ __forceinline__ float b_expm1(float x) { return expm1f(x); }
+
+template <class Real>
+__device__ __forceinline__ Real b_path(Real z, Real thickness, Real nz) {
+    const Real inv_nz = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
+    const Real depth = fmin(fmax(z, (Real)0), thickness);
+    return nz < (Real)0 ? depth * inv_nz : (thickness - depth) * inv_nz;
+}
+
+template <class Real>
+__device__ __forceinline__ Real b_mean_transmission(Real t0, Real t1) {
+    const Real lo = fmin(t0, t1);
+    const Real d = fabs(t1 - t0);
+    const Real safe = d > (Real)1.0e-4 ? d : (Real)1;
+    const Real ratio = d > (Real)1.0e-4 ? -b_expm1(-safe) / safe : (Real)1 - (Real)0.5 * d + d * d / (Real)6;
+    return b_exp(-lo) * ratio;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a, int64_t n_seg) {
+    __shared__ BremSeg<Real> segs[kBremChunk];
+    __shared__ Real Zs[kBremMaxEl];
+    const int d = blockIdx.z;
+    const double *nh = a.n_hat + 3 * d;
+    const Real nz = (Real)nh[2];
+    const Real T_slab = (Real)a.thickness;
+    const int n_el = a.n_el;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = e < a.n_E;
+    const Real mc2 = (Real)510.99895;
+    const Real za = (Real)(2.0 * kPi * kAlphaFs);
+    if (threadIdx.x < n_el) Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+    const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
+    const Real k = (Real)k_kev_d;
+    const Real mu = on ? (Real)a.mu[e] : (Real)0;
+    const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
+    const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
+    double acc = 0.0;
+    if (a.n_seg_device) {
+        const int64_t live = (int64_t)*a.n_seg_device;
+        if (live < n_seg) n_seg = live;
+    }
+    const int64_t per = (a.n_seg + gridDim.y - 1) / gridDim.y;
+    const int64_t s_begin = per * blockIdx.y;
+    int64_t s_end = s_begin + per < n_seg ? s_begin + per : n_seg;
+    if (s_end < s_begin) s_end = s_begin;
+    for (int64_t c0s = s_begin; c0s < s_end; c0s += kBremChunk) {
+        const int nc = (int)((s_end - c0s) < kBremChunk ? (s_end - c0s) : kBremChunk);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const int64_t s = c0s + j;
+            BremSeg<Real> &b = segs[j];
+            const Real T = (Real)a.E_keV[s];
+            b.T = T;
+            const Real p_i = b_sqrt(T * (T + (Real)2 * mc2)) / mc2;
+            b.p_i = p_i;
+            b.beta_i = p_i / ((Real)1 + T / mc2);
+            const Real half = (Real)0.5 * (Real)a.L[s];
+            const Real z = (Real)a.r_mid[3 * s + 2];
+            const Real vz = (Real)a.v_hat[3 * s + 2];
+            b.path0 = b_path<Real>(z - half * vz, T_slab, nz);
+            b.path1 = b_path<Real>(z + half * vz, T_slab, nz);
+            const bool rad = a.elec_id[s] < a.Ne;
+            const Real path_cm = (Real)a.L[s] * (Real)1e-8;
+            for (int el = 0; el < n_el; ++el) {
+                b.nL[el] = rad ? (Real)(a.n_ang3[el] * 1e24) * (Real)1 * path_cm : (Real)0;
+                b.den_i[el] = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
+            }
+        }
+        __syncthreads();
+        if (!on) continue;
+        for (int j = 0; j < nc; ++j) {
+            const BremSeg<Real> &b = segs[j];
+            const Real T_f = b.T - k;
+            if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
+            const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
+            const Real beta_f = p_f / ((Real)1 + T_f / mc2);
+            Real diff;
+            if constexpr (sizeof(Real) == 8) {
+                diff = b.p_i - p_f;
+            } else {
+                diff = k * (b.T + T_f + (Real)2 * mc2) / (mc2 * mc2 * (b.p_i + p_f));
+            }
+            const Real born_log = b_log((b.p_i + p_f) / fmax(diff, (Real)1e-30));
+            const Real T_abs = b_mean_transmission<Real>(b.path0 * mu, b.path1 * mu);
+            Real sum = 0;
+            for (int el = 0; el < n_el; ++el) {
+                const Real Z = Zs[el];
+                const Real elwert = b.beta_i / beta_f * b.den_i[el] / ((Real)1 - b_exp(-za * Z / beta_f));
+                const Real dsig = c0 * (Z * Z) / k_ev / (b.p_i * b.p_i) * born_log * elwert;
+                sum += b.nL[el] * (dsig * T_abs);
+            }
+            acc += (double)sum;
+        }
+    }
+    if (on && acc != 0.0) atomicAdd(&a.spec[(int64_t)d * a.n_E + e], acc);
+}
+
+cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
+    if (a.n_el > kBremMaxEl || a.n_el < 1) return cudaErrorInvalidValue;
+    int64_t n_seg = a.n_seg;
+    const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
+    int64_t gy = ((int64_t)sms * 4 + (int64_t)gx * a.n_dir - 1) / ((int64_t)gx * a.n_dir);
+    const int64_t max_y = (n_seg + kBremChunk - 1) / kBremChunk;
+    if (gy > max_y) gy = max_y;
+    if (gy < 1) gy = 1;
+    dim3 grid(gx, (unsigned)gy, (unsigned)a.n_dir);
+    if (a.precision == PB_MIXED) brem_kernel<float><<<grid, kBremThreads, 0, s>>>(a, n_seg);
+    else brem_kernel<double><<<grid, kBremThreads, 0, s>>>(a, n_seg);
+    return cudaGetLastError();
+}
+
+}  // namespace pb

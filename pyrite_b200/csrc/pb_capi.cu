@@ -1,0 +1,146 @@
+// C ABI of pyrite_b200: argument checks, error reporting, launches.
+//
+// Every entry point validates its plain-C arguments on the host, launches on
+// the caller's stream and returns a pb_status. Errors carry a message in a
+// thread-local buffer read by pb_last_error(). Nothing here allocates.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "pb_internal.h"
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    return fail(PB_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+// Streaming multiprocessors of the current device (cached per device).
+int device_sms() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+int pb_abi_version(void) { return PB_ABI_VERSION; }
+
+const char *pb_last_error(void) { return g_err; }
+
+int pb_device_count(int *count) {
+    if (!count) return fail(PB_ERR_INVALID, "pb_device_count: count is NULL");
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    return PB_OK;
+}
+
+int pb_transport(const pb_transport_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_transport: args is NULL");
+    if (a->n < 0) return fail(PB_ERR_INVALID, "pb_transport: n = %lld < 0", (long long)a->n);
+    if (a->n == 0) return PB_OK;
+    if (a->layers.n_layers < 1 || a->layers.n_layers > 8)
+        return fail(PB_ERR_INVALID, "pb_transport: n_layers = %d outside [1, 8]", a->layers.n_layers);
+    if (a->layers.max_el < 1 || a->layers.max_el > 8)
+        return fail(PB_ERR_INVALID, "pb_transport: max_el = %d outside [1, 8]", a->layers.max_el);
+    if (!a->layers.z_top || !a->layers.z_bot || !a->layers.n_el || !a->layers.J || !a->layers.k ||
+        !a->layers.coeff || !a->layers.E_cross || !a->layers.sr_rate_numer || !a->layers.sr_joy_numer)
+        return fail(PB_ERR_INVALID, "pb_transport: layer tables must all be set");
+    if (!a->work_counter) return fail(PB_ERR_INVALID, "pb_transport: work_counter is NULL");
+    if (a->rng != PB_RNG_SPLITMIX && a->rng != PB_RNG_PHILOX)
+        return fail(PB_ERR_INVALID, "pb_transport: unknown rng %d", a->rng);
+    if (a->precision != PB_FP64 && a->precision != PB_MIXED)
+        return fail(PB_ERR_INVALID, "pb_transport: unknown precision %d", a->precision);
+    if (a->use_lut) {
+        const int eb = a->precision == PB_MIXED ? 4 : 8;
+        if (!a->lut.base || a->lut.elem_bytes != eb)
+            return fail(PB_ERR_INVALID, "pb_transport: LUT needs %d-byte values for this precision", eb);
+        if (a->lut.n_energy < 2) return fail(PB_ERR_INVALID, "pb_transport: LUT n_energy < 2");
+        if (a->lut.total_bytes % 16 != 0 || ((uintptr_t)a->lut.base % 16) != 0)
+            return fail(PB_ERR_INVALID, "pb_transport: LUT buffer must be 16-byte aligned and sized");
+    }
+    if (a->beam.mode == PB_BEAM_EXPLICIT && (!a->beam.pos0 || !a->beam.dir0 || !a->beam.E0))
+        return fail(PB_ERR_INVALID, "pb_transport: explicit beam needs pos0, dir0 and E0");
+    if (a->beam.mode < 0 || a->beam.mode > 2)
+        return fail(PB_ERR_INVALID, "pb_transport: unknown beam mode %d", a->beam.mode);
+    if (a->rows.L && a->cap < 1) return fail(PB_ERR_INVALID, "pb_transport: rows need cap >= 1");
+    if (a->seg.L && (!a->seg.count || a->seg.capacity < 0))
+        return fail(PB_ERR_INVALID, "pb_transport: segment list needs a count and a capacity");
+    if (a->tallies.exit_E && (a->tallies.n_E < 1 || a->tallies.n_E > 256))
+        return fail(PB_ERR_INVALID, "pb_transport: exit energy bins must be in [1, 256]");
+    if (a->tallies.exit_theta && (a->tallies.n_theta < 1 || a->tallies.n_theta > 256))
+        return fail(PB_ERR_INVALID, "pb_transport: exit angle bins must be in [1, 256]");
+    if (a->block_threads != 0 && (a->block_threads % 32 != 0 || a->block_threads > 256))
+        return fail(PB_ERR_INVALID, "pb_transport: block_threads must be a multiple of 32 <= 256");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(a->work_counter, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_transport: zero work counter");
+    e = pb::launch_transport(*a, s, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_transport: launch");
+    return PB_OK;
+}
+
+int pb_cxr_score(const pb_cxr_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_cxr_score: args is NULL");
+    if (a->n_seg < 0 || a->n_dir < 1 || a->n_E < 1)
+        return fail(PB_ERR_INVALID, "pb_cxr_score: need n_seg >= 0, n_dir >= 1, n_E >= 1");
+    if (a->n_seg == 0) return PB_OK;
+    const pb_cxr_tables &t = a->tables;
+    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4)
+        return fail(PB_ERR_INVALID, "pb_cxr_score: need n_g >= 1, n_tab >= 2, 1 <= n_mu <= 4");
+    if (!t.G || !t.ES || !t.EP || !t.WM || !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im ||
+        !t.u_re || !t.u_im || !t.log_mu || !t.delta)
+        return fail(PB_ERR_INVALID, "pb_cxr_score: every table pointer must be set");
+    if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id)
+        return fail(PB_ERR_INVALID, "pb_cxr_score: segment and direction pointers must be set");
+    if (a->quadrature == PB_QUAD_BINMEAN) {
+        if (!a->edges || !a->spec) return fail(PB_ERR_INVALID, "pb_cxr_score: bin-mean needs edges and spec");
+        if (a->exact_widths > 0.0 && a->far_pad >= 0 && !a->far_moments)
+            return fail(PB_ERR_INVALID, "pb_cxr_score: far field needs the far_moments workspace");
+    } else if (a->quadrature == PB_QUAD_NODE) {
+        if (!a->E_grid || !a->spec || !a->line_E || !a->line_a || !a->line_w || !a->line_dir || !a->line_count)
+            return fail(PB_ERR_INVALID, "pb_cxr_score: node quadrature needs the grid and a line buffer");
+    } else {
+        return fail(PB_ERR_INVALID, "pb_cxr_score: unknown quadrature %d", a->quadrature);
+    }
+    if (a->line_E && (!a->line_count || a->line_capacity < 1))
+        return fail(PB_ERR_INVALID, "pb_cxr_score: line buffer needs a count and a capacity");
+    cudaError_t e = pb::launch_cxr(*a, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_cxr_score: launch");
+    return PB_OK;
+}
+
+int pb_brem_score(const pb_brem_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_brem_score: args is NULL");
+    if (a->n_seg < 0 || a->n_dir < 1 || a->n_E < 1)
+        return fail(PB_ERR_INVALID, "pb_brem_score: need n_seg >= 0, n_dir >= 1, n_E >= 1");
+    if (a->n_seg == 0) return PB_OK;
+    if (a->n_el < 1 || a->n_el > 4) return fail(PB_ERR_INVALID, "pb_brem_score: 1 <= n_el <= 4");
+    if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->Z ||
+        !a->n_ang3 || !a->E_grid || !a->mu || !a->spec)
+        return fail(PB_ERR_INVALID, "pb_brem_score: every pointer must be set");
+    cudaError_t e = pb::launch_brem(*a, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_brem_score: launch");
+    return PB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,738 @@
+// Incoherent PXR + CBS line scoring of a segment list (sm_100a).
+//
+// For every (segment, reflection row, detector direction) the kernels follow
+// the reference's batched line chain (src/pyrite/montecarlo/spectrum/cxr/
+// _batched.py:461-931): exact-recoil vacuum root, three fixed-point passes
+// of the first-order Snell resonance (cxr/_kernels.py:702-765), the shared
+// interpolation bracket for chi/U/mu (cxr/_kernels.py:482-620), the exact
+// second-order PXR+CBS amplitude of both polarisations (cxr/_recoil.py:35),
+// the segment-mean Beer-Lambert escape (segment_escape.py:276) and the
+// line weight and width (cxr/_kernels.py:658, cxr/_batched.py:702-730).
+//
+// Reductions:
+//  * bin-mean (production): each kept line is integrated exactly over the
+//    bins within ``exact_widths`` sinc widths of its centre (FP64 sine
+//    integral), and its far field -- the cycle-averaged envelope
+//    1/(2 a^2 (E_lo - E_r)(E_hi - E_r)) -- is carried by three moments per
+//    centre bin in shared memory and spread onto the grid by one finalize
+//    pass (cxr/_bin_quadrature.py:280-560 for the exact and far forms).
+//    Lines never leave the SM: warp work -> shared-memory spectrum -> one
+//    global atomic per bin per block.
+//  * node sampling: kept lines are appended to a line buffer and reduced
+//    against the grid nodes by a separate kernel (cxr/_cpu_reduce.py:26-50).
+//
+// PB_FP64 evaluates the chain in double; PB_MIXED in float, with the line
+// phase a (E - E_r) formed and range-reduced in double and every
+// accumulation in double.
+#include <cstdint>
+
+#include "pb_common.cuh"
+#include "pb_internal.h"
+
+namespace pb {
+
+constexpr int kSegTile = 32;
+constexpr int kRowChunk = 128;
+constexpr int kCxrThreads = 256;
+constexpr int kMaxTab = 4096;   // E_tab / delta staged in shared memory up to this size
+constexpr int kMaxMu = 4;
+
+__device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double r_exp(double x) { return exp(x); }
+__device__ __forceinline__ float r_exp(float x) { return expf(x); }
+__device__ __forceinline__ double r_expm1(double x) { return expm1(x); }
+__device__ __forceinline__ float r_expm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double r_log1p(double x) { return log1p(x); }
+__device__ __forceinline__ float r_log1p(float x) { return log1pf(x); }
+
+// Per (segment, direction) quantities shared by every reflection row.
+template <class Real>
+struct SegPre {
+    Real vx, vy, vz;        // beta v_hat
+    Real gamma;
+    Real denom_row;         // 1 - beta v_hat.n, cancellation free
+    Real t_L;               // L / beta
+    Real path0, path1;      // escape paths at the segment ends
+    Real gx, gy, gz;        // grad L
+    Real grad2;
+    Real v_dot_grad;
+    Real inv_E;             // hbar c / E
+    int radiates;           // elec_id < Ne
+};
+
+template <class Real>
+struct RowPre {
+    Real G[3];
+    Real ES[3];
+    Real EP[3];
+    Real g2, n_dot_g, g_dot_es, g_dot_ep, wm;
+    int row;
+};
+
+template <class Real>
+__device__ __forceinline__ Real slab_path(Real z, Real thickness, Real nz) {
+    const Real inv_nz = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
+    const Real depth = fmin(fmax(z, (Real)0), thickness);
+    return nz < (Real)0 ? depth * inv_nz : (thickness - depth) * inv_nz;
+}
+
+template <class Real>
+__device__ void seg_precompute(SegPre<Real> &sp, const pb_cxr_args &a, int64_t s, const double *nh) {
+    const double E = a.E_keV[s];
+    const Real Er = (Real)E;
+    const Real vhx = (Real)a.v_hat[3 * s], vhy = (Real)a.v_hat[3 * s + 1], vhz = (Real)a.v_hat[3 * s + 2];
+    const Real nx = (Real)nh[0], ny = (Real)nh[1], nz = (Real)nh[2];
+    // cxr/_setup.py:945-1005; kinematics.py:151-154
+    const Real g0 = (Real)1 + Er / (Real)510.99895;
+    const Real beta = r_sqrt((Real)1 - (Real)1 / (g0 * g0));
+    sp.vx = beta * vhx;
+    sp.vy = beta * vhy;
+    sp.vz = beta * vhz;
+    // cxr/_kernels.py:678-699
+    const Real gamma = (Real)1 + Er / (Real)(kMeEv / 1e3);
+    const Real omb = (Real)1 / (gamma * gamma * ((Real)1 + beta));
+    const Real dvx = vhx - nx, dvy = vhy - ny, dvz = vhz - nz;
+    const Real omc = (Real)0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
+    sp.gamma = gamma;
+    sp.denom_row = omb + beta * omc;
+    sp.t_L = (Real)a.L[s] / beta;
+    // segment_escape.py:239-270, single slab
+    const Real T = (Real)a.thickness;
+    const Real half = (Real)0.5 * (Real)a.L[s];
+    const Real z_mid = (Real)a.r_mid[3 * s + 2];
+    sp.path0 = slab_path<Real>(z_mid - half * vhz, T, nz);
+    sp.path1 = slab_path<Real>(z_mid + half * vhz, T, nz);
+    // segment_escape.py:95-131
+    Real gx = (Real)-0.0 / nz, gy = (Real)-0.0 / nz, gz = (Real)-1 / nz;
+    if (z_mid < (Real)0 || z_mid > T) { gx = 0; gy = 0; gz = 0; }
+    sp.gx = gx; sp.gy = gy; sp.gz = gz;
+    sp.grad2 = gx * gx + gy * gy + gz * gz;
+    sp.v_dot_grad = sp.vx * gx + sp.vy * gy + sp.vz * gz;
+    sp.inv_E = (Real)kHbarcEvAng / (gamma * (Real)kMeEv);
+    sp.radiates = a.elec_id[s] < a.Ne;
+}
+
+// searchsorted(grid, x, side="left") clipped to [1, n-1] and the blend
+// fraction (cxr/_kernels.py:328-349).
+template <class Real>
+__device__ __forceinline__ void bracket(const Real *grid, int n, Real x, int &idx, Real &frac,
+                                        bool &below, bool &above) {
+    int i;
+    if (isnan(x)) {
+        i = n;
+    } else {
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (grid[mid] < x) lo = mid + 1; else hi = mid;
+        }
+        i = lo;
+    }
+    i = i < 1 ? 1 : (i > n - 1 ? n - 1 : i);
+    idx = i;
+    frac = (x - grid[i - 1]) / (grid[i] - grid[i - 1]);
+    below = x <= grid[0];
+    above = x >= grid[n - 1];
+}
+
+template <class Real, class T>
+__device__ __forceinline__ Real gather(const T *f, int n, int idx, Real frac, bool below, bool above) {
+    const Real f0 = (Real)f[idx - 1];
+    Real y = f0 + frac * ((Real)f[idx] - f0);
+    if (below) y = (Real)f[0];
+    if (above) y = (Real)f[n - 1];
+    return y;
+}
+
+// cxr/_recoil.py:35-76
+template <class Real>
+__device__ __forceinline__ void quantum_line_factors(Real h, Real gamma, Real vdg, Real k_dot_v,
+                                                     Real k_dot_g, Real g2, Real k2, Real v_dot_e,
+                                                     Real g_dot_e, Real k_dot_e, Real &pxr_num,
+                                                     Real &f_cbs) {
+    const Real gg = gamma * gamma;
+    const Real n_1 = h * g2 - (Real)2 * gamma * vdg;
+    const Real n_2 = n_1 + (Real)2 * h * k_dot_g;
+    const Real n_f = h * (g2 + (Real)2 * k_dot_g + k2) - (Real)2 * gamma * (vdg + k_dot_v);
+    const Real e_1 = r_sqrt(gg + h * n_1);
+    const Real e_2 = r_sqrt(gg + h * (h * k2 - (Real)2 * gamma * k_dot_v));
+    const Real e_f = r_sqrt(gg + h * n_f);
+    const Real s_if = gamma + e_f;
+    const Real ge_ke = g_dot_e + k_dot_e;
+    pxr_num = (-n_f * ge_ke - k2 * ((Real)2 * gamma * v_dot_e - h * ge_ke)) / s_if;
+    const Real s_1 = e_1 + gamma;
+    const Real s_3 = e_1 + e_f;
+    const Real s_4 = gamma + e_2;
+    const Real x = (Real)2 * gamma * v_dot_e - h * k_dot_e;
+    const Real sigma = s_if + e_1 + e_2;
+    f_cbs = (Real)2 * g_dot_e * s_1 / (s_3 * n_1) +
+            x * (n_1 * (n_f / s_if) * sigma - (Real)2 * s_1 * s_4 * k_dot_g) / (s_3 * s_4 * n_1 * n_2);
+}
+
+// segment_escape.py:276-289
+template <class Real>
+__device__ __forceinline__ Real mean_transmission(Real t0, Real t1) {
+    const Real lo = fmin(t0, t1);
+    const Real d = fabs(t1 - t0);
+    const Real safe = d > (Real)1.0e-4 ? d : (Real)1;
+    const Real ratio = d > (Real)1.0e-4 ? -r_expm1(-safe) / safe
+                                         : (Real)1 - (Real)0.5 * d + d * d / (Real)6;
+    return r_exp(-lo) * ratio;
+}
+
+template <class Real>
+struct Line {
+    Real E_res, a_width, weight;
+    bool good;
+};
+
+// The per-pair chain. ``tab`` points at E_tab / delta / log_mu (shared or
+// global), ``n_tab`` their length.
+template <class Real>
+__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, const double *nh,
+                                const Real *E_tab, const Real *delta_tab, const Real *log_mu,
+                                int n_tab, int n_mu, const pb_cxr_tables &t) {
+    const Real nx = (Real)nh[0], ny = (Real)nh[1], nz = (Real)nh[2];
+    const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
+    const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
+    (void)nx; (void)ny; (void)nz;
+    const Real hbarc = (Real)kHbarcEvAng;
+    // cxr/_block_prologue.py:18-38, cxr/_recoil.py:79-97
+    const Real r_num = (Real)0.5 * g2 * sp.inv_E;
+    const Real r_den = n_dot_g * sp.inv_E;
+    const Real v_dot_g_exact = (sp.vx * Gx + sp.vy * Gy + sp.vz * Gz) - r_num;
+    const Real denom_vac = sp.denom_row + r_den;
+    // cxr/_kernels.py:702-765
+    Real denom = denom_vac, previous = denom, delta = (Real)NAN;
+    for (int pass = 0; pass < 3; ++pass) {
+        const Real Er = hbarc * (v_dot_g_exact / denom);
+        int ix;
+        Real fr;
+        bool bl, ab;
+        bracket<Real>(E_tab, n_tab, Er, ix, fr, bl, ab);
+        delta = gather<Real>(delta_tab, n_tab, ix, fr, bl, ab);
+        previous = denom;
+        denom = denom_vac - delta * sp.v_dot_grad;
+    }
+    bool settled = fabs(denom - previous) <= (Real)1e-3 * fabs(denom);
+    settled = settled && ((Real)2 * fabs(delta) * sp.grad2 < (Real)1);
+    if (!settled) denom = (Real)NAN;
+    const Real n_dot_g_blk = n_dot_g + delta * (sp.gx * Gx + sp.gy * Gy + sp.gz * Gz);
+    // cxr/_kernels.py:624-655
+    const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
+    const Real omega = (v_dot_g - r_num) / denom;
+    const Real k_dot_v = omega * (((Real)1 - denom) + r_den);
+    const Real k_dot_g = omega * n_dot_g_blk;
+    const Real detuning = g2 + (Real)2 * k_dot_g;
+    // cxr/_batched.py:435-458
+    const Real k_mag = omega * r_sqrt(sp.grad2 == (Real)0 ? (Real)1
+                                                           : (Real)1 - (Real)2 * delta + delta * delta * sp.grad2);
+    const Real E_res = hbarc * omega;
+    bool keep = sp.radiates && (E_res > (Real)t.lo_keep) && (E_res > (Real)10) && (E_res < (Real)t.hi_keep);
+    int ix;
+    Real fr;
+    bool bl, ab;
+    bracket<Real>(E_tab, n_tab, E_res, ix, fr, bl, ab);
+    Real lfr;
+    {
+        const Real x0 = E_tab[ix - 1], x1 = E_tab[ix];
+        Real bx = fmin(fmax(E_res, x0), x1);
+        if (isnan(E_res)) bx = E_res;
+        lfr = r_log1p((bx - x0) / x0) / r_log1p((x1 - x0) / x0);
+    }
+    // cxr/_block_prologue.py:53-62, cxr/_recoil.py:100-118
+    const Real slope = denom * ((Real)1 / ((Real)1 - omega * sp.inv_E));
+    keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - (Real)1 / sp.gamma);
+    // cxr/_kernels.py:482-506 couplings, 369-388 attenuation
+    const int64_t base = (int64_t)rw.row * n_tab;
+    const Real chi_re = gather<Real>(t.chi_re + base, n_tab, ix, fr, bl, ab);
+    const Real chi_im = gather<Real>(t.chi_im + base, n_tab, ix, fr, bl, ab);
+    const Real u_re = gather<Real>(t.u_re + base, n_tab, ix, fr, bl, ab);
+    const Real u_im = gather<Real>(t.u_im + base, n_tab, ix, fr, bl, ab);
+    Real mu = 0;
+    for (int el = 0; el < n_mu; ++el) {
+        const Real *lm = log_mu + (int64_t)el * n_tab;
+        const Real f0 = lm[ix - 1];
+        Real v = r_exp(f0 + lfr * (lm[ix] - f0));
+        if (bl) v = r_exp(lm[0]);
+        if (ab) v = r_exp(lm[n_tab - 1]);
+        mu += v;
+    }
+    // cxr/_batched.py:789-826, cxr/_line_amplitude.py:14-37
+    const Real h = (Real)(kHbarcEvAng / kMeEv);
+    const Real k2 = k_mag * k_mag;
+    Real A2 = 0;
+#pragma unroll
+    for (int pol = 0; pol < 2; ++pol) {
+        const Real *Ev = pol == 0 ? rw.ES : rw.EP;
+        const Real g_dot_e = pol == 0 ? rw.g_dot_es : rw.g_dot_ep;
+        const Real v_dot_e = sp.vx * Ev[0] + sp.vy * Ev[1] + sp.vz * Ev[2];
+        const Real k_dot_e = omega * delta * (sp.gx * Ev[0] + sp.gy * Ev[1] + sp.gz * Ev[2]);
+        Real pxr_num, f_cbs;
+        quantum_line_factors<Real>(h, sp.gamma, v_dot_g, k_dot_v, k_dot_g, g2, k2, v_dot_e, g_dot_e,
+                                   k_dot_e, pxr_num, f_cbs);
+        const Real f_pxr = pxr_num / detuning;
+        const Real re = chi_re * f_pxr + u_re * f_cbs;
+        const Real im = chi_im * f_pxr + u_im * f_cbs;
+        const Real a2 = re * re + im * im;
+        A2 = pol == 0 ? a2 : A2 + a2;
+    }
+    // cxr/_batched.py:702-730, cxr/_kernels.py:658-668
+    const Real T_abs = mean_transmission<Real>(sp.path0 * mu, sp.path1 * mu);
+    const Real pref_c1 = (Real)(4.0 * (kPi * kPi) * kHbarcEvAng);
+    const Real pref = (Real)kAlphaFs * omega / pref_c1 * (sp.t_L * sp.t_L) * T_abs;
+    Line<Real> out;
+    out.E_res = E_res;
+    out.a_width = slope * sp.t_L / ((Real)2 * hbarc) * (Real)1;
+    out.weight = pref * A2 * rw.wm;
+    out.good = keep && isfinite(out.weight) && (out.weight > (Real)0);
+    return out;
+}
+
+// ---- sine integral and the sinc^2 antiderivative --------------------------
+// Si(t) - pi/2 for t >= 0: power series for t <= 4; the continued fraction of
+// E1(i t) by the modified Lentz method (Numerical Recipes "cisi") for
+// 4 < t < 40; the asymptotic auxiliary-function series beyond
+// (Abramowitz & Stegun 5.2.34-5.2.35): Si - pi/2 = -f cos t - g sin t.
+__device__ double si_minus_half_pi(double t) {
+    if (t <= 4.0) {
+        const double t2 = t * t;
+        double term = t, sum = t;
+        for (int k = 1; k < 40; ++k) {
+            term *= -t2 / ((2.0 * k) * (2.0 * k + 1.0));
+            const double add = term / (2.0 * k + 1.0);
+            sum += add;
+            if (fabs(add) < 1e-18 * fabs(sum)) break;
+        }
+        return sum - 0.5 * kPi;
+    }
+    double s, c;
+    sincos(t, &s, &c);
+    if (t >= 40.0) {
+        const double y = 1.0 / (t * t);
+        // f t = 1 - 2!/t^2 + 4!/t^4 - ..., g t^2 = 1 - 3!/t^2 + 5!/t^4 - ...
+        double f = 1.0, g = 1.0, tf = 1.0, tg = 1.0;
+        for (int k = 1; k < 12; ++k) {
+            tf *= -(2.0 * k - 1.0) * (2.0 * k) * y;
+            tg *= -(2.0 * k) * (2.0 * k + 1.0) * y;
+            f += tf;
+            g += tg;
+            if (fabs(tf) < 1e-17 && fabs(tg) < 1e-17) break;
+        }
+        f /= t;
+        g *= y;
+        return -f * c - g * s;
+    }
+    double br = 1.0, bi = t;
+    double den = br * br + bi * bi;
+    double dr = br / den, di = -bi / den;
+    double hr = dr, hi = di;
+    double cr = 1e300, ci = 0.0;
+    for (int i = 2; i < 200; ++i) {
+        const double a = -(double)(i - 1) * (double)(i - 1);
+        br += 2.0;
+        const double xr = a * dr + br, xi = a * di + bi;
+        den = xr * xr + xi * xi;
+        dr = xr / den;
+        di = -xi / den;
+        den = cr * cr + ci * ci;
+        cr = br + a * cr / den;
+        ci = bi - a * ci / den;
+        const double delr = cr * dr - ci * di, deli = cr * di + ci * dr;
+        const double nhr = hr * delr - hi * deli, nhi = hr * deli + hi * delr;
+        hr = nhr;
+        hi = nhi;
+        if (fabs(delr - 1.0) + fabs(deli) < 1e-16) break;
+    }
+    return c * hi - s * hr;
+}
+
+// R(x) = F(x) - sign(x)/2, F the integral of sinc^2 from 0.
+__device__ double sincsq_tail(double x) {
+    const double u = fabs(x);
+    const double t = 2.0 * kPi * u;
+    double su;
+    if (u == 0.0) {
+        su = 1.0;
+    } else {
+        su = sin(kPi * u) / (kPi * u);
+    }
+    const double r = si_minus_half_pi(t) / kPi - u * su * su;
+    return x >= 0.0 ? r : -r;
+}
+
+struct BinAxis {
+    const double *edges;
+    int n;
+    double lo, w, inv_w;  // uniform axis: edges[b] = lo + b w
+    bool uniform;
+    int pad;              // virtual centre bins on each side (uniform axes)
+};
+
+__device__ __forceinline__ int bin_of(const BinAxis &ax, double E) {
+    if (ax.uniform) return (int)floor((E - ax.lo) * ax.inv_w);
+    if (E < ax.edges[0]) return -1;
+    if (E >= ax.edges[ax.n]) return ax.n;
+    int lo = 0, hi = ax.n;  // last edge index with edges[b] <= E
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (ax.edges[mid] <= E) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double centre_of(const BinAxis &ax, int c) {
+    if (ax.uniform) return ax.lo + ((double)c + 0.5) * ax.w;
+    return 0.5 * (ax.edges[c] + ax.edges[c + 1]);
+}
+
+// Far-field envelope expansion about centre c: 1/((A-d)(B-d)) ~
+// f0 + f1 d + f2 d^2 with A = E_lo - E_c, B = E_hi - E_c, d = E_r - E_c.
+__device__ __forceinline__ double far_envelope(double A, double B, double d) {
+    const double AB = A * B;
+    const double f0 = 1.0 / AB;
+    const double f1 = (A + B) / (AB * AB);
+    const double f2 = (A * A + AB + B * B) / (AB * AB * AB);
+    return f0 + d * (f1 + d * f2);
+}
+
+// Deposit one line's bin means: exact within the line's window; beyond it
+// the far envelope w/(2 a^2) / ((E_lo - E_r)(E_hi - E_r)) is carried by three
+// moments about the centre bin and spread by far_field_kernel onto every bin
+// more than K_far bins away. A line whose window is wider than K_far
+// removes the envelope again from its extra exact bins, so each bin takes
+// exactly one of the two forms.
+__device__ void deposit_binmean(double E_r, double a, double w, const BinAxis &ax,
+                                double exact_widths, int K_far, double *spec, double *mom) {
+    const int n = ax.n;
+    int c = bin_of(ax, E_r);
+    bool use_mom = mom != nullptr && K_far > 0;
+    if (use_mom && (c < -ax.pad || c >= n + ax.pad)) use_mom = false;
+    int K;
+    if (!use_mom) {
+        K = n + (c < 0 ? -c : (c >= n ? c - n + 1 : 0));
+    } else {
+        const double kk = ceil(exact_widths * kPi / (a * ax.w));
+        K = kk > (double)(2 * n) ? 2 * n : (kk < (double)K_far ? K_far : (int)kk);
+    }
+    int b0 = c - K, b1 = c + K;
+    if (b0 < 0) b0 = 0;
+    if (b1 > n - 1) b1 = n - 1;
+    const double m = w / (2.0 * a * a);
+    const double E_c = use_mom ? centre_of(ax, c) : 0.0;
+    if (b0 <= b1) {
+        const double scale = kPi / a;
+        double x_lo = a * (ax.edges[b0] - E_r) / kPi;
+        double r_lo = sincsq_tail(x_lo);
+        for (int b = b0; b <= b1; ++b) {
+            const double x_hi = a * (ax.edges[b + 1] - E_r) / kPi;
+            const double r_hi = sincsq_tail(x_hi);
+            const double mass = r_hi - r_lo + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
+            const double width = ax.edges[b + 1] - ax.edges[b];
+            double v = w * (mass * scale / width);
+            if (use_mom && (b - c > K_far || c - b > K_far))
+                v -= m * far_envelope(ax.edges[b] - E_c, ax.edges[b + 1] - E_c, E_r - E_c);
+            atomicAdd(&spec[b], v);
+            x_lo = x_hi;
+            r_lo = r_hi;
+        }
+    }
+    if (use_mom) {
+        const int slot = c + ax.pad;
+        const double dd = E_r - E_c;
+        atomicAdd(&mom[3 * slot + 0], m);
+        atomicAdd(&mom[3 * slot + 1], m * dd);
+        atomicAdd(&mom[3 * slot + 2], m * dd * dd);
+    }
+}
+
+// One block: a direction (blockIdx.y) and a strided range of segment tiles.
+template <class Real>
+__global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int d = blockIdx.y;
+    const double *nh = a.n_hat + 3 * d;
+    const int n_g = a.tables.n_g;
+    const int n_tab = a.tables.n_tab;
+    const int n_mu = a.tables.n_mu;
+    const bool binmean = a.quadrature == PB_QUAD_BINMEAN;
+    const int n_E = a.n_E;
+    int64_t n_seg = a.n_seg;
+    if (a.n_seg_device) n_seg = (int64_t)*a.n_seg_device;
+    if (n_seg > a.n_seg && a.n_seg > 0) n_seg = a.n_seg;
+
+    // Shared layout: [rows chunk][seg tile][E_tab][delta][log_mu][spec][moments]
+    unsigned char *cur = smem_raw;
+    RowPre<Real> *rows = reinterpret_cast<RowPre<Real> *>(cur);
+    cur += sizeof(RowPre<Real>) * kRowChunk;
+    SegPre<Real> *segs = reinterpret_cast<SegPre<Real> *>(cur);
+    cur += sizeof(SegPre<Real>) * kSegTile;
+    cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
+    const bool tab_smem = n_tab <= kMaxTab;
+    Real *E_tab_s = reinterpret_cast<Real *>(cur);
+    Real *delta_s = E_tab_s + (tab_smem ? n_tab : 0);
+    Real *logmu_s = delta_s + (tab_smem ? n_tab : 0);
+    cur = reinterpret_cast<unsigned char *>(logmu_s + (tab_smem ? n_tab * n_mu : 0));
+    cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
+    double *spec_s = reinterpret_cast<double *>(cur);
+    double *mom_s = spec_s + (binmean ? n_E : 0);
+    const int n_mom = n_E + 2 * far_pad;
+
+    const int tid = threadIdx.x;
+    if (tab_smem) {
+        for (int j = tid; j < n_tab; j += blockDim.x) {
+            E_tab_s[j] = (Real)a.tables.E_tab[j];
+            delta_s[j] = (Real)a.tables.delta[j];
+        }
+        for (int j = tid; j < n_tab * n_mu; j += blockDim.x) logmu_s[j] = (Real)a.tables.log_mu[j];
+    }
+    if (binmean) {
+        for (int j = tid; j < n_E; j += blockDim.x) spec_s[j] = 0.0;
+        if (K_far > 0)
+            for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
+    }
+    // The tables are converted to the flight precision in global memory only
+    // for FP64, where the layouts agree; the float path reads the staged copy.
+    const Real *E_tab = tab_smem ? E_tab_s : reinterpret_cast<const Real *>(a.tables.E_tab);
+    const Real *delta_tab = tab_smem ? delta_s : reinterpret_cast<const Real *>(a.tables.delta);
+    const Real *log_mu = tab_smem ? logmu_s : reinterpret_cast<const Real *>(a.tables.log_mu);
+
+    BinAxis ax{};
+    if (binmean) {
+        ax.edges = a.edges;
+        ax.n = n_E;
+        ax.uniform = K_far > 0;  // the launcher enables moments on uniform axes only
+        ax.lo = a.edges[0];
+        ax.w = (a.edges[n_E] - a.edges[0]) / n_E;
+        ax.inv_w = 1.0 / ax.w;
+        ax.pad = far_pad;
+    }
+    __syncthreads();
+
+    const int64_t n_tiles = (n_seg + kSegTile - 1) / kSegTile;
+    const bool pairs_out = a.pair_E != nullptr;
+    const bool lines_out = a.line_E != nullptr;
+    const double exact_widths = K_far > 0 ? a.exact_widths : 0.0;
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int64_t s0 = tile * kSegTile;
+        const int nst = (int)((n_seg - s0) < kSegTile ? (n_seg - s0) : kSegTile);
+        __syncthreads();
+        if (tid < nst) seg_precompute<Real>(segs[tid], a, s0 + tid, nh);
+        for (int g0 = 0; g0 < n_g; g0 += kRowChunk) {
+            const int ng = (n_g - g0) < kRowChunk ? (n_g - g0) : kRowChunk;
+            __syncthreads();
+            for (int j = tid; j < ng; j += blockDim.x) {
+                const int g = g0 + j;
+                RowPre<Real> &r = rows[j];
+                const double *G = a.tables.G + 3 * g;
+                const double *ES = a.tables.ES + 3 * g;
+                const double *EP = a.tables.EP + 3 * g;
+                for (int c = 0; c < 3; ++c) {
+                    r.G[c] = (Real)G[c];
+                    r.ES[c] = (Real)ES[c];
+                    r.EP[c] = (Real)EP[c];
+                }
+                r.g2 = r.G[0] * r.G[0] + r.G[1] * r.G[1] + r.G[2] * r.G[2];
+                r.n_dot_g = r.G[0] * (Real)nh[0] + r.G[1] * (Real)nh[1] + r.G[2] * (Real)nh[2];
+                r.g_dot_es = r.G[0] * r.ES[0] + r.G[1] * r.ES[1] + r.G[2] * r.ES[2];
+                r.g_dot_ep = r.G[0] * r.EP[0] + r.G[1] * r.EP[1] + r.G[2] * r.EP[2];
+                r.wm = (Real)a.tables.WM[g];
+                r.row = a.tables.row_table[g];
+            }
+            __syncthreads();
+            const int n_pairs = nst * ng;
+            for (int q = tid; q < n_pairs; q += blockDim.x) {
+                const int si = q / ng;
+                const int gi = q - si * ng;
+                const Line<Real> ln =
+                    pair_line<Real>(segs[si], rows[gi], nh, E_tab, delta_tab, log_mu, n_tab, n_mu, a.tables);
+                if (pairs_out) {
+                    const int64_t o = ((int64_t)d * n_seg + s0 + si) * n_g + g0 + gi;
+                    a.pair_E[o] = (double)ln.E_res;
+                    a.pair_a[o] = (double)ln.a_width;
+                    a.pair_w[o] = (double)ln.weight;
+                    a.pair_good[o] = ln.good ? 1 : 0;
+                }
+                if (!ln.good) continue;
+                if (lines_out) {
+                    const unsigned long long slot = atomicAdd(a.line_count, 1ULL);
+                    if (slot < (unsigned long long)a.line_capacity) {
+                        a.line_E[slot] = (double)ln.E_res;
+                        a.line_a[slot] = (double)ln.a_width;
+                        a.line_w[slot] = (double)ln.weight;
+                        a.line_dir[slot] = d;
+                    } else {
+                        set_status(a.status, PB_DEV_QUEUE_OVERFLOW);
+                    }
+                }
+                if (binmean)
+                    deposit_binmean((double)ln.E_res, (double)ln.a_width, (double)ln.weight, ax,
+                                    exact_widths, K_far, spec_s, K_far > 0 ? mom_s : nullptr);
+            }
+        }
+    }
+    __syncthreads();
+    if (binmean) {
+        double *gspec = a.spec + (int64_t)d * n_E;
+        for (int j = tid; j < n_E; j += blockDim.x)
+            if (spec_s[j] != 0.0) atomicAdd(&gspec[j], spec_s[j]);
+        if (K_far > 0) {
+            double *gm = a.far_moments + (int64_t)d * n_mom * 3;
+            for (int j = tid; j < 3 * n_mom; j += blockDim.x)
+                if (mom_s[j] != 0.0) atomicAdd(&gm[j], mom_s[j]);
+        }
+    }
+}
+
+// Far-field finalize: spec[d][b] += sum_c M[d][c] . envelope(b, c) over the
+// (padded, uniform) centre bins c farther than K_far bins from b.
+__global__ void far_field_kernel(const double *edges, int n_E, int pad, const double *mom,
+                                 double *spec, int K_far) {
+    const int d = blockIdx.y;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_E) return;
+    const int n_mom = n_E + 2 * pad;
+    const double *m = mom + (int64_t)d * n_mom * 3;
+    const double lo = edges[0];
+    const double w = (edges[n_E] - edges[0]) / n_E;
+    const double E_lo = edges[b], E_hi = edges[b + 1];
+    double acc = 0.0;
+    for (int slot = 0; slot < n_mom; ++slot) {
+        const int c = slot - pad;
+        if (c >= b - K_far && c <= b + K_far) continue;
+        const double m0 = m[3 * slot];
+        if (m0 == 0.0) continue;
+        const double E_c = lo + ((double)c + 0.5) * w;
+        const double A = E_lo - E_c, B = E_hi - E_c;
+        const double AB = A * B;
+        const double f0 = 1.0 / AB;
+        const double f1 = (A + B) / (AB * AB);
+        const double f2 = (A * A + AB + B * B) / (AB * AB * AB);
+        acc += m0 * f0 + m[3 * slot + 1] * f1 + m[3 * slot + 2] * f2;
+    }
+    spec[(int64_t)d * n_E + b] += acc;
+}
+
+// Node reduction of buffered lines: spec[d][e] += sum_j w_j sinc^2(x_je),
+// x = a (E_e - E_j) / pi, with the phase a (E_e - E_j) formed in double.
+template <class Real>
+__global__ void node_reduce_kernel(const double *E_grid, int n_E, const double *line_E,
+                                   const double *line_a, const double *line_w, const int32_t *line_dir,
+                                   const unsigned long long *line_count, int64_t capacity,
+                                   double *spec) {
+    constexpr int kTile = 256;
+    __shared__ double sE[kTile], sA[kTile], sW[kTile];
+    __shared__ int sD[kTile];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t n_lines = (int64_t)*line_count;
+    if (n_lines > capacity) n_lines = capacity;
+    const int64_t per = (n_lines + gridDim.y - 1) / gridDim.y;
+    const int64_t j0 = per * blockIdx.y;
+    const int64_t j1 = j0 + per < n_lines ? j0 + per : n_lines;
+    const double E = e < n_E ? E_grid[e] : 0.0;
+    // Accumulate per direction seen in this chunk (directions are few).
+    double acc = 0.0;
+    int cur_dir = -1;
+    for (int64_t t0 = j0; t0 < j1; t0 += kTile) {
+        const int nt = (int)((j1 - t0) < kTile ? (j1 - t0) : kTile);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+            sE[j] = line_E[t0 + j];
+            sA[j] = line_a[t0 + j];
+            sW[j] = line_w[t0 + j];
+            sD[j] = line_dir[t0 + j];
+        }
+        __syncthreads();
+        if (e < n_E) {
+            for (int k = 0; k < nt; ++k) {
+                if (sD[k] != cur_dir) {
+                    if (cur_dir >= 0 && acc != 0.0) atomicAdd(&spec[(int64_t)cur_dir * n_E + e], acc);
+                    acc = 0.0;
+                    cur_dir = sD[k];
+                }
+                double x = sA[k] * (E - sE[k]) / kPi;
+                if (x == 0.0) x = 1.0e-20;
+                double s;
+                if constexpr (sizeof(Real) == 8) {
+                    const double y = kPi * x;
+                    s = sin(y) / y;
+                } else {
+                    // y = pi x reduced to [-pi, pi] in double, sine in float.
+                    const double y = kPi * x;
+                    const double r = y - 2.0 * kPi * rint(y / (2.0 * kPi));
+                    s = (double)__sinf((float)r) / y;
+                }
+                acc += sW[k] * (s * s);
+            }
+        }
+    }
+    if (e < n_E && cur_dir >= 0 && acc != 0.0) atomicAdd(&spec[(int64_t)cur_dir * n_E + e], acc);
+}
+
+template <class Real>
+static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moments) {
+    size_t b = sizeof(RowPre<Real>) * kRowChunk + sizeof(SegPre<Real>) * kSegTile + 16;
+    if (a.tables.n_tab <= kMaxTab) b += sizeof(Real) * (size_t)a.tables.n_tab * (2 + a.tables.n_mu);
+    b += 16;
+    if (a.quadrature == PB_QUAD_BINMEAN) {
+        b += sizeof(double) * (size_t)a.n_E;
+        if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
+    }
+    return b;
+}
+
+
+
+template <class Real>
+static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, int far_pad) {
+    const bool binmean = a.quadrature == PB_QUAD_BINMEAN;
+    const int K_far = (binmean && a.exact_widths > 0.0 && a.far_moments && far_pad >= 0) ? 2 : 0;
+    if (K_far == 0) far_pad = 0;
+    size_t smem = cxr_smem_bytes<Real>(a, far_pad, K_far > 0);
+    if (smem > 220 * 1024) return cudaErrorInvalidValue;
+    auto kern = cxr_kernel<Real>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    if (K_far > 0) {
+        err = cudaMemsetAsync(a.far_moments, 0,
+                              sizeof(double) * (size_t)a.n_dir * (a.n_E + 2 * far_pad) * 3, s);
+        if (err != cudaSuccess) return err;
+    }
+    if (a.line_count) {
+        err = cudaMemsetAsync(a.line_count, 0, sizeof(unsigned long long), s);
+        if (err != cudaSuccess) return err;
+    }
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCxrThreads, smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t tiles = (a.n_seg + kSegTile - 1) / kSegTile;
+    int64_t gx = ((int64_t)sms * per_sm + a.n_dir - 1) / a.n_dir;
+    if (gx > tiles) gx = tiles;
+    if (gx < 1) gx = 1;
+    dim3 grid((unsigned)gx, (unsigned)a.n_dir);
+    kern<<<grid, kCxrThreads, smem, s>>>(a, K_far, far_pad);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (K_far > 0) {
+        dim3 fg((unsigned)((a.n_E + 127) / 128), (unsigned)a.n_dir);
+        far_field_kernel<<<fg, 128, 0, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
+        err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+    }
+    if (a.quadrature == PB_QUAD_NODE && a.line_E != nullptr) {
+        dim3 ng((unsigned)((a.n_E + 127) / 128), 64);
+        node_reduce_kernel<Real><<<ng, 128, 0, s>>>(a.E_grid, a.n_E, a.line_E, a.line_a, a.line_w,
+                                                    a.line_dir, a.line_count, a.line_capacity, a.spec);
+        err = cudaGetLastError();
+    }
+    return err;
+}
+
+cudaError_t launch_cxr(const pb_cxr_args &a, cudaStream_t s, int sms) {
+    if (a.precision == PB_MIXED) return launch_cxr_t<float>(a, s, sms, a.far_pad);
+    return launch_cxr_t<double>(a, s, sms, a.far_pad);
+}
+
+}  // namespace pb

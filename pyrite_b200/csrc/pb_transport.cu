@@ -1,0 +1,645 @@
+// Persistent electron-transport kernel (sm_100a).
+//
+// One history per thread, structure-of-arrays state in registers, refilled
+// from a global work counter: after every event the warp ballots its idle
+// lanes and one lane claims that many new histories with a single atomic, so
+// lanes never sit on a finished history while the rest of the warp works.
+//
+// Physics is the reference's per-electron core with the data-free set
+// (src/pyrite/montecarlo/transport/cores.py:379-1230): screened-Rutherford
+// elastic scattering, spliced Joy-Luo / Berger-Seltzer stopping, the
+// midpoint (RK2) energy rule, layered slabs. Two forms of the energy
+// dependence are compiled: the exact analytic expressions (FP64 parity with
+// the reference's exact core) and the reference's default uniform-log-energy
+// LUT (transport/lut.py), staged once per block into shared memory by a
+// non-multicast bulk copy. The RNG is either the reference's SplitMix64
+// counter stream (bit-compatible draws) or Philox4x32-10 keyed by
+// (seed, history) with the draw index as counter.
+//
+// Precision: PB_FP64 runs everything in double. PB_MIXED runs rates,
+// geometry and flight steps in float and keeps the per-history energy and
+// clock bookkeeping in double.
+#include <cstdint>
+#include <cstdio>
+
+#include "pb_common.cuh"
+#include "pb_internal.h"
+
+namespace pb {
+
+constexpr int kMaxLayers = 8;
+constexpr int kMaxEl = 8;
+constexpr double kEps = 1e-6;
+
+enum : int8_t {
+    EV_ELASTIC = 0,
+    EV_LAYER_BOUNDARY = 2,
+    EV_EXIT_TOP = 4,
+    EV_EXIT_BOTTOM = 5,
+    EV_CUTOFF = 7
+};
+enum : int8_t {
+    EXIT_CUTOFF = 0,
+    EXIT_BACK = 1,
+    EXIT_TRANS = 2,
+    EXIT_SIDE = 3,
+    EXIT_STEP = 4,
+    EXIT_NOT_ENTERED = 5
+};
+
+// Layer geometry and exact-physics coefficients, copied to shared memory.
+struct LayerSmem {
+    double z_top[kMaxLayers];
+    double z_bot[kMaxLayers];
+    int n_el[kMaxLayers];
+    double J[kMaxLayers * kMaxEl];
+    double k[kMaxLayers * kMaxEl];
+    double coeff[kMaxLayers * kMaxEl];
+    double E_cross[kMaxLayers * kMaxEl];
+    double srn[kMaxLayers * kMaxEl];
+    double sjn[kMaxLayers * kMaxEl];
+};
+
+// Math in the precision of the flight arithmetic.
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sin(double x) { return sin(x); }
+__device__ __forceinline__ float m_sin(float x) { return sinf(x); }
+__device__ __forceinline__ double m_cos(double x) { return cos(x); }
+__device__ __forceinline__ float m_cos(float x) { return cosf(x); }
+
+// stopping.py:384-410 (_dEds_spliced_packed_scalar), density effect 0.
+template <class Real>
+__device__ __forceinline__ Real dEds_spliced(const LayerSmem &ly, int max_el, int L, Real E) {
+    const Real tau = E / (Real)kMc2Kev;
+    const Real gamma = (Real)1 + tau;
+    const Real beta_sq = (Real)1 - (Real)1 / (gamma * gamma);
+    const Real f_minus = (Real)1 - beta_sq +
+                         (tau * tau / (Real)8 - ((Real)2 * tau + (Real)1) * (Real)kLn2) / (gamma * gamma);
+    Real jl = 0, bs = 0;
+    const int n = ly.n_el[L];
+    for (int i = 0; i < n; ++i) {
+        const int ix = L * max_el + i;
+        const Real J = (Real)ly.J[ix], coeff = (Real)ly.coeff[ix];
+        if (E < (Real)ly.E_cross[ix]) {
+            jl += coeff * m_log((Real)1.166 * (E + (Real)ly.k[ix] * J) / J);
+        } else {
+            const Real I_rel = J / (Real)kMc2Kev;
+            bs += coeff * (m_log(tau * tau * (tau + (Real)2) / ((Real)2 * I_rel * I_rel)) + f_minus - (Real)0);
+        }
+    }
+    return -(Real)7.85e-4 / E * jl - (Real)kBsPrefactor / beta_sq * bs;
+}
+
+// scattering.py:208-218
+template <class Real>
+__device__ __forceinline__ Real sr_rate(Real E, Real srn, Real sjn) {
+    const Real a = sjn / E;
+    const Real r = (E + (Real)511) / (E + (Real)1024);
+    return srn / (E * E) / (a * ((Real)1 + a)) * (r * r);
+}
+
+// kinematics.py:162-166
+template <class Real>
+__device__ __forceinline__ Real beta_from_keV(Real E) {
+    const Real g = (Real)1 + E / (Real)kMc2Kev;
+    const Real gis = (Real)1 / (g * g);
+    return m_sqrt((Real)1 - gis);
+}
+
+// core_geometry.py:16-35
+template <class Real>
+__device__ __forceinline__ void rotate(Real &dx, Real &dy, Real &dz, Real cos_t, Real phi) {
+    const Real st2 = (Real)1 - cos_t * cos_t;
+    const Real sin_t = m_sqrt(st2 > (Real)0 ? st2 : (Real)0);
+    const Real cp = m_cos(phi), sp = m_sin(phi);
+    Real refx, refy;
+    if (fabs(dx) < (Real)0.9) { refx = 1; refy = 0; } else { refx = 0; refy = 1; }
+    Real ux = -dz * refy, uy = dz * refx, uz = dx * refy - dy * refx;
+    const Real um = m_sqrt(ux * ux + uy * uy + uz * uz);
+    ux /= um; uy /= um; uz /= um;
+    const Real wx = dy * uz - dz * uy, wy = dz * ux - dx * uz, wz = dx * uy - dy * ux;
+    const Real a = sin_t * cp, b = sin_t * sp;
+    const Real ox = cos_t * dx + a * ux + b * wx;
+    const Real oy = cos_t * dy + a * uy + b * wy;
+    const Real oz = cos_t * dz + a * uz + b * wz;
+    const Real m = m_sqrt(ox * ox + oy * oy + oz * oz);
+    dx = ox / m; dy = oy / m; dz = oz / m;
+}
+
+// LUT view (shared or global memory) in the flight precision.
+template <class Real>
+struct LutView {
+    const Real *rate;
+    const Real *dEds;
+    const Real *inv_beta;
+    const Real *cdf;
+    const Real *alpha;
+    int ne;
+    double log_E_min;
+    double inv_dlogE;
+};
+
+// lut.py:118-137: one log, one multiply, clamped index and fraction.
+template <class Real>
+__device__ __forceinline__ void lut_index(const LutView<Real> &t, double E, int &i, Real &f) {
+    Real x;
+    if constexpr (sizeof(Real) == 8) x = (log(E) - t.log_E_min) * t.inv_dlogE;
+    else x = (logf((float)E) - (float)t.log_E_min) * (float)t.inv_dlogE;
+    const int last = t.ne - 1;
+    if (x >= (Real)last) { i = last - 1; f = 1; return; }
+    if (x > (Real)0) { const int ii = (int)x; i = ii; f = x - (Real)ii; return; }
+    i = 0;
+    f = 0;
+}
+
+template <class Real>
+__device__ __forceinline__ Real lerp(const Real *row, int i, Real f) {
+    return row[i] + f * (row[i + 1] - row[i]);
+}
+
+// Normal quantile of an open uniform (the reference uses scipy ndtri,
+// kinematics.py:302-311; normcdfinv is CUDA's inverse normal CDF).
+__device__ __forceinline__ double normal_from(double u) { return normcdfinv(u); }
+
+// Entrance state of history ``e`` (global index) at local index ``i``.
+template <int kRng>
+__device__ void sample_entry(const pb_transport_args &p, int64_t i, int64_t e, double pos[3],
+                             double dir[3], double &E) {
+    const pb_beam &b = p.beam;
+    if (b.mode == PB_BEAM_EXPLICIT) {
+        pos[0] = b.pos0[3 * i]; pos[1] = b.pos0[3 * i + 1]; pos[2] = b.pos0[3 * i + 2];
+        dir[0] = b.dir0[3 * i]; dir[1] = b.dir0[3 * i + 1]; dir[2] = b.dir0[3 * i + 2];
+        E = b.E0[i];
+        return;
+    }
+    // Counter-addressed normals of the entry namespace (kinematics.py:270-311).
+    const uint64_t key = stream_key(b.root, (uint64_t)e);
+    double z[4];
+    const int nz = b.mode == PB_BEAM_TWISS ? 4 : 2;
+    for (int c = 0; c < nz; ++c) {
+        double u;
+        if constexpr (kRng == PB_RNG_PHILOX) {
+            // 52-bit open uniform built from one Philox draw.
+            const double w = philox_uniform(key, (uint64_t)c);
+            u = (floor(w * 4503599627370496.0) + 0.5) * (1.0 / 4503599627370496.0);
+        } else {
+            u = splitmix_open_uniform(key, (uint64_t)c);
+        }
+        z[c] = normal_from(u);
+    }
+    double u_off, v_off, xp = 0.0, yp = 0.0;
+    if (b.mode == PB_BEAM_TWISS) {
+        // transverse.py:177-186 with eps [mm rad], beta [mm/rad]
+        const double ex = b.twiss_x[0], bx = b.twiss_x[1], ax = b.twiss_x[2];
+        const double ey = b.twiss_y[0], by = b.twiss_y[1], ay = b.twiss_y[2];
+        const double x_mm = sqrt(ex * bx) * z[0];
+        xp = sqrt(ex / bx) * (z[1] - ax * z[0]);
+        const double y_mm = sqrt(ey * by) * z[2];
+        yp = sqrt(ey / by) * (z[3] - ay * z[2]);
+        u_off = x_mm * 1.0e7;
+        v_off = y_mm * 1.0e7;
+    } else {
+        u_off = z[0] * b.sigma_x_ang;
+        v_off = z[1] * b.sigma_y_ang;
+    }
+    // geometry.py:374-390 (_project_entry_rows)
+    if (b.tilted) {
+        const double s_star = -(u_off * b.e_x[2] + v_off * b.e_y[2]) / b.beam_dir[2];
+        pos[0] = (u_off * b.e_x[0] + v_off * b.e_y[0]) + s_star * b.beam_dir[0];
+        pos[1] = (u_off * b.e_x[1] + v_off * b.e_y[1]) + s_star * b.beam_dir[1];
+    } else {
+        pos[0] = u_off;
+        pos[1] = v_off;
+    }
+    pos[2] = 0.0;
+    if (b.mode == PB_BEAM_TWISS) {
+        // beam_entry.py:347-359: (x', y', 1) in the beam frame, normalised
+        double d[3];
+        for (int c = 0; c < 3; ++c)
+            d[c] = (xp * b.basis[3 * c + 0] + yp * b.basis[3 * c + 1]) + b.beam_dir[c];
+        const double nrm = sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+        dir[0] = d[0] / nrm; dir[1] = d[1] / nrm; dir[2] = d[2] / nrm;
+    } else {
+        dir[0] = b.beam_dir[0]; dir[1] = b.beam_dir[1]; dir[2] = b.beam_dir[2];
+    }
+    E = b.E0_keV;
+}
+
+struct TallySmem {
+    unsigned long long fates[6];
+    unsigned long long exit_E[258];
+    unsigned long long exit_theta[258];
+    double deposit[kMaxLayers];
+};
+
+__device__ __forceinline__ int hist_slot(double v, double lo, double hi, int n) {
+    if (!(v >= lo)) return 0;  // underflow (NaN counts as underflow)
+    if (v > hi) return n + 1;
+    int b = (int)((v - lo) / (hi - lo) * n);
+    if (b >= n) b = n - 1;
+    return b + 1;
+}
+
+template <class Real, bool kLut, int kRng>
+__global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ LayerSmem ly;
+    __shared__ TallySmem tal;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int lut_in_smem;
+
+    const int tid = threadIdx.x;
+    const int n_layers = p.layers.n_layers;
+    const int max_el = p.layers.max_el;
+    for (int j = tid; j < n_layers; j += blockDim.x) {
+        ly.z_top[j] = p.layers.z_top[j];
+        ly.z_bot[j] = p.layers.z_bot[j];
+        ly.n_el[j] = p.layers.n_el[j];
+    }
+    for (int j = tid; j < n_layers * max_el; j += blockDim.x) {
+        ly.J[j] = p.layers.J[j];
+        ly.k[j] = p.layers.k[j];
+        ly.coeff[j] = p.layers.coeff[j];
+        ly.E_cross[j] = p.layers.E_cross[j];
+        ly.srn[j] = p.layers.sr_rate_numer[j];
+        ly.sjn[j] = p.layers.sr_joy_numer[j];
+    }
+    for (int j = tid; j < 6; j += blockDim.x) tal.fates[j] = 0;
+    const bool want_E = p.tallies.exit_E != nullptr && p.tallies.n_E <= 256;
+    const bool want_th = p.tallies.exit_theta != nullptr && p.tallies.n_theta <= 256;
+    for (int j = tid; j < 258; j += blockDim.x) { tal.exit_E[j] = 0; tal.exit_theta[j] = 0; }
+    for (int j = tid; j < kMaxLayers; j += blockDim.x) tal.deposit[j] = 0.0;
+
+    // Stage the LUT into shared memory with one bulk copy per 64 KiB chunk.
+    LutView<Real> lut{};
+    if constexpr (kLut) {
+        const Real *base = reinterpret_cast<const Real *>(p.lut.base);
+        const uint32_t bytes = (uint32_t)p.lut.total_bytes;
+        const bool fits = p.lut.total_bytes <= (int64_t)kLutSmemBytes;
+        if (tid == 0) {
+            lut_in_smem = 0;
+            if (fits) {
+                mbar_init(&mbar, 1);
+                mbar_expect_tx(&mbar, bytes);
+                for (uint32_t off = 0; off < bytes; off += 65536u) {
+                    const uint32_t chunk = bytes - off < 65536u ? bytes - off : 65536u;
+                    bulk_g2s(smem_raw + off, reinterpret_cast<const unsigned char *>(base) + off,
+                             chunk, &mbar);
+                }
+                if (mbar_wait(&mbar, 0)) {
+                    lut_in_smem = 1;
+                } else {
+                    set_status(p.status, PB_DEV_WAIT_TIMEOUT);
+                }
+            }
+        }
+        __syncthreads();
+        const Real *src = lut_in_smem ? reinterpret_cast<const Real *>(smem_raw) : base;
+        lut.rate = src + p.lut.off_total_rate;
+        lut.dEds = src + p.lut.off_dEds;
+        lut.inv_beta = src + p.lut.off_inv_beta;
+        lut.cdf = src + p.lut.off_cdf;
+        lut.alpha = src + p.lut.off_alpha;
+        lut.ne = p.lut.n_energy;
+        lut.log_E_min = p.lut.log_E_min;
+        lut.inv_dlogE = p.lut.inv_dlogE;
+    }
+    __syncthreads();
+
+    const unsigned lane = tid & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const double E_cut = p.E_cut_keV;
+    const double z_total = ly.z_bot[n_layers - 1];
+    const bool want_rows = p.rows.L != nullptr;
+    const bool want_seg = p.seg.L != nullptr;
+    double dep_acc[kMaxLayers];
+#pragma unroll
+    for (int j = 0; j < kMaxLayers; ++j) dep_acc[j] = 0.0;
+
+    // Per-history state.
+    int64_t i = -1;  // local history index; -1 idle, -2 drained
+    uint64_t key = 0, draws = 0;
+    Real px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 1;
+    double E = 0.0, clk = 0.0;
+    int64_t nseg = 0, steps = 0;
+    Real tau_left = -1;
+
+    while (true) {
+        const bool idle = (i == -1);
+        const unsigned idle_mask = __ballot_sync(0xffffffffu, idle);
+        if (idle_mask) {
+            const int leader = __ffs(idle_mask) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(p.work_counter, (unsigned long long)__popc(idle_mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (idle) {
+                const unsigned long long mine = base + __popc(idle_mask & lt_mask);
+                if (mine < (unsigned long long)p.n) {
+                    i = (int64_t)mine;
+                    const int64_t e = p.e_start + i;
+                    double pos[3], dir[3], E0;
+                    sample_entry<kRng>(p, i, e, pos, dir, E0);
+                    px = (Real)pos[0]; py = (Real)pos[1]; pz = (Real)pos[2];
+                    dx = (Real)dir[0]; dy = (Real)dir[1]; dz = (Real)dir[2];
+                    E = E0;
+                    clk = 0.0;
+                    key = stream_key(p.seed, (uint64_t)e);
+                    draws = 0;
+                    nseg = 0;
+                    steps = 0;
+                    tau_left = -1;
+                } else {
+                    i = -2;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, i >= 0) == 0u) break;
+        if (i < 0) continue;
+
+        // ---- one event (cores.py:402-1230) ----
+        int8_t code = -1;
+        if (steps >= p.max_steps) {
+            code = EXIT_STEP;
+            set_status(p.status, PB_DEV_STEP_LIMIT);
+        } else {
+            int L = 0;
+            if (n_layers > 1) {
+                // searchsorted(internal_bounds, z, side="right")
+                for (int j = 1; j < n_layers; ++j) L += (ly.z_top[j] <= (double)pz) ? 1 : 0;
+            }
+            const double z_top = ly.z_top[L], z_bot = ly.z_bot[L];
+            const int n_el = ly.n_el[L];
+            const double E_j = E;
+            const Real Er = (Real)E_j;
+            int li = 0;
+            Real lf = 0;
+            Real total_rate = 0;
+            if constexpr (kLut) {
+                lut_index(lut, E_j, li, lf);
+                total_rate = lerp(lut.rate + (int64_t)L * lut.ne, li, lf);
+            } else {
+                for (int k = 0; k < n_el; ++k) {
+                    const int ix = L * max_el + k;
+                    total_rate += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
+                }
+            }
+            const Real lam = (Real)1e8 / total_rate;
+            if (tau_left < (Real)0) {
+                tau_left = (Real)(-log(uniform<kRng>(key, draws)));
+                draws += 1;
+            }
+            Real step = tau_left * lam;
+            bool cross_up = false, cross_dn = false;
+            if (dz < (Real)0) {
+                const Real sb = (pz - (Real)z_top) / (-dz);
+                if (step > sb) { step = sb; cross_up = true; }
+            } else if (dz > (Real)0) {
+                const Real sb = ((Real)z_bot - pz) / dz;
+                if (step > sb) { step = sb; cross_dn = true; }
+            }
+            bool exit_top = cross_up && z_top <= 0.0;
+            bool exit_bot = cross_dn && z_bot >= z_total;
+            const bool geometry_event = cross_up || cross_dn;
+            Real dEds, cutoff_rate;
+            if constexpr (kLut) {
+                const Real *row = lut.dEds + (int64_t)L * lut.ne;
+                dEds = lerp(row, li, lf);
+                int ci;
+                Real cf;
+                lut_index(lut, 0.5 * (E_j + E_cut), ci, cf);
+                cutoff_rate = lerp(row, ci, cf);
+            } else {
+                dEds = dEds_spliced<Real>(ly, max_el, L, Er);
+                cutoff_rate = dEds_spliced<Real>(ly, max_el, L, (Real)(0.5 * (E_j + E_cut)));
+            }
+            const Real cutoff_distance = (Real)(E_cut - E_j) / cutoff_rate;
+            bool cutoff = false;
+            if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
+                step = cutoff_distance;
+                cutoff = true;
+                cross_up = cross_dn = exit_top = exit_bot = false;
+            }
+            double E_end;
+            if (cutoff) {
+                E_end = E_cut;
+            } else {
+                const double E_pred = E_j + (double)(dEds * step);
+                const double E_mid = 0.5 * (E_j + E_pred);
+                Real mid_rate;
+                if constexpr (kLut) {
+                    int mi;
+                    Real mf;
+                    lut_index(lut, E_mid, mi, mf);
+                    mid_rate = lerp(lut.dEds + (int64_t)L * lut.ne, mi, mf);
+                } else {
+                    mid_rate = dEds_spliced<Real>(ly, max_el, L, (Real)E_mid);
+                }
+                E_end = E_j + (double)(step * mid_rate);
+            }
+            Real inv_beta_mid;
+            if constexpr (kLut) {
+                int ki;
+                Real kf;
+                lut_index(lut, 0.5 * (E_j + E_end), ki, kf);
+                inv_beta_mid = lerp(lut.inv_beta, ki, kf);
+            }
+            double t_end;
+            if constexpr (kLut) t_end = clk + (double)(step * inv_beta_mid);
+            else t_end = clk + (double)step / (double)beta_from_keV<Real>((Real)(0.5 * (E_j + E_end)));
+            int8_t event;
+            if (cutoff) event = EV_CUTOFF;
+            else if (exit_top) event = EV_EXIT_TOP;
+            else if (exit_bot) event = EV_EXIT_BOTTOM;
+            else if (cross_up || cross_dn) event = EV_LAYER_BOUNDARY;
+            else event = EV_ELASTIC;
+            const Real half = (Real)0.5 * step;
+            if (want_rows) {
+                if (nseg < p.cap) {
+                    const int64_t s = i * p.cap + nseg;
+                    p.rows.v_hat[3 * s] = (double)dx;
+                    p.rows.v_hat[3 * s + 1] = (double)dy;
+                    p.rows.v_hat[3 * s + 2] = (double)dz;
+                    p.rows.r_mid[3 * s] = (double)(px + half * dx);
+                    p.rows.r_mid[3 * s + 1] = (double)(py + half * dy);
+                    p.rows.r_mid[3 * s + 2] = (double)(pz + half * dz);
+                    p.rows.L[s] = (double)step;
+                    p.rows.E_start[s] = E_j;
+                    p.rows.E_end[s] = E_end;
+                    p.rows.t_start[s] = clk;
+                    p.rows.t_end[s] = t_end;
+                    p.rows.elec_id[s] = p.e_start + i;
+                    p.rows.layer[s] = (int16_t)L;
+                    p.rows.flight[s] = nseg;
+                    p.rows.event[s] = event;
+                } else {
+                    set_status(p.status, PB_DEV_ROW_OVERFLOW);
+                }
+            }
+            if (want_seg) {
+                // Warp-aggregated append to the compact segment list.
+                const unsigned active = __activemask();
+                const int leader = __ffs(active) - 1;
+                unsigned long long base = 0;
+                if ((int)lane == leader) base = atomicAdd(p.seg.count, (unsigned long long)__popc(active));
+                base = __shfl_sync(active, base, leader);
+                const unsigned long long slot = base + __popc(active & lt_mask);
+                if (slot < (unsigned long long)p.seg.capacity) {
+                    p.seg.v_hat[3 * slot] = (double)dx;
+                    p.seg.v_hat[3 * slot + 1] = (double)dy;
+                    p.seg.v_hat[3 * slot + 2] = (double)dz;
+                    p.seg.r_mid[3 * slot] = (double)(px + half * dx);
+                    p.seg.r_mid[3 * slot + 1] = (double)(py + half * dy);
+                    p.seg.r_mid[3 * slot + 2] = (double)(pz + half * dz);
+                    p.seg.L[slot] = (double)step;
+                    p.seg.E_repr[slot] = 0.5 * (E_j + E_end);
+                    p.seg.elec_id[slot] = p.e_start + i;
+                    p.seg.layer[slot] = L;
+                } else {
+                    set_status(p.status, PB_DEV_QUEUE_OVERFLOW);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kMaxLayers; ++j)
+                if (j == L) dep_acc[j] += E_j - E_end;
+            nseg += 1;
+            px = px + step * dx;
+            py = py + step * dy;
+            pz = pz + step * dz;
+            E = E_end;
+            clk = t_end;
+            tau_left = (Real)-1;
+            if (exit_top || exit_bot || cutoff) {
+                code = exit_top ? EXIT_BACK : exit_bot ? EXIT_TRANS : EXIT_CUTOFF;
+            } else if (cross_up || cross_dn) {
+                pz += (dz > (Real)0 ? (Real)1 : (Real)-1) * (Real)kEps;
+                steps += 1;
+            } else {
+                int i_el = 0;
+                if (n_el > 1) {
+                    const double u = uniform<kRng>(key, draws);
+                    draws += 1;
+                    i_el = n_el - 1;
+                    if constexpr (kLut) {
+                        for (int k = 0; k < n_el; ++k) {
+                            const Real *cdf = lut.cdf + ((int64_t)L * max_el + k) * lut.ne;
+                            if ((double)lerp(cdf, li, lf) > u) { i_el = k; break; }
+                        }
+                    } else {
+                        const Real target = (Real)u * total_rate;
+                        Real cum = 0;
+                        for (int k = 0; k < n_el; ++k) {
+                            const int ix = L * max_el + k;
+                            cum += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
+                            if (cum > target) { i_el = k; break; }
+                        }
+                    }
+                }
+                Real alpha;
+                if constexpr (kLut) {
+                    int ai;
+                    Real af;
+                    lut_index(lut, E, ai, af);
+                    alpha = lerp(lut.alpha + ((int64_t)L * max_el + i_el) * lut.ne, ai, af);
+                } else {
+                    alpha = (Real)ly.sjn[L * max_el + i_el] / (Real)E;
+                }
+                const Real cos_u = (Real)uniform<kRng>(key, draws);
+                draws += 1;
+                const Real phi_u = (Real)uniform<kRng>(key, draws);
+                draws += 1;
+                const Real cos_t = (Real)1 - (Real)2 * alpha * cos_u / ((Real)1 + alpha - cos_u);
+                rotate<Real>(dx, dy, dz, cos_t, (Real)(2.0 * kPi) * phi_u);
+                steps += 1;
+            }
+        }
+        if (code >= 0) {
+            if (p.seg_count) p.seg_count[i] = nseg;
+            if (p.exit_code) p.exit_code[i] = code;
+            if (p.final_pos) {
+                p.final_pos[3 * i] = (double)px;
+                p.final_pos[3 * i + 1] = (double)py;
+                p.final_pos[3 * i + 2] = (double)pz;
+            }
+            if (p.final_dir) {
+                p.final_dir[3 * i] = (double)dx;
+                p.final_dir[3 * i + 1] = (double)dy;
+                p.final_dir[3 * i + 2] = (double)dz;
+            }
+            if (p.final_E) p.final_E[i] = E;
+            if (p.tallies.fates) atomicAdd(&tal.fates[code], 1ULL);
+            const bool escaped = code == EXIT_BACK || code == EXIT_TRANS || code == EXIT_SIDE;
+            if (escaped && want_E)
+                atomicAdd(&tal.exit_E[hist_slot(E, p.tallies.E_lo, p.tallies.E_hi, p.tallies.n_E)], 1ULL);
+            if (escaped && want_th) {
+                const double th = acos(fmin(fmax((double)dz, -1.0), 1.0));
+                atomicAdd(&tal.exit_theta[hist_slot(th, p.tallies.theta_lo, p.tallies.theta_hi,
+                                                    p.tallies.n_theta)],
+                          1ULL);
+            }
+            i = -1;
+        }
+    }
+
+    // Flush block tallies.
+    if (p.tallies.deposit) {
+        for (int j = 0; j < n_layers && j < kMaxLayers; ++j) {
+            double v = dep_acc[j];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0 && v != 0.0) atomicAdd(&tal.deposit[j], v);
+        }
+    }
+    __syncthreads();
+    if (p.tallies.fates)
+        for (int j = tid; j < 6; j += blockDim.x)
+            if (tal.fates[j]) atomicAdd(&p.tallies.fates[j], tal.fates[j]);
+    if (want_E)
+        for (int j = tid; j < p.tallies.n_E + 2; j += blockDim.x)
+            if (tal.exit_E[j]) atomicAdd(&p.tallies.exit_E[j], tal.exit_E[j]);
+    if (want_th)
+        for (int j = tid; j < p.tallies.n_theta + 2; j += blockDim.x)
+            if (tal.exit_theta[j]) atomicAdd(&p.tallies.exit_theta[j], tal.exit_theta[j]);
+    if (p.tallies.deposit)
+        for (int j = tid; j < n_layers && j < kMaxLayers; j += blockDim.x)
+            if (tal.deposit[j] != 0.0) atomicAdd(&p.tallies.deposit[j], tal.deposit[j]);
+}
+
+template <class Real, bool kLut, int kRng>
+static cudaError_t launch_transport_t(const pb_transport_args &a, cudaStream_t s, int sms) {
+    auto kern = transport_kernel<Real, kLut, kRng>;
+    size_t dyn = 0;
+    if (kLut && a.lut.total_bytes <= (int64_t)kLutSmemBytes) dyn = (size_t)a.lut.total_bytes;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kLutSmemBytes);
+    if (err != cudaSuccess) return err;
+    const int threads = a.block_threads > 0 ? a.block_threads : 128;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    int64_t want = (a.n + threads - 1) / threads;
+    int64_t grid = (int64_t)sms * per_sm;
+    if (want < grid) grid = want < 1 ? 1 : want;
+    kern<<<(unsigned)grid, threads, dyn, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transport(const pb_transport_args &a, cudaStream_t s, int sms) {
+    const bool mixed = a.precision == PB_MIXED;
+    const bool lut = a.use_lut != 0;
+    const bool philox = a.rng == PB_RNG_PHILOX;
+#define PB_DISPATCH(R, L, G) return launch_transport_t<R, L, G>(a, s, sms)
+    if (mixed) {
+        if (lut) { if (philox) PB_DISPATCH(float, true, PB_RNG_PHILOX); PB_DISPATCH(float, true, PB_RNG_SPLITMIX); }
+        if (philox) PB_DISPATCH(float, false, PB_RNG_PHILOX);
+        PB_DISPATCH(float, false, PB_RNG_SPLITMIX);
+    }
+    if (lut) { if (philox) PB_DISPATCH(double, true, PB_RNG_PHILOX); PB_DISPATCH(double, true, PB_RNG_SPLITMIX); }
+    if (philox) PB_DISPATCH(double, false, PB_RNG_PHILOX);
+    PB_DISPATCH(double, false, PB_RNG_SPLITMIX);
+#undef PB_DISPATCH
+}
+
+}  // namespace pb

@@ -1,0 +1,90 @@
+"""CUDA PXR + CBS scorer against the oracle and the reference's spectra.
+
+Pairs: every (segment, reflection) line of the FP64 kernel equals the oracle's
+to 1e-9 relative. Spectra: FP64 node and exact bin-mean agree with the
+reference to 1e-8 of the peak; the far-envelope bin-mean and the mixed
+precision kernel stay within 1e-3 and 1e-2 of the peak respectively (the
+north-star tolerance for mixed precision is 1 % spectrum error).
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import CXR_CASES, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def inputs(name):
+    from pyrite_b200 import LineTables
+    from pyrite_b200.tables import ReflectionRows
+
+    d = golden(f"cxr_{name}")
+    tr = golden(f"transport_{d['transport']}")
+    seg = dict(v_hat=tr["v_hat"], E_repr_keV=tr["E_repr_keV"], L_ang=tr["L_ang"], r_mid=tr["r_mid"],
+               elec_id=tr["elec_id"], Ne=int(d["Ne"]), thickness_ang=float(d["thickness"]))
+    tables = LineTables(d["E_tab"], d["chi_re"], d["chi_im"], d["u_re"], d["u_im"], d["log_mu"], d["delta"])
+    rows = ReflectionRows(d["G"], d["ES"][None], d["EP"][None], d["WM"], d["row_table"])
+    return d, seg, tables, rows
+
+
+def score(name, cuda_device, **kw):
+    from pyrite_b200 import mc_cxr_spectrum
+
+    d, seg, tables, rows = inputs(name)
+    return d, mc_cxr_spectrum(seg, d["E_grid"], str(d["crystal"]), None, tables=tables, n_hat=d["n_hat"],
+                              rows=rows, device=cuda_device, **kw)
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_pairs_match_oracle(case, cuda_device):
+    d, (spec, pairs) = score(case, cuda_device, line_quadrature="node", return_pairs=True)
+    E, a, w, good = pairs[0]
+    tr = golden(f"transport_{d['transport']}")
+    seg = dict(v_hat=tr["v_hat"], E_keV=tr["E_repr_keV"], L_ang=tr["L_ang"], r_mid=tr["r_mid"],
+               elec_id=tr["elec_id"])
+    E_grid = d["E_grid"]
+    pad = 0.2 * (E_grid[-1] - E_grid[0])
+    t = {k: d[k] for k in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re",
+                            "u_im", "log_mu", "delta")}
+    t["lo_keep"], t["hi_keep"] = E_grid[0] - pad, E_grid[-1] + pad
+    oE, oa, ow, og = oracle.cxr_lines(t, d["n_hat"], d["thickness"], seg, int(d["Ne"]))
+    good = good.astype(bool)
+    assert np.mean(good == og) > 0.9999
+    both = good & og
+    np.testing.assert_allclose(E[both], oE[both], rtol=1e-9)
+    np.testing.assert_allclose(a[both], oa[both], rtol=1e-9)
+    np.testing.assert_allclose(w[both], ow[both], rtol=1e-8)
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_node_spectrum_fp64(case, cuda_device):
+    d, spec = score(case, cuda_device, line_quadrature="node")
+    peak = np.max(np.abs(d["spec_node"]))
+    assert np.max(np.abs(spec - d["spec_node"])) <= 1e-8 * peak
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_binmean_exact_fp64(case, cuda_device):
+    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=None)
+    peak = np.max(np.abs(d["spec_binmean"]))
+    assert np.max(np.abs(spec - d["spec_binmean"])) <= 1e-8 * peak
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_binmean_far_envelope(case, cuda_device):
+    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=64.0)
+    ref = d["spec_binmean"]
+    peak = np.max(np.abs(ref))
+    assert np.max(np.abs(spec - ref)) <= 1e-3 * peak
+    assert spec.sum() == pytest.approx(ref.sum(), rel=1e-3)
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_mixed_precision_within_one_percent(case, cuda_device):
+    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=64.0, precision="mixed")
+    ref = d["spec_binmean"]
+    peak = np.max(np.abs(ref))
+    assert np.max(np.abs(spec - ref)) <= 1e-2 * peak
+    assert spec.sum() == pytest.approx(ref.sum(), rel=1e-2)
