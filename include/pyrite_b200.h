@@ -183,8 +183,8 @@ typedef struct pb_transport_args {
 typedef struct pb_cxr_tables {
     int32_t n_g;
     const double *G;        /* [n_g*3] 1/Angstrom, sample frame */
-    const double *ES;       /* [n_g*3] */
-    const double *EP;       /* [n_g*3] */
+    const double *ES;       /* [n_dir*n_g*3] sigma polarisation per direction */
+    const double *EP;       /* [n_dir*n_g*3] pi polarisation per direction */
     const double *WM;       /* [n_g] */
     const int32_t *row_table;  /* [n_g] */
     int32_t n_tab;
@@ -197,6 +197,10 @@ typedef struct pb_cxr_tables {
     const double *log_mu;   /* [n_mu*n_tab] */
     const double *delta;    /* [n_tab] */
     double lo_keep, hi_keep;
+    /* Geometric E_tab (E_tab[i] = exp(tab_log0 + i tab_log_step)) enables a
+     * closed-form bracket; tab_log_step <= 0 means a general ascending grid. */
+    double tab_log0;
+    double tab_log_step;
 } pb_cxr_tables;
 
 typedef struct pb_cxr_args {

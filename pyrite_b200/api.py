@@ -26,6 +26,7 @@ from .tables import (
     build_transport_lut,
     child_stream_root,
     energy_bin_edges,
+    geometric_grid,
     line_keep_window,
     reflection_rows,
 )
@@ -48,17 +49,20 @@ class _Holder:
     def __init__(self, device):
         self.device = device
         self.keep = []
+        self.inputs = []  # device tensors filled from host data (the call's inputs)
 
     def f64(self, a) -> torch.Tensor:
         t = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64) if not torch.is_tensor(a) else a)
         t = t.to(self.device, torch.float64).contiguous()
         self.keep.append(t)
+        self.inputs.append(t)
         return t
 
     def typed(self, a, dtype) -> torch.Tensor:
         t = a if torch.is_tensor(a) else torch.as_tensor(np.ascontiguousarray(a))
         t = t.to(self.device, dtype).contiguous()
         self.keep.append(t)
+        self.inputs.append(t)
         return t
 
     def zeros(self, shape, dtype) -> torch.Tensor:
@@ -325,6 +329,7 @@ def _fill_tables(h: _Holder, rows, tables: LineTables, lo_keep, hi_keep, d_index
     t.log_mu = _ptr(h.f64(lm))
     t.delta = _ptr(h.f64(tables.delta))
     t.lo_keep, t.hi_keep = float(lo_keep), float(hi_keep)
+    t.tab_log0, t.tab_log_step = geometric_grid(tables.E_tab)
     return t
 
 

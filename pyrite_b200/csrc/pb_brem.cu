@@ -24,6 +24,7 @@ namespace pb {
 constexpr int kBremThreads = 256;
 constexpr int kBremChunk = 256;
 constexpr int kBremMaxEl = 4;
+constexpr int kBremMaxDir = 16;
 
 template <class Real>
 struct BremSeg {
@@ -61,12 +62,12 @@ __device__ __forceinline__ Real b_mean_transmission(Real t0, Real t1) {
 }
 
 template <class Real>
-__global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a, int64_t n_seg) {
+__global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
     __shared__ BremSeg<Real> segs[kBremChunk];
     __shared__ Real Zs[kBremMaxEl];
-    const int d = blockIdx.z;
-    const double *nh = a.n_hat + 3 * d;
-    const Real nz = (Real)nh[2];
+    __shared__ Real inv_nz[kBremMaxDir];
+    __shared__ int up[kBremMaxDir];
+    const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
     const Real T_slab = (Real)a.thickness;
     const int n_el = a.n_el;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -74,12 +75,19 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
     const Real mc2 = (Real)510.99895;
     const Real za = (Real)(2.0 * kPi * kAlphaFs);
     if (threadIdx.x < n_el) Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+    if (threadIdx.x < nd) {
+        const Real nz = (Real)a.n_hat[3 * (d0 + threadIdx.x) + 2];
+        inv_nz[threadIdx.x] = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
+        up[threadIdx.x] = nz < (Real)0;
+    }
     const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
     const Real k = (Real)k_kev_d;
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
     const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
     const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
-    double acc = 0.0;
+    double acc[kBremMaxDir];
+#pragma unroll
+    for (int j = 0; j < kBremMaxDir; ++j) acc[j] = 0.0;
     if (a.n_seg_device) {
         const int64_t live = (int64_t)*a.n_seg_device;
         if (live < n_seg) n_seg = live;
@@ -102,8 +110,10 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
             const Real half = (Real)0.5 * (Real)a.L[s];
             const Real z = (Real)a.r_mid[3 * s + 2];
             const Real vz = (Real)a.v_hat[3 * s + 2];
-            b.path0 = b_path<Real>(z - half * vz, T_slab, nz);
-            b.path1 = b_path<Real>(z + half * vz, T_slab, nz);
+            // Depth of each segment end below the top face, clipped to the slab;
+            // the escape path toward n is depth/|n_z| (up) or (T - depth)/|n_z|.
+            b.path0 = fmin(fmax(z - half * vz, (Real)0), T_slab);
+            b.path1 = fmin(fmax(z + half * vz, (Real)0), T_slab);
             const bool rad = a.elec_id[s] < a.Ne;
             const Real path_cm = (Real)a.L[s] * (Real)1e-8;
             for (int el = 0; el < n_el; ++el) {
@@ -113,45 +123,90 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
         }
         __syncthreads();
         if (!on) continue;
+        // Float partial sums per chunk, folded into the FP64 accumulators once
+        // per chunk; FP64 accumulates directly.
+        Real part[kBremMaxDir];
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd) part[dd] = 0;
         for (int j = 0; j < nc; ++j) {
             const BremSeg<Real> &b = segs[j];
             const Real T_f = b.T - k;
             if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-            const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
-            const Real beta_f = p_f / ((Real)1 + T_f / mc2);
-            Real diff;
+            Real nsig = 0;  // sum_el n_el L dsigma/dk
             if constexpr (sizeof(Real) == 8) {
-                diff = b.p_i - p_f;
+                const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
+                const Real beta_f = p_f / ((Real)1 + T_f / mc2);
+                const Real born_log = b_log((b.p_i + p_f) / fmax(b.p_i - p_f, (Real)1e-30));
+                for (int el = 0; el < n_el; ++el) {
+                    const Real Z = Zs[el];
+                    const Real elwert = b.beta_i / beta_f * b.den_i[el] / ((Real)1 - b_exp(-za * Z / beta_f));
+                    const Real dsig = c0 * (Z * Z) / k_ev / (b.p_i * b.p_i) * born_log * elwert;
+                    nsig += b.nL[el] * dsig;
+                }
             } else {
-                diff = k * (b.T + T_f + (Real)2 * mc2) / (mc2 * mc2 * (b.p_i + p_f));
+                const float inv_mc2 = 1.0f / 510.99895f;
+                const float q = T_f * (T_f + 2.0f * mc2);
+                const float p_f = q * rsqrtf(q) * inv_mc2;
+                const float beta_f = __fdividef(p_f, 1.0f + T_f * inv_mc2);
+                const float diff = __fdividef(k * (b.T + T_f + 2.0f * mc2) * inv_mc2 * inv_mc2, b.p_i + p_f);
+                const float born_log = __logf(__fdividef(b.p_i + p_f, fmaxf(diff, 1e-30f)));
+                const float inv_beta_f = __fdividef(1.0f, beta_f);
+                const float common = __fdividef(c0, k_ev * b.p_i * b.p_i) * born_log * b.beta_i * inv_beta_f;
+                for (int el = 0; el < n_el; ++el) {
+                    const float Z = Zs[el];
+                    const float den_f = 1.0f - __expf(-za * Z * inv_beta_f);
+                    nsig += b.nL[el] * (Z * Z) * common * __fdividef(b.den_i[el], den_f);
+                }
             }
-            const Real born_log = b_log((b.p_i + p_f) / fmax(diff, (Real)1e-30));
-            const Real T_abs = b_mean_transmission<Real>(b.path0 * mu, b.path1 * mu);
-            Real sum = 0;
-            for (int el = 0; el < n_el; ++el) {
-                const Real Z = Zs[el];
-                const Real elwert = b.beta_i / beta_f * b.den_i[el] / ((Real)1 - b_exp(-za * Z / beta_f));
-                const Real dsig = c0 * (Z * Z) / k_ev / (b.p_i * b.p_i) * born_log * elwert;
-                sum += b.nL[el] * (dsig * T_abs);
+#pragma unroll
+            for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                if (dd < nd) {
+                    const Real f = inv_nz[dd];
+                    const Real p0 = up[dd] ? b.path0 * f : (T_slab - b.path0) * f;
+                    const Real p1 = up[dd] ? b.path1 * f : (T_slab - b.path1) * f;
+                    if constexpr (sizeof(Real) == 8) {
+                        acc[dd] += (double)(nsig * b_mean_transmission<Real>(p0 * mu, p1 * mu));
+                    } else {
+                        // exp(-lo) (1 - e^-d)/d with base-2 exponentials; the
+                        // series below d = 0.01 keeps float accuracy.
+                        const float t0 = p0 * mu, t1 = p1 * mu;
+                        const float lo = fminf(t0, t1);
+                        const float d = fabsf(t1 - t0);
+                        const float ratio = d > 0.01f ? __fdividef(1.0f - exp2f(-d * 1.44269504f), d)
+                                                      : 1.0f - d * (0.5f - d * (1.0f / 6.0f - d * (1.0f / 24.0f)));
+                        part[dd] += nsig * exp2f(-lo * 1.44269504f) * ratio;
+                    }
+                }
             }
-            acc += (double)sum;
+        }
+        if constexpr (sizeof(Real) == 4) {
+#pragma unroll
+            for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd] += (double)part[dd];
         }
     }
-    if (on && acc != 0.0) atomicAdd(&a.spec[(int64_t)d * a.n_E + e], acc);
+    if (on) {
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd)
+            if (dd < nd && acc[dd] != 0.0) atomicAdd(&a.spec[(int64_t)(d0 + dd) * a.n_E + e], acc[dd]);
+    }
 }
 
 cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     if (a.n_el > kBremMaxEl || a.n_el < 1) return cudaErrorInvalidValue;
     int64_t n_seg = a.n_seg;
     const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
-    int64_t gy = ((int64_t)sms * 4 + (int64_t)gx * a.n_dir - 1) / ((int64_t)gx * a.n_dir);
+    int64_t gy = ((int64_t)sms * 4 + (int64_t)gx - 1) / (int64_t)gx;
     const int64_t max_y = (n_seg + kBremChunk - 1) / kBremChunk;
     if (gy > max_y) gy = max_y;
     if (gy < 1) gy = 1;
-    dim3 grid(gx, (unsigned)gy, (unsigned)a.n_dir);
-    if (a.precision == PB_MIXED) brem_kernel<float><<<grid, kBremThreads, 0, s>>>(a, n_seg);
-    else brem_kernel<double><<<grid, kBremThreads, 0, s>>>(a, n_seg);
-    return cudaGetLastError();
+    dim3 grid(gx, (unsigned)gy, 1);
+    for (int d0 = 0; d0 < a.n_dir; d0 += kBremMaxDir) {
+        if (a.precision == PB_MIXED) brem_kernel<float><<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
+        else brem_kernel<double><<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace pb

@@ -24,6 +24,7 @@
 // PB_FP64 evaluates the chain in double; PB_MIXED in float, with the line
 // phase a (E - E_r) formed and range-reduced in double and every
 // accumulation in double.
+#include <climits>
 #include <cstdint>
 
 #include "pb_common.cuh"
@@ -31,20 +32,28 @@
 
 namespace pb {
 
-constexpr int kSegTile = 32;
-constexpr int kRowChunk = 128;
-constexpr int kCxrThreads = 256;
+constexpr int kSegTile = 16;
+constexpr int kRowChunk = 64;
+constexpr int kCxrThreads = 512;
+constexpr int kQueue = kSegTile * kRowChunk;  // every pair of a pass may keep a line
 constexpr int kMaxTab = 4096;   // E_tab / delta staged in shared memory up to this size
 constexpr int kMaxMu = 4;
 
+// Math of the line chain. FP64 uses IEEE operations throughout (parity with
+// the reference's FP64 chain); the float path uses the SFU approximations
+// (division by reciprocal, sqrt by reciprocal square root, base-2 exp/log),
+// each within a few ulp, which the 1 % spectrum tolerance of the mixed path
+// absorbs many times over.
 __device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ float r_sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : sqrtf(x); }
 __device__ __forceinline__ double r_exp(double x) { return exp(x); }
-__device__ __forceinline__ float r_exp(float x) { return expf(x); }
+__device__ __forceinline__ float r_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double r_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float r_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double r_log1p(double x) { return log1p(x); }
 __device__ __forceinline__ float r_log1p(float x) { return log1pf(x); }
+__device__ __forceinline__ double rdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdividef(a, b); }
 
 // Per (segment, direction) quantities shared by every reflection row.
 template <class Real>
@@ -115,12 +124,35 @@ __device__ void seg_precompute(SegPre<Real> &sp, const pb_cxr_args &a, int64_t s
 
 // searchsorted(grid, x, side="left") clipped to [1, n-1] and the blend
 // fraction (cxr/_kernels.py:328-349).
+// Geometric tabulation grids (grid[i] = exp(log0 + i h)) are indexed in
+// closed form and then corrected to the exact searchsorted answer, which
+// replaces ~log2(n) dependent shared-memory loads by one logarithm.
+struct TabIndex {
+    bool geometric;
+    double log0;
+    double inv_h;
+};
+
+__device__ __forceinline__ double t_log(double x) { return log(x); }
+__device__ __forceinline__ float t_log(float x) { return __logf(x); }
+
 template <class Real>
 __device__ __forceinline__ void bracket(const Real *grid, int n, Real x, int &idx, Real &frac,
-                                        bool &below, bool &above) {
+                                        bool &below, bool &above, const TabIndex &ti) {
     int i;
     if (isnan(x)) {
         i = n;
+    } else if (ti.geometric) {
+        int c = 0;
+        if (x > grid[0]) {
+            const Real f = (t_log(x) - (Real)ti.log0) * (Real)ti.inv_h;
+            c = f >= (Real)(n - 1) ? n : (int)ceil(f);
+            if (c < 0) c = 0;
+        }
+        // searchsorted(side="left"): first index with grid[i] >= x
+        while (c > 0 && !(grid[c - 1] < x)) --c;
+        while (c < n && grid[c] < x) ++c;
+        i = c;
     } else {
         int lo = 0, hi = n;
         while (lo < hi) {
@@ -160,25 +192,32 @@ __device__ __forceinline__ void quantum_line_factors(Real h, Real gamma, Real vd
     const Real e_f = r_sqrt(gg + h * n_f);
     const Real s_if = gamma + e_f;
     const Real ge_ke = g_dot_e + k_dot_e;
-    pxr_num = (-n_f * ge_ke - k2 * ((Real)2 * gamma * v_dot_e - h * ge_ke)) / s_if;
+    pxr_num = rdiv(-n_f * ge_ke - k2 * ((Real)2 * gamma * v_dot_e - h * ge_ke), s_if);
     const Real s_1 = e_1 + gamma;
     const Real s_3 = e_1 + e_f;
     const Real s_4 = gamma + e_2;
     const Real x = (Real)2 * gamma * v_dot_e - h * k_dot_e;
     const Real sigma = s_if + e_1 + e_2;
-    f_cbs = (Real)2 * g_dot_e * s_1 / (s_3 * n_1) +
-            x * (n_1 * (n_f / s_if) * sigma - (Real)2 * s_1 * s_4 * k_dot_g) / (s_3 * s_4 * n_1 * n_2);
+    f_cbs = rdiv((Real)2 * g_dot_e * s_1, s_3 * n_1) +
+            rdiv(x * (n_1 * rdiv(n_f, s_if) * sigma - (Real)2 * s_1 * s_4 * k_dot_g), s_3 * s_4 * n_1 * n_2);
 }
 
-// segment_escape.py:276-289
+// segment_escape.py:276-289. The float path switches to the series below
+// d = 0.01, where 1 - exp(-d) in float would lose digits.
 template <class Real>
 __device__ __forceinline__ Real mean_transmission(Real t0, Real t1) {
     const Real lo = fmin(t0, t1);
     const Real d = fabs(t1 - t0);
-    const Real safe = d > (Real)1.0e-4 ? d : (Real)1;
-    const Real ratio = d > (Real)1.0e-4 ? -r_expm1(-safe) / safe
-                                         : (Real)1 - (Real)0.5 * d + d * d / (Real)6;
-    return r_exp(-lo) * ratio;
+    if constexpr (sizeof(Real) == 8) {
+        const Real safe = d > (Real)1.0e-4 ? d : (Real)1;
+        const Real ratio = d > (Real)1.0e-4 ? -r_expm1(-safe) / safe
+                                             : (Real)1 - (Real)0.5 * d + d * d / (Real)6;
+        return r_exp(-lo) * ratio;
+    } else {
+        const float ratio = d > 0.01f ? rdiv(1.0f - __expf(-d), d)
+                                      : 1.0f - d * (0.5f - d * (1.0f / 6.0f - d * (1.0f / 24.0f)));
+        return __expf(-lo) * ratio;
+    }
 }
 
 template <class Real>
@@ -187,30 +226,29 @@ struct Line {
     bool good;
 };
 
-// The per-pair chain. ``tab`` points at E_tab / delta / log_mu (shared or
-// global), ``n_tab`` their length.
+// The per-pair chain. ``E_tab``/``delta_tab``/``log_mu`` point at the
+// shared-memory staging (or global memory for a large FP64 grid).
 template <class Real>
-__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, const double *nh,
+__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
                                 const Real *E_tab, const Real *delta_tab, const Real *log_mu,
-                                int n_tab, int n_mu, const pb_cxr_tables &t) {
-    const Real nx = (Real)nh[0], ny = (Real)nh[1], nz = (Real)nh[2];
+                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti) {
     const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
     const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
-    (void)nx; (void)ny; (void)nz;
     const Real hbarc = (Real)kHbarcEvAng;
     // cxr/_block_prologue.py:18-38, cxr/_recoil.py:79-97
     const Real r_num = (Real)0.5 * g2 * sp.inv_E;
     const Real r_den = n_dot_g * sp.inv_E;
-    const Real v_dot_g_exact = (sp.vx * Gx + sp.vy * Gy + sp.vz * Gz) - r_num;
+    const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
+    const Real v_dot_g_exact = v_dot_g - r_num;
     const Real denom_vac = sp.denom_row + r_den;
     // cxr/_kernels.py:702-765
     Real denom = denom_vac, previous = denom, delta = (Real)NAN;
     for (int pass = 0; pass < 3; ++pass) {
-        const Real Er = hbarc * (v_dot_g_exact / denom);
+        const Real Er = hbarc * rdiv(v_dot_g_exact, denom);
         int ix;
         Real fr;
         bool bl, ab;
-        bracket<Real>(E_tab, n_tab, Er, ix, fr, bl, ab);
+        bracket<Real>(E_tab, n_tab, Er, ix, fr, bl, ab, ti);
         delta = gather<Real>(delta_tab, n_tab, ix, fr, bl, ab);
         previous = denom;
         denom = denom_vac - delta * sp.v_dot_grad;
@@ -220,8 +258,7 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, 
     if (!settled) denom = (Real)NAN;
     const Real n_dot_g_blk = n_dot_g + delta * (sp.gx * Gx + sp.gy * Gy + sp.gz * Gz);
     // cxr/_kernels.py:624-655
-    const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
-    const Real omega = (v_dot_g - r_num) / denom;
+    const Real omega = rdiv(v_dot_g - r_num, denom);
     const Real k_dot_v = omega * (((Real)1 - denom) + r_den);
     const Real k_dot_g = omega * n_dot_g_blk;
     const Real detuning = g2 + (Real)2 * k_dot_g;
@@ -230,20 +267,36 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, 
                                                            : (Real)1 - (Real)2 * delta + delta * delta * sp.grad2);
     const Real E_res = hbarc * omega;
     bool keep = sp.radiates && (E_res > (Real)t.lo_keep) && (E_res > (Real)10) && (E_res < (Real)t.hi_keep);
+    Line<Real> out;
+    out.good = false;
+    out.E_res = E_res;
+    out.a_width = (Real)NAN;
+    out.weight = (Real)NAN;
+    // cxr/_block_prologue.py:53-62, cxr/_recoil.py:100-118
+    const Real slope = denom * rdiv((Real)1, (Real)1 - omega * sp.inv_E);
+    keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - rdiv((Real)1, sp.gamma));
+    if constexpr (sizeof(Real) == 4) {
+        // The float path stops here for dropped pairs (FP64 completes every
+        // pair so its per-pair output matches the reference's arrays).
+        if (!keep) return out;
+    }
     int ix;
     Real fr;
     bool bl, ab;
-    bracket<Real>(E_tab, n_tab, E_res, ix, fr, bl, ab);
+    bracket<Real>(E_tab, n_tab, E_res, ix, fr, bl, ab, ti);
     Real lfr;
     {
         const Real x0 = E_tab[ix - 1], x1 = E_tab[ix];
         Real bx = fmin(fmax(E_res, x0), x1);
         if (isnan(E_res)) bx = E_res;
-        lfr = r_log1p((bx - x0) / x0) / r_log1p((x1 - x0) / x0);
+        if constexpr (sizeof(Real) == 8) {
+            lfr = r_log1p((bx - x0) / x0) / r_log1p((x1 - x0) / x0);
+        } else {
+            // cxr/_kernels.py:352-366 on a geometric grid: log(bx/x0)/h.
+            lfr = ti.geometric ? __logf(rdiv(bx, x0)) * (float)ti.inv_h
+                               : rdiv(log1pf(rdiv(bx - x0, x0)), log1pf(rdiv(x1 - x0, x0)));
+        }
     }
-    // cxr/_block_prologue.py:53-62, cxr/_recoil.py:100-118
-    const Real slope = denom * ((Real)1 / ((Real)1 - omega * sp.inv_E));
-    keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - (Real)1 / sp.gamma);
     // cxr/_kernels.py:482-506 couplings, 369-388 attenuation
     const int64_t base = (int64_t)rw.row * n_tab;
     const Real chi_re = gather<Real>(t.chi_re + base, n_tab, ix, fr, bl, ab);
@@ -272,7 +325,7 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, 
         Real pxr_num, f_cbs;
         quantum_line_factors<Real>(h, sp.gamma, v_dot_g, k_dot_v, k_dot_g, g2, k2, v_dot_e, g_dot_e,
                                    k_dot_e, pxr_num, f_cbs);
-        const Real f_pxr = pxr_num / detuning;
+        const Real f_pxr = rdiv(pxr_num, detuning);
         const Real re = chi_re * f_pxr + u_re * f_cbs;
         const Real im = chi_im * f_pxr + u_im * f_cbs;
         const Real a2 = re * re + im * im;
@@ -281,10 +334,8 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, 
     // cxr/_batched.py:702-730, cxr/_kernels.py:658-668
     const Real T_abs = mean_transmission<Real>(sp.path0 * mu, sp.path1 * mu);
     const Real pref_c1 = (Real)(4.0 * (kPi * kPi) * kHbarcEvAng);
-    const Real pref = (Real)kAlphaFs * omega / pref_c1 * (sp.t_L * sp.t_L) * T_abs;
-    Line<Real> out;
-    out.E_res = E_res;
-    out.a_width = slope * sp.t_L / ((Real)2 * hbarc) * (Real)1;
+    const Real pref = rdiv((Real)kAlphaFs * omega, pref_c1) * (sp.t_L * sp.t_L) * T_abs;
+    out.a_width = rdiv(slope * sp.t_L, (Real)2 * hbarc) * (Real)1;
     out.weight = pref * A2 * rw.wm;
     out.good = keep && isfinite(out.weight) && (out.weight > (Real)0);
     return out;
@@ -397,60 +448,134 @@ __device__ __forceinline__ double far_envelope(double A, double B, double d) {
     return f0 + d * (f1 + d * f2);
 }
 
-// Deposit one line's bin means: exact within the line's window; beyond it
-// the far envelope w/(2 a^2) / ((E_lo - E_r)(E_hi - E_r)) is carried by three
-// moments about the centre bin and spread by far_field_kernel onto every bin
-// more than K_far bins away. A line whose window is wider than K_far
-// removes the envelope again from its extra exact bins, so each bin takes
-// exactly one of the two forms.
-__device__ void deposit_binmean(double E_r, double a, double w, const BinAxis &ax,
-                                double exact_widths, int K_far, double *spec, double *mom) {
+// Oscillatory part of the sinc^2 antiderivative beyond the asymptotic
+// threshold (Abramowitz & Stegun 5.2.8, 5.2.34-35): with u = 2 pi |x|,
+//   int sinc^2 = (1/(2 pi^2)) (1/x_a - 1/x_b) + (1/pi) [Q(u)]_a^b,
+//   Q(u) = cos u (1/u - f(u)) - g(u) sin u,
+// where 1/u - f(u) ~ (1/u) sum_{k>=1} (-1)^(k+1) (2k)!/u^2k and
+// g(u) ~ (1/u^2) sum_{k>=0} (-1)^k (2k+1)!/u^2k. The envelope term carries
+// the mass without the cancellation of a difference of antiderivatives.
+__device__ __forceinline__ double q_osc_f64(double u) {
+    const double y = 1.0 / (u * u);
+    double p1 = 0.0, p2 = 0.0;
+    // 13 terms: the first omitted one at u = 48 is below 1e-17 of the leading.
+    double t1 = 2.0 * y, t2 = 1.0;
+    for (int k = 1; k <= 13; ++k) {
+        p1 += t1;
+        p2 += t2;
+        t1 *= -(2.0 * k + 1.0) * (2.0 * k + 2.0) * y;
+        t2 *= -(2.0 * k) * (2.0 * k + 1.0) * y;
+    }
+    double sn, cs;
+    sincos(u, &sn, &cs);
+    return cs * p1 / u - sn * p2 * y;
+}
+
+// Float form for the mixed path; the phase u is reduced in double first.
+__device__ __forceinline__ double q_osc_f32(double u) {
+    const float yf = (float)(1.0 / (u * u));
+    const float p1 = yf * (2.0f + yf * (-24.0f + yf * (720.0f + yf * (-40320.0f + yf * 3628800.0f))));
+    const float p2 = 1.0f + yf * (-6.0f + yf * (120.0f + yf * (-5040.0f + yf * 362880.0f)));
+    const double r = u - 2.0 * kPi * rint(u * (0.5 / kPi));
+    float sn, cs;
+    __sincosf((float)r, &sn, &cs);
+    return (double)(cs * p1 / (float)u - sn * p2 * yf);
+}
+
+// Exact mass of sinc^2 over [x_lo, x_hi] (line-centred first-zero units).
+template <bool kMixed>
+__device__ __forceinline__ double bin_mass(double x_lo, double x_hi, double &r_lo, bool &have_r_lo) {
+    const double u_lim = kMixed ? 24.0 : 48.0;
+    const double u_lo = 2.0 * kPi * fabs(x_lo), u_hi = 2.0 * kPi * fabs(x_hi);
+    if ((x_lo > 0.0 || x_hi < 0.0) && fmin(u_lo, u_hi) >= u_lim) {
+        // Both edges far on one side: closed form (mirror the negative side).
+        const double a = x_lo > 0.0 ? x_lo : -x_hi;
+        const double b = x_lo > 0.0 ? x_hi : -x_lo;
+        const double ua = 2.0 * kPi * a, ub = 2.0 * kPi * b;
+        const double env = (b - a) / (2.0 * kPi * kPi * a * b);
+        const double osc = kMixed ? (q_osc_f32(ub) - q_osc_f32(ua)) : (q_osc_f64(ub) - q_osc_f64(ua));
+        have_r_lo = false;
+        return env + osc / kPi;
+    }
+    if (!have_r_lo) r_lo = sincsq_tail(x_lo);
+    const double r_hi = sincsq_tail(x_hi);
+    const double mass = r_hi - r_lo + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
+    r_lo = r_hi;
+    have_r_lo = true;
+    return mass;
+}
+
+// Bin-mean deposit of a line: exact bin integrals within the line's window
+// (``exact_widths`` first-zero widths, at least K_far bins); beyond it the far
+// envelope w/(2 a^2) / ((E_lo - E_r)(E_hi - E_r)) is carried by three moments
+// about the centre bin and spread by far_field_kernel onto every bin more
+// than K_far bins away. A line whose window is wider than K_far removes the
+// envelope again from its extra exact bins, so each bin takes exactly one of
+// the two forms. Lines centred off a non-uniform axis, or too wide for a
+// window, are integrated exactly over the whole axis.
+struct LineWindow {
+    int c;        // centre bin (may lie off the axis)
+    int b0, nb;   // first exact bin and count
+    bool mom;     // far field through the moments
+};
+
+__device__ __forceinline__ LineWindow line_window(double E_r, double a, const BinAxis &ax,
+                                                  double exact_widths, int K_far, bool moments) {
     const int n = ax.n;
-    int c = bin_of(ax, E_r);
-    bool use_mom = mom != nullptr && K_far > 0;
-    if (use_mom && (c < -ax.pad || c >= n + ax.pad)) use_mom = false;
+    LineWindow lw;
+    lw.c = bin_of(ax, E_r);
+    lw.mom = moments && K_far > 0 && lw.c >= -ax.pad && lw.c < n + ax.pad;
     int K;
-    if (!use_mom) {
-        K = n + (c < 0 ? -c : (c >= n ? c - n + 1 : 0));
+    if (!lw.mom) {
+        K = n + (lw.c < 0 ? -lw.c : (lw.c >= n ? lw.c - n + 1 : 0));
     } else {
         const double kk = ceil(exact_widths * kPi / (a * ax.w));
         K = kk > (double)(2 * n) ? 2 * n : (kk < (double)K_far ? K_far : (int)kk);
     }
-    int b0 = c - K, b1 = c + K;
+    int b0 = lw.c - K, b1 = lw.c + K;
     if (b0 < 0) b0 = 0;
     if (b1 > n - 1) b1 = n - 1;
+    lw.b0 = b0;
+    lw.nb = b1 >= b0 ? b1 - b0 + 1 : 0;
+    return lw;
+}
+
+template <bool kMixed>
+__device__ __forceinline__ double line_bin_value(double E_r, double a, double w, int b, const LineWindow &lw,
+                                                 const BinAxis &ax, int K_far) {
+    const double x_lo = a * (ax.edges[b] - E_r) / kPi;
+    const double x_hi = a * (ax.edges[b + 1] - E_r) / kPi;
+    double r_lo = 0.0;
+    bool have = false;
+    const double mass = bin_mass<kMixed>(x_lo, x_hi, r_lo, have);
+    const double width = ax.edges[b + 1] - ax.edges[b];
+    double v = w * (mass * (kPi / a) / width);
+    if (lw.mom && (b - lw.c > K_far || lw.c - b > K_far)) {
+        const double E_c = centre_of(ax, lw.c);
+        v -= w / (2.0 * a * a) * far_envelope(ax.edges[b] - E_c, ax.edges[b + 1] - E_c, E_r - E_c);
+    }
+    return v;
+}
+
+__device__ __forceinline__ void line_moments(double E_r, double a, double w, const LineWindow &lw,
+                                             const BinAxis &ax, double *mom) {
+    const int slot = lw.c + ax.pad;
     const double m = w / (2.0 * a * a);
-    const double E_c = use_mom ? centre_of(ax, c) : 0.0;
-    if (b0 <= b1) {
-        const double scale = kPi / a;
-        double x_lo = a * (ax.edges[b0] - E_r) / kPi;
-        double r_lo = sincsq_tail(x_lo);
-        for (int b = b0; b <= b1; ++b) {
-            const double x_hi = a * (ax.edges[b + 1] - E_r) / kPi;
-            const double r_hi = sincsq_tail(x_hi);
-            const double mass = r_hi - r_lo + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
-            const double width = ax.edges[b + 1] - ax.edges[b];
-            double v = w * (mass * scale / width);
-            if (use_mom && (b - c > K_far || c - b > K_far))
-                v -= m * far_envelope(ax.edges[b] - E_c, ax.edges[b + 1] - E_c, E_r - E_c);
-            atomicAdd(&spec[b], v);
-            x_lo = x_hi;
-            r_lo = r_hi;
-        }
-    }
-    if (use_mom) {
-        const int slot = c + ax.pad;
-        const double dd = E_r - E_c;
-        atomicAdd(&mom[3 * slot + 0], m);
-        atomicAdd(&mom[3 * slot + 1], m * dd);
-        atomicAdd(&mom[3 * slot + 2], m * dd * dd);
-    }
+    const double dd = E_r - centre_of(ax, lw.c);
+    atomicAdd(&mom[3 * slot + 0], m);
+    atomicAdd(&mom[3 * slot + 1], m * dd);
+    atomicAdd(&mom[3 * slot + 2], m * dd * dd);
 }
 
 // One block: a direction (blockIdx.y) and a strided range of segment tiles.
+// Phase A evaluates the (segment x row) pairs of a tile and pushes every
+// kept line onto a shared-memory queue (warp ballot + one shared atomic per
+// warp); phase B spreads the queued lines' (line, bin) work items evenly over
+// the block, so line deposits never run in a lone lane of a divergent warp.
 template <class Real>
 __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool kMixed = sizeof(Real) == 4;
     const int d = blockIdx.y;
     const double *nh = a.n_hat + 3 * d;
     const int n_g = a.tables.n_g;
@@ -462,12 +587,21 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     if (a.n_seg_device) n_seg = (int64_t)*a.n_seg_device;
     if (n_seg > a.n_seg && a.n_seg > 0) n_seg = a.n_seg;
 
-    // Shared layout: [rows chunk][seg tile][E_tab][delta][log_mu][spec][moments]
+    // Shared layout: [rows][segs][queue][E_tab][delta][log_mu][spec][moments]
     unsigned char *cur = smem_raw;
     RowPre<Real> *rows = reinterpret_cast<RowPre<Real> *>(cur);
     cur += sizeof(RowPre<Real>) * kRowChunk;
     SegPre<Real> *segs = reinterpret_cast<SegPre<Real> *>(cur);
     cur += sizeof(SegPre<Real>) * kSegTile;
+    cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
+    Real *qE = reinterpret_cast<Real *>(cur);
+    Real *qA = qE + kQueue;
+    Real *qW = qA + kQueue;
+    int *qStart = reinterpret_cast<int *>(qW + kQueue);   // kQueue + 1 prefix entries
+    int *qB0 = qStart + kQueue + 1;
+    int *qC = qB0 + kQueue;
+    int *scratch = qC + kQueue;                             // warp sums + counter
+    cur = reinterpret_cast<unsigned char *>(scratch + 64);
     cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
     const bool tab_smem = n_tab <= kMaxTab;
     Real *E_tab_s = reinterpret_cast<Real *>(cur);
@@ -478,8 +612,10 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     double *spec_s = reinterpret_cast<double *>(cur);
     double *mom_s = spec_s + (binmean ? n_E : 0);
     const int n_mom = n_E + 2 * far_pad;
+    int &q_count = scratch[40];
 
     const int tid = threadIdx.x;
+    const unsigned lane = tid & 31u;
     if (tab_smem) {
         for (int j = tid; j < n_tab; j += blockDim.x) {
             E_tab_s[j] = (Real)a.tables.E_tab[j];
@@ -492,11 +628,15 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         if (K_far > 0)
             for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
-    // The tables are converted to the flight precision in global memory only
-    // for FP64, where the layouts agree; the float path reads the staged copy.
+    if (tid == 0) q_count = 0;
     const Real *E_tab = tab_smem ? E_tab_s : reinterpret_cast<const Real *>(a.tables.E_tab);
     const Real *delta_tab = tab_smem ? delta_s : reinterpret_cast<const Real *>(a.tables.delta);
     const Real *log_mu = tab_smem ? logmu_s : reinterpret_cast<const Real *>(a.tables.log_mu);
+
+    TabIndex ti{};
+    ti.geometric = a.tables.tab_log_step > 0.0;
+    ti.log0 = a.tables.tab_log0;
+    ti.inv_h = ti.geometric ? 1.0 / a.tables.tab_log_step : 0.0;
 
     BinAxis ax{};
     if (binmean) {
@@ -514,6 +654,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     const bool pairs_out = a.pair_E != nullptr;
     const bool lines_out = a.line_E != nullptr;
     const double exact_widths = K_far > 0 ? a.exact_widths : 0.0;
+    const int n_warps = blockDim.x >> 5;
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int64_t s0 = tile * kSegTile;
         const int nst = (int)((n_seg - s0) < kSegTile ? (n_seg - s0) : kSegTile);
@@ -526,8 +667,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 const int g = g0 + j;
                 RowPre<Real> &r = rows[j];
                 const double *G = a.tables.G + 3 * g;
-                const double *ES = a.tables.ES + 3 * g;
-                const double *EP = a.tables.EP + 3 * g;
+                const double *ES = a.tables.ES + 3 * ((int64_t)d * n_g + g);
+                const double *EP = a.tables.EP + 3 * ((int64_t)d * n_g + g);
                 for (int c = 0; c < 3; ++c) {
                     r.G[c] = (Real)G[c];
                     r.ES[c] = (Real)ES[c];
@@ -541,35 +682,106 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 r.row = a.tables.row_table[g];
             }
             __syncthreads();
+            // ---- phase A: pairs -> queue ----
             const int n_pairs = nst * ng;
-            for (int q = tid; q < n_pairs; q += blockDim.x) {
-                const int si = q / ng;
-                const int gi = q - si * ng;
-                const Line<Real> ln =
-                    pair_line<Real>(segs[si], rows[gi], nh, E_tab, delta_tab, log_mu, n_tab, n_mu, a.tables);
-                if (pairs_out) {
-                    const int64_t o = ((int64_t)d * n_seg + s0 + si) * n_g + g0 + gi;
-                    a.pair_E[o] = (double)ln.E_res;
-                    a.pair_a[o] = (double)ln.a_width;
-                    a.pair_w[o] = (double)ln.weight;
-                    a.pair_good[o] = ln.good ? 1 : 0;
-                }
-                if (!ln.good) continue;
-                if (lines_out) {
-                    const unsigned long long slot = atomicAdd(a.line_count, 1ULL);
-                    if (slot < (unsigned long long)a.line_capacity) {
-                        a.line_E[slot] = (double)ln.E_res;
-                        a.line_a[slot] = (double)ln.a_width;
-                        a.line_w[slot] = (double)ln.weight;
-                        a.line_dir[slot] = d;
-                    } else {
-                        set_status(a.status, PB_DEV_QUEUE_OVERFLOW);
+            const int n_iter = (n_pairs + (int)blockDim.x - 1) / (int)blockDim.x;
+            for (int it = 0; it < n_iter; ++it) {
+                const int q = it * blockDim.x + tid;
+                Line<Real> ln;
+                ln.good = false;
+                if (q < n_pairs) {
+                    const int si = q / ng;
+                    const int gi = q - si * ng;
+                    ln = pair_line<Real>(segs[si], rows[gi], E_tab, delta_tab, log_mu, n_tab, n_mu,
+                                         a.tables, ti);
+                    if (pairs_out) {
+                        const int64_t o = ((int64_t)d * n_seg + s0 + si) * n_g + g0 + gi;
+                        a.pair_E[o] = (double)ln.E_res;
+                        a.pair_a[o] = (double)ln.a_width;
+                        a.pair_w[o] = (double)ln.weight;
+                        a.pair_good[o] = ln.good ? 1 : 0;
+                    }
+                    if (ln.good && lines_out) {
+                        const unsigned long long slot = atomicAdd(a.line_count, 1ULL);
+                        if (slot < (unsigned long long)a.line_capacity) {
+                            a.line_E[slot] = (double)ln.E_res;
+                            a.line_a[slot] = (double)ln.a_width;
+                            a.line_w[slot] = (double)ln.weight;
+                            a.line_dir[slot] = d;
+                        } else {
+                            set_status(a.status, PB_DEV_QUEUE_OVERFLOW);
+                        }
                     }
                 }
-                if (binmean)
-                    deposit_binmean((double)ln.E_res, (double)ln.a_width, (double)ln.weight, ax,
-                                    exact_widths, K_far, spec_s, K_far > 0 ? mom_s : nullptr);
+                if (binmean) {
+                    const unsigned mask = __ballot_sync(0xffffffffu, ln.good);
+                    int base = 0;
+                    if (lane == 0 && mask) base = atomicAdd(&q_count, __popc(mask));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (ln.good) {
+                        const int k = base + __popc(mask & ((1u << lane) - 1u));
+                        qE[k] = ln.E_res;
+                        qA[k] = ln.a_width;
+                        qW[k] = ln.weight;
+                    }
+                }
             }
+            if (!binmean) continue;
+            __syncthreads();
+            // ---- phase B: windows, scan, spread (line, bin) items ----
+            const int nq = q_count;
+            for (int j = tid; j < nq; j += blockDim.x) {
+                const LineWindow lw = line_window((double)qE[j], (double)qA[j], ax, exact_widths, K_far,
+                                                  K_far > 0);
+                qStart[j] = lw.nb;
+                qB0[j] = lw.b0;
+                qC[j] = lw.mom ? lw.c : INT_MIN;
+                if (lw.mom) line_moments((double)qE[j], (double)qA[j], (double)qW[j], lw, ax, mom_s);
+            }
+            __syncthreads();
+            // exclusive scan of qStart[0..nq) (at most kQueue entries)
+            {
+                const int per = (nq + (int)blockDim.x - 1) / (int)blockDim.x;
+                const int j0 = tid * per;
+                int local = 0;
+                for (int j = j0; j < j0 + per && j < nq; ++j) local += qStart[j];
+                int incl = local;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if ((int)lane >= o) incl += v;
+                }
+                if (lane == 31) scratch[tid >> 5] = incl;
+                __syncthreads();
+                if (tid == 0) {
+                    int run = 0;
+                    for (int w = 0; w < n_warps; ++w) { const int v = scratch[w]; scratch[w] = run; run += v; }
+                    scratch[41] = run;
+                }
+                __syncthreads();
+                int run = scratch[tid >> 5] + incl - local;
+                for (int j = j0; j < j0 + per && j < nq; ++j) { const int v = qStart[j]; qStart[j] = run; run += v; }
+                __syncthreads();
+                if (tid == 0) qStart[nq] = scratch[41];
+                __syncthreads();
+            }
+            const int n_items = qStart[nq];
+            for (int item = tid; item < n_items; item += blockDim.x) {
+                int lo = 0, hi = nq;  // last line with qStart[line] <= item
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (qStart[mid] <= item) lo = mid; else hi = mid;
+                }
+                LineWindow lw;
+                lw.c = qC[lo];
+                lw.mom = lw.c != INT_MIN;
+                lw.b0 = qB0[lo];
+                const int b = qB0[lo] + (item - qStart[lo]);
+                const double v = line_bin_value<kMixed>((double)qE[lo], (double)qA[lo], (double)qW[lo], b,
+                                                        lw, ax, K_far);
+                atomicAdd(&spec_s[b], v);
+            }
+            __syncthreads();
+            if (tid == 0) q_count = 0;
         }
     }
     __syncthreads();
@@ -673,6 +885,7 @@ __global__ void node_reduce_kernel(const double *E_grid, int n_E, const double *
 template <class Real>
 static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moments) {
     size_t b = sizeof(RowPre<Real>) * kRowChunk + sizeof(SegPre<Real>) * kSegTile + 16;
+    b += sizeof(Real) * 3 * kQueue + sizeof(int) * (3 * kQueue + 1 + 64) + 16;
     if (a.tables.n_tab <= kMaxTab) b += sizeof(Real) * (size_t)a.tables.n_tab * (2 + a.tables.n_mu);
     b += 16;
     if (a.quadrature == PB_QUAD_BINMEAN) {
@@ -691,6 +904,8 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
     if (K_far == 0) far_pad = 0;
     size_t smem = cxr_smem_bytes<Real>(a, far_pad, K_far > 0);
     if (smem > 220 * 1024) return cudaErrorInvalidValue;
+    // The float path reads its tables from the shared-memory staging only.
+    if (sizeof(Real) == 4 && a.tables.n_tab > kMaxTab) return cudaErrorInvalidValue;
     auto kern = cxr_kernel<Real>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;

@@ -550,6 +550,19 @@ def diamond_hkls(g_max: float, crystal: Crystal = SILICON):
     return out
 
 
+def geometric_grid(E_tab, rtol=1e-9):
+    """(log E_0, log step) when E_tab is geometric to ``rtol`` of a step, else (0, 0)."""
+    E = np.asarray(E_tab, dtype=float)
+    if E.size < 3 or np.any(E <= 0) or np.any(np.diff(E) <= 0):
+        return 0.0, 0.0
+    lg = np.log(E)
+    step = (lg[-1] - lg[0]) / (E.size - 1)
+    pred = lg[0] + step * np.arange(E.size)
+    if np.max(np.abs(pred - lg)) <= rtol * step:
+        return float(lg[0]), float(step)
+    return 0.0, 0.0
+
+
 def energy_bin_edges(E_grid):
     """Bin edges of the bin-mean routes (spectrum/characteristic.py:621-646)."""
     grid = np.asarray(E_grid, dtype=float)

@@ -88,3 +88,33 @@ def test_mixed_precision_within_one_percent(case, cuda_device):
     peak = np.max(np.abs(ref))
     assert np.max(np.abs(spec - ref)) <= 1e-2 * peak
     assert spec.sum() == pytest.approx(ref.sum(), rel=1e-2)
+
+
+def test_general_tabulation_grid_uses_search(cuda_device):
+    """A non-geometric tabulation grid takes the binary-search bracket."""
+    from pyrite_b200 import LineTables, mc_cxr_spectrum
+    from pyrite_b200.tables import ReflectionRows, geometric_grid
+
+    d, seg, tables, rows = inputs("si50")
+    E0 = d["E_tab"]
+    E1 = E0 * (1.0 + 1e-3 * np.sin(np.arange(E0.size)))
+    E1 = np.maximum.accumulate(E1)
+    assert geometric_grid(E1)[1] == 0.0
+    interp = lambda tab: np.array([np.interp(E1, E0, row) for row in np.atleast_2d(tab)])
+    t1 = LineTables(E1, interp(d["chi_re"]), interp(d["chi_im"]), interp(d["u_re"]), interp(d["u_im"]),
+                    interp(d["log_mu"]), np.interp(E1, E0, d["delta"]))
+    spec, pairs = mc_cxr_spectrum(seg, d["E_grid"], "silicon", None, tables=t1, n_hat=d["n_hat"], rows=rows,
+                                  line_quadrature="node", return_pairs=True, device=cuda_device)
+    E, a, w, good = pairs[0]
+    tr = golden(f"transport_{d['transport']}")
+    oseg = dict(v_hat=tr["v_hat"], E_keV=tr["E_repr_keV"], L_ang=tr["L_ang"], r_mid=tr["r_mid"],
+                elec_id=tr["elec_id"])
+    E_grid = d["E_grid"]
+    pad = 0.2 * (E_grid[-1] - E_grid[0])
+    t = dict(G=d["G"], ES=d["ES"], EP=d["EP"], WM=d["WM"], row_table=d["row_table"], E_tab=E1,
+             chi_re=t1.chi_re, chi_im=t1.chi_im, u_re=t1.u_re, u_im=t1.u_im, log_mu=t1.log_mu,
+             delta=t1.delta, lo_keep=E_grid[0] - pad, hi_keep=E_grid[-1] + pad)
+    oE, oa, ow, og = oracle.cxr_lines(t, d["n_hat"], d["thickness"], oseg, int(d["Ne"]))
+    both = good.astype(bool) & og
+    assert np.mean(good.astype(bool) == og) > 0.9999
+    np.testing.assert_allclose(w[both], ow[both], rtol=1e-8)
