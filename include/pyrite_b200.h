@@ -201,6 +201,10 @@ typedef struct pb_cxr_tables {
      * closed-form bracket; tab_log_step <= 0 means a general ascending grid. */
     double tab_log0;
     double tab_log_step;
+    /* Optional [n_tab]: max |delta| over E_tab[i:]. Bounds the refraction
+     * shift of a root, so the mixed path can drop pairs that cannot reach
+     * the keep window before solving for the root. */
+    const double *delta_tail_absmax;
 } pb_cxr_tables;
 
 typedef struct pb_cxr_args {

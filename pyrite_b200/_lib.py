@@ -88,6 +88,7 @@ class PbCxrTables(C.Structure):
         ("n_tab", _i32), ("E_tab", _vp), ("chi_re", _vp), ("chi_im", _vp), ("u_re", _vp),
         ("u_im", _vp), ("n_mu", _i32), ("log_mu", _vp), ("delta", _vp), ("lo_keep", _f64),
         ("hi_keep", _f64), ("tab_log0", _f64), ("tab_log_step", _f64),
+        ("delta_tail_absmax", _vp),
     ]
 
 

@@ -330,6 +330,7 @@ def _fill_tables(h: _Holder, rows, tables: LineTables, lo_keep, hi_keep, d_index
     t.delta = _ptr(h.f64(tables.delta))
     t.lo_keep, t.hi_keep = float(lo_keep), float(hi_keep)
     t.tab_log0, t.tab_log_step = geometric_grid(tables.E_tab)
+    t.delta_tail_absmax = _ptr(h.f64(np.maximum.accumulate(np.abs(np.asarray(tables.delta, float))[::-1])[::-1]))
     return t
 
 

@@ -226,6 +226,30 @@ struct Line {
     bool good;
 };
 
+// Cheap test of whether a pair's resonance can reach the keep window under
+// any refraction the table allows: omega <= 0 is never kept (denom > 0 is
+// required); above the window, with D the largest |delta| the table holds at
+// or above E_vac / 1.5, D |grad L| <= denom_vac / 2 keeps every root iterate
+// (and so the root) at or above E_vac / 1.5, by induction over the passes.
+template <class Real>
+__device__ __forceinline__ bool pair_may_keep(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                              const Real *E_tab, const Real *dtail, int n_tab,
+                                              const pb_cxr_tables &t, const TabIndex &ti) {
+    const Real r_num = (Real)0.5 * rw.g2 * sp.inv_E;
+    const Real r_den = rw.n_dot_g * sp.inv_E;
+    const Real num = (sp.vx * rw.G[0] + sp.vy * rw.G[1] + sp.vz * rw.G[2]) - r_num;
+    const Real denom_vac = sp.denom_row + r_den;
+    if (!sp.radiates || !(num > (Real)0) || !(denom_vac > (Real)0)) return false;
+    if (dtail == nullptr) return true;
+    const Real E_low = (Real)kHbarcEvAng * rdiv(num, denom_vac) * (Real)(1.0 / 1.5);
+    if (E_low < (Real)t.hi_keep) return true;
+    int ix;
+    Real fr;
+    bool bl, ab;
+    bracket<Real>(E_tab, n_tab, E_low, ix, fr, bl, ab, ti);
+    return !(dtail[ix - 1] * r_sqrt(sp.grad2) <= (Real)0.5 * denom_vac);
+}
+
 // The per-pair chain. ``E_tab``/``delta_tab``/``log_mu`` point at the
 // shared-memory staging (or global memory for a large FP64 grid).
 template <class Real>
@@ -482,27 +506,49 @@ __device__ __forceinline__ double q_osc_f32(double u) {
     return (double)(cs * p1 / (float)u - sn * p2 * yf);
 }
 
-// Exact mass of sinc^2 over [x_lo, x_hi] (line-centred first-zero units).
+// One bin edge of a line, in both antiderivative forms it may be needed in.
+struct EdgeCache {
+    bool valid;
+    double x;       // line-centred first-zero units
+    bool has_r, has_q;
+    double r;       // R(x), the sinc^2 antiderivative minus sign(x)/2
+    double q;       // Q(2 pi |x|), the oscillatory part of the far form
+};
+
 template <bool kMixed>
-__device__ __forceinline__ double bin_mass(double x_lo, double x_hi, double &r_lo, bool &have_r_lo) {
+__device__ __forceinline__ double edge_r(EdgeCache &e) {
+    if (!e.has_r) { e.r = sincsq_tail(e.x); e.has_r = true; }
+    return e.r;
+}
+
+template <bool kMixed>
+__device__ __forceinline__ double edge_q(EdgeCache &e) {
+    if (!e.has_q) {
+        const double u = 2.0 * kPi * fabs(e.x);
+        e.q = kMixed ? q_osc_f32(u) : q_osc_f64(u);
+        e.has_q = true;
+    }
+    return e.q;
+}
+
+// Exact mass of sinc^2 over [lo.x, hi.x]: the far closed form when both
+// edges are beyond the asymptotic threshold on one side, else the
+// difference of antiderivatives.
+template <bool kMixed>
+__device__ __forceinline__ double bin_mass(EdgeCache &lo, EdgeCache &hi) {
     const double u_lim = kMixed ? 24.0 : 48.0;
+    const double x_lo = lo.x, x_hi = hi.x;
     const double u_lo = 2.0 * kPi * fabs(x_lo), u_hi = 2.0 * kPi * fabs(x_hi);
     if ((x_lo > 0.0 || x_hi < 0.0) && fmin(u_lo, u_hi) >= u_lim) {
-        // Both edges far on one side: closed form (mirror the negative side).
-        const double a = x_lo > 0.0 ? x_lo : -x_hi;
-        const double b = x_lo > 0.0 ? x_hi : -x_lo;
-        const double ua = 2.0 * kPi * a, ub = 2.0 * kPi * b;
+        const bool pos = x_lo > 0.0;
+        const double a = pos ? x_lo : -x_hi;
+        const double b = pos ? x_hi : -x_lo;
         const double env = (b - a) / (2.0 * kPi * kPi * a * b);
-        const double osc = kMixed ? (q_osc_f32(ub) - q_osc_f32(ua)) : (q_osc_f64(ub) - q_osc_f64(ua));
-        have_r_lo = false;
+        const double osc = pos ? (edge_q<kMixed>(hi) - edge_q<kMixed>(lo))
+                               : (edge_q<kMixed>(lo) - edge_q<kMixed>(hi));
         return env + osc / kPi;
     }
-    if (!have_r_lo) r_lo = sincsq_tail(x_lo);
-    const double r_hi = sincsq_tail(x_hi);
-    const double mass = r_hi - r_lo + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
-    r_lo = r_hi;
-    have_r_lo = true;
-    return mass;
+    return edge_r<kMixed>(hi) - edge_r<kMixed>(lo) + ((x_lo < 0.0 && x_hi >= 0.0) ? 1.0 : 0.0);
 }
 
 // Bin-mean deposit of a line: exact bin integrals within the line's window
@@ -542,12 +588,21 @@ __device__ __forceinline__ LineWindow line_window(double E_r, double a, const Bi
 
 template <bool kMixed>
 __device__ __forceinline__ double line_bin_value(double E_r, double a, double w, int b, const LineWindow &lw,
-                                                 const BinAxis &ax, int K_far) {
-    const double x_lo = a * (ax.edges[b] - E_r) / kPi;
-    const double x_hi = a * (ax.edges[b + 1] - E_r) / kPi;
-    double r_lo = 0.0;
-    bool have = false;
-    const double mass = bin_mass<kMixed>(x_lo, x_hi, r_lo, have);
+                                                 const BinAxis &ax, int K_far, EdgeCache &ec) {
+    EdgeCache lo_e;
+    if (ec.valid && ec.x == a * (ax.edges[b] - E_r) / kPi) {
+        lo_e = ec;
+    } else {
+        lo_e.valid = true;
+        lo_e.x = a * (ax.edges[b] - E_r) / kPi;
+        lo_e.has_r = lo_e.has_q = false;
+    }
+    EdgeCache hi_e;
+    hi_e.valid = true;
+    hi_e.x = a * (ax.edges[b + 1] - E_r) / kPi;
+    hi_e.has_r = hi_e.has_q = false;
+    const double mass = bin_mass<kMixed>(lo_e, hi_e);
+    ec = hi_e;
     const double width = ax.edges[b + 1] - ax.edges[b];
     double v = w * (mass * (kPi / a) / width);
     if (lw.mom && (b - lw.c > K_far || lw.c - b > K_far)) {
@@ -567,17 +622,21 @@ __device__ __forceinline__ void line_moments(double E_r, double a, double w, con
     atomicAdd(&mom[3 * slot + 2], m * dd * dd);
 }
 
-// One block: a direction (blockIdx.y) and a strided range of segment tiles.
-// Phase A evaluates the (segment x row) pairs of a tile and pushes every
-// kept line onto a shared-memory queue (warp ballot + one shared atomic per
-// warp); phase B spreads the queued lines' (line, bin) work items evenly over
-// the block, so line deposits never run in a lone lane of a divergent warp.
+// Persistent blocks over the flattened (direction, segment tile) work, in
+// contiguous ranges, so the grid is an exact multiple of the SM count; a
+// block flushes its on-chip spectrum whenever its direction changes.
+// Per pass (a segment tile x a chunk of reflection rows):
+//   A0  a cheap prefilter drops pairs whose resonance cannot reach the keep
+//       window and compacts the survivors into a shared queue (warp ballot);
+//   A1  the full chain runs densely over the survivors and pushes kept lines
+//       onto a second shared queue;
+//   B   the queued lines' (line, bin) work is cut into 4-item chunks spread
+//       over the block; edges shared by consecutive bins are evaluated once.
 template <class Real>
 __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool kMixed = sizeof(Real) == 4;
-    const int d = blockIdx.y;
-    const double *nh = a.n_hat + 3 * d;
+    constexpr int kChunk = 4;
     const int n_g = a.tables.n_g;
     const int n_tab = a.tables.n_tab;
     const int n_mu = a.tables.n_mu;
@@ -587,7 +646,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     if (a.n_seg_device) n_seg = (int64_t)*a.n_seg_device;
     if (n_seg > a.n_seg && a.n_seg > 0) n_seg = a.n_seg;
 
-    // Shared layout: [rows][segs][queue][E_tab][delta][log_mu][spec][moments]
+    // Shared layout: [rows][segs][queues][tables][spec][moments][float spec]
     unsigned char *cur = smem_raw;
     RowPre<Real> *rows = reinterpret_cast<RowPre<Real> *>(cur);
     cur += sizeof(RowPre<Real>) * kRowChunk;
@@ -600,19 +659,24 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     int *qStart = reinterpret_cast<int *>(qW + kQueue);   // kQueue + 1 prefix entries
     int *qB0 = qStart + kQueue + 1;
     int *qC = qB0 + kQueue;
-    int *scratch = qC + kQueue;                             // warp sums + counter
+    int *pq = qC + kQueue;                                  // surviving pair ids
+    int *scratch = pq + kQueue;                             // warp sums + counters
     cur = reinterpret_cast<unsigned char *>(scratch + 64);
     cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
     const bool tab_smem = n_tab <= kMaxTab;
     Real *E_tab_s = reinterpret_cast<Real *>(cur);
     Real *delta_s = E_tab_s + (tab_smem ? n_tab : 0);
     Real *logmu_s = delta_s + (tab_smem ? n_tab : 0);
-    cur = reinterpret_cast<unsigned char *>(logmu_s + (tab_smem ? n_tab * n_mu : 0));
+    Real *dtail_s = logmu_s + (tab_smem ? n_tab * n_mu : 0);
+    const bool has_dtail = kMixed && tab_smem && a.tables.delta_tail_absmax != nullptr && a.pair_E == nullptr;
+    cur = reinterpret_cast<unsigned char *>(dtail_s + (tab_smem ? n_tab : 0));
     cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
     double *spec_s = reinterpret_cast<double *>(cur);
     double *mom_s = spec_s + (binmean ? n_E : 0);
     const int n_mom = n_E + 2 * far_pad;
+    float *spec_f = reinterpret_cast<float *>(mom_s + (K_far > 0 ? 3 * n_mom : 0));
     int &q_count = scratch[40];
+    int &p_count = scratch[42];
 
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -620,15 +684,17 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         for (int j = tid; j < n_tab; j += blockDim.x) {
             E_tab_s[j] = (Real)a.tables.E_tab[j];
             delta_s[j] = (Real)a.tables.delta[j];
+            if (has_dtail) dtail_s[j] = (Real)a.tables.delta_tail_absmax[j];
         }
         for (int j = tid; j < n_tab * n_mu; j += blockDim.x) logmu_s[j] = (Real)a.tables.log_mu[j];
     }
+    const Real *dtail = has_dtail ? dtail_s : nullptr;
     if (binmean) {
-        for (int j = tid; j < n_E; j += blockDim.x) spec_s[j] = 0.0;
+        for (int j = tid; j < n_E; j += blockDim.x) { spec_s[j] = 0.0; spec_f[j] = 0.0f; }
         if (K_far > 0)
             for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
-    if (tid == 0) q_count = 0;
+    if (tid == 0) { q_count = 0; p_count = 0; }
     const Real *E_tab = tab_smem ? E_tab_s : reinterpret_cast<const Real *>(a.tables.E_tab);
     const Real *delta_tab = tab_smem ? delta_s : reinterpret_cast<const Real *>(a.tables.delta);
     const Real *log_mu = tab_smem ? logmu_s : reinterpret_cast<const Real *>(a.tables.log_mu);
@@ -651,11 +717,43 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     __syncthreads();
 
     const int64_t n_tiles = (n_seg + kSegTile - 1) / kSegTile;
+    const int64_t n_work = n_tiles * a.n_dir;
+    const int64_t w_begin = n_work * blockIdx.x / gridDim.x;
+    const int64_t w_end = n_work * (blockIdx.x + 1) / gridDim.x;
     const bool pairs_out = a.pair_E != nullptr;
     const bool lines_out = a.line_E != nullptr;
     const double exact_widths = K_far > 0 ? a.exact_widths : 0.0;
     const int n_warps = blockDim.x >> 5;
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    int d_cur = -1;
+
+    auto flush = [&](int d) {
+        // Publish (and clear) the block's spectrum of direction d.
+        __syncthreads();
+        if (binmean && d >= 0) {
+            double *gspec = a.spec + (int64_t)d * n_E;
+            for (int j = tid; j < n_E; j += blockDim.x) {
+                if (spec_s[j] != 0.0) atomicAdd(&gspec[j], spec_s[j]);
+                spec_s[j] = 0.0;
+            }
+            if (K_far > 0) {
+                double *gm = a.far_moments + (int64_t)d * n_mom * 3;
+                for (int j = tid; j < 3 * n_mom; j += blockDim.x) {
+                    if (mom_s[j] != 0.0) atomicAdd(&gm[j], mom_s[j]);
+                    mom_s[j] = 0.0;
+                }
+            }
+        }
+        __syncthreads();
+    };
+
+    for (int64_t wk = w_begin; wk < w_end; ++wk) {
+        const int d = (int)(wk / n_tiles);
+        const int64_t tile = wk - (int64_t)d * n_tiles;
+        if (d != d_cur) {
+            flush(d_cur);
+            d_cur = d;
+        }
+        const double *nh = a.n_hat + 3 * d;
         const int64_t s0 = tile * kSegTile;
         const int nst = (int)((n_seg - s0) < kSegTile ? (n_seg - s0) : kSegTile);
         __syncthreads();
@@ -682,14 +780,37 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 r.row = a.tables.row_table[g];
             }
             __syncthreads();
-            // ---- phase A: pairs -> queue ----
+            // ---- A0: prefilter and compact the surviving pairs ----
             const int n_pairs = nst * ng;
-            const int n_iter = (n_pairs + (int)blockDim.x - 1) / (int)blockDim.x;
-            for (int it = 0; it < n_iter; ++it) {
-                const int q = it * blockDim.x + tid;
+            int n_surv;
+            if (dtail != nullptr) {
+                const int n_it0 = (n_pairs + (int)blockDim.x - 1) / (int)blockDim.x;
+                for (int it = 0; it < n_it0; ++it) {
+                    const int q = it * blockDim.x + tid;
+                    bool ok = false;
+                    if (q < n_pairs) {
+                        const int si = q / ng;
+                        ok = pair_may_keep<Real>(segs[si], rows[q - si * ng], E_tab, dtail, n_tab, a.tables, ti);
+                    }
+                    const unsigned mask = __ballot_sync(0xffffffffu, ok);
+                    int base = 0;
+                    if (lane == 0 && mask) base = atomicAdd(&p_count, __popc(mask));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (ok) pq[base + __popc(mask & ((1u << lane) - 1u))] = q;
+                }
+                __syncthreads();
+                n_surv = p_count;
+            } else {
+                n_surv = n_pairs;
+            }
+            // ---- A1: the full chain over the survivors ----
+            const int n_it1 = (n_surv + (int)blockDim.x - 1) / (int)blockDim.x;
+            for (int it = 0; it < n_it1; ++it) {
+                const int k = it * blockDim.x + tid;
                 Line<Real> ln;
                 ln.good = false;
-                if (q < n_pairs) {
+                if (k < n_surv) {
+                    const int q = dtail != nullptr ? pq[k] : k;
                     const int si = q / ng;
                     const int gi = q - si * ng;
                     ln = pair_line<Real>(segs[si], rows[gi], E_tab, delta_tab, log_mu, n_tab, n_mu,
@@ -719,16 +840,20 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                     if (lane == 0 && mask) base = atomicAdd(&q_count, __popc(mask));
                     base = __shfl_sync(0xffffffffu, base, 0);
                     if (ln.good) {
-                        const int k = base + __popc(mask & ((1u << lane) - 1u));
-                        qE[k] = ln.E_res;
-                        qA[k] = ln.a_width;
-                        qW[k] = ln.weight;
+                        const int kk = base + __popc(mask & ((1u << lane) - 1u));
+                        qE[kk] = ln.E_res;
+                        qA[kk] = ln.a_width;
+                        qW[kk] = ln.weight;
                     }
                 }
             }
-            if (!binmean) continue;
+            if (!binmean) {
+                __syncthreads();
+                if (tid == 0) p_count = 0;
+                continue;
+            }
             __syncthreads();
-            // ---- phase B: windows, scan, spread (line, bin) items ----
+            // ---- B: windows, scan, spread (line, bin) chunks ----
             const int nq = q_count;
             for (int j = tid; j < nq; j += blockDim.x) {
                 const LineWindow lw = line_window((double)qE[j], (double)qA[j], ax, exact_widths, K_far,
@@ -739,7 +864,6 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 if (lw.mom) line_moments((double)qE[j], (double)qA[j], (double)qW[j], lw, ax, mom_s);
             }
             __syncthreads();
-            // exclusive scan of qStart[0..nq) (at most kQueue entries)
             {
                 const int per = (nq + (int)blockDim.x - 1) / (int)blockDim.x;
                 const int j0 = tid * per;
@@ -765,36 +889,44 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 __syncthreads();
             }
             const int n_items = qStart[nq];
-            for (int item = tid; item < n_items; item += blockDim.x) {
-                int lo = 0, hi = nq;  // last line with qStart[line] <= item
+            const int n_chunks = (n_items + kChunk - 1) / kChunk;
+            for (int ch = tid; ch < n_chunks; ch += blockDim.x) {
+                const int i0 = ch * kChunk;
+                const int i1 = min(i0 + kChunk, n_items);
+                int lo = 0, hi = nq;  // last line with qStart[line] <= i0
                 while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
-                    if (qStart[mid] <= item) lo = mid; else hi = mid;
+                    if (qStart[mid] <= i0) lo = mid; else hi = mid;
                 }
-                LineWindow lw;
-                lw.c = qC[lo];
-                lw.mom = lw.c != INT_MIN;
-                lw.b0 = qB0[lo];
-                const int b = qB0[lo] + (item - qStart[lo]);
-                const double v = line_bin_value<kMixed>((double)qE[lo], (double)qA[lo], (double)qW[lo], b,
-                                                        lw, ax, K_far);
-                atomicAdd(&spec_s[b], v);
+                int line = lo;
+                EdgeCache ec;
+                ec.valid = false;
+                for (int item = i0; item < i1; ++item) {
+                    while (item >= qStart[line + 1]) { ++line; ec.valid = false; }
+                    LineWindow lw;
+                    lw.c = qC[line];
+                    lw.mom = lw.c != INT_MIN;
+                    lw.b0 = qB0[line];
+                    const int b = lw.b0 + (item - qStart[line]);
+                    const double v = line_bin_value<kMixed>((double)qE[line], (double)qA[line],
+                                                            (double)qW[line], b, lw, ax, K_far, ec);
+                    if constexpr (kMixed) atomicAdd(&spec_f[b], (float)v);
+                    else atomicAdd(&spec_s[b], v);
+                }
+            }
+            if constexpr (kMixed) {
+                // Fold the pass's float partials into the FP64 spectrum.
+                __syncthreads();
+                for (int j = tid; j < n_E; j += blockDim.x) {
+                    const float v = spec_f[j];
+                    if (v != 0.0f) { spec_s[j] += (double)v; spec_f[j] = 0.0f; }
+                }
             }
             __syncthreads();
-            if (tid == 0) q_count = 0;
+            if (tid == 0) { q_count = 0; p_count = 0; }
         }
     }
-    __syncthreads();
-    if (binmean) {
-        double *gspec = a.spec + (int64_t)d * n_E;
-        for (int j = tid; j < n_E; j += blockDim.x)
-            if (spec_s[j] != 0.0) atomicAdd(&gspec[j], spec_s[j]);
-        if (K_far > 0) {
-            double *gm = a.far_moments + (int64_t)d * n_mom * 3;
-            for (int j = tid; j < 3 * n_mom; j += blockDim.x)
-                if (mom_s[j] != 0.0) atomicAdd(&gm[j], mom_s[j]);
-        }
-    }
+    flush(d_cur);
 }
 
 // Far-field finalize: spec[d][b] += sum_c M[d][c] . envelope(b, c) over the
@@ -885,11 +1017,11 @@ __global__ void node_reduce_kernel(const double *E_grid, int n_E, const double *
 template <class Real>
 static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moments) {
     size_t b = sizeof(RowPre<Real>) * kRowChunk + sizeof(SegPre<Real>) * kSegTile + 16;
-    b += sizeof(Real) * 3 * kQueue + sizeof(int) * (3 * kQueue + 1 + 64) + 16;
-    if (a.tables.n_tab <= kMaxTab) b += sizeof(Real) * (size_t)a.tables.n_tab * (2 + a.tables.n_mu);
+    b += sizeof(Real) * 3 * kQueue + sizeof(int) * (4 * kQueue + 1 + 64) + 16;
+    if (a.tables.n_tab <= kMaxTab) b += sizeof(Real) * (size_t)a.tables.n_tab * (3 + a.tables.n_mu);
     b += 16;
     if (a.quadrature == PB_QUAD_BINMEAN) {
-        b += sizeof(double) * (size_t)a.n_E;
+        b += (sizeof(double) + sizeof(float)) * (size_t)a.n_E;
         if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
     }
     return b;
@@ -922,12 +1054,11 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCxrThreads, smem);
     if (err != cudaSuccess) return err;
     if (per_sm < 1) per_sm = 1;
-    const int64_t tiles = (a.n_seg + kSegTile - 1) / kSegTile;
-    int64_t gx = ((int64_t)sms * per_sm + a.n_dir - 1) / a.n_dir;
-    if (gx > tiles) gx = tiles;
+    const int64_t work = (a.n_seg + kSegTile - 1) / kSegTile * (int64_t)a.n_dir;
+    int64_t gx = (int64_t)sms * per_sm;
+    if (gx > work) gx = work;
     if (gx < 1) gx = 1;
-    dim3 grid((unsigned)gx, (unsigned)a.n_dir);
-    kern<<<grid, kCxrThreads, smem, s>>>(a, K_far, far_pad);
+    kern<<<(unsigned)gx, kCxrThreads, smem, s>>>(a, K_far, far_pad);
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     if (K_far > 0) {

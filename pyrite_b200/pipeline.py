@@ -148,6 +148,7 @@ class ScoringCase:
         t.delta = _ptr(h.f64(lt.delta))
         t.lo_keep, t.hi_keep = lo_keep, hi_keep
         t.tab_log0, t.tab_log_step = geometric_grid(lt.E_tab)
+        t.delta_tail_absmax = _ptr(h.f64(np.maximum.accumulate(np.abs(np.asarray(lt.delta, float))[::-1])[::-1]))
         c.tables = t
         c.n_E = self.n_E
         c.E_grid = _ptr(h.f64(E_grid))
