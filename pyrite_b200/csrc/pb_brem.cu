@@ -45,6 +45,13 @@ __device__ __forceinline__ float b_log(float x) { return logf(x); }
 __device__ __forceinline__ double b_expm1(double x) { return expm1(x); }
 __device__ __forceinline__ float b_expm1(float x) { return expm1f(x); }
 
+// Base-2 exponential on the SFU (about 2 ulp), for the float path.
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <class Real>
 __device__ __forceinline__ Real b_path(Real z, Real thickness, Real nz) {
     const Real inv_nz = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
@@ -67,6 +74,7 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
     __shared__ Real Zs[kBremMaxEl];
     __shared__ Real inv_nz[kBremMaxDir];
     __shared__ int up[kBremMaxDir];
+    __shared__ float inv_f_ln2[kBremMaxDir];
     const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
     const Real T_slab = (Real)a.thickness;
     const int n_el = a.n_el;
@@ -79,6 +87,7 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
         const Real nz = (Real)a.n_hat[3 * (d0 + threadIdx.x) + 2];
         inv_nz[threadIdx.x] = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
         up[threadIdx.x] = nz < (Real)0;
+        inv_f_ln2[threadIdx.x] = (float)(fmax(fabs((double)nz), 1.0e-12) / 0.6931471805599453);
     }
     const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
     const Real k = (Real)k_kev_d;
@@ -158,23 +167,36 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
                     nsig += b.nL[el] * (Z * Z) * common * __fdividef(b.den_i[el], den_f);
                 }
             }
+            if constexpr (sizeof(Real) == 8) {
 #pragma unroll
-            for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                if (dd < nd) {
-                    const Real f = inv_nz[dd];
-                    const Real p0 = up[dd] ? b.path0 * f : (T_slab - b.path0) * f;
-                    const Real p1 = up[dd] ? b.path1 * f : (T_slab - b.path1) * f;
-                    if constexpr (sizeof(Real) == 8) {
+                for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                    if (dd < nd) {
+                        const Real f = inv_nz[dd];
+                        const Real p0 = up[dd] ? b.path0 * f : (T_slab - b.path0) * f;
+                        const Real p1 = up[dd] ? b.path1 * f : (T_slab - b.path1) * f;
                         acc[dd] += (double)(nsig * b_mean_transmission<Real>(p0 * mu, p1 * mu));
-                    } else {
-                        // exp(-lo) (1 - e^-d)/d with base-2 exponentials; the
-                        // series below d = 0.01 keeps float accuracy.
-                        const float t0 = p0 * mu, t1 = p1 * mu;
-                        const float lo = fminf(t0, t1);
-                        const float d = fabsf(t1 - t0);
-                        const float ratio = d > 0.01f ? __fdividef(1.0f - exp2f(-d * 1.44269504f), d)
-                                                      : 1.0f - d * (0.5f - d * (1.0f / 6.0f - d * (1.0f / 24.0f)));
-                        part[dd] += nsig * exp2f(-lo * 1.44269504f) * ratio;
+                    }
+                }
+            } else {
+                // Escape mean exp(-lo) (1 - e^-D)/D per direction with base-2
+                // optical depths A_s f (lower end, per side s) and B f (depth
+                // difference): two SFU exponentials per direction and one
+                // reciprocal per (segment, energy). Below D = 0.01 the series
+                // keeps float accuracy.
+                const float mu2 = mu * 1.44269504f;
+                const float A_dn = mu2 * fminf(T_slab - b.path0, T_slab - b.path1);
+                const float A_up = mu2 * fminf(b.path0, b.path1);
+                const float B = mu2 * fabsf(b.path1 - b.path0);
+                const float inv_B = B > 0.0f ? __fdividef(1.0f, B) : 0.0f;
+#pragma unroll
+                for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                    if (dd < nd) {
+                        const float f = inv_nz[dd];
+                        const float x = B * f;                 // D / ln 2
+                        const float D = x * 0.69314718f;
+                        const float ratio = D > 0.01f ? (1.0f - ex2_approx(-x)) * inv_B * inv_f_ln2[dd]
+                                                      : 1.0f - D * (0.5f - D * (1.0f / 6.0f - D * (1.0f / 24.0f)));
+                        part[dd] += nsig * ex2_approx(-(up[dd] ? A_up : A_dn) * f) * ratio;
                     }
                 }
             }
