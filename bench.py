@@ -256,6 +256,9 @@ def main():
         results[precision] = dict(total_ms=total_ms, n_steps=n_steps, t_tr=t_tr, t_cxr=t_cxr, t_brem=t_brem,
                                   status=case.device_status(), res=case.results())
     mixed = results["mixed"]
+    for name, r in results.items():
+        if not (r["res"]["cxr"].sum() > 0 and r["res"].get("brem", np.ones(1)).sum() > 0):
+            raise SystemExit(f"bench: the {name} spectra are empty; refusing to report a rate")
     ms_per_step = mixed["total_ms"] / mixed["n_steps"]
     value = world * args.histories / (ms_per_step / 1e3)
     case = cases["mixed"]
@@ -273,6 +276,11 @@ def main():
         "pairs_per_s": world * pairs / (ms_per_step / 1e3),
         "kernel_ms": {"transport": mixed["t_tr"], "cxr": mixed["t_cxr"], "brem": mixed["t_brem"]},
         "device_status": mixed["status"],
+        "spectrum_check": {
+            "cxr_integral": float(mixed["res"]["cxr"].sum()),
+            "brem_integral": float(mixed["res"]["brem"].sum()) if "brem" in mixed["res"] else None,
+            "fates": [int(v) for v in mixed["res"]["fates"]],
+        },
         "roofline": {
             "bound": "fp32", "kernel": "cxr_kernel<float> (PXR+CBS lines + bin-mean deposit)",
             "achieved": achieved_tflops, "peak": peak_fp32, "unit": "TFLOP/s",

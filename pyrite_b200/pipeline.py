@@ -129,6 +129,8 @@ class ScoringCase:
         c.n_dir = self.n_dir
         c.n_hat = _ptr(h.f64(n_hats))
         c.thickness = st.thickness
+        # Every streamed history radiates (elec_id < Ne for all of them).
+        c.Ne = 1 << 62
         c.n_seg = cap
         c.r_mid, c.v_hat, c.L = _ptr(self.seg_r), _ptr(self.seg_v), _ptr(self.seg_L)
         c.E_keV, c.elec_id = _ptr(self.seg_E), _ptr(self.seg_id)
@@ -174,6 +176,7 @@ class ScoringCase:
             b.n_dir = self.n_dir
             b.n_hat = c.n_hat
             b.thickness = st.thickness
+            b.Ne = c.Ne
             b.n_seg = cap
             b.r_mid, b.v_hat, b.L, b.E_keV, b.elec_id = c.r_mid, c.v_hat, c.L, c.E_keV, c.elec_id
             b.n_seg_device = c.n_seg_device
