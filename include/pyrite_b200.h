@@ -276,6 +276,23 @@ int pb_cxr_score(const pb_cxr_args *args, void *stream);
 /* Bethe-Heitler + Elwert track-length bremsstrahlung of a segment list. */
 int pb_brem_score(const pb_brem_args *args, void *stream);
 
+/* pb_cxr_score without any device allocation, for callers that cannot call
+ * cudaMalloc: code running inside an allocator or memory-pool callback, an
+ * embedding runtime that owns all device memory, or a deployment that fixes
+ * every allocation at load time. No counterpart in the reference.
+ *
+ * Bin-mean quadrature only. ``far_moments`` is ignored: the far-field
+ * workspace is a fixed device array built into the library (2 MiB per GPU
+ * that loads it, held until the process exits), limited to
+ * n_dir * (n_E + 2 far_pad) * 3 <= 262144 FP64 moments; larger requests
+ * fail with PB_ERR_CAPACITY. The caller still owns every input and output.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array and clear it on entry: calls that overlap
+ * on the GPU (different streams, threads or processes sharing a context)
+ * race on it and must be serialised by the caller. */
+int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -122,6 +122,7 @@ EXPORTS = (
     "pb_transport",
     "pb_cxr_score",
     "pb_brem_score",
+    "pb_cxr_score_noalloc",
 )
 
 _lib = None
@@ -148,6 +149,7 @@ def load(path: Path | None = None):
     lib.pb_transport.argtypes = [C.POINTER(PbTransportArgs), _vp]
     lib.pb_cxr_score.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_brem_score.argtypes = [C.POINTER(PbBremArgs), _vp]
+    lib.pb_cxr_score_noalloc.argtypes = [C.POINTER(PbCxrArgs), _vp]
     if path is None:
         _lib = lib
     return lib

@@ -41,6 +41,10 @@ int device_sms() {
 
 }  // namespace
 
+namespace pb {
+void set_last_error(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+}  // namespace pb
+
 extern "C" {
 
 int pb_abi_version(void) { return PB_ABI_VERSION; }

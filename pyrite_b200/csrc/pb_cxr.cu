@@ -26,6 +26,8 @@
 // accumulation in double.
 #include <climits>
 #include <cstdint>
+#include <cstdio>
+#include <mutex>
 
 #include "pb_common.cuh"
 #include "pb_internal.h"
@@ -1082,3 +1084,88 @@ cudaError_t launch_cxr(const pb_cxr_args &a, cudaStream_t s, int sms) {
 }
 
 }  // namespace pb
+
+// ---------------------------------------------------------------------------
+// pb_cxr_score_noalloc: the bin-mean scorer for callers that cannot allocate
+// device memory (code running inside a host-side allocator or memory-pool
+// callback, an embedding runtime that owns all device memory and forbids
+// cudaMalloc, or a static-memory deployment that fixes every allocation at
+// load time). Its far-field workspace is this file-scope device array; every
+// GPU that loads the library reserves it until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocFarDoubles = size_t(1) << 18;  // 2 MiB of FP64 moments
+static __device__ __align__(256) double g_noalloc_far[kNoAllocFarDoubles];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {};
+thread_local char g_noalloc_err[256] = "";
+
+int noalloc_fail(int code, const char *msg) {
+    snprintf(g_noalloc_err, sizeof(g_noalloc_err), "%s", msg);
+    pb::set_last_error(g_noalloc_err);
+    return code;
+}
+
+}  // namespace
+
+extern "C" int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream) {
+    if (!args) return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: args is NULL");
+    if (args->quadrature != PB_QUAD_BINMEAN)
+        return noalloc_fail(PB_ERR_UNSUPPORTED,
+                            "pb_cxr_score_noalloc: only bin-mean quadrature (node sampling needs a line buffer)");
+    if (args->n_seg < 0 || args->n_dir < 1 || args->n_E < 1)
+        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: need n_seg >= 0, n_dir >= 1, n_E >= 1");
+    if (args->n_seg == 0) return PB_OK;
+    const pb_cxr_tables &t = args->tables;
+    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4 || !t.G || !t.ES || !t.EP || !t.WM ||
+        !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im || !t.u_re || !t.u_im || !t.log_mu || !t.delta)
+        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: incomplete reflection tables");
+    if (!args->n_hat || !args->r_mid || !args->v_hat || !args->L || !args->E_keV || !args->elec_id ||
+        !args->edges || !args->spec)
+        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: segment, axis and output pointers must be set");
+    const bool far = args->exact_widths > 0.0 && args->far_pad >= 0;
+    if (far) {
+        const size_t need = (size_t)args->n_dir * ((size_t)args->n_E + 2 * (size_t)args->far_pad) * 3;
+        if (need > kNoAllocFarDoubles) {
+            char msg[256];
+            snprintf(msg, sizeof(msg),
+                     "pb_cxr_score_noalloc: the far field needs %zu FP64 moments (n_dir * (n_E + 2 far_pad) * 3), "
+                     "over the fixed workspace of %zu; score fewer directions per call",
+                     need, kNoAllocFarDoubles);
+            return noalloc_fail(PB_ERR_CAPACITY, msg);
+        }
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return noalloc_fail(PB_ERR_CUDA, "pb_cxr_score_noalloc: no current CUDA device");
+    double *ws = nullptr;
+    {
+        // First call on a device: resolve the array's device address (host
+        // code must not use the symbol itself as a pointer).
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_far);
+            if (e != cudaSuccess) {
+                char msg[256];
+                snprintf(msg, sizeof(msg), "pb_cxr_score_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return noalloc_fail(PB_ERR_CUDA, msg);
+            }
+            g_noalloc_ptr[dev] = static_cast<double *>(p);
+        }
+        ws = g_noalloc_ptr[dev];
+    }
+    pb_cxr_args a = *args;
+    a.far_moments = far ? ws : nullptr;
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    const cudaError_t e = pb::launch_cxr(a, (cudaStream_t)stream, sms);
+    if (e != cudaSuccess) {
+        char msg[256];
+        snprintf(msg, sizeof(msg), "pb_cxr_score_noalloc: launch: %s", cudaGetErrorString(e));
+        return noalloc_fail(PB_ERR_CUDA, msg);
+    }
+    return PB_OK;
+}

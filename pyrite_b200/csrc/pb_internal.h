@@ -14,4 +14,7 @@ cudaError_t launch_transport(const pb_transport_args &a, cudaStream_t s, int sms
 cudaError_t launch_cxr(const pb_cxr_args &a, cudaStream_t s, int sms);
 cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms);
 
+// Record the message pb_last_error() returns on this thread.
+void set_last_error(const char *msg);
+
 }  // namespace pb
