@@ -25,6 +25,7 @@
 // phase a (E - E_r) formed and range-reduced in double and every
 // accumulation in double.
 #include <climits>
+#include <type_traits>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -38,6 +39,7 @@ constexpr int kSegTile = 16;
 constexpr int kRowChunk = 64;
 constexpr int kCxrThreads = 512;
 constexpr int kQueue = kSegTile * kRowChunk;  // every pair of a pass may keep a line
+constexpr int kXQueue = 2048;   // queued exact-window bins per class and pass
 constexpr int kMaxTab = 4096;   // E_tab / delta staged in shared memory up to this size
 constexpr int kMaxMu = 4;
 
@@ -368,26 +370,40 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
 }
 
 // ---- sine integral and the sinc^2 antiderivative --------------------------
-// Si(t) - pi/2 for t >= 0: power series for t <= 4; the continued fraction of
+// Si(t) - pi/2 for t >= 0: power series for t <= 13; the continued fraction of
 // E1(i t) by the modified Lentz method (Numerical Recipes "cisi") for
-// 4 < t < 40; the asymptotic auxiliary-function series beyond
+// 13 < t < 40; the asymptotic auxiliary-function series beyond
 // (Abramowitz & Stegun 5.2.34-5.2.35): Si - pi/2 = -f cos t - g sin t.
+constexpr int kSiTerms = 31;  // k = 30 term at t = 13 is ~3e-18
+struct SiSeries {
+    double c[kSiTerms];  // (-1)^k / ((2k+1) (2k+1)!)
+};
+__host__ __device__ constexpr SiSeries make_si_series() {
+    SiSeries s{};
+    double fact = 1.0;
+    for (int k = 0; k < kSiTerms; ++k) {
+        if (k > 0) fact *= (2.0 * k) * (2.0 * k + 1.0);
+        s.c[k] = ((k & 1) ? -1.0 : 1.0) / ((2.0 * k + 1.0) * fact);
+    }
+    return s;
+}
+
 __device__ double si_minus_half_pi(double t) {
-    if (t <= 4.0) {
+    if (t <= 13.0) {
+        // Power series in Horner form with compile-time coefficients; the
+        // sum of |terms| at t = 13 is ~2e4, so ~5e-12 absolute accuracy.
+        constexpr SiSeries kSi = make_si_series();
         const double t2 = t * t;
-        double term = t, sum = t;
-        for (int k = 1; k < 40; ++k) {
-            term *= -t2 / ((2.0 * k) * (2.0 * k + 1.0));
-            const double add = term / (2.0 * k + 1.0);
-            sum += add;
-            if (fabs(add) < 1e-18 * fabs(sum)) break;
-        }
-        return sum - 0.5 * kPi;
+        double p = kSi.c[kSiTerms - 1];
+#pragma unroll
+        for (int k = kSiTerms - 2; k >= 0; --k) p = fma(p, t2, kSi.c[k]);
+        return p * t - 0.5 * kPi;
     }
     double s, c;
     sincos(t, &s, &c);
     if (t >= 40.0) {
-        const double y = 1.0 / (t * t);
+        const double inv_t = 1.0 / t;
+        const double y = inv_t * inv_t;
         // f t = 1 - 2!/t^2 + 4!/t^4 - ..., g t^2 = 1 - 3!/t^2 + 5!/t^4 - ...
         double f = 1.0, g = 1.0, tf = 1.0, tg = 1.0;
         for (int k = 1; k < 12; ++k) {
@@ -397,25 +413,25 @@ __device__ double si_minus_half_pi(double t) {
             g += tg;
             if (fabs(tf) < 1e-17 && fabs(tg) < 1e-17) break;
         }
-        f /= t;
+        f *= inv_t;
         g *= y;
         return -f * c - g * s;
     }
     double br = 1.0, bi = t;
-    double den = br * br + bi * bi;
-    double dr = br / den, di = -bi / den;
+    double inv = 1.0 / (br * br + bi * bi);
+    double dr = br * inv, di = -bi * inv;
     double hr = dr, hi = di;
     double cr = 1e300, ci = 0.0;
     for (int i = 2; i < 200; ++i) {
         const double a = -(double)(i - 1) * (double)(i - 1);
         br += 2.0;
         const double xr = a * dr + br, xi = a * di + bi;
-        den = xr * xr + xi * xi;
-        dr = xr / den;
-        di = -xi / den;
-        den = cr * cr + ci * ci;
-        cr = br + a * cr / den;
-        ci = bi - a * ci / den;
+        inv = 1.0 / (xr * xr + xi * xi);
+        dr = xr * inv;
+        di = -xi * inv;
+        inv = a / (cr * cr + ci * ci);
+        cr = br + cr * inv;
+        ci = bi - ci * inv;
         const double delr = cr * dr - ci * di, deli = cr * di + ci * dr;
         const double nhr = hr * delr - hi * deli, nhi = hr * deli + hi * delr;
         hr = nhr;
@@ -438,6 +454,9 @@ __device__ double sincsq_tail(double x) {
     const double r = si_minus_half_pi(t) / kPi - u * su * su;
     return x >= 0.0 ? r : -r;
 }
+
+constexpr double kInvPi = 1.0 / kPi;
+constexpr double kInv2Pi2 = 1.0 / (2.0 * kPi * kPi);
 
 struct BinAxis {
     const double *edges;
@@ -465,13 +484,24 @@ __device__ __forceinline__ double centre_of(const BinAxis &ax, int c) {
 }
 
 // Far-field envelope expansion about centre c: 1/((A-d)(B-d)) ~
-// f0 + f1 d + f2 d^2 with A = E_lo - E_c, B = E_hi - E_c, d = E_r - E_c.
+// f0 + f1 d + f2 d^2 with A = E_lo - E_c, B = E_hi - E_c, d = E_r - E_c
+// (any common unit: the form scales as 1/unit^2). Float on the mixed path.
+template <bool kMixed>
 __device__ __forceinline__ double far_envelope(double A, double B, double d) {
-    const double AB = A * B;
-    const double f0 = 1.0 / AB;
-    const double f1 = (A + B) / (AB * AB);
-    const double f2 = (A * A + AB + B * B) / (AB * AB * AB);
-    return f0 + d * (f1 + d * f2);
+    if constexpr (kMixed) {
+        const float Af = (float)A, Bf = (float)B, df = (float)d;
+        const float AB = Af * Bf;
+        const float r = __frcp_rn(AB);
+        const float f1 = (Af + Bf) * r * r;
+        const float f2 = (Af * Af + AB + Bf * Bf) * r * r * r;
+        return (double)(r + df * (f1 + df * f2));
+    } else {
+        const double AB = A * B;
+        const double r = 1.0 / AB;
+        const double f1 = (A + B) * r * r;
+        const double f2 = (A * A + AB + B * B) * r * r * r;
+        return r + d * (f1 + d * f2);
+    }
 }
 
 // Oscillatory part of the sinc^2 antiderivative beyond the asymptotic
@@ -482,7 +512,8 @@ __device__ __forceinline__ double far_envelope(double A, double B, double d) {
 // g(u) ~ (1/u^2) sum_{k>=0} (-1)^k (2k+1)!/u^2k. The envelope term carries
 // the mass without the cancellation of a difference of antiderivatives.
 __device__ __forceinline__ double q_osc_f64(double u) {
-    const double y = 1.0 / (u * u);
+    const double inv_u = 1.0 / u;
+    const double y = inv_u * inv_u;
     double p1 = 0.0, p2 = 0.0;
     // 13 terms: the first omitted one at u = 48 is below 1e-17 of the leading.
     double t1 = 2.0 * y, t2 = 1.0;
@@ -494,18 +525,19 @@ __device__ __forceinline__ double q_osc_f64(double u) {
     }
     double sn, cs;
     sincos(u, &sn, &cs);
-    return cs * p1 / u - sn * p2 * y;
+    return cs * p1 * inv_u - sn * p2 * y;
 }
 
 // Float form for the mixed path; the phase u is reduced in double first.
 __device__ __forceinline__ double q_osc_f32(double u) {
-    const float yf = (float)(1.0 / (u * u));
+    const float inv_u = __frcp_rn((float)u);
+    const float yf = inv_u * inv_u;
     const float p1 = yf * (2.0f + yf * (-24.0f + yf * (720.0f + yf * (-40320.0f + yf * 3628800.0f))));
     const float p2 = 1.0f + yf * (-6.0f + yf * (120.0f + yf * (-5040.0f + yf * 362880.0f)));
     const double r = u - 2.0 * kPi * rint(u * (0.5 / kPi));
     float sn, cs;
     __sincosf((float)r, &sn, &cs);
-    return (double)(cs * p1 / (float)u - sn * p2 * yf);
+    return (double)(cs * p1 * inv_u - sn * p2 * yf);
 }
 
 // One bin edge of a line, in both antiderivative forms it may be needed in.
@@ -545,7 +577,12 @@ __device__ __forceinline__ double bin_mass(EdgeCache &lo, EdgeCache &hi) {
         const bool pos = x_lo > 0.0;
         const double a = pos ? x_lo : -x_hi;
         const double b = pos ? x_hi : -x_lo;
-        const double env = (b - a) / (2.0 * kPi * kPi * a * b);
+        double env;
+        if constexpr (kMixed) {
+            env = (double)__fdividef((float)((b - a) * kInv2Pi2), (float)a * (float)b);
+        } else {
+            env = (b - a) * kInv2Pi2 / (a * b);
+        }
         const double osc = pos ? (edge_q<kMixed>(hi) - edge_q<kMixed>(lo))
                                : (edge_q<kMixed>(lo) - edge_q<kMixed>(hi));
         return env + osc / kPi;
@@ -588,30 +625,134 @@ __device__ __forceinline__ LineWindow line_window(double E_r, double a, const Bi
     return lw;
 }
 
+// Mean of sinc^2 over [xc - dx/2, xc + dx/2] by its midpoint Taylor series
+// f + f2 dx^2/24 + f4 dx^4/1920 + f6 dx^6/322560, f = (1 - cos 2 pi x)/(2 pi^2 x^2),
+// with the derivatives by the Leibniz rule on (1 - cos 2 pi x) and x^-2
+// (montecarlo/spectrum/cxr/_bin_quadrature.py:179-221, the reference's
+// device bin mean, on by default there). Valid for dx <= 0.1 and |xc| >= 2, where the omitted term is below
+// 2.5e-9 of the envelope 1/(2 pi^2 xc^2).
 template <bool kMixed>
-__device__ __forceinline__ double line_bin_value(double E_r, double a, double w, int b, const LineWindow &lw,
-                                                 const BinAxis &ax, int K_far, EdgeCache &ec) {
-    EdgeCache lo_e;
-    if (ec.valid && ec.x == a * (ax.edges[b] - E_r) / kPi) {
-        lo_e = ec;
+__device__ __forceinline__ double sincsq_midpoint_mean(double xc, double dx) {
+    using R = typename std::conditional<kMixed, float, double>::type;
+    // sin(pi xc), cos(pi xc) from the argument reduced to [-1, 1] in double.
+    R sp, cp;
+    if constexpr (kMixed) {
+        // Reduce to [-1, 1] exactly in double before the float argument.
+        const double red = xc - 2.0 * rint(0.5 * xc);
+        __sincosf((float)(kPi * red), &sp, &cp);
     } else {
-        lo_e.valid = true;
-        lo_e.x = a * (ax.edges[b] - E_r) / kPi;
-        lo_e.has_r = lo_e.has_q = false;
+        sincospi(xc, &sp, &cp);
     }
-    EdgeCache hi_e;
-    hi_e.valid = true;
-    hi_e.x = a * (ax.edges[b + 1] - E_r) / kPi;
-    hi_e.has_r = hi_e.has_q = false;
+    const R om = (R)(2.0 * kPi);
+    const R a0 = (R)2 * sp * sp;
+    const R s2 = (R)2 * sp * cp;
+    const R c2 = (cp - sp) * (cp + sp);
+    const R a1 = om * s2, a2 = om * om * c2;
+    const R om3 = om * om * om;
+    const R a3 = -om3 * s2, a4 = -om3 * om * c2;
+    const R a5 = om3 * om * om * s2, a6 = om3 * om3 * c2;
+    R q;
+    if constexpr (kMixed) q = __frcp_rn((float)xc);
+    else q = 1.0 / xc;
+    const R h0 = q * q;
+    const R h1 = (R)-2 * h0 * q;
+    const R h2 = (R)-3 * h1 * q;
+    const R h3 = (R)-4 * h2 * q;
+    const R h4 = (R)-5 * h3 * q;
+    const R h5 = (R)-6 * h4 * q;
+    const R h6 = (R)-7 * h5 * q;
+    const R f0 = a0 * h0;
+    const R f2 = a2 * h0 + (R)2 * a1 * h1 + a0 * h2;
+    const R f4 = a4 * h0 + (R)4 * a3 * h1 + (R)6 * a2 * h2 + (R)4 * a1 * h3 + a0 * h4;
+    const R f6 = a6 * h0 + (R)6 * a5 * h1 + (R)15 * a4 * h2 + (R)20 * a3 * h3 + (R)15 * a2 * h4 +
+                 (R)6 * a1 * h5 + a0 * h6;
+    const R d2 = (R)(dx * dx);
+    const R series = f0 + d2 * (f2 * (R)(1.0 / 24.0) + d2 * (f4 * (R)(1.0 / 1920.0) + d2 * (f6 * (R)(1.0 / 322560.0))));
+    return (double)series * kInv2Pi2;
+}
+
+// Per-line constants of the deposit: s = a / pi converts energy to
+// first-zero units and scale = w pi / a turns a bin's mass into its weighted
+// mean; both are formed once per line, so a bin on a uniform axis costs no
+// FP64 division beyond the far-envelope reciprocal.
+struct LineDep {
+    double E_r, s, scale;
+};
+
+// The far envelope this line's moments already spread onto bin b (more than
+// K_far bins from the centre), which the exact window takes back out:
+// w / (2 a^2) / ((E_lo - E_r)(E_hi - E_r)) = (w / (2 pi^2)) / (x_lo x_hi).
+template <bool kMixed>
+__device__ __forceinline__ double far_correction(const LineDep &L, int b, const LineWindow &lw, const BinAxis &ax,
+                                                 int K_far, double e0, double e1) {
+    if (!(lw.mom && (b - lw.c > K_far || lw.c - b > K_far))) return 0.0;
+    const double E_c = centre_of(ax, lw.c);
+    return (L.scale * L.s) * kInv2Pi2 *
+           far_envelope<kMixed>(L.s * (e0 - E_c), L.s * (e1 - E_c), L.s * (L.E_r - E_c));
+}
+
+// Exact-window classes of a bin. The cheap ones are evaluated where they are
+// found; the others are queued so that a warp evaluates one kind at a time.
+enum BinClass { kBinDone = 0, kBinExact = 1, kBinExactCf = 2 };
+
+// Evaluates bin b of a line when it is cheap: the midpoint series for a bin
+// much narrower than the line, the far closed form when both edges lie past
+// the asymptotic threshold on one side (ec carries the shared edge between
+// consecutive such bins). Otherwise returns the class of exact work it needs:
+// kBinExactCf when an edge falls in the continued-fraction range of Si.
+template <bool kMixed>
+__device__ __forceinline__ int bin_fast(const LineDep &L, int b, const LineWindow &lw, const BinAxis &ax,
+                                        int K_far, EdgeCache &ec, double &v) {
+    const double e0 = ax.edges[b], e1 = ax.edges[b + 1];
+    const double x_lo = L.s * (e0 - L.E_r), x_hi = L.s * (e1 - L.E_r);
+    const double dxw = L.s * (e1 - e0);
+    const double xc = 0.5 * (x_lo + x_hi);
+    if (dxw <= 0.1 && fabs(xc) >= 2.0) {
+        ec.valid = false;
+        v = (L.scale * L.s) * sincsq_midpoint_mean<kMixed>(xc, dxw);
+    } else {
+        constexpr double u_lim = kMixed ? 24.0 : 48.0;
+        const double u_min = 2.0 * kPi * fmin(fabs(x_lo), fabs(x_hi));
+        if (!((x_lo > 0.0 || x_hi < 0.0) && u_min >= u_lim)) {
+            ec.valid = false;
+            const double t_lo = 2.0 * kPi * fabs(x_lo), t_hi = 2.0 * kPi * fabs(x_hi);
+            const bool cf = (t_lo > 13.0 && t_lo < 40.0) || (t_hi > 13.0 && t_hi < 40.0);
+            return cf ? kBinExactCf : kBinExact;
+        }
+        EdgeCache lo_e;
+        if (ec.valid && ec.x == x_lo) {
+            lo_e = ec;
+        } else {
+            lo_e.valid = true;
+            lo_e.x = x_lo;
+            lo_e.has_r = lo_e.has_q = false;
+        }
+        EdgeCache hi_e;
+        hi_e.valid = true;
+        hi_e.x = x_hi;
+        hi_e.has_r = hi_e.has_q = false;
+        const double mass = bin_mass<kMixed>(lo_e, hi_e);
+        ec = hi_e;
+        const double inv_width = ax.uniform ? ax.inv_w : 1.0 / (e1 - e0);
+        v = mass * L.scale * inv_width;
+    }
+    v -= far_correction<kMixed>(L, b, lw, ax, K_far, e0, e1);
+    return kBinDone;
+}
+
+// Bin b of a line by the difference of sinc^2 antiderivatives at its edges.
+template <bool kMixed>
+__device__ __forceinline__ double bin_exact(const LineDep &L, int b, const LineWindow &lw, const BinAxis &ax,
+                                            int K_far) {
+    const double e0 = ax.edges[b], e1 = ax.edges[b + 1];
+    EdgeCache lo_e, hi_e;
+    lo_e.valid = hi_e.valid = true;
+    lo_e.x = L.s * (e0 - L.E_r);
+    hi_e.x = L.s * (e1 - L.E_r);
+    lo_e.has_r = lo_e.has_q = hi_e.has_r = hi_e.has_q = false;
     const double mass = bin_mass<kMixed>(lo_e, hi_e);
-    ec = hi_e;
-    const double width = ax.edges[b + 1] - ax.edges[b];
-    double v = w * (mass * (kPi / a) / width);
-    if (lw.mom && (b - lw.c > K_far || lw.c - b > K_far)) {
-        const double E_c = centre_of(ax, lw.c);
-        v -= w / (2.0 * a * a) * far_envelope(ax.edges[b] - E_c, ax.edges[b + 1] - E_c, E_r - E_c);
-    }
-    return v;
+    const double inv_width = ax.uniform ? ax.inv_w : 1.0 / (e1 - e0);
+    return mass * L.scale * inv_width - far_correction<kMixed>(L, b, lw, ax, K_far, e0, e1);
 }
 
 __device__ __forceinline__ void line_moments(double E_r, double a, double w, const LineWindow &lw,
@@ -663,7 +804,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     int *qC = qB0 + kQueue;
     int *pq = qC + kQueue;                                  // surviving pair ids
     int *scratch = pq + kQueue;                             // warp sums + counters
-    cur = reinterpret_cast<unsigned char *>(scratch + 64);
+    int *xq = scratch + 64;                                 // exact bins: [plain | continued fraction]
+    cur = reinterpret_cast<unsigned char *>(xq + (binmean ? 2 * kXQueue : 0));
     cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
     const bool tab_smem = n_tab <= kMaxTab;
     Real *E_tab_s = reinterpret_cast<Real *>(cur);
@@ -679,6 +821,9 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     float *spec_f = reinterpret_cast<float *>(mom_s + (K_far > 0 ? 3 * n_mom : 0));
     int &q_count = scratch[40];
     int &p_count = scratch[42];
+    int *xq_count = scratch + 44;  // two counters
+    // A queued bin packs (line, bin) as line << 21 | bin.
+    const bool use_xq = n_E < (1 << 21);
 
     const int tid = threadIdx.x;
     const unsigned lane = tid & 31u;
@@ -696,7 +841,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         if (K_far > 0)
             for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
-    if (tid == 0) { q_count = 0; p_count = 0; }
+    if (tid == 0) { q_count = 0; p_count = 0; xq_count[0] = 0; xq_count[1] = 0; }
     const Real *E_tab = tab_smem ? E_tab_s : reinterpret_cast<const Real *>(a.tables.E_tab);
     const Real *delta_tab = tab_smem ? delta_s : reinterpret_cast<const Real *>(a.tables.delta);
     const Real *log_mu = tab_smem ? logmu_s : reinterpret_cast<const Real *>(a.tables.log_mu);
@@ -864,6 +1009,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 qB0[j] = lw.b0;
                 qC[j] = lw.mom ? lw.c : INT_MIN;
                 if (lw.mom) line_moments((double)qE[j], (double)qA[j], (double)qW[j], lw, ax, mom_s);
+                // From here on qW holds the line's mass-to-mean scale w pi / a.
+                qW[j] = (Real)((double)qW[j] * kPi / (double)qA[j]);
             }
             __syncthreads();
             {
@@ -910,8 +1057,35 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                     lw.mom = lw.c != INT_MIN;
                     lw.b0 = qB0[line];
                     const int b = lw.b0 + (item - qStart[line]);
-                    const double v = line_bin_value<kMixed>((double)qE[line], (double)qA[line],
-                                                            (double)qW[line], b, lw, ax, K_far, ec);
+                    const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
+                    double v;
+                    const int cls = bin_fast<kMixed>(L, b, lw, ax, K_far, ec, v);
+                    if (cls != kBinDone) {
+                        const int slot = use_xq ? atomicAdd(&xq_count[cls - 1], 1) : kXQueue;
+                        if (slot < kXQueue) {
+                            xq[(cls - 1) * kXQueue + slot] = (line << 21) | b;
+                            continue;
+                        }
+                        v = bin_exact<kMixed>(L, b, lw, ax, K_far);  // queue full
+                    }
+                    if constexpr (kMixed) atomicAdd(&spec_f[b], (float)v);
+                    else atomicAdd(&spec_s[b], v);
+                }
+            }
+            // Queued exact bins, one class at a time.
+            __syncthreads();
+            for (int cls = 0; cls < 2; ++cls) {
+                const int nx = min(xq_count[cls], kXQueue);
+                for (int k = tid; k < nx; k += blockDim.x) {
+                    const int packed = xq[cls * kXQueue + k];
+                    const int line = packed >> 21;
+                    const int b = packed & ((1 << 21) - 1);
+                    LineWindow lw;
+                    lw.c = qC[line];
+                    lw.mom = lw.c != INT_MIN;
+                    lw.b0 = qB0[line];
+                    const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
+                    const double v = bin_exact<kMixed>(L, b, lw, ax, K_far);
                     if constexpr (kMixed) atomicAdd(&spec_f[b], (float)v);
                     else atomicAdd(&spec_s[b], v);
                 }
@@ -925,7 +1099,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 }
             }
             __syncthreads();
-            if (tid == 0) { q_count = 0; p_count = 0; }
+            if (tid == 0) { q_count = 0; p_count = 0; xq_count[0] = 0; xq_count[1] = 0; }
         }
     }
     flush(d_cur);
@@ -1023,7 +1197,7 @@ static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moment
     if (a.tables.n_tab <= kMaxTab) b += sizeof(Real) * (size_t)a.tables.n_tab * (3 + a.tables.n_mu);
     b += 16;
     if (a.quadrature == PB_QUAD_BINMEAN) {
-        b += (sizeof(double) + sizeof(float)) * (size_t)a.n_E;
+        b += (sizeof(double) + sizeof(float)) * (size_t)a.n_E + sizeof(int) * 2 * kXQueue;
         if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
     }
     return b;
