@@ -755,6 +755,152 @@ __device__ __forceinline__ double bin_exact(const LineDep &L, int b, const LineW
     return mass * L.scale * inv_width - far_correction<kMixed>(L, b, lw, ax, K_far, e0, e1);
 }
 
+// ---- mixed path: the cheap classes entirely in float ----------------------
+// The line's E_r is float on this path already, so first-zero coordinates in
+// float lose nothing further: |x| < ~2^8 in any window keeps ~1e-5 absolute.
+struct EdgeCacheF {
+    bool valid, has_r;
+    float x, q, r;  // q = Q(2 pi |x|) of the far form, r = R(x)
+};
+
+// R(x) = F(x) - sign(x)/2 of sincsq_tail in float:
+// Si(t) - pi/2 = -f(t) cos t - g(t) sin t with t = 2 pi |x| and the rational
+// auxiliary functions of Abramowitz & Stegun 5.2.38-5.2.39 (|error| < 5e-7 for
+// t >= 1); its Maclaurin series below t = 1.
+__device__ __forceinline__ float sincsq_tail_f32(float x) {
+    const float u = fabsf(x);
+    const float red = u - rintf(u);
+    float sp, cp;
+    __sincosf(3.14159265358979324f * red, &sp, &cp);  // sin(pi u) up to sign
+    const float t = 6.28318530717958648f * u;
+    const float t2 = t * t;
+    float si_m;  // Si(t) - pi/2
+    if (t < 1.0f) {
+        si_m = t * (1.0f + t2 * (-1.0f / 18.0f + t2 * (1.0f / 600.0f + t2 * (-1.0f / 35280.0f + t2 * (1.0f / 3265920.0f))))) -
+               1.57079632679489662f;
+    } else {
+        const float f = __fdividef(t2 * (t2 * (t2 * (t2 + 38.027264f) + 265.187033f) + 335.677320f) + 38.102495f,
+                                   (t2 * (t2 * (t2 * (t2 + 40.021433f) + 322.624911f) + 570.236280f) + 157.105423f) * t);
+        const float g = __fdividef(t2 * (t2 * (t2 * (t2 + 42.242855f) + 302.757865f) + 352.018498f) + 21.821899f,
+                                   (t2 * (t2 * (t2 * (t2 + 48.196927f) + 482.485984f) + 1114.978885f) + 449.690326f) * t2);
+        const float sin_t = 2.0f * sp * cp, cos_t = (cp - sp) * (cp + sp);
+        si_m = -f * cos_t - g * sin_t;
+    }
+    const float lobe = u > 0.0f ? __fdividef(sp * sp, 9.86960440108935862f * u) : 0.0f;
+    const float r = si_m * (float)kInvPi - lobe;
+    return x >= 0.0f ? r : -r;
+}
+
+// Q(2 pi |x|) of q_osc_f32 with the phase reduced in float.
+__device__ __forceinline__ float q_osc_x_f32(float x) {
+    const float u = 6.28318530717958648f * fabsf(x);
+    const float inv_u = __frcp_rn(u);
+    const float yf = inv_u * inv_u;
+    const float p1 = yf * (2.0f + yf * (-24.0f + yf * (720.0f + yf * (-40320.0f + yf * 3628800.0f))));
+    const float p2 = 1.0f + yf * (-6.0f + yf * (120.0f + yf * (-5040.0f + yf * 362880.0f)));
+    // sin u, cos u with u = 2 pi |x|: reduce |x| to [-1/2, 1/2] turns.
+    const float ax = fabsf(x);
+    const float red = ax - rintf(ax);
+    float sn, cs;
+    __sincosf(6.28318530717958648f * red, &sn, &cs);
+    return cs * p1 * inv_u - sn * p2 * yf;
+}
+
+// Mean of sinc^2 over a bin of width dx in first-zero units centred on xc
+// (the midpoint series of sincsq_midpoint_mean), in float.
+__device__ __forceinline__ float sincsq_midpoint_mean_f32(float xc, float dx) {
+    const float red = xc - 2.0f * rintf(0.5f * xc);
+    float sp, cp;
+    __sincosf(3.14159265358979324f * red, &sp, &cp);
+    const float om = 6.28318530717958648f;
+    const float a0 = 2.0f * sp * sp;
+    const float s2 = 2.0f * sp * cp;
+    const float c2 = (cp - sp) * (cp + sp);
+    const float a1 = om * s2, a2 = om * om * c2;
+    const float om3 = om * om * om;
+    const float a3 = -om3 * s2, a4 = -om3 * om * c2;
+    const float a5 = om3 * om * om * s2, a6 = om3 * om3 * c2;
+    const float q = __frcp_rn(xc);
+    const float h0 = q * q;
+    const float h1 = -2.0f * h0 * q;
+    const float h2 = -3.0f * h1 * q;
+    const float h3 = -4.0f * h2 * q;
+    const float h4 = -5.0f * h3 * q;
+    const float h5 = -6.0f * h4 * q;
+    const float h6 = -7.0f * h5 * q;
+    const float f0 = a0 * h0;
+    const float f2 = a2 * h0 + 2.0f * a1 * h1 + a0 * h2;
+    const float f4 = a4 * h0 + 4.0f * a3 * h1 + 6.0f * a2 * h2 + 4.0f * a1 * h3 + a0 * h4;
+    const float f6 = a6 * h0 + 6.0f * a5 * h1 + 15.0f * a4 * h2 + 20.0f * a3 * h3 + 15.0f * a2 * h4 +
+                     6.0f * a1 * h5 + a0 * h6;
+    const float d2 = dx * dx;
+    const float series = f0 + d2 * (f2 * (1.0f / 24.0f) + d2 * (f4 * (1.0f / 1920.0f) + d2 * (f6 * (1.0f / 322560.0f))));
+    return series * (float)kInv2Pi2;
+}
+
+// Bin b of a line on the mixed path, every class in float (always returns
+// kBinDone): edges_f is the float copy of the bin edges, c the line's centre
+// bin when its far field goes through the moments (else INT_MIN), E_c that
+// bin's centre.
+__device__ __forceinline__ int bin_fast_f32(float E_r, float s, float scale, int b, int c, float E_c,
+                                            const float *edges_f, bool uniform, float inv_w, int K_far,
+                                            EdgeCacheF &ec, float &v) {
+    const float e0 = edges_f[b], e1 = edges_f[b + 1];
+    const float x_lo = s * (e0 - E_r), x_hi = s * (e1 - E_r);
+    const float dxw = s * (e1 - e0);
+    const float xc = 0.5f * (x_lo + x_hi);
+    const float w = scale * s;
+    if (dxw <= 0.1f && fabsf(xc) >= 2.0f) {
+        ec.valid = false;
+        v = w * sincsq_midpoint_mean_f32(xc, dxw);
+    } else {
+        // Far closed form (u_lim = 24): both edges past 24 / (2 pi) on one side.
+        constexpr float x_lim = (float)(24.0 / (2.0 * kPi));
+        const bool cached = ec.valid && ec.x == x_lo;
+        float mass;
+        if (!((x_lo > 0.0f && x_lo >= x_lim) || (x_hi < 0.0f && -x_hi >= x_lim))) {
+            // Difference of antiderivatives.
+            const float r_lo = (cached && ec.has_r) ? ec.r : sincsq_tail_f32(x_lo);
+            const float r_hi = sincsq_tail_f32(x_hi);
+            ec.valid = true;
+            ec.has_r = true;
+            ec.x = x_hi;
+            ec.r = r_hi;
+            mass = r_hi - r_lo + ((x_lo < 0.0f && x_hi >= 0.0f) ? 1.0f : 0.0f);
+        } else {
+            const float q_lo = (cached && !ec.has_r) ? ec.q : q_osc_x_f32(x_lo);
+            const float q_hi = q_osc_x_f32(x_hi);
+            ec.valid = true;
+            ec.has_r = false;
+            ec.x = x_hi;
+            ec.q = q_hi;
+            const bool pos = x_lo > 0.0f;
+            const float lo = pos ? x_lo : -x_hi;
+            const float hi = pos ? x_hi : -x_lo;
+            const float env = __fdividef((hi - lo) * (float)kInv2Pi2, lo * hi);
+            const float osc = pos ? (q_hi - q_lo) : (q_lo - q_hi);
+            mass = env + osc * (float)kInvPi;
+        }
+        v = mass * scale * (uniform ? inv_w : __frcp_rn(e1 - e0));
+    }
+    if (c != INT_MIN && (b - c > K_far || c - b > K_far)) {
+        const float A = s * (e0 - E_c), B = s * (e1 - E_c), d = s * (E_r - E_c);
+        const float AB = A * B;
+        const float r = __frcp_rn(AB);
+        const float f1 = (A + B) * r * r;
+        const float f2 = (A * A + AB + B * B) * r * r * r;
+        v -= w * (float)kInv2Pi2 * (r + d * (f1 + d * f2));
+    }
+    return kBinDone;
+}
+
+__device__ __forceinline__ void smem_add(float *p, float v) {
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "f"(v) : "memory");
+}
+__device__ __forceinline__ void smem_add(double *p, double v) {
+    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "d"(v) : "memory");
+}
+
 __device__ __forceinline__ void line_moments(double E_r, double a, double w, const LineWindow &lw,
                                              const BinAxis &ax, double *mom) {
     const int slot = lw.c + ax.pad;
@@ -819,6 +965,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     double *mom_s = spec_s + (binmean ? n_E : 0);
     const int n_mom = n_E + 2 * far_pad;
     float *spec_f = reinterpret_cast<float *>(mom_s + (K_far > 0 ? 3 * n_mom : 0));
+    float *edges_f = spec_f + (binmean ? n_E : 0);  // mixed path: float bin edges
     int &q_count = scratch[40];
     int &p_count = scratch[42];
     int *xq_count = scratch + 44;  // two counters
@@ -838,6 +985,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     const Real *dtail = has_dtail ? dtail_s : nullptr;
     if (binmean) {
         for (int j = tid; j < n_E; j += blockDim.x) { spec_s[j] = 0.0; spec_f[j] = 0.0f; }
+        if (kMixed)
+            for (int j = tid; j <= n_E; j += blockDim.x) edges_f[j] = (float)a.edges[j];
         if (K_far > 0)
             for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
@@ -1050,17 +1199,33 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 int line = lo;
                 EdgeCache ec;
                 ec.valid = false;
+                EdgeCacheF ecf;
+                ecf.valid = false;
                 for (int item = i0; item < i1; ++item) {
-                    while (item >= qStart[line + 1]) { ++line; ec.valid = false; }
+                    while (item >= qStart[line + 1]) { ++line; ec.valid = false; ecf.valid = false; }
                     LineWindow lw;
                     lw.c = qC[line];
                     lw.mom = lw.c != INT_MIN;
                     lw.b0 = qB0[line];
                     const int b = lw.b0 + (item - qStart[line]);
-                    const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
+                    int cls;
                     double v;
-                    const int cls = bin_fast<kMixed>(L, b, lw, ax, K_far, ec, v);
+                    if constexpr (kMixed) {
+                        const float s_f = (float)qA[line] * (float)kInvPi;
+                        const float E_c = lw.mom ? (float)centre_of(ax, lw.c) : 0.0f;
+                        float vf;
+                        cls = bin_fast_f32((float)qE[line], s_f, (float)qW[line], b, lw.c, E_c, edges_f, ax.uniform,
+                                           (float)ax.inv_w, K_far, ecf, vf);
+                        if (cls == kBinDone) {
+                            smem_add(&spec_f[b], vf);
+                            continue;
+                        }
+                    } else {
+                        const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
+                        cls = bin_fast<kMixed>(L, b, lw, ax, K_far, ec, v);
+                    }
                     if (cls != kBinDone) {
+                        const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
                         const int slot = use_xq ? atomicAdd(&xq_count[cls - 1], 1) : kXQueue;
                         if (slot < kXQueue) {
                             xq[(cls - 1) * kXQueue + slot] = (line << 21) | b;
@@ -1068,8 +1233,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                         }
                         v = bin_exact<kMixed>(L, b, lw, ax, K_far);  // queue full
                     }
-                    if constexpr (kMixed) atomicAdd(&spec_f[b], (float)v);
-                    else atomicAdd(&spec_s[b], v);
+                    if constexpr (kMixed) smem_add(&spec_f[b], (float)v);
+                    else smem_add(&spec_s[b], v);
                 }
             }
             // Queued exact bins, one class at a time.
@@ -1086,8 +1251,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                     lw.b0 = qB0[line];
                     const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
                     const double v = bin_exact<kMixed>(L, b, lw, ax, K_far);
-                    if constexpr (kMixed) atomicAdd(&spec_f[b], (float)v);
-                    else atomicAdd(&spec_s[b], v);
+                    if constexpr (kMixed) smem_add(&spec_f[b], (float)v);
+                    else smem_add(&spec_s[b], v);
                 }
             }
             if constexpr (kMixed) {
@@ -1198,6 +1363,7 @@ static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moment
     b += 16;
     if (a.quadrature == PB_QUAD_BINMEAN) {
         b += (sizeof(double) + sizeof(float)) * (size_t)a.n_E + sizeof(int) * 2 * kXQueue;
+        if (sizeof(Real) == 4) b += sizeof(float) * ((size_t)a.n_E + 1) + 16;
         if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
     }
     return b;
