@@ -33,7 +33,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "e- histories/s on 1 B200: surrogate+mixed vs plain FP64, at <=1% spectrum error"
 UNIT = "histories/s"
-ALG_FLOPS_PAIR = 300.0   # FP32 census of one (segment, reflection, tile) line; see DESIGN.md
+ALG_FLOPS_PAIR = 300.0   # FP32 census of one (segment, reflection, tile) line: kinematics, amplitudes, escape
 
 
 def workload_config(args, n_dir, n_g, n_bins):
@@ -251,7 +251,7 @@ def main():
             clocks = clk.summary()
         else:
             total_ms, t_tr, t_cxr, t_brem = time_pipeline(case, args, rank, world, torch, dist,
-                                                          max(1, args.steps // 2), 1)
+                                                          max(1, args.steps // 2), args.warmup)
         n_steps = args.steps if precision == "mixed" else max(1, args.steps // 2)
         results[precision] = dict(total_ms=total_ms, n_steps=n_steps, t_tr=t_tr, t_cxr=t_cxr, t_brem=t_brem,
                                   status=case.device_status(), res=case.results())
@@ -305,11 +305,12 @@ def main():
             "max_rel_to_peak": float(np.max(np.abs(a.sum(0) - b.sum(0))) / (n_dir * peak)) if peak > 0 else None,
         }
     # e2e through the public API with host buffers.
-    line["e2e"] = e2e_measure(spec, args, torch, rank)
+    line["e2e"] = e2e_measure(spec, args, torch, rank, world, dist)
     if world > 1:
-        # Final tally exchange: one NCCL all-reduce of the FP64 spectra.
-        t = cases["mixed"].spec_cxr
-        dist.all_reduce(t)
+        # Final tally exchange: one all-reduce per FP64 spectrum / int64 tally.
+        from pyrite_b200.shard import reduce_results
+
+        reduce_results(cases["mixed"].device_results())
         torch.cuda.synchronize()
     if rank == 0 and world == 1 and not args.skip_cpu:
         rate, cores, sample = run_cpu_reference(args)
@@ -320,15 +321,25 @@ def main():
         dist.destroy_process_group()
 
 
-def e2e_measure(spec, args, torch, rank):
-    """Same batches through ``pyrite_b200.simulate_case`` with host buffers."""
+def e2e_measure(spec, args, torch, rank, world, dist):
+    """Same batches through ``pyrite_b200.simulate_case_host`` with host buffers.
+
+    Whole-job rate: every rank runs its own histories; the slowest rank's
+    time sets the rate of all of them.
+    """
     from pyrite_b200.pipeline import simulate_case_host
 
     steps = max(1, args.steps // 2)
-    res = simulate_case_host(spec, args.histories, steps=steps, warmup=1, precision="mixed",
+    res = simulate_case_host(spec, args.histories, steps=steps, warmup=args.warmup, precision="mixed",
                              e_start=10_000_000 + rank * 10_000_000)
-    return {"value": res["histories_per_s"], "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes_per_step"],
-            "d2h_bytes_per_step": res["d2h_bytes_per_step"], "steps": steps}
+    ms = float(res["ms_per_step"])
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return {"value": world * args.histories / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": res["h2d_bytes_per_step"], "d2h_bytes_per_step": res["d2h_bytes_per_step"],
+            "steps": steps, "warmup": args.warmup}
 
 
 if __name__ == "__main__":

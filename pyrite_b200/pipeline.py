@@ -241,6 +241,14 @@ class ScoringCase:
             out["brem"] = self.spec_brem.cpu().numpy() / (4.0 * np.pi) / Ne
         return out
 
+    def device_results(self) -> dict:
+        """The device-resident accumulators (un-normalised), for a cross-rank sum."""
+        out = {"cxr": self.spec_cxr, "fates": self.fates, "exit_E": self.exit_E,
+               "exit_theta": self.exit_theta, "deposit": self.deposit}
+        if self.bargs is not None:
+            out["brem"] = self.spec_brem
+        return out
+
     def reset(self):
         for t in (self.spec_cxr, self.fates, self.exit_E, self.exit_theta, self.deposit):
             t.zero_()

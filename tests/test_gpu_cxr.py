@@ -4,7 +4,7 @@ Pairs: every (segment, reflection) line of the FP64 kernel equals the oracle's
 to 1e-9 relative. Spectra: FP64 node and exact bin-mean agree with the
 reference to 1e-8 of the peak; the far-envelope bin-mean and the mixed
 precision kernel stay within 1e-3 and 1e-2 of the peak respectively (the
-north-star tolerance for mixed precision is 1 % spectrum error).
+accuracy target of the mixed-precision path is 1 % spectrum error).
 """
 
 import numpy as np
