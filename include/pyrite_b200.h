@@ -27,9 +27,11 @@
  *   pb_brem_score     -- mc_brem_spectrum, Bethe-Heitler + Elwert
  *                        src/pyrite/montecarlo/spectrum/brem.py:829.
  *   pb_char_yields    -- the characteristic-line chunk kernel
- *                        src/pyrite/montecarlo/spectrum/_characteristic_chunk_kernel.py:120.
+ *                        src/pyrite/montecarlo/spectrum/_characteristic_chunk_kernel.py:120
+ *                        and _accumulate_line_yields, characteristic.py:837;
+ *   pb_char_spectrum  -- spec += line_yield * profile, characteristic.py:1219.
  *   pb_mlp_*          -- BF16 MLP surrogate of the reflection sum (no
- *                        counterpart in the reference).
+ *                        counterpart in the reference; 6 -> 4x256 SiLU -> 512).
  */
 #ifndef PYRITE_B200_H
 #define PYRITE_B200_H
@@ -263,6 +265,35 @@ typedef struct pb_brem_args {
     unsigned int *status;
 } pb_brem_args;
 
+/* Characteristic lines of one emitting element: per-segment shell
+ * ionisation x cascade response x segment-mean escape transmission, summed
+ * into line yields per direction. Tables are injected by the caller (the
+ * reference's EEDL/EADL-derived inputs of _accumulate_line_yields). */
+typedef struct pb_char_args {
+    int32_t precision;      /* pb_precision: FP64, or MIXED (float escape exponentials) */
+    int32_t n_dir;
+    const double *n_hat;    /* [n_dir*3] */
+    double thickness;       /* single slab [0, thickness] when n_layer == 0 */
+    int32_t n_layer;        /* absorber layers (0: the single slab); <= 8 */
+    const double *z_top;    /* [n_layer] Angstrom */
+    const double *z_bot;    /* [n_layer] */
+    int64_t Ne;             /* segments with elec_id < Ne emit */
+    int64_t n_seg;
+    const double *r_mid, *v_hat, *L, *E_keV;  /* segment list (device) */
+    const int64_t *elec_id;
+    const unsigned long long *n_seg_device;   /* optional: read n_seg on device */
+    double n_atoms;         /* emitting number density, atoms / Angstrom^3 */
+    int32_t n_shell;        /* ionised subshells, <= 40 */
+    const double *shell_E;        /* packed per-shell projectile energies, eV, ascending per shell */
+    const double *shell_sigma;    /* packed ionisation cross sections, cm^2 */
+    const int64_t *shell_offset;  /* [n_shell+1] */
+    int32_t n_line;         /* <= 256 */
+    const double *response; /* [n_shell*n_line] photons per primary vacancy */
+    const double *mu;       /* [max(n_layer,1)*n_line] attenuation at the line energies, 1/Angstrom */
+    double *line_yield;     /* [n_dir*n_line] accumulated (+=), FP64: sum n L sigma_line T_escape */
+    unsigned int *status;
+} pb_char_args;
+
 int pb_abi_version(void);
 const char *pb_last_error(void);
 int pb_device_count(int *count);
@@ -275,6 +306,15 @@ int pb_cxr_score(const pb_cxr_args *args, void *stream);
 
 /* Bethe-Heitler + Elwert track-length bremsstrahlung of a segment list. */
 int pb_brem_score(const pb_brem_args *args, void *stream);
+
+/* Characteristic line yields of a segment list (accumulated). */
+int pb_char_yields(const pb_char_args *args, void *stream);
+
+/* spec[d][b] += sum_j line_yield[d][j] * profiles[j][b]: the yields spread
+ * on the bins by per-eV line profiles (bin-integrated Lorentzians), before
+ * the 1/(4 pi Ne) normalisation. All pointers device, FP64. */
+int pb_char_spectrum(int32_t n_dir, int32_t n_line, int32_t n_E, const double *line_yield,
+                     const double *profiles, double *spec, void *stream);
 
 /* pb_cxr_score without any device allocation, for callers that cannot call
  * cudaMalloc: code running inside an allocator or memory-pool callback, an

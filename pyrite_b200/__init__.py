@@ -7,8 +7,10 @@ and the tables they need. There is no CPU fallback.
 
 from .api import (  # noqa: F401
     BeamSpec,
+    CharacteristicLines,
     LineTables,
     mc_brem_spectrum,
+    mc_characteristic_spectrum,
     mc_cxr_spectrum,
     simulate_trajectories,
 )
@@ -16,10 +18,12 @@ from ._lib import PyriteB200Error, load  # noqa: F401
 
 __all__ = [
     "BeamSpec",
+    "CharacteristicLines",
     "LineTables",
     "PyriteB200Error",
     "load",
     "mc_brem_spectrum",
+    "mc_characteristic_spectrum",
     "mc_cxr_spectrum",
     "simulate_trajectories",
 ]

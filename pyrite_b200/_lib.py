@@ -114,6 +114,16 @@ class PbBremArgs(C.Structure):
     ]
 
 
+class PbCharArgs(C.Structure):
+    _fields_ = [
+        ("precision", _i32), ("n_dir", _i32), ("n_hat", _vp), ("thickness", _f64), ("n_layer", _i32),
+        ("z_top", _vp), ("z_bot", _vp), ("Ne", _i64), ("n_seg", _i64), ("r_mid", _vp), ("v_hat", _vp),
+        ("L", _vp), ("E_keV", _vp), ("elec_id", _vp), ("n_seg_device", _vp), ("n_atoms", _f64),
+        ("n_shell", _i32), ("shell_E", _vp), ("shell_sigma", _vp), ("shell_offset", _vp), ("n_line", _i32),
+        ("response", _vp), ("mu", _vp), ("line_yield", _vp), ("status", _vp),
+    ]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -123,6 +133,8 @@ EXPORTS = (
     "pb_cxr_score",
     "pb_brem_score",
     "pb_cxr_score_noalloc",
+    "pb_char_yields",
+    "pb_char_spectrum",
 )
 
 _lib = None
@@ -150,6 +162,8 @@ def load(path: Path | None = None):
     lib.pb_cxr_score.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_brem_score.argtypes = [C.POINTER(PbBremArgs), _vp]
     lib.pb_cxr_score_noalloc.argtypes = [C.POINTER(PbCxrArgs), _vp]
+    lib.pb_char_yields.argtypes = [C.POINTER(PbCharArgs), _vp]
+    lib.pb_char_spectrum.argtypes = [_i32, _i32, _i32, _vp, _vp, _vp, _vp]
     if path is None:
         _lib = lib
     return lib

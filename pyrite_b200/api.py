@@ -465,3 +465,147 @@ def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu, precision="
     torch.cuda.synchronize(dev)
     out = spec.cpu().numpy() / (4.0 * np.pi) / int(segments["Ne"])
     return out[0] if single else out
+
+
+# ---------------------------------------------------------------------------
+# Characteristic lines (pyrite/montecarlo/spectrum/characteristic.py:1033)
+# ---------------------------------------------------------------------------
+CHARACTERISTIC_TRANSPORT_FLOOR_KEV = 1.0
+
+
+@dataclass
+class CharacteristicLines:
+    """Line data of one emitting element, as the reference derives it from
+    EEDL/EADL/xraydb (``characteristic.py:111-160``): per-shell ionisation
+    tables (projectile energy [eV] ascending, cross section [cm^2]), line
+    energies and natural FWHMs [eV], and ``response[shell, line]``, the
+    photons of each line per primary vacancy in each shell after the cascade.
+    """
+
+    shell_E: tuple
+    shell_sigma: tuple
+    line_E: np.ndarray
+    line_fwhm: np.ndarray
+    response: np.ndarray
+    recommended_cutoff_eV: float = 50.0
+
+
+def characteristic_bin_edges(E_grid_eV):
+    """Edges and widths of the characteristic bins (``characteristic.py:621-646``):
+    midpoints inside, reflected half-widths outside, the low edge clamped at 0."""
+    g = np.asarray(E_grid_eV, dtype=float)
+    if g.ndim != 1 or g.size < 2 or not np.all(np.isfinite(g)) or np.any(np.diff(g) <= 0.0):
+        raise ValueError("characteristic energy-bin centres must be >= 2 finite, strictly increasing values")
+    edges = np.empty(g.size + 1)
+    edges[1:-1] = 0.5 * (g[:-1] + g[1:])
+    edges[0] = max(0.0, g[0] - 0.5 * (g[1] - g[0]))
+    edges[-1] = g[-1] + 0.5 * (g[-1] - g[-2])
+    return edges, np.diff(edges)
+
+
+def lorentzian_bin_weights(edges_eV, line_energy_eV, fwhm_eV):
+    """Exact in-window bin masses of a Lorentzian normalised on all energies
+    (``characteristic.py:649-680``); the tail outside the window is not
+    redistributed."""
+    if not (np.isfinite(fwhm_eV) and fwhm_eV > 0.0 and np.isfinite(line_energy_eV) and line_energy_eV > 0.0):
+        raise ValueError("line energy and FWHM must be finite and positive")
+    gamma = 0.5 * float(fwhm_eV)
+    e = np.asarray(edges_eV, dtype=float)
+    w = (np.arctan((e[1:] - line_energy_eV) / gamma) - np.arctan((e[:-1] - line_energy_eV) / gamma)) / np.pi
+    w = np.maximum(w, 0.0)
+    if not np.all(np.isfinite(w)):
+        raise ValueError("Lorentzian line has no finite mass on the requested energy grid")
+    return w
+
+
+def prepare_characteristic_lines(lines: CharacteristicLines, E_grid_eV, relaxation_cutoff_eV=None):
+    """Kept line indices and their per-eV profiles ``[n_kept, n_bin]``
+    (``_prepare_lines``, ``characteristic.py:935-990``): lines above the
+    relaxation cutoff, fed by some shell, with mass on the grid."""
+    cutoff = lines.recommended_cutoff_eV if relaxation_cutoff_eV is None else float(relaxation_cutoff_eV)
+    if cutoff < lines.recommended_cutoff_eV:
+        raise ValueError(f"relaxation_cutoff_eV={cutoff:g} is below the data's minimum "
+                         f"{lines.recommended_cutoff_eV:g} eV")
+    edges, widths = characteristic_bin_edges(E_grid_eV)
+    response = np.asarray(lines.response, dtype=float)
+    kept, profiles = [], []
+    for j, (E, fwhm) in enumerate(zip(lines.line_E, lines.line_fwhm)):
+        if E <= cutoff or not np.any(response[:, j] > 0.0):
+            continue
+        w = lorentzian_bin_weights(edges, float(E), float(fwhm))
+        if not np.any(w > 0.0):
+            continue
+        kept.append(j)
+        profiles.append(w / widths)
+    return np.asarray(kept, dtype=np.int64), (np.stack(profiles) if profiles else np.zeros((0, widths.size)))
+
+
+def mc_characteristic_spectrum(segments, E_grid_eV, *, lines: CharacteristicLines, n_atoms_per_ang3, n_hat,
+                               mu_by_line, layers=None, relaxation_cutoff_eV=None, E_cut_keV=None,
+                               precision="fp64", device=None, stream=None, return_yields=False):
+    """Characteristic X-ray density [photons/eV/sr/electron] of one emitting element.
+
+    ``mu_by_line[k, j]`` is the attenuation [1/Angstrom] of absorber layer k
+    (one row for the single slab) at line j's energy (the reference reads
+    EPDL, ``characteristic.py:975-985``); ``layers`` is the absorber stack as
+    ``(z_top, z_bot)`` bounds in Angstrom, or None for the slab of
+    ``segments["thickness_ang"]``. Segments are expected above the 1 keV
+    transport floor already (a transport cutoff >= 1 keV makes the
+    reference's clipping the identity).
+    """
+    if E_cut_keV is not None and float(E_cut_keV) < CHARACTERISTIC_TRANSPORT_FLOOR_KEV:
+        raise ValueError("characteristic scoring requires E_cut_keV >= 1 keV")
+    kept, profiles = prepare_characteristic_lines(lines, E_grid_eV, relaxation_cutoff_eV)
+    n_hats = np.atleast_2d(np.asarray(n_hat, dtype=float))
+    n_hats = n_hats / np.linalg.norm(n_hats, axis=1, keepdims=True)
+    single = np.asarray(n_hat).ndim == 1
+    n_dir, n_E = n_hats.shape[0], profiles.shape[1]
+    Ne = int(segments["Ne"])
+    if kept.size == 0:
+        out = np.zeros((n_dir, n_E))
+        return out[0] if single else out
+    dev = _device(device)
+    lib = L.load()
+    h = _Holder(dev)
+    seg = _segments_on_device(h, segments)
+    mu = np.atleast_2d(np.asarray(mu_by_line, dtype=float))[:, kept]
+    n_layer = 0 if layers is None else len(layers)
+    if mu.shape[0] != max(n_layer, 1):
+        raise ValueError("mu_by_line needs one row per absorber layer (one for the slab)")
+    offs = np.cumsum([0] + [int(np.size(e)) for e in lines.shell_E]).astype(np.int64)
+    a = L.PbCharArgs()
+    a.precision = _PREC[precision]
+    a.n_dir = n_dir
+    a.n_hat = _ptr(h.f64(n_hats))
+    a.thickness = float(segments.get("thickness_ang", 0.0) or 0.0)
+    a.n_layer = n_layer
+    if n_layer:
+        a.z_top = _ptr(h.f64([float(l[0]) for l in layers]))
+        a.z_bot = _ptr(h.f64([float(l[1]) for l in layers]))
+    a.Ne = Ne
+    a.n_seg = seg["n"]
+    a.r_mid, a.v_hat, a.L = _ptr(seg["r_mid"]), _ptr(seg["v_hat"]), _ptr(seg["L"])
+    a.E_keV, a.elec_id = _ptr(seg["E"]), _ptr(seg["elec_id"])
+    a.n_atoms = float(n_atoms_per_ang3)
+    a.n_shell = len(lines.shell_E)
+    a.shell_E = _ptr(h.f64(np.concatenate([np.asarray(e, float) for e in lines.shell_E])))
+    a.shell_sigma = _ptr(h.f64(np.concatenate([np.asarray(v, float) for v in lines.shell_sigma])))
+    a.shell_offset = _ptr(h.typed(offs, torch.int64))
+    a.n_line = int(kept.size)
+    a.response = _ptr(h.f64(np.asarray(lines.response, float)[:, kept]))
+    a.mu = _ptr(h.f64(mu))
+    yields = h.zeros((n_dir, int(kept.size)), torch.float64)
+    a.line_yield = _ptr(yields)
+    a.status = _ptr(h.zeros(1, torch.int32))
+    s = _stream_ptr(stream)
+    L.check(lib.pb_char_yields(C.byref(a), s), "pb_char_yields")
+    spec = h.zeros((n_dir, n_E), torch.float64)
+    L.check(lib.pb_char_spectrum(n_dir, int(kept.size), n_E, _ptr(yields), _ptr(h.f64(profiles)), _ptr(spec), s),
+            "pb_char_spectrum")
+    torch.cuda.synchronize(dev)
+    out = spec.cpu().numpy() / (4.0 * np.pi) / Ne
+    out = out[0] if single else out
+    if return_yields:
+        y = yields.cpu().numpy()
+        return out, (y[0] if single else y), kept
+    return out

@@ -147,4 +147,37 @@ int pb_brem_score(const pb_brem_args *a, void *stream) {
     return PB_OK;
 }
 
+int pb_char_yields(const pb_char_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_char_yields: args is NULL");
+    if (a->n_seg < 0 || a->n_dir < 1 || a->n_line < 1 || a->n_shell < 1)
+        return fail(PB_ERR_INVALID, "pb_char_yields: need n_seg >= 0, n_dir >= 1, n_line >= 1, n_shell >= 1");
+    if (a->n_seg == 0) return PB_OK;
+    if (a->n_shell > 40 || a->n_line > 256 || a->n_layer < 0 || a->n_layer > 8)
+        return fail(PB_ERR_UNSUPPORTED, "pb_char_yields: n_shell <= 40, n_line <= 256, 0 <= n_layer <= 8");
+    if ((size_t)a->n_dir * (size_t)a->n_line * sizeof(double) > 200 * 1024)
+        return fail(PB_ERR_UNSUPPORTED, "pb_char_yields: n_dir * n_line above the shared accumulator");
+    if (a->precision != PB_FP64 && a->precision != PB_MIXED)
+        return fail(PB_ERR_INVALID, "pb_char_yields: unknown precision");
+    if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->shell_E ||
+        !a->shell_sigma || !a->shell_offset || !a->response || !a->mu || !a->line_yield)
+        return fail(PB_ERR_INVALID, "pb_char_yields: every table, segment and output pointer must be set");
+    if (a->n_layer > 0 && (!a->z_top || !a->z_bot))
+        return fail(PB_ERR_INVALID, "pb_char_yields: layer bounds missing");
+    if (a->n_layer == 0 && !(a->thickness > 0.0))
+        return fail(PB_ERR_INVALID, "pb_char_yields: single slab needs thickness > 0");
+    cudaError_t e = pb::launch_char(*a, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_char_yields: launch");
+    return PB_OK;
+}
+
+int pb_char_spectrum(int32_t n_dir, int32_t n_line, int32_t n_E, const double *line_yield, const double *profiles,
+                     double *spec, void *stream) {
+    if (n_dir < 1 || n_line < 1 || n_E < 1 || n_dir > 65535)
+        return fail(PB_ERR_INVALID, "pb_char_spectrum: need 1 <= n_dir <= 65535, n_line >= 1, n_E >= 1");
+    if (!line_yield || !profiles || !spec) return fail(PB_ERR_INVALID, "pb_char_spectrum: pointers must be set");
+    cudaError_t e = pb::launch_char_spectrum(n_dir, n_line, n_E, line_yield, profiles, spec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_char_spectrum: launch");
+    return PB_OK;
+}
+
 }  // extern "C"

@@ -534,6 +534,115 @@ def gen_transport_lut():
         )
 
 
+# ---------------------------------------------------------------------------
+# Characteristic lines (pyrite/montecarlo/spectrum/characteristic.py:1033):
+# the EEDL/EADL tables are absent, so a synthetic element table (smooth shell
+# ionisation cross sections on per-shell grids, line energies and widths) and
+# a synthetic cascade response are injected through the module's own seams;
+# the reference's arithmetic turns them into Lorentzian profiles, escape
+# paths, line yields and the spectrum.
+# ---------------------------------------------------------------------------
+CHAR_ELEMENTS = {
+    # binding energies [eV] of the ionised shells; lines (energy, FWHM) [eV]
+    "Si": dict(Z=14, shells=[1839.0, 149.7, 99.8, 99.2],
+               lines=[(1739.98, 0.52), (1739.38, 0.52), (1835.94, 0.60), (91.5, 0.3)]),
+    "W": dict(Z=74, shells=[69525.0, 12100.0, 11544.0, 10207.0, 2820.0, 2575.0],
+              lines=[(59318.2, 43.0), (57981.7, 45.0), (8397.6, 6.2), (8335.2, 6.4), (9672.4, 7.1),
+                     (9961.5, 7.3), (11285.9, 8.4), (2775.0, 3.0), (67244.3, 52.0)]),
+    "C": dict(Z=6, shells=[288.0], lines=[(277.0, 0.2)]),
+}
+
+
+def synthetic_char_table(element):
+    from types import SimpleNamespace
+
+    spec = CHAR_ELEMENTS[element]
+    rng = np.random.default_rng(spec["Z"])
+    grids, sigmas = [], []
+    for i, Eb in enumerate(spec["shells"]):
+        n_pts = 60 + 7 * i
+        E = np.geomspace(Eb, 1.0e9, n_pts)
+        u = E / Eb
+        sig = 1.0e-20 * (spec["Z"] / 14.0) ** -1.5 * (1.0 + 0.3 * i) * np.log(u) / (u + 0.5) * (1.0 + 0.02 * np.sin(3.0 * np.log(u)))
+        sig[0] = 0.0
+        grids.append(E)
+        sigmas.append(sig)
+    lines = np.array([e for e, _ in spec["lines"]])
+    fwhm = np.array([w for _, w in spec["lines"]])
+    response = rng.uniform(0.0, 0.3, size=(len(spec["shells"]), lines.size))
+    response[rng.uniform(size=response.shape) < 0.25] = 0.0
+    return SimpleNamespace(
+        element=element, atomic_number=spec["Z"], recommended_cutoff_eV=50.0,
+        projectile_energy_eV_by_shell=tuple(grids), ionization_cross_sections_cm2_by_shell=tuple(sigmas),
+        ionization_shell_labels=tuple(f"S{i}" for i in range(len(spec["shells"]))),
+        line_energy_eV=lines, cxr_fwhm_eV=fwhm, line_labels=np.array([f"L{i}" for i in range(lines.size)]),
+        _response=response,
+    )
+
+
+def synthetic_char_mu(composition, E):
+    E = np.asarray(E, dtype=float)
+    return 1.0e-4 * synthetic_mu_total(composition, E)
+
+
+def gen_char():
+    from pyrite.montecarlo.spectrum import characteristic as CH
+
+    cases = (
+        # name, transport, element, emitting composition, layers, grid
+        ("si50", "si50mev", "Si", [("Si", 0.04994)], None, np.linspace(1000.0, 60000.0, 2048)),
+        ("stack_w", "stack10mev", "W", [("W", 0.0632)], True, np.linspace(1000.0, 80000.0, 1024)),
+        ("c20", "c20mev", "C", [("C", 0.1133)], None, np.linspace(1000.0, 40000.0, 780)),
+    )
+    saved = (CH.load_characteristic_cross_sections, CH._cascade_line_yields, CH._mu_total_inv_ang)
+    tables = {}
+    try:
+        CH.load_characteristic_cross_sections = lambda el, **kw: tables.setdefault(el, synthetic_char_table(el))
+        CH._cascade_line_yields = lambda table, cutoff: (None, table._response)
+        CH._mu_total_inv_ang = lambda comp, E: synthetic_char_mu(comp, E)
+        for name, tname, el, comp, layered, E_grid in cases:
+            tr = np.load(OUT / f"transport_{tname}.npz")
+            seg = {
+                "r_mid": tr["r_mid"], "v_hat": tr["v_hat"], "L_ang": tr["L_ang"], "E_keV": tr["E_keV"],
+                "E_repr_keV": tr["E_repr_keV"], "elec_id": tr["elec_id"], "layer": tr["layer"],
+                "Ne": int(tr["Ne"]), "thickness_ang": float(tr["z_bot"][-1]),
+            }
+            layers = None
+            if layered:
+                z_top, z_bot = tr["z_top"], tr["z_bot"]
+                layers = []
+                for i in range(z_top.size):
+                    n = int(tr["n_el"][i])
+                    syms = [["C", "Si", "O", "W"][[6, 14, 8, 74].index(int(z))] for z in tr["Z"][i][:n]]
+                    layers.append((float(z_top[i]), float(z_bot[i]), list(zip(syms, [float(x) for x in tr["N"][i][:n]]))))
+                keep = tr["layer"] == z_top.size - 1  # segments of the emitting (last) layer
+                seg = {k: (v[keep] if isinstance(v, np.ndarray) and v.shape[:1] == tr["layer"].shape else v)
+                       for k, v in seg.items()}
+            spec = np.asarray(CH.mc_characteristic_spectrum(seg, E_grid, composition=comp, n_hat=tr["n_hat"],
+                                                            layers=layers))
+            table = tables[el]
+            edges, widths = CH._energy_bin_edges_and_widths(E_grid)
+            prep = CH._prepare_lines(table, comp, layers, edges, widths, 50.0)
+            absorbers = [comp] if layers is None else [c for _a, _b, c in layers]
+            offs = np.cumsum([0] + [g.size for g in table.projectile_energy_eV_by_shell])
+            _save(
+                f"char_{name}", transport=tname, element=el, n_atoms=float(comp[0][1]), E_grid=E_grid,
+                n_hat=tr["n_hat"], thickness=seg["thickness_ang"], Ne=seg["Ne"],
+                layer_z_top=np.array([l[0] for l in layers]) if layers else np.zeros(0),
+                layer_z_bot=np.array([l[1] for l in layers]) if layers else np.zeros(0),
+                seg_mask=(tr["layer"] == tr["z_top"].size - 1) if layered else np.ones(tr["layer"].size, bool),
+                shell_E=np.concatenate(table.projectile_energy_eV_by_shell),
+                shell_sigma=np.concatenate(table.ionization_cross_sections_cm2_by_shell),
+                shell_offset=offs.astype(np.int64), line_E=table.line_energy_eV, line_fwhm=table.cxr_fwhm_eV,
+                response_all=table._response, kept_response=np.asarray(prep.response),
+                mu_by_line=np.asarray(prep.mu_by_line), profiles=np.asarray(prep.profiles),
+                absorber_mu_check=np.stack([synthetic_char_mu(c, table.line_energy_eV) for c in absorbers]),
+                spec=spec,
+            )
+    finally:
+        CH.load_characteristic_cross_sections, CH._cascade_line_yields, CH._mu_total_inv_ang = saved
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
@@ -542,6 +651,7 @@ GENERATORS = {
     "cxr": gen_cxr,
     "brem": gen_brem,
     "cxr_leaves": gen_cxr_leaves,
+    "char": gen_char,
 }
 
 
