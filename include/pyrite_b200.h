@@ -294,6 +294,31 @@ typedef struct pb_char_args {
     unsigned int *status;
 } pb_char_args;
 
+/* One GEMM of the BF16 MLP surrogate on tcgen05:
+ *   D[M x N] = A[M x K] . B[N x K]^T   (bf16 in, FP32 accumulate)
+ * then, per element: x = D + bias[n]; x *= silu'(dsilu_z[m][n]) when set;
+ * out_f32[m][n] = x + beta out_f32[m][n]; h = act ? SiLU(x) : x;
+ * out_bf16[m][n] = h; out_bf16_t[n][m] = h. Every output optional. */
+typedef struct pb_mlp_gemm_args {
+    int32_t M, N, K;          /* K a multiple of 16 */
+    const void *A;            /* bf16 [M][lda], K contiguous */
+    int64_t lda;
+    const void *B;            /* bf16 [N][ldb], K contiguous */
+    int64_t ldb;
+    const float *bias;        /* [N] or NULL */
+    int32_t act;              /* 0 identity, 1 SiLU */
+    const float *dsilu_z;     /* [M][ldz] or NULL */
+    int64_t ldz;
+    float *out_f32;           /* [M][ldc] or NULL */
+    int64_t ldc;
+    float beta;
+    void *out_bf16;           /* bf16 [M][ldh] or NULL */
+    int64_t ldh;
+    void *out_bf16_t;         /* bf16 [N][ldt] or NULL */
+    int64_t ldt;
+    unsigned int *status;     /* PB_DEV_WAIT_TIMEOUT if an MMA wait gave up */
+} pb_mlp_gemm_args;
+
 int pb_abi_version(void);
 const char *pb_last_error(void);
 int pb_device_count(int *count);
@@ -315,6 +340,22 @@ int pb_char_yields(const pb_char_args *args, void *stream);
  * the 1/(4 pi Ne) normalisation. All pointers device, FP64. */
 int pb_char_spectrum(int32_t n_dir, int32_t n_line, int32_t n_E, const double *line_yield,
                      const double *profiles, double *spec, void *stream);
+
+/* Surrogate training: GEMM + fused epilogue (above). */
+int pb_mlp_gemm(const pb_mlp_gemm_args *args, void *stream);
+/* dY = g_scale (Y - t_scale T) (bf16, row-major [rows][cols] and transposed
+ * [cols][ld_t]); *loss += sum (Y - t_scale T)^2. Y FP32 [rows][cols], T bf16 [rows][ldt_in]. */
+int pb_mlp_mse_grad(int32_t rows, int32_t cols, const float *Y, const void *T, int64_t ldt_in, float t_scale,
+                    float g_scale, void *dY, void *dYt, int64_t ld_t, float *loss, void *stream);
+/* out[c] += sum_r X[r][c], X FP32 [rows][ld]. */
+int pb_mlp_colsum(int32_t rows, int32_t cols, const float *X, int64_t ld, float *out, void *stream);
+/* Adam (decoupled weight decay) on n packed FP32 parameters; bc1, bc2 the bias corrections. */
+int pb_mlp_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps,
+                float wd, float bc1, float bc2, void *stream);
+/* W FP32 [rows][cols] -> bf16 [rows][ldb] (zero padded) and, when Wt is set,
+ * bf16 [pad_cols][ldt] transposed. */
+int pb_mlp_pack(int32_t rows, int32_t cols, const float *W, void *Wb, int32_t ldb, void *Wt, int32_t ldt,
+                int32_t pad_cols, void *stream);
 
 /* pb_cxr_score without any device allocation, for callers that cannot call
  * cudaMalloc: code running inside an allocator or memory-pool callback, an

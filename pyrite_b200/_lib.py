@@ -124,6 +124,14 @@ class PbCharArgs(C.Structure):
     ]
 
 
+class PbMlpGemmArgs(C.Structure):
+    _fields_ = [
+        ("M", _i32), ("N", _i32), ("K", _i32), ("A", _vp), ("lda", _i64), ("B", _vp), ("ldb", _i64),
+        ("bias", _vp), ("act", _i32), ("dsilu_z", _vp), ("ldz", _i64), ("out_f32", _vp), ("ldc", _i64),
+        ("beta", C.c_float), ("out_bf16", _vp), ("ldh", _i64), ("out_bf16_t", _vp), ("ldt", _i64), ("status", _vp),
+    ]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -135,6 +143,11 @@ EXPORTS = (
     "pb_cxr_score_noalloc",
     "pb_char_yields",
     "pb_char_spectrum",
+    "pb_mlp_gemm",
+    "pb_mlp_mse_grad",
+    "pb_mlp_colsum",
+    "pb_mlp_adam",
+    "pb_mlp_pack",
 )
 
 _lib = None
@@ -164,6 +177,12 @@ def load(path: Path | None = None):
     lib.pb_cxr_score_noalloc.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_char_yields.argtypes = [C.POINTER(PbCharArgs), _vp]
     lib.pb_char_spectrum.argtypes = [_i32, _i32, _i32, _vp, _vp, _vp, _vp]
+    _f32 = C.c_float
+    lib.pb_mlp_gemm.argtypes = [C.POINTER(PbMlpGemmArgs), _vp]
+    lib.pb_mlp_mse_grad.argtypes = [_i32, _i32, _vp, _vp, _i64, _f32, _f32, _vp, _vp, _i64, _vp, _vp]
+    lib.pb_mlp_colsum.argtypes = [_i32, _i32, _vp, _i64, _vp, _vp]
+    lib.pb_mlp_adam.argtypes = [_i64, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _f32, _f32, _f32, _vp]
+    lib.pb_mlp_pack.argtypes = [_i32, _i32, _vp, _vp, _i32, _vp, _i32, _i32, _vp]
     if path is None:
         _lib = lib
     return lib

@@ -180,4 +180,55 @@ int pb_char_spectrum(int32_t n_dir, int32_t n_line, int32_t n_E, const double *l
     return PB_OK;
 }
 
+int pb_mlp_gemm(const pb_mlp_gemm_args *g, void *stream) {
+    if (!g) return fail(PB_ERR_INVALID, "pb_mlp_gemm: args is NULL");
+    if (g->M < 1 || g->N < 1 || g->K < 16 || g->K % 16 != 0)
+        return fail(PB_ERR_INVALID, "pb_mlp_gemm: need M, N >= 1 and K a positive multiple of 16");
+    if (!g->A || !g->B) return fail(PB_ERR_INVALID, "pb_mlp_gemm: A and B must be set");
+    if (g->lda < g->K || g->ldb < g->K || g->lda % 8 != 0 || g->ldb % 8 != 0 ||
+        ((uintptr_t)g->A & 15u) != 0 || ((uintptr_t)g->B & 15u) != 0)
+        return fail(PB_ERR_INVALID, "pb_mlp_gemm: lda, ldb >= K, multiples of 8, operands 16-byte aligned");
+    if ((g->out_f32 && g->ldc < g->N) || (g->out_bf16 && g->ldh < g->N) || (g->out_bf16_t && g->ldt < g->M) ||
+        (g->dsilu_z && g->ldz < g->N))
+        return fail(PB_ERR_INVALID, "pb_mlp_gemm: an output leading dimension is too small");
+    if (g->act != 0 && g->act != 1) return fail(PB_ERR_INVALID, "pb_mlp_gemm: act is 0 or 1");
+    cudaError_t e = pb::launch_mlp_gemm(*g, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_gemm: launch");
+    return PB_OK;
+}
+
+int pb_mlp_mse_grad(int32_t rows, int32_t cols, const float *Y, const void *T, int64_t ldt_in, float t_scale,
+                    float g_scale, void *dY, void *dYt, int64_t ld_t, float *loss, void *stream) {
+    if (rows < 1 || cols < 1 || !Y || !T || !dY || !dYt || !loss || ldt_in < cols || ld_t < rows)
+        return fail(PB_ERR_INVALID, "pb_mlp_mse_grad: bad sizes or pointers");
+    cudaError_t e = pb::launch_mlp_mse_grad(rows, cols, Y, T, ldt_in, t_scale, g_scale, dY, dYt, ld_t, loss,
+                                            (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_mse_grad: launch");
+    return PB_OK;
+}
+
+int pb_mlp_colsum(int32_t rows, int32_t cols, const float *X, int64_t ld, float *out, void *stream) {
+    if (rows < 1 || cols < 1 || !X || !out || ld < cols) return fail(PB_ERR_INVALID, "pb_mlp_colsum: bad arguments");
+    cudaError_t e = pb::launch_mlp_colsum(rows, cols, X, ld, out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_colsum: launch");
+    return PB_OK;
+}
+
+int pb_mlp_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps,
+                float wd, float bc1, float bc2, void *stream) {
+    if (n < 1 || !p || !g || !m || !v) return fail(PB_ERR_INVALID, "pb_mlp_adam: bad arguments");
+    cudaError_t e = pb::launch_mlp_adam(n, p, g, m, v, lr, b1, b2, eps, wd, bc1, bc2, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_adam: launch");
+    return PB_OK;
+}
+
+int pb_mlp_pack(int32_t rows, int32_t cols, const float *W, void *Wb, int32_t ldb, void *Wt, int32_t ldt,
+                int32_t pad_cols, void *stream) {
+    if (rows < 1 || cols < 1 || !W || !Wb || ldb < cols || (Wt && (ldt < rows || pad_cols < 1 || pad_cols > ldb)))
+        return fail(PB_ERR_INVALID, "pb_mlp_pack: bad arguments");
+    cudaError_t e = pb::launch_mlp_pack(rows, cols, W, Wb, ldb, Wt, ldt, pad_cols, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_pack: launch");
+    return PB_OK;
+}
+
 }  // extern "C"

@@ -17,6 +17,15 @@ cudaError_t launch_char(const pb_char_args &a, cudaStream_t s, int sms);
 cudaError_t launch_char_spectrum(int n_dir, int n_line, int n_E, const double *yield, const double *profiles,
                                  double *spec, cudaStream_t s);
 
+cudaError_t launch_mlp_gemm(const pb_mlp_gemm_args &g, cudaStream_t s);
+cudaError_t launch_mlp_mse_grad(int rows, int cols, const float *Y, const void *T, int64_t ldt_in, float t_scale,
+                                float g_scale, void *dY, void *dYt, int64_t ld_t, float *loss, cudaStream_t s);
+cudaError_t launch_mlp_colsum(int rows, int cols, const float *X, int64_t ld, float *out, cudaStream_t s);
+cudaError_t launch_mlp_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2,
+                            float eps, float wd, float bc1, float bc2, cudaStream_t s);
+cudaError_t launch_mlp_pack(int rows, int cols, const float *W, void *Wb, int ldb, void *Wt, int ldt, int pad_cols,
+                            cudaStream_t s);
+
 // Record the message pb_last_error() returns on this thread.
 void set_last_error(const char *msg);
 
