@@ -34,6 +34,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = "e- histories/s on 1 B200: surrogate+mixed vs plain FP64, at <=1% spectrum error"
 UNIT = "histories/s"
 ALG_FLOPS_PAIR = 300.0   # FP32 census of one (segment, reflection, tile) line: kinematics, amplitudes, escape
+# Surrogate: one (segment, tile) pair through the hidden layers, 2 (6*256 + 3*256*256); the linear
+# output layer is applied once per tile to the length-weighted sums, not per pair.
+ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
+# Bethe-Heitler + Elwert per (segment, tile, energy): ~60 flops of dsigma/dk shared by the 16 tiles plus
+# ~15 of segment-mean escape per tile (transcendental-heavy: the FP32 roofline is a loose bound).
+ALG_FLOPS_BREM = 20.0
+MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"]) \
+    if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
 
 
 def workload_config(args, n_dir, n_g, n_bins):
@@ -171,7 +179,8 @@ def time_pipeline(case, args, rank, world, torch, dist, n_steps, n_warm):
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_steps)]
+    n_ev = 5 if getattr(case, "surrogates", None) else 4
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(n_ev)] for _ in range(n_steps)]
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -184,6 +193,10 @@ def time_pipeline(case, args, rank, world, torch, dist, n_steps, n_warm):
     t_tr = np.mean([e[0].elapsed_time(e[1]) for e in ev])
     t_cxr = np.mean([e[1].elapsed_time(e[2]) for e in ev])
     t_brem = np.mean([e[2].elapsed_time(e[3]) for e in ev])
+    if n_ev == 5:
+        # surrogate arm: split the PXR+CBS part into exact sub-sample and surrogate
+        case.t_split = (float(np.mean([e[1].elapsed_time(e[4]) for e in ev])),
+                        float(np.mean([e[4].elapsed_time(e[2]) for e in ev])))
     if dist is not None:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -202,6 +215,12 @@ def main():
                     help="histories per host process in the CPU baseline (about 4 s each)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--exact-stride", type=int, default=50,
+                    help="exact control-variate sub-sample: every n-th history")
+    ap.add_argument("--train-segments", type=int, default=16384)
+    ap.add_argument("--train-dirs", type=int, default=512)
+    ap.add_argument("--train-epochs", type=int, default=6)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -239,78 +258,144 @@ def main():
     from pyrite_b200.pipeline import ScoringCase
 
     spec = configs.c2_si_50mev(seed=12345)
-    cases = {}
-    results = {}
-    for precision in (["mixed"] if args.skip_fp64 else ["mixed", "fp64"]):
-        case = ScoringCase(spec, precision=precision, rng="philox", lut=True, batch_histories=args.histories)
-        cases[precision] = case
-        if precision == "mixed":
-            with ClockSampler(local) as clk:
-                total_ms, t_tr, t_cxr, t_brem = time_pipeline(case, args, rank, world, torch, dist,
-                                                              args.steps, args.warmup)
-            clocks = clk.summary()
-        else:
-            total_ms, t_tr, t_cxr, t_brem = time_pipeline(case, args, rank, world, torch, dist,
-                                                          max(1, args.steps // 2), args.warmup)
-        n_steps = args.steps if precision == "mixed" else max(1, args.steps // 2)
-        results[precision] = dict(total_ms=total_ms, n_steps=n_steps, t_tr=t_tr, t_cxr=t_cxr, t_brem=t_brem,
-                                  status=case.device_status(), res=case.results())
-    mixed = results["mixed"]
+    H = args.histories
+    cases, results, clocks = {}, {}, {}
+
+    def arm(name, case, n_steps):
+        with ClockSampler(local) as clk:
+            total_ms, t_tr, t_cxr, t_brem = time_pipeline(case, args, rank, world, torch, dist, n_steps, args.warmup)
+        clocks[name] = clk.summary()
+        cases[name] = case
+        results[name] = dict(total_ms=total_ms, n_steps=n_steps, t_tr=t_tr, t_cxr=t_cxr, t_brem=t_brem,
+                             status=case.device_status(), res=case.results())
+
+    # 1. exact mixed precision (FP32 flight and lines, FP64 bookkeeping)
+    arm("mixed", ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H), args.steps)
+    # 2. surrogate + exact control variate on the same histories
+    sur = None
+    if not args.no_surrogate:
+        from pyrite_b200 import surrogate as S
+
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        data = S.make_training_set(spec, n_seg=args.train_segments, n_dir=args.train_dirs,
+                                   dir_chunk=max(1, 2 ** 20 // args.train_segments), seed=1000, device="cuda")
+        model = S.Surrogate("cuda", seed=0)
+        losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5)
+        n_pairs = int(data["X"].shape[0])
+        del data
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        cs = ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H)
+        cs.use_surrogate([model], exact_stride=args.exact_stride)
+        arm("surrogate", cs, args.steps)
+        hyb = cs.surrogate_spectrum()
+        exact_c = (cs.coarse(cases["mixed"].spec_cxr) / cases["mixed"].histories).cpu().numpy()
+        pure = cs._head(cs.sur_hsum, cs.sur_lsum).cpu().numpy() / cs.histories
+
+        def errs(a):
+            per = np.max(np.abs(a - exact_c), axis=1) / np.max(np.abs(exact_c), axis=1)
+            te, ta = exact_c.sum(0), a.sum(0)
+            return float(per.max()), float(np.max(np.abs(ta - te)) / np.max(te))
+
+        e_tile, e_tot = errs(hyb)
+        sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
+               "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
+               "final_mse": losses[-1], "exact_stride": args.exact_stride,
+               "coarse_bins": int(model.n_out),
+               "spectrum_error": {"reference": "exact mixed-precision scorer on the same histories, coarse bins",
+                                  "max_over_tiles_rel_to_tile_peak": e_tile, "detector_total_rel_to_peak": e_tot,
+                                  "surrogate_alone": dict(zip(("max_over_tiles", "detector_total"), errs(pure)))},
+               "gate": 0.01, "passed": bool(e_tile <= 0.01)}
+    if not args.skip_fp64:
+        arm("fp64", ScoringCase(spec, precision="fp64", rng="philox", lut=True, batch_histories=H),
+            max(1, args.steps // 2))
     for name, r in results.items():
-        if not (r["res"]["cxr"].sum() > 0 and r["res"].get("brem", np.ones(1)).sum() > 0):
+        if not (r["res"]["cxr"].sum() > 0 or name == "surrogate") or not r["res"].get("brem", np.ones(1)).sum() > 0:
             raise SystemExit(f"bench: the {name} spectra are empty; refusing to report a rate")
-    ms_per_step = mixed["total_ms"] / mixed["n_steps"]
-    value = world * args.histories / (ms_per_step / 1e3)
-    case = cases["mixed"]
+
+    def rate(name):
+        r = results[name]
+        return world * H / (r["total_ms"] / r["n_steps"] / 1e3), r["total_ms"] / r["n_steps"]
+
+    head = "surrogate" if sur is not None and sur["passed"] else "mixed"
+    value, ms_per_step = rate(head)
+    r_head = results[head]
+    mixed = results["mixed"]
+    ce = cases["mixed"]
     n_seg = mixed["res"]["segments_last_batch"]
-    n_g, n_dir, n_E = int(case.rows.G.shape[0]), case.n_dir, case.n_E
+    n_g, n_dir, n_E = int(ce.rows.G.shape[0]), ce.n_dir, ce.n_E
     pairs = n_seg * n_g * n_dir
-    achieved_tflops = pairs * ALG_FLOPS_PAIR / (mixed["t_cxr"] / 1e3) / 1e12
     peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
+    cxr_tflops = pairs * ALG_FLOPS_PAIR / (mixed["t_cxr"] / 1e3) / 1e12
+    brem_flops = n_seg * n_dir * n_E * ALG_FLOPS_BREM
+    brem_tflops = brem_flops / (r_head["t_brem"] / 1e3) / 1e12
+    rooflines = {
+        "cxr_kernel": {"bound": "fp32", "kernel": "cxr_kernel<float> (exact PXR+CBS lines + bin-mean deposit)",
+                       "achieved": cxr_tflops, "peak": peak_fp32, "unit": "TFLOP/s", "frac": cxr_tflops / peak_fp32,
+                       "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
+                       "traffic": None},
+        "brem_kernel": {"bound": "fp32", "kernel": "brem_kernel<float> (Bethe-Heitler + Elwert, 16 tiles)",
+                        "achieved": brem_tflops, "peak": peak_fp32, "unit": "TFLOP/s",
+                        "frac": brem_tflops / peak_fp32, "peak_source": "nominal FP32 CUDA-core peak",
+                        "traffic": None},
+    }
+    if sur is not None:
+        t_sample, t_inf = cases["surrogate"].t_split
+        inf_pairs = n_seg * n_dir * (1.0 + 1.0 / max(args.exact_stride, 1))
+        inf_tflops = inf_pairs * ALG_FLOPS_INFER / (t_inf / 1e3) / 1e12
+        rooflines["mlp_infer_kernel"] = {
+            "bound": "tensor", "kernel": "mlp_infer_kernel (tcgen05 BF16, 4 hidden layers per segment x tile)",
+            "achieved": inf_tflops, "peak": MEASURED_BF16_SUSTAINED, "unit": "TFLOP/s",
+            "frac": inf_tflops / MEASURED_BF16_SUSTAINED,
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)", "traffic": None}
+        sur["kernel_ms"] = {"transport": r_head["t_tr"] if head == "surrogate" else results["surrogate"]["t_tr"],
+                            "exact_subsample": t_sample, "surrogate_infer": t_inf,
+                            "brem": results["surrogate"]["t_brem"]}
+        sur["value"], sur["ms_per_step"] = rate("surrogate")
+    dominant = max(("brem_kernel", r_head["t_brem"]), ("cxr_kernel" if head == "mixed" else "mlp_infer_kernel",
+                   r_head["t_cxr"] if head == "mixed" else cases["surrogate"].t_split[1]), key=lambda kv: kv[1])[0]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "bf16+f32+f64" if head == "surrogate" else "f32+f64", "data": "synthetic",
+        "variant": "surrogate+mixed" if head == "surrogate" else "mixed (surrogate off or failed its gate)",
         "config": workload_config(args, n_dir, n_g, n_E),
         "segments_per_s": world * n_seg / (ms_per_step / 1e3),
-        "pairs_per_s": world * pairs / (ms_per_step / 1e3),
-        "kernel_ms": {"transport": mixed["t_tr"], "cxr": mixed["t_cxr"], "brem": mixed["t_brem"]},
-        "device_status": mixed["status"],
-        "spectrum_check": {
-            "cxr_integral": float(mixed["res"]["cxr"].sum()),
-            "brem_integral": float(mixed["res"]["brem"].sum()) if "brem" in mixed["res"] else None,
-            "fates": [int(v) for v in mixed["res"]["fates"]],
-        },
-        "roofline": {
-            "bound": "fp32", "kernel": "cxr_kernel<float> (PXR+CBS lines + bin-mean deposit)",
-            "achieved": achieved_tflops, "peak": peak_fp32, "unit": "TFLOP/s",
-            "frac": achieved_tflops / peak_fp32,
-            "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz); "
-                           "MEASURED_PEAKS.json has HBM and bf16 tensor figures only",
-            "traffic": None,
-        },
-        "gpu_launches": case.kernel_launches_per_batch() * args.steps,
-        "clocks": clocks,
+        "kernel_ms": {"transport": r_head["t_tr"], "cxr": r_head["t_cxr"], "brem": r_head["t_brem"]},
+        "device_status": r_head["status"],
+        "roofline": dict(rooflines[dominant], dominant_in_step=True),
+        "rooflines": rooflines,
+        "gpu_launches": cases[head].kernel_launches_per_batch() * args.steps,
+        "clocks": clocks[head],
+        "surrogate": sur,
+        "mixed_exact": {"value": rate("mixed")[0], "ms_per_step": rate("mixed")[1], "pairs_per_s": world * pairs /
+                        (rate("mixed")[1] / 1e3), "kernel_ms": {"transport": mixed["t_tr"], "cxr": mixed["t_cxr"],
+                                                                 "brem": mixed["t_brem"]},
+                        "spectrum_check": {"cxr_integral": float(mixed["res"]["cxr"].sum()),
+                                           "brem_integral": float(mixed["res"]["brem"].sum()),
+                                           "fates": [int(v) for v in mixed["res"]["fates"]]}},
     }
     if "fp64" in results:
         f = results["fp64"]
-        fp64_ms = f["total_ms"] / f["n_steps"]
-        line["fp64"] = {"value": world * args.histories / (fp64_ms / 1e3), "ms_per_step": fp64_ms,
+        fp64_value, fp64_ms = rate("fp64")
+        line["fp64"] = {"value": fp64_value, "ms_per_step": fp64_ms,
                         "kernel_ms": {"transport": f["t_tr"], "cxr": f["t_cxr"], "brem": f["t_brem"]}}
-        line["speedup_vs_fp64"] = line["value"] / line["fp64"]["value"]
+        line["speedup_vs_fp64"] = value / fp64_value
         a, b = mixed["res"]["cxr"], f["res"]["cxr"]
-        peak = np.max(np.abs(b))
-        line["spectrum_error_vs_fp64"] = {
-            "note": "different history batches; statistical comparison of the tile-summed CXR spectra",
-            "max_rel_to_peak": float(np.max(np.abs(a.sum(0) - b.sum(0))) / (n_dir * peak)) if peak > 0 else None,
+        peak = np.max(np.abs(b.sum(0)))
+        line["mixed_exact"]["spectrum_error_vs_fp64"] = {
+            "note": "different history batches (statistical): tile-summed exact CXR spectra, mixed vs FP64",
+            "max_rel_to_peak": float(np.max(np.abs(a.sum(0) - b.sum(0))) / peak) if peak > 0 else None,
         }
     # e2e through the public API with host buffers.
-    line["e2e"] = e2e_measure(spec, args, torch, rank, world, dist)
+    line["e2e"] = e2e_measure(spec, args, torch, rank, world, dist,
+                              surrogates=cases["surrogate"].surrogates if head == "surrogate" else None)
     if world > 1:
         # Final tally exchange: one all-reduce per FP64 spectrum / int64 tally.
         from pyrite_b200.shard import reduce_results
 
-        reduce_results(cases["mixed"].device_results())
+        reduce_results(cases[head].device_results())
         torch.cuda.synchronize()
     if rank == 0 and world == 1 and not args.skip_cpu:
         rate, cores, sample = run_cpu_reference(args)
@@ -321,7 +406,7 @@ def main():
         dist.destroy_process_group()
 
 
-def e2e_measure(spec, args, torch, rank, world, dist):
+def e2e_measure(spec, args, torch, rank, world, dist, surrogates=None):
     """Same batches through ``pyrite_b200.simulate_case_host`` with host buffers.
 
     Whole-job rate: every rank runs its own histories; the slowest rank's
@@ -331,7 +416,8 @@ def e2e_measure(spec, args, torch, rank, world, dist):
 
     steps = max(1, args.steps // 2)
     res = simulate_case_host(spec, args.histories, steps=steps, warmup=args.warmup, precision="mixed",
-                             e_start=10_000_000 + rank * 10_000_000)
+                             e_start=10_000_000 + rank * 10_000_000, surrogates=surrogates,
+                             exact_stride=args.exact_stride)
     ms = float(res["ms_per_step"])
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)

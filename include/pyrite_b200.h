@@ -243,6 +243,9 @@ typedef struct pb_cxr_args {
     double *pair_w;
     uint8_t *pair_good;
     unsigned int *status;
+    /* Optional, with the line buffer: segment index of every kept line
+     * (surrogate training targets are binned per (segment, direction)). */
+    int64_t *line_seg;
 } pb_cxr_args;
 
 typedef struct pb_brem_args {
@@ -319,6 +322,33 @@ typedef struct pb_mlp_gemm_args {
     unsigned int *status;     /* PB_DEV_WAIT_TIMEOUT if an MMA wait gave up */
 } pb_mlp_gemm_args;
 
+/* Surrogate inference: per (segment, direction) features
+ *   x = (2 (ln E_MeV - ln E_lo)/(ln E_hi - ln E_lo) - 1, v.e_x / theta_max,
+ *        v.e_y / theta_max, 2 clamp(z / thickness, 0, 1) - 1, u_d, v_d)
+ * through 4 hidden layers of 256 SiLU units (bf16 weights, FP32 accumulate
+ * on tcgen05); accumulates hsum[d][256] += L h4 and lsum[d] += L over the
+ * segments with elec_id < Ne. The linear output layer is applied afterwards
+ * by pb_mlp_head. Weights are pre-packed by pb_mlp_pack_umma. */
+typedef struct pb_mlp_infer_args {
+    int32_t n_dir;
+    const float *dir_uv;      /* [n_dir][2] detector coordinates of each direction in [-1, 1] */
+    double e_x[3], e_y[3];    /* transverse beam axes */
+    double theta_max;         /* angle scale, rad */
+    double E_lo_MeV, E_hi_MeV;
+    double thickness;         /* Angstrom */
+    int64_t Ne;
+    int64_t n_seg;
+    const double *r_mid, *v_hat, *L, *E_keV;
+    const int64_t *elec_id;
+    const unsigned long long *n_seg_device;
+    const void *w1_packed;    /* pb_mlp_pack_umma(W1 [256][6..16], kc = 16): 8 KB */
+    const void *w_packed[3];  /* pb_mlp_pack_umma(W2..W4 [256][256], kc = 64): 128 KB each */
+    const float *bias[4];     /* b1..b4 [256] */
+    double *hsum;             /* [n_dir][256] accumulated */
+    double *lsum;             /* [n_dir] accumulated */
+    unsigned int *status;
+} pb_mlp_infer_args;
+
 int pb_abi_version(void);
 const char *pb_last_error(void);
 int pb_device_count(int *count);
@@ -347,6 +377,13 @@ int pb_mlp_gemm(const pb_mlp_gemm_args *args, void *stream);
  * [cols][ld_t]); *loss += sum (Y - t_scale T)^2. Y FP32 [rows][cols], T bf16 [rows][ldt_in]. */
 int pb_mlp_mse_grad(int32_t rows, int32_t cols, const float *Y, const void *T, int64_t ldt_in, float t_scale,
                     float g_scale, void *dY, void *dYt, int64_t ld_t, float *loss, void *stream);
+/* Group-aggregate loss gradient: rows in groups of S with normalised weights
+ * w; per group and column A_hat = sum_s w_s Y_s, A = t_scale sum_s w_s T_s,
+ * d = A_hat - A; *loss += sum d^2; dY_s = g_scale w_s d (bf16, row-major and
+ * transposed [cols][ld_t]). */
+int pb_mlp_group_mse_grad(int32_t groups, int32_t S, int32_t cols, const float *Y, const void *T, int64_t ldt_in,
+                          const float *w, float t_scale, float g_scale, void *dY, void *dYt, int64_t ld_t,
+                          float *loss, void *stream);
 /* out[c] += sum_r X[r][c], X FP32 [rows][ld]. */
 int pb_mlp_colsum(int32_t rows, int32_t cols, const float *X, int64_t ld, float *out, void *stream);
 /* Adam (decoupled weight decay) on n packed FP32 parameters; bc1, bc2 the bias corrections. */
@@ -356,6 +393,34 @@ int pb_mlp_adam(int64_t n, float *p, const float *g, float *m, float *v, float l
  * bf16 [pad_cols][ldt] transposed. */
 int pb_mlp_pack(int32_t rows, int32_t cols, const float *W, void *Wb, int32_t ldb, void *Wt, int32_t ldt,
                 int32_t pad_cols, void *stream);
+
+/* Copy the segments of every stride-th history (elec_id % stride == 0) from
+ * src into dst (dst->count zeroed by the call, then the number copied; beyond
+ * dst->capacity the status word gets PB_DEV_QUEUE_OVERFLOW). src->count is
+ * read on the device. */
+int pb_segments_sample(const pb_segments *src, int64_t stride, const pb_segments *dst, unsigned int *status,
+                       void *stream);
+
+/* Surrogate inference (above). */
+int pb_mlp_infer(const pb_mlp_infer_args *args, void *stream);
+/* The inference kernel's inputs as a matrix, for training: X bf16
+ * [n_dir * n_seg][16] (row d * n_seg + s) and weight [n_dir * n_seg]. */
+int pb_mlp_features(const pb_mlp_infer_args *args, void *X, float *weight, void *stream);
+/* spec[d][o] += t_scale (W5[o] . hsum[d] + b5[o] lsum[d]); W5 FP32 [n_out][256]. */
+int pb_mlp_head(int32_t n_dir, int32_t n_out, const float *W5, const float *b5, const double *hsum,
+                const double *lsum, double t_scale, double *spec, void *stream);
+/* W FP32 [256][cols] -> bf16 chunks of kc (16 or 64) columns in the
+ * interleaved core-matrix layout the inference kernel streams. */
+int pb_mlp_pack_umma(int32_t cols, int32_t kc, const float *W, void *out, void *stream);
+
+/* Bin a line buffer per (segment, direction) pair onto a uniform coarse
+ * grid: target[(line_dir - dir0) * n_seg + line_seg][b] += w (pi / a) m_b /
+ * width, m_b the line's exact sinc^2 mass in bin b (float antiderivatives,
+ * bins within 64 first-zero widths and 64 bins of the centre). Lines whose
+ * direction falls outside [dir0, dir0 + n_dir_chunk) are skipped. */
+int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a, const double *line_w,
+                     const int32_t *line_dir, const int64_t *line_seg, int32_t dir0, int32_t n_dir_chunk,
+                     int64_t n_seg, double lo_eV, double width_eV, int32_t n_bins, float *target, void *stream);
 
 /* pb_cxr_score without any device allocation, for callers that cannot call
  * cudaMalloc: code running inside an allocator or memory-pool callback, an

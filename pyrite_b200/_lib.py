@@ -101,7 +101,7 @@ class PbCxrArgs(C.Structure):
         ("exact_widths", _f64), ("far_pad", _i32), ("spec", _vp), ("far_moments", _vp),
         ("line_capacity", _i64), ("line_count", _vp), ("line_E", _vp), ("line_a", _vp),
         ("line_w", _vp), ("line_dir", _vp), ("pair_E", _vp), ("pair_a", _vp), ("pair_w", _vp),
-        ("pair_good", _vp), ("status", _vp),
+        ("pair_good", _vp), ("status", _vp), ("line_seg", _vp),
     ]
 
 
@@ -132,6 +132,16 @@ class PbMlpGemmArgs(C.Structure):
     ]
 
 
+class PbMlpInferArgs(C.Structure):
+    _fields_ = [
+        ("n_dir", _i32), ("dir_uv", _vp), ("e_x", _f64 * 3), ("e_y", _f64 * 3), ("theta_max", _f64),
+        ("E_lo_MeV", _f64), ("E_hi_MeV", _f64), ("thickness", _f64), ("Ne", _i64), ("n_seg", _i64),
+        ("r_mid", _vp), ("v_hat", _vp), ("L", _vp), ("E_keV", _vp), ("elec_id", _vp), ("n_seg_device", _vp),
+        ("w1_packed", _vp), ("w_packed", _vp * 3), ("bias", _vp * 4), ("hsum", _vp), ("lsum", _vp),
+        ("status", _vp),
+    ]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -145,9 +155,16 @@ EXPORTS = (
     "pb_char_spectrum",
     "pb_mlp_gemm",
     "pb_mlp_mse_grad",
+    "pb_mlp_group_mse_grad",
     "pb_mlp_colsum",
     "pb_mlp_adam",
     "pb_mlp_pack",
+    "pb_mlp_infer",
+    "pb_segments_sample",
+    "pb_mlp_head",
+    "pb_mlp_pack_umma",
+    "pb_mlp_features",
+    "pb_cxr_bin_lines",
 )
 
 _lib = None
@@ -181,8 +198,15 @@ def load(path: Path | None = None):
     lib.pb_mlp_gemm.argtypes = [C.POINTER(PbMlpGemmArgs), _vp]
     lib.pb_mlp_mse_grad.argtypes = [_i32, _i32, _vp, _vp, _i64, _f32, _f32, _vp, _vp, _i64, _vp, _vp]
     lib.pb_mlp_colsum.argtypes = [_i32, _i32, _vp, _i64, _vp, _vp]
+    lib.pb_mlp_group_mse_grad.argtypes = [_i32, _i32, _i32, _vp, _vp, _i64, _vp, _f32, _f32, _vp, _vp, _i64, _vp, _vp]
     lib.pb_mlp_adam.argtypes = [_i64, _vp, _vp, _vp, _vp, _f32, _f32, _f32, _f32, _f32, _f32, _f32, _vp]
     lib.pb_mlp_pack.argtypes = [_i32, _i32, _vp, _vp, _i32, _vp, _i32, _i32, _vp]
+    lib.pb_mlp_infer.argtypes = [C.POINTER(PbMlpInferArgs), _vp]
+    lib.pb_segments_sample.argtypes = [C.POINTER(PbSegments), _i64, C.POINTER(PbSegments), _vp, _vp]
+    lib.pb_mlp_features.argtypes = [C.POINTER(PbMlpInferArgs), _vp, _vp, _vp]
+    lib.pb_mlp_head.argtypes = [_i32, _i32, _vp, _vp, _vp, _vp, _f64, _vp, _vp]
+    lib.pb_mlp_pack_umma.argtypes = [_i32, _i32, _vp, _vp, _vp]
+    lib.pb_cxr_bin_lines.argtypes = [_i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _f64, _f64, _i32, _vp, _vp]
     if path is None:
         _lib = lib
     return lib

@@ -67,4 +67,5 @@ def c2_si_50mev(seed=0, angular_shape=(4, 4), n_bins=2048):
         crystal=SILICON, hkl_list=hkl, n_hats=n_hats, E_grid=E_grid,
         line_tables=P.line_tables(SILICON, hkl, E_grid, comp), surface_hkl=(2, 2, 0),
         brem_composition=comp, brem_mu=P.mu_total(comp, E_grid), seed=seed,
+        detector=det, angular_shape=tuple(angular_shape),
     )

@@ -207,6 +207,18 @@ int pb_mlp_mse_grad(int32_t rows, int32_t cols, const float *Y, const void *T, i
     return PB_OK;
 }
 
+int pb_mlp_group_mse_grad(int32_t groups, int32_t S, int32_t cols, const float *Y, const void *T, int64_t ldt_in,
+                          const float *w, float t_scale, float g_scale, void *dY, void *dYt, int64_t ld_t,
+                          float *loss, void *stream) {
+    if (groups < 1 || groups > 65535 || S < 1 || cols < 1 || !Y || !T || !w || !dY || !dYt || !loss ||
+        ldt_in < cols || ld_t < (int64_t)groups * S)
+        return fail(PB_ERR_INVALID, "pb_mlp_group_mse_grad: bad sizes or pointers");
+    cudaError_t e = pb::launch_mlp_group_mse_grad(groups, S, cols, Y, T, ldt_in, w, t_scale, g_scale, dY, dYt, ld_t,
+                                                  loss, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_group_mse_grad: launch");
+    return PB_OK;
+}
+
 int pb_mlp_colsum(int32_t rows, int32_t cols, const float *X, int64_t ld, float *out, void *stream) {
     if (rows < 1 || cols < 1 || !X || !out || ld < cols) return fail(PB_ERR_INVALID, "pb_mlp_colsum: bad arguments");
     cudaError_t e = pb::launch_mlp_colsum(rows, cols, X, ld, out, (cudaStream_t)stream);
@@ -228,6 +240,75 @@ int pb_mlp_pack(int32_t rows, int32_t cols, const float *W, void *Wb, int32_t ld
         return fail(PB_ERR_INVALID, "pb_mlp_pack: bad arguments");
     cudaError_t e = pb::launch_mlp_pack(rows, cols, W, Wb, ldb, Wt, ldt, pad_cols, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_pack: launch");
+    return PB_OK;
+}
+
+int pb_segments_sample(const pb_segments *src, int64_t stride, const pb_segments *dst, unsigned int *status,
+                       void *stream) {
+    if (!src || !dst || stride < 1) return fail(PB_ERR_INVALID, "pb_segments_sample: need src, dst, stride >= 1");
+    if (!src->count || !src->r_mid || !src->v_hat || !src->L || !src->E_repr || !src->elec_id || !dst->count ||
+        !dst->r_mid || !dst->v_hat || !dst->L || !dst->E_repr || !dst->elec_id || src->capacity < 0 ||
+        dst->capacity < 0)
+        return fail(PB_ERR_INVALID, "pb_segments_sample: segment arrays must be set");
+    cudaError_t e = pb::launch_segments_sample(*src, stride, *dst, status, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_segments_sample: launch");
+    return PB_OK;
+}
+
+int pb_mlp_infer(const pb_mlp_infer_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_mlp_infer: args is NULL");
+    if (a->n_seg < 0 || a->n_dir < 1) return fail(PB_ERR_INVALID, "pb_mlp_infer: need n_seg >= 0, n_dir >= 1");
+    if (a->n_seg == 0) return PB_OK;
+    if (!a->dir_uv || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->w1_packed ||
+        !a->w_packed[0] || !a->w_packed[1] || !a->w_packed[2] || !a->bias[0] || !a->bias[1] || !a->bias[2] ||
+        !a->bias[3] || !a->hsum || !a->lsum)
+        return fail(PB_ERR_INVALID, "pb_mlp_infer: every pointer must be set");
+    if (((uintptr_t)a->w1_packed & 15u) || ((uintptr_t)a->w_packed[0] & 15u) || ((uintptr_t)a->w_packed[1] & 15u) ||
+        ((uintptr_t)a->w_packed[2] & 15u))
+        return fail(PB_ERR_INVALID, "pb_mlp_infer: packed weights must be 16-byte aligned");
+    if (!(a->theta_max > 0.0) || !(a->E_hi_MeV > a->E_lo_MeV) || !(a->E_lo_MeV > 0.0) || !(a->thickness > 0.0))
+        return fail(PB_ERR_INVALID, "pb_mlp_infer: need theta_max > 0, 0 < E_lo < E_hi, thickness > 0");
+    cudaError_t e = pb::launch_mlp_infer(*a, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_infer: launch");
+    return PB_OK;
+}
+
+int pb_mlp_head(int32_t n_dir, int32_t n_out, const float *W5, const float *b5, const double *hsum,
+                const double *lsum, double t_scale, double *spec, void *stream) {
+    if (n_dir < 1 || n_dir > 65535 || n_out < 1 || !W5 || !b5 || !hsum || !lsum || !spec)
+        return fail(PB_ERR_INVALID, "pb_mlp_head: bad arguments");
+    cudaError_t e = pb::launch_mlp_head(n_dir, n_out, W5, b5, hsum, lsum, t_scale, spec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_head: launch");
+    return PB_OK;
+}
+
+int pb_mlp_pack_umma(int32_t cols, int32_t kc, const float *W, void *out, void *stream) {
+    if (cols < 1 || (kc != 16 && kc != 64) || !W || !out) return fail(PB_ERR_INVALID, "pb_mlp_pack_umma: bad arguments");
+    cudaError_t e = pb::launch_mlp_pack_umma(cols, kc, W, out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_pack_umma: launch");
+    return PB_OK;
+}
+
+int pb_mlp_features(const pb_mlp_infer_args *a, void *X, float *weight, void *stream) {
+    if (!a || !X || a->n_seg < 1 || a->n_dir < 1 || !a->dir_uv || !a->r_mid || !a->v_hat || !a->L || !a->E_keV ||
+        !a->elec_id || !(a->theta_max > 0.0) || !(a->E_hi_MeV > a->E_lo_MeV) || !(a->E_lo_MeV > 0.0) ||
+        !(a->thickness > 0.0))
+        return fail(PB_ERR_INVALID, "pb_mlp_features: bad arguments");
+    cudaError_t e = pb::launch_mlp_features(*a, X, weight, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_features: launch");
+    return PB_OK;
+}
+
+int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a, const double *line_w,
+                     const int32_t *line_dir, const int64_t *line_seg, int32_t dir0, int32_t n_dir_chunk,
+                     int64_t n_seg, double lo_eV, double width_eV, int32_t n_bins, float *target, void *stream) {
+    if (n_lines < 0 || n_dir_chunk < 1 || n_seg < 1 || n_bins < 1 || !(width_eV > 0.0))
+        return fail(PB_ERR_INVALID, "pb_cxr_bin_lines: bad sizes");
+    if (n_lines > 0 && (!line_E || !line_a || !line_w || !line_dir || !line_seg || !target))
+        return fail(PB_ERR_INVALID, "pb_cxr_bin_lines: pointers must be set");
+    cudaError_t e = pb::launch_bin_lines(n_lines, line_E, line_a, line_w, line_dir, line_seg, dir0, n_dir_chunk,
+                                         n_seg, lo_eV, width_eV, n_bins, target, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_cxr_bin_lines: launch");
     return PB_OK;
 }
 

@@ -24,6 +24,7 @@
 // PB_FP64 evaluates the chain in double; PB_MIXED in float, with the line
 // phase a (E - E_r) formed and range-reduced in double and every
 // accumulation in double.
+#include <algorithm>
 #include <climits>
 #include <type_traits>
 #include <cstdint>
@@ -906,9 +907,9 @@ __device__ __forceinline__ void line_moments(double E_r, double a, double w, con
     const int slot = lw.c + ax.pad;
     const double m = w / (2.0 * a * a);
     const double dd = E_r - centre_of(ax, lw.c);
-    atomicAdd(&mom[3 * slot + 0], m);
-    atomicAdd(&mom[3 * slot + 1], m * dd);
-    atomicAdd(&mom[3 * slot + 2], m * dd * dd);
+    smem_add(&mom[3 * slot + 0], m);
+    smem_add(&mom[3 * slot + 1], m * dd);
+    smem_add(&mom[3 * slot + 2], m * dd * dd);
 }
 
 // Persistent blocks over the flattened (direction, segment tile) work, in
@@ -925,7 +926,6 @@ template <class Real>
 __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool kMixed = sizeof(Real) == 4;
-    constexpr int kChunk = 4;
     const int n_g = a.tables.n_g;
     const int n_tab = a.tables.n_tab;
     const int n_mu = a.tables.n_mu;
@@ -1125,6 +1125,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                             a.line_a[slot] = (double)ln.a_width;
                             a.line_w[slot] = (double)ln.weight;
                             a.line_dir[slot] = d;
+                            if (a.line_seg) a.line_seg[slot] = s0 + si;
                         } else {
                             set_status(a.status, PB_DEV_QUEUE_OVERFLOW);
                         }
@@ -1187,54 +1188,69 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 __syncthreads();
             }
             const int n_items = qStart[nq];
-            const int n_chunks = (n_items + kChunk - 1) / kChunk;
-            for (int ch = tid; ch < n_chunks; ch += blockDim.x) {
-                const int i0 = ch * kChunk;
-                const int i1 = min(i0 + kChunk, n_items);
-                int lo = 0, hi = nq;  // last line with qStart[line] <= i0
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (qStart[mid] <= i0) lo = mid; else hi = mid;
+            // Each thread walks one contiguous run of (line, bin) items: one
+            // line search per pass, line constants held in registers, and
+            // consecutive bins of a line share their edge evaluations.
+            {
+                const int per = (n_items + (int)blockDim.x - 1) / (int)blockDim.x;
+                const int i_begin = min(tid * per, n_items);
+                const int i_end = min(i_begin + per, n_items);
+                int line = 0;
+                if (i_begin < i_end) {
+                    int lo = 0, hi = nq;  // last line with qStart[line] <= i_begin
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (qStart[mid] <= i_begin) lo = mid; else hi = mid;
+                    }
+                    line = lo - 1;
                 }
-                int line = lo;
+                int next = i_begin, start = 0;
+                LineWindow lw{};
+                LineDep L{};
+                float Er_f = 0.0f, s_f = 0.0f, scale_f = 0.0f, Ec_f = 0.0f;
                 EdgeCache ec;
                 ec.valid = false;
                 EdgeCacheF ecf;
                 ecf.valid = false;
-                for (int item = i0; item < i1; ++item) {
-                    while (item >= qStart[line + 1]) { ++line; ec.valid = false; ecf.valid = false; }
-                    LineWindow lw;
-                    lw.c = qC[line];
-                    lw.mom = lw.c != INT_MIN;
-                    lw.b0 = qB0[line];
-                    const int b = lw.b0 + (item - qStart[line]);
-                    int cls;
-                    double v;
+                for (int item = i_begin; item < i_end; ++item) {
+                    if (item >= next) {
+                        do {
+                            ++line;
+                            next = qStart[line + 1];
+                        } while (item >= next);
+                        start = qStart[line];
+                        lw.c = qC[line];
+                        lw.mom = lw.c != INT_MIN;
+                        lw.b0 = qB0[line];
+                        L = LineDep{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
+                        if constexpr (kMixed) {
+                            Er_f = (float)qE[line];
+                            s_f = (float)qA[line] * (float)kInvPi;
+                            scale_f = (float)qW[line];
+                            Ec_f = lw.mom ? (float)centre_of(ax, lw.c) : 0.0f;
+                        }
+                        ec.valid = false;
+                        ecf.valid = false;
+                    }
+                    const int b = lw.b0 + (item - start);
                     if constexpr (kMixed) {
-                        const float s_f = (float)qA[line] * (float)kInvPi;
-                        const float E_c = lw.mom ? (float)centre_of(ax, lw.c) : 0.0f;
                         float vf;
-                        cls = bin_fast_f32((float)qE[line], s_f, (float)qW[line], b, lw.c, E_c, edges_f, ax.uniform,
-                                           (float)ax.inv_w, K_far, ecf, vf);
-                        if (cls == kBinDone) {
-                            smem_add(&spec_f[b], vf);
-                            continue;
-                        }
+                        bin_fast_f32(Er_f, s_f, scale_f, b, lw.c, Ec_f, edges_f, ax.uniform, (float)ax.inv_w, K_far,
+                                     ecf, vf);
+                        smem_add(&spec_f[b], vf);
                     } else {
-                        const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
-                        cls = bin_fast<kMixed>(L, b, lw, ax, K_far, ec, v);
-                    }
-                    if (cls != kBinDone) {
-                        const LineDep L{(double)qE[line], (double)qA[line] * kInvPi, (double)qW[line]};
-                        const int slot = use_xq ? atomicAdd(&xq_count[cls - 1], 1) : kXQueue;
-                        if (slot < kXQueue) {
-                            xq[(cls - 1) * kXQueue + slot] = (line << 21) | b;
-                            continue;
+                        double v;
+                        const int cls = bin_fast<kMixed>(L, b, lw, ax, K_far, ec, v);
+                        if (cls != kBinDone) {
+                            const int slot = use_xq ? atomicAdd(&xq_count[cls - 1], 1) : kXQueue;
+                            if (slot < kXQueue) {
+                                xq[(cls - 1) * kXQueue + slot] = (line << 21) | b;
+                                continue;
+                            }
+                            v = bin_exact<kMixed>(L, b, lw, ax, K_far);  // queue full
                         }
-                        v = bin_exact<kMixed>(L, b, lw, ax, K_far);  // queue full
+                        smem_add(&spec_s[b], v);
                     }
-                    if constexpr (kMixed) smem_add(&spec_f[b], (float)v);
-                    else smem_add(&spec_s[b], v);
                 }
             }
             // Queued exact bins, one class at a time.
@@ -1421,6 +1437,45 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
 cudaError_t launch_cxr(const pb_cxr_args &a, cudaStream_t s, int sms) {
     if (a.precision == PB_MIXED) return launch_cxr_t<float>(a, s, sms, a.far_pad);
     return launch_cxr_t<double>(a, s, sms, a.far_pad);
+}
+
+// Coarse per-pair binning of a line buffer (surrogate training targets).
+__global__ void bin_lines_kernel(int64_t n_lines, const double *line_E, const double *line_a, const double *line_w,
+                                 const int32_t *line_dir, const int64_t *line_seg, int dir0, int n_dir_chunk,
+                                 int64_t n_seg, double lo, double width, int n_bins, float *target) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_lines;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int dl = line_dir[i] - dir0;
+        if (dl < 0 || dl >= n_dir_chunk) continue;
+        const int64_t pair = (int64_t)dl * n_seg + line_seg[i];
+        const double E_r = line_E[i], a = line_a[i];
+        const float s = (float)(a / kPi);
+        const float scale = (float)(line_w[i] * kPi / a / width);
+        const int c = (int)floor((E_r - lo) / width);
+        int K = (int)ceil(64.0 * kPi / (a * width));
+        K = K < 1 ? 1 : (K > 64 ? 64 : K);
+        const int b0 = max(c - K, 0), b1 = min(c + K, n_bins - 1);
+        float r_lo = 0.0f;
+        for (int b = b0; b <= b1; ++b) {
+            const float x_lo = s * (float)(lo + b * width - E_r);
+            const float x_hi = s * (float)(lo + (b + 1) * width - E_r);
+            if (b == b0) r_lo = sincsq_tail_f32(x_lo);
+            const float r_hi = sincsq_tail_f32(x_hi);
+            const float m = r_hi - r_lo + ((x_lo < 0.0f && x_hi >= 0.0f) ? 1.0f : 0.0f);
+            r_lo = r_hi;
+            if (m != 0.0f) atomicAdd(&target[pair * n_bins + b], scale * m);
+        }
+    }
+}
+
+cudaError_t launch_bin_lines(int64_t n_lines, const double *line_E, const double *line_a, const double *line_w,
+                             const int32_t *line_dir, const int64_t *line_seg, int dir0, int n_dir_chunk,
+                             int64_t n_seg, double lo, double width, int n_bins, float *target, cudaStream_t st) {
+    if (n_lines <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>((n_lines + 255) / 256, 148 * 16);
+    bin_lines_kernel<<<(unsigned)blocks, 256, 0, st>>>(n_lines, line_E, line_a, line_w, line_dir, line_seg, dir0,
+                                                        n_dir_chunk, n_seg, lo, width, n_bins, target);
+    return cudaGetLastError();
 }
 
 }  // namespace pb

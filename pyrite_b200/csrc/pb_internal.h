@@ -26,6 +26,23 @@ cudaError_t launch_mlp_adam(int64_t n, float *p, const float *g, float *m, float
 cudaError_t launch_mlp_pack(int rows, int cols, const float *W, void *Wb, int ldb, void *Wt, int ldt, int pad_cols,
                             cudaStream_t s);
 
+cudaError_t launch_mlp_infer(const pb_mlp_infer_args &a, cudaStream_t s, int sms);
+cudaError_t launch_mlp_head(int n_dir, int n_out, const float *W5, const float *b5, const double *hsum,
+                            const double *lsum, double t_scale, double *spec, cudaStream_t s);
+cudaError_t launch_mlp_pack_umma(int cols, int kc, const float *W, void *out, cudaStream_t s);
+
+cudaError_t launch_bin_lines(int64_t n_lines, const double *line_E, const double *line_a, const double *line_w,
+                             const int32_t *line_dir, const int64_t *line_seg, int dir0, int n_dir_chunk,
+                             int64_t n_seg, double lo, double width, int n_bins, float *target, cudaStream_t st);
+cudaError_t launch_mlp_features(const pb_mlp_infer_args &a, void *X, float *weight, cudaStream_t s);
+
+cudaError_t launch_mlp_group_mse_grad(int groups, int S, int cols, const float *Y, const void *T, int64_t ldt_in,
+                                      const float *w, float t_scale, float g_scale, void *dY, void *dYt, int64_t ld_t,
+                                      float *loss, cudaStream_t s);
+
+cudaError_t launch_segments_sample(const pb_segments &src, int64_t stride, const pb_segments &dst,
+                                   unsigned int *status, cudaStream_t s, int sms);
+
 // Record the message pb_last_error() returns on this thread.
 void set_last_error(const char *msg);
 

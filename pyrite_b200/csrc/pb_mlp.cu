@@ -12,7 +12,8 @@
 // through the status word. The epilogue reads the accumulator with
 // tcgen05.ld (warp w owns rows 32w..32w+31) and applies, in order: bias,
 // multiplication by silu'(z) (backward), storage of the pre-activation in
-// FP32, SiLU, storage in bf16 row-major and/or transposed.
+// FP32, SiLU, storage in bf16 row-major and/or transposed. SiLU is the tanh
+// form of silu_fast, the one the inference kernel evaluates.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -34,7 +35,19 @@ constexpr uint32_t kGemmTileA = kGemmBM * kGemmBK * 2;   // 16 KB
 constexpr uint32_t kGemmTileB = kGemmBN * kGemmBK * 2;   // 32 KB
 constexpr uint32_t kGemmSmem = kGemmStages * (kGemmTileA + kGemmTileB) + 64;
 
-__device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + __expf(-x)); }
+// SiLU as x (1 + tanh(x / 2)) / 2 with the hardware tanh approximation; the
+// training and inference kernels use this same form (and its derivative), so
+// the trained function is the one inference evaluates.
+__device__ __forceinline__ float tanh_fast(float x) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
+    return t;
+}
+__device__ __forceinline__ float silu_fast(float x) { return 0.5f * x * (1.0f + tanh_fast(0.5f * x)); }
+__device__ __forceinline__ float dsilu_fast(float z) {
+    const float t = tanh_fast(0.5f * z);
+    return 0.5f * (1.0f + t) + 0.25f * z * (1.0f - t * t);
+}
 
 // Stage one K chunk of A (128 rows) and B (256 rows) into shared memory;
 // rows or columns outside the matrices are zero-filled.
@@ -157,15 +170,13 @@ __global__ void __launch_bounds__(kGemmThreads) mlp_gemm_kernel(const pb_mlp_gem
                 float x = v[i];
                 if (g.bias) x += g.bias[n];
                 if (g.dsilu_z) {
-                    const float z = g.dsilu_z[(int64_t)m * g.ldz + n];
-                    const float sg = sigmoidf_(z);
-                    x *= sg * (1.0f + z * (1.0f - sg));
+                    x *= dsilu_fast(g.dsilu_z[(int64_t)m * g.ldz + n]);
                 }
                 if (g.out_f32) {
                     float *o = g.out_f32 + (int64_t)m * g.ldc + n;
                     *o = g.beta != 0.0f ? x + g.beta * *o : x;
                 }
-                const float h = g.act == 1 ? x * sigmoidf_(x) : x;
+                const float h = g.act == 1 ? silu_fast(x) : x;
                 if (g.out_bf16) reinterpret_cast<__nv_bfloat16 *>(g.out_bf16)[(int64_t)m * g.ldh + n] = __float2bfloat16_rn(h);
                 if (g.out_bf16_t) reinterpret_cast<__nv_bfloat16 *>(g.out_bf16_t)[(int64_t)n * g.ldt + m] = __float2bfloat16_rn(h);
             }
@@ -204,6 +215,45 @@ __global__ void mse_grad_kernel(int rows, int cols, const float *Y, const __nv_b
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc != 0.0f) atomicAdd(loss, acc);
+}
+
+// Group-aggregate loss: rows come in groups of S (one detector direction and
+// S segments each); with w the rows' normalised weights, per group and output
+//   A_hat = sum_s w_s Y_s,  A = t_scale sum_s w_s T_s,  d = A_hat - A,
+// loss += d^2 and dY_s = g_scale w_s d (bf16, row-major and transposed).
+__global__ void group_mse_grad_kernel(int groups, int S, int cols, const float *Y, const __nv_bfloat16 *T,
+                                      int64_t ldt_in, const float *w, float t_scale, float g_scale, __nv_bfloat16 *dY,
+                                      __nv_bfloat16 *dYt, int64_t ld_t, float *loss) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y;
+    float acc = 0.0f;
+    if (o < cols) {
+        float ah = 0.0f, at = 0.0f;
+        for (int s = 0; s < S; ++s) {
+            const int64_t r = (int64_t)g * S + s;
+            ah += w[r] * Y[r * cols + o];
+            at += w[r] * __bfloat162float(T[r * ldt_in + o]);
+        }
+        const float d = ah - t_scale * at;
+        acc = d * d;
+        for (int s = 0; s < S; ++s) {
+            const int64_t r = (int64_t)g * S + s;
+            const __nv_bfloat16 v = __float2bfloat16_rn(g_scale * w[r] * d);
+            dY[r * cols + o] = v;
+            dYt[(int64_t)o * ld_t + r] = v;
+        }
+    }
+    for (int k = 16; k > 0; k >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, k);
+    if ((threadIdx.x & 31) == 0 && acc != 0.0f) atomicAdd(loss, acc);
+}
+
+cudaError_t launch_mlp_group_mse_grad(int groups, int S, int cols, const float *Y, const void *T, int64_t ldt_in,
+                                      const float *w, float t_scale, float g_scale, void *dY, void *dYt, int64_t ld_t,
+                                      float *loss, cudaStream_t s) {
+    dim3 grid((unsigned)((cols + 127) / 128), (unsigned)groups);
+    group_mse_grad_kernel<<<grid, 128, 0, s>>>(groups, S, cols, Y, (const __nv_bfloat16 *)T, ldt_in, w, t_scale,
+                                               g_scale, (__nv_bfloat16 *)dY, (__nv_bfloat16 *)dYt, ld_t, loss);
+    return cudaGetLastError();
 }
 
 // out[c] += sum_r X[r][c] (FP32).
@@ -272,6 +322,401 @@ cudaError_t launch_mlp_pack(int rows, int cols, const float *W, void *Wb, int ld
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
     pack_weights_kernel<<<blocks, 256, 0, s>>>(rows, cols, W, (__nv_bfloat16 *)Wb, ldb, (__nv_bfloat16 *)Wt, ldt,
                                                pad_cols);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Fused surrogate inference: features -> 4 x (256, SiLU) -> length-weighted
+// per-direction sums of the last hidden layer.
+//
+// The output layer is linear, so for every direction d
+//   sum_s L_s (W5 h4(x_sd) + b5) = W5 (sum_s L_s h4(x_sd)) + b5 sum_s L_s,
+// and the kernel only accumulates hsum[d] = sum_s L_s h4 and lsum[d] =
+// sum_s L_s; mlp_head_kernel applies W5 and b5 once per direction.
+//
+// A persistent block (one per SM, 128 threads, thread = row) walks
+// contiguous (direction, 128-segment tile) work. Per tile: features -> X
+// (128 x 16 bf16) in shared memory; layer 1 is one K=16 MMA against W1 held
+// in shared memory; layers 2-4 stream their weights from global memory (L2)
+// in four 32 KB K-chunks, pre-packed in the interleaved layout so each chunk
+// is one bulk copy, double-buffered against the MMAs. Each epilogue reads the
+// 128 x 256 FP32 accumulator from tensor memory, adds the bias, applies SiLU
+// (x (1 + tanh(x/2)) / 2) and writes bf16 activations back over the layer's
+// input in shared memory; the last one weights each row by its segment
+// length and reduces the tile's rows with a 16-shuffle transpose-reduce
+// into the block's per-direction sum.
+// ---------------------------------------------------------------------------
+constexpr int kInfThreads = 128;
+constexpr uint32_t kInfSboX = 256;    // X: 128 x 16, 2 core matrices along K
+constexpr uint32_t kInfSboH = 4096;   // H: 128 x 256
+constexpr uint32_t kInfSboW = 1024;   // W chunk: 256 x 64
+constexpr uint32_t kInfChunk = 256 * 64 * 2;  // 32 KB
+constexpr uint32_t kInfW1 = 256 * 16 * 2;     // 8 KB
+constexpr uint32_t kInfSmem = kInfW1 + 128 * 16 * 2 + 128 * 256 * 2 + 2 * kInfChunk + 4 * 256 * 4 + 257 * 4 + 128;
+
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// Feature vector of segment s seen from direction d (pb_mlp_infer_args);
+// returns the segment's weight (its length, 0 when it does not count).
+struct FeatureMap {
+    float Ex, Ey, Ez, Fx, Fy, Fz, inv_th, lnElo, inv_lnE, inv_thick;
+    __device__ explicit FeatureMap(const pb_mlp_infer_args &a)
+        : Ex((float)a.e_x[0]), Ey((float)a.e_x[1]), Ez((float)a.e_x[2]), Fx((float)a.e_y[0]),
+          Fy((float)a.e_y[1]), Fz((float)a.e_y[2]), inv_th(1.0f / (float)a.theta_max),
+          lnElo(logf((float)a.E_lo_MeV)), inv_lnE(1.0f / (logf((float)a.E_hi_MeV) - logf((float)a.E_lo_MeV))),
+          inv_thick(1.0f / (float)a.thickness) {}
+    __device__ float operator()(const pb_mlp_infer_args &a, int64_t s, int64_t n_seg, int d, float *x) const {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) x[i] = 0.0f;
+        if (s >= n_seg || a.elec_id[s] >= a.Ne) return 0.0f;
+        const float vx = (float)a.v_hat[3 * s], vy = (float)a.v_hat[3 * s + 1], vz = (float)a.v_hat[3 * s + 2];
+        x[0] = 2.0f * (logf((float)a.E_keV[s] * 1.0e-3f) - lnElo) * inv_lnE - 1.0f;
+        x[1] = (vx * Ex + vy * Ey + vz * Ez) * inv_th;
+        x[2] = (vx * Fx + vy * Fy + vz * Fz) * inv_th;
+        x[3] = 2.0f * fminf(fmaxf((float)a.r_mid[3 * s + 2] * inv_thick, 0.0f), 1.0f) - 1.0f;
+        x[4] = a.dir_uv[2 * d];
+        x[5] = a.dir_uv[2 * d + 1];
+        return (float)a.L[s];
+    }
+};
+
+// Training inputs: X[(d n_seg + s)][16] bf16 (features, zero padded) and
+// weight[d n_seg + s], exactly the inference kernel's rows.
+__global__ void mlp_features_kernel(const pb_mlp_infer_args a, __nv_bfloat16 *X, float *weight) {
+    const FeatureMap fm(a);
+    const int64_t n = (int64_t)a.n_dir * a.n_seg;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int d = (int)(i / a.n_seg);
+        const int64_t s = i - (int64_t)d * a.n_seg;
+        float x[6];
+        const float w = fm(a, s, a.n_seg, d, x);
+        for (int k = 0; k < 16; ++k) X[i * 16 + k] = __float2bfloat16_rn(k < 6 ? x[k] : 0.0f);
+        if (weight) weight[i] = w;
+    }
+}
+
+cudaError_t launch_mlp_features(const pb_mlp_infer_args &a, void *X, float *weight, cudaStream_t s) {
+    const int64_t n = (int64_t)a.n_dir * a.n_seg;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    mlp_features_kernel<<<blocks, 256, 0, s>>>(a, (__nv_bfloat16 *)X, weight);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_infer_args a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sW1 = smem;
+    uint8_t *sX = sW1 + kInfW1;
+    uint8_t *sH = sX + 128 * 16 * 2;
+    uint8_t *sW = sH + 128 * 256 * 2;  // two chunk stages
+    float *sBias = reinterpret_cast<float *>(sW + 2 * kInfChunk);  // [4][256]
+    float *sHsum = sBias + 4 * 256;                                 // [256] + lsum
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sHsum + 257 + 3);  // 8-byte aligned
+    uint64_t *full = bar;        // [2] weight chunk landed
+    uint64_t *empty = bar + 2;   // [2] MMAs of the chunk done
+    uint64_t *mma_done = bar + 4;
+    uint64_t *w1_bar = bar + 5;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 6);
+    volatile int *s_ok = reinterpret_cast<volatile int *>(tslot + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int64_t n_seg = a.n_seg;
+    if (a.n_seg_device && (int64_t)*a.n_seg_device < n_seg) n_seg = (int64_t)*a.n_seg_device;
+    const int64_t n_tiles = (n_seg + 127) / 128;
+    const int64_t n_work = n_tiles * a.n_dir;
+    const int64_t w_begin = n_work * blockIdx.x / gridDim.x;
+    const int64_t w_end = n_work * (blockIdx.x + 1) / gridDim.x;
+
+    if (warp == 0) {
+        umma::tmem_alloc(tslot, 256);
+        umma::tmem_relinquish();
+    }
+    for (int i = tid; i < 4 * 256; i += kInfThreads) sBias[i] = a.bias[i / 256][i % 256];
+    for (int i = tid; i < 257; i += kInfThreads) sHsum[i] = 0.0f;
+    if (tid == 0) {
+        for (int i = 0; i < 6; ++i) mbar_init(&bar[i], 1);
+        *s_ok = 1;
+        mbar_expect_tx(w1_bar, kInfW1);
+        bulk_g2s(sW1, a.w1_packed, kInfW1, w1_bar);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t taddr = *tslot;
+    const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+    const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
+    // Thread 0's pipeline state.
+    uint32_t q_load = 0, q_mma = 0, mma_phase = 0;
+    bool w1_ready = false;
+    const uint8_t *wsrc[3] = {static_cast<const uint8_t *>(a.w_packed[0]), static_cast<const uint8_t *>(a.w_packed[1]),
+                              static_cast<const uint8_t *>(a.w_packed[2])};
+
+    // Issue the bulk copy of chunk q (layer 2 + (q / 4) % 3, K-chunk q % 4).
+    auto load_chunk = [&](uint32_t q) -> bool {
+        const uint32_t s = q & 1u;
+        if (q >= 2 && !mbar_wait(&empty[s], ((q >> 1) - 1u) & 1u)) return false;
+        const uint32_t layer = (q >> 2) % 3u, kc = q & 3u;
+        mbar_expect_tx(&full[s], kInfChunk);
+        bulk_g2s(sW + s * kInfChunk, wsrc[layer] + (size_t)kc * kInfChunk, kInfChunk, &full[s]);
+        return true;
+    };
+    if (tid == 0 && w_begin < w_end) {
+        if (!load_chunk(0)) *s_ok = 0;
+        q_load = 1;
+    }
+
+    const FeatureMap fm(a);
+    int d_cur = -1;
+
+    auto flush = [&](int d) {
+        __syncthreads();
+        if (d >= 0) {
+            for (int i = tid; i < 257; i += kInfThreads) {
+                const float v = sHsum[i];
+                if (v != 0.0f) {
+                    if (i < 256) atomicAdd(&a.hsum[(int64_t)d * 256 + i], (double)v);
+                    else atomicAdd(&a.lsum[d], (double)v);
+                }
+                sHsum[i] = 0.0f;
+            }
+        }
+        __syncthreads();
+    };
+
+    for (int64_t wk = w_begin; wk < w_end; ++wk) {
+        const int d = (int)(wk / n_tiles);
+        const int64_t t = wk - (int64_t)d * n_tiles;
+        if (d != d_cur) {
+            flush(d_cur);
+            d_cur = d;
+        }
+        // ---- features of this thread's row ----
+        const int64_t sidx = t * 128 + tid;
+        float x[6];
+        const float wrow = fm(a, sidx, n_seg, d, x);
+        {
+            uint4 lo = make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
+            *reinterpret_cast<uint4 *>(sX + umma::core_offset((uint32_t)tid, 0u, kInfSboX)) = lo;
+            *reinterpret_cast<uint4 *>(sX + umma::core_offset((uint32_t)tid, 8u, kInfSboX)) =
+                make_uint4(0u, 0u, 0u, 0u);
+        }
+        umma::fence_smem_to_async();
+        __syncthreads();
+        if (!*s_ok) break;
+
+        for (int layer = 0; layer < 4; ++layer) {
+            // ---- MMAs of this layer (thread 0) ----
+            if (tid == 0) {
+                umma::fence_after_sync();
+                bool good = true;
+                if (layer == 0) {
+                    if (!w1_ready) {
+                        good = mbar_wait(w1_bar, 0u);
+                        w1_ready = good;
+                    }
+                    if (good)
+                        umma::mma_bf16(taddr, umma::smem_desc(smem_addr(sX), 128u, kInfSboX),
+                                       umma::smem_desc(smem_addr(sW1), 128u, kInfSboX), idesc, 0u);
+                } else {
+                    for (int kc = 0; kc < 4 && good; ++kc) {
+                        const uint32_t s = q_mma & 1u;
+                        good = mbar_wait(&full[s], (q_mma >> 1) & 1u);
+                        if (!good) break;
+                        const uint32_t w0 = smem_addr(sW + s * kInfChunk);
+                        const uint32_t h0 = smem_addr(sH) + (uint32_t)kc * 1024u;  // K offset 64 = 8 core matrices
+                        for (int ks = 0; ks < 4; ++ks)
+                            umma::mma_bf16(taddr, umma::smem_desc(h0 + ks * 256u, 128u, kInfSboH),
+                                           umma::smem_desc(w0 + ks * 256u, 128u, kInfSboW), idesc,
+                                           (kc > 0 || ks > 0) ? 1u : 0u);
+                        umma::commit(&empty[s]);
+                        ++q_mma;
+                        // Load the next chunk (weights are the same every tile) into
+                        // the stage whose MMAs were issued one chunk earlier; the MMAs
+                        // just issued keep the tensor core busy meanwhile.
+                        if (q_load < q_mma + 1) {
+                            good = load_chunk(q_load);
+                            ++q_load;
+                        }
+                    }
+                }
+                umma::commit(mma_done);
+                if (good) good = mbar_wait(mma_done, mma_phase);
+                mma_phase ^= 1u;
+                if (!good) {
+                    *s_ok = 0;
+                    set_status(a.status, PB_DEV_WAIT_TIMEOUT);
+                }
+            }
+            __syncthreads();
+            if (!*s_ok) break;
+            umma::fence_after_sync();
+            // ---- epilogue ----
+            const float *bias = sBias + layer * 256;
+            if (layer < 3) {
+                for (int c0 = 0; c0 < 256; c0 += 16) {
+                    float v[16];
+                    umma::tmem_ld16(taddr + lane_off + (uint32_t)c0, v);
+                    uint32_t p[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        p[i] = pack_bf16x2(silu_fast(v[2 * i] + bias[c0 + 2 * i]),
+                                           silu_fast(v[2 * i + 1] + bias[c0 + 2 * i + 1]));
+                    *reinterpret_cast<uint4 *>(sH + umma::core_offset((uint32_t)tid, (uint32_t)c0, kInfSboH)) =
+                        make_uint4(p[0], p[1], p[2], p[3]);
+                    *reinterpret_cast<uint4 *>(sH + umma::core_offset((uint32_t)tid, (uint32_t)c0 + 8u, kInfSboH)) =
+                        make_uint4(p[4], p[5], p[6], p[7]);
+                }
+                umma::fence_before_sync();
+                umma::fence_smem_to_async();
+                __syncthreads();
+            } else {
+                for (int c0 = 0; c0 < 256; c0 += 16) {
+                    float v[16];
+                    umma::tmem_ld16(taddr + lane_off + (uint32_t)c0, v);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] = wrow * silu_fast(v[i] + bias[c0 + i]);
+                    // Transpose-reduce: after the four halving steps lane l holds
+                    // the partial sum of column (l >> 1); the last step adds the pair.
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const bool up = lane & 16;
+                        const float send = up ? v[i] : v[i + 8], keep = up ? v[i + 8] : v[i];
+                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const bool up = lane & 8;
+                        const float send = up ? v[i] : v[i + 4], keep = up ? v[i + 4] : v[i];
+                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const bool up = lane & 4;
+                        const float send = up ? v[i] : v[i + 2], keep = up ? v[i + 2] : v[i];
+                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+                    }
+                    {
+                        const bool up = lane & 2;
+                        const float send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
+                        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+                    }
+                    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+                    if ((lane & 1) == 0) atomicAdd(&sHsum[c0 + (lane >> 1)], v[0]);
+                }
+                float wsum = wrow;
+                for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+                if (lane == 0 && wsum != 0.0f) atomicAdd(&sHsum[256], wsum);
+                umma::fence_before_sync();
+                __syncthreads();
+            }
+        }
+        if (!*s_ok) break;
+    }
+    flush(d_cur);
+    if (tid == 0) {
+        // Drain weight copies still in flight before the block exits.
+        for (uint32_t q = q_mma; q < q_load; ++q) mbar_wait(&full[q & 1u], (q >> 1) & 1u);
+        if (!w1_ready) mbar_wait(w1_bar, 0u);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(taddr, 256);
+}
+
+// spec[d][o] += t_scale (sum_k W5[o][k] hsum[d][k] + b5[o] lsum[d]).
+__global__ void mlp_head_kernel(int n_dir, int n_out, const float *W5, const float *b5, const double *hsum,
+                                const double *lsum, double t_scale, double *spec) {
+    const int d = blockIdx.y;
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n_out) return;
+    double acc = (double)b5[o] * lsum[d];
+    for (int k = 0; k < 256; ++k) acc += (double)W5[(int64_t)o * 256 + k] * hsum[(int64_t)d * 256 + k];
+    spec[(int64_t)d * n_out + o] += t_scale * acc;
+}
+
+// Segments of every stride-th history (elec_id % stride == 0), appended to
+// dst with one atomic per warp; the exact sub-sample of the surrogate's
+// control-variate correction.
+__global__ void segments_sample_kernel(const pb_segments src, int64_t stride, pb_segments dst, unsigned int *status) {
+    const int64_t n = (int64_t)*src.count < src.capacity ? (int64_t)*src.count : src.capacity;
+    const int lane = threadIdx.x & 31;
+    const int64_t n_iter = (n + (int64_t)gridDim.x * blockDim.x - 1) / ((int64_t)gridDim.x * blockDim.x);
+    for (int64_t it = 0; it < n_iter; ++it) {
+        const int64_t i = (it * gridDim.x + blockIdx.x) * (int64_t)blockDim.x + threadIdx.x;
+        const bool take = i < n && src.elec_id[i] % stride == 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, take);
+        unsigned long long base = 0;
+        if (lane == 0 && mask) base = atomicAdd(dst.count, (unsigned long long)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (!take) continue;
+        const int64_t j = (int64_t)base + __popc(mask & ((1u << lane) - 1u));
+        if (j >= dst.capacity) {
+            set_status(status, PB_DEV_QUEUE_OVERFLOW);
+            continue;
+        }
+        for (int c = 0; c < 3; ++c) {
+            dst.r_mid[3 * j + c] = src.r_mid[3 * i + c];
+            dst.v_hat[3 * j + c] = src.v_hat[3 * i + c];
+        }
+        dst.L[j] = src.L[i];
+        dst.E_repr[j] = src.E_repr[i];
+        dst.elec_id[j] = src.elec_id[i];
+        if (dst.layer && src.layer) dst.layer[j] = src.layer[i];
+    }
+}
+
+cudaError_t launch_segments_sample(const pb_segments &src, int64_t stride, const pb_segments &dst,
+                                   unsigned int *status, cudaStream_t s, int sms) {
+    cudaError_t e = cudaMemsetAsync(dst.count, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    int64_t blocks = (src.capacity + 255) / 256;
+    if (blocks > (int64_t)sms * 8) blocks = (int64_t)sms * 8;
+    if (blocks < 1) blocks = 1;
+    segments_sample_kernel<<<(unsigned)blocks, 256, 0, s>>>(src, stride, dst, status);
+    return cudaGetLastError();
+}
+
+// W FP32 [256][cols] -> interleaved bf16 chunks of kc columns (zero padded).
+__global__ void pack_umma_kernel(int cols, int kc, const float *W, __nv_bfloat16 *out) {
+    const int n_chunks = (cols + kc - 1) / kc;
+    const int64_t n = (int64_t)256 * n_chunks * kc;
+    const uint32_t sbo = (uint32_t)(kc / 8) * 128u;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(i / (n_chunks * kc));
+        const int k = (int)(i - (int64_t)r * n_chunks * kc);
+        const int c = k / kc, kk = k - c * kc;
+        const float w = k < cols ? W[(int64_t)r * cols + k] : 0.0f;
+        const size_t byte = (size_t)c * 256 * kc * 2 + umma::core_offset((uint32_t)r, (uint32_t)kk, sbo);
+        out[byte / 2] = __float2bfloat16_rn(w);
+    }
+}
+
+cudaError_t launch_mlp_infer(const pb_mlp_infer_args &a, cudaStream_t s, int sms) {
+    cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem);
+    if (e != cudaSuccess) return e;
+    const int64_t work = (a.n_seg + 127) / 128 * (int64_t)a.n_dir;
+    int64_t grid = sms;
+    if (grid > work) grid = work;
+    if (grid < 1) return cudaSuccess;
+    mlp_infer_kernel<<<(unsigned)grid, kInfThreads, kInfSmem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_head(int n_dir, int n_out, const float *W5, const float *b5, const double *hsum,
+                            const double *lsum, double t_scale, double *spec, cudaStream_t s) {
+    dim3 grid((unsigned)((n_out + 127) / 128), (unsigned)n_dir);
+    mlp_head_kernel<<<grid, 128, 0, s>>>(n_dir, n_out, W5, b5, hsum, lsum, t_scale, spec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_pack_umma(int cols, int kc, const float *W, void *out, cudaStream_t s) {
+    const int n_chunks = (cols + kc - 1) / kc;
+    const int64_t n = (int64_t)256 * n_chunks * kc;
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    pack_umma_kernel<<<blocks, 256, 0, s>>>(cols, kc, W, (__nv_bfloat16 *)out);
     return cudaGetLastError();
 }
 

@@ -80,3 +80,30 @@ def tiles_in_sample_frame(det: PlanarDetector, angular_shape, tilt_polar_rad, ti
     idx, lab, omega = angular_tiles(det, angular_shape)
     R = sample_to_lab(tilt_polar_rad, tilt_azim_rad)
     return idx, lab @ R, omega
+
+
+def directions_at(det: PlanarDetector, uv, tilt_polar_rad, tilt_azim_rad=0.0):
+    """Sample-frame unit directions toward detector-plane points at normalised
+    coordinates ``uv[:, 0]`` (along the plane's x axis) and ``uv[:, 1]`` (y),
+    each in [-1, 1] across the active area (the surrogate's pixel inputs)."""
+    uv = np.atleast_2d(np.asarray(uv, dtype=float))
+    c = np.array([np.sin(det.theta_obs_rad), 0.0, np.cos(det.theta_obs_rad)])
+    x_axis = np.array([np.cos(det.theta_obs_rad), 0.0, -np.sin(det.theta_obs_rad)])
+    y_axis = np.array([0.0, 1.0, 0.0])
+    pts = (c * det.distance_mm)[None, :] + (0.5 * det.width_mm * uv[:, 0])[:, None] * x_axis \
+        + (0.5 * det.height_mm * uv[:, 1])[:, None] * y_axis
+    dirs = pts / np.linalg.norm(pts, axis=1, keepdims=True)
+    return dirs @ sample_to_lab(tilt_polar_rad, tilt_azim_rad)
+
+
+def tile_uv(det: PlanarDetector, angular_shape):
+    """Normalised detector coordinates (n_tile, 2) of each angular tile's pixel
+    centroid, in the tile order of ``angular_tiles``."""
+    ay, ax = angular_shape
+    xs = (np.arange(det.nx) - (det.nx - 1) / 2.0) / (det.nx / 2.0)
+    ys = (np.arange(det.ny) - (det.ny - 1) / 2.0) / (det.ny / 2.0)
+    out = []
+    for r in np.array_split(np.arange(det.ny), ay):
+        for c in np.array_split(np.arange(det.nx), ax):
+            out.append((xs[c].mean(), ys[r].mean()))
+    return np.asarray(out)

@@ -51,6 +51,13 @@ def mse_grad(Y, T, t_scale, g_scale, dY, dYt, loss, stream=None):
                                      _p(dY), _p(dYt), int(dYt.stride(0)), _p(loss), _s(stream)), "pb_mlp_mse_grad")
 
 
+def group_mse_grad(Y, T, w, S, t_scale, g_scale, dY, dYt, loss, stream=None):
+    rows, cols = Y.shape
+    L.check(L.load().pb_mlp_group_mse_grad(rows // S, S, cols, _p(Y), _p(T), int(T.stride(0)), _p(w), float(t_scale),
+                                           float(g_scale), _p(dY), _p(dYt), int(dYt.stride(0)), _p(loss), _s(stream)),
+            "pb_mlp_group_mse_grad")
+
+
 def colsum(X, out, stream=None):
     rows, cols = X.shape
     L.check(L.load().pb_mlp_colsum(rows, cols, _p(X), int(X.stride(0)), _p(out), _s(stream)), "pb_mlp_colsum")

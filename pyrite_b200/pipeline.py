@@ -59,6 +59,10 @@ class CaseSpec:
     brem_mu: np.ndarray | None = None  # [1/Angstrom] on E_grid
     exact_widths: float = 64.0
     seed: int = 0
+    # Detector plane and angular tiling behind n_hats (the surrogate's pixel
+    # coordinates); None when the directions were given directly.
+    detector: object | None = None
+    angular_shape: tuple | None = None
 
 
 class ScoringCase:
@@ -193,6 +197,89 @@ class ScoringCase:
         self.histories = 0
 
     # -- one batch ---------------------------------------------------------
+    def use_surrogate(self, models, exact_stride=20):
+        """Score PXR+CBS with an ensemble of trained surrogates plus an exact
+        control variate, instead of the exact reflection sum on every segment.
+
+        Per batch: one ``pb_mlp_infer`` launch per model over all segments
+        (length-weighted last-layer sums per direction; the linear output
+        layers are applied at readout), and, on the segments of every
+        ``exact_stride``-th history (``pb_segments_sample``), the exact
+        mixed-precision scorer and the surrogate again. The estimate
+            S = S_sur(all) + stride (S_exact(sample) - S_sur(sample))
+        is unbiased for the exact spectrum whatever the surrogate's error; the
+        surrogate only has to make the sampled difference small. The result
+        lives on the coarse grid of the surrogate (``surrogate_spectrum``).
+        ``exact_stride=0`` uses the surrogate alone."""
+        from .detector import tile_uv
+
+        if self.spec.detector is None or self.spec.angular_shape is None:
+            raise ValueError("the surrogate needs the case's detector tiling")
+        n_out = models[0].n_out
+        if self.n_E % n_out != 0:
+            raise ValueError("the case's bins must split evenly into the surrogate's coarse bins")
+        self.surrogates = list(models)
+        self.sur_stride = int(exact_stride)
+        dev, h = self.device, self.h
+        self.sur_uv = torch.as_tensor(tile_uv(self.spec.detector, self.spec.angular_shape), dtype=torch.float32,
+                                      device=dev)
+
+        def infer_set(seg, cap, count):
+            hs = [torch.zeros(self.n_dir, 256, device=dev, dtype=torch.float64) for _ in self.surrogates]
+            ls = [torch.zeros(self.n_dir, device=dev, dtype=torch.float64) for _ in self.surrogates]
+            args = [m.infer_args(self.spec, seg, cap, self.sur_uv, a, b, n_seg_device=count, status=self.status)
+                    for m, a, b in zip(self.surrogates, hs, ls)]
+            return hs, ls, args
+
+        seg_all = {"r": self.seg_r, "v": self.seg_v, "L": self.seg_L, "E": self.seg_E, "id": self.seg_id}
+        self.sur_hsum, self.sur_lsum, self.sur_args = infer_set(seg_all, self.seg_capacity, self.seg_count)
+        self.sur_args_s = []
+        if self.sur_stride > 0:
+            cap_s = self.seg_capacity // self.sur_stride * 2 + 4096
+            self.smp = {"r": h.empty((cap_s, 3), torch.float64), "v": h.empty((cap_s, 3), torch.float64),
+                        "L": h.empty(cap_s, torch.float64), "E": h.empty(cap_s, torch.float64),
+                        "id": h.empty(cap_s, torch.int64), "count": h.zeros(1, torch.int64)}
+            src = L.PbSegments()
+            src.capacity, src.count = self.seg_capacity, _ptr(self.seg_count)
+            src.r_mid, src.v_hat, src.L = _ptr(self.seg_r), _ptr(self.seg_v), _ptr(self.seg_L)
+            src.E_repr, src.elec_id = _ptr(self.seg_E), _ptr(self.seg_id)
+            dst = L.PbSegments()
+            dst.capacity, dst.count = cap_s, _ptr(self.smp["count"])
+            dst.r_mid, dst.v_hat, dst.L = _ptr(self.smp["r"]), _ptr(self.smp["v"]), _ptr(self.smp["L"])
+            dst.E_repr, dst.elec_id = _ptr(self.smp["E"]), _ptr(self.smp["id"])
+            self.smp_src, self.smp_dst = src, dst
+            cs = L.PbCxrArgs.from_buffer_copy(self.cargs)
+            cs.n_seg = cap_s
+            cs.r_mid, cs.v_hat, cs.L = _ptr(self.smp["r"]), _ptr(self.smp["v"]), _ptr(self.smp["L"])
+            cs.E_keV, cs.elec_id = _ptr(self.smp["E"]), _ptr(self.smp["id"])
+            cs.n_seg_device = _ptr(self.smp["count"])
+            self.spec_sample = h.zeros((self.n_dir, self.n_E), torch.float64)
+            cs.spec = _ptr(self.spec_sample)
+            self.cargs_s = cs
+            self.sur_hsum_s, self.sur_lsum_s, self.sur_args_s = infer_set(self.smp, cap_s, self.smp["count"])
+
+    def _head(self, hsums, lsums):
+        out = torch.zeros(self.n_dir, self.surrogates[0].n_out, device=self.device, dtype=torch.float64)
+        k = len(self.surrogates)
+        for m, hs, ls in zip(self.surrogates, hsums, lsums):
+            L.check(self.lib.pb_mlp_head(self.n_dir, m.n_out, m.W5r.data_ptr(), m.p["b5"].data_ptr(),
+                                         hs.data_ptr(), ls.data_ptr(), float(m.t_scale) / k, out.data_ptr(),
+                                         torch.cuda.current_stream().cuda_stream), "pb_mlp_head")
+        return out
+
+    def coarse(self, spec_fine):
+        """Mean of each run of n_E / n_out fine bins: the surrogate's coarse bins."""
+        n_out = self.surrogates[0].n_out
+        return spec_fine.view(spec_fine.shape[0], n_out, -1).mean(-1)
+
+    def surrogate_spectrum(self):
+        """Surrogate (+ exact control variate) spectrum [n_dir, n_coarse] so far,
+        per history, in the exact scorer's units."""
+        s = self._head(self.sur_hsum, self.sur_lsum)
+        if self.sur_stride > 0:
+            s += self.sur_stride * (self.coarse(self.spec_sample) - self._head(self.sur_hsum_s, self.sur_lsum_s))
+        return s.cpu().numpy() / max(self.histories, 1)
+
     def run_batch(self, e_start: int, n: int, stream=None, events=None):
         """Transport histories [e_start, e_start + n) and score them. Stream ordered."""
         if n > self.batch:
@@ -206,7 +293,17 @@ class ScoringCase:
         L.check(self.lib.pb_transport(C.byref(a), s), "pb_transport")
         if events is not None:
             events[1].record()
-        L.check(self.lib.pb_cxr_score(C.byref(self.cargs), s), "pb_cxr_score")
+        if getattr(self, "surrogates", None):
+            if self.sur_stride > 0:
+                L.check(self.lib.pb_segments_sample(C.byref(self.smp_src), self.sur_stride, C.byref(self.smp_dst),
+                                                    _ptr(self.status), s), "pb_segments_sample")
+                L.check(self.lib.pb_cxr_score(C.byref(self.cargs_s), s), "pb_cxr_score")
+            if events is not None and len(events) > 4:
+                events[4].record()  # exact sub-sample done; the surrogate follows
+            for sa in self.sur_args + self.sur_args_s:
+                L.check(self.lib.pb_mlp_infer(C.byref(sa), s), "pb_mlp_infer")
+        else:
+            L.check(self.lib.pb_cxr_score(C.byref(self.cargs), s), "pb_cxr_score")
         if events is not None:
             events[2].record()
         if self.bargs is not None:
@@ -218,7 +315,12 @@ class ScoringCase:
     def kernel_launches_per_batch(self) -> int:
         """This library's kernels launched per batch (transport 1, CXR 2 with
         the far-field finalize, brem one per 16 directions)."""
-        n = 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
+        if getattr(self, "surrogates", None):
+            n = 1 + len(self.surrogates) * (2 if self.sur_stride > 0 else 1)
+            if self.sur_stride > 0:
+                n += 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
+        else:
+            n = 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
         if self.bargs is not None:
             n += (self.n_dir + 15) // 16
         return n
@@ -252,21 +354,36 @@ class ScoringCase:
     def reset(self):
         for t in (self.spec_cxr, self.fates, self.exit_E, self.exit_theta, self.deposit):
             t.zero_()
+        for t in (getattr(self, "sur_hsum", []) + getattr(self, "sur_lsum", []) + getattr(self, "sur_hsum_s", [])
+                  + getattr(self, "sur_lsum_s", [])):
+            t.zero_()
+        if getattr(self, "spec_sample", None) is not None:
+            self.spec_sample.zero_()
         if self.bargs is not None:
             self.spec_brem.zero_()
         self.histories = 0
 
 
 def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 1, warmup: int = 1,
-                       precision="mixed", rng="philox", e_start: int = 0, device=None) -> dict:
+                       precision="mixed", rng="philox", e_start: int = 0, device=None, surrogates=None,
+                       exact_stride=50) -> dict:
     """End-to-end run through host buffers: every step copies the case's input
     tables from pinned host memory to the device, runs one batch, and reads
     the spectra and tallies back to pinned host memory. Returns the rate and
-    the bytes moved per step."""
+    the bytes moved per step. With ``surrogates`` the PXR+CBS part is the
+    surrogate with its exact sub-sample; the per-direction accumulators read
+    back each step are the ones its readout needs."""
     case = ScoringCase(spec, precision=precision, rng=rng, batch_histories=histories_per_step,
                        device=device)
+    if surrogates:
+        case.use_surrogate(surrogates, exact_stride=exact_stride)
     pairs = [(t.cpu().pin_memory(), t) for t in case.h.inputs]
-    outs = [case.spec_cxr, case.fates, case.exit_E, case.exit_theta, case.deposit]
+    if surrogates:
+        outs = case.sur_hsum + case.sur_lsum + case.sur_hsum_s + case.sur_lsum_s
+        outs += [case.spec_sample] if case.sur_stride > 0 else []
+        outs += [case.fates, case.exit_E, case.exit_theta, case.deposit]
+    else:
+        outs = [case.spec_cxr, case.fates, case.exit_E, case.exit_theta, case.deposit]
     if case.bargs is not None:
         outs.append(case.spec_brem)
     host_out = [torch.empty_like(t, device="cpu").pin_memory() for t in outs]

@@ -64,7 +64,7 @@ def test_gemm_backward_epilogue(cuda_device):
     z = torch.randn(M, N, device=cuda_device, generator=g)
     out = torch.empty(M, N, device=cuda_device)
     mlp.gemm(A, B, dsilu_z=z, out_f32=out)
-    s = torch.sigmoid(z)
-    ref = _ref(A, B) * (s * (1 + z * (1 - s)))
+    t = torch.tanh(0.5 * z)
+    ref = _ref(A, B) * (0.5 * (1 + t) + 0.25 * z * (1 - t * t))
     torch.cuda.synchronize()
-    assert float((out - ref).abs().max()) < 1e-4
+    assert float((out - ref).abs().max()) < 3e-3 * float(ref.abs().max())
