@@ -69,8 +69,15 @@ __device__ __forceinline__ Real b_mean_transmission(Real t0, Real t1) {
 }
 
 template <class Real>
-__global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
-    __shared__ BremSeg<Real> segs[kBremChunk];
+__global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 3 : 1)
+    brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
+    // Segment chunk staged in shared memory (half as many FP64 segments, to
+    // stay within the static shared-memory limit next to the accumulators).
+    constexpr int kChunk = sizeof(Real) == 4 ? kBremChunk : kBremChunk / 2;
+    __shared__ BremSeg<Real> segs[kChunk];
+    // Per-thread FP64 sums over the block's segments, one per direction, in
+    // shared memory (keeps the registers for the per-chunk partials).
+    __shared__ double acc[kBremMaxDir][kBremThreads];
     __shared__ Real Zs[kBremMaxEl];
     __shared__ Real inv_nz[kBremMaxDir];
     __shared__ int up[kBremMaxDir];
@@ -94,9 +101,8 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
     const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
     const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
-    double acc[kBremMaxDir];
 #pragma unroll
-    for (int j = 0; j < kBremMaxDir; ++j) acc[j] = 0.0;
+    for (int j = 0; j < kBremMaxDir; ++j) acc[j][threadIdx.x] = 0.0;
     if (a.n_seg_device) {
         const int64_t live = (int64_t)*a.n_seg_device;
         if (live < n_seg) n_seg = live;
@@ -105,8 +111,8 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
     const int64_t s_begin = per * blockIdx.y;
     int64_t s_end = s_begin + per < n_seg ? s_begin + per : n_seg;
     if (s_end < s_begin) s_end = s_begin;
-    for (int64_t c0s = s_begin; c0s < s_end; c0s += kBremChunk) {
-        const int nc = (int)((s_end - c0s) < kBremChunk ? (s_end - c0s) : kBremChunk);
+    for (int64_t c0s = s_begin; c0s < s_end; c0s += kChunk) {
+        const int nc = (int)((s_end - c0s) < kChunk ? (s_end - c0s) : kChunk);
         __syncthreads();
         for (int j = threadIdx.x; j < nc; j += blockDim.x) {
             const int64_t s = c0s + j;
@@ -132,8 +138,8 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
         }
         __syncthreads();
         if (!on) continue;
-        // Float partial sums per chunk, folded into the FP64 accumulators once
-        // per chunk; FP64 accumulates directly.
+        // Partial sums per chunk (float on the mixed path), folded into the
+        // FP64 accumulators once per chunk.
         Real part[kBremMaxDir];
 #pragma unroll
         for (int dd = 0; dd < kBremMaxDir; ++dd) part[dd] = 0;
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
                         const Real f = inv_nz[dd];
                         const Real p0 = up[dd] ? b.path0 * f : (T_slab - b.path0) * f;
                         const Real p1 = up[dd] ? b.path1 * f : (T_slab - b.path1) * f;
-                        acc[dd] += (double)(nsig * b_mean_transmission<Real>(p0 * mu, p1 * mu));
+                        part[dd] += nsig * b_mean_transmission<Real>(p0 * mu, p1 * mu);
                     }
                 }
             } else {
@@ -201,15 +207,14 @@ __global__ void __launch_bounds__(kBremThreads) brem_kernel(const pb_brem_args a
                 }
             }
         }
-        if constexpr (sizeof(Real) == 4) {
 #pragma unroll
-            for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd] += (double)part[dd];
-        }
+        for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd][threadIdx.x] += (double)part[dd];
     }
     if (on) {
 #pragma unroll
         for (int dd = 0; dd < kBremMaxDir; ++dd)
-            if (dd < nd && acc[dd] != 0.0) atomicAdd(&a.spec[(int64_t)(d0 + dd) * a.n_E + e], acc[dd]);
+            if (dd < nd && acc[dd][threadIdx.x] != 0.0)
+                atomicAdd(&a.spec[(int64_t)(d0 + dd) * a.n_E + e], acc[dd][threadIdx.x]);
     }
 }
 
@@ -217,7 +222,14 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     if (a.n_el > kBremMaxEl || a.n_el < 1) return cudaErrorInvalidValue;
     int64_t n_seg = a.n_seg;
     const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
-    int64_t gy = ((int64_t)sms * 4 + (int64_t)gx - 1) / (int64_t)gx;
+    // One wave: as many segment slices as keep every SM at its resident limit.
+    int per_sm = 0;
+    cudaError_t oe = a.precision == PB_MIXED
+                         ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_kernel<float>, kBremThreads, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_kernel<double>, kBremThreads, 0);
+    if (oe != cudaSuccess) return oe;
+    if (per_sm < 1) per_sm = 1;
+    int64_t gy = (int64_t)sms * per_sm / (int64_t)gx;
     const int64_t max_y = (n_seg + kBremChunk - 1) / kBremChunk;
     if (gy > max_y) gy = max_y;
     if (gy < 1) gy = 1;

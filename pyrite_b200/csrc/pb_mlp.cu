@@ -339,7 +339,7 @@ cudaError_t launch_mlp_pack(int rows, int cols, const float *W, void *Wb, int ld
 // (128 x 16 bf16) in shared memory; layer 1 is one K=16 MMA against W1 held
 // in shared memory; layers 2-4 stream their weights from global memory (L2)
 // in four 32 KB K-chunks, pre-packed in the interleaved layout so each chunk
-// is one bulk copy, double-buffered against the MMAs. Each epilogue reads the
+// is one bulk copy, with three chunks kept in flight ahead of the MMAs. Each epilogue reads the
 // 128 x 256 FP32 accumulator from tensor memory, adds the bias, applies SiLU
 // (x (1 + tanh(x/2)) / 2) and writes bf16 activations back over the layer's
 // input in shared memory; the last one weights each row by its segment
@@ -352,7 +352,8 @@ constexpr uint32_t kInfSboH = 4096;   // H: 128 x 256
 constexpr uint32_t kInfSboW = 1024;   // W chunk: 256 x 64
 constexpr uint32_t kInfChunk = 256 * 64 * 2;  // 32 KB
 constexpr uint32_t kInfW1 = 256 * 16 * 2;     // 8 KB
-constexpr uint32_t kInfSmem = kInfW1 + 128 * 16 * 2 + 128 * 256 * 2 + 2 * kInfChunk + 4 * 256 * 4 + 257 * 4 + 128;
+constexpr int kInfStages = 4;                 // weight chunk stages: one whole layer in flight
+constexpr uint32_t kInfSmem = kInfW1 + 128 * 16 * 2 + 128 * 256 * 2 + kInfStages * kInfChunk + 4 * 256 * 4 + 257 * 4 + 160;
 
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
@@ -411,15 +412,15 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
     uint8_t *sW1 = smem;
     uint8_t *sX = sW1 + kInfW1;
     uint8_t *sH = sX + 128 * 16 * 2;
-    uint8_t *sW = sH + 128 * 256 * 2;  // two chunk stages
-    float *sBias = reinterpret_cast<float *>(sW + 2 * kInfChunk);  // [4][256]
-    float *sHsum = sBias + 4 * 256;                                 // [256] + lsum
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sHsum + 257 + 3);  // 8-byte aligned
-    uint64_t *full = bar;        // [2] weight chunk landed
-    uint64_t *empty = bar + 2;   // [2] MMAs of the chunk done
-    uint64_t *mma_done = bar + 4;
-    uint64_t *w1_bar = bar + 5;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 6);
+    uint8_t *sW = sH + 128 * 256 * 2;  // kInfStages chunk stages
+    float *sBias = reinterpret_cast<float *>(sW + kInfStages * kInfChunk);  // [4][256]
+    float *sHsum = sBias + 4 * 256;                                          // [256] + lsum
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sHsum + 257 + 3);           // 8-byte aligned
+    uint64_t *full = bar;                      // [kInfStages] weight chunk landed
+    uint64_t *empty = bar + kInfStages;        // [kInfStages] MMAs of the chunk done
+    uint64_t *mma_done = bar + 2 * kInfStages;
+    uint64_t *w1_bar = mma_done + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(w1_bar + 1);
     volatile int *s_ok = reinterpret_cast<volatile int *>(tslot + 1);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
     for (int i = tid; i < 4 * 256; i += kInfThreads) sBias[i] = a.bias[i / 256][i % 256];
     for (int i = tid; i < 257; i += kInfThreads) sHsum[i] = 0.0f;
     if (tid == 0) {
-        for (int i = 0; i < 6; ++i) mbar_init(&bar[i], 1);
+        for (int i = 0; i < 2 * kInfStages + 2; ++i) mbar_init(&bar[i], 1);
         *s_ok = 1;
         mbar_expect_tx(w1_bar, kInfW1);
         bulk_g2s(sW1, a.w1_packed, kInfW1, w1_bar);
@@ -454,18 +455,20 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
     const uint8_t *wsrc[3] = {static_cast<const uint8_t *>(a.w_packed[0]), static_cast<const uint8_t *>(a.w_packed[1]),
                               static_cast<const uint8_t *>(a.w_packed[2])};
 
-    // Issue the bulk copy of chunk q (layer 2 + (q / 4) % 3, K-chunk q % 4).
+    // Issue the bulk copy of chunk q (layer 2 + (q / 4) % 3, K-chunk q % 4)
+    // into stage q % kInfStages, once the MMAs of chunk q - kInfStages left it.
     auto load_chunk = [&](uint32_t q) -> bool {
-        const uint32_t s = q & 1u;
-        if (q >= 2 && !mbar_wait(&empty[s], ((q >> 1) - 1u) & 1u)) return false;
+        const uint32_t s = q % kInfStages;
+        if (q >= kInfStages && !mbar_wait(&empty[s], (q / kInfStages - 1u) & 1u)) return false;
         const uint32_t layer = (q >> 2) % 3u, kc = q & 3u;
         mbar_expect_tx(&full[s], kInfChunk);
         bulk_g2s(sW + s * kInfChunk, wsrc[layer] + (size_t)kc * kInfChunk, kInfChunk, &full[s]);
         return true;
     };
     if (tid == 0 && w_begin < w_end) {
-        if (!load_chunk(0)) *s_ok = 0;
-        q_load = 1;
+        for (uint32_t q = 0; q + 1 < (uint32_t)kInfStages; ++q)
+            if (!load_chunk(q)) *s_ok = 0;
+        q_load = kInfStages - 1;
     }
 
     const FeatureMap fm(a);
@@ -522,8 +525,8 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
                                        umma::smem_desc(smem_addr(sW1), 128u, kInfSboX), idesc, 0u);
                 } else {
                     for (int kc = 0; kc < 4 && good; ++kc) {
-                        const uint32_t s = q_mma & 1u;
-                        good = mbar_wait(&full[s], (q_mma >> 1) & 1u);
+                        const uint32_t s = q_mma % kInfStages;
+                        good = mbar_wait(&full[s], (q_mma / kInfStages) & 1u);
                         if (!good) break;
                         const uint32_t w0 = smem_addr(sW + s * kInfChunk);
                         const uint32_t h0 = smem_addr(sH) + (uint32_t)kc * 1024u;  // K offset 64 = 8 core matrices
@@ -533,10 +536,10 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
                                            (kc > 0 || ks > 0) ? 1u : 0u);
                         umma::commit(&empty[s]);
                         ++q_mma;
-                        // Load the next chunk (weights are the same every tile) into
-                        // the stage whose MMAs were issued one chunk earlier; the MMAs
-                        // just issued keep the tensor core busy meanwhile.
-                        if (q_load < q_mma + 1) {
+                        // Keep kInfStages - 1 chunks ahead (weights are the same every
+                        // tile): the next load reuses the stage of the chunk issued one
+                        // step earlier, while the MMAs just issued keep the core busy.
+                        if (q_load < q_mma + kInfStages - 1) {
                             good = load_chunk(q_load);
                             ++q_load;
                         }
@@ -618,7 +621,7 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
     flush(d_cur);
     if (tid == 0) {
         // Drain weight copies still in flight before the block exits.
-        for (uint32_t q = q_mma; q < q_load; ++q) mbar_wait(&full[q & 1u], (q >> 1) & 1u);
+        for (uint32_t q = q_mma; q < q_load; ++q) mbar_wait(&full[q % kInfStages], (q / kInfStages) & 1u);
         if (!w1_ready) mbar_wait(w1_bar, 0u);
     }
     umma::fence_before_sync();
