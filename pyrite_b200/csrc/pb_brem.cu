@@ -96,6 +96,25 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 3 : 1)
         up[threadIdx.x] = nz < (Real)0;
         inv_f_ln2[threadIdx.x] = (float)(fmax(fabs((double)nz), 1.0e-12) / 0.6931471805599453);
     }
+    // Whether every direction of this launch leaves through the same face
+    // (+1 top, -1 bottom, 0 mixed), read from the directions themselves; with
+    // a full set of directions on one side the per-direction factors live in
+    // registers (the fast form of the escape loop below).
+    int side_all = 0;
+    float fr[kBremMaxDir];
+    float f_min_ln2 = 3.0e38f;
+    {
+        int n_up = 0;
+        for (int dd = 0; dd < nd; ++dd) n_up += a.n_hat[3 * (d0 + dd) + 2] < 0.0 ? 1 : 0;
+        side_all = n_up == nd ? 1 : (n_up == 0 ? -1 : 0);
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd) {
+            const double nz = dd < nd ? fabs(a.n_hat[3 * (d0 + dd) + 2]) : 1.0;
+            fr[dd] = (float)(1.0 / fmax(nz, 1.0e-12));
+            if (dd < nd) f_min_ln2 = fminf(f_min_ln2, fr[dd] * 0.69314718f);
+        }
+    }
+    const bool fast = sizeof(Real) == 4 && nd == kBremMaxDir && side_all != 0;
     const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
     const Real k = (Real)k_kev_d;
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
@@ -184,31 +203,63 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 3 : 1)
                     }
                 }
             } else {
-                // Escape mean exp(-lo) (1 - e^-D)/D per direction with base-2
-                // optical depths A_s f (lower end, per side s) and B f (depth
-                // difference): two SFU exponentials per direction and one
-                // reciprocal per (segment, energy). Below D = 0.01 the series
-                // keeps float accuracy.
+                // Escape mean exp(-lo) (1 - e^-D)/D per direction, with base-2
+                // optical depths A f (lower end) and B f (depth difference),
+                // D = B f ln 2. Sums are kept without the factor 1/(f ln 2),
+                // applied once per chunk:
+                //   D > 0.01 for every direction: [nsig / B] 2^(-A f) (1 - 2^(-B f));
+                //   otherwise:                  nsig 2^(-A f) (1 - D/2 + D^2/6 - D^3/24) f ln 2,
+                // the series where the difference would cancel (D^4/120 < 1e-10).
+                // The fast form (all 16 tiles on one side, per-thread registers
+                // for f) costs two SFU exponentials and ~6 FMAs per direction.
                 const float mu2 = mu * 1.44269504f;
                 const float A_dn = mu2 * fminf(T_slab - b.path0, T_slab - b.path1);
                 const float A_up = mu2 * fminf(b.path0, b.path1);
                 const float B = mu2 * fabsf(b.path1 - b.path0);
-                const float inv_B = B > 0.0f ? __fdividef(1.0f, B) : 0.0f;
+                if (fast) {
+                    const float A = side_all > 0 ? A_up : A_dn;
+                    if (B * f_min_ln2 > 0.01f) {
+                        const float w = __fdividef(nsig, B);
 #pragma unroll
-                for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                    if (dd < nd) {
-                        const float f = inv_nz[dd];
-                        const float x = B * f;                 // D / ln 2
-                        const float D = x * 0.69314718f;
-                        const float ratio = D > 0.01f ? (1.0f - ex2_approx(-x)) * inv_B * inv_f_ln2[dd]
-                                                      : 1.0f - D * (0.5f - D * (1.0f / 6.0f - D * (1.0f / 24.0f)));
-                        part[dd] += nsig * ex2_approx(-(up[dd] ? A_up : A_dn) * f) * ratio;
+                        for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                            const float m = 1.0f - ex2_approx(-B * fr[dd]);
+                            part[dd] = fmaf(w * m, ex2_approx(-A * fr[dd]), part[dd]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                            const float fl = fr[dd] * 0.69314718f;
+                            const float D = B * fl;
+                            const float ratio = fmaf(D, fmaf(D, fmaf(D, -1.0f / 24.0f, 1.0f / 6.0f), -0.5f), 1.0f);
+                            part[dd] = fmaf(nsig * fl * ratio, ex2_approx(-A * fr[dd]), part[dd]);
+                        }
+                    }
+                } else {
+                    const float w = B > 0.0f ? __fdividef(nsig, B) : 0.0f;
+#pragma unroll
+                    for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                        if (dd < nd) {
+                            const float f = inv_nz[dd];
+                            const float fl = f * 0.69314718f;
+                            const float D = B * fl;
+                            const float A = up[dd] ? A_up : A_dn;
+                            const float e_lo = ex2_approx(-A * f);
+                            const float t = D > 0.01f
+                                                ? w * (1.0f - ex2_approx(-B * f))
+                                                : nsig * fl * fmaf(D, fmaf(D, fmaf(D, -1.0f / 24.0f, 1.0f / 6.0f), -0.5f), 1.0f);
+                            part[dd] = fmaf(t, e_lo, part[dd]);
+                        }
                     }
                 }
             }
         }
+        if constexpr (sizeof(Real) == 4) {
 #pragma unroll
-        for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd][threadIdx.x] += (double)part[dd];
+            for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd][threadIdx.x] += (double)part[dd] * (double)inv_f_ln2[dd];
+        } else {
+#pragma unroll
+            for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd][threadIdx.x] += (double)part[dd];
+        }
     }
     if (on) {
 #pragma unroll
