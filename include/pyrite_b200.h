@@ -227,7 +227,8 @@ typedef struct pb_cxr_args {
     double exact_widths;    /* bin-mean: exact within this many widths; <=0: all exact */
     int32_t far_pad;        /* bin-mean, uniform axis: virtual centre bins each side
                                covering the keep window; -1 disables the far field */
-    double *spec;           /* [n_dir*n_E] accumulated (+=), FP64, not normalised */
+    double *spec;           /* [n_dir*n_E] accumulated (+=), FP64, not normalised;
+                               node quadrature: NULL keeps the lines only */
     double *far_moments;    /* workspace [n_dir*(n_E+2*far_pad)*3], zeroed by the call */
     /* Line buffer (node quadrature, and optional output of every kept line):
      * [line_capacity] each; direction index in line_dir. */

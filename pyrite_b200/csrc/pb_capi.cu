@@ -121,8 +121,9 @@ int pb_cxr_score(const pb_cxr_args *a, void *stream) {
         if (a->exact_widths > 0.0 && a->far_pad >= 0 && !a->far_moments)
             return fail(PB_ERR_INVALID, "pb_cxr_score: far field needs the far_moments workspace");
     } else if (a->quadrature == PB_QUAD_NODE) {
-        if (!a->E_grid || !a->spec || !a->line_E || !a->line_a || !a->line_w || !a->line_dir || !a->line_count)
-            return fail(PB_ERR_INVALID, "pb_cxr_score: node quadrature needs the grid and a line buffer");
+        if (!a->line_E || !a->line_a || !a->line_w || !a->line_dir || !a->line_count)
+            return fail(PB_ERR_INVALID, "pb_cxr_score: node quadrature needs a line buffer");
+        if (a->spec && !a->E_grid) return fail(PB_ERR_INVALID, "pb_cxr_score: node spectrum needs E_grid");
     } else {
         return fail(PB_ERR_INVALID, "pb_cxr_score: unknown quadrature %d", a->quadrature);
     }

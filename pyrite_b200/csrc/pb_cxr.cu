@@ -1425,7 +1425,7 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }
-    if (a.quadrature == PB_QUAD_NODE && a.line_E != nullptr) {
+    if (a.quadrature == PB_QUAD_NODE && a.line_E != nullptr && a.spec != nullptr) {
         dim3 ng((unsigned)((a.n_E + 127) / 128), 64);
         node_reduce_kernel<Real><<<ng, 128, 0, s>>>(a.E_grid, a.n_E, a.line_E, a.line_a, a.line_w,
                                                     a.line_dir, a.line_count, a.line_capacity, a.spec);

@@ -299,7 +299,7 @@ def _cxr_lines(spec, seg, n_seg, n_hats, device, cap_per_pair=64):
     a.tables = t
     a.n_E = 1
     a.E_grid = _ptr(h.f64([30000.0]))
-    a.spec = _ptr(h.zeros(n_dir, torch.float64))
+    a.spec = None  # lines only, no node spectrum
     cap = int(n_seg) * n_dir * cap_per_pair
     count = h.zeros(1, torch.int64)
     lines = {"E": h.empty(cap, torch.float64), "a": h.empty(cap, torch.float64), "w": h.empty(cap, torch.float64),
