@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "pb_common.cuh"
 #include "pb_internal.h"
@@ -629,6 +630,288 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
     if (warp == 0) umma::tmem_dealloc(taddr, 256);
 }
 
+// ---------------------------------------------------------------------------
+// Two-tile ping-pong variant: the epilogues of one tile overlap the MMAs of
+// the other.
+//
+// 288 threads: warpgroup 0 (warps 0-3) and warpgroup 1 (warps 4-7) each own a
+// tile slot -- 256 tensor-memory columns, an X and an H buffer -- and warp 8's
+// lane 0 is the producer: it streams weight chunks and issues the MMAs of the
+// two slots in the order (layer 1: slot 0, slot 1), (layer 2: slot 0, slot 1),
+// ..., so the tensor core works on one slot while the other slot's warpgroup
+// runs its epilogue. A warpgroup hands its slot to the producer through
+// in_ready[s] (one arrival by its leader after a named-barrier sync of the
+// group) and gets the accumulator back through acc_full[s] (tcgen05.commit).
+// Blocks own an even number of tiles (an odd range gets one empty tile, all
+// of whose rows weigh 0). Every wait is bounded; a timeout sets the status
+// word and an abort flag that every role checks after its waits.
+// ---------------------------------------------------------------------------
+// PB_MLP_INFER=serial selects the single-tile kernel above (the reference
+// point for the ping-pong one); the default is the ping-pong kernel.
+static int infer_variant() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("PB_MLP_INFER");
+        v = (e && e[0] == 's') ? 1 : 2;
+    }
+    return v;
+}
+
+constexpr int kPPThreads = 288;
+constexpr int kPPStages = 2;
+constexpr uint32_t kPPSmem = kInfW1 + 2 * (128 * 16 * 2) + 2 * (128 * 256 * 2) + kPPStages * kInfChunk +
+                             4 * 256 * 4 + 2 * 257 * 4 + 256;
+
+__device__ __forceinline__ void wg_sync(int slot) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + slot) : "memory");
+}
+
+__global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_mlp_infer_args a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *sW1 = smem;
+    uint8_t *sX = sW1 + kInfW1;                 // [2] x 4 KB
+    uint8_t *sH = sX + 2 * (128 * 16 * 2);      // [2] x 64 KB
+    uint8_t *sW = sH + 2 * (128 * 256 * 2);     // kPPStages x 32 KB
+    float *sBias = reinterpret_cast<float *>(sW + kPPStages * kInfChunk);  // [4][256]
+    float *sHsum = sBias + 4 * 256;                                         // [2][257]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(
+        (reinterpret_cast<uintptr_t>(sHsum + 2 * 257) + 15) & ~static_cast<uintptr_t>(15));
+    uint64_t *full = bar;                        // [kPPStages]
+    uint64_t *empty = bar + kPPStages;           // [kPPStages]
+    uint64_t *in_ready = bar + 2 * kPPStages;    // [2]
+    uint64_t *acc_full = in_ready + 2;           // [2]
+    uint64_t *w1_bar = acc_full + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(w1_bar + 1);
+    volatile int *s_abort = reinterpret_cast<volatile int *>(tslot + 1);
+    volatile int *s_ok = s_abort + 1;  // [2] per-slot result of the leader's last wait
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int64_t n_seg = a.n_seg;
+    if (a.n_seg_device && (int64_t)*a.n_seg_device < n_seg) n_seg = (int64_t)*a.n_seg_device;
+    const int64_t n_tiles = (n_seg + 127) / 128;
+    const int64_t n_work = n_tiles * a.n_dir;
+    const int64_t w_begin = n_work * blockIdx.x / gridDim.x;
+    const int64_t w_end = n_work * (blockIdx.x + 1) / gridDim.x;
+    const int64_t T = w_end - w_begin;
+    const int64_t n_pairs = (T + 1) / 2;
+
+    if (warp == 0) {
+        umma::tmem_alloc(tslot, 512);
+        umma::tmem_relinquish();
+    }
+    for (int i = tid; i < 4 * 256; i += kPPThreads) sBias[i] = a.bias[i / 256][i % 256];
+    for (int i = tid; i < 2 * 257; i += kPPThreads) sHsum[i] = 0.0f;
+    if (tid == 0) {
+        for (int i = 0; i < 2 * kPPStages + 5; ++i) mbar_init(&bar[i], 1);
+        *s_abort = 0;
+        s_ok[0] = s_ok[1] = 1;
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t taddr = *tslot;
+
+    if (warp == 8) {
+        // ------------------------- producer -------------------------
+        if (lane == 0 && n_pairs > 0) {
+            const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
+            const uint8_t *wsrc[3] = {static_cast<const uint8_t *>(a.w_packed[0]),
+                                      static_cast<const uint8_t *>(a.w_packed[1]),
+                                      static_cast<const uint8_t *>(a.w_packed[2])};
+            // Chunk q of the stream: per tile pair 24 chunks, layer (q % 24) / 8
+            // of W2..W4, K-chunk q % 4 (each layer's four chunks twice, once
+            // per slot).
+            auto load_chunk = [&](uint32_t q) -> bool {
+                const uint32_t st = q % kPPStages;
+                if (q >= kPPStages && !mbar_wait(&empty[st], (q / kPPStages - 1u) & 1u)) return false;
+                const uint32_t layer = (q % 24u) / 8u, kc = q & 3u;
+                mbar_expect_tx(&full[st], kInfChunk);
+                bulk_g2s(sW + st * kInfChunk, wsrc[layer] + (size_t)kc * kInfChunk, kInfChunk, &full[st]);
+                return true;
+            };
+            bool good = true;
+            mbar_expect_tx(w1_bar, kInfW1);
+            bulk_g2s(sW1, a.w1_packed, kInfW1, w1_bar);
+            const uint32_t q_total = (uint32_t)n_pairs * 24u;
+            uint32_t q_load = 0, q_mma = 0;
+            for (; q_load + 1 < (uint32_t)kPPStages && q_load < q_total && good; ++q_load) good = load_chunk(q_load);
+            uint32_t in_phase[2] = {0u, 0u};
+            good = good && mbar_wait(w1_bar, 0u);
+            for (int64_t p = 0; p < n_pairs && good; ++p) {
+                for (int layer = 0; layer < 4 && good; ++layer) {
+                    for (int slot = 0; slot < 2 && good; ++slot) {
+                        good = mbar_wait(&in_ready[slot], in_phase[slot]);
+                        in_phase[slot] ^= 1u;
+                        if (!good || *s_abort) { good = false; break; }
+                        umma::fence_after_sync();
+                        const uint32_t d_tmem = taddr + (uint32_t)(slot * 256);
+                        if (layer == 0) {
+                            umma::mma_bf16(d_tmem, umma::smem_desc(smem_addr(sX + slot * 4096), 128u, kInfSboX),
+                                           umma::smem_desc(smem_addr(sW1), 128u, kInfSboX), idesc, 0u);
+                        } else {
+                            const uint32_t h0 = smem_addr(sH + slot * 65536);
+                            for (int kc = 0; kc < 4 && good; ++kc) {
+                                const uint32_t st = q_mma % kPPStages;
+                                good = mbar_wait(&full[st], (q_mma / kPPStages) & 1u);
+                                if (!good) break;
+                                const uint32_t w0 = smem_addr(sW + st * kInfChunk);
+                                for (int ks = 0; ks < 4; ++ks)
+                                    umma::mma_bf16(d_tmem,
+                                                   umma::smem_desc(h0 + (uint32_t)kc * 1024u + ks * 256u, 128u,
+                                                                   kInfSboH),
+                                                   umma::smem_desc(w0 + ks * 256u, 128u, kInfSboW), idesc,
+                                                   (kc > 0 || ks > 0) ? 1u : 0u);
+                                umma::commit(&empty[st]);
+                                ++q_mma;
+                                if (q_load < q_total && q_load < q_mma + kPPStages - 1) {
+                                    good = load_chunk(q_load);
+                                    ++q_load;
+                                }
+                            }
+                        }
+                        umma::commit(&acc_full[slot]);
+                    }
+                }
+            }
+            if (!good) {
+                *s_abort = 1;
+                set_status(a.status, PB_DEV_WAIT_TIMEOUT);
+            }
+            // Drain copies still in flight (bounded) before the block exits.
+            for (uint32_t q = q_mma; q < q_load; ++q) mbar_wait(&full[q % kPPStages], (q / kPPStages) & 1u);
+        }
+    } else {
+        // --------------------- epilogue warpgroups ---------------------
+        const int slot = warp >> 2;
+        const int r = tid - 128 * slot;  // row of the tile
+        const int wq = r >> 5;           // warp within the group: TMEM lanes 32 wq..
+        const bool leader = r == 0;
+        uint8_t *mX = sX + slot * 4096;
+        uint8_t *mH = sH + slot * 65536;
+        float *hs = sHsum + slot * 257;
+        const uint32_t t_base = taddr + (uint32_t)(slot * 256) + ((uint32_t)(wq * 32) << 16);
+        const FeatureMap fm(a);
+        uint32_t acc_phase = 0;
+        int d_cur = -1;
+        auto flush = [&](int d) {
+            wg_sync(slot);
+            if (d >= 0) {
+                for (int i = r; i < 257; i += 128) {
+                    const float v = hs[i];
+                    if (v != 0.0f) {
+                        if (i < 256) atomicAdd(&a.hsum[(int64_t)d * 256 + i], (double)v);
+                        else atomicAdd(&a.lsum[d], (double)v);
+                    }
+                    hs[i] = 0.0f;
+                }
+            }
+            wg_sync(slot);
+        };
+        // Hand the slot to the producer: every thread's shared-memory writes
+        // and tensor-memory reads are done, then one arrival.
+        auto hand_over = [&]() {
+            umma::fence_smem_to_async();
+            umma::fence_before_sync();
+            wg_sync(slot);
+            if (leader) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&in_ready[slot])) : "memory");
+        };
+        // Wait for this slot's accumulator; false (for the whole group) on abort.
+        auto wait_acc = [&]() -> bool {
+            if (leader) {
+                const bool ok = mbar_wait(&acc_full[slot], acc_phase) && !*s_abort;
+                if (!ok) *s_abort = 1;
+                s_ok[slot] = ok ? 1 : 0;
+            }
+            acc_phase ^= 1u;
+            wg_sync(slot);
+            const bool ok = s_ok[slot] != 0;
+            umma::fence_after_sync();
+            return ok;
+        };
+        for (int64_t p = 0; p < n_pairs; ++p) {
+            const int64_t t = 2 * p + slot;
+            const bool real = t < T;
+            const int64_t wk = w_begin + (real ? t : T - 1);
+            const int d = (int)(wk / n_tiles);
+            const int64_t tile = wk - (int64_t)d * n_tiles;
+            if (real && d != d_cur) {
+                flush(d_cur);
+                d_cur = d;
+            }
+            float x[6];
+            const float wrow = real ? fm(a, tile * 128 + r, n_seg, d, x) : (fm(a, n_seg, n_seg, d, x), 0.0f);
+            *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 0u, kInfSboX)) =
+                make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
+            *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 8u, kInfSboX)) = make_uint4(0u, 0u, 0u, 0u);
+            hand_over();
+            bool ok = true;
+            for (int layer = 0; layer < 4 && ok; ++layer) {
+                ok = wait_acc();
+                if (!ok) break;
+                const float *bias = sBias + layer * 256;
+                if (layer < 3) {
+                    for (int c0 = 0; c0 < 256; c0 += 16) {
+                        float v[16];
+                        umma::tmem_ld16(t_base + (uint32_t)c0, v);
+                        uint32_t pk[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                            pk[i] = pack_bf16x2(silu_fast(v[2 * i] + bias[c0 + 2 * i]),
+                                                silu_fast(v[2 * i + 1] + bias[c0 + 2 * i + 1]));
+                        *reinterpret_cast<uint4 *>(mH + umma::core_offset((uint32_t)r, (uint32_t)c0, kInfSboH)) =
+                            make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                        *reinterpret_cast<uint4 *>(mH + umma::core_offset((uint32_t)r, (uint32_t)c0 + 8u, kInfSboH)) =
+                            make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                    }
+                    hand_over();
+                } else {
+                    for (int c0 = 0; c0 < 256; c0 += 16) {
+                        float v[16];
+                        umma::tmem_ld16(t_base + (uint32_t)c0, v);
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) v[i] = wrow * silu_fast(v[i] + bias[c0 + i]);
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const bool up = lane & 16;
+                            const float send = up ? v[i] : v[i + 8], keep = up ? v[i + 8] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const bool up = lane & 8;
+                            const float send = up ? v[i] : v[i + 4], keep = up ? v[i + 4] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 2; ++i) {
+                            const bool up = lane & 4;
+                            const float send = up ? v[i] : v[i + 2], keep = up ? v[i + 2] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+                        }
+                        {
+                            const bool up = lane & 2;
+                            const float send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
+                            v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+                        }
+                        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+                        if ((lane & 1) == 0 && v[0] != 0.0f) atomicAdd(&hs[c0 + (lane >> 1)], v[0]);
+                    }
+                    float wsum = wrow;
+                    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+                    if (lane == 0 && wsum != 0.0f) atomicAdd(&hs[256], wsum);
+                    // Tensor-memory reads of this slot are complete before the
+                    // next tile's features are handed over (hand_over fences).
+                }
+            }
+            if (!ok) break;
+        }
+        flush(d_cur);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(taddr, 512);
+}
+
 // spec[d][o] += t_scale (sum_k W5[o][k] hsum[d][k] + b5[o] lsum[d]).
 __global__ void mlp_head_kernel(int n_dir, int n_out, const float *W5, const float *b5, const double *hsum,
                                 const double *lsum, double t_scale, double *spec) {
@@ -698,13 +981,21 @@ __global__ void pack_umma_kernel(int cols, int kc, const float *W, __nv_bfloat16
 }
 
 cudaError_t launch_mlp_infer(const pb_mlp_infer_args &a, cudaStream_t s, int sms) {
-    cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem);
-    if (e != cudaSuccess) return e;
     const int64_t work = (a.n_seg + 127) / 128 * (int64_t)a.n_dir;
     int64_t grid = sms;
     if (grid > work) grid = work;
     if (grid < 1) return cudaSuccess;
-    mlp_infer_kernel<<<(unsigned)grid, kInfThreads, kInfSmem, s>>>(a);
+    if (infer_variant() == 1) {
+        cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kInfSmem);
+        if (e != cudaSuccess) return e;
+        mlp_infer_kernel<<<(unsigned)grid, kInfThreads, kInfSmem, s>>>(a);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(mlp_infer_pp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kPPSmem);
+        if (e != cudaSuccess) return e;
+        mlp_infer_pp_kernel<<<(unsigned)grid, kPPThreads, kPPSmem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
