@@ -69,7 +69,7 @@ __device__ __forceinline__ Real b_mean_transmission(Real t0, Real t1) {
 }
 
 template <class Real>
-__global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
     // Segment chunk staged in shared memory (half as many FP64 segments, to
     // stay within the static shared-memory limit next to the accumulators).
