@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 1
+#define PB_ABI_VERSION 2
 
 enum pb_status {
     PB_OK = 0,
@@ -247,6 +247,28 @@ typedef struct pb_cxr_args {
     /* Optional, with the line buffer: segment index of every kept line
      * (surrogate training targets are binned per (segment, direction)). */
     int64_t *line_seg;
+    /* Layered absorber (cxr/_setup.py:1089 segment_escape_pieces with
+     * layers, cxr/_batched.py:702-720). n_layer = 0 keeps the single slab
+     * [0, thickness] and the log_mu escape rows. With 1 <= n_layer <= 4
+     * contiguous planar layers [z_top[k], z_bot[k]) in depth order (thickness
+     * = z_bot[n_layer-1]), each segment's escape is cut at the layer
+     * boundaries it crosses and layer k attenuates with the piecewise-linear
+     * mu_k(E) = mu_value[j] + (E - mu_knot[j]) mu_slope[j], 1/Angstrom at
+     * the line energy E in eV, over its knots j in [mu_off[k], mu_off[k+1])
+     * (j the last knot <= E, clipped to the table; 0 below the first knot),
+     * as cxr/_escape_mu.py:41-57 evaluates a layer's composition. */
+    int32_t n_layer;
+    const double *z_top;    /* [n_layer] Angstrom */
+    const double *z_bot;    /* [n_layer] */
+    const int32_t *mu_off;  /* [n_layer + 1] */
+    const double *mu_knot;  /* [mu_off[n_layer]] eV, ascending per layer */
+    const double *mu_value;
+    const double *mu_slope;
+    /* Optional emitting-layer filter (cxr/_kernels.py:768-778, one crystal
+     * layer of a stack per call): with seg_layer set, only segments whose
+     * layer equals emit_layer radiate. */
+    const int32_t *seg_layer;
+    int32_t emit_layer;
 } pb_cxr_args;
 
 typedef struct pb_brem_args {
@@ -267,6 +289,20 @@ typedef struct pb_brem_args {
     const double *mu;       /* [n_E] 1/Angstrom attenuation at the grid */
     double *spec;           /* [n_dir*n_E] accumulated (+=), not normalised */
     unsigned int *status;
+    /* Layered absorber (brem.py:978-1005, 1195-1200): n_layer = 0 keeps the
+     * single slab [0, thickness] with ``mu``; 1 <= n_layer <= 4 contiguous
+     * planar layers [z_top[k], z_bot[k]) (thickness = z_bot[n_layer-1]),
+     * each segment cut at the boundaries it crosses, layer k attenuating
+     * with mu_layer[k][e] at grid energy e. */
+    int32_t n_layer;
+    const double *z_top;    /* [n_layer] Angstrom */
+    const double *z_bot;    /* [n_layer] */
+    const double *mu_layer; /* [n_layer*n_E] 1/Angstrom */
+    /* Optional emitting-layer filter (emission.py:155-172: each layer
+     * radiates with its own composition Z/n_ang3): with seg_layer set, only
+     * segments whose layer equals emit_layer radiate. */
+    const int32_t *seg_layer;
+    int32_t emit_layer;
 } pb_brem_args;
 
 /* Characteristic lines of one emitting element: per-segment shell

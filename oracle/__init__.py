@@ -123,8 +123,44 @@ class _CxrTables(C.Structure):
     ]
 
 
+class _LayerEscape(C.Structure):
+    _fields_ = [
+        ("n_layer", C.c_int), ("z_top", _D), ("z_bot", _D), ("mu_off", _I32),
+        ("mu_knot", _D), ("mu_value", _D), ("mu_slope", _D),
+    ]
+
+
 class _CxrGeom(C.Structure):
-    _fields_ = [("n_hat", C.c_double * 3), ("thickness", C.c_double)]
+    _fields_ = [("n_hat", C.c_double * 3), ("thickness", C.c_double), ("layers", C.POINTER(_LayerEscape))]
+
+
+class LayerEscape:
+    """A planar layered absorber for the oracle: bounds [z_top, z_bot) per
+    layer and, for the CXR chain, each layer's piecewise-linear mu(E) as
+    (knots, values, slopes) (cxr/_escape_mu.py:41-57)."""
+
+    def __init__(self, z_top, z_bot, mu_tables=None):
+        self.z_top = _f64(z_top)
+        self.z_bot = _f64(z_bot)
+        n = int(self.z_top.size)
+        if mu_tables is None:
+            mu_tables = [(np.array([1.0]), np.zeros(1), np.zeros(1))] * n
+        self.mu_off = np.ascontiguousarray(np.cumsum([0] + [len(k) for k, _v, _s in mu_tables]), dtype=np.int32)
+        self.mu_knot = _f64(np.concatenate([k for k, _v, _s in mu_tables]))
+        self.mu_value = _f64(np.concatenate([v for _k, v, _s in mu_tables]))
+        self.mu_slope = _f64(np.concatenate([sl for _k, _v, sl in mu_tables]))
+        self.c = _LayerEscape(n, _p(self.z_top, _D), _p(self.z_bot, _D), _p(self.mu_off, _I32),
+                              _p(self.mu_knot, _D), _p(self.mu_value, _D), _p(self.mu_slope, _D))
+
+    def pieces(self, z0, z1, n_z):
+        """(fraction[P], path0[P, K], path1[P, K]) of one segment."""
+        K = int(self.z_top.size)
+        f = np.zeros(8)
+        p0 = np.zeros(64)
+        p1 = np.zeros(64)
+        P = lib().or_layer_pieces(float(z0), float(z1), C.byref(self.c), float(n_z), _p(f, _D), _p(p0, _D),
+                                  _p(p1, _D))
+        return f[:P].copy(), p0[:P * K].reshape(P, K).copy(), p1[:P * K].reshape(P, K).copy()
 
 
 def _declare(L):
@@ -167,6 +203,13 @@ def _declare(L):
     L.or_mean_transmission.argtypes = [C.c_double, C.c_double]
     L.or_quantum_line_factors.restype = None
     L.or_quantum_line_factors.argtypes = [C.c_double] * 10 + [_D, _D]
+    L.or_layer_pieces.restype = C.c_int
+    L.or_layer_pieces.argtypes = [C.c_double, C.c_double, C.POINTER(_LayerEscape), C.c_double, _D, _D, _D]
+    L.or_brem_spectrum_layered.restype = None
+    L.or_brem_spectrum_layered.argtypes = [
+        C.c_int64, _D, _D, _D, _D, C.c_int, _D, _D, C.POINTER(_LayerEscape), _D, C.c_int64, _D, _D, _D,
+        C.c_int,
+    ]
     L.or_brem_spectrum.restype = None
     L.or_brem_spectrum.argtypes = [
         C.c_int64, _D, _D, _D, _D, C.c_int, _D, _D, C.c_double, _D, C.c_int64, _D, _D, _D,
@@ -309,8 +352,9 @@ def transport(layers, pos, direction, E, *, seed, E_cut, rng=RNG_SPLITMIX,
 # ---------------------------------------------------------------------------
 # CXR line chain and reductions
 # ---------------------------------------------------------------------------
-def cxr_lines(tables: dict, n_hat, thickness, seg: dict, Ne):
-    """Line (E_res, a_width, weight, good) per (segment, row), segment-major."""
+def cxr_lines(tables: dict, n_hat, thickness, seg: dict, Ne, layers: LayerEscape | None = None):
+    """Line (E_res, a_width, weight, good) per (segment, row), segment-major.
+    ``layers``: a layered absorber (escape pieces with each layer's exact mu)."""
     G = _f64(tables["G"])
     ES, EP, WM = _f64(tables["ES"]), _f64(tables["EP"]), _f64(tables["WM"])
     row_table = np.ascontiguousarray(tables["row_table"], dtype=np.int32)
@@ -325,7 +369,8 @@ def cxr_lines(tables: dict, n_hat, thickness, seg: dict, Ne):
         _p(u_im, _D), int(log_mu.shape[0]), _p(log_mu, _D), _p(delta, _D),
         float(tables["lo_keep"]), float(tables["hi_keep"]),
     )
-    geo = _CxrGeom((C.c_double * 3)(*[float(v) for v in n_hat]), float(thickness))
+    geo = _CxrGeom((C.c_double * 3)(*[float(v) for v in n_hat]), float(thickness),
+                   C.pointer(layers.c) if layers is not None else None)
     v_hat = _f64(seg["v_hat"])
     E = _f64(seg["E_keV"])
     L = _f64(seg["L_ang"])
@@ -402,4 +447,23 @@ def brem_spectrum(seg: dict, Z, n_ang3, thickness, n_hat, E_grid, mu_grid, Ne):
     lib().or_brem_spectrum(E.size, _p(E, _D), _p(L, _D), _p(r, _D), _p(v, _D), int(Z.size),
                            _p(Z, _D), _p(n_ang3, _D), float(thickness), _p(nh, _D), E_grid.size,
                            _p(E_grid, _D), _p(mu_grid, _D), _p(spec, _D), 1)
+    return spec / (4.0 * np.pi) / Ne
+
+
+def brem_spectrum_layered(seg: dict, Z, n_ang3, layers: LayerEscape, n_hat, E_grid, mu_layer, Ne):
+    """Layered BH + Elwert spectrum of the given segments (one emitting
+    layer's composition Z/n_ang3; brem.py:978-1005,1195-1239)."""
+    E = _f64(seg["E_keV"])
+    L = _f64(seg["L_ang"])
+    r = _f64(seg["r_mid"])
+    v = _f64(seg["v_hat"])
+    Z = _f64(Z)
+    n_ang3 = _f64(n_ang3)
+    nh = _f64(n_hat)
+    E_grid = _f64(E_grid)
+    mu_layer = _f64(np.atleast_2d(mu_layer))
+    spec = np.zeros(E_grid.size)
+    lib().or_brem_spectrum_layered(E.size, _p(E, _D), _p(L, _D), _p(r, _D), _p(v, _D), int(Z.size), _p(Z, _D),
+                                   _p(n_ang3, _D), C.byref(layers.c), _p(nh, _D), E_grid.size, _p(E_grid, _D),
+                                   _p(mu_layer, _D), _p(spec, _D), 1)
     return spec / (4.0 * np.pi) / Ne

@@ -125,9 +125,20 @@ typedef struct {
     double lo_keep, hi_keep;
 } or_cxr_tables;
 
+/* Planar layered absorber (segment_escape.py:193-272): layers [z_top, z_bot)
+ * in depth order; mu_off/mu_knot/mu_value/mu_slope give each layer's exact
+ * piecewise-linear mu(E) (cxr/_escape_mu.py:41-57), used by the CXR chain. */
+typedef struct {
+    int n_layer;
+    const double *z_top, *z_bot;
+    const int *mu_off;
+    const double *mu_knot, *mu_value, *mu_slope;
+} or_layer_escape;
+
 typedef struct {
     double n_hat[3];
-    double thickness;  /* Angstrom; slab 0 <= z <= thickness */
+    double thickness;  /* Angstrom; slab 0 <= z <= thickness (stack: its total) */
+    const or_layer_escape *layers;  /* NULL: the single slab */
 } or_cxr_geom;
 
 /* One line per (segment, row): E_res [eV], a_width [1/eV], weight; good = 0
@@ -163,6 +174,19 @@ void or_brem_spectrum(int64_t n_seg, const double *E_keV, const double *L_ang,
                       const double *r_mid, const double *v_hat, int n_el, const double *Z,
                       const double *n_cm3, double thickness, const double n_hat[3], int64_t n_e,
                       const double *E_grid, const double *mu_grid, double *spec, int n_threads);
+
+/* Layered bremsstrahlung (brem.py:978-1005,1195-1239): segments cut into
+ * escape pieces, each piece attenuated by sum_k path_k mu_layer[k][e]. */
+void or_brem_spectrum_layered(int64_t n_seg, const double *E_keV, const double *L_ang,
+                              const double *r_mid, const double *v_hat, int n_el, const double *Z,
+                              const double *n_ang3, const or_layer_escape *layers, const double n_hat[3],
+                              int64_t n_e, const double *E_grid, const double *mu_layer, double *spec,
+                              int n_threads);
+
+/* Escape pieces of one segment (segment_escape.py:193-272 with layers):
+ * returns the piece count P (<= 8) and writes frac[P], path0[P*K], path1[P*K]. */
+int or_layer_pieces(double z0, double z1, const or_layer_escape *ly, double n_z, double *frac,
+                    double *path0, double *path1);
 
 #ifdef __cplusplus
 }

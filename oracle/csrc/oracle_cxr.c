@@ -101,6 +101,77 @@ static double slab_path(double z, double thickness, double nz) {
     return nz < 0 ? depth * inv_nz : (thickness - depth) * inv_nz;
 }
 
+/* attenuation.py:270-277: z-extent of layer [z_top, z_bot] crossed leaving depth z. */
+static double layer_dz(double z, double n_z, double z_top, double z_bot) {
+    if (n_z < 0) return fmax(fmin(z, z_bot) - z_top, 0.0);
+    return fmax(z_bot - fmax(z, z_top), 0.0);
+}
+
+/* segment_escape.py:134-140 */
+static double cut_at_zero(double start, double end) {
+    double den = start - end;
+    double fr = start / (den == 0.0 ? 1.0 : den);
+    return (fr > 0.0 && fr < 1.0) ? fr : 1.0;
+}
+
+#define OR_MAX_LAYERS 8
+
+/* segment_escape.py:193-272 (layers, no footprint): cut at the tops of
+ * layers 1..K-1, keep pieces wider than 1e-12, per-layer paths at the 1/4 and
+ * 3/4 points (segment_escape.py:59-70) extrapolated to the piece ends and
+ * clipped at zero. */
+int or_layer_pieces(double z0, double z1, const or_layer_escape *ly, double n_z, double *frac,
+                    double *path0, double *path1) {
+    const int K = ly->n_layer;
+    double cuts[OR_MAX_LAYERS + 1];
+    int nc = 0;
+    cuts[nc++] = 0.0;
+    cuts[nc++] = 1.0;
+    for (int k = 1; k < K; ++k) cuts[nc++] = cut_at_zero(z0 - ly->z_top[k], z1 - ly->z_top[k]);
+    for (int i = 1; i < nc; ++i) {  /* np.sort */
+        double v = cuts[i];
+        int j = i - 1;
+        while (j >= 0 && cuts[j] > v) { cuts[j + 1] = cuts[j]; --j; }
+        cuts[j + 1] = v;
+    }
+    const double inv_nz = 1.0 / fmax(fabs(n_z), 1.0e-12);
+    int P = 0;
+    for (int i = 0; i + 1 < nc; ++i) {
+        double w = cuts[i + 1] - cuts[i];
+        if (!(w > 1.0e-12)) continue;
+        double left = cuts[i];
+        double delta = z1 - z0;
+        double zq = z0 + (left + 0.25 * w) * delta;
+        double z3 = z0 + (left + 0.75 * w) * delta;
+        frac[P] = w;
+        for (int k = 0; k < K; ++k) {
+            double q = layer_dz(zq, n_z, ly->z_top[k], ly->z_bot[k]) * inv_nz;
+            double tq = layer_dz(z3, n_z, ly->z_top[k], ly->z_bot[k]) * inv_nz;
+            path0[P * K + k] = fmax(1.5 * q - 0.5 * tq, 0.0);
+            path1[P * K + k] = fmax(1.5 * tq - 0.5 * q, 0.0);
+        }
+        ++P;
+    }
+    return P;
+}
+
+/* cxr/_escape_mu.py:49-57 */
+static double exact_mu(const or_layer_escape *ly, int k, double E) {
+    const int o = ly->mu_off[k], n = ly->mu_off[k + 1] - o;
+    const double *kn = ly->mu_knot + o;
+    int lo = 0, hi = n;
+    while (lo < hi) {  /* searchsorted(..., side="right") */
+        int mid = (lo + hi) / 2;
+        if (kn[mid] <= E) lo = mid + 1; else hi = mid;
+    }
+    int j = lo - 1;
+    if (j < 0) j = 0;
+    if (j > n - 1) j = n - 1;
+    double mu = ly->mu_value[o + j] + (E - kn[j]) * ly->mu_slope[o + j];
+    if (E < kn[0]) mu = 0.0;
+    return mu;
+}
+
 void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
                   const double *v_hat, const double *E_keV, const double *L_ang,
                   const double *r_mid, const int64_t *elec_id, int64_t Ne, double *E_res_out,
@@ -129,6 +200,11 @@ void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
         const double z_mid = r_mid[3 * s + 2];
         const double path0 = slab_path(z_mid - half * vhz, T, nz);
         const double path1 = slab_path(z_mid + half * vhz, T, nz);
+        /* layered absorber: linear escape pieces (cxr/_setup.py:1089) */
+        const or_layer_escape *ly = geo->layers;
+        double pf[OR_MAX_LAYERS], pp0[OR_MAX_LAYERS * OR_MAX_LAYERS], pp1[OR_MAX_LAYERS * OR_MAX_LAYERS];
+        int n_piece = 0;
+        if (ly) n_piece = or_layer_pieces(z_mid - half * vhz, z_mid + half * vhz, ly, nz, pf, pp0, pp1);
         /* segment_escape.py:95-131: grad L = -z_hat / (z_hat . n), zero outside */
         double gx = -0.0 / nz, gy = -0.0 / nz, gz = -1.0 / nz;
         if (z_mid < 0.0 || z_mid > T) { gx = 0.0; gy = 0.0; gz = 0.0; }
@@ -217,7 +293,24 @@ void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
                 A2 = pol == 0 ? a2 : A2 + a2;
             }
             /* cxr/_batched.py:702-730 + cxr/_kernels.py:658-668 */
-            const double T_abs = or_mean_transmission(path0 * mu, path1 * mu);
+            double T_abs;
+            if (!ly) {
+                T_abs = or_mean_transmission(path0 * mu, path1 * mu);
+            } else {
+                /* piece_mean_transmission (segment_escape.py:335-355) with the
+                 * exact per-layer mu at E_res (cxr/_batched.py:714-720) */
+                double mu_k[OR_MAX_LAYERS];
+                for (int k = 0; k < ly->n_layer; ++k) mu_k[k] = exact_mu(ly, k, E_res);
+                T_abs = 0.0;
+                for (int p = 0; p < n_piece; ++p) {
+                    double t0 = 0.0, t1 = 0.0;
+                    for (int k = 0; k < ly->n_layer; ++k) {
+                        t0 += pp0[p * ly->n_layer + k] * mu_k[k];
+                        t1 += pp1[p * ly->n_layer + k] * mu_k[k];
+                    }
+                    T_abs += pf[p] * or_mean_transmission(t0, t1);
+                }
+            }
             const double pref = ALPHA_FS * omega / pref_c1 * (t_L * t_L) * T_abs;
             const double a_width = slope * t_L / (2.0 * HBARC_EV_ANG) * 1.0;
             const double weight = pref * A2 * t->WM[g];
@@ -373,6 +466,41 @@ void or_brem_spectrum(int64_t n_seg, const double *E_keV, const double *L_ang,
             for (int el = 0; el < n_el; ++el) {
                 double d = brem_dsigma_dk(E_keV[s], k, Z[el]);
                 acc += (n_ang3[el] * 1e24 * 1.0 * path_cm) * (d * T_abs);
+            }
+        }
+        spec[e] += acc;
+    }
+}
+
+void or_brem_spectrum_layered(int64_t n_seg, const double *E_keV, const double *L_ang,
+                              const double *r_mid, const double *v_hat, int n_el, const double *Z,
+                              const double *n_ang3, const or_layer_escape *ly, const double n_hat[3],
+                              int64_t n_e, const double *E_grid, const double *mu_layer, double *spec,
+                              int n_threads) {
+    const int K = ly->n_layer;
+#pragma omp parallel for schedule(static) num_threads(n_threads > 0 ? n_threads : 1)
+    for (int64_t e = 0; e < n_e; ++e) {
+        const double k = E_grid[e] / 1e3;
+        double acc = 0.0;
+        for (int64_t s = 0; s < n_seg; ++s) {
+            const double half = 0.5 * L_ang[s];
+            const double z = r_mid[3 * s + 2];
+            double pf[OR_MAX_LAYERS], p0[OR_MAX_LAYERS * OR_MAX_LAYERS], p1[OR_MAX_LAYERS * OR_MAX_LAYERS];
+            const int P = or_layer_pieces(z - half * v_hat[3 * s + 2], z + half * v_hat[3 * s + 2], ly, n_hat[2],
+                                          pf, p0, p1);
+            for (int p = 0; p < P; ++p) {
+                /* _layer_depth (brem.py:814-820): fixed layer order */
+                double t0 = p0[p * K] * mu_layer[e], t1 = p1[p * K] * mu_layer[e];
+                for (int kk = 1; kk < K; ++kk) {
+                    t0 = t0 + p0[p * K + kk] * mu_layer[(int64_t)kk * n_e + e];
+                    t1 = t1 + p1[p * K + kk] * mu_layer[(int64_t)kk * n_e + e];
+                }
+                const double T_abs = or_mean_transmission(t0, t1);
+                const double path_cm = (L_ang[s] * pf[p]) * 1e-8;
+                for (int el = 0; el < n_el; ++el) {
+                    double d = brem_dsigma_dk(E_keV[s], k, Z[el]);
+                    acc += (n_ang3[el] * 1e24 * 1.0 * path_cm) * (d * T_abs);
+                }
             }
         }
         spec[e] += acc;

@@ -102,6 +102,8 @@ class PbCxrArgs(C.Structure):
         ("line_capacity", _i64), ("line_count", _vp), ("line_E", _vp), ("line_a", _vp),
         ("line_w", _vp), ("line_dir", _vp), ("pair_E", _vp), ("pair_a", _vp), ("pair_w", _vp),
         ("pair_good", _vp), ("status", _vp), ("line_seg", _vp),
+        ("n_layer", _i32), ("z_top", _vp), ("z_bot", _vp), ("mu_off", _vp), ("mu_knot", _vp),
+        ("mu_value", _vp), ("mu_slope", _vp), ("seg_layer", _vp), ("emit_layer", _i32),
     ]
 
 
@@ -111,6 +113,8 @@ class PbBremArgs(C.Structure):
         ("n_seg", _i64), ("r_mid", _vp), ("v_hat", _vp), ("L", _vp), ("E_keV", _vp),
         ("elec_id", _vp), ("n_seg_device", _vp), ("n_el", _i32), ("Z", _vp), ("n_ang3", _vp),
         ("n_E", _i32), ("E_grid", _vp), ("mu", _vp), ("spec", _vp), ("status", _vp),
+        ("n_layer", _i32), ("z_top", _vp), ("z_bot", _vp), ("mu_layer", _vp), ("seg_layer", _vp),
+        ("emit_layer", _i32),
     ]
 
 
@@ -174,6 +178,9 @@ class PyriteB200Error(RuntimeError):
     """A pyrite_b200 C-ABI call returned a non-zero status."""
 
 
+ABI_VERSION = 2  # PB_ABI_VERSION of include/pyrite_b200.h
+
+
 def load(path: Path | None = None):
     """Load the shared library (once); raise if it has not been built."""
     global _lib
@@ -186,6 +193,10 @@ def load(path: Path | None = None):
         )
     lib = C.CDLL(str(p))
     lib.pb_abi_version.restype = C.c_int
+    if lib.pb_abi_version() != ABI_VERSION:
+        raise PyriteB200Error(
+            f"{p} has ABI {lib.pb_abi_version()}, this binding expects {ABI_VERSION}: rebuild it"
+        )
     lib.pb_last_error.restype = C.c_char_p
     lib.pb_device_count.argtypes = [C.POINTER(C.c_int)]
     lib.pb_transport.argtypes = [C.POINTER(PbTransportArgs), _vp]

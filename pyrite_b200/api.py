@@ -314,6 +314,29 @@ def _segments_on_device(h: _Holder, segments: dict):
     return out
 
 
+MAX_ESCAPE_LAYERS = 4
+
+
+def _escape_layers(layers):
+    """(z_top, z_bot) of a layered absorber given as the reference's
+    ``layers`` list of (z_top, z_bot, composition); contiguous, in depth
+    order, at most MAX_ESCAPE_LAYERS."""
+    z_top = np.array([float(l[0]) for l in layers])
+    z_bot = np.array([float(l[1]) for l in layers])
+    if not 1 <= z_top.size <= MAX_ESCAPE_LAYERS:
+        raise ValueError(f"layered escape supports 1..{MAX_ESCAPE_LAYERS} layers, got {z_top.size}")
+    if np.any(z_bot <= z_top) or np.any(np.abs(z_bot[:-1] - z_top[1:]) > 1e-9 * np.maximum(1.0, np.abs(z_bot[:-1]))):
+        raise ValueError("layers must be contiguous [z_top, z_bot) intervals in depth order")
+    return z_top, z_bot
+
+
+def _seg_layer(h: _Holder, segments: dict, emit_layer):
+    if emit_layer is None:
+        return None
+    lay = segments["layer"]
+    return h.typed(lay if torch.is_tensor(lay) else np.asarray(lay, dtype=np.int32), torch.int32)
+
+
 def _fill_tables(h: _Holder, rows, tables: LineTables, lo_keep, hi_keep, d_index=None):
     t = L.PbCxrTables()
     t.n_g = int(rows.G.shape[0])
@@ -337,13 +360,21 @@ def _fill_tables(h: _Holder, rows, tables: LineTables, lo_keep, hi_keep, d_index
 def mc_cxr_spectrum(segments, E_grid_eV, crystal, hkl_list, *, tables: LineTables, n_hat,
                     surface_hkl=None, beam_uvw=None, azimuth_rad=0.0, mosaic_fwhm_rad=None,
                     mosaic_nodes=1, line_quadrature="node", precision="fp64", exact_widths=None,
-                    rows=None, return_pairs=False, device=None, stream=None):
+                    rows=None, return_pairs=False, layers=None, mu_tables=None, emit_layer=None,
+                    device=None, stream=None):
     """Per-electron incoherent PXR + CBS density [photons/eV/sr/electron].
 
     ``n_hat`` is one direction (3,) or several (n_dir, 3); the result is then
     (n_dir, n_E). ``exact_widths`` (bin-mean) keeps exact bin integrals within
     that many sinc widths of each line and the far envelope beyond; None is
     exact everywhere.
+
+    ``layers`` (the reference's list of (z_top, z_bot, composition)) makes the
+    escape run through a layered absorber, with ``mu_tables`` one
+    (knots [eV], values, slopes [per eV]) piecewise-linear attenuation per
+    layer (cxr/_escape_mu.py:41-57); ``emit_layer`` keeps only the segments
+    of that layer (``segments["layer"]``) radiating, as the reference scores
+    each crystalline layer of a stack (runner/case_driver.py:742-770).
     """
     dev = _device(device)
     lib = L.load()
@@ -383,6 +414,19 @@ def mc_cxr_spectrum(segments, E_grid_eV, crystal, hkl_list, *, tables: LineTable
         t.ES = _ptr(h.f64(rows.ES[d]))
         t.EP = _ptr(h.f64(rows.EP[d]))
         a.tables = t
+        if layers is not None:
+            z_top, z_bot = _escape_layers(layers)
+            if mu_tables is None or len(mu_tables) != z_top.size:
+                raise ValueError("a layered absorber needs one mu table per layer")
+            a.n_layer = int(z_top.size)
+            a.z_top, a.z_bot = _ptr(h.f64(z_top)), _ptr(h.f64(z_bot))
+            a.mu_off = _ptr(h.typed(np.cumsum([0] + [len(k) for k, _v, _s in mu_tables]).astype(np.int32), torch.int32))
+            a.mu_knot = _ptr(h.f64(np.concatenate([np.asarray(k, float) for k, _v, _s in mu_tables])))
+            a.mu_value = _ptr(h.f64(np.concatenate([np.asarray(v, float) for _k, v, _s in mu_tables])))
+            a.mu_slope = _ptr(h.f64(np.concatenate([np.asarray(sl, float) for _k, _v, sl in mu_tables])))
+        sl_t = _seg_layer(h, segments, emit_layer)
+        if sl_t is not None:
+            a.seg_layer, a.emit_layer = _ptr(sl_t), int(emit_layer)
         a.n_E = n_E
         a.E_grid = _ptr(h.f64(E_grid))
         spec_d = h.zeros(n_E, torch.float64)
@@ -425,12 +469,17 @@ def mc_cxr_spectrum(segments, E_grid_eV, crystal, hkl_list, *, tables: LineTable
     return result
 
 
-def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu, precision="fp64",
-                     device=None, stream=None):
+def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu=None, precision="fp64",
+                     layers=None, mu_layer=None, emit_layer=None, device=None, stream=None):
     """Bethe-Heitler + Elwert continuum density [photons/eV/sr/electron].
 
     ``mu`` is the absorber's total attenuation [1/Angstrom] on ``E_grid_eV``
     (the reference reads EPDL, brem.py:961-963; the tables are an input here).
+    ``layers`` (the reference's list of (z_top, z_bot, composition)) with
+    ``mu_layer`` [n_layer, n_E] makes the escape run through a layered
+    absorber (brem.py:978-1005); ``composition`` is then the emitting layer's
+    and ``emit_layer`` keeps only that layer's segments radiating
+    (runner/emission.py:155-172).
     """
     from .tables import ELEMENTS
 
@@ -457,7 +506,21 @@ def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu, precision="
     a.n_ang3 = _ptr(h.f64([float(n) for _, n in composition]))
     a.n_E = n_E
     a.E_grid = _ptr(h.f64(E_grid))
-    a.mu = _ptr(h.f64(mu))
+    if layers is None:
+        if mu is None:
+            raise ValueError("a single slab needs mu")
+        a.mu = _ptr(h.f64(mu))
+    else:
+        z_top, z_bot = _escape_layers(layers)
+        ml = np.atleast_2d(np.asarray(mu_layer, dtype=np.float64))
+        if ml.shape != (z_top.size, n_E):
+            raise ValueError(f"mu_layer must be [{z_top.size}, {n_E}]")
+        a.n_layer = int(z_top.size)
+        a.z_top, a.z_bot = _ptr(h.f64(z_top)), _ptr(h.f64(z_bot))
+        a.mu_layer = _ptr(h.f64(ml))
+    sl_t = _seg_layer(h, segments, emit_layer)
+    if sl_t is not None:
+        a.seg_layer, a.emit_layer = _ptr(sl_t), int(emit_layer)
     spec = h.zeros((n_dir, n_E), torch.float64)
     a.spec = _ptr(spec)
     a.status = _ptr(h.zeros(1, torch.int32))

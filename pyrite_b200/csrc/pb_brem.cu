@@ -18,6 +18,7 @@
 
 #include "pb_common.cuh"
 #include "pb_internal.h"
+#include "pb_layers.cuh"
 
 namespace pb {
 
@@ -66,6 +67,63 @@ __device__ __forceinline__ Real b_mean_transmission(Real t0, Real t1) {
     const Real safe = d > (Real)1.0e-4 ? d : (Real)1;
     const Real ratio = d > (Real)1.0e-4 ? -b_expm1(-safe) / safe : (Real)1 - (Real)0.5 * d + d * d / (Real)6;
     return b_exp(-lo) * ratio;
+}
+
+// Stage one segment's energy-independent parts.
+template <class Real>
+__device__ __forceinline__ void brem_stage(BremSeg<Real> &b, const pb_brem_args &a, int64_t s, Real T_slab,
+                                           Real mc2, Real za) {
+    const Real T = (Real)a.E_keV[s];
+    b.T = T;
+    const Real p_i = b_sqrt(T * (T + (Real)2 * mc2)) / mc2;
+    b.p_i = p_i;
+    b.beta_i = p_i / ((Real)1 + T / mc2);
+    const Real half = (Real)0.5 * (Real)a.L[s];
+    const Real z = (Real)a.r_mid[3 * s + 2];
+    const Real vz = (Real)a.v_hat[3 * s + 2];
+    // Depth of each segment end below the top face, clipped to the slab;
+    // the escape path toward n is depth/|n_z| (up) or (T - depth)/|n_z|.
+    b.path0 = fmin(fmax(z - half * vz, (Real)0), T_slab);
+    b.path1 = fmin(fmax(z + half * vz, (Real)0), T_slab);
+    const bool rad = a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
+    const Real path_cm = (Real)a.L[s] * (Real)1e-8;
+    for (int el = 0; el < a.n_el; ++el) {
+        b.nL[el] = rad ? (Real)(a.n_ang3[el] * 1e24) * (Real)1 * path_cm : (Real)0;
+        b.den_i[el] = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
+    }
+}
+
+// sum_el n_el L dsigma/dk(Z_el, T, k) of one staged segment (brem.py:396-479).
+template <class Real>
+__device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T_f, const Real *Zs, int n_el,
+                                          Real k_ev, Real c0, Real za, Real mc2) {
+    Real nsig = 0;
+    if constexpr (sizeof(Real) == 8) {
+        const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
+        const Real beta_f = p_f / ((Real)1 + T_f / mc2);
+        const Real born_log = b_log((b.p_i + p_f) / fmax(b.p_i - p_f, (Real)1e-30));
+        for (int el = 0; el < n_el; ++el) {
+            const Real Z = Zs[el];
+            const Real elwert = b.beta_i / beta_f * b.den_i[el] / ((Real)1 - b_exp(-za * Z / beta_f));
+            const Real dsig = c0 * (Z * Z) / k_ev / (b.p_i * b.p_i) * born_log * elwert;
+            nsig += b.nL[el] * dsig;
+        }
+    } else {
+        const float inv_mc2 = 1.0f / 510.99895f;
+        const float q = T_f * (T_f + 2.0f * mc2);
+        const float p_f = q * rsqrtf(q) * inv_mc2;
+        const float beta_f = __fdividef(p_f, 1.0f + T_f * inv_mc2);
+        const float diff = __fdividef(k * (b.T + T_f + 2.0f * mc2) * inv_mc2 * inv_mc2, b.p_i + p_f);
+        const float born_log = __logf(__fdividef(b.p_i + p_f, fmaxf(diff, 1e-30f)));
+        const float inv_beta_f = __fdividef(1.0f, beta_f);
+        const float common = __fdividef(c0, k_ev * b.p_i * b.p_i) * born_log * b.beta_i * inv_beta_f;
+        for (int el = 0; el < n_el; ++el) {
+            const float Z = Zs[el];
+            const float den_f = 1.0f - __expf(-za * Z * inv_beta_f);
+            nsig += b.nL[el] * (Z * Z) * common * __fdividef(b.den_i[el], den_f);
+        }
+    }
+    return nsig;
 }
 
 template <class Real>
@@ -134,26 +192,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         const int nc = (int)((s_end - c0s) < kChunk ? (s_end - c0s) : kChunk);
         __syncthreads();
         for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-            const int64_t s = c0s + j;
-            BremSeg<Real> &b = segs[j];
-            const Real T = (Real)a.E_keV[s];
-            b.T = T;
-            const Real p_i = b_sqrt(T * (T + (Real)2 * mc2)) / mc2;
-            b.p_i = p_i;
-            b.beta_i = p_i / ((Real)1 + T / mc2);
-            const Real half = (Real)0.5 * (Real)a.L[s];
-            const Real z = (Real)a.r_mid[3 * s + 2];
-            const Real vz = (Real)a.v_hat[3 * s + 2];
-            // Depth of each segment end below the top face, clipped to the slab;
-            // the escape path toward n is depth/|n_z| (up) or (T - depth)/|n_z|.
-            b.path0 = fmin(fmax(z - half * vz, (Real)0), T_slab);
-            b.path1 = fmin(fmax(z + half * vz, (Real)0), T_slab);
-            const bool rad = a.elec_id[s] < a.Ne;
-            const Real path_cm = (Real)a.L[s] * (Real)1e-8;
-            for (int el = 0; el < n_el; ++el) {
-                b.nL[el] = rad ? (Real)(a.n_ang3[el] * 1e24) * (Real)1 * path_cm : (Real)0;
-                b.den_i[el] = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
-            }
+            brem_stage<Real>(segs[j], a, c0s + j, T_slab, mc2, za);
         }
         __syncthreads();
         if (!on) continue;
@@ -166,32 +205,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
             const BremSeg<Real> &b = segs[j];
             const Real T_f = b.T - k;
             if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-            Real nsig = 0;  // sum_el n_el L dsigma/dk
-            if constexpr (sizeof(Real) == 8) {
-                const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
-                const Real beta_f = p_f / ((Real)1 + T_f / mc2);
-                const Real born_log = b_log((b.p_i + p_f) / fmax(b.p_i - p_f, (Real)1e-30));
-                for (int el = 0; el < n_el; ++el) {
-                    const Real Z = Zs[el];
-                    const Real elwert = b.beta_i / beta_f * b.den_i[el] / ((Real)1 - b_exp(-za * Z / beta_f));
-                    const Real dsig = c0 * (Z * Z) / k_ev / (b.p_i * b.p_i) * born_log * elwert;
-                    nsig += b.nL[el] * dsig;
-                }
-            } else {
-                const float inv_mc2 = 1.0f / 510.99895f;
-                const float q = T_f * (T_f + 2.0f * mc2);
-                const float p_f = q * rsqrtf(q) * inv_mc2;
-                const float beta_f = __fdividef(p_f, 1.0f + T_f * inv_mc2);
-                const float diff = __fdividef(k * (b.T + T_f + 2.0f * mc2) * inv_mc2 * inv_mc2, b.p_i + p_f);
-                const float born_log = __logf(__fdividef(b.p_i + p_f, fmaxf(diff, 1e-30f)));
-                const float inv_beta_f = __fdividef(1.0f, beta_f);
-                const float common = __fdividef(c0, k_ev * b.p_i * b.p_i) * born_log * b.beta_i * inv_beta_f;
-                for (int el = 0; el < n_el; ++el) {
-                    const float Z = Zs[el];
-                    const float den_f = 1.0f - __expf(-za * Z * inv_beta_f);
-                    nsig += b.nL[el] * (Z * Z) * common * __fdividef(b.den_i[el], den_f);
-                }
-            }
+            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2);
             if constexpr (sizeof(Real) == 8) {
 #pragma unroll
                 for (int dd = 0; dd < kBremMaxDir; ++dd) {
@@ -269,8 +283,181 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     }
 }
 
+// Layered absorber: each staged segment also carries its escape pieces
+// (pb_layers.cuh); per photon energy a thread holds every layer's mu and the
+// whole-layer optical depths above and below each layer, so a piece's end
+// depths cost one FMA each and its transmission the reference's closed form
+// (brem.py:1195-1200, segment_escape.py:276-289), weighted by its fraction.
+template <class Real>
+struct BremPieces {
+    int np;
+    int m[kMaxEscLayers];
+    Real f[kMaxEscLayers], u0[kMaxEscLayers], u1[kMaxEscLayers];
+};
+
+constexpr int kBremChunkLayered = 64;
+
+template <class Real>
+__global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
+    constexpr int kChunk = kBremChunkLayered;
+    __shared__ BremSeg<Real> segs[kChunk];
+    __shared__ BremPieces<Real> pcs[kChunk];
+    __shared__ double acc[kBremMaxDir][kBremThreads];
+    __shared__ Real Zs[kBremMaxEl];
+    __shared__ Real inv_nz[kBremMaxDir];
+    __shared__ int up[kBremMaxDir];
+    __shared__ double zt_s[kMaxEscLayers], zb_s[kMaxEscLayers];
+    __shared__ int bad;
+    const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
+    const int n_el = a.n_el;
+    const int nl = a.n_layer;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool on = e < a.n_E;
+    const Real mc2 = (Real)510.99895;
+    const Real za = (Real)(2.0 * kPi * kAlphaFs);
+    if (threadIdx.x < n_el) Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+    if (threadIdx.x < nd) {
+        const Real nz = (Real)a.n_hat[3 * (d0 + threadIdx.x) + 2];
+        inv_nz[threadIdx.x] = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
+        up[threadIdx.x] = nz < (Real)0;
+    }
+    if (threadIdx.x < nl) {
+        zt_s[threadIdx.x] = a.z_top[threadIdx.x];
+        zb_s[threadIdx.x] = a.z_bot[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+        // Contiguous layers in depth order, as the pieces assume.
+        int b = 0;
+        for (int k = 0; k < nl; ++k) {
+            if (!(a.z_bot[k] > a.z_top[k])) b = 1;
+            if (k + 1 < nl && fabs(a.z_bot[k] - a.z_top[k + 1]) > 1e-9 * fmax(1.0, fabs(a.z_bot[k]))) b = 1;
+        }
+        bad = b;
+        if (b && a.status) atomicOr(a.status, PB_DEV_BAD_INPUT);
+    }
+    __syncthreads();
+    if (bad) return;
+    // Per-energy layer attenuation and whole-layer depths above / below.
+    Real mu_l[kMaxEscLayers], t_l[kMaxEscLayers], c_up[kMaxEscLayers], c_dn[kMaxEscLayers];
+#pragma unroll
+    for (int k = 0; k < kMaxEscLayers; ++k) {
+        mu_l[k] = (k < nl && on) ? (Real)a.mu_layer[(int64_t)k * a.n_E + e] : (Real)0;
+        t_l[k] = k < nl ? (Real)(zb_s[k] - zt_s[k]) : (Real)0;
+    }
+    {
+        Real run = 0;
+#pragma unroll
+        for (int k = 0; k < kMaxEscLayers; ++k) {
+            c_up[k] = run;
+            run += mu_l[k] * t_l[k];
+        }
+        run = 0;
+#pragma unroll
+        for (int k = kMaxEscLayers - 1; k >= 0; --k) {
+            c_dn[k] = run;
+            run += mu_l[k] * t_l[k];
+        }
+    }
+    const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
+    const Real k = (Real)k_kev_d;
+    const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
+    const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
+#pragma unroll
+    for (int j = 0; j < kBremMaxDir; ++j) acc[j][threadIdx.x] = 0.0;
+    if (a.n_seg_device) {
+        const int64_t live = (int64_t)*a.n_seg_device;
+        if (live < n_seg) n_seg = live;
+    }
+    const int64_t per = (a.n_seg + gridDim.y - 1) / gridDim.y;
+    const int64_t s_begin = per * blockIdx.y;
+    int64_t s_end = s_begin + per < n_seg ? s_begin + per : n_seg;
+    if (s_end < s_begin) s_end = s_begin;
+    const Real T_stack = (Real)zb_s[nl - 1];
+    for (int64_t c0s = s_begin; c0s < s_end; c0s += kChunk) {
+        const int nc = (int)((s_end - c0s) < kChunk ? (s_end - c0s) : kChunk);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            const int64_t s = c0s + j;
+            brem_stage<Real>(segs[j], a, s, T_stack, mc2, za);
+            const double half = 0.5 * a.L[s];
+            const double z = a.r_mid[3 * s + 2], vz = a.v_hat[3 * s + 2];
+            EscPiece pp[kMaxEscLayers];
+            const int np = esc_pieces(z - half * vz, z + half * vz, nl, zt_s, zb_s, pp);
+            BremPieces<Real> &P = pcs[j];
+            P.np = np;
+            for (int p = 0; p < np; ++p) {
+                P.m[p] = pp[p].m;
+                P.f[p] = (Real)pp[p].f;
+                P.u0[p] = (Real)pp[p].u0;
+                P.u1[p] = (Real)pp[p].u1;
+            }
+        }
+        __syncthreads();
+        if (!on) continue;
+        Real part[kBremMaxDir];
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd) part[dd] = 0;
+        for (int j = 0; j < nc; ++j) {
+            const BremSeg<Real> &b = segs[j];
+            const Real T_f = b.T - k;
+            if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
+            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2);
+            const BremPieces<Real> &P = pcs[j];
+            for (int p = 0; p < P.np; ++p) {
+                const int m = P.m[p];
+                const Real mum = esc_pick<Real>(mu_l, m), tm = esc_pick<Real>(t_l, m);
+                const Real cu = esc_pick<Real>(c_up, m), cd = esc_pick<Real>(c_dn, m);
+                const Real up0 = cu + mum * P.u0[p], up1 = cu + mum * P.u1[p];
+                const Real dn0 = cd + mum * (tm - P.u0[p]), dn1 = cd + mum * (tm - P.u1[p]);
+                const Real w = nsig * P.f[p];
+#pragma unroll
+                for (int dd = 0; dd < kBremMaxDir; ++dd) {
+                    if (dd < nd) {
+                        const Real f = inv_nz[dd];
+                        const Real t0 = (up[dd] ? up0 : dn0) * f;
+                        const Real t1 = (up[dd] ? up1 : dn1) * f;
+                        part[dd] += w * b_mean_transmission<Real>(t0, t1);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd) acc[dd][threadIdx.x] += (double)part[dd];
+    }
+    if (on) {
+#pragma unroll
+        for (int dd = 0; dd < kBremMaxDir; ++dd)
+            if (dd < nd && acc[dd][threadIdx.x] != 0.0)
+                atomicAdd(&a.spec[(int64_t)(d0 + dd) * a.n_E + e], acc[dd][threadIdx.x]);
+    }
+}
+
 cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     if (a.n_el > kBremMaxEl || a.n_el < 1) return cudaErrorInvalidValue;
+    if (a.n_layer > 0) {
+        if (a.n_layer > kMaxEscLayers) return cudaErrorInvalidValue;
+        const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
+        int per_sm = 0;
+        cudaError_t oe = a.precision == PB_MIXED
+                             ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_layered_kernel<float>,
+                                                                             kBremThreads, 0)
+                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_layered_kernel<double>,
+                                                                             kBremThreads, 0);
+        if (oe != cudaSuccess) return oe;
+        if (per_sm < 1) per_sm = 1;
+        int64_t gy = (int64_t)sms * per_sm / (int64_t)gx;
+        const int64_t max_y = (a.n_seg + kBremChunkLayered - 1) / kBremChunkLayered;
+        if (gy > max_y) gy = max_y;
+        if (gy < 1) gy = 1;
+        dim3 grid(gx, (unsigned)gy, 1);
+        for (int d0 = 0; d0 < a.n_dir; d0 += kBremMaxDir) {
+            if (a.precision == PB_MIXED) brem_layered_kernel<float><<<grid, kBremThreads, 0, s>>>(a, a.n_seg, d0);
+            else brem_layered_kernel<double><<<grid, kBremThreads, 0, s>>>(a, a.n_seg, d0);
+            cudaError_t err = cudaGetLastError();
+            if (err != cudaSuccess) return err;
+        }
+        return cudaSuccess;
+    }
     int64_t n_seg = a.n_seg;
     const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
     // One wave: as many segment slices as keep every SM at its resident limit.

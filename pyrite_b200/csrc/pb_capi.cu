@@ -129,6 +129,10 @@ int pb_cxr_score(const pb_cxr_args *a, void *stream) {
     }
     if (a->line_E && (!a->line_count || a->line_capacity < 1))
         return fail(PB_ERR_INVALID, "pb_cxr_score: line buffer needs a count and a capacity");
+    if (a->n_layer < 0 || a->n_layer > 4)
+        return fail(PB_ERR_UNSUPPORTED, "pb_cxr_score: n_layer = %d outside [0, 4]", a->n_layer);
+    if (a->n_layer > 0 && (!a->z_top || !a->z_bot || !a->mu_off || !a->mu_knot || !a->mu_value || !a->mu_slope))
+        return fail(PB_ERR_INVALID, "pb_cxr_score: a layered absorber needs bounds and mu tables");
     cudaError_t e = pb::launch_cxr(*a, (cudaStream_t)stream, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_cxr_score: launch");
     return PB_OK;
@@ -140,8 +144,12 @@ int pb_brem_score(const pb_brem_args *a, void *stream) {
         return fail(PB_ERR_INVALID, "pb_brem_score: need n_seg >= 0, n_dir >= 1, n_E >= 1");
     if (a->n_seg == 0) return PB_OK;
     if (a->n_el < 1 || a->n_el > 4) return fail(PB_ERR_INVALID, "pb_brem_score: 1 <= n_el <= 4");
+    if (a->n_layer < 0 || a->n_layer > 4)
+        return fail(PB_ERR_UNSUPPORTED, "pb_brem_score: n_layer = %d outside [0, 4]", a->n_layer);
+    if (a->n_layer > 0 && (!a->z_top || !a->z_bot || !a->mu_layer))
+        return fail(PB_ERR_INVALID, "pb_brem_score: a layered absorber needs bounds and mu_layer");
     if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->Z ||
-        !a->n_ang3 || !a->E_grid || !a->mu || !a->spec)
+        !a->n_ang3 || !a->E_grid || (!a->mu && a->n_layer == 0) || !a->spec)
         return fail(PB_ERR_INVALID, "pb_brem_score: every pointer must be set");
     cudaError_t e = pb::launch_brem(*a, (cudaStream_t)stream, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_brem_score: launch");

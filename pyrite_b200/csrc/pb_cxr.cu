@@ -33,6 +33,7 @@
 
 #include "pb_common.cuh"
 #include "pb_internal.h"
+#include "pb_layers.cuh"
 
 namespace pb {
 
@@ -124,7 +125,7 @@ __device__ void seg_precompute(SegPre<Real> &sp, const pb_cxr_args &a, int64_t s
     sp.grad2 = gx * gx + gy * gy + gz * gz;
     sp.v_dot_grad = sp.vx * gx + sp.vy * gy + sp.vz * gz;
     sp.inv_E = (Real)kHbarcEvAng / (gamma * (Real)kMeEv);
-    sp.radiates = a.elec_id[s] < a.Ne;
+    sp.radiates = a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
 }
 
 // searchsorted(grid, x, side="left") clipped to [1, n-1] and the blend
@@ -225,6 +226,77 @@ __device__ __forceinline__ Real mean_transmission(Real t0, Real t1) {
     }
 }
 
+// Layered escape of one (segment, direction): its pieces (pb_layers.cuh)
+// with the exit-side depth inside the piece's layer at both ends, already
+// divided by |n_z|.
+template <class Real>
+struct EscSeg {
+    int np;
+    int up;                 // exits through the entrance face (n_z < 0)
+    Real inv_nz;
+    int m[kMaxEscLayers];
+    Real f[kMaxEscLayers], w0[kMaxEscLayers], w1[kMaxEscLayers];
+};
+
+template <class Real>
+__device__ void esc_precompute(EscSeg<Real> &es, const pb_cxr_args &a, int64_t s, const double *nh,
+                               const double *zt, const double *zb) {
+    const double nz = nh[2];
+    const double inv_nz = 1.0 / fmax(fabs(nz), 1.0e-12);
+    const double half = 0.5 * a.L[s];
+    const double z = a.r_mid[3 * s + 2], vz = a.v_hat[3 * s + 2];
+    EscPiece pp[kMaxEscLayers];
+    const int np = esc_pieces(z - half * vz, z + half * vz, a.n_layer, zt, zb, pp);
+    es.np = np;
+    es.up = nz < 0.0;
+    es.inv_nz = (Real)inv_nz;
+    for (int p = 0; p < np; ++p) {
+        const double t = zb[pp[p].m] - zt[pp[p].m];
+        es.m[p] = pp[p].m;
+        es.f[p] = (Real)pp[p].f;
+        es.w0[p] = (Real)((nz < 0.0 ? pp[p].u0 : t - pp[p].u0) * inv_nz);
+        es.w1[p] = (Real)((nz < 0.0 ? pp[p].u1 : t - pp[p].u1) * inv_nz);
+    }
+}
+
+// piece_mean_transmission (segment_escape.py:335-355) with every layer's
+// exact mu at the line energy (cxr/_batched.py:702-720): the layers between
+// a piece's layer and the exit face are crossed whole.
+template <class Real>
+__device__ Real esc_transmission(const EscSeg<Real> &es, const pb_cxr_args &a, const Real *lay_t, double E_eV) {
+    Real mu[kMaxEscLayers], c[kMaxEscLayers];
+    const int nl = a.n_layer;
+#pragma unroll
+    for (int k = 0; k < kMaxEscLayers; ++k) {
+        mu[k] = 0;
+        if (k < nl) {
+            const int o = a.mu_off[k];
+            mu[k] = (Real)esc_mu_at(a.mu_knot + o, a.mu_value + o, a.mu_slope + o, a.mu_off[k + 1] - o, E_eV);
+        }
+    }
+    Real run = 0;
+    if (es.up) {
+#pragma unroll
+        for (int k = 0; k < kMaxEscLayers; ++k) {
+            c[k] = run;
+            if (k < nl) run += mu[k] * lay_t[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = kMaxEscLayers - 1; k >= 0; --k) {
+            c[k] = run;
+            if (k < nl) run += mu[k] * lay_t[k];
+        }
+    }
+    Real T = 0;
+    for (int p = 0; p < es.np; ++p) {
+        const int m = es.m[p];
+        const Real mm = esc_pick<Real>(mu, m), cm = esc_pick<Real>(c, m) * es.inv_nz;
+        T += es.f[p] * mean_transmission<Real>(cm + mm * es.w0[p], cm + mm * es.w1[p]);
+    }
+    return T;
+}
+
 template <class Real>
 struct Line {
     Real E_res, a_width, weight;
@@ -257,10 +329,11 @@ __device__ __forceinline__ bool pair_may_keep(const SegPre<Real> &sp, const RowP
 
 // The per-pair chain. ``E_tab``/``delta_tab``/``log_mu`` point at the
 // shared-memory staging (or global memory for a large FP64 grid).
-template <class Real>
+template <class Real, bool kLayered>
 __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
                                 const Real *E_tab, const Real *delta_tab, const Real *log_mu,
-                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti) {
+                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti,
+                                const EscSeg<Real> *es, const pb_cxr_args &a, const Real *lay_t) {
     const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
     const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
     const Real hbarc = (Real)kHbarcEvAng;
@@ -333,7 +406,7 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
     const Real u_re = gather<Real>(t.u_re + base, n_tab, ix, fr, bl, ab);
     const Real u_im = gather<Real>(t.u_im + base, n_tab, ix, fr, bl, ab);
     Real mu = 0;
-    for (int el = 0; el < n_mu; ++el) {
+    for (int el = 0; el < (kLayered ? 0 : n_mu); ++el) {
         const Real *lm = log_mu + (int64_t)el * n_tab;
         const Real f0 = lm[ix - 1];
         Real v = r_exp(f0 + lfr * (lm[ix] - f0));
@@ -361,7 +434,9 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
         A2 = pol == 0 ? a2 : A2 + a2;
     }
     // cxr/_batched.py:702-730, cxr/_kernels.py:658-668
-    const Real T_abs = mean_transmission<Real>(sp.path0 * mu, sp.path1 * mu);
+    Real T_abs;
+    if constexpr (kLayered) T_abs = esc_transmission<Real>(*es, a, lay_t, (double)E_res);
+    else T_abs = mean_transmission<Real>(sp.path0 * mu, sp.path1 * mu);
     const Real pref_c1 = (Real)(4.0 * (kPi * kPi) * kHbarcEvAng);
     const Real pref = rdiv((Real)kAlphaFs * omega, pref_c1) * (sp.t_L * sp.t_L) * T_abs;
     out.a_width = rdiv(slope * sp.t_L, (Real)2 * hbarc) * (Real)1;
@@ -922,7 +997,7 @@ __device__ __forceinline__ void line_moments(double E_r, double a, double w, con
 //       onto a second shared queue;
 //   B   the queued lines' (line, bin) work is cut into 4-item chunks spread
 //       over the block; edges shared by consecutive bins are evaluated once.
-template <class Real>
+template <class Real, bool kLayered>
 __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool kMixed = sizeof(Real) == 4;
@@ -966,6 +1041,13 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     const int n_mom = n_E + 2 * far_pad;
     float *spec_f = reinterpret_cast<float *>(mom_s + (K_far > 0 ? 3 * n_mom : 0));
     float *edges_f = spec_f + (binmean ? n_E : 0);  // mixed path: float bin edges
+    // Layered absorber: per-segment escape pieces, layer thicknesses and bounds.
+    unsigned char *esc_raw = reinterpret_cast<unsigned char *>(edges_f + (binmean && kMixed ? n_E + 1 : 0));
+    esc_raw = (unsigned char *)(((uintptr_t)esc_raw + 15) & ~(uintptr_t)15);
+    EscSeg<Real> *esc = reinterpret_cast<EscSeg<Real> *>(esc_raw);
+    double *lay_zt = reinterpret_cast<double *>(esc + (kLayered ? kSegTile : 0));
+    double *lay_zb = lay_zt + (kLayered ? kMaxEscLayers : 0);
+    Real *lay_t = reinterpret_cast<Real *>(lay_zb + (kLayered ? kMaxEscLayers : 0));
     int &q_count = scratch[40];
     int &p_count = scratch[42];
     int *xq_count = scratch + 44;  // two counters
@@ -991,6 +1073,24 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
             for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
     if (tid == 0) { q_count = 0; p_count = 0; xq_count[0] = 0; xq_count[1] = 0; }
+    if constexpr (kLayered) {
+        if (tid < a.n_layer) {
+            lay_zt[tid] = a.z_top[tid];
+            lay_zb[tid] = a.z_bot[tid];
+            lay_t[tid] = (Real)(a.z_bot[tid] - a.z_top[tid]);
+        }
+        if (tid == 0) {
+            // Contiguous layers in depth order, as the pieces assume.
+            int bad = 0;
+            for (int k = 0; k < a.n_layer; ++k) {
+                if (!(a.z_bot[k] > a.z_top[k])) bad = 1;
+                if (k + 1 < a.n_layer && fabs(a.z_bot[k] - a.z_top[k + 1]) > 1e-9 * fmax(1.0, fabs(a.z_bot[k])))
+                    bad = 1;
+            }
+            scratch[46] = bad;
+            if (bad && a.status) atomicOr(a.status, PB_DEV_BAD_INPUT);
+        }
+    }
     const Real *E_tab = tab_smem ? E_tab_s : reinterpret_cast<const Real *>(a.tables.E_tab);
     const Real *delta_tab = tab_smem ? delta_s : reinterpret_cast<const Real *>(a.tables.delta);
     const Real *log_mu = tab_smem ? logmu_s : reinterpret_cast<const Real *>(a.tables.log_mu);
@@ -1011,6 +1111,7 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         ax.pad = far_pad;
     }
     __syncthreads();
+    if (kLayered && scratch[46]) return;
 
     const int64_t n_tiles = (n_seg + kSegTile - 1) / kSegTile;
     const int64_t n_work = n_tiles * a.n_dir;
@@ -1054,6 +1155,9 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         const int nst = (int)((n_seg - s0) < kSegTile ? (n_seg - s0) : kSegTile);
         __syncthreads();
         if (tid < nst) seg_precompute<Real>(segs[tid], a, s0 + tid, nh);
+        if constexpr (kLayered) {
+            if (tid < nst) esc_precompute<Real>(esc[tid], a, s0 + tid, nh, lay_zt, lay_zb);
+        }
         for (int g0 = 0; g0 < n_g; g0 += kRowChunk) {
             const int ng = (n_g - g0) < kRowChunk ? (n_g - g0) : kRowChunk;
             __syncthreads();
@@ -1109,8 +1213,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                     const int q = dtail != nullptr ? pq[k] : k;
                     const int si = q / ng;
                     const int gi = q - si * ng;
-                    ln = pair_line<Real>(segs[si], rows[gi], E_tab, delta_tab, log_mu, n_tab, n_mu,
-                                         a.tables, ti);
+                    ln = pair_line<Real, kLayered>(segs[si], rows[gi], E_tab, delta_tab, log_mu, n_tab, n_mu,
+                                                   a.tables, ti, esc + si, a, lay_t);
                     if (pairs_out) {
                         const int64_t o = ((int64_t)d * n_seg + s0 + si) * n_g + g0 + gi;
                         a.pair_E[o] = (double)ln.E_res;
@@ -1382,6 +1486,8 @@ static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moment
         if (sizeof(Real) == 4) b += sizeof(float) * ((size_t)a.n_E + 1) + 16;
         if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
     }
+    if (a.n_layer > 0)
+        b += 16 + sizeof(EscSeg<Real>) * kSegTile + sizeof(double) * 2 * kMaxEscLayers + sizeof(Real) * kMaxEscLayers;
     return b;
 }
 
@@ -1392,11 +1498,14 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
     const bool binmean = a.quadrature == PB_QUAD_BINMEAN;
     const int K_far = (binmean && a.exact_widths > 0.0 && a.far_moments && far_pad >= 0) ? 2 : 0;
     if (K_far == 0) far_pad = 0;
+    if (a.n_layer < 0 || a.n_layer > kMaxEscLayers) return cudaErrorInvalidValue;
+    if (a.n_layer > 0 && (!a.z_top || !a.z_bot || !a.mu_off || !a.mu_knot || !a.mu_value || !a.mu_slope))
+        return cudaErrorInvalidValue;
     size_t smem = cxr_smem_bytes<Real>(a, far_pad, K_far > 0);
     if (smem > 220 * 1024) return cudaErrorInvalidValue;
     // The float path reads its tables from the shared-memory staging only.
     if (sizeof(Real) == 4 && a.tables.n_tab > kMaxTab) return cudaErrorInvalidValue;
-    auto kern = cxr_kernel<Real>;
+    auto kern = a.n_layer > 0 ? cxr_kernel<Real, true> : cxr_kernel<Real, false>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     if (K_far > 0) {

@@ -643,6 +643,129 @@ def gen_char():
         CH.load_characteristic_cross_sections, CH._cascade_line_yields, CH._mu_total_inv_ang = saved
 
 
+def synthetic_exact_mu(composition, knots=None):
+    """Piecewise-linear mu(E) tables of one composition on a fixed knot set
+    (the shape of cxr/_escape_mu.py:ExactMuTable), from synthetic_mu_total."""
+    kn = np.geomspace(500.0, 2.0e5, 400) if knots is None else np.asarray(knots, dtype=float)
+    val = synthetic_mu_total(composition, kn)
+    slope = np.empty_like(val)
+    slope[:-1] = np.diff(val) / np.diff(kn)
+    slope[-1] = slope[-2]
+    return kn, val, slope
+
+
+def _stack_layers(tr):
+    layers = []
+    for i in range(tr["z_top"].size):
+        n = int(tr["n_el"][i])
+        syms = [["C", "Si", "O", "W"][[6, 14, 8, 74].index(int(z))] for z in tr["Z"][i][:n]]
+        layers.append((float(tr["z_top"][i]), float(tr["z_bot"][i]), list(zip(syms, [float(x) for x in tr["N"][i][:n]]))))
+    return layers
+
+
+def _layer_segments(tr, L):
+    keep = tr["layer"] == L
+    seg = {
+        "r_mid": tr["r_mid"][keep], "v_hat": tr["v_hat"][keep], "L_ang": tr["L_ang"][keep],
+        "E_keV": tr["E_keV"][keep], "E_repr_keV": tr["E_repr_keV"][keep], "elec_id": tr["elec_id"][keep],
+        "layer": tr["layer"][keep], "Ne": int(tr["Ne"]), "thickness_ang": float(tr["z_bot"][-1]),
+    }
+    return seg, keep
+
+
+def gen_layered():
+    """Layered-absorber escape on the 10 MeV C / Si / W stack: per-layer
+    Bethe-Heitler (each layer its own composition, escape through the whole
+    stack; runner/emission.py:155-172) and PXR+CBS of the two crystalline
+    layers (runner/case_driver.py:742-770) with exact per-layer mu tables."""
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+    from pyrite.materials.crystal import CRYSTALS, reciprocal_g_vector
+    from pyrite.montecarlo.spectrum import brem as ref_brem
+    from pyrite.montecarlo.spectrum.cxr import _batched, _setup
+    from pyrite.montecarlo.spectrum.cxr._escape_mu import ExactMuTable
+    from pyrite.montecarlo.spectrum.cxr._spectrum import mc_cxr_spectrum
+
+    tr = np.load(OUT / "transport_stack10mev.npz")
+    layers = _stack_layers(tr)
+    out = {"z_top": tr["z_top"], "z_bot": tr["z_bot"], "n_hat": tr["n_hat"], "Ne": int(tr["Ne"]),
+           "thickness": float(tr["z_bot"][-1])}
+    # bremsstrahlung, every layer
+    E_brem = np.linspace(1000.0, 80000.0, 300)
+    saved = ref_brem._mu_total_inv_ang
+    ref_brem._mu_total_inv_ang = lambda c, E: synthetic_mu_total(c, np.asarray(E, dtype=float))
+    try:
+        for L, (_zt, _zb, comp) in enumerate(layers):
+            seg, _keep = _layer_segments(tr, L)
+            out[f"brem_spec_{L}"] = np.asarray(ref_brem.mc_brem_spectrum(
+                seg, E_brem, composition=comp, n_hat=tr["n_hat"], layers=layers,
+                cross_section_model="bethe-heitler"))
+            out[f"brem_Z_{L}"] = np.array([float(TRANSPORT_ELEMENTS[e]["Z"]) for e, _ in comp])
+            out[f"brem_n_{L}"] = np.array([n for _, n in comp])
+    finally:
+        ref_brem._mu_total_inv_ang = saved
+    out["brem_E_grid"] = E_brem
+    out["brem_mu_layer"] = np.stack([synthetic_mu_total(c, E_brem) for _a, _b, c in layers])
+    # PXR + CBS of the HOPG-like carbon layer and the Si layer
+    E_grid = np.linspace(1000.0, 60000.0, 1024)
+    E_tab = synthetic_E_tab(E_grid)
+    mu_tabs = [synthetic_exact_mu(c) for _a, _b, c in layers]
+    for k, (kn, val, sl) in enumerate(mu_tabs):
+        out[f"mu_knot_{k}"], out[f"mu_value_{k}"], out[f"mu_slope_{k}"] = kn, val, sl
+    radiators = {0: ("hopg", (0, 0, 1), [(0, 0, l) for l in range(-8, 9) if l != 0]),
+                 1: ("silicon", (2, 2, 0), _diamond_hkls(4))}
+    for L, (crystal, surface, hkl) in radiators.items():
+        info = CRYSTALS[crystal]
+        g_mags = np.array([reciprocal_g_vector(h, info["lattice"])[1] for h in hkl])
+        tables = synthetic_couplings(g_mags, E_tab)
+        comp = layers[L][2]
+        seg, keep = _layer_segments(tr, L)
+        captured = {}
+        orig_brt = _batched._batched_reflection_tables
+
+        def capture(st, _orig=orig_brt):
+            res = _orig(st)
+            captured["rows"] = res
+            return res
+
+        def exact_tables(req, abs_comp):
+            return tuple(ExactMuTable(knots=kn, value=val, slope=sl) for kn, val, sl in mu_tabs)
+
+        patches = [
+            (_setup, "_line_tabulation_grid", lambda *a, **k: E_tab),
+            (_setup, "_elemental_log_mu_table", lambda c, E: synthetic_log_mu(c, E)),
+            (_setup, "refractive_index", lambda cr, E, uh=True: (1.0 - synthetic_delta(E)) + 0j),
+            (_batched, "_reflection_tables", lambda *a, **k: tuple(np.array(t) for t in tables)),
+            (_batched, "_batched_reflection_tables", capture),
+            (_batched, "escape_mu_tables", exact_tables),
+        ]
+        saved_p = [(m, n, getattr(m, n)) for m, n, _ in patches]
+        for m, n, f in patches:
+            setattr(m, n, f)
+        try:
+            common = dict(
+                crystal=crystal, hkl_list=[tuple(h) for h in hkl],
+                B_ang2=float(info.get("B_ang2", 0.0) or 0.0), composition=comp,
+                n_hat=tr["n_hat"], surface_hkl=surface, layers=layers,
+                mosaic_fwhm_rad=None, mosaic_nodes=1, node_support_cutoff=None,
+            )
+            spec_node = np.asarray(mc_cxr_spectrum(seg, E_grid, line_quadrature="node", **common))
+            spec_bin = np.asarray(mc_cxr_spectrum(seg, E_grid, line_quadrature="bin-mean", **common))
+        finally:
+            for m, n, f in saved_p:
+                setattr(m, n, f)
+        G, ES, EP, WM, _cr, _ci, _ur, _ui, ROW_TABLE = captured["rows"][:9]
+        out.update({
+            f"cxr_hkl_{L}": np.array(hkl, dtype=np.int64), f"cxr_g_mags_{L}": g_mags,
+            f"cxr_chi_re_{L}": tables[0], f"cxr_chi_im_{L}": tables[1], f"cxr_u_re_{L}": tables[2],
+            f"cxr_u_im_{L}": tables[3], f"cxr_G_{L}": np.asarray(G), f"cxr_ES_{L}": np.asarray(ES),
+            f"cxr_EP_{L}": np.asarray(EP), f"cxr_WM_{L}": np.asarray(WM).reshape(-1),
+            f"cxr_row_table_{L}": np.asarray(ROW_TABLE), f"cxr_log_mu_{L}": synthetic_log_mu(comp, E_tab),
+            f"cxr_spec_node_{L}": spec_node, f"cxr_spec_binmean_{L}": spec_bin,
+        })
+    out.update(cxr_E_grid=E_grid, cxr_E_tab=E_tab, cxr_delta=synthetic_delta(E_tab))
+    _save("layered_stack10", **out)
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
@@ -652,6 +775,7 @@ GENERATORS = {
     "brem": gen_brem,
     "cxr_leaves": gen_cxr_leaves,
     "char": gen_char,
+    "layered": gen_layered,
 }
 
 
