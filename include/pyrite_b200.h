@@ -332,6 +332,10 @@ typedef struct pb_char_args {
     const double *mu;       /* [max(n_layer,1)*n_line] attenuation at the line energies, 1/Angstrom */
     double *line_yield;     /* [n_dir*n_line] accumulated (+=), FP64: sum n L sigma_line T_escape */
     unsigned int *status;
+    /* Optional emitting-layer filter: with seg_layer set, only segments whose
+     * layer equals emit_layer emit (the element's own layer of a stack). */
+    const int32_t *seg_layer;
+    int32_t emit_layer;
 } pb_char_args;
 
 /* One GEMM of the BF16 MLP surrogate on tcgen05:

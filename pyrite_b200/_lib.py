@@ -125,6 +125,7 @@ class PbCharArgs(C.Structure):
         ("L", _vp), ("E_keV", _vp), ("elec_id", _vp), ("n_seg_device", _vp), ("n_atoms", _f64),
         ("n_shell", _i32), ("shell_E", _vp), ("shell_sigma", _vp), ("shell_offset", _vp), ("n_line", _i32),
         ("response", _vp), ("mu", _vp), ("line_yield", _vp), ("status", _vp),
+        ("seg_layer", _vp), ("emit_layer", _i32),
     ]
 
 

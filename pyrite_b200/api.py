@@ -605,7 +605,8 @@ def prepare_characteristic_lines(lines: CharacteristicLines, E_grid_eV, relaxati
 
 def mc_characteristic_spectrum(segments, E_grid_eV, *, lines: CharacteristicLines, n_atoms_per_ang3, n_hat,
                                mu_by_line, layers=None, relaxation_cutoff_eV=None, E_cut_keV=None,
-                               precision="fp64", device=None, stream=None, return_yields=False):
+                               precision="fp64", emit_layer=None, device=None, stream=None,
+                               return_yields=False):
     """Characteristic X-ray density [photons/eV/sr/electron] of one emitting element.
 
     ``mu_by_line[k, j]`` is the attenuation [1/Angstrom] of absorber layer k
@@ -614,7 +615,8 @@ def mc_characteristic_spectrum(segments, E_grid_eV, *, lines: CharacteristicLine
     ``(z_top, z_bot)`` bounds in Angstrom, or None for the slab of
     ``segments["thickness_ang"]``. Segments are expected above the 1 keV
     transport floor already (a transport cutoff >= 1 keV makes the
-    reference's clipping the identity).
+    reference's clipping the identity). ``emit_layer`` keeps only the
+    segments of that layer (``segments["layer"]``) emitting.
     """
     if E_cut_keV is not None and float(E_cut_keV) < CHARACTERISTIC_TRANSPORT_FLOOR_KEV:
         raise ValueError("characteristic scoring requires E_cut_keV >= 1 keV")
@@ -660,6 +662,9 @@ def mc_characteristic_spectrum(segments, E_grid_eV, *, lines: CharacteristicLine
     yields = h.zeros((n_dir, int(kept.size)), torch.float64)
     a.line_yield = _ptr(yields)
     a.status = _ptr(h.zeros(1, torch.int32))
+    sl_t = _seg_layer(h, segments, emit_layer)
+    if sl_t is not None:
+        a.seg_layer, a.emit_layer = _ptr(sl_t), int(emit_layer)
     s = _stream_ptr(stream)
     L.check(lib.pb_char_yields(C.byref(a), s), "pb_char_yields")
     spec = h.zeros((n_dir, n_E), torch.float64)

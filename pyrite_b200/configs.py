@@ -69,3 +69,55 @@ def c2_si_50mev(seed=0, angular_shape=(4, 4), n_bins=2048):
         brem_composition=comp, brem_mu=P.mu_total(comp, E_grid), seed=seed,
         detector=det, angular_shape=tuple(angular_shape),
     )
+
+
+W_N_PER_ANG3 = 19.3 / 183.84 * 0.602214076  # amorphous W at 19.3 g/cm^3
+
+
+def c5_stack_10mev(seed=0, angular_shape=(4, 4), n_bins=4096, si_g_max=8.0, detector_angles_deg=(20.0, 45.0, 90.0, 135.0)):
+    """10 MeV, 0.5 mm / 0.5 mrad, normal incidence on a three-layer stack:
+    20 um HOPG with (002) at 45 deg to the beam, 200 um Si with (220) at
+    10 deg, 1 mm amorphous W (19.3 g/cm^3). Four 64x64-pixel 2x2 cm^2
+    detectors at 1 m and 20/45/90/135 deg, each scored in angular tiles;
+    1-80 keV in 4096 bins. Both crystals radiate PXR/CBS, every layer
+    bremsstrahlung with its own composition, and C/Si/W their K and L lines,
+    all escaping through the whole stack. The lattice tilts are crystal
+    miscuts (the beam stays on the stack normal).
+
+    One electron population is transported, at the 5 keV line cutoff; the
+    reference transports bremsstrahlung and characteristic emitters again at
+    1 keV with secondary electrons, which need EEDL tables this build does
+    not have."""
+    from .detector import PlanarDetector, tiles_in_sample_frame
+    from .pipeline import CharEmitter, Radiator
+
+    E0 = 10000.0
+    beam_dir, _ = tilted_geometry(np.deg2rad(detector_angles_deg[0]), 0.0)
+    tw = _twiss(E0, 0.5, 0.5e-3)
+    n_c, n_si, n_w = HOPG.n_atoms_per_ang3, SILICON.n_atoms_per_ang3, W_N_PER_ANG3
+    comps = [[("C", n_c)], [("Si", n_si)], [("W", n_w)]]
+    bounds = [(0.0, 2.0e5), (2.0e5, 2.2e6), (2.2e6, 1.22e7)]
+    stack = LayerStack([(a, b, c) for (a, b), c in zip(bounds, comps)])
+    E_grid = np.linspace(1000.0, 80000.0, n_bins)
+    dets = [PlanarDetector(np.deg2rad(a), 1000.0, 20.0, 20.0, 64, 64) for a in detector_angles_deg]
+    n_hats = np.concatenate([tiles_in_sample_frame(d, angular_shape, 0.0)[1] for d in dets])
+    hopg_hkl = [(0, 0, l) for l in range(-8, 9) if l != 0]
+    si_hkl = diamond_hkls(si_g_max)
+    radiators = [
+        Radiator(0, HOPG, hopg_hkl, P.line_tables(HOPG, hopg_hkl, E_grid, comps[0]), surface_hkl=(0, 0, 1),
+                 recip_miscut_rad=(np.deg2rad(45.0), 0.0)),
+        Radiator(1, SILICON, si_hkl, P.line_tables(SILICON, si_hkl, E_grid, comps[1]), surface_hkl=(2, 2, 0),
+                 recip_miscut_rad=(np.deg2rad(10.0), 0.0)),
+    ]
+    emitters = []
+    for k, (el, n) in enumerate([("C", n_c), ("Si", n_si), ("W", n_w)]):
+        lines = P.characteristic_lines(el)
+        mu_by_line = np.stack([P.mu_total(c, lines.line_E) for c in comps])
+        emitters.append(CharEmitter(lines, n, mu_by_line, layer=k))
+    return CaseSpec(
+        stack=stack, beam=BeamSpec(E0, beam_dir, 0.0, 0.0, twiss_x=tw, twiss_y=tw), E_cut_keV=5.0,
+        crystal=None, hkl_list=None, n_hats=n_hats, E_grid=E_grid, line_tables=None,
+        radiators=radiators, escape_mu_tables=[P.exact_mu_table(c) for c in comps],
+        brem_layers=comps, brem_mu_layer=np.stack([P.mu_total(c, E_grid) for c in comps]),
+        char_emitters=emitters, seed=seed,
+    )

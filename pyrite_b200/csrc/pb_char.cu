@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kCharThreads) char_yield_kernel(const pb_char_
     const int64_t n_iter = (n_seg + stride - 1) / stride;
     for (int64_t it = 0; it < n_iter; ++it) {
         const int64_t s = it * stride + (int64_t)blockIdx.x * blockDim.x + tid;
-        const bool valid = s < n_seg && a.elec_id[s] < a.Ne;
+        const bool valid = s < n_seg && a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
         double sig[kCharMaxShell];
         double r0z = 0.0, r1z = 0.0, path_cm = 0.0;
         // Pieces: cut fractions at the interior layer boundaries, sorted.

@@ -41,8 +41,39 @@ _RNG = {"splitmix": L.PB_RNG_SPLITMIX, "philox": L.PB_RNG_PHILOX}
 
 
 @dataclass
+class Radiator:
+    """A crystalline layer of a stack and its PXR/CBS reflections; the layer's
+    segments radiate its lines, which escape through the whole stack
+    (runner/case_driver.py:742-770)."""
+
+    layer: int
+    crystal: Crystal
+    hkl_list: list
+    line_tables: LineTables
+    surface_hkl: tuple | None = None
+    recip_miscut_rad: tuple | None = None
+    mosaic_fwhm_rad: float | None = None
+    mosaic_nodes: int = 1
+
+
+@dataclass
+class CharEmitter:
+    """One element's characteristic lines, emitted by the segments of its
+    layer (``layer`` None: every segment) and escaping through the stack;
+    ``mu_by_line[k, j]`` the attenuation of layer k at line j
+    (characteristic.py:975-985)."""
+
+    lines: object                 # api.CharacteristicLines
+    n_atoms_per_ang3: float
+    mu_by_line: np.ndarray
+    layer: int | None = None
+
+
+@dataclass
 class CaseSpec:
-    """One beam/crystal scene."""
+    """One beam/crystal scene: a single crystal slab, or a layered stack with
+    per-layer radiators, bremsstrahlung compositions and characteristic
+    emitters (``radiators`` / ``brem_layers`` / ``char_emitters``)."""
 
     stack: LayerStack
     beam: BeamSpec
@@ -63,6 +94,15 @@ class CaseSpec:
     # coordinates); None when the directions were given directly.
     detector: object | None = None
     angular_shape: tuple | None = None
+    # Layered stack (the reference's layer_radiators / abs_layers cases): the
+    # CXR escape runs through every layer with its exact mu(E) table
+    # (knots, values, slopes per layer), each layer radiates bremsstrahlung
+    # with its own composition and mu_layer [n_layer, n_E].
+    radiators: list | None = None
+    escape_mu_tables: list | None = None
+    brem_layers: list | None = None
+    brem_mu_layer: np.ndarray | None = None
+    char_emitters: list | None = None
 
 
 class ScoringCase:
@@ -117,21 +157,137 @@ class ScoringCase:
         self.status = h.zeros(1, torch.int32)
         a.work_counter, a.status = _ptr(self.work), _ptr(self.status)
         self.targs = a
-        # ---- CXR scorer ----
+        # ---- CXR scorer (one argument set per radiator) ----
         n_hats = np.atleast_2d(np.asarray(spec.n_hats, dtype=float))
         self.n_dir = n_hats.shape[0]
-        rows = reflection_rows(spec.crystal, spec.hkl_list, n_hats, surface_hkl=spec.surface_hkl,
-                               mosaic_fwhm_rad=spec.mosaic_fwhm_rad, mosaic_nodes=spec.mosaic_nodes)
-        self.rows = rows
         E_grid = np.asarray(spec.E_grid, dtype=np.float64)
         self.n_E = int(E_grid.size)
+        self._n_hat_dev = h.f64(n_hats)
+        self._E_grid_dev = h.f64(E_grid)
+        self.spec_cxr = h.zeros((self.n_dir, self.n_E), torch.float64)
+        self.far = None
+        self.layered = spec.radiators is not None
+        if self.layered:
+            z_top = np.array([l[0] for l in st.layers], dtype=float)
+            z_bot = np.array([l[1] for l in st.layers], dtype=float)
+            self._z_top, self._z_bot = h.f64(z_top), h.f64(z_bot)
+            mt = spec.escape_mu_tables
+            if mt is None or len(mt) != st.n_layers:
+                raise ValueError("a stack needs one escape mu table per layer")
+            self._mu_off = h.typed(np.cumsum([0] + [len(k) for k, _v, _s in mt]).astype(np.int32), torch.int32)
+            self._mu_knot = h.f64(np.concatenate([np.asarray(k, float) for k, _v, _s in mt]))
+            self._mu_value = h.f64(np.concatenate([np.asarray(v, float) for _k, v, _s in mt]))
+            self._mu_slope = h.f64(np.concatenate([np.asarray(sl, float) for _k, _v, sl in mt]))
+            radiators = list(spec.radiators)
+        else:
+            radiators = [Radiator(-1, spec.crystal, spec.hkl_list, spec.line_tables, spec.surface_hkl, None,
+                                  spec.mosaic_fwhm_rad, spec.mosaic_nodes)]
+        self.cargs_all = [self._cxr_args(r, n_hats, E_grid, cap) for r in radiators]
+        self.cargs = self.cargs_all[0]
+        self.rows = self._rows[0]
+        # ---- brem scorer (one argument set per emitting layer) ----
+        self.bargs = None
+        self.bargs_all = []
+        brem_sets = []
+        if spec.brem_layers:
+            brem_sets = [(k, comp) for k, comp in enumerate(spec.brem_layers) if comp]
+        elif spec.brem_composition:
+            brem_sets = [(None, spec.brem_composition)]
+        if brem_sets:
+            self.spec_brem = h.zeros((self.n_dir, self.n_E), torch.float64)
+            mu_layer = None
+            if spec.brem_layers:
+                mu_layer = h.f64(np.asarray(spec.brem_mu_layer, dtype=np.float64).reshape(st.n_layers, self.n_E))
+                if st.n_layers > 4:
+                    raise ValueError("layered bremsstrahlung supports up to 4 layers")
+            for k, comp in brem_sets:
+                b = L.PbBremArgs()
+                b.precision = self.precision
+                b.n_dir = self.n_dir
+                b.n_hat = _ptr(self._n_hat_dev)
+                b.thickness = st.thickness
+                b.Ne = 1 << 62
+                b.n_seg = cap
+                b.r_mid, b.v_hat, b.L = _ptr(self.seg_r), _ptr(self.seg_v), _ptr(self.seg_L)
+                b.E_keV, b.elec_id = _ptr(self.seg_E), _ptr(self.seg_id)
+                b.n_seg_device = _ptr(self.seg_count)
+                b.n_el = len(comp)
+                b.Z = _ptr(h.f64([float(ELEMENTS[el][0]) for el, _ in comp]))
+                b.n_ang3 = _ptr(h.f64([float(n) for _, n in comp]))
+                b.n_E = self.n_E
+                b.E_grid = _ptr(self._E_grid_dev)
+                if mu_layer is None:
+                    b.mu = _ptr(h.f64(spec.brem_mu))
+                else:
+                    b.n_layer = st.n_layers
+                    b.z_top, b.z_bot = _ptr(self._z_top), _ptr(self._z_bot)
+                    b.mu_layer = _ptr(mu_layer)
+                    b.seg_layer, b.emit_layer = _ptr(self.seg_layer), int(k)
+                b.spec = _ptr(self.spec_brem)
+                b.status = _ptr(self.status)
+                self.bargs_all.append(b)
+            self.bargs = self.bargs_all[0]
+        # ---- characteristic lines (one argument set per emitter) ----
+        self.chargs_all = []
+        self.char_yields = []
+        self.char_profiles = []
+        if spec.char_emitters:
+            from .api import prepare_characteristic_lines
+
+            self.spec_char = h.zeros((self.n_dir, self.n_E), torch.float64)
+            layered = st.n_layers > 1
+            for em in spec.char_emitters:
+                kept, profiles = prepare_characteristic_lines(em.lines, E_grid)
+                if kept.size == 0:
+                    continue
+                ch = L.PbCharArgs()
+                ch.precision = self.precision
+                ch.n_dir = self.n_dir
+                ch.n_hat = _ptr(self._n_hat_dev)
+                ch.thickness = st.thickness
+                mu = np.atleast_2d(np.asarray(em.mu_by_line, dtype=float))[:, kept]
+                if layered:
+                    ch.n_layer = st.n_layers
+                    ch.z_top = _ptr(h.f64([l[0] for l in st.layers]))
+                    ch.z_bot = _ptr(h.f64([l[1] for l in st.layers]))
+                ch.Ne = 1 << 62
+                ch.n_seg = cap
+                ch.r_mid, ch.v_hat, ch.L = _ptr(self.seg_r), _ptr(self.seg_v), _ptr(self.seg_L)
+                ch.E_keV, ch.elec_id = _ptr(self.seg_E), _ptr(self.seg_id)
+                ch.n_seg_device = _ptr(self.seg_count)
+                ch.n_atoms = float(em.n_atoms_per_ang3)
+                ch.n_shell = len(em.lines.shell_E)
+                offs = np.cumsum([0] + [int(np.size(e)) for e in em.lines.shell_E]).astype(np.int64)
+                ch.shell_E = _ptr(h.f64(np.concatenate([np.asarray(e, float) for e in em.lines.shell_E])))
+                ch.shell_sigma = _ptr(h.f64(np.concatenate([np.asarray(v, float) for v in em.lines.shell_sigma])))
+                ch.shell_offset = _ptr(h.typed(offs, torch.int64))
+                ch.n_line = int(kept.size)
+                ch.response = _ptr(h.f64(np.asarray(em.lines.response, float)[:, kept]))
+                ch.mu = _ptr(h.f64(mu))
+                y = h.zeros((self.n_dir, int(kept.size)), torch.float64)
+                ch.line_yield = _ptr(y)
+                ch.status = _ptr(self.status)
+                if em.layer is not None:
+                    ch.seg_layer, ch.emit_layer = _ptr(self.seg_layer), int(em.layer)
+                self.chargs_all.append(ch)
+                self.char_yields.append(y)
+                self.char_profiles.append(h.f64(profiles))
+        self.histories = 0
+
+    def _cxr_args(self, rad: Radiator, n_hats, E_grid, cap):
+        """pb_cxr_args of one radiator over the case's segment buffer."""
+        h, spec, st = self.h, self.spec, self.spec.stack
+        rows = reflection_rows(rad.crystal, rad.hkl_list, n_hats, surface_hkl=rad.surface_hkl,
+                               mosaic_fwhm_rad=rad.mosaic_fwhm_rad, mosaic_nodes=rad.mosaic_nodes,
+                               recip_miscut_rad=rad.recip_miscut_rad)
+        self._rows = getattr(self, "_rows", []) + [rows]
         lo_keep, hi_keep = line_keep_window(E_grid)
         edges = energy_bin_edges(E_grid)
         c = L.PbCxrArgs()
         c.precision = self.precision
         c.quadrature = L.PB_QUAD_BINMEAN
         c.n_dir = self.n_dir
-        c.n_hat = _ptr(h.f64(n_hats))
+        c.n_hat = _ptr(self._n_hat_dev)
         c.thickness = st.thickness
         # Every streamed history radiates (elec_id < Ne for all of them).
         c.Ne = 1 << 62
@@ -140,7 +296,7 @@ class ScoringCase:
         c.E_keV, c.elec_id = _ptr(self.seg_E), _ptr(self.seg_id)
         c.n_seg_device = _ptr(self.seg_count)
         t = L.PbCxrTables()
-        lt = spec.line_tables
+        lt = rad.line_tables
         t.n_g = int(rows.G.shape[0])
         t.G, t.WM = _ptr(h.f64(rows.G)), _ptr(h.f64(rows.WM))
         t.ES, t.EP = _ptr(h.f64(rows.ES)), _ptr(h.f64(rows.EP))
@@ -157,44 +313,27 @@ class ScoringCase:
         t.delta_tail_absmax = _ptr(h.f64(np.maximum.accumulate(np.abs(np.asarray(lt.delta, float))[::-1])[::-1]))
         c.tables = t
         c.n_E = self.n_E
-        c.E_grid = _ptr(h.f64(E_grid))
+        c.E_grid = _ptr(self._E_grid_dev)
         c.edges = _ptr(h.f64(edges))
         w = np.diff(edges)
         uniform = np.allclose(w, w[0], rtol=1e-9, atol=0.0)
         if spec.exact_widths and spec.exact_widths > 0 and uniform:
             pad = int(np.ceil(max(edges[0] - lo_keep, hi_keep - edges[-1]) / w[0])) + 2
             c.exact_widths, c.far_pad = float(spec.exact_widths), pad
-            self.far = h.zeros(self.n_dir * (self.n_E + 2 * pad) * 3, torch.float64)
+            if self.far is None:  # shared by the radiators: each call clears it
+                self.far = h.zeros(self.n_dir * (self.n_E + 2 * pad) * 3, torch.float64)
             c.far_moments = _ptr(self.far)
         else:
             c.exact_widths, c.far_pad = 0.0, -1
-        self.spec_cxr = h.zeros((self.n_dir, self.n_E), torch.float64)
         c.spec = _ptr(self.spec_cxr)
         c.status = _ptr(self.status)
-        self.cargs = c
-        # ---- brem scorer ----
-        self.bargs = None
-        if spec.brem_composition:
-            b = L.PbBremArgs()
-            b.precision = self.precision
-            b.n_dir = self.n_dir
-            b.n_hat = c.n_hat
-            b.thickness = st.thickness
-            b.Ne = c.Ne
-            b.n_seg = cap
-            b.r_mid, b.v_hat, b.L, b.E_keV, b.elec_id = c.r_mid, c.v_hat, c.L, c.E_keV, c.elec_id
-            b.n_seg_device = c.n_seg_device
-            b.n_el = len(spec.brem_composition)
-            b.Z = _ptr(h.f64([float(ELEMENTS[el][0]) for el, _ in spec.brem_composition]))
-            b.n_ang3 = _ptr(h.f64([float(n) for _, n in spec.brem_composition]))
-            b.n_E = self.n_E
-            b.E_grid = c.E_grid
-            b.mu = _ptr(h.f64(spec.brem_mu))
-            self.spec_brem = h.zeros((self.n_dir, self.n_E), torch.float64)
-            b.spec = _ptr(self.spec_brem)
-            b.status = c.status
-            self.bargs = b
-        self.histories = 0
+        if self.layered:
+            c.n_layer = st.n_layers
+            c.z_top, c.z_bot = _ptr(self._z_top), _ptr(self._z_bot)
+            c.mu_off, c.mu_knot = _ptr(self._mu_off), _ptr(self._mu_knot)
+            c.mu_value, c.mu_slope = _ptr(self._mu_value), _ptr(self._mu_slope)
+            c.seg_layer, c.emit_layer = _ptr(self.seg_layer), int(rad.layer)
+        return c
 
     # -- one batch ---------------------------------------------------------
     def use_surrogate(self, models, exact_stride=20):
@@ -215,6 +354,8 @@ class ScoringCase:
 
         if self.spec.detector is None or self.spec.angular_shape is None:
             raise ValueError("the surrogate needs the case's detector tiling")
+        if len(self.cargs_all) != 1 or self.layered:
+            raise ValueError("the surrogate covers a single-crystal slab; a stack scores its layers exactly")
         n_out = models[0].n_out
         if self.n_E % n_out != 0:
             raise ValueError("the case's bins must split evenly into the surrogate's coarse bins")
@@ -303,11 +444,14 @@ class ScoringCase:
             for sa in self.sur_args + self.sur_args_s:
                 L.check(self.lib.pb_mlp_infer(C.byref(sa), s), "pb_mlp_infer")
         else:
-            L.check(self.lib.pb_cxr_score(C.byref(self.cargs), s), "pb_cxr_score")
+            for ca in self.cargs_all:
+                L.check(self.lib.pb_cxr_score(C.byref(ca), s), "pb_cxr_score")
         if events is not None:
             events[2].record()
-        if self.bargs is not None:
-            L.check(self.lib.pb_brem_score(C.byref(self.bargs), s), "pb_brem_score")
+        for ba in self.bargs_all:
+            L.check(self.lib.pb_brem_score(C.byref(ba), s), "pb_brem_score")
+        for ch in self.chargs_all:
+            L.check(self.lib.pb_char_yields(C.byref(ch), s), "pb_char_yields")
         if events is not None:
             events[3].record()
         self.histories += int(n)
@@ -320,9 +464,9 @@ class ScoringCase:
             if self.sur_stride > 0:
                 n += 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
         else:
-            n = 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
-        if self.bargs is not None:
-            n += (self.n_dir + 15) // 16
+            n = 1 + sum(1 + (1 if ca.exact_widths > 0 else 0) for ca in self.cargs_all)
+        n += len(self.bargs_all) * ((self.n_dir + 15) // 16)
+        n += len(self.chargs_all)
         return n
 
     def device_status(self) -> int:
@@ -341,7 +485,19 @@ class ScoringCase:
         }
         if self.bargs is not None:
             out["brem"] = self.spec_brem.cpu().numpy() / (4.0 * np.pi) / Ne
+        if self.chargs_all:
+            out["characteristic"] = self.characteristic_spectrum().cpu().numpy() / (4.0 * np.pi) / Ne
         return out
+
+    def characteristic_spectrum(self):
+        """Line yields so far spread on the bins (pb_char_spectrum), summed
+        over emitters, un-normalised [n_dir, n_E]."""
+        self.spec_char.zero_()
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        for y, prof in zip(self.char_yields, self.char_profiles):
+            L.check(self.lib.pb_char_spectrum(self.n_dir, int(y.shape[1]), self.n_E, _ptr(y), _ptr(prof),
+                                              _ptr(self.spec_char), s), "pb_char_spectrum")
+        return self.spec_char
 
     def device_results(self) -> dict:
         """The device-resident accumulators (un-normalised), for a cross-rank sum."""
@@ -349,6 +505,8 @@ class ScoringCase:
                "exit_theta": self.exit_theta, "deposit": self.deposit}
         if self.bargs is not None:
             out["brem"] = self.spec_brem
+        for i, y in enumerate(self.char_yields):
+            out[f"char_yield_{i}"] = y
         return out
 
     def reset(self):
@@ -361,6 +519,8 @@ class ScoringCase:
             self.spec_sample.zero_()
         if self.bargs is not None:
             self.spec_brem.zero_()
+        for y in self.char_yields:
+            y.zero_()
         self.histories = 0
 
 
@@ -386,6 +546,7 @@ def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 
         outs = [case.spec_cxr, case.fates, case.exit_E, case.exit_theta, case.deposit]
     if case.bargs is not None:
         outs.append(case.spec_brem)
+    outs += case.char_yields
     host_out = [torch.empty_like(t, device="cpu").pin_memory() for t in outs]
     h2d = sum(h.numel() * h.element_size() for h, _ in pairs)
     d2h = sum(t.numel() * t.element_size() for t in outs)

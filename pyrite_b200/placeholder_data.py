@@ -109,3 +109,55 @@ def mu_element(element: str, n_per_ang3: float, E):
 
 def mu_total(composition, E):
     return sum(mu_element(el, n, E) for el, n in composition)
+
+
+def exact_mu_table(composition, knots=None):
+    """mu(E) of a composition as the piecewise-linear (knots, values, slopes)
+    tables of the layered escape (cxr/_escape_mu.py:41-57), on a geometric
+    knot set."""
+    kn = np.geomspace(200.0, 3.0e5, 600) if knots is None else np.asarray(knots, dtype=float)
+    val = mu_total(composition, kn)
+    slope = np.empty_like(val)
+    slope[:-1] = np.diff(val) / np.diff(kn)
+    slope[-1] = slope[-2]
+    return kn, val, slope
+
+
+# Edge and line energies [eV] (standard X-ray data) with placeholder widths;
+# ionisation cross sections and cascade responses are smooth stand-ins for the
+# EEDL/EADL-derived tables the reference reads (characteristic.py:111-160).
+_CHAR_DATA = {
+    "C": dict(shells=[284.2], lines=[(277.0, 0.5)], resp=[[0.0026]]),
+    "Si": dict(shells=[1839.0, 149.7], lines=[(1739.98, 0.5), (1835.94, 0.6)],
+               resp=[[0.045, 0.002], [0.0, 0.0]]),
+    "W": dict(
+        shells=[69525.0, 12100.0, 11544.0, 10207.0],
+        lines=[(59318.2, 43.0), (57981.7, 44.0), (67244.3, 45.0), (8397.6, 6.5), (9672.4, 7.0),
+               (9961.5, 7.5), (11285.9, 9.0)],
+        resp=[[0.52, 0.30, 0.12, 0.11, 0.04, 0.02, 0.0],
+              [0.0, 0.0, 0.0, 0.05, 0.02, 0.01, 0.08],
+              [0.0, 0.0, 0.0, 0.0, 0.21, 0.0, 0.06],
+              [0.0, 0.0, 0.0, 0.22, 0.0, 0.05, 0.0]],
+    ),
+}
+
+
+def characteristic_lines(element: str):
+    """Placeholder ``CharacteristicLines`` of C, Si or W (K and L lines)."""
+    from .api import CharacteristicLines
+
+    d = _CHAR_DATA[element]
+    Z = ELEMENTS[element][0]
+    grids, sigmas = [], []
+    for i, Eb in enumerate(d["shells"]):
+        E = np.geomspace(Eb, 1.0e9, 80)
+        u = E / Eb
+        sig = 2.0e-20 * (Eb / 1000.0) ** -2 * (1.0 + 0.5 * i) * np.log(u) / (u + 1.0) * (Z / 14.0) ** 0.2
+        sig[0] = 0.0
+        grids.append(E)
+        sigmas.append(sig)
+    return CharacteristicLines(
+        shell_E=tuple(grids), shell_sigma=tuple(sigmas),
+        line_E=np.array([e for e, _ in d["lines"]]), line_fwhm=np.array([w for _, w in d["lines"]]),
+        response=np.array(d["resp"], dtype=float), recommended_cutoff_eV=50.0,
+    )

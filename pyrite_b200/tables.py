@@ -429,8 +429,10 @@ class Crystal:
         g = np.asarray(hkl, dtype=float) @ self.reciprocal_basis()
         return g, float(np.linalg.norm(g))
 
-    def orientation(self, surface_hkl=None, beam_uvw=None, azimuth_rad=0.0):
-        """Rotation of every reciprocal vector (crystal.py:919-961, no miscut)."""
+    def orientation(self, surface_hkl=None, beam_uvw=None, azimuth_rad=0.0, recip_miscut_rad=None):
+        """Rotation of every reciprocal vector (crystal.py:919-963): the cut
+        direction onto +z, a roll about +z, then an optional miscut
+        (polar, azimuth) tilting the lattice away from the slab normal."""
         if beam_uvw is not None and surface_hkl is not None:
             raise ValueError("beam_uvw and surface_hkl are mutually exclusive")
         R = None
@@ -446,6 +448,12 @@ class Crystal:
             ca, sa = np.cos(azimuth_rad), np.sin(azimuth_rad)
             Rz = np.array([[ca, -sa, 0.0], [sa, ca, 0.0], [0.0, 0.0, 1.0]])
             R = Rz if R is None else Rz @ R
+        if recip_miscut_rad is not None:
+            mp, ma = recip_miscut_rad
+            if mp:
+                st, ct = np.sin(mp), np.cos(mp)
+                R_m = rotation_between(np.array([0.0, 0.0, 1.0]), np.array([st * np.cos(ma), st * np.sin(ma), ct]))
+                R = R_m if R is None else R_m @ R
         return R
 
     @property
@@ -509,9 +517,9 @@ class ReflectionRows:
 
 
 def reflection_rows(crystal: Crystal, hkl_list, n_hats, *, surface_hkl=None, beam_uvw=None,
-                    azimuth_rad=0.0, mosaic_fwhm_rad=None, mosaic_nodes=1) -> ReflectionRows:
+                    azimuth_rad=0.0, mosaic_fwhm_rad=None, mosaic_nodes=1, recip_miscut_rad=None) -> ReflectionRows:
     """One row per (reflection, mosaic orientation); polarisations per direction."""
-    R_orient = crystal.orientation(surface_hkl, beam_uvw, azimuth_rad)
+    R_orient = crystal.orientation(surface_hkl, beam_uvw, azimuth_rad, recip_miscut_rad)
     quad = mosaic_quadrature(mosaic_fwhm_rad, mosaic_nodes)
     orients = ((None, 1.0),) if quad is None else quad
     g_rows, wm_rows, table_rows = [], [], []

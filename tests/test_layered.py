@@ -237,3 +237,20 @@ def test_layered_kernels_match_oracle_on_crossing_segments():
     assert np.array_equal(pg.astype(bool), good)
     np.testing.assert_allclose(pw[good], w[good], rtol=1e-9)
     torch.cuda.synchronize()
+
+
+def test_stack_case_spec_builds():
+    from pyrite_b200.configs import c5_stack_10mev
+    from pyrite_b200.tables import HOPG, reflection_rows
+
+    spec = c5_stack_10mev(angular_shape=(1, 1), n_bins=512, si_g_max=4.0)
+    assert spec.n_hats.shape == (4, 3)
+    assert spec.stack.n_layers == 3 and spec.stack.thickness == 1.22e7
+    assert [r.layer for r in spec.radiators] == [0, 1]
+    assert spec.brem_mu_layer.shape == (3, 512) and len(spec.escape_mu_tables) == 3
+    assert [e.layer for e in spec.char_emitters] == [0, 1, 2]
+    # the HOPG (002) normal sits 45 deg from the stack normal (the beam axis)
+    rows = reflection_rows(HOPG, [(0, 0, 2)], spec.n_hats[:1], surface_hkl=(0, 0, 1),
+                           recip_miscut_rad=spec.radiators[0].recip_miscut_rad)
+    g = rows.G[0] / np.linalg.norm(rows.G[0])
+    assert abs(np.degrees(np.arccos(g[2])) - 45.0) < 1e-9
