@@ -32,7 +32,10 @@ struct BremSeg {
     Real T;       // keV
     Real p_i;     // momentum / (m c)
     Real beta_i;
-    Real path0, path1;
+    // Escape geometry: FP64 keeps the clipped end depths (e0, e1); the float
+    // path keeps the exit-side depth of the shallower end toward the top (e0)
+    // and the bottom (e1) and the depth difference |end1 - end0| (e2).
+    Real e0, e1, e2;
     Real nL[kBremMaxEl];     // n_el * 1e24 * L * 1e-8  [1/cm^2]
     Real den_i[kBremMaxEl];  // 1 - exp(-2 pi Z alpha / beta_i)
 };
@@ -83,8 +86,17 @@ __device__ __forceinline__ void brem_stage(BremSeg<Real> &b, const pb_brem_args 
     const Real vz = (Real)a.v_hat[3 * s + 2];
     // Depth of each segment end below the top face, clipped to the slab;
     // the escape path toward n is depth/|n_z| (up) or (T - depth)/|n_z|.
-    b.path0 = fmin(fmax(z - half * vz, (Real)0), T_slab);
-    b.path1 = fmin(fmax(z + half * vz, (Real)0), T_slab);
+    const Real d0 = fmin(fmax(z - half * vz, (Real)0), T_slab);
+    const Real d1 = fmin(fmax(z + half * vz, (Real)0), T_slab);
+    if constexpr (sizeof(Real) == 8) {
+        b.e0 = d0;
+        b.e1 = d1;
+        b.e2 = 0;
+    } else {
+        b.e0 = fmin(d0, d1);
+        b.e1 = fmin(T_slab - d0, T_slab - d1);
+        b.e2 = fabs(d1 - d0);
+    }
     const bool rad = a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
     const Real path_cm = (Real)a.L[s] * (Real)1e-8;
     for (int el = 0; el < a.n_el; ++el) {
@@ -211,8 +223,8 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
                 for (int dd = 0; dd < kBremMaxDir; ++dd) {
                     if (dd < nd) {
                         const Real f = inv_nz[dd];
-                        const Real p0 = up[dd] ? b.path0 * f : (T_slab - b.path0) * f;
-                        const Real p1 = up[dd] ? b.path1 * f : (T_slab - b.path1) * f;
+                        const Real p0 = up[dd] ? b.e0 * f : (T_slab - b.e0) * f;
+                        const Real p1 = up[dd] ? b.e1 * f : (T_slab - b.e1) * f;
                         part[dd] += nsig * b_mean_transmission<Real>(p0 * mu, p1 * mu);
                     }
                 }
@@ -225,27 +237,39 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
                 //   otherwise:                  nsig 2^(-A f) (1 - D/2 + D^2/6 - D^3/24) f ln 2,
                 // the series where the difference would cancel (D^4/120 < 1e-10).
                 // The fast form (all 16 tiles on one side, per-thread registers
-                // for f) costs two SFU exponentials and ~6 FMAs per direction.
+                // for f) is instruction-issue bound, so each direction costs six
+                // instructions on either branch: the difference form
+                //   w 2^(-A f) - w 2^(-(A+B) f)          (2 FMUL, 2 SFU, 2 FMA), or
+                // the series folded per (segment, energy) into a polynomial in f,
+                //   f (m0 + f (m1 + f m2)) 2^(-A f),  m0 = nsig ln 2,
+                //   m1 = -m0 Bl / 2, m2 = m0 Bl^2 / 6, Bl = B ln 2
+                // (2 FMA, 2 FMUL, 1 SFU, 1 FMA; the D^3/24 term is below float
+                // rounding for D <= 0.01).
                 const float mu2 = mu * 1.44269504f;
-                const float A_dn = mu2 * fminf(T_slab - b.path0, T_slab - b.path1);
-                const float A_up = mu2 * fminf(b.path0, b.path1);
-                const float B = mu2 * fabsf(b.path1 - b.path0);
+                const float A_dn = mu2 * b.e1;
+                const float A_up = mu2 * b.e0;
+                const float B = mu2 * b.e2;
                 if (fast) {
                     const float A = side_all > 0 ? A_up : A_dn;
                     if (B * f_min_ln2 > 0.01f) {
                         const float w = __fdividef(nsig, B);
+                        const float nA = -A, nC = -(A + B);
 #pragma unroll
                         for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                            const float m = 1.0f - ex2_approx(-B * fr[dd]);
-                            part[dd] = fmaf(w * m, ex2_approx(-A * fr[dd]), part[dd]);
+                            part[dd] = fmaf(w, ex2_approx(nA * fr[dd]), part[dd]);
+                            part[dd] = fmaf(-w, ex2_approx(nC * fr[dd]), part[dd]);
                         }
                     } else {
+                        const float m0 = nsig * 0.69314718f;
+                        const float Bl = B * 0.69314718f;
+                        const float m1 = -0.5f * m0 * Bl;
+                        const float m2 = m0 * Bl * Bl * (1.0f / 6.0f);
+                        const float nA = -A;
 #pragma unroll
                         for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                            const float fl = fr[dd] * 0.69314718f;
-                            const float D = B * fl;
-                            const float ratio = fmaf(D, fmaf(D, fmaf(D, -1.0f / 24.0f, 1.0f / 6.0f), -0.5f), 1.0f);
-                            part[dd] = fmaf(nsig * fl * ratio, ex2_approx(-A * fr[dd]), part[dd]);
+                            const float f = fr[dd];
+                            const float t = fmaf(f, fmaf(f, m2, m1), m0) * f;
+                            part[dd] = fmaf(t, ex2_approx(nA * f), part[dd]);
                         }
                     }
                 } else {
