@@ -301,7 +301,8 @@ def main():
         e_tile, e_tot = errs(hyb)
         sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
                "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
-               "final_mse": losses[-1], "exact_stride": args.exact_stride,
+               "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
+               "diverged_epochs_redone": int(model.retries), "exact_stride": args.exact_stride,
                "coarse_bins": int(model.n_out),
                "spectrum_error": {"reference": "exact mixed-precision scorer on the same histories, coarse bins",
                                   "max_over_tiles_rel_to_tile_peak": e_tile, "detector_total_rel_to_peak": e_tot,

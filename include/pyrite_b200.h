@@ -450,7 +450,7 @@ int pb_mlp_features(const pb_mlp_infer_args *args, void *X, float *weight, void 
 /* spec[d][o] += t_scale (W5[o] . hsum[d] + b5[o] lsum[d]); W5 FP32 [n_out][256]. */
 int pb_mlp_head(int32_t n_dir, int32_t n_out, const float *W5, const float *b5, const double *hsum,
                 const double *lsum, double t_scale, double *spec, void *stream);
-/* W FP32 [256][cols] -> bf16 chunks of kc (16 or 64) columns in the
+/* W FP32 [256][cols] -> bf16 chunks of kc (16, 32 or 64) columns in the
  * interleaved core-matrix layout the inference kernel streams. */
 int pb_mlp_pack_umma(int32_t cols, int32_t kc, const float *W, void *out, void *stream);
 

@@ -292,7 +292,8 @@ int pb_mlp_head(int32_t n_dir, int32_t n_out, const float *W5, const float *b5, 
 }
 
 int pb_mlp_pack_umma(int32_t cols, int32_t kc, const float *W, void *out, void *stream) {
-    if (cols < 1 || (kc != 16 && kc != 64) || !W || !out) return fail(PB_ERR_INVALID, "pb_mlp_pack_umma: bad arguments");
+    if (cols < 1 || (kc != 16 && kc != 32 && kc != 64) || !W || !out)
+        return fail(PB_ERR_INVALID, "pb_mlp_pack_umma: bad arguments");
     cudaError_t e = pb::launch_mlp_pack_umma(cols, kc, W, out, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "pb_mlp_pack_umma: launch");
     return PB_OK;

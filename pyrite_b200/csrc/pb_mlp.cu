@@ -634,14 +634,15 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_kernel(const pb_mlp_
 // Two-tile ping-pong variant: the epilogues of one tile overlap the MMAs of
 // the other.
 //
-// 288 threads: warpgroup 0 (warps 0-3) and warpgroup 1 (warps 4-7) each own a
-// tile slot -- 256 tensor-memory columns, an X and an H buffer -- and warp 8's
-// lane 0 is the producer: it streams weight chunks and issues the MMAs of the
-// two slots in the order (layer 1: slot 0, slot 1), (layer 2: slot 0, slot 1),
-// ..., so the tensor core works on one slot while the other slot's warpgroup
-// runs its epilogue. A warpgroup hands its slot to the producer through
-// in_ready[s] (one arrival by its leader after a named-barrier sync of the
-// group) and gets the accumulator back through acc_full[s] (tcgen05.commit).
+// 576 threads: warps 0-7 and warps 8-15 each own a tile slot -- 256
+// tensor-memory columns, an X and an H buffer -- as two warpgroups, one per
+// 128-column half of every layer's epilogue; warp 17's lane 0 streams the
+// weight chunks through the stages and warp 16's lane 0 issues the MMAs of
+// the two slots in the order (layer 1: slot 0, slot 1), (layer 2: slot 0,
+// slot 1), ..., so the tensor core works on one slot while the other slot's
+// warps run its epilogue, and a weight copy never waits behind an MMA issue. A slot's 256 threads hand it to the producer through in_ready[s]
+// (one arrival by its leader after a named-barrier sync of the slot) and get
+// the accumulator back through acc_full[s] (tcgen05.commit).
 // Blocks own an even number of tiles (an odd range gets one empty tile, all
 // of whose rows weigh 0). Every wait is bounded; a timeout sets the status
 // word and an abort flag that every role checks after its waits.
@@ -657,13 +658,16 @@ static int infer_variant() {
     return v;
 }
 
-constexpr int kPPThreads = 288;
+constexpr int kPPThreads = 576;
+constexpr int kPPProducerWarp = 16;  // MMA issue
+constexpr int kPPLoaderWarp = 17;    // weight streaming
 constexpr int kPPStages = 2;
-constexpr uint32_t kPPSmem = kInfW1 + 2 * (128 * 16 * 2) + 2 * (128 * 256 * 2) + kPPStages * kInfChunk +
+constexpr uint32_t kPPChunk = kInfChunk;
+constexpr uint32_t kPPSmem = kInfW1 + 2 * (128 * 16 * 2) + 2 * (128 * 256 * 2) + kPPStages * kPPChunk +
                              4 * 256 * 4 + 2 * 257 * 4 + 256;
 
 __device__ __forceinline__ void wg_sync(int slot) {
-    asm volatile("bar.sync %0, 128;" ::"r"(1 + slot) : "memory");
+    asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
 }
 
 __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_mlp_infer_args a) {
@@ -672,7 +676,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
     uint8_t *sX = sW1 + kInfW1;                 // [2] x 4 KB
     uint8_t *sH = sX + 2 * (128 * 16 * 2);      // [2] x 64 KB
     uint8_t *sW = sH + 2 * (128 * 256 * 2);     // kPPStages x 32 KB
-    float *sBias = reinterpret_cast<float *>(sW + kPPStages * kInfChunk);  // [4][256]
+    float *sBias = reinterpret_cast<float *>(sW + kPPStages * kPPChunk);   // [4][256]
     float *sHsum = sBias + 4 * 256;                                         // [2][257]
     uint64_t *bar = reinterpret_cast<uint64_t *>(
         (reinterpret_cast<uintptr_t>(sHsum + 2 * 257) + 15) & ~static_cast<uintptr_t>(15));
@@ -711,32 +715,47 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
     umma::fence_after_sync();
     const uint32_t taddr = *tslot;
 
-    if (warp == 8) {
-        // ------------------------- producer -------------------------
+    if (warp == kPPLoaderWarp) {
+        // -------------------------- loader --------------------------
+        // Streams the weight chunks into the stages as soon as the MMAs of a
+        // stage's previous chunk are done, independently of the MMA issue.
         if (lane == 0 && n_pairs > 0) {
-            const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
             const uint8_t *wsrc[3] = {static_cast<const uint8_t *>(a.w_packed[0]),
                                       static_cast<const uint8_t *>(a.w_packed[1]),
                                       static_cast<const uint8_t *>(a.w_packed[2])};
+            mbar_expect_tx(w1_bar, kInfW1);
+            bulk_g2s(sW1, a.w1_packed, kInfW1, w1_bar);
             // Chunk q of the stream: per tile pair 24 chunks, layer (q % 24) / 8
             // of W2..W4, K-chunk q % 4 (each layer's four chunks twice, once
             // per slot).
-            auto load_chunk = [&](uint32_t q) -> bool {
-                const uint32_t st = q % kPPStages;
-                if (q >= kPPStages && !mbar_wait(&empty[st], (q / kPPStages - 1u) & 1u)) return false;
-                const uint32_t layer = (q % 24u) / 8u, kc = q & 3u;
-                mbar_expect_tx(&full[st], kInfChunk);
-                bulk_g2s(sW + st * kInfChunk, wsrc[layer] + (size_t)kc * kInfChunk, kInfChunk, &full[st]);
-                return true;
-            };
-            bool good = true;
-            mbar_expect_tx(w1_bar, kInfW1);
-            bulk_g2s(sW1, a.w1_packed, kInfW1, w1_bar);
             const uint32_t q_total = (uint32_t)n_pairs * 24u;
-            uint32_t q_load = 0, q_mma = 0;
-            for (; q_load + 1 < (uint32_t)kPPStages && q_load < q_total && good; ++q_load) good = load_chunk(q_load);
+            bool good = true;
+            uint32_t q = 0;
+            for (; q < q_total; ++q) {
+                const uint32_t st = q % kPPStages;
+                if (q >= kPPStages) good = mbar_wait(&empty[st], (q / kPPStages - 1u) & 1u);
+                if (!good || *s_abort) break;
+                const uint32_t layer = (q % 24u) / 8u, kc = q & 3u;
+                mbar_expect_tx(&full[st], kPPChunk);
+                bulk_g2s(sW + st * kPPChunk, wsrc[layer] + (size_t)kc * kPPChunk, kPPChunk, &full[st]);
+            }
+            if (!good) {
+                *s_abort = 1;
+                set_status(a.status, PB_DEV_WAIT_TIMEOUT);
+            }
+            // Drain the copies still in flight (bounded) before the block exits:
+            // the last kPPStages issued chunks, whose stages nothing reuses.
+            for (uint32_t k = q > (uint32_t)kPPStages ? q - kPPStages : 0u; k < q; ++k)
+                mbar_wait(&full[k % kPPStages], (k / kPPStages) & 1u);
+            mbar_wait(w1_bar, 0u);
+        }
+    } else if (warp == kPPProducerWarp) {
+        // ------------------------- MMA issue -------------------------
+        if (lane == 0 && n_pairs > 0) {
+            const uint32_t idesc = umma::idesc_bf16_f32(128, 256);
+            uint32_t q_mma = 0;
             uint32_t in_phase[2] = {0u, 0u};
-            good = good && mbar_wait(w1_bar, 0u);
+            bool good = mbar_wait(w1_bar, 0u);
             for (int64_t p = 0; p < n_pairs && good; ++p) {
                 for (int layer = 0; layer < 4 && good; ++layer) {
                     for (int slot = 0; slot < 2 && good; ++slot) {
@@ -754,7 +773,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                                 const uint32_t st = q_mma % kPPStages;
                                 good = mbar_wait(&full[st], (q_mma / kPPStages) & 1u);
                                 if (!good) break;
-                                const uint32_t w0 = smem_addr(sW + st * kInfChunk);
+                                const uint32_t w0 = smem_addr(sW + st * kPPChunk);
                                 for (int ks = 0; ks < 4; ++ks)
                                     umma::mma_bf16(d_tmem,
                                                    umma::smem_desc(h0 + (uint32_t)kc * 1024u + ks * 256u, 128u,
@@ -763,10 +782,6 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                                                    (kc > 0 || ks > 0) ? 1u : 0u);
                                 umma::commit(&empty[st]);
                                 ++q_mma;
-                                if (q_load < q_total && q_load < q_mma + kPPStages - 1) {
-                                    good = load_chunk(q_load);
-                                    ++q_load;
-                                }
                             }
                         }
                         umma::commit(&acc_full[slot]);
@@ -777,15 +792,16 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                 *s_abort = 1;
                 set_status(a.status, PB_DEV_WAIT_TIMEOUT);
             }
-            // Drain copies still in flight (bounded) before the block exits.
-            for (uint32_t q = q_mma; q < q_load; ++q) mbar_wait(&full[q % kPPStages], (q / kPPStages) & 1u);
         }
     } else {
         // --------------------- epilogue warpgroups ---------------------
-        const int slot = warp >> 2;
-        const int r = tid - 128 * slot;  // row of the tile
-        const int wq = r >> 5;           // warp within the group: TMEM lanes 32 wq..
-        const bool leader = r == 0;
+        const int slot = warp >> 3;
+        const int half = (warp >> 2) & 1;     // columns [128 half, 128 half + 128)
+        const int rs = tid - 256 * slot;      // thread within the slot
+        const int r = rs & 127;               // row of the tile
+        const int wq = warp & 3;              // TMEM lanes 32 wq.. (the warp's quadrant)
+        const bool leader = rs == 0;
+        const int col0 = 128 * half;
         uint8_t *mX = sX + slot * 4096;
         uint8_t *mH = sH + slot * 65536;
         float *hs = sHsum + slot * 257;
@@ -796,7 +812,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
         auto flush = [&](int d) {
             wg_sync(slot);
             if (d >= 0) {
-                for (int i = r; i < 257; i += 128) {
+                for (int i = rs; i < 257; i += 256) {
                     const float v = hs[i];
                     if (v != 0.0f) {
                         if (i < 256) atomicAdd(&a.hsum[(int64_t)d * 256 + i], (double)v);
@@ -840,9 +856,12 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
             }
             float x[6];
             const float wrow = real ? fm(a, tile * 128 + r, n_seg, d, x) : (fm(a, n_seg, n_seg, d, x), 0.0f);
-            *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 0u, kInfSboX)) =
-                make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
-            *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 8u, kInfSboX)) = make_uint4(0u, 0u, 0u, 0u);
+            if (half == 0) {
+                *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 0u, kInfSboX)) =
+                    make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
+                *reinterpret_cast<uint4 *>(mX + umma::core_offset((uint32_t)r, 8u, kInfSboX)) =
+                    make_uint4(0u, 0u, 0u, 0u);
+            }
             hand_over();
             bool ok = true;
             for (int layer = 0; layer < 4 && ok; ++layer) {
@@ -850,7 +869,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                 if (!ok) break;
                 const float *bias = sBias + layer * 256;
                 if (layer < 3) {
-                    for (int c0 = 0; c0 < 256; c0 += 16) {
+                    for (int c0 = col0; c0 < col0 + 128; c0 += 16) {
                         float v[16];
                         umma::tmem_ld16(t_base + (uint32_t)c0, v);
                         uint32_t pk[8];
@@ -865,7 +884,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                     }
                     hand_over();
                 } else {
-                    for (int c0 = 0; c0 < 256; c0 += 16) {
+                    for (int c0 = col0; c0 < col0 + 128; c0 += 16) {
                         float v[16];
                         umma::tmem_ld16(t_base + (uint32_t)c0, v);
 #pragma unroll
@@ -898,7 +917,7 @@ __global__ void __launch_bounds__(kPPThreads, 1) mlp_infer_pp_kernel(const pb_ml
                     }
                     float wsum = wrow;
                     for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
-                    if (lane == 0 && wsum != 0.0f) atomicAdd(&hs[256], wsum);
+                    if (half == 0 && lane == 0 && wsum != 0.0f) atomicAdd(&hs[256], wsum);
                     // Tensor-memory reads of this slot are complete before the
                     // next tile's features are handed over (hand_over fences).
                 }

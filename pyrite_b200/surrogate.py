@@ -191,27 +191,50 @@ class Surrogate:
         mlp.adam(self.flat, self.grad, self.m, self.v, lr, b1, b2, eps, wd, self.step)
         self.repack()
 
-    def train(self, data, *, epochs=3, batch=8192, lr=2e-3, lr_final=1e-4, log=None):
-        """Adam over the pre-shuffled dataset ``data`` (``make_training_set``)."""
+    def train(self, data, *, epochs=3, batch=8192, lr=2e-3, lr_final=1e-4, log=None, max_retries=3):
+        """Adam over the pre-shuffled dataset ``data`` (``make_training_set``).
+
+        An epoch whose loss is not finite (a divergent step) is undone: the
+        parameters and Adam moments go back to the end of the previous epoch,
+        the learning-rate schedule is halved, and the epoch runs again (at
+        most ``max_retries`` times in all)."""
         X, Xt, T = data["X"], data["Xt"], data["T"]
         self.t_scale = float(data["t_scale"])
         N = X.shape[0] // batch * batch
         ws = self._workspace(batch)
-        steps = epochs * (N // batch)
+        per_epoch = N // batch
+        steps = epochs * per_epoch
         losses = []
-        k = 0
-        for ep in range(epochs):
+        self.retries = 0
+        scale = 1.0
+        ep = 0
+        while ep < epochs:
+            snap = (self.flat.clone(), self.m.clone(), self.v.clone(), self.step)
             ws["loss"].zero_()
+            k = ep * per_epoch
             for b0 in range(0, N, batch):
                 frac = k / max(steps - 1, 1)
-                lr_k = lr * (lr_final / lr) ** frac
+                lr_k = scale * lr * (lr_final / lr) ** frac
                 self.train_step(X[b0:b0 + batch], Xt[:, b0:b0 + batch], T[b0:b0 + batch], ws, lr_k)
                 k += 1
             torch.cuda.synchronize(self.device)
             loss = float(ws["loss"].item()) / (N * self.n_out)
+            finite = bool(np.isfinite(loss)) and bool(torch.isfinite(self.flat).all().item())
+            if not finite and self.retries < max_retries:
+                self.flat.copy_(snap[0])
+                self.m.copy_(snap[1])
+                self.v.copy_(snap[2])
+                self.step = snap[3]
+                self.repack()
+                self.retries += 1
+                scale *= 0.5
+                if log:
+                    log(f"epoch {ep}: loss {loss} not finite; restarting it at {scale:g} x the learning rate")
+                continue
             losses.append(loss)
             if log:
                 log(f"epoch {ep}: mse {loss:.4e}")
+            ep += 1
         if int(ws["status"].item()) != 0:
             raise L.PyriteB200Error(f"surrogate training: device status {int(ws['status'].item())}")
         return losses
