@@ -40,6 +40,11 @@ ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
 # Bethe-Heitler + Elwert per (segment, tile, energy): ~60 flops of dsigma/dk shared by the 16 tiles plus
 # ~15 of segment-mean escape per tile (transcendental-heavy: the FP32 roofline is a loose bound).
 ALG_FLOPS_BREM = 20.0
+# DRAM bytes (read + write) per history of the three scorers, from one ncu
+# capture each of a 2,048-history batch of this workload (profiles/*_si50_2048hist.md);
+# a kernel's traffic grows with its segments, so a full launch is this x histories.
+DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 7.0e6 / 2048, "brem_kernel": 5.226752e6 / 2048,
+                          "mlp_infer_kernel": 5.484032e6 / 2048}
 MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"]) \
     if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
 
@@ -335,11 +340,11 @@ def main():
         "cxr_kernel": {"bound": "fp32", "kernel": "cxr_kernel<float> (exact PXR+CBS lines + bin-mean deposit)",
                        "achieved": cxr_tflops, "peak": peak_fp32, "unit": "TFLOP/s", "frac": cxr_tflops / peak_fp32,
                        "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
-                       "traffic": None},
+                       "traffic": DRAM_BYTES_PER_HISTORY["cxr_kernel"] * H},
         "brem_kernel": {"bound": "fp32", "kernel": "brem_kernel<float> (Bethe-Heitler + Elwert, 16 tiles)",
                         "achieved": brem_tflops, "peak": peak_fp32, "unit": "TFLOP/s",
                         "frac": brem_tflops / peak_fp32, "peak_source": "nominal FP32 CUDA-core peak",
-                        "traffic": None},
+                        "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H},
     }
     if sur is not None:
         t_sample, t_inf = cases["surrogate"].t_split
@@ -349,7 +354,8 @@ def main():
             "bound": "tensor", "kernel": "mlp_infer_kernel (tcgen05 BF16, 4 hidden layers per segment x tile)",
             "achieved": inf_tflops, "peak": MEASURED_BF16_SUSTAINED, "unit": "TFLOP/s",
             "frac": inf_tflops / MEASURED_BF16_SUSTAINED,
-            "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)", "traffic": None}
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+            "traffic": DRAM_BYTES_PER_HISTORY["mlp_infer_kernel"] * H}
         sur["kernel_ms"] = {"transport": r_head["t_tr"] if head == "surrogate" else results["surrogate"]["t_tr"],
                             "exact_subsample": t_sample, "surrogate_infer": t_inf,
                             "brem": results["surrogate"]["t_brem"]}
