@@ -27,6 +27,9 @@ constexpr int kBremChunk = 256;
 constexpr int kBremMaxEl = 4;
 constexpr int kBremMaxDir = 16;
 
+// A staged segment. FP64 keeps the reference's factors; the float path
+// folds the per-segment ones of its cross-section form (brem_nsig):
+// beta_i holds beta_i / p_i^2 and nL[el] holds n_el L Z_el^2 den_i[el].
 template <class Real>
 struct BremSeg {
     Real T;       // keV
@@ -53,6 +56,13 @@ __device__ __forceinline__ float b_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Reciprocal on the SFU (about 1 ulp), for the float path.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 
@@ -102,13 +112,33 @@ __device__ __forceinline__ void brem_stage(BremSeg<Real> &b, const pb_brem_args 
     for (int el = 0; el < a.n_el; ++el) {
         b.nL[el] = rad ? (Real)(a.n_ang3[el] * 1e24) * (Real)1 * path_cm : (Real)0;
         b.den_i[el] = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
+        if constexpr (sizeof(Real) == 4) {
+            const Real Z = (Real)a.Z[el];
+            b.nL[el] *= Z * Z * b.den_i[el];
+        }
     }
+    if constexpr (sizeof(Real) == 4) b.beta_i = b.beta_i / (p_i * p_i);
 }
 
+// Per-thread constants of the float cross-section form.
+struct BremKConst {
+    float kc;     // k / (m c^2)^2  [1/keV]
+    float c2mk;   // 2 m c^2 - k    [keV]
+    float c0k;    // c0 ln 2 / k_ev
+};
+
 // sum_el n_el L dsigma/dk(Z_el, T, k) of one staged segment (brem.py:396-479).
+// The float path evaluates the same expression as
+//   rs = 1/sqrt(q), q = T_f (T_f + 2 m c^2):   p_f = q rs / m c^2,
+//   1/beta_f = (1 + T_f / m c^2) m c^2 rs,
+//   ln((p_i + p_f) / (p_i - p_f)) = ln 2 log2((p_i + p_f)^2 / (k (T + T_f + 2 m c^2) / (m c^2)^2)),
+//   (p_i^2 - p_f^2 = k (T + T_f + 2 m c^2) / (m c^2)^2, without cancellation),
+// so one (segment, energy) costs five SFU operations (rsqrt, rcp, lg2, and
+// ex2 + rcp per element of the Elwert factor).
 template <class Real>
 __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T_f, const Real *Zs, int n_el,
-                                          Real k_ev, Real c0, Real za, Real mc2) {
+                                          Real k_ev, Real c0, Real za, Real mc2, const BremKConst &kk,
+                                          const float *zl) {
     Real nsig = 0;
     if constexpr (sizeof(Real) == 8) {
         const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
@@ -123,16 +153,16 @@ __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T
     } else {
         const float inv_mc2 = 1.0f / 510.99895f;
         const float q = T_f * (T_f + 2.0f * mc2);
-        const float p_f = q * rsqrtf(q) * inv_mc2;
-        const float beta_f = __fdividef(p_f, 1.0f + T_f * inv_mc2);
-        const float diff = __fdividef(k * (b.T + T_f + 2.0f * mc2) * inv_mc2 * inv_mc2, b.p_i + p_f);
-        const float born_log = __logf(__fdividef(b.p_i + p_f, fmaxf(diff, 1e-30f)));
-        const float inv_beta_f = __fdividef(1.0f, beta_f);
-        const float common = __fdividef(c0, k_ev * b.p_i * b.p_i) * born_log * b.beta_i * inv_beta_f;
+        const float rs = rsqrtf(q);
+        const float p_f = q * rs * inv_mc2;
+        const float sp = b.p_i + p_f;
+        const float dpp = kk.kc * fmaf(2.0f, b.T, kk.c2mk);  // p_i^2 - p_f^2
+        const float lg = __log2f(fmaxf(sp * sp * rcp_approx(fmaxf(dpp, 1e-30f)), 1e-30f));
+        const float inv_beta_f = fmaf(T_f, inv_mc2, 1.0f) * (rs * mc2);
+        const float common = kk.c0k * b.beta_i * lg * inv_beta_f;  // beta_i holds beta_i / p_i^2
         for (int el = 0; el < n_el; ++el) {
-            const float Z = Zs[el];
-            const float den_f = 1.0f - __expf(-za * Z * inv_beta_f);
-            nsig += b.nL[el] * (Z * Z) * common * __fdividef(b.den_i[el], den_f);
+            const float den_f = 1.0f - ex2_approx(-zl[el] * inv_beta_f);
+            nsig = fmaf(b.nL[el] * common, rcp_approx(den_f), nsig);  // nL holds n L Z^2 den_i
         }
     }
     return nsig;
@@ -149,6 +179,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     // shared memory (keeps the registers for the per-chunk partials).
     __shared__ double acc[kBremMaxDir][kBremThreads];
     __shared__ Real Zs[kBremMaxEl];
+    __shared__ float zl[kBremMaxEl];  // 2 pi alpha Z log2(e)
     __shared__ Real inv_nz[kBremMaxDir];
     __shared__ int up[kBremMaxDir];
     __shared__ float inv_f_ln2[kBremMaxDir];
@@ -159,7 +190,10 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     const bool on = e < a.n_E;
     const Real mc2 = (Real)510.99895;
     const Real za = (Real)(2.0 * kPi * kAlphaFs);
-    if (threadIdx.x < n_el) Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+    if (threadIdx.x < n_el) {
+        Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+        zl[threadIdx.x] = (float)(2.0 * kPi * kAlphaFs * a.Z[threadIdx.x] * 1.4426950408889634);
+    }
     if (threadIdx.x < nd) {
         const Real nz = (Real)a.n_hat[3 * (d0 + threadIdx.x) + 2];
         inv_nz[threadIdx.x] = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
@@ -190,6 +224,10 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
     const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
     const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
+    BremKConst kk;
+    kk.kc = (float)(k_kev_d / (510.99895 * 510.99895));
+    kk.c2mk = (float)(2.0 * 510.99895 - k_kev_d);
+    kk.c0k = (float)(16.0 / 3.0 * kAlphaFs * kReCm2 * 0.6931471805599453 / fmax(k_kev_d * 1e3, 1e-30));
 #pragma unroll
     for (int j = 0; j < kBremMaxDir; ++j) acc[j][threadIdx.x] = 0.0;
     if (a.n_seg_device) {
@@ -217,7 +255,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
             const BremSeg<Real> &b = segs[j];
             const Real T_f = b.T - k;
             if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2);
+            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
             if constexpr (sizeof(Real) == 8) {
 #pragma unroll
                 for (int dd = 0; dd < kBremMaxDir; ++dd) {
@@ -328,6 +366,7 @@ __global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_bre
     __shared__ BremPieces<Real> pcs[kChunk];
     __shared__ double acc[kBremMaxDir][kBremThreads];
     __shared__ Real Zs[kBremMaxEl];
+    __shared__ float zl[kBremMaxEl];  // 2 pi alpha Z log2(e)
     __shared__ Real inv_nz[kBremMaxDir];
     __shared__ int up[kBremMaxDir];
     __shared__ double zt_s[kMaxEscLayers], zb_s[kMaxEscLayers];
@@ -339,7 +378,10 @@ __global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_bre
     const bool on = e < a.n_E;
     const Real mc2 = (Real)510.99895;
     const Real za = (Real)(2.0 * kPi * kAlphaFs);
-    if (threadIdx.x < n_el) Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+    if (threadIdx.x < n_el) {
+        Zs[threadIdx.x] = (Real)a.Z[threadIdx.x];
+        zl[threadIdx.x] = (float)(2.0 * kPi * kAlphaFs * a.Z[threadIdx.x] * 1.4426950408889634);
+    }
     if (threadIdx.x < nd) {
         const Real nz = (Real)a.n_hat[3 * (d0 + threadIdx.x) + 2];
         inv_nz[threadIdx.x] = (Real)1 / fmax(fabs(nz), (Real)1.0e-12);
@@ -386,6 +428,10 @@ __global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_bre
     const Real k = (Real)k_kev_d;
     const Real k_ev = fmax((Real)(k_kev_d * 1e3), (Real)1e-30);
     const Real c0 = (Real)(16.0 / 3.0 * kAlphaFs * kReCm2);
+    BremKConst kk;
+    kk.kc = (float)(k_kev_d / (510.99895 * 510.99895));
+    kk.c2mk = (float)(2.0 * 510.99895 - k_kev_d);
+    kk.c0k = (float)(16.0 / 3.0 * kAlphaFs * kReCm2 * 0.6931471805599453 / fmax(k_kev_d * 1e3, 1e-30));
 #pragma unroll
     for (int j = 0; j < kBremMaxDir; ++j) acc[j][threadIdx.x] = 0.0;
     if (a.n_seg_device) {
@@ -425,7 +471,7 @@ __global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_bre
             const BremSeg<Real> &b = segs[j];
             const Real T_f = b.T - k;
             if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2);
+            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
             const BremPieces<Real> &P = pcs[j];
             for (int p = 0; p < P.np; ++p) {
                 const int m = P.m[p];
