@@ -209,6 +209,59 @@ def time_pipeline(case, args, rank, world, torch, dist, n_steps, n_warm):
     return total_ms, t_tr, t_cxr, t_brem
 
 
+def run_sweep(args, torch):
+    """The design sweep: 256 configurations (seed 1; tilt, thickness, Si/HOPG,
+    energy, histories), each case scored exactly in mixed precision (PXR+CBS
+    bin means on 1024 bins, Bethe-Heitler, exit tallies). Timed twice on the
+    same histories: every case's batches launched one after another with the
+    default plan (largest batch, default transport block) on one stream, and
+    the whole sweep autotuned per case, spread over concurrent streams and
+    replayed as one CUDA graph."""
+    from pyrite_b200.sweep import DesignSweep, c3_configs
+
+    torch.cuda.set_device(0)
+    configs = c3_configs(n=256, seed=1, histories_scale=args.sweep_scale)
+    t0 = time.perf_counter()
+    sw = DesignSweep(configs, device="cuda")
+    t_build = time.perf_counter() - t0
+    # warm every case once (module load, tables) outside both timings
+    for case in sw.cases:
+        case.run_batch(1 << 40, min(256, case.batch))
+        case.reset()
+    torch.cuda.synchronize()
+    plain, t_plain = sw.run(use_graph=False)
+    t0 = time.perf_counter()
+    sw.autotune()
+    sw.set_streams(args.sweep_streams)
+    t_tune = time.perf_counter() - t0
+    tuned_eager, t_tuned = sw.run(use_graph=False)
+    sw.capture()
+    sw.run(use_graph=True)  # warm replay
+    graph, t_graph = sw.run(use_graph=True)
+    n_hist = sw.total_histories
+    worst = 0.0
+    for a, b in zip(plain, graph):
+        for k in ("cxr", "brem"):
+            peak = float(np.max(np.abs(a[k])))
+            if peak > 0:
+                worst = max(worst, float(np.max(np.abs(a[k] - b[k]))) / peak)
+    line = {
+        "metric": "design sweep histories/s (256 configurations, one graph replay)", "value": n_hist / t_graph,
+        "unit": "histories/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "256 configs from seed 1: tilt U(0,20) deg, thickness logU(10,1000) um, Si or HOPG, "
+                               "E0 logU(5,100) MeV, histories logU(1e4,1e6) x %g; 1024 bins 1-60 keV; "
+                               "PXR+CBS bin-mean + Bethe-Heitler + exit tallies" % args.sweep_scale,
+                   "histories": n_hist},
+        "sequential_plain": {"value": n_hist / t_plain, "seconds": t_plain},
+        "autotuned_eager": {"value": n_hist / t_tuned, "seconds": t_tuned},
+        "graph": {"seconds": t_graph, "launches_in_graph": sw.launches(), "streams": sw.n_streams},
+        "speedup_vs_sequential_plain": t_plain / t_graph,
+        "max_spectrum_difference_vs_plain": worst,
+        "setup_s": {"build": t_build, "autotune": t_tune},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,6 +279,11 @@ def main():
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
     ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--workload", default="c2", choices=["c2", "sweep"],
+                    help="c2: the headline step (default); sweep: the 256-configuration design sweep, "
+                         "one graph replay against sequential plain launches (its own JSON line)")
+    ap.add_argument("--sweep-scale", type=float, default=1.0, help="scale of every sweep case's histories")
+    ap.add_argument("--sweep-streams", type=int, default=8, help="concurrent case streams of the tuned sweep")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -247,6 +305,11 @@ def main():
         return
 
     import torch
+
+    if args.workload == "sweep":
+        if rank == 0:
+            run_sweep(args, torch)
+        return
 
     dist = None
     if world > 1:

@@ -4,13 +4,16 @@ A sweep is a list of independent cases (crystal, tilt, thickness, beam
 energy, history count), as the reference runs design studies
 (``pyrite/montecarlo/runner/case_driver.py:1025`` once per case). Each case
 keeps its own device-resident tables and segment buffer (``ScoringCase``);
-its histories are split into batches whose size and transport block shape
-the autotuner picks per case by timing trial batches. The whole sweep --
-every batch of every case: transport, PXR+CBS lines, bremsstrahlung and
-tallies -- is then captured once into a CUDA graph and launched with a
-single replay, so thousands of small launches cost one host submission.
+its histories are split into batches of the largest size its buffer holds,
+and the autotuner picks each case's transport block shape by timing one
+full batch per option. Cases run concurrently on several streams, assigned
+largest-first to the least-loaded stream, so a small case (a thin slab, a
+few thousand histories) does not leave most of the GPU idle. The whole
+sweep -- every batch of every case: transport, PXR+CBS lines,
+bremsstrahlung and tallies, on every stream -- is captured once into a CUDA
+graph (a fork/join of the streams) and launched with a single replay.
 Histories are keyed by (case seed, history index), so the graph, the eager
-loop and any batch split give the same histories.
+loop, any batch split and any stream assignment give the same histories.
 """
 
 from __future__ import annotations
@@ -104,7 +107,7 @@ class DesignSweep:
     SEG_BYTES = 76  # segment list row: r_mid, v_hat, L, E (FP64), elec_id (i64), layer (i32)
 
     def __init__(self, configs, *, precision="mixed", device=None, batch_options=(4096, 16384),
-                 thread_options=(128, 256), n_bins=1024, segment_budget_bytes=256 << 20):
+                 thread_options=(128, 256), n_bins=1024, segment_budget_bytes=256 << 20, streams=1):
         self.configs = list(configs)
         self.device = torch.device(device or "cuda")
         self.batch_options = tuple(sorted(batch_options))
@@ -117,6 +120,20 @@ class DesignSweep:
         self.plan = [(c.batch, 0) for c in self.cases]
         self.graph = None
         self.tuning = []
+        self.set_streams(streams)
+
+    def set_streams(self, n):
+        """Assign the cases to ``n`` streams, largest expected work first to
+        the least-loaded stream (work ~ histories x segments per history)."""
+        self.n_streams = max(1, int(n))
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.n_streams)]
+        work = [cfg.histories * c.seg_capacity / max(c.batch, 1) for cfg, c in zip(self.configs, self.cases)]
+        load = [0.0] * self.n_streams
+        self.assign = [0] * len(self.cases)
+        for i in sorted(range(len(work)), key=lambda i: -work[i]):
+            s = min(range(self.n_streams), key=lambda k: load[k])
+            self.assign[i] = s
+            load[s] += work[i]
 
     def _case(self, i, segs_per_history):
         cap_hist = min(max(self.batch_options), self.configs[i].histories,
@@ -140,36 +157,50 @@ class DesignSweep:
         return self._case(i, segs)
 
     def autotune(self, trial_histories=None, e_start=1 << 40):
-        """Pick (batch size, transport block threads) per case from timed trial
-        batches (histories outside the sweep's own range; accumulators reset)."""
+        """Pick the transport block threads per case from one timed batch per
+        option at the case's own batch size (histories outside the sweep's
+        own range; accumulators reset). Batches stay at the largest size the
+        case's buffer holds: a smaller batch only adds launches. A trial
+        smaller than a full batch (``trial_histories``) under-fills the GPU
+        and times nothing useful, so it is capped below at the batch size
+        unless the case has fewer histories."""
         self.tuning = []
         for i, (cfg, case) in enumerate(zip(self.configs, self.cases)):
+            b = min(case.batch, cfg.histories)
+            n = b if trial_histories is None else min(b, max(int(trial_histories), b))
             best = None
-            for b in sorted({min(b, case.batch) for b in self.batch_options}):
-                for t in self.thread_options:
-                    case.targs.block_threads = t
-                    n = b if trial_histories is None else min(b, trial_histories)
-                    case.run_batch(e_start, n)  # warm (LUT staging, module load)
-                    ev0 = torch.cuda.Event(enable_timing=True)
-                    ev1 = torch.cuda.Event(enable_timing=True)
-                    ev0.record()
-                    case.run_batch(e_start + n, n)
-                    ev1.record()
-                    torch.cuda.synchronize(self.device)
-                    per_hist = ev0.elapsed_time(ev1) / n
-                    if best is None or per_hist < best[0]:
-                        best = (per_hist, b, t)
+            for t in self.thread_options:
+                case.targs.block_threads = t
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record()
+                case.run_batch(e_start, n)
+                ev1.record()
+                torch.cuda.synchronize(self.device)
+                per_hist = ev0.elapsed_time(ev1) / n
+                if best is None or per_hist < best[0]:
+                    best = (per_hist, t)
             case.reset()
-            case.targs.block_threads = best[2]
-            self.plan[i] = (best[1], best[2])
-            self.tuning.append({"case": i, "batch": best[1], "block_threads": best[2], "us_per_history": 1e3 * best[0]})
+            case.targs.block_threads = best[1]
+            self.plan[i] = (case.batch, best[1])
+            self.tuning.append({"case": i, "batch": case.batch, "block_threads": best[1],
+                                "us_per_history": 1e3 * best[0]})
         return self.tuning
 
     def _launch_all(self):
-        for cfg, case, (b, t) in zip(self.configs, self.cases, self.plan):
+        """Every batch of every case, each case on its assigned stream, the
+        streams forked from and joined back to the current one."""
+        main = torch.cuda.current_stream(self.device)
+        for st in self.streams:
+            st.wait_stream(main)
+        for i, (cfg, case, (b, t)) in enumerate(zip(self.configs, self.cases, self.plan)):
+            st = self.streams[self.assign[i]]
             case.targs.block_threads = t
-            for e in range(0, cfg.histories, b):
-                case.run_batch(e, min(b, cfg.histories - e))
+            with torch.cuda.stream(st):
+                for e in range(0, cfg.histories, b):
+                    case.run_batch(e, min(b, cfg.histories - e), stream=st)
+        for st in self.streams:
+            main.wait_stream(st)
 
     def capture(self):
         """Record every batch of every case into one CUDA graph."""

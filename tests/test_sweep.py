@@ -1,8 +1,10 @@
 """Batched design sweep: configurations, autotuned batching, one-graph replay.
 
 GPU: the graph replay of the whole sweep gives the eager loop's results
-(same histories; to the float rounding of per-pass partial sums, whose grouping follows the nondeterministic segment order), and a different batch
-split gives the same spectra (histories keyed by index).
+(same histories; to the float rounding of per-pass partial sums, whose
+grouping follows the nondeterministic segment order), so do the cases spread
+over concurrent streams (eager and as one fork/join graph), and a different
+batch split gives the same spectra (histories keyed by index).
 """
 
 import numpy as np
@@ -45,7 +47,21 @@ def test_graph_replay_matches_eager(cuda_device):
             peak = np.max(np.abs(a[k]))
             assert peak > 0
             assert np.max(np.abs(a[k] - b[k])) <= 2e-6 * peak  # float partial sums, segment order
+    # cases spread over concurrent streams, eager and as one fork/join graph
+    sw.set_streams(3)
+    assert sorted(set(sw.assign)) == [0, 1, 2]
+    multi, _ = sw.run(use_graph=False)
+    sw.capture()
+    multi_graph, _ = sw.run(use_graph=True)
+    for a, b, c in zip(eager, multi, multi_graph):
+        np.testing.assert_array_equal(a["fates"], b["fates"])
+        np.testing.assert_array_equal(a["fates"], c["fates"])
+        for k in ("cxr", "brem"):
+            peak = np.max(np.abs(a[k]))
+            assert np.max(np.abs(a[k] - b[k])) <= 2e-6 * peak
+            assert np.max(np.abs(a[k] - c[k])) <= 2e-6 * peak
     # another batch split, same histories
+    sw.set_streams(1)
     sw.plan = [(512, t) for _b, t in sw.plan]
     split, _ = sw.run(use_graph=False)
     for a, b in zip(eager, split):
