@@ -39,7 +39,7 @@ namespace pb {
 
 constexpr int kSegTile = 16;
 constexpr int kRowChunk = 64;
-constexpr int kCxrThreads = 512;
+constexpr int kCxrThreads = 256;  // two resident blocks per SM (128 registers each)
 constexpr int kQueue = kSegTile * kRowChunk;  // every pair of a pass may keep a line
 constexpr int kXQueue = 2048;   // queued exact-window bins per class and pass
 constexpr int kMaxTab = 4096;   // E_tab / delta staged in shared memory up to this size
@@ -977,14 +977,17 @@ __device__ __forceinline__ void smem_add(double *p, double v) {
     asm volatile("red.shared.add.f64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "d"(v) : "memory");
 }
 
+// A kept line's three far-field moments about its centre bin, added to the
+// direction's moments in global memory (L2 reductions: a few per kept line,
+// so the block keeps no on-chip copy of the moment array).
 __device__ __forceinline__ void line_moments(double E_r, double a, double w, const LineWindow &lw,
                                              const BinAxis &ax, double *mom) {
     const int slot = lw.c + ax.pad;
     const double m = w / (2.0 * a * a);
     const double dd = E_r - centre_of(ax, lw.c);
-    smem_add(&mom[3 * slot + 0], m);
-    smem_add(&mom[3 * slot + 1], m * dd);
-    smem_add(&mom[3 * slot + 2], m * dd * dd);
+    atomicAdd(&mom[3 * slot + 0], m);
+    atomicAdd(&mom[3 * slot + 1], m * dd);
+    atomicAdd(&mom[3 * slot + 2], m * dd * dd);
 }
 
 // Persistent blocks over the flattened (direction, segment tile) work, in
@@ -998,7 +1001,7 @@ __device__ __forceinline__ void line_moments(double E_r, double a, double w, con
 //   B   the queued lines' (line, bin) work is cut into 4-item chunks spread
 //       over the block; edges shared by consecutive bins are evaluated once.
 template <class Real, bool kLayered>
-__global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
+__global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a, int K_far, int far_pad) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool kMixed = sizeof(Real) == 4;
     const int n_g = a.tables.n_g;
@@ -1037,9 +1040,8 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
     cur = reinterpret_cast<unsigned char *>(dtail_s + (tab_smem ? n_tab : 0));
     cur = (unsigned char *)(((uintptr_t)cur + 15) & ~(uintptr_t)15);
     double *spec_s = reinterpret_cast<double *>(cur);
-    double *mom_s = spec_s + (binmean ? n_E : 0);
     const int n_mom = n_E + 2 * far_pad;
-    float *spec_f = reinterpret_cast<float *>(mom_s + (K_far > 0 ? 3 * n_mom : 0));
+    float *spec_f = reinterpret_cast<float *>(spec_s + (binmean ? n_E : 0));
     float *edges_f = spec_f + (binmean ? n_E : 0);  // mixed path: float bin edges
     // Layered absorber: per-segment escape pieces, layer thicknesses and bounds.
     unsigned char *esc_raw = reinterpret_cast<unsigned char *>(edges_f + (binmean && kMixed ? n_E + 1 : 0));
@@ -1069,8 +1071,6 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
         for (int j = tid; j < n_E; j += blockDim.x) { spec_s[j] = 0.0; spec_f[j] = 0.0f; }
         if (kMixed)
             for (int j = tid; j <= n_E; j += blockDim.x) edges_f[j] = (float)a.edges[j];
-        if (K_far > 0)
-            for (int j = tid; j < 3 * n_mom; j += blockDim.x) mom_s[j] = 0.0;
     }
     if (tid == 0) { q_count = 0; p_count = 0; xq_count[0] = 0; xq_count[1] = 0; }
     if constexpr (kLayered) {
@@ -1131,13 +1131,6 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
             for (int j = tid; j < n_E; j += blockDim.x) {
                 if (spec_s[j] != 0.0) atomicAdd(&gspec[j], spec_s[j]);
                 spec_s[j] = 0.0;
-            }
-            if (K_far > 0) {
-                double *gm = a.far_moments + (int64_t)d * n_mom * 3;
-                for (int j = tid; j < 3 * n_mom; j += blockDim.x) {
-                    if (mom_s[j] != 0.0) atomicAdd(&gm[j], mom_s[j]);
-                    mom_s[j] = 0.0;
-                }
             }
         }
         __syncthreads();
@@ -1262,7 +1255,9 @@ __global__ void __launch_bounds__(kCxrThreads) cxr_kernel(const pb_cxr_args a, i
                 qStart[j] = lw.nb;
                 qB0[j] = lw.b0;
                 qC[j] = lw.mom ? lw.c : INT_MIN;
-                if (lw.mom) line_moments((double)qE[j], (double)qA[j], (double)qW[j], lw, ax, mom_s);
+                if (lw.mom)
+                    line_moments((double)qE[j], (double)qA[j], (double)qW[j], lw, ax,
+                                 a.far_moments + (int64_t)d * n_mom * 3);
                 // From here on qW holds the line's mass-to-mean scale w pi / a.
                 qW[j] = (Real)((double)qW[j] * kPi / (double)qA[j]);
             }
@@ -1484,7 +1479,6 @@ static size_t cxr_smem_bytes(const pb_cxr_args &a, int far_pad, bool with_moment
     if (a.quadrature == PB_QUAD_BINMEAN) {
         b += (sizeof(double) + sizeof(float)) * (size_t)a.n_E + sizeof(int) * 2 * kXQueue;
         if (sizeof(Real) == 4) b += sizeof(float) * ((size_t)a.n_E + 1) + 16;
-        if (with_moments) b += sizeof(double) * 3 * ((size_t)a.n_E + 2 * (size_t)far_pad);
     }
     if (a.n_layer > 0)
         b += 16 + sizeof(EscSeg<Real>) * kSegTile + sizeof(double) * 2 * kMaxEscLayers + sizeof(Real) * kMaxEscLayers;
