@@ -346,11 +346,16 @@ def main():
 
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        data = S.make_training_set(spec, n_seg=args.train_segments, n_dir=args.train_dirs,
-                                   dir_chunk=max(1, 2 ** 20 // args.train_segments), seed=1000, device="cuda")
+        # Data-parallel on N > 1 GPUs: each rank builds 1/N of the segments of
+        # the training set (its own seed) and the gradients are averaged.
+        n_seg_rank = max(1024, args.train_segments // world)
+        pg = dist.group.WORLD if dist is not None else None
+        data = S.make_training_set(spec, n_seg=n_seg_rank, n_dir=args.train_dirs,
+                                   dir_chunk=max(1, 2 ** 20 // n_seg_rank), seed=1000 + rank, device="cuda",
+                                   process_group=pg)
         model = S.Surrogate("cuda", seed=0)
-        losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5)
-        n_pairs = int(data["X"].shape[0])
+        losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5, process_group=pg)
+        n_pairs = int(data["X"].shape[0]) * world
         del data
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0

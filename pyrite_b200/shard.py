@@ -67,3 +67,17 @@ def reduce_results(results: dict, group=None) -> dict:
         if buf is not t:
             t.copy_(buf)
     return results
+
+
+def average_gradients(grad, group=None):
+    """Data-parallel training step: replace ``grad`` (one flat tensor of every
+    parameter's gradient) by its mean over the process group, in place, so
+    every rank applies the same optimizer step to the same parameters. One
+    all-reduce of the ~330 k surrogate parameters per step."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    if world > 1:
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+        grad.div_(world)
+    return grad

@@ -150,7 +150,7 @@ class Surrogate:
         ws["status"] = torch.zeros(1, device=dev, dtype=torch.int32)
         return ws
 
-    def train_step(self, X, Xt, T, ws, lr, wd=0.0, b1=0.9, b2=0.999, eps=1e-8, group=None):
+    def train_step(self, X, Xt, T, ws, lr, wd=0.0, b1=0.9, b2=0.999, eps=1e-8, group=None, grad_hook=None):
         """One Adam step on the batch X [B,16] bf16 (Xt its transpose view
         [16, B] with any row stride), T [B, n_out] bf16 scaled targets.
 
@@ -187,20 +187,43 @@ class Surrogate:
             mlp.gemm(ws["dZt"], a_prev_t, out_f32=g[f"W{i}"], M=HIDDEN, N=K_IN if i == 1 else HIDDEN, K=B, status=st)
             if i > 1:
                 up, up_t = dzb, self.Wt[f"W{i}"]
+        if grad_hook is not None:
+            grad_hook(self.grad)
         self.step += 1
         mlp.adam(self.flat, self.grad, self.m, self.v, lr, b1, b2, eps, wd, self.step)
         self.repack()
 
-    def train(self, data, *, epochs=3, batch=8192, lr=2e-3, lr_final=1e-4, log=None, max_retries=3):
+    def train(self, data, *, epochs=3, batch=8192, lr=2e-3, lr_final=1e-4, log=None, max_retries=3,
+              process_group=None):
         """Adam over the pre-shuffled dataset ``data`` (``make_training_set``).
 
         An epoch whose loss is not finite (a divergent step) is undone: the
         parameters and Adam moments go back to the end of the previous epoch,
         the learning-rate schedule is halved, and the epoch runs again (at
-        most ``max_retries`` times in all)."""
+        most ``max_retries`` times in all).
+
+        ``process_group`` trains data-parallel: every rank holds its own
+        shard of the data (same size on every rank) and the same initial
+        parameters, the gradient is averaged over the group before each
+        Adam step (``shard.average_gradients``), and the epoch loss is the
+        group's, so every rank takes the same steps, retries included."""
+        import torch.distributed as dist
+
+        from .shard import average_gradients
+
+        hook = None
+        world = 1
+        if process_group is not None:
+            world = dist.get_world_size(process_group)
+            hook = lambda g: average_gradients(g, process_group)  # noqa: E731
         X, Xt, T = data["X"], data["Xt"], data["T"]
         self.t_scale = float(data["t_scale"])
         N = X.shape[0] // batch * batch
+        if world > 1:
+            # the same number of steps on every rank; one target scale (rank 0's)
+            nt = torch.tensor([N], device=self.device, dtype=torch.int64)
+            dist.all_reduce(nt, op=dist.ReduceOp.MIN, group=process_group)
+            N = int(nt.item())
         ws = self._workspace(batch)
         per_epoch = N // batch
         steps = epochs * per_epoch
@@ -215,11 +238,19 @@ class Surrogate:
             for b0 in range(0, N, batch):
                 frac = k / max(steps - 1, 1)
                 lr_k = scale * lr * (lr_final / lr) ** frac
-                self.train_step(X[b0:b0 + batch], Xt[:, b0:b0 + batch], T[b0:b0 + batch], ws, lr_k)
+                self.train_step(X[b0:b0 + batch], Xt[:, b0:b0 + batch], T[b0:b0 + batch], ws, lr_k,
+                                grad_hook=hook)
                 k += 1
             torch.cuda.synchronize(self.device)
-            loss = float(ws["loss"].item()) / (N * self.n_out)
-            finite = bool(np.isfinite(loss)) and bool(torch.isfinite(self.flat).all().item())
+            if world > 1:
+                red = torch.stack([ws["loss"].reshape(()).double(),
+                                   (~torch.isfinite(self.flat)).any().double()])
+                dist.all_reduce(red, group=process_group)
+                loss = float(red[0].item()) / (world * N * self.n_out)
+                finite = bool(np.isfinite(loss)) and float(red[1].item()) == 0.0
+            else:
+                loss = float(ws["loss"].item()) / (N * self.n_out)
+                finite = bool(np.isfinite(loss)) and bool(torch.isfinite(self.flat).all().item())
             if not finite and self.retries < max_retries:
                 self.flat.copy_(snap[0])
                 self.m.copy_(snap[1])
@@ -349,11 +380,13 @@ def _bin(lines, n_lines, dir0, n_dir, n_seg, grid, out):
 
 
 def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None, seed=101, device=None,
-                      grid=None, log=None, shuffle=True):
+                      grid=None, log=None, shuffle=True, process_group=None):
     """Exact per-(segment, direction) coarse spectra per unit length with their features.
 
     Returns a dict with X [N, 16] bf16, Xt [16, N] bf16, T [N, n_bins] bf16
-    (targets / t_scale), t_scale, grid; rows shuffled.
+    (targets / t_scale), t_scale, grid; rows shuffled. With ``process_group``
+    (data-parallel training, each rank its own ``seed``) the ranks agree on
+    one target scale: the RMS over the first direction chunk of every rank.
     """
     device = torch.device(device or "cuda")
     grid = grid or CoarseGrid.of(spec.E_grid)
@@ -380,7 +413,13 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
         _bin(lines, n_lines, 0, nd, n_seg, grid, tgt)
         tgt.view(nd, n_seg, grid.n_bins).mul_(inv_L[None, :, None])
         if t_scale is None:
-            t_scale = float(tgt.square().mean().sqrt().item()) or 1.0
+            ms = tgt.square().mean().double().reshape(1)
+            if process_group is not None:
+                import torch.distributed as dist
+
+                dist.all_reduce(ms, group=process_group)
+                ms /= dist.get_world_size(process_group)
+            t_scale = float(ms.sqrt().item()) or 1.0
         T[d0 * n_seg:(d0 + nd) * n_seg] = (tgt / t_scale).to(torch.bfloat16)
         a = _feature_args(spec, seg, n_seg, torch.as_tensor(uv[d0:d0 + nd], dtype=torch.float32, device=device))
         L.check(L.load().pb_mlp_features(C.byref(a), X[d0 * n_seg:].data_ptr(), None, _stream()), "pb_mlp_features")

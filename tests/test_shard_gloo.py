@@ -99,3 +99,54 @@ def test_two_gloo_ranks_equal_one_process():
         peak = np.max(np.abs(ref[k]))
         assert peak > 0
         assert np.max(np.abs(got[k] - ref[k])) <= 1e-12 * peak
+
+
+def _dp_data():
+    rng = np.random.default_rng(5)
+    X = rng.normal(size=(64, 6))
+    t = X @ np.array([0.5, -1.0, 2.0, 0.0, 0.3, -0.7]) + 0.1 * rng.normal(size=64)
+    return X, t
+
+
+def _dp_steps(X, t, grad_fn, steps=20, lr=0.05):
+    import torch
+
+    w = torch.zeros(6, dtype=torch.float64)
+    Xt, tt = torch.from_numpy(X), torch.from_numpy(t)
+    for _ in range(steps):
+        g = 2.0 * Xt.T @ (Xt @ w - tt) / Xt.shape[0]
+        g = grad_fn(g)
+        w -= lr * g
+    return w.numpy()
+
+
+def _dp_rank_main(rank, world, port, out_path):
+    import torch.distributed as dist
+
+    from pyrite_b200.shard import average_gradients, history_range
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        X, t = _dp_data()
+        lo, n = history_range(X.shape[0], rank, world)  # equal shards (64 / 2)
+        w = _dp_steps(X[lo:lo + n], t[lo:lo + n], lambda g: average_gradients(g))
+        np.save(out_path + f".{rank}.npy", w)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_gradient_average_equals_full_batch():
+    """Surrogate training on N ranks averages the flat gradient before every
+    optimizer step (``shard.average_gradients``): with equal shards and equal
+    initial parameters every rank follows the full-batch trajectory."""
+    import torch.multiprocessing as mp
+
+    X, t = _dp_data()
+    ref = _dp_steps(X, t, lambda g: g)
+    with tempfile.TemporaryDirectory() as tmp:
+        out_path = os.path.join(tmp, "w")
+        mp.start_processes(_dp_rank_main, args=(2, _free_port(), out_path), nprocs=2, join=True,
+                           start_method="spawn")
+        w0, w1 = np.load(out_path + ".0.npy"), np.load(out_path + ".1.npy")
+    np.testing.assert_array_equal(w0, w1)
+    np.testing.assert_allclose(w0, ref, rtol=1e-12, atol=1e-14)
