@@ -354,7 +354,7 @@ def _cxr_lines(spec, seg, n_seg, n_hats, device, cap_per_pair=64):
     a.n_E = 1
     a.E_grid = _ptr(h.f64([30000.0]))
     a.spec = None  # lines only, no node spectrum
-    cap = int(n_seg) * n_dir * cap_per_pair
+    cap = int(int(n_seg) * n_dir * cap_per_pair)
     count = h.zeros(1, torch.int64)
     lines = {"E": h.empty(cap, torch.float64), "a": h.empty(cap, torch.float64), "w": h.empty(cap, torch.float64),
              "dir": h.zeros(cap, torch.int32), "seg": h.zeros(cap, torch.int64)}
