@@ -356,6 +356,7 @@ def main():
         model = S.Surrogate("cuda", seed=0)
         losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5, process_group=pg)
         n_pairs = int(data["X"].shape[0]) * world
+        n_dropped = int(data.get("nonfinite_pairs_dropped", 0))
         del data
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
@@ -375,7 +376,8 @@ def main():
         sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
                "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
                "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
-               "diverged_epochs_redone": int(model.retries), "exact_stride": args.exact_stride,
+               "diverged_epochs_redone": int(model.retries), "nonfinite_pairs_dropped": n_dropped,
+               "exact_stride": args.exact_stride,
                "coarse_bins": int(model.n_out),
                "spectrum_error": {"reference": "exact mixed-precision scorer on the same histories, coarse bins",
                                   "max_over_tiles_rel_to_tile_peak": e_tile, "detector_total_rel_to_peak": e_tot,

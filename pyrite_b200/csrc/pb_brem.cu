@@ -59,11 +59,40 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
+// Two floats in one 64-bit register pair, and the packed FP32 arithmetic of
+// sm_100 (one instruction for both halves).
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 // Reciprocal on the SFU (about 1 ulp), for the float path.
 __device__ __forceinline__ float rcp_approx(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
+}
+
+// 2^x of both halves.
+__device__ __forceinline__ unsigned long long f2_ex2(unsigned long long x) {
+    float lo, hi;
+    f2_unpack(x, lo, hi);
+    return f2_pack(ex2_approx(lo), ex2_approx(hi));
 }
 
 template <class Real>
@@ -219,6 +248,10 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         }
     }
     const bool fast = sizeof(Real) == 4 && nd == kBremMaxDir && side_all != 0;
+    // The fast form keeps the 16 direction factors as 8 packed pairs.
+    unsigned long long fr2[kBremMaxDir / 2];
+#pragma unroll
+    for (int i = 0; i < kBremMaxDir / 2; ++i) fr2[i] = f2_pack(fr[2 * i], fr[2 * i + 1]);
     const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
     const Real k = (Real)k_kev_d;
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
@@ -246,6 +279,57 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         }
         __syncthreads();
         if (!on) continue;
+        if constexpr (sizeof(Real) == 4) {
+            if (fast) {
+                // The fast form below (see the scalar form's comment), on
+                // packed direction pairs: per pair of directions the
+                // difference form costs 2 FMUL2, 4 SFU, 2 FFMA2 and the series
+                // form 2 FFMA2, 2 FMUL2, 2 SFU, 1 FFMA2.
+                unsigned long long part2[kBremMaxDir / 2];
+#pragma unroll
+                for (int i = 0; i < kBremMaxDir / 2; ++i) part2[i] = 0ull;
+                const float mu2 = mu * 1.44269504f;
+                for (int j = 0; j < nc; ++j) {
+                    const BremSeg<Real> &b = segs[j];
+                    const Real T_f = b.T - k;
+                    if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
+                    const float nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
+                    const float A = mu2 * (side_all > 0 ? b.e0 : b.e1);
+                    const float B = mu2 * b.e2;
+                    if (B * f_min_ln2 > 0.01f) {
+                        const float w = __fdividef(nsig, B);
+                        const unsigned long long nA = f2_pack(-A, -A), nC = f2_pack(-(A + B), -(A + B));
+                        const unsigned long long w2 = f2_pack(w, w), nw2 = f2_pack(-w, -w);
+#pragma unroll
+                        for (int i = 0; i < kBremMaxDir / 2; ++i) {
+                            part2[i] = f2_fma(w2, f2_ex2(f2_mul(nA, fr2[i])), part2[i]);
+                            part2[i] = f2_fma(nw2, f2_ex2(f2_mul(nC, fr2[i])), part2[i]);
+                        }
+                    } else {
+                        const float m0 = nsig * 0.69314718f;
+                        const float Bl = B * 0.69314718f;
+                        const float m1 = -0.5f * m0 * Bl;
+                        const float m2 = m0 * Bl * Bl * (1.0f / 6.0f);
+                        const unsigned long long m0_2 = f2_pack(m0, m0), m1_2 = f2_pack(m1, m1),
+                                                 m2_2 = f2_pack(m2, m2), nA = f2_pack(-A, -A);
+#pragma unroll
+                        for (int i = 0; i < kBremMaxDir / 2; ++i) {
+                            const unsigned long long f = fr2[i];
+                            const unsigned long long t = f2_mul(f2_fma(f, f2_fma(f, m2_2, m1_2), m0_2), f);
+                            part2[i] = f2_fma(t, f2_ex2(f2_mul(nA, f)), part2[i]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < kBremMaxDir / 2; ++i) {
+                    float lo, hi;
+                    f2_unpack(part2[i], lo, hi);
+                    acc[2 * i][threadIdx.x] += (double)lo * (double)inv_f_ln2[2 * i];
+                    acc[2 * i + 1][threadIdx.x] += (double)hi * (double)inv_f_ln2[2 * i + 1];
+                }
+                continue;
+            }
+        }
         // Partial sums per chunk (float on the mixed path), folded into the
         // FP64 accumulators once per chunk.
         Real part[kBremMaxDir];

@@ -325,8 +325,15 @@ def transported_segments(spec, n_hist, seed, device, precision="mixed"):
     L.check(case.lib.pb_transport(C.byref(t), _stream()), "pb_transport")
     torch.cuda.synchronize(device)
     n = int(case.seg_count.item())
-    seg = {"r": case.seg_r[:n].clone(), "v": case.seg_v[:n].clone(), "L": case.seg_L[:n].clone(),
-           "E": case.seg_E[:n].clone(), "id": torch.zeros(n, dtype=torch.int64, device=device)}
+    # The transport appends segments in a nondeterministic order; put them in
+    # history order (decreasing energy along each track) so a seeded pick is
+    # reproducible.
+    E = case.seg_E[:n]
+    order = torch.argsort(E, descending=True, stable=True)
+    order = order[torch.argsort(case.seg_id[:n][order], stable=True)]
+    seg = {"r": case.seg_r[:n][order].contiguous(), "v": case.seg_v[:n][order].contiguous(),
+           "L": case.seg_L[:n][order].contiguous(), "E": E[order].contiguous(),
+           "id": torch.zeros(n, dtype=torch.int64, device=device)}
     return seg, n
 
 
@@ -395,7 +402,10 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
     n_hist = n_hist or max(4096, 4 * n_seg)
     all_seg, n_all = transported_segments(spec, n_hist, seed, device)
     gen = torch.Generator(device="cpu").manual_seed(seed)
-    pick = torch.randperm(n_all, generator=gen)[:n_seg].to(device)
+    # Targets are per unit length: segments of zero length carry no emission
+    # and would divide by zero, so they are not candidates.
+    cand = torch.nonzero(all_seg["L"] > 0.0).flatten().cpu()
+    pick = cand[torch.randperm(cand.numel(), generator=gen)[:n_seg]].to(device)
     seg = {k: v[pick].contiguous() for k, v in all_seg.items()}
     n_seg = int(pick.numel())
     rng = np.random.default_rng(seed)
@@ -427,13 +437,23 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
         if log and (d0 // dir_chunk) % 8 == 0:
             log(f"targets: {d0 + nd}/{n_dir} directions")
     Lrow = seg["L"].to(torch.float32).repeat(n_dir)
+    # A pair whose target or features are not finite (a degenerate line of
+    # the exact scorer) is dropped rather than poisoning every step after it.
+    good = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
+    n_bad = int((~good).sum().item())
+    if n_bad:
+        keep = torch.nonzero(good).flatten()
+        X, T, Lrow = X[keep], T[keep], Lrow[keep]
+        N = int(keep.numel())
+        if log:
+            log(f"targets: dropped {n_bad} pairs with non-finite values")
     if shuffle:
         perm = torch.randperm(N, generator=gen).to(device)
         X = X[perm].contiguous()
         T = T[perm].contiguous()
         Lrow = Lrow[perm].contiguous()
     return {"X": X, "Xt": X.t().contiguous(), "T": T, "L": Lrow, "t_scale": t_scale, "grid": grid,
-            "n_seg": n_seg, "n_dir": n_dir}
+            "n_seg": n_seg, "n_dir": n_dir, "nonfinite_pairs_dropped": n_bad}
 
 
 def _feature_args(spec, seg, n_seg, dir_uv_t):
