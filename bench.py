@@ -274,7 +274,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
-    ap.add_argument("--exact-stride", type=int, default=100,
+    ap.add_argument("--exact-stride", type=int, default=150,
                     help="exact control-variate sub-sample: every n-th history")
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
