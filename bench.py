@@ -82,7 +82,8 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)  # nvidia-smi's start-up, so samples cover the whole region
         except (OSError, FileNotFoundError):
             self.proc = None
         return self

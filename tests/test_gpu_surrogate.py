@@ -235,3 +235,21 @@ def test_control_variate_identity_and_accuracy(cuda_device):
     assert peak > 0
     assert np.max(np.abs(out[1] - exact)) <= 1e-5 * peak
     assert np.max(np.abs(out[8].sum(0) - exact.sum(0))) <= 0.05 * np.max(exact.sum(0))
+
+
+def test_single_tile_inference_variant_matches_torch(cuda_device):
+    """The single-tile inference kernel (``PB_MLP_INFER=serial``, the
+    reference point of the ping-pong kernel; the variant is read once per
+    process) passes the same check against the torch forward pass."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, PB_MLP_INFER="serial")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider",
+                        str(root / "tests" / "test_gpu_surrogate.py"), "-k", "test_infer_matches_torch"],
+                       cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "1 passed" in r.stdout
