@@ -210,6 +210,54 @@ def time_pipeline(case, args, rank, world, torch, dist, n_steps, n_warm):
     return total_ms, t_tr, t_cxr, t_brem
 
 
+def run_stack(args, torch):
+    """The layered stack: 10 MeV on 20 um HOPG / 200 um Si / 1 mm W, four
+    detectors (20/45/90/135 deg) in 4x4 angular tiles each, 4096 bins 1-80 keV;
+    per batch transport, PXR+CBS of both crystal layers, per-layer brem,
+    C/Si/W characteristic lines and tallies, in mixed precision and in FP64."""
+    from pyrite_b200.configs import c5_stack_10mev
+    from pyrite_b200.pipeline import ScoringCase
+
+    torch.cuda.set_device(0)
+    spec = c5_stack_10mev()
+    H = 256
+    out = {}
+    for prec in ("mixed", "fp64"):
+        per = 4096
+        while True:  # size the segment buffer from a trial batch
+            case = ScoringCase(spec, precision=prec, batch_histories=H, segs_per_history=per)
+            case.run_batch(1 << 40, H)
+            torch.cuda.synchronize()
+            if case.device_status() != 4 or per >= 1 << 15:
+                break
+            per *= 2
+            del case
+        case.reset()
+        for w in range(args.warmup):
+            case.run_batch((1 << 40) + (w + 1) * H, H)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for i in range(args.steps):
+            case.run_batch(i * H, H)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        res = case.results()
+        out[prec] = {"histories_per_s": H / (ms / 1e3), "ms_per_batch": ms, "device_status": case.device_status(),
+                     "segments_per_history": float(case.seg_count.item()) / H,
+                     "launches_per_batch": case.kernel_launches_per_batch(),
+                     "cxr_integral": float(res["cxr"].sum()), "brem_integral": float(res["brem"].sum()),
+                     "characteristic_integral": float(res["characteristic"].sum())}
+        del case
+    line = {"metric": "stacked case histories/s (10 MeV HOPG/Si/W, 4 detectors x 16 tiles, 4096 bins)",
+            "value": out["mixed"]["histories_per_s"], "unit": "histories/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic", "histories_per_batch": H, "steps": args.steps,
+            "mixed": out["mixed"], "fp64": out["fp64"],
+            "speedup_mixed_vs_fp64": out["mixed"]["histories_per_s"] / out["fp64"]["histories_per_s"]}
+    print(json.dumps(line), flush=True)
+
+
 def run_sweep(args, torch):
     """The design sweep: 256 configurations (seed 1; tilt, thickness, Si/HOPG,
     energy, histories), each case scored exactly in mixed precision (PXR+CBS
@@ -280,9 +328,10 @@ def main():
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
     ap.add_argument("--train-epochs", type=int, default=6)
-    ap.add_argument("--workload", default="c2", choices=["c2", "sweep"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "sweep", "stack"],
                     help="c2: the headline step (default); sweep: the 256-configuration design sweep, "
-                         "one graph replay against sequential plain launches (its own JSON line)")
+                         "one graph replay against sequential plain launches; stack: the 10 MeV HOPG / Si / W "
+                         "stack with four detectors (each its own JSON line)")
     ap.add_argument("--sweep-scale", type=float, default=1.0, help="scale of every sweep case's histories")
     ap.add_argument("--sweep-streams", type=int, default=8, help="concurrent case streams of the tuned sweep")
     args = ap.parse_args()
@@ -310,6 +359,10 @@ def main():
     if args.workload == "sweep":
         if rank == 0:
             run_sweep(args, torch)
+        return
+    if args.workload == "stack":
+        if rank == 0:
+            run_stack(args, torch)
         return
 
     dist = None

@@ -322,7 +322,12 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
     // Per-history state.
     int64_t i = -1;  // local history index; -1 idle, -2 drained
     uint64_t key = 0, draws = 0;
-    Real px = 0, py = 0, pz = 0, dx = 0, dy = 0, dz = 1;
+    // Positions stay FP64 in both precisions: deep in a thick stack (z ~ 1e7
+    // Angstrom) a float position cannot resolve the boundary nudge or an
+    // Angstrom-scale step, and a particle leaving a layer upward would sit on
+    // the boundary for ever. Flight lengths and physics follow Real.
+    double px = 0, py = 0, pz = 0;
+    Real dx = 0, dy = 0, dz = 1;
     double E = 0.0, clk = 0.0;
     int64_t nseg = 0, steps = 0;
     Real tau_left = -1;
@@ -342,7 +347,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     const int64_t e = p.e_start + i;
                     double pos[3], dir[3], E0;
                     sample_entry<kRng>(p, i, e, pos, dir, E0);
-                    px = (Real)pos[0]; py = (Real)pos[1]; pz = (Real)pos[2];
+                    px = pos[0]; py = pos[1]; pz = pos[2];
                     dx = (Real)dir[0]; dy = (Real)dir[1]; dz = (Real)dir[2];
                     E = E0;
                     clk = 0.0;
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             int L = 0;
             if (n_layers > 1) {
                 // searchsorted(internal_bounds, z, side="right")
-                for (int j = 1; j < n_layers; ++j) L += (ly.z_top[j] <= (double)pz) ? 1 : 0;
+                for (int j = 1; j < n_layers; ++j) L += (ly.z_top[j] <= pz) ? 1 : 0;
             }
             const double z_top = ly.z_top[L], z_bot = ly.z_bot[L];
             const int n_el = ly.n_el[L];
@@ -394,10 +399,10 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             Real step = tau_left * lam;
             bool cross_up = false, cross_dn = false;
             if (dz < (Real)0) {
-                const Real sb = (pz - (Real)z_top) / (-dz);
+                const Real sb = (Real)((pz - z_top) / (double)(-dz));
                 if (step > sb) { step = sb; cross_up = true; }
             } else if (dz > (Real)0) {
-                const Real sb = ((Real)z_bot - pz) / dz;
+                const Real sb = (Real)((z_bot - pz) / (double)dz);
                 if (step > sb) { step = sb; cross_dn = true; }
             }
             bool exit_top = cross_up && z_top <= 0.0;
@@ -462,9 +467,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     p.rows.v_hat[3 * s] = (double)dx;
                     p.rows.v_hat[3 * s + 1] = (double)dy;
                     p.rows.v_hat[3 * s + 2] = (double)dz;
-                    p.rows.r_mid[3 * s] = (double)(px + half * dx);
-                    p.rows.r_mid[3 * s + 1] = (double)(py + half * dy);
-                    p.rows.r_mid[3 * s + 2] = (double)(pz + half * dz);
+                    p.rows.r_mid[3 * s] = px + (double)(half * dx);
+                    p.rows.r_mid[3 * s + 1] = py + (double)(half * dy);
+                    p.rows.r_mid[3 * s + 2] = pz + (double)(half * dz);
                     p.rows.L[s] = (double)step;
                     p.rows.E_start[s] = E_j;
                     p.rows.E_end[s] = E_end;
@@ -490,9 +495,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     p.seg.v_hat[3 * slot] = (double)dx;
                     p.seg.v_hat[3 * slot + 1] = (double)dy;
                     p.seg.v_hat[3 * slot + 2] = (double)dz;
-                    p.seg.r_mid[3 * slot] = (double)(px + half * dx);
-                    p.seg.r_mid[3 * slot + 1] = (double)(py + half * dy);
-                    p.seg.r_mid[3 * slot + 2] = (double)(pz + half * dz);
+                    p.seg.r_mid[3 * slot] = px + (double)(half * dx);
+                    p.seg.r_mid[3 * slot + 1] = py + (double)(half * dy);
+                    p.seg.r_mid[3 * slot + 2] = pz + (double)(half * dz);
                     p.seg.L[slot] = (double)step;
                     p.seg.E_repr[slot] = 0.5 * (E_j + E_end);
                     p.seg.elec_id[slot] = p.e_start + i;
@@ -505,16 +510,16 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             for (int j = 0; j < kMaxLayers; ++j)
                 if (j == L) dep_acc[j] += E_j - E_end;
             nseg += 1;
-            px = px + step * dx;
-            py = py + step * dy;
-            pz = pz + step * dz;
+            px = px + (double)(step * dx);
+            py = py + (double)(step * dy);
+            pz = pz + (double)(step * dz);
             E = E_end;
             clk = t_end;
             tau_left = (Real)-1;
             if (exit_top || exit_bot || cutoff) {
                 code = exit_top ? EXIT_BACK : exit_bot ? EXIT_TRANS : EXIT_CUTOFF;
             } else if (cross_up || cross_dn) {
-                pz += (dz > (Real)0 ? (Real)1 : (Real)-1) * (Real)kEps;
+                pz += (dz > (Real)0 ? 1.0 : -1.0) * kEps;
                 steps += 1;
             } else {
                 int i_el = 0;

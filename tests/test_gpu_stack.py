@@ -80,3 +80,24 @@ def test_stack_brem_and_lines_equal_per_layer_scorers(stack_run):
                for em in spec.char_emitters)
     assert char.max() > 0
     assert np.max(np.abs(res["characteristic"] - char)) <= 1e-10 * np.max(char)
+
+
+def test_mixed_transport_through_the_stack_matches_fp64_step_counts():
+    """The mixed-precision transport keeps FP64 positions: millimetres deep
+    in the stack a float position cannot resolve the boundary nudge, and a
+    particle crossing back out of the W layer would loop on the boundary
+    until the step limit."""
+    from pyrite_b200.configs import c5_stack_10mev
+    from pyrite_b200.pipeline import ScoringCase
+
+    spec = c5_stack_10mev(angular_shape=(1, 1), n_bins=256, si_g_max=4.0)
+    per_hist = {}
+    for prec in ("fp64", "mixed"):
+        case = ScoringCase(spec, precision=prec, batch_histories=64, segs_per_history=1 << 15)
+        case.run_batch(0, 64)
+        torch.cuda.synchronize()
+        assert case.device_status() == 0, (prec, case.device_status())
+        per_hist[prec] = int(case.seg_count.item()) / 64
+        assert int(case.fates.sum().item()) == 64
+    ratio = per_hist["mixed"] / per_hist["fp64"]
+    assert 0.8 < ratio < 1.25, per_hist
