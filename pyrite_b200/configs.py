@@ -3,7 +3,7 @@
 Each builder returns a ``pipeline.CaseSpec`` with the scene's geometry, beam,
 crystal, reflections, detector tiles and spectral grid. The atomic data
 tables come from ``placeholder_data`` (the real Chantler/EPDL data are not
-available to this build); see that module.
+shipped with this package); see that module.
 """
 
 from __future__ import annotations
@@ -86,8 +86,8 @@ def c5_stack_10mev(seed=0, angular_shape=(4, 4), n_bins=4096, si_g_max=8.0, dete
 
     One electron population is transported, at the 5 keV line cutoff; the
     reference transports bremsstrahlung and characteristic emitters again at
-    1 keV with secondary electrons, which need EEDL tables this build does
-    not have."""
+    1 keV with secondary electrons, which need EEDL tables this package does
+    not ship."""
     from .detector import PlanarDetector, tiles_in_sample_frame
     from .pipeline import CharEmitter, Radiator
 

@@ -2,8 +2,8 @@
 
 The reference reads Waasmaier-Kirfel f0 and Chantler f'/f'' through xraydb
 (src/pyrite/materials/atomic.py:1-20) and EPDL attenuation
-(materials/photon_cross_sections.py:74). Neither dataset is available to
-this build, so the tables that the hot path consumes are produced here from
+(materials/photon_cross_sections.py:74). Neither dataset ships with this
+package, so the tables that the hot path consumes are produced here from
 smooth placeholder form factors with the right structure and magnitude:
 
 * f0(s) = Z (0.6 exp(-b s^2) + 0.4 exp(-b s^2 / 4)), b = 8 / (1 + 0.05 Z),
