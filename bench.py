@@ -328,6 +328,9 @@ def main():
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
     ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--train-domain", default="case", choices=["case", "uniform"],
+                    help="surrogate training segments: the case's transport, or spread over the whole input "
+                         "domain (5-100 MeV, +-5 mrad, every depth; adds a 1e5-segment held-out audit)")
     ap.add_argument("--workload", default="c2", choices=["c2", "sweep", "stack"],
                     help="c2: the headline step (default); sweep: the 256-configuration design sweep, "
                          "one graph replay against sequential plain launches; stack: the 10 MeV HOPG / Si / W "
@@ -406,7 +409,7 @@ def main():
         pg = dist.group.WORLD if dist is not None else None
         data = S.make_training_set(spec, n_seg=n_seg_rank, n_dir=args.train_dirs,
                                    dir_chunk=max(1, 2 ** 20 // n_seg_rank), seed=1000 + rank, device="cuda",
-                                   process_group=pg)
+                                   process_group=pg, domain=args.train_domain)
         model = S.Surrogate("cuda", seed=0)
         losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5, process_group=pg)
         n_pairs = int(data["X"].shape[0]) * world
@@ -431,12 +434,18 @@ def main():
                "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
                "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
                "diverged_epochs_redone": int(model.retries), "nonfinite_pairs_dropped": n_dropped,
+               "train_domain": args.train_domain,
                "exact_stride": args.exact_stride,
                "coarse_bins": int(model.n_out),
                "spectrum_error": {"reference": "exact mixed-precision scorer on the same histories, coarse bins",
                                   "max_over_tiles_rel_to_tile_peak": e_tile, "detector_total_rel_to_peak": e_tot,
                                   "surrogate_alone": dict(zip(("max_over_tiles", "detector_total"), errs(pure)))},
                "gate": 0.01, "passed": bool(e_tile <= 0.01)}
+        if args.train_domain == "uniform":
+            # held-out segments over the whole input domain, surrogate alone
+            au = S.audit_uniform(model, spec, n_seg=100_000, device="cuda")
+            sur["audit_uniform_1e5"] = {"max_over_tiles": au["err_tile_max"], "detector_total": au["err_total"],
+                                        "segments": au["segments"], "status": au["status"]}
     if not args.skip_fp64:
         arm("fp64", ScoringCase(spec, precision="fp64", rng="philox", lut=True, batch_histories=H),
             max(1, args.steps // 2))

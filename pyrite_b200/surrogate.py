@@ -386,14 +386,47 @@ def _bin(lines, n_lines, dir0, n_dir, n_seg, grid, out):
             "pb_cxr_bin_lines")
 
 
+def uniform_segments(spec, n_seg, seed, device, L_pool, E_MeV=(E_LO_MEV, E_HI_MEV), half_angle=5e-3):
+    """Synthetic segments spread over the surrogate's input domain: energy
+    log-uniform over ``E_MeV``, direction uniform within +-``half_angle`` of
+    the beam axis on both transverse axes, depth uniform through the slab,
+    and lengths drawn from ``L_pool`` (a case's transported segment lengths:
+    the line shape depends on the length, which is not an input)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(E_MeV[0] * 1e3), np.log(E_MeV[1] * 1e3)
+    E = np.exp(rng.uniform(lo, hi, n_seg))
+    d0 = np.asarray(spec.beam.beam_dir, dtype=float)
+    d0 = d0 / np.linalg.norm(d0)
+    e_x, e_y = _beam_axes(spec)
+    ax, ay = rng.uniform(-half_angle, half_angle, (2, n_seg))
+    v = d0[None, :] + ax[:, None] * e_x[None, :] + ay[:, None] * e_y[None, :]
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    pool = np.asarray(L_pool, dtype=float)
+    L = pool[rng.integers(0, pool.size, n_seg)]
+    T = float(spec.stack.thickness)
+    # keep the whole segment inside the slab
+    half = 0.5 * L * np.abs(v[:, 2])
+    z = rng.uniform(0.0, 1.0, n_seg) * np.maximum(T - 2.0 * half, 0.0) + half
+    r = np.zeros((n_seg, 3))
+    r[:, 2] = z
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=device)  # noqa: E731
+    return {"r": t(r), "v": t(v), "L": t(L), "E": t(E), "id": torch.zeros(n_seg, dtype=torch.int64, device=device)}
+
+
 def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None, seed=101, device=None,
-                      grid=None, log=None, shuffle=True, process_group=None):
+                      grid=None, log=None, shuffle=True, process_group=None, domain="case"):
     """Exact per-(segment, direction) coarse spectra per unit length with their features.
 
     Returns a dict with X [N, 16] bf16, Xt [16, N] bf16, T [N, n_bins] bf16
     (targets / t_scale), t_scale, grid; rows shuffled. With ``process_group``
     (data-parallel training, each rank its own ``seed``) the ranks agree on
     one target scale: the RMS over the first direction chunk of every rank.
+
+    ``domain="case"`` picks segments of the case's own transport (the
+    workload's joint energy / angle / depth distribution); ``"uniform"``
+    spreads them over the surrogate's whole input domain (``uniform_segments``:
+    5-100 MeV log-uniform, +-5 mrad, every depth), with lengths from the
+    case's transport.
     """
     device = torch.device(device or "cuda")
     grid = grid or CoarseGrid.of(spec.E_grid)
@@ -406,7 +439,12 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
     # and would divide by zero, so they are not candidates.
     cand = torch.nonzero(all_seg["L"] > 0.0).flatten().cpu()
     pick = cand[torch.randperm(cand.numel(), generator=gen)[:n_seg]].to(device)
-    seg = {k: v[pick].contiguous() for k, v in all_seg.items()}
+    if domain == "uniform":
+        seg = uniform_segments(spec, int(pick.numel()), seed, device, all_seg["L"][pick].cpu().numpy())
+    elif domain == "case":
+        seg = {k: v[pick].contiguous() for k, v in all_seg.items()}
+    else:
+        raise ValueError(f"unknown training domain {domain!r}")
     n_seg = int(pick.numel())
     rng = np.random.default_rng(seed)
     uv = rng.uniform(-1.0, 1.0, size=(n_dir, 2))
@@ -570,6 +608,19 @@ def train_ensemble(spec, *, k=4, n_seg=16384, n_dir=1024, epochs=10, lr=2e-3, se
     return models
 
 
+def audit_uniform(model, spec, *, n_seg=100_000, seed=303, device=None, grid=None, n_hist=4096):
+    """Surrogate vs exact on held-out segments spread over the input domain
+    (``uniform_segments``, lengths from ``n_hist`` transported histories of a
+    seed of their own), aggregated per tile: the same error measures as
+    ``audit``."""
+    device = torch.device(device or "cuda")
+    grid = grid or CoarseGrid.of(spec.E_grid)
+    pool, n_pool = transported_segments(spec, n_hist, seed, device)
+    Lp = pool["L"][:n_pool]
+    seg = uniform_segments(spec, n_seg, seed, device, Lp[Lp > 0].cpu().numpy())
+    return _audit_on(model, spec, seg, n_seg, device, grid)
+
+
 def audit(model, spec, *, n_hist=4096, seed=202, device=None, grid=None):
     """Surrogate vs exact aggregate spectra on held-out histories at the case's tiles.
 
@@ -581,6 +632,10 @@ def audit(model, spec, *, n_hist=4096, seed=202, device=None, grid=None):
     device = torch.device(device or "cuda")
     grid = grid or CoarseGrid.of(spec.E_grid)
     seg, n_seg = transported_segments(spec, n_hist, seed, device)
+    return _audit_on(model, spec, seg, n_seg, device, grid)
+
+
+def _audit_on(model, spec, seg, n_seg, device, grid):
     n_hats = np.atleast_2d(np.asarray(spec.n_hats, dtype=float))
     uv = tile_uv(spec.detector, spec.angular_shape)
     exact = exact_aggregate(spec, seg, n_seg, n_hats, grid, device).double()

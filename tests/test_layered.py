@@ -254,3 +254,26 @@ def test_stack_case_spec_builds():
                            recip_miscut_rad=spec.radiators[0].recip_miscut_rad)
     g = rows.G[0] / np.linalg.norm(rows.G[0])
     assert abs(np.degrees(np.arccos(g[2])) - 45.0) < 1e-9
+
+
+def test_uniform_training_segments_cover_the_input_domain():
+    """The surrogate's domain-wide training segments: energies log-uniform
+    over 5-100 MeV, directions within 5 mrad of the beam, whole segments
+    inside the slab, lengths from the given pool."""
+    from pyrite_b200.configs import c2_si_50mev
+    from pyrite_b200.surrogate import uniform_segments
+
+    spec = c2_si_50mev(angular_shape=(1, 1))
+    pool = np.array([10.0, 1.0e3, 5.0e4])
+    seg = uniform_segments(spec, 4000, 7, "cpu", pool)
+    E = seg["E"].numpy()
+    assert E.min() >= 5e3 and E.max() <= 1e5
+    assert np.mean(E < np.sqrt(5e3 * 1e5)) == pytest.approx(0.5, abs=0.05)  # log-uniform median
+    v = seg["v"].numpy()
+    d0 = np.asarray(spec.beam.beam_dir) / np.linalg.norm(spec.beam.beam_dir)
+    ang = np.arccos(np.clip(v @ d0, -1, 1))
+    assert ang.max() <= 5e-3 * np.sqrt(2) + 1e-9
+    L, z = seg["L"].numpy(), seg["r"].numpy()[:, 2]
+    assert set(np.unique(L)) <= set(pool)
+    half = 0.5 * L * np.abs(v[:, 2])
+    assert np.all(z - half >= 0) and np.all(z + half <= spec.stack.thickness)
