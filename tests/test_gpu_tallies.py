@@ -55,3 +55,11 @@ def test_tallies_match_per_history_outputs(precision, cuda_device):
     lost = float(n * spec.beam.E0_keV - fE.cpu().numpy().sum())
     dep = float(case.deposit.sum().item())
     assert abs(dep - lost) <= 1e-6 * lost
+    # the same tallies in the reference's summary-table layout
+    from pyrite_b200.summary import case_tally_tables
+
+    tab = case_tally_tables(case)
+    assert int(tab["fates"]["count"].sum()) == n
+    np.testing.assert_array_equal(tab["exit_energy"]["count"].to_numpy(), want_E)
+    np.testing.assert_array_equal(tab["exit_angle"]["count"].to_numpy(), want_th)
+    assert abs(float(tab["depth_loss"]["continuous_loss_keV"].sum()) - dep) <= 1e-9 * dep
