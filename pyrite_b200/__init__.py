@@ -15,6 +15,7 @@ from .api import (  # noqa: F401
     simulate_trajectories,
 )
 from ._lib import PyriteB200Error, load  # noqa: F401
+from .summary import tally_tables  # noqa: F401
 
 __all__ = [
     "BeamSpec",
@@ -26,4 +27,5 @@ __all__ = [
     "mc_characteristic_spectrum",
     "mc_cxr_spectrum",
     "simulate_trajectories",
+    "tally_tables",
 ]
