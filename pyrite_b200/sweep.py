@@ -90,6 +90,20 @@ def case_spec(cfg: SweepConfig, n_bins=1024, theta_obs_deg=20.0):
     )
 
 
+def assign_streams(work, n_streams):
+    """Longest-processing-time assignment: items in decreasing ``work``, each
+    to the stream with the least work so far (ties to the lowest index).
+    Returns the stream index of every item."""
+    n_streams = max(1, int(n_streams))
+    load = [0.0] * n_streams
+    out = [0] * len(work)
+    for i in sorted(range(len(work)), key=lambda i: -work[i]):
+        s = min(range(n_streams), key=lambda k: load[k])
+        out[i] = s
+        load[s] += work[i]
+    return out
+
+
 def L_check(case):
     """Transport one trial batch of ``case`` (transport only) and wait."""
     import ctypes as C
@@ -128,12 +142,7 @@ class DesignSweep:
         self.n_streams = max(1, int(n))
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.n_streams)]
         work = [cfg.histories * c.seg_capacity / max(c.batch, 1) for cfg, c in zip(self.configs, self.cases)]
-        load = [0.0] * self.n_streams
-        self.assign = [0] * len(self.cases)
-        for i in sorted(range(len(work)), key=lambda i: -work[i]):
-            s = min(range(self.n_streams), key=lambda k: load[k])
-            self.assign[i] = s
-            load[s] += work[i]
+        self.assign = assign_streams(work, self.n_streams)
 
     def _case(self, i, segs_per_history):
         cap_hist = min(max(self.batch_options), self.configs[i].histories,

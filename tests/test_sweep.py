@@ -30,6 +30,21 @@ def test_c3_configurations():
     assert c3_configs()[:3] == cfg[:3]  # seeded
 
 
+def test_stream_assignment_balances_work():
+    from pyrite_b200.sweep import assign_streams, c3_configs
+
+    work = [float(c.histories) for c in c3_configs()]
+    a = assign_streams(work, 8)
+    load = np.zeros(8)
+    for w, s in zip(work, a):
+        load[s] += w
+    # largest-first greedy: within the largest item of the mean load
+    assert load.max() - load.mean() <= max(work)
+    assert load.max() / load.mean() < 1.1
+    assert assign_streams([5.0, 1.0, 1.0], 1) == [0, 0, 0]
+    assert assign_streams([5.0, 3.0, 3.0], 2) == [0, 1, 1]
+
+
 @pytest.mark.gpu
 def test_graph_replay_matches_eager(cuda_device):
     from pyrite_b200.sweep import DesignSweep, c3_configs
