@@ -430,6 +430,11 @@ def main():
             return float(per.max()), float(np.max(np.abs(ta - te)) / np.max(te))
 
         e_tile, e_tot = errs(hyb)
+        if dist is not None:
+            # one gate for the whole job: the worst rank's error decides
+            t = torch.tensor([e_tile, e_tot], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_tile, e_tot = float(t[0].item()), float(t[1].item())
         sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
                "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
                "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
