@@ -12,7 +12,9 @@ from .api import (  # noqa: F401
     mc_brem_spectrum,
     mc_characteristic_spectrum,
     mc_cxr_spectrum,
+    retry_step_budget,
     simulate_trajectories,
+    TransportStepLimitError,
 )
 from ._lib import PyriteB200Error, load  # noqa: F401
 from .summary import tally_tables  # noqa: F401
@@ -26,6 +28,8 @@ __all__ = [
     "mc_brem_spectrum",
     "mc_characteristic_spectrum",
     "mc_cxr_spectrum",
+    "retry_step_budget",
     "simulate_trajectories",
+    "TransportStepLimitError",
     "tally_tables",
 ]

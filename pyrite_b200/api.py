@@ -283,6 +283,34 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     return out
 
 
+TRANSPORT_MAX_STEPS = 400_000  # per-history step ceiling (runner/step_budget.py:8-10)
+
+
+class TransportStepLimitError(L.PyriteB200Error):
+    """Some histories reached the step budget at the ceiling."""
+
+
+def retry_step_budget(simulate, *args, initial_max_steps=TRANSPORT_MAX_STEPS, ceiling=TRANSPORT_MAX_STEPS,
+                      **kwargs):
+    """Run ``simulate`` (``simulate_trajectories`` or a function with its
+    result keys) from ``initial_max_steps``, doubling the budget while any
+    history ends step-limited, up to ``ceiling``, where the step limit raises
+    ``TransportStepLimitError`` (runner/step_budget.py:33-53). Trajectories
+    depend on the seed alone, so a rerun at a doubled budget is exactly the
+    run that budget gives from the start."""
+    if not 1 <= int(initial_max_steps) <= int(ceiling):
+        raise ValueError(f"initial_max_steps must be in [1, {ceiling}]")
+    max_steps = int(initial_max_steps)
+    while True:
+        out = simulate(*args, max_steps=max_steps, **kwargs)
+        if int(out.get("n_step_limited", 0)) == 0:
+            return out
+        if max_steps >= ceiling:
+            raise TransportStepLimitError(
+                f"{out['n_step_limited']} histories reached the step budget of {max_steps}")
+        max_steps = min(2 * max_steps, int(ceiling))
+
+
 # ---------------------------------------------------------------------------
 # Emission scoring
 # ---------------------------------------------------------------------------
