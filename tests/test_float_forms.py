@@ -1,0 +1,104 @@
+"""The float path's rewrites of the reference's expressions, emulated in
+float32 NumPy against the double-precision forms (CPU; the kernels' own
+results are checked against the reference on the GPU).
+
+- Bethe-Heitler + Elwert (brem.py:396-479): the float kernel takes
+  1/p_f = m c^2 / sqrt(q), 1/beta_f = (1 + T_f / m c^2) m c^2 / sqrt(q) and
+  ln((p_i + p_f)/(p_i - p_f)) = ln((p_i + p_f)^2 / (p_i^2 - p_f^2)) with
+  p_i^2 - p_f^2 = k (T + T_f + 2 m c^2) / (m c^2)^2, free of cancellation;
+- the segment-mean escape (segment_escape.py:276-289) as the difference
+  2^(-A f) - 2^(-(A+B) f) over B (D > 0.01) or the series
+  f (m0 + f (m1 + f m2)) 2^(-A f) (D <= 0.01), with D = B f ln 2.
+"""
+
+import numpy as np
+
+import oracle
+
+MC2 = 510.99895
+ALPHA = 1.0 / 137.035999
+RE_CM = 2.8179403262e-13
+
+
+def bh_double(T, k, Z):
+    """brem.py:431-479 in float64, the reference's expression order."""
+    T_f = T - k
+    p_i = np.sqrt(T * (T + 2 * MC2)) / MC2
+    p_f = np.sqrt(T_f * (T_f + 2 * MC2)) / MC2
+    b_i = p_i / (1 + T / MC2)
+    b_f = p_f / (1 + T_f / MC2)
+    born = np.log((p_i + p_f) / np.maximum(p_i - p_f, 1e-30))
+    elw = b_i / b_f * (1 - np.exp(-2 * np.pi * Z * ALPHA / b_i)) / (1 - np.exp(-2 * np.pi * Z * ALPHA / b_f))
+    return 16 / 3 * ALPHA * RE_CM ** 2 * Z * Z / (k * 1e3) / (p_i * p_i) * born * elw
+
+
+def bh_float_form(T, k, Z):
+    f = np.float32
+    T, k, Z = f(T), f(k), f(Z)
+    mc2, inv = f(MC2), f(1.0 / MC2)
+    T_f = T - k
+    q = T_f * (T_f + f(2) * mc2)
+    rs = f(1) / np.sqrt(q)
+    p_f = q * rs * inv
+    p_i = np.sqrt(T * (T + f(2) * mc2)) * inv
+    b_i = p_i / (f(1) + T * inv)
+    g_i = b_i / (p_i * p_i)
+    sp = p_i + p_f
+    dpp = f(k / (MC2 * MC2)) * (f(2) * T + f(2 * MC2 - float(k)))
+    lg = np.log2(sp * sp / dpp)
+    inv_b_f = (T_f * inv + f(1)) * (rs * mc2)
+    za = f(2 * np.pi * ALPHA)
+    den_i = f(1) - np.exp(-za * Z / b_i)
+    den_f = f(1) - np.exp2(-f(2 * np.pi * ALPHA * 1.4426950408889634) * Z * inv_b_f)
+    c0k = f(16 / 3 * ALPHA * RE_CM ** 2 * np.log(2) / (float(k) * 1e3))
+    return float(c0k * g_i * lg * inv_b_f * Z * Z * den_i / den_f)
+
+
+def test_cross_section_rewrite():
+    """Within 2e-5 up to k = 0.99 T; at the tip (k -> T of a 50-100 MeV
+    electron) T_f = T - k itself loses digits in float (its spacing near
+    1e5 keV is 0.008 keV), so the bound there is 2e-4."""
+    worst, worst_tip = 0.0, 0.0
+    for T in (20.0, 300.0, 5000.0, 50000.0, 100000.0):
+        for frac in (1e-4, 0.01, 0.3, 0.9, 0.99, 0.999):
+            k = T * frac
+            for Z in (6.0, 14.0, 74.0):
+                ref = bh_double(T, k, Z)
+                err = abs(bh_float_form(T, k, Z) - ref) / ref
+                if frac <= 0.99:
+                    worst = max(worst, err)
+                else:
+                    worst_tip = max(worst_tip, err)
+    assert worst < 2e-5, worst
+    assert worst_tip < 2e-4, worst_tip
+
+
+def escape_float(A, B, f):
+    f32 = np.float32
+    A, B, f = f32(A), f32(B), f32(f)
+    D = B * f * f32(np.log(2))
+    if D > f32(0.01):
+        w = f32(1) / B
+        return float((w * np.exp2(-A * f) - w * np.exp2(-(A + B) * f)) / (f * f32(np.log(2))))
+    m0 = f32(np.log(2))
+    Bl = B * f32(np.log(2))
+    m1 = f32(-0.5) * m0 * Bl
+    m2 = m0 * Bl * Bl / f32(6)
+    t = f * (m0 + f * (m1 + f * m2))
+    return float(t * np.exp2(-A * f) / (f * f32(np.log(2))))
+
+
+def test_escape_forms():
+    """Both forms, divided by f ln 2 as the kernel does per chunk, against
+    the reference's mean transmission of the base-e depths A f ln 2 and
+    (A + B) f ln 2 (A, B are the base-2 depths the kernel carries)."""
+    worst = 0.0
+    for A in (0.0, 0.3, 4.0, 30.0):
+        for B in (0.0, 1e-6, 1e-3, 0.02, 0.5, 8.0):
+            for f in (1.0, 1.06, 3.0):
+                ln2 = np.log(2.0)
+                ref = oracle.mean_transmission(A * f * ln2, (A + B) * f * ln2)
+                got = escape_float(A, B, f)
+                scale = max(ref, 1e-30)
+                worst = max(worst, abs(got - ref) / scale)
+    assert worst < 1e-4, worst
