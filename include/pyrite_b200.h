@@ -30,6 +30,8 @@
  *                        src/pyrite/montecarlo/spectrum/_characteristic_chunk_kernel.py:120
  *                        and _accumulate_line_yields, characteristic.py:837;
  *   pb_char_spectrum  -- spec += line_yield * profile, characteristic.py:1219.
+ *   pb_coherent_reduce -- the coherent (field-sum) CXR reduction of per-row
+ *                        line records, cxr/_batched_finalize.py:209-243.
  *   pb_mlp_*          -- BF16 MLP surrogate of the reflection sum (no
  *                        counterpart in the reference; 6 -> 4x256 SiLU -> 512).
  */
@@ -42,7 +44,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 2
+#define PB_ABI_VERSION 3
 
 enum pb_status {
     PB_OK = 0,
@@ -479,6 +481,49 @@ int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a
  * on the GPU (different streams, threads or processes sharing a context)
  * race on it and must be serialised by the caller. */
 int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream);
+
+/* Coherent (field-sum) CXR reduction of per-row line records: for every row
+ * r (one reflection x mosaic orientation) and output energy E_k,
+ *   F_pol(E) = sum_j c_pol,j F_j(E) exp(i phi_j(E)),  pol = sigma, pi,
+ *   phi_j(E) = phase_slope_j E - g_phase_j - L_esc,j delta_omega(E),
+ *   F_j(E)   = formation factor of v = a_vac_j (E - E_vac_j) - half_dL_j
+ *              delta_omega(E) with (apb_j, bma_j, q_j),
+ *   spec[k] += scale * sum_r row_weight[r] (|F_sigma|^2 + |F_pi|^2).
+ * Rows add incoherently; lines inside a row keep their phase. Replaces the
+ * per-row reduction of the reference's coherent route,
+ * src/pyrite/montecarlo/spectrum/cxr/_batched_finalize.py:209-243 and its
+ * CUDA form run_coherent_reduction_kernel
+ * (src/pyrite/montecarlo/spectrum/coherent_jit_kernel.py), formation factor
+ * cxr/_formation.py:84-130; the record fields are the ``per_cxr`` tuple of
+ * cxr/_batched.py:646-660, laid out row after row (row r holds lines
+ * row_off[r] .. row_off[r+1]). Phases are evaluated in FP64 and reduced to
+ * [-pi, pi] before FP32 sin/cos; per-chunk fields are FP32 and the row sums
+ * FP64, in a fixed order (the result does not depend on the launch). */
+typedef struct pb_coherent_args {
+    int32_t n_row;
+    int32_t n_E;
+    int64_t n_line;                 /* == row_off[n_row] */
+    const int64_t *row_off;         /* [n_row + 1], nondecreasing, row_off[0] = 0 */
+    const double *row_weight;       /* [n_row] */
+    const double *E;                /* [n_E] photon energies, eV */
+    const double *delta_omega;      /* [n_E] delta(E) omega(E), 1/Angstrom */
+    const double *E_vac, *a_vac, *phase_slope, *g_phase;   /* [n_line] each */
+    const double *cs_re, *cs_im, *cp_re, *cp_im;
+    const double *L_esc, *half_dL, *apb, *bma, *q;
+    double scale;                   /* e.g. 1 / electrons */
+    double sinc_cutoff;             /* > 0: a line adds nothing where |v| > sinc_cutoff
+                                       (coherent_jit_kernel.py:752-760); 0 = no window */
+    double *spec;                   /* [n_E], accumulated into */
+    void *work;                     /* pb_coherent_work_size bytes, 256-byte aligned */
+    uint64_t work_bytes;
+    unsigned int *status;           /* optional device word: PB_DEV_BAD_INPUT when row_off
+                                       is not a partition of [0, n_line) (rows are then
+                                       clamped into it) */
+} pb_coherent_args;
+
+/* Workspace bytes pb_coherent_reduce needs for these sizes. */
+int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes);
+int pb_coherent_reduce(const pb_coherent_args *args, void *stream);
 
 #ifdef __cplusplus
 }

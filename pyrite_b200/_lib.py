@@ -147,6 +147,16 @@ class PbMlpInferArgs(C.Structure):
     ]
 
 
+class PbCoherentArgs(C.Structure):
+    _fields_ = [
+        ("n_row", _i32), ("n_E", _i32), ("n_line", _i64), ("row_off", _vp), ("row_weight", _vp),
+        ("E", _vp), ("delta_omega", _vp), ("E_vac", _vp), ("a_vac", _vp), ("phase_slope", _vp),
+        ("g_phase", _vp), ("cs_re", _vp), ("cs_im", _vp), ("cp_re", _vp), ("cp_im", _vp), ("L_esc", _vp),
+        ("half_dL", _vp), ("apb", _vp), ("bma", _vp), ("q", _vp), ("scale", _f64), ("sinc_cutoff", _f64), ("spec", _vp),
+        ("work", _vp), ("work_bytes", _u64), ("status", _vp),
+    ]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -170,6 +180,8 @@ EXPORTS = (
     "pb_mlp_pack_umma",
     "pb_mlp_features",
     "pb_cxr_bin_lines",
+    "pb_coherent_work_size",
+    "pb_coherent_reduce",
 )
 
 _lib = None
@@ -179,7 +191,7 @@ class PyriteB200Error(RuntimeError):
     """A pyrite_b200 C-ABI call returned a non-zero status."""
 
 
-ABI_VERSION = 2  # PB_ABI_VERSION of include/pyrite_b200.h
+ABI_VERSION = 3  # PB_ABI_VERSION of include/pyrite_b200.h
 
 
 def load(path: Path | None = None):
@@ -219,6 +231,8 @@ def load(path: Path | None = None):
     lib.pb_mlp_head.argtypes = [_i32, _i32, _vp, _vp, _vp, _vp, _f64, _vp, _vp]
     lib.pb_mlp_pack_umma.argtypes = [_i32, _i32, _vp, _vp, _vp]
     lib.pb_cxr_bin_lines.argtypes = [_i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _f64, _f64, _i32, _vp, _vp]
+    lib.pb_coherent_work_size.argtypes = [_i32, _i64, _i32, C.POINTER(_u64)]
+    lib.pb_coherent_reduce.argtypes = [C.POINTER(PbCoherentArgs), _vp]
     if path is None:
         _lib = lib
     return lib

@@ -1,0 +1,145 @@
+"""Coherent (field-sum) CXR: the per-row field reduction on the device.
+
+The reference's coherent route (``mc_cxr_spectrum(..., coherent=True)``,
+``pyrite/montecarlo/spectrum/cxr/_batched.py:1029-1240``) turns every
+(segment, reflection row) pair into a line record -- the ``per_cxr`` tuple of
+``cxr/_batched.py:646-660`` -- and then reduces each row separately: the
+complex field of both polarisations summed over the row's lines at every
+output energy, squared, weighted by the row's mosaic weight and summed over
+rows (``cxr/_batched_finalize.py:209-243``; its CUDA form
+``run_coherent_reduction_kernel``, ``coherent_jit_kernel.py:716``). This module
+hands that reduction to ``pb_coherent_reduce``: every row in one call, FP64
+phases, a deterministic FP64 row sum.
+
+``coherent_reduce`` takes the records of all rows at once;
+``run_coherent_reduction_kernel`` keeps the reference's one-row signature
+(vacuum sinc, in-medium phase, formation factor and sinc window as optional
+groups, with the same pairing rules and errors).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .api import _device, _Holder, _stream_ptr
+
+# Line record fields, in the order of cxr/_batched.py:646-660 (the emitting
+# electron id, which only the decoherence blend reads, is not needed).
+RECORD_FIELDS = ("E_vac", "a_vac", "phase_slope", "g_phase", "cs_re", "cs_im", "cp_re", "cp_im",
+                 "L_esc", "half_dL", "apb", "bma", "q")
+
+
+def _work(h: _Holder, n_row: int, n_line: int, n_E: int):
+    lib = L.load()
+    nbytes = C.c_uint64()
+    L.check(lib.pb_coherent_work_size(n_row, n_line, n_E, C.byref(nbytes)), "pb_coherent_work_size")
+    # torch's caching allocator hands out 512-byte aligned blocks
+    return h.empty((max(int(nbytes.value), 1),), torch.uint8), int(nbytes.value)
+
+
+def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, scale=1.0, sinc_cutoff=None,
+                    spec=None, device=None, stream=None, status=None) -> torch.Tensor:
+    """``spec += scale * sum_rows w_r (|F_sigma|^2 + |F_pi|^2)`` on the device.
+
+    ``records`` maps ``RECORD_FIELDS`` to per-line arrays (numpy or tensors),
+    laid out row after row; ``row_count[r]`` lines belong to row ``r``, whose
+    intensity is weighted by ``row_weight[r]``. ``delta_omega`` is
+    ``(1 - Re n(E)) omega(E)`` on ``E_grid_eV`` [1/Angstrom]. Returns the FP64
+    device spectrum (``spec`` when given, accumulated into).
+    """
+    dev = _device(device)
+    h = _Holder(dev)
+    row_count = np.asarray(row_count, dtype=np.int64)
+    if row_count.ndim != 1 or row_count.size < 1 or np.any(row_count < 0):
+        raise ValueError("row_count must be a nonempty 1-D array of nonnegative counts")
+    n_row = int(row_count.size)
+    n_line = int(row_count.sum())
+    E = h.f64(E_grid_eV)
+    n_E = int(E.numel())
+    dom = h.f64(delta_omega)
+    if int(dom.numel()) != n_E:
+        raise ValueError("delta_omega must have one entry per energy")
+    w = h.f64(row_weight)
+    if int(w.numel()) != n_row:
+        raise ValueError("row_weight must have one entry per row")
+    fields = {}
+    for name in RECORD_FIELDS:
+        t = h.f64(records[name]).reshape(-1)
+        if int(t.numel()) != n_line:
+            raise ValueError(f"record field {name!r} has {int(t.numel())} lines, the rows hold {n_line}")
+        fields[name] = t
+    row_off = h.typed(np.concatenate([[0], np.cumsum(row_count)]).astype(np.int64), torch.int64)
+    if spec is None:
+        spec = h.zeros((n_E,), torch.float64)
+    elif spec.dtype != torch.float64 or spec.device != dev or int(spec.numel()) != n_E or not spec.is_contiguous():
+        raise ValueError("spec must be a contiguous float64 tensor on the device with one entry per energy")
+    work, nbytes = _work(h, n_row, n_line, n_E)
+    a = L.PbCoherentArgs()
+    a.n_row, a.n_E, a.n_line = n_row, n_E, n_line
+    a.row_off, a.row_weight, a.E, a.delta_omega = (t.data_ptr() for t in (row_off, w, E, dom))
+    for name in RECORD_FIELDS:
+        setattr(a, name, fields[name].data_ptr())
+    a.scale = float(scale)
+    a.sinc_cutoff = 0.0 if sinc_cutoff is None else float(sinc_cutoff)
+    a.spec = spec.data_ptr()
+    a.work, a.work_bytes = work.data_ptr(), nbytes
+    a.status = None if status is None else status.data_ptr()
+    L.check(L.load().pb_coherent_reduce(C.byref(a), _stream_ptr(stream)), "pb_coherent_reduce")
+    if stream is not None:
+        # freed on torch's current stream: keep the blocks until the call has run
+        for t in h.keep:
+            t.record_stream(stream)
+    return spec
+
+
+def coherent_spectrum(records, row_count, row_weight, E_grid_eV, delta_omega, Ne, *, sinc_cutoff=None,
+                      device=None) -> np.ndarray:
+    """The coherent route's spectrum per electron [photons/eV/sr/electron],
+    as ``_finalize_spectrum`` returns it (``cxr/_spectrum.py:285-318``)."""
+    if Ne < 1:
+        raise ValueError("Ne must be >= 1")
+    spec = coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, scale=1.0 / Ne,
+                           sinc_cutoff=sinc_cutoff, device=device)
+    return spec.cpu().numpy()
+
+
+def run_coherent_reduction_kernel(E_r, aw, phase_slope, g_phase, c_s_re, c_s_im, c_p_re, c_p_im, E_grid, *, out,
+                                  mosaic_weight=1.0, L_esc=None, delta_omega=None, half_dL=None, apb=None,
+                                  bma=None, q=None, sinc_cutoff=None, config=None):
+    """One row's coherent intensity accumulated into ``out`` (the reference's
+    signature, ``coherent_jit_kernel.py:716-766``).
+
+    Without the in-medium pair the phase is the vacuum one; without the
+    formation group each line is the real sinc ``sin(v)/v`` of
+    ``v = aw (E - E_r)``, i.e. the formation factor with ``apb = 2``,
+    ``bma = q = half_dL = 0``. ``config`` is accepted for signature
+    compatibility; the launch shape is the library's. ``out`` is a float64
+    device tensor.
+    """
+    del config
+    if (L_esc is None) != (delta_omega is None):
+        raise ValueError("L_esc and delta_omega must be given together")
+    formation = (half_dL, apb, bma, q)
+    use_formation = half_dL is not None
+    if any((f is None) != (not use_formation) for f in formation):
+        raise ValueError("half_dL, apb, bma and q must be given together")
+    if use_formation and L_esc is None:
+        raise ValueError("the formation factor needs L_esc and delta_omega")
+    n = int(np.asarray(E_r).size) if not torch.is_tensor(E_r) else int(E_r.numel())
+    n_E = int(np.asarray(E_grid).size) if not torch.is_tensor(E_grid) else int(E_grid.numel())
+    if n_E == 0 or n == 0:
+        return out
+    zeros = np.zeros(n)
+    if L_esc is None:
+        L_esc, delta_omega = zeros, np.zeros(n_E)
+    if not use_formation:
+        half_dL, apb, bma, q = zeros, np.full(n, 2.0), zeros, zeros
+    records = dict(E_vac=E_r, a_vac=aw, phase_slope=phase_slope, g_phase=g_phase, cs_re=c_s_re, cs_im=c_s_im,
+                   cp_re=c_p_re, cp_im=c_p_im, L_esc=L_esc, half_dL=half_dL, apb=apb, bma=bma, q=q)
+    coherent_reduce(records, [n], [float(mosaic_weight)], E_grid, delta_omega, sinc_cutoff=sinc_cutoff,
+                    spec=out, device=out.device)
+    return out

@@ -322,4 +322,41 @@ int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a
     return PB_OK;
 }
 
+// Sizes the coherent reduction accepts: one energy-tile grid dimension, an
+// int item count, the items kernel's 1024-thread row split.
+static int coherent_sizes_ok(int32_t n_row, int64_t n_line, int32_t n_E) {
+    return n_row >= 1 && n_row <= (1 << 24) && n_line >= 0 && n_line <= (int64_t(1) << 40) && n_E >= 1 &&
+           n_E <= (1 << 24);
+}
+
+int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes) {
+    if (!bytes) return fail(PB_ERR_INVALID, "pb_coherent_work_size: bytes is NULL");
+    if (!coherent_sizes_ok(n_row, n_line, n_E))
+        return fail(PB_ERR_INVALID, "pb_coherent_work_size: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    *bytes = pb::coherent_work_bytes(n_row, n_line, n_E);
+    return PB_OK;
+}
+
+int pb_coherent_reduce(const pb_coherent_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_coherent_reduce: args is NULL");
+    if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_INVALID, "pb_coherent_reduce: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    if (!a->row_off || !a->row_weight || !a->E || !a->delta_omega || !a->spec || !a->work)
+        return fail(PB_ERR_INVALID, "pb_coherent_reduce: row_off, row_weight, E, delta_omega, spec, work must be set");
+    if (a->n_line > 0 && (!a->E_vac || !a->a_vac || !a->phase_slope || !a->g_phase || !a->cs_re || !a->cs_im ||
+                          !a->cp_re || !a->cp_im || !a->L_esc || !a->half_dL || !a->apb || !a->bma || !a->q))
+        return fail(PB_ERR_INVALID, "pb_coherent_reduce: every line record array must be set");
+    if (reinterpret_cast<uintptr_t>(a->work) % 256 != 0)
+        return fail(PB_ERR_INVALID, "pb_coherent_reduce: work must be 256-byte aligned");
+    if (!(a->sinc_cutoff >= 0.0)) return fail(PB_ERR_INVALID, "pb_coherent_reduce: sinc_cutoff must be >= 0");
+    const uint64_t need = pb::coherent_work_bytes(a->n_row, a->n_line, a->n_E);
+    if (a->work_bytes < need)
+        return fail(PB_ERR_CAPACITY, "pb_coherent_reduce: work holds %llu bytes, needs %llu",
+                    (unsigned long long)a->work_bytes, (unsigned long long)need);
+    if (a->n_line == 0) return PB_OK;  // no line: the spectrum is unchanged
+    cudaError_t e = pb::launch_coherent(*a, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_reduce: launch");
+    return PB_OK;
+}
+
 }  // extern "C"

@@ -43,6 +43,9 @@ cudaError_t launch_mlp_group_mse_grad(int groups, int S, int cols, const float *
 cudaError_t launch_segments_sample(const pb_segments &src, int64_t stride, const pb_segments &dst,
                                    unsigned int *status, cudaStream_t s, int sms);
 
+uint64_t coherent_work_bytes(int n_row, int64_t n_line, int n_E);
+cudaError_t launch_coherent(const pb_coherent_args &a, cudaStream_t s);
+
 // Record the message pb_last_error() returns on this thread.
 void set_last_error(const char *msg);
 

@@ -766,6 +766,86 @@ def gen_layered():
     _save("layered_stack10", **out)
 
 
+COHERENT_FIELDS = ("E_vac", "a_vac", "phase_slope", "g_phase", "cs_re", "cs_im", "cp_re", "cp_im",
+                   "L_esc", "elec_id", "half_dL", "apb", "bma", "q")
+# The reference's coherent route on the first electrons of two CXR cases
+# (fixture size), with segment start ages, so the emission-time phase is live.
+COHERENT_CASES = {"hopg20": 8, "si50": 6}
+
+
+def gen_coherent():
+    """Coherent (field-sum) CXR on the batched route (cxr/_batched.py:1029-1240).
+
+    Captures the per-row line records the block loop hands to
+    ``_batched_coherent_finalize`` (cxr/_batched_finalize.py:22; record
+    layout cxr/_batched.py:646-660), concatenated per row in the finalize's
+    order, and the reference's coherent spectrum from those records. Inter-
+    electron decoherence is off (no initial beam offsets), so the reduction is
+    the flat per-row field sum of _batched_finalize.py:209-243.
+    """
+    from pyrite.materials.crystal import CRYSTALS, reciprocal_g_vector
+    from pyrite.montecarlo.spectrum.cxr import _batched, _setup
+    from pyrite.montecarlo.spectrum.cxr._spectrum import mc_cxr_spectrum
+
+    for name, n_elec in COHERENT_CASES.items():
+        case = CXR_CASES[name]
+        tr = np.load(OUT / f"transport_{case['transport']}.npz")
+        sel = tr["elec_id"] < n_elec
+        seg = {k: tr[k][sel] for k in ("r_mid", "v_hat", "L_ang", "E_keV", "E_repr_keV", "elec_id", "t_ang")}
+        seg.update(Ne=n_elec, thickness_ang=float(tr["z_bot"][-1]))
+        info = CRYSTALS[case["crystal"]]
+        hkl = _diamond_hkls(4) if case["hkl"] == "diamond<=4" else case["hkl"]
+        g_mags = np.array([reciprocal_g_vector(h, info["lattice"])[1] for h in hkl])
+        E_grid = case["E_grid"]
+        E_tab = synthetic_E_tab(E_grid)
+        tables = synthetic_couplings(g_mags, E_tab)
+        captured = {}
+        orig_fin = _batched._batched_coherent_finalize
+
+        def capture(st, bt, coh_blocks, coh_counts, *a, _orig=orig_fin, **k):
+            captured.update(st=st, bt=bt, blocks=[[np.array(f) for f in b] for b in coh_blocks],
+                            counts=[np.array(c) for c in coh_counts])
+            return _orig(st, bt, coh_blocks, coh_counts, *a, **k)
+
+        patches = [
+            (_setup, "_line_tabulation_grid", lambda *a, **k: E_tab),
+            (_setup, "_elemental_log_mu_table", lambda c, E: synthetic_log_mu(c, E)),
+            (_setup, "refractive_index", lambda cr, E, uh=True: (1.0 - synthetic_delta(E)) + 0j),
+            (_batched, "_reflection_tables", lambda *a, **k: tuple(np.array(t) for t in tables)),
+            (_batched, "_batched_coherent_finalize", capture),
+        ]
+        saved = [(m, n, getattr(m, n)) for m, n, _ in patches]
+        for m, n, f in patches:
+            setattr(m, n, f)
+        try:
+            spec = np.asarray(mc_cxr_spectrum(
+                seg, E_grid, crystal=case["crystal"], hkl_list=[tuple(h) for h in hkl],
+                B_ang2=float(info.get("B_ang2", 0.0) or 0.0), absorber_element=case["absorber"],
+                n_hat=tr["n_hat"], surface_hkl=case["surface_hkl"],
+                mosaic_fwhm_rad=None if case["mosaic_fwhm_deg"] is None else np.deg2rad(case["mosaic_fwhm_deg"]),
+                mosaic_nodes=case["mosaic_nodes"], node_support_cutoff=None, coherent=True))
+        finally:
+            for m, n, f in saved:
+                setattr(m, n, f)
+        st, bt = captured["st"], captured["bt"]
+        if st.decoherence_active:
+            raise RuntimeError("coherent fixture expects the flat reduction (no beam offsets)")
+        counts = np.stack(captured["counts"])                      # (n_block, N_g)
+        starts = np.concatenate([np.zeros((counts.shape[0], 1), counts.dtype), np.cumsum(counts, axis=1)], axis=1)
+        rows = {f: [] for f in COHERENT_FIELDS}
+        for i_row in range(int(bt.N_g)):
+            for b, flat in enumerate(captured["blocks"]):
+                for f, arr in zip(COHERENT_FIELDS, flat, strict=True):
+                    rows[f].append(arr[int(starts[b, i_row]):int(starts[b, i_row + 1])])
+        _save(
+            f"coherent_{name}",
+            transport=case["transport"], n_elec=n_elec, Ne=n_elec, E_grid=np.asarray(st.E_grid),
+            delta_omega=np.asarray(st.delta_omega_grid), row_weight=np.asarray(bt.wm_rows, dtype=float).reshape(-1),
+            row_count=counts.sum(axis=0).astype(np.int64), spec=spec,
+            **{f: np.concatenate(rows[f]) for f in COHERENT_FIELDS},
+        )
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
@@ -776,6 +856,7 @@ GENERATORS = {
     "cxr_leaves": gen_cxr_leaves,
     "char": gen_char,
     "layered": gen_layered,
+    "coherent": gen_coherent,
 }
 
 

@@ -27,13 +27,14 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(L.EXPORTS)
     for name in names:
         assert hasattr(lib, name), name
-    assert lib.pb_abi_version() == L.ABI_VERSION == 2
+    assert lib.pb_abi_version() == L.ABI_VERSION == 3
 
 
 STRUCTS = {
     "pb_layers": L.PbLayers, "pb_lut": L.PbLut, "pb_beam": L.PbBeam, "pb_rows": L.PbRows,
     "pb_segments": L.PbSegments, "pb_tallies": L.PbTallies, "pb_transport_args": L.PbTransportArgs,
     "pb_cxr_tables": L.PbCxrTables, "pb_cxr_args": L.PbCxrArgs, "pb_brem_args": L.PbBremArgs,
+    "pb_coherent_args": L.PbCoherentArgs,
 }
 
 

@@ -1,0 +1,332 @@
+"""Coherent (field-sum) CXR reduction: oracle pinned to the reference, the
+kernel's precision plan emulated on the CPU, the C ABI's checks, and (GPU)
+``pb_coherent_reduce`` against the reference's spectra and the oracle.
+
+Golden vectors: ``tests/golden/coherent_{hopg20,si50}.npz``, made by
+``make_golden.py --only coherent`` from the reference's own coherent route
+(``cxr/_batched.py:1029-1240`` -> ``_batched_finalize.py:209-243``).
+
+Tolerance of the device path against FP64: the spectrum within 2e-5 of its
+peak everywhere and within 1e-4 relative wherever it exceeds 1e-3 of the
+peak. Phases reach 1e8 rad; they are formed and reduced in FP64, the
+trigonometry and the per-chunk field sums are FP32.
+"""
+
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import coherent as oc
+from pyrite_b200 import _lib as L
+
+CASES = ("hopg20", "si50")
+PEAK_TOL = 2e-5
+REL_TOL = 1e-4
+
+
+def _golden(name):
+    return oc.load_golden(GOLDEN / f"coherent_{name}.npz")
+
+
+def _assert_close(got, ref, peak_tol=PEAK_TOL, rel_tol=REL_TOL):
+    peak = float(np.max(np.abs(ref)))
+    assert peak > 0
+    err = np.abs(got - ref)
+    assert err.max() <= peak_tol * peak, (err.max() / peak)
+    big = np.abs(ref) > 1e-3 * peak
+    assert np.all(err[big] <= rel_tol * np.abs(ref[big])), np.max(err[big] / np.abs(ref[big]))
+
+
+# ---------------------------------------------------------------------------
+# oracle against the reference
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_coherent_spectrum(name):
+    rec, cnt, w, E, dom, Ne, spec = _golden(name)
+    got = oc.coherent_spectrum(rec, cnt, w, E, dom, Ne)
+    assert np.max(np.abs(got - spec)) <= 1e-12 * np.max(spec)
+
+
+def test_golden_records_exercise_the_hard_cases():
+    """Phases near 1e8 rad, formation arguments far from resonance, heavy
+    absorption (apb underflowing FP32) and several rows with weights."""
+    rec, cnt, w, E, dom, Ne, _ = _golden("si50")
+    phi_max = np.max(np.abs(rec["phase_slope"])) * E.max() + np.max(np.abs(rec["g_phase"]))
+    assert phi_max > 1e7
+    assert np.min(rec["apb"]) < 1e-38
+    rec_h, cnt_h, w_h, *_ = _golden("hopg20")
+    assert len(np.unique(w_h)) > 1 and np.count_nonzero(cnt_h) > 50
+
+
+def test_formation_factor_limits():
+    v = np.linspace(-40.0, 40.0, 4001)
+    # no absorption: the real sinc
+    F = oc.formation_factor(v, np.full_like(v, 2.0), np.zeros_like(v), np.zeros_like(v))
+    np.testing.assert_allclose(F.real, np.sinc(v / np.pi), atol=1e-12)
+    assert np.max(np.abs(F.imag)) == 0.0
+    # series branch and closed form agree at the switch
+    for q in (1e-4, 3e-4):
+        vv = np.array([math.sqrt(max(1e-6 - q * q, 0.0)) * (1 - 1e-9), math.sqrt(1e-6 - q * q) * (1 + 1e-9)])
+        a, b = math.exp(-0.1), math.exp(-0.1 - 2 * q)
+        Fs = oc.formation_factor(vv, np.full(2, a + b), np.full(2, b - a), np.full(2, q))
+        assert abs(Fs[0] - Fs[1]) < 1e-9
+
+
+def test_formation_parseval():
+    """int |F|^2 dv = pi <exp(-tau)> over the piece (_formation.py:37-40)."""
+    tau_s, tau_e = 0.3, 2.1
+    q = 0.25 * (tau_e - tau_s)
+    a, b = math.exp(-0.5 * tau_s), math.exp(-0.5 * tau_e)
+    v = np.linspace(-4000.0, 4000.0, 4_000_001)
+    F = oc.formation_factor(v, np.full_like(v, a + b), np.full_like(v, b - a), np.full_like(v, q))
+    integral = np.trapezoid(np.abs(F) ** 2, v)
+    mean_T = (math.exp(-tau_s) - math.exp(-tau_e)) / (tau_e - tau_s)
+    assert abs(integral - math.pi * mean_T) < 2e-3 * math.pi * mean_T
+
+
+def test_rows_add_incoherently_lines_coherently():
+    rec, cnt, w, E, dom, Ne, spec = _golden("hopg20")
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    total = np.zeros_like(spec)
+    for r in np.flatnonzero(cnt)[:12]:
+        sub = {k: v[off[r]:off[r + 1]] for k, v in rec.items()}
+        total += oc.coherent_spectrum(sub, [cnt[r]], [w[r]], E, dom, Ne)
+    rows = np.flatnonzero(cnt)[:12]
+    sel = np.concatenate([np.arange(off[r], off[r + 1]) for r in rows])
+    both = oc.coherent_spectrum({k: v[sel] for k, v in rec.items()}, cnt[rows], w[rows], E, dom, Ne)
+    np.testing.assert_allclose(both, total, rtol=1e-12, atol=1e-14 * total.max())
+    # one row holding two rows' lines interferes: not the incoherent sum
+    r0, r1 = rows[-2], rows[-1]
+    pair = np.concatenate([np.arange(off[r0], off[r0 + 1]), np.arange(off[r1], off[r1 + 1])])
+    one = oc.coherent_spectrum({k: v[pair] for k, v in rec.items()}, [pair.size], [1.0], E, dom, Ne)
+    two = oc.coherent_spectrum({k: v[pair] for k, v in rec.items()}, [cnt[r0], cnt[r1]], [1.0, 1.0], E, dom, Ne)
+    assert np.max(np.abs(one - two)) > 1e-3 * np.max(two)
+
+
+# ---------------------------------------------------------------------------
+# the kernel's arithmetic, emulated in float32 numpy
+# ---------------------------------------------------------------------------
+def _chunk_lines(n_line, n_E):
+    """pb_coherent.cu chunk_lines: items for ~8 CTAs per SM over 512-energy tiles."""
+    tiles = -(-n_E // 512)
+    items = max(1, (148 * 8) // tiles)
+    k = max(-(-n_line // items), 256)
+    return -(-k // 128) * 128
+
+
+def kernel_emulation(rec, cnt, w, E, dom, Ne):
+    f32 = np.float32
+    E = np.asarray(E, dtype=np.float64)
+    spec = np.zeros(E.size)
+    K = _chunk_lines(int(np.sum(cnt)), E.size)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    inv2pi = 0.15915494309189535
+    for r in range(len(cnt)):
+        F = np.zeros((4, E.size))
+        for j0 in range(off[r], off[r + 1], K):
+            acc = np.zeros((4, E.size), dtype=f32)
+            for j in range(j0, min(j0 + K, off[r + 1])):
+                v = rec["a_vac"][j] * (E - rec["E_vac"][j]) - rec["half_dL"][j] * dom
+                vf = v.astype(f32)
+                q, apb, bma = f32(rec["q"][j]), f32(rec["apb"][j]), f32(rec["bma"][j])
+                w2 = q * q + vf * vf
+                t = v * inv2pi
+                x = ((t - np.rint(t)) * 2.0).astype(f32)
+                sv = np.sin(np.pi * x.astype(np.float64)).astype(f32)
+                cv = np.cos(np.pi * x.astype(np.float64)).astype(f32)
+                with np.errstate(divide="ignore", over="ignore"):
+                    inv = (f32(1.0) / (f32(2.0) * w2)).astype(f32)
+                fr = (vf * apb * sv - q * bma * cv) * inv
+                fi = -(vf * bma * cv + q * apb * sv) * inv
+                series = w2 < f32(1e-6)
+                half = f32(0.5) * apb
+                fr = np.where(series, half * (f32(1) - q * q * f32(1 / 3) - vf * vf * f32(1 / 6)), fr)
+                fi = np.where(series, -half * q * vf * f32(1 / 3), fi)
+                phi = rec["phase_slope"][j] * E - rec["g_phase"][j] - rec["L_esc"][j] * dom
+                tp = phi * inv2pi
+                rp = ((tp - np.rint(tp)) * 6.283185307179586).astype(f32)
+                sp, cp = np.sin(rp).astype(f32), np.cos(rp).astype(f32)
+                pr, pi = fr * cp - fi * sp, fr * sp + fi * cp
+                csr, csi, cpr, cpi = (f32(rec[k][j]) for k in ("cs_re", "cs_im", "cp_re", "cp_im"))
+                acc[0] += csr * pr - csi * pi
+                acc[1] += csr * pi + csi * pr
+                acc[2] += cpr * pr - cpi * pi
+                acc[3] += cpr * pi + cpi * pr
+            F += acc.astype(np.float64)
+        spec += w[r] * np.sum(F * F, axis=0)
+    return spec / Ne
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_float_plan_meets_tolerance_on_reference_records(name):
+    rec, cnt, w, E, dom, Ne, spec = _golden(name)
+    _assert_close(kernel_emulation(rec, cnt, w, E, dom, Ne), spec, PEAK_TOL / 4, REL_TOL / 4)
+
+
+def test_phase_in_float32_would_not_do():
+    """The reason the phase stays FP64: formed in FP32, the si50 spectrum is off."""
+    rec, cnt, w, E, dom, Ne, spec = _golden("si50")
+    f32 = np.float32
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    r = int(np.argmax(cnt))
+    sl = slice(off[r], off[r + 1])
+    phi64 = rec["phase_slope"][sl, None] * E[None, :] - rec["g_phase"][sl, None]
+    phi32 = (rec["phase_slope"][sl, None].astype(f32) * E[None, :].astype(f32) - rec["g_phase"][sl, None].astype(f32))
+    assert np.max(np.abs(np.angle(np.exp(1j * (phi32.astype(np.float64) - phi64))))) > 1.0
+
+
+# ---------------------------------------------------------------------------
+# C ABI (no device work)
+# ---------------------------------------------------------------------------
+def test_abi_work_size_and_argument_errors():
+    lib = L.load()
+    nb = C.c_uint64()
+    assert lib.pb_coherent_work_size(144, 6003, 781, C.byref(nb)) == 0
+    # item offsets (145 int64, 256-aligned) + (144 + 6003 // 256) items x 4 x 781 floats
+    assert nb.value == 1280 + (144 + 6003 // 256) * 4 * 781 * 4
+    assert lib.pb_coherent_work_size(0, 10, 10, C.byref(nb)) == 1
+    assert lib.pb_coherent_work_size(1, 10, 0, C.byref(nb)) == 1
+    assert lib.pb_coherent_work_size(1, -1, 10, C.byref(nb)) == 1
+    a = L.PbCoherentArgs()
+    a.n_row, a.n_E, a.n_line = 2, 16, 0
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 1
+    assert b"must be set" in lib.pb_last_error()
+    fake = 1 << 20
+    a.row_off = a.row_weight = a.E = a.delta_omega = a.spec = fake
+    a.work = fake + 8
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 1
+    assert b"aligned" in lib.pb_last_error()
+    a.work = fake
+    a.work_bytes = 16
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 4
+    a.work_bytes = 1 << 30
+    a.sinc_cutoff = -1.0
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 1
+    a.sinc_cutoff = 0.0
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 0  # no lines: nothing to launch
+    a.n_line = 5
+    assert lib.pb_coherent_reduce(C.byref(a), None) == 1
+    assert b"line record" in lib.pb_last_error()
+
+
+# ---------------------------------------------------------------------------
+# GPU: the kernel
+# ---------------------------------------------------------------------------
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_coherent_matches_reference(name):
+    from pyrite_b200.coherent import coherent_spectrum
+
+    rec, cnt, w, E, dom, Ne, spec = _golden(name)
+    got = coherent_spectrum(rec, cnt, w, E, dom, Ne)
+    _assert_close(got, spec)
+
+
+def _random_rows(rng, n_rows, n_per_row, E_lo, E_hi):
+    n = n_rows * n_per_row
+    E_vac = rng.uniform(E_lo, E_hi, n)
+    a_vac = rng.uniform(0.5, 60.0, n)
+    tau_s = rng.uniform(0.0, 6.0, n)
+    tau_e = tau_s + rng.uniform(-tau_s, 6.0, n)
+    q = 0.25 * (tau_e - tau_s)
+    a, b = np.exp(-0.5 * tau_s), np.exp(-0.5 * tau_e)
+    rec = dict(
+        E_vac=E_vac, a_vac=a_vac, phase_slope=rng.uniform(-3000.0, 3000.0, n),
+        g_phase=rng.uniform(-6e7, 6e7, n), cs_re=rng.normal(0, 1e-4, n), cs_im=rng.normal(0, 1e-5, n),
+        cp_re=rng.normal(0, 1e-4, n), cp_im=rng.normal(0, 1e-5, n), L_esc=rng.uniform(0.0, 2e5, n),
+        half_dL=rng.uniform(-1e5, 1e5, n), apb=a + b, bma=b - a, q=q,
+    )
+    return rec, np.full(n_rows, n_per_row), rng.uniform(0.1, 1.0, n_rows)
+
+
+@pytest.mark.gpu
+def test_gpu_coherent_random_rows_against_oracle():
+    """3 rows x 20k lines over 4096 energies (2.5e8 line-energy pairs), the
+    oracle on every 16th energy; deterministic across calls."""
+    import torch
+
+    from pyrite_b200.coherent import coherent_reduce
+
+    rng = np.random.default_rng(11)
+    rec, cnt, w = _random_rows(rng, 3, 20000, 2000.0, 40000.0)
+    E = np.linspace(1000.0, 41000.0, 4096)
+    dom = 2.3e-4 * (1e4 / (E + 500.0)) ** 2 * E / 1973.27
+    got = coherent_reduce(rec, cnt, w, E, dom).cpu().numpy()
+    again = coherent_reduce(rec, cnt, w, E, dom).cpu().numpy()
+    assert np.array_equal(got, again)
+    sub = np.arange(0, E.size, 16)
+    ref = oc.coherent_spectrum(rec, cnt, w, E[sub], dom[sub])
+    _assert_close(got[sub], ref)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_gpu_coherent_sinc_window_and_one_row_signature():
+    """The reference's one-row call: vacuum sinc lines (no medium, no
+    formation group) and the |v| window."""
+    import torch
+
+    from pyrite_b200.coherent import run_coherent_reduction_kernel
+
+    rng = np.random.default_rng(5)
+    n = 3000
+    E = np.linspace(5000.0, 15000.0, 1500)
+    rec = dict(E_vac=rng.uniform(6000, 14000, n), a_vac=rng.uniform(0.05, 2.0, n),
+               phase_slope=rng.uniform(-50, 50, n), g_phase=rng.uniform(-1e5, 1e5, n),
+               cs_re=rng.normal(0, 1, n), cs_im=rng.normal(0, 1, n), cp_re=rng.normal(0, 1, n),
+               cp_im=rng.normal(0, 1, n))
+    out = torch.zeros(E.size, dtype=torch.float64, device="cuda")
+    run_coherent_reduction_kernel(rec["E_vac"], rec["a_vac"], rec["phase_slope"], rec["g_phase"], rec["cs_re"],
+                                  rec["cs_im"], rec["cp_re"], rec["cp_im"], E, out=out, mosaic_weight=0.5)
+    full = dict(rec, L_esc=np.zeros(n), half_dL=np.zeros(n), apb=np.full(n, 2.0), bma=np.zeros(n), q=np.zeros(n))
+    ref = 0.5 * oc.coherent_spectrum(full, [n], [1.0], E, np.zeros(E.size))
+    _assert_close(out.cpu().numpy(), ref)
+    # window: lines beyond |v| > 30 add nothing
+    out.zero_()
+    run_coherent_reduction_kernel(rec["E_vac"], rec["a_vac"], rec["phase_slope"], rec["g_phase"], rec["cs_re"],
+                                  rec["cs_im"], rec["cp_re"], rec["cp_im"], E, out=out, sinc_cutoff=30.0)
+    f_s = np.zeros(E.size, complex)
+    f_p = np.zeros(E.size, complex)
+    for j in range(n):
+        v = rec["a_vac"][j] * (E - rec["E_vac"][j])
+        keep = np.abs(v) <= 30.0
+        sp = np.where(keep, np.sinc(v / np.pi), 0.0) * np.exp(1j * (rec["phase_slope"][j] * E - rec["g_phase"][j]))
+        f_s += (rec["cs_re"][j] + 1j * rec["cs_im"][j]) * sp
+        f_p += (rec["cp_re"][j] + 1j * rec["cp_im"][j]) * sp
+    _assert_close(out.cpu().numpy(), np.abs(f_s) ** 2 + np.abs(f_p) ** 2)
+
+
+@pytest.mark.gpu
+def test_gpu_coherent_bad_row_offsets_are_clamped_and_flagged():
+    """A row_off that is not a partition (a row ending before it starts, one
+    past n_line) stays inside the record arrays and sets PB_DEV_BAD_INPUT."""
+    import torch
+
+    lib = L.load()
+    dev = torch.device("cuda")
+    n_line, n_E = 10, 64
+    f = {k: torch.ones(n_line, dtype=torch.float64, device=dev) for k in oc.FIELDS}
+    E = torch.linspace(1000.0, 2000.0, n_E, dtype=torch.float64, device=dev)
+    dom = torch.zeros(n_E, dtype=torch.float64, device=dev)
+    for offs in ([0, 5, 3, 10], [0, 20, 10, 10]):
+        row_off = torch.tensor(offs, dtype=torch.int64, device=dev)
+        w = torch.ones(3, dtype=torch.float64, device=dev)
+        spec = torch.zeros(n_E, dtype=torch.float64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        nb = C.c_uint64()
+        assert lib.pb_coherent_work_size(3, n_line, n_E, C.byref(nb)) == 0
+        work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+        a = L.PbCoherentArgs()
+        a.n_row, a.n_E, a.n_line = 3, n_E, n_line
+        a.row_off, a.row_weight, a.E, a.delta_omega = row_off.data_ptr(), w.data_ptr(), E.data_ptr(), dom.data_ptr()
+        for k in oc.FIELDS:
+            setattr(a, k, f[k].data_ptr())
+        a.scale = 1.0
+        a.spec, a.work, a.work_bytes, a.status = spec.data_ptr(), work.data_ptr(), nb.value, status.data_ptr()
+        L.check(lib.pb_coherent_reduce(C.byref(a), torch.cuda.current_stream().cuda_stream), "pb_coherent_reduce")
+        torch.cuda.synchronize()
+        assert int(status.item()) & L.PB_DEV_BAD_INPUT
+        assert torch.isfinite(spec).all()
