@@ -15,11 +15,14 @@
 //
 // Precision: the propagation phase phi = phase_slope E - g_phase - L_esc
 // delta_omega(E) reaches 1e8 rad (emission time over hbar c times E), and the
-// formation argument v can reach 1e5 rad, so both are evaluated in FP64 and
-// reduced exactly to one turn (t = x / 2 pi, t - rint(t), Cody and Waite's
-// reduction with the integer part taken in FP64) before FP32 sin/cos. sin v
-// also divides by v near resonance, so it takes the accurate sincospif on the
-// half-turn remainder; the unit phasor exp(i phi) takes the SFU __sincosf.
+// formation argument v = a_vac (E - E_vac) - half_dL delta_omega reaches
+// 1e5 rad. Both are formed in FP64, in turns, and their integer parts removed
+// there (round to nearest by adding and subtracting 1.5 * 2^52); g_phase is
+// reduced once per line. The remaining fractions go to the SFU sine and
+// cosine in FP32 (absolute error about 2^-21 on [-pi, pi]). Near resonance,
+// |v| <= 1, sin v and cos v come instead from their Taylor series about 0
+// (Horner form in v^2, to the v^11 and v^12 terms: truncation below 2e-10),
+// since the formation factor divides sin v by v there.
 #include <cstdint>
 
 #include "pb_internal.h"
@@ -35,11 +38,22 @@ constexpr int64_t kMinChunk = 256;             // lines per work item, lower bou
 constexpr int64_t kTargetItemsTimesTiles = 148 * 8;
 constexpr float kSeriesW2 = 1.0e-6f;           // _formation.py:55 FORMATION_SERIES_W2
 
+// One line record as the field loop reads it: phase terms in turns.
 struct alignas(16) CohLine {
-    double ps, gp, L, a, Ev, h;                // phase slope, g.r, L_esc, a_vac, E_vac, half_dL
-    float apb, bma, q, csr, csi, cpr, cpi, pad;
+    double ps_t;    // phase_slope / 2 pi
+    double L_t;     // L_esc / 2 pi
+    double Ev;      // E_vac
+    double a, h;    // a_vac, half_dL
+    float gp_frac;  // g_phase / 2 pi minus its nearest integer
+    float apb, bma, q, csr, csi, cpr, cpi;
+    float pad[2];
 };
 static_assert(sizeof(CohLine) == 80, "CohLine packs into five 16-byte words");
+
+constexpr double kInv2Pi = 0.15915494309189535;
+constexpr double kRound64 = 6755399441055744.0;  // 1.5 * 2^52: x + c - c rounds |x| < 2^51 to an integer
+constexpr float kRound32 = 12582912.0f;          // 1.5 * 2^23, for |x| < 2^22
+constexpr float kTwoPiF = 6.2831853071795865f;
 
 __host__ __device__ __forceinline__ int64_t imin(int64_t x, int64_t y) { return x < y ? x : y; }
 __host__ __device__ __forceinline__ int64_t imax(int64_t x, int64_t y) { return x > y ? x : y; }
@@ -101,16 +115,20 @@ __global__ void __launch_bounds__(1024) coh_items_kernel(const int64_t *__restri
     if (bad && status) atomicOr(status, PB_DEV_BAD_INPUT);
 }
 
-// Half-turn remainder of x radians: x / pi reduced to [-1, 1].
-__device__ __forceinline__ float half_turns(double x) {
-    const double t = x * 0.15915494309189535;  // 1 / (2 pi)
-    return (float)((t - rint(t)) * 2.0);
-}
-
-// Radian remainder of x in [-pi, pi].
-__device__ __forceinline__ float radians_reduced(double x) {
-    const double t = x * 0.15915494309189535;
-    return (float)((t - rint(t)) * 6.283185307179586);
+// sin v and cos v for |v| <= 1 from their Taylor series (Horner in v^2).
+__device__ __forceinline__ void sincos_taylor(float v, float &sv, float &cv) {
+    const float z = v * v;
+    float ps = fmaf(z, -1.f / 39916800.f, 1.f / 362880.f);
+    ps = fmaf(z, ps, -1.f / 5040.f);
+    ps = fmaf(z, ps, 1.f / 120.f);
+    ps = fmaf(z, ps, -1.f / 6.f);
+    sv = fmaf(v * z, ps, v);
+    float pc = fmaf(z, 1.f / 479001600.f, -1.f / 3628800.f);
+    pc = fmaf(z, pc, 1.f / 40320.f);
+    pc = fmaf(z, pc, -1.f / 720.f);
+    pc = fmaf(z, pc, 1.f / 24.f);
+    pc = fmaf(z, pc, -0.5f);
+    cv = fmaf(z, pc, 1.f);
 }
 
 struct CohArgs {
@@ -118,13 +136,13 @@ struct CohArgs {
     const double *E, *dom;
     const double *E_vac, *a_vac, *ps, *gp, *csr, *csi, *cpr, *cpi, *L, *h, *apb, *bma, *q;
     int n_row, n_E;
-    double cutoff;  // > 0: |v| window
+    float cutoff;  // > 0: |v| window
     int64_t n_line, K, n_item_max;
     const int64_t *item_off;
     float *partial;  // [n_item_max][4][n_E]
 };
 
-__global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) coh_field_kernel(const CohArgs a) {
     __shared__ CohLine sm[kStage];
     const int64_t item = blockIdx.x;
     const int64_t n_item = a.item_off[a.n_row];
@@ -160,11 +178,12 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
         if (tid < n) {
             const int64_t j = s0 + tid;
             CohLine l;
-            l.ps = a.ps[j];
-            l.gp = a.gp[j];
-            l.L = a.L[j];
-            l.a = a.a_vac[j];
+            l.ps_t = a.ps[j] * kInv2Pi;
+            l.L_t = a.L[j] * kInv2Pi;
             l.Ev = a.E_vac[j];
+            const double gt = a.gp[j] * kInv2Pi;
+            l.gp_frac = (float)(gt - ((gt + kRound64) - kRound64));
+            l.a = a.a_vac[j];
             l.h = a.h[j];
             l.apb = (float)a.apb[j];
             l.bma = (float)a.bma[j];
@@ -173,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
             l.csi = (float)a.csi[j];
             l.cpr = (float)a.cpr[j];
             l.cpi = (float)a.cpi[j];
-            l.pad = 0.f;
+            l.pad[0] = l.pad[1] = 0.f;
             sm[tid] = l;
         }
         __syncthreads();
@@ -182,10 +201,10 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
 #pragma unroll
             for (int m = 0; m < kEPT; ++m) {
                 // formation factor of the absorbed piece (_formation.py:84-110)
-                const double v = l.a * (E[m] - l.Ev) - l.h * D[m];
-                if (a.cutoff > 0.0 && fabs(v) > a.cutoff) continue;
+                const double v = fma(l.a, E[m] - l.Ev, -l.h * D[m]);
                 const float vf = (float)v;
-                const float w2 = l.q * l.q + vf * vf;
+                if (a.cutoff > 0.f && fabsf(vf) > a.cutoff) continue;
+                const float w2 = fmaf(l.q, l.q, vf * vf);
                 float fr, fi;
                 if (w2 < kSeriesW2) {
                     const float half = 0.5f * l.apb;
@@ -193,15 +212,22 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
                     fi = -half * l.q * vf * (1.f / 3.f);
                 } else {
                     float sv, cv;
-                    sincospif(half_turns(v), &sv, &cv);
-                    const float inv = __frcp_rn(2.f * w2);
+                    if (fabsf(vf) <= 1.f) {
+                        sincos_taylor(vf, sv, cv);
+                    } else {
+                        const double tv = v * kInv2Pi;
+                        __sincosf((float)(tv - ((tv + kRound64) - kRound64)) * kTwoPiF, &sv, &cv);
+                    }
+                    const float inv = __fdividef(1.f, 2.f * w2);
                     fr = (vf * l.apb * sv - l.q * l.bma * cv) * inv;
                     fi = -(vf * l.bma * cv + l.q * l.apb * sv) * inv;
                 }
-                // propagation phase (_batched_finalize.py:213-215)
-                const double phi = l.ps * E[m] - l.gp - l.L * D[m];
+                // propagation phase (_batched_finalize.py:213-215), in turns
+                const double t = fma(l.ps_t, E[m], -l.L_t * D[m]);
+                float x = (float)(t - ((t + kRound64) - kRound64)) - l.gp_frac;
+                x -= (x + kRound32) - kRound32;
                 float sp, cp;
-                __sincosf(radians_reduced(phi), &sp, &cp);
+                __sincosf(x * kTwoPiF, &sp, &cp);
                 const float pr = fr * cp - fi * sp;
                 const float pi = fr * sp + fi * cp;
                 acc[m][0] += l.csr * pr - l.csi * pi;
@@ -279,7 +305,7 @@ cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
     a.q = p.q;
     a.n_row = p.n_row;
     a.n_E = p.n_E;
-    a.cutoff = p.sinc_cutoff;
+    a.cutoff = (float)p.sinc_cutoff;
     a.n_line = p.n_line;
     a.K = K;
     a.n_item_max = n_item_max;

@@ -117,7 +117,25 @@ def _chunk_lines(n_line, n_E):
     return -(-k // 128) * 128
 
 
+def _taylor_sincos(v):
+    """pb_coherent.cu sincos_taylor in float32: Taylor series to v^11 / v^12."""
+    f32 = np.float32
+    v = np.where(np.abs(v) <= 1, v, f32(0))  # the kernel takes this branch only for |v| <= 1
+    z = v * v
+    ps = z * f32(-1 / 39916800) + f32(1 / 362880)
+    for c in (-1 / 5040, 1 / 120, -1 / 6):
+        ps = z * ps + f32(c)
+    pc = z * f32(1 / 479001600) + f32(-1 / 3628800)
+    for c in (1 / 40320, -1 / 720, 1 / 24, -0.5):
+        pc = z * pc + f32(c)
+    return (v * z * ps + v).astype(f32), (z * pc + f32(1)).astype(f32)
+
+
 def kernel_emulation(rec, cnt, w, E, dom, Ne):
+    """The field kernel's arithmetic with float32 numpy: the formation
+    argument and the propagation phase formed and reduced to one turn in
+    float64, everything else float32, float32 sums per work item, float64
+    across items (SFU errors not modelled)."""
     f32 = np.float32
     E = np.asarray(E, dtype=np.float64)
     spec = np.zeros(E.size)
@@ -131,12 +149,14 @@ def kernel_emulation(rec, cnt, w, E, dom, Ne):
             for j in range(j0, min(j0 + K, off[r + 1])):
                 v = rec["a_vac"][j] * (E - rec["E_vac"][j]) - rec["half_dL"][j] * dom
                 vf = v.astype(f32)
+                tv = v * inv2pi
+                vr = ((tv - np.rint(tv)).astype(f32) * f32(2 * np.pi)).astype(f32)
                 q, apb, bma = f32(rec["q"][j]), f32(rec["apb"][j]), f32(rec["bma"][j])
-                w2 = q * q + vf * vf
-                t = v * inv2pi
-                x = ((t - np.rint(t)) * 2.0).astype(f32)
-                sv = np.sin(np.pi * x.astype(np.float64)).astype(f32)
-                cv = np.cos(np.pi * x.astype(np.float64)).astype(f32)
+                w2 = (q.astype(np.float64) * q + (vf * vf).astype(np.float64)).astype(f32)
+                st, ct = _taylor_sincos(vf)
+                near = np.abs(vf) <= 1
+                sv = np.where(near, st, np.sin(vr).astype(f32))
+                cv = np.where(near, ct, np.cos(vr).astype(f32))
                 with np.errstate(divide="ignore", over="ignore"):
                     inv = (f32(1.0) / (f32(2.0) * w2)).astype(f32)
                 fr = (vf * apb * sv - q * bma * cv) * inv
@@ -145,9 +165,12 @@ def kernel_emulation(rec, cnt, w, E, dom, Ne):
                 half = f32(0.5) * apb
                 fr = np.where(series, half * (f32(1) - q * q * f32(1 / 3) - vf * vf * f32(1 / 6)), fr)
                 fi = np.where(series, -half * q * vf * f32(1 / 3), fi)
-                phi = rec["phase_slope"][j] * E - rec["g_phase"][j] - rec["L_esc"][j] * dom
-                tp = phi * inv2pi
-                rp = ((tp - np.rint(tp)) * 6.283185307179586).astype(f32)
+                gt = rec["g_phase"][j] * inv2pi
+                gp_frac = f32(gt - np.rint(gt))
+                t = (rec["phase_slope"][j] * inv2pi) * E - (rec["L_esc"][j] * inv2pi) * dom
+                x = (t - np.rint(t)).astype(f32) - gp_frac
+                x = x - np.rint(x)
+                rp = (x * f32(2 * np.pi)).astype(f32)
                 sp, cp = np.sin(rp).astype(f32), np.cos(rp).astype(f32)
                 pr, pi = fr * cp - fi * sp, fr * sp + fi * cp
                 csr, csi, cpr, cpi = (f32(rec[k][j]) for k in ("cs_re", "cs_im", "cp_re", "cp_im"))
@@ -158,6 +181,15 @@ def kernel_emulation(rec, cnt, w, E, dom, Ne):
             F += acc.astype(np.float64)
         spec += w[r] * np.sum(F * F, axis=0)
     return spec / Ne
+
+
+def test_taylor_sincos_accuracy():
+    v = np.linspace(-1.0, 1.0, 20001).astype(np.float32)
+    s, c = _taylor_sincos(v)
+    assert np.max(np.abs(s - np.sin(v.astype(np.float64)))) < 2e-7
+    assert np.max(np.abs(c - np.cos(v.astype(np.float64)))) < 2e-7
+    small = np.abs(v) > 1e-30
+    assert np.max(np.abs(s[small] / np.sin(v[small].astype(np.float64)) - 1)) < 3e-7
 
 
 @pytest.mark.parametrize("name", CASES)
