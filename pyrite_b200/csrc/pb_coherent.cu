@@ -16,13 +16,18 @@
 // Precision: the propagation phase phi = phase_slope E - g_phase - L_esc
 // delta_omega(E) reaches 1e8 rad (emission time over hbar c times E), and the
 // formation argument v = a_vac (E - E_vac) - half_dL delta_omega reaches
-// 1e5 rad. Both are formed in FP64, in turns, and their integer parts removed
-// there (round to nearest by adding and subtracting 1.5 * 2^52); g_phase is
-// reduced once per line. The remaining fractions go to the SFU sine and
-// cosine in FP32 (absolute error about 2^-21 on [-pi, pi]). Near resonance,
-// |v| <= 1, sin v and cos v come instead from their Taylor series about 0
-// (Horner form in v^2, to the v^11 and v^12 terms: truncation below 2e-10),
-// since the formation factor divides sin v by v there.
+// 1e5 rad. Both are formed in FP64, in turns, as a chain of FMAs that
+// carries the constant 1.5 * 2^29: the sum then lies in [2^29, 2^30), whose
+// unit in the last place is 2^-23 turn, so the low 23 bits of its mantissa
+// are the fractional turn -- one bit mask instead of a rounding, a
+// subtraction and a conversion. A line whose terms could leave that binade
+// (checked per line against the CTA's energies) takes the plain FP64 path
+// instead: turns reduced by adding and subtracting 1.5 * 2^52, converted to
+// FP32. The fractions go to the SFU sine and cosine (absolute error about
+// 2^-21 on [-pi, pi]). Near resonance, |v| <= 1, sin v and cos v come from
+// their Taylor series about 0 (Horner form in v^2, to the v^11 and v^12
+// terms: truncation below 2e-10), since the formation factor divides sin v
+// by v there.
 #include <cstdint>
 
 #include "pb_internal.h"
@@ -31,36 +36,53 @@ namespace pb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kEPT = 2;                        // energies per thread
+constexpr int kEPT = 4;                        // energies per thread
 constexpr int kETile = kThreads * kEPT;        // energies per CTA
 constexpr int kStage = 128;                    // lines per shared-memory stage
 constexpr int64_t kMinChunk = 256;             // lines per work item, lower bound
-constexpr int64_t kTargetItemsTimesTiles = 148 * 8;
+constexpr int64_t kTargetItemsTimesTiles = 148 * 3 * 4;  // ~4 waves of 3 CTAs per SM
 constexpr float kSeriesW2 = 1.0e-6f;           // _formation.py:55 FORMATION_SERIES_W2
 
-// One line record as the field loop reads it: phase terms in turns.
+// One line record as the field loop reads it, phases in turns. ``fast``
+// lines hold the offset forms Gx = 1.5 * 2^29 - g_phase / 2 pi and
+// Vx = 1.5 * 2^29 - a_vac E_vac / 2 pi; the others hold g_phase / 2 pi and
+// E_vac.
 struct alignas(16) CohLine {
-    double ps_t;    // phase_slope / 2 pi
-    double L_t;     // L_esc / 2 pi
-    double Ev;      // E_vac
-    double a, h;    // a_vac, half_dL
-    float gp_frac;  // g_phase / 2 pi minus its nearest integer
-    float apb, bma, q, csr, csi, cpr, cpi;
+    double ps_t, L_t, a_t, h_t;  // phase_slope, L_esc, a_vac, half_dL over 2 pi
+    double Gx, Vx;
+    float apb, bma, q, qapb, qbma, csr, csi, cpr, cpi;
+    int fast;
     float pad[2];
 };
-static_assert(sizeof(CohLine) == 80, "CohLine packs into five 16-byte words");
+static_assert(sizeof(CohLine) == 96, "CohLine packs into six 16-byte words");
 
 constexpr double kInv2Pi = 0.15915494309189535;
 constexpr double kRound64 = 6755399441055744.0;  // 1.5 * 2^52: x + c - c rounds |x| < 2^51 to an integer
-constexpr float kRound32 = 12582912.0f;          // 1.5 * 2^23, for |x| < 2^22
 constexpr float kTwoPiF = 6.2831853071795865f;
+constexpr double kTurnBase = 805306368.0;        // 1.5 * 2^29
+constexpr double kFastLimit = 134217728.0;       // 2^27 turns: offset sums stay in [2^29, 2^30)
+
+// (sin, cos) of 2 pi f, f the fraction of x - kTurnBase, for x in [2^29, 2^30).
+__device__ __forceinline__ void sincos_turns_offset(double x, float &s, float &c) {
+    const unsigned lo = (unsigned)__double2loint(x);
+    const float g = __uint_as_float((lo & 0x7FFFFFu) | 0x3F800000u) - 1.5f;  // f - 1/2 in [-1/2, 1/2)
+    float sg, cg;
+    __sincosf(g * kTwoPiF, &sg, &cg);
+    s = -sg;  // sin(2 pi f) = -sin(2 pi (f - 1/2))
+    c = -cg;
+}
+
+// (sin, cos) of 2 pi t for any FP64 t with |t| < 2^51.
+__device__ __forceinline__ void sincos_turns(double t, float &s, float &c) {
+    __sincosf((float)(t - ((t + kRound64) - kRound64)) * kTwoPiF, &s, &c);
+}
 
 __host__ __device__ __forceinline__ int64_t imin(int64_t x, int64_t y) { return x < y ? x : y; }
 __host__ __device__ __forceinline__ int64_t imax(int64_t x, int64_t y) { return x > y ? x : y; }
 
 __host__ __device__ inline int64_t n_etiles(int n_E) { return (n_E + kETile - 1) / kETile; }
 
-// Lines per work item: enough items for ~8 CTAs per SM over the energy tiles,
+// Lines per work item: enough items for ~4 waves over the energy tiles,
 // never below kMinChunk, a multiple of kStage.
 __host__ inline int64_t chunk_lines(int64_t n_line, int n_E) {
     int64_t items = kTargetItemsTimesTiles / n_etiles(n_E);
@@ -131,6 +153,30 @@ __device__ __forceinline__ void sincos_taylor(float v, float &sv, float &cv) {
     cv = fmaf(z, pc, 1.f);
 }
 
+// acc += (c_sigma, c_pi) F(v) exp(i phi): the formation factor of the
+// absorbed piece (_formation.py:84-110, series below |w|^2 < 1e-6) rotated by
+// the propagation phase (_batched_finalize.py:213-218).
+__device__ __forceinline__ void add_line_field(const CohLine &l, float vf, float sv, float cv, float sp, float cp,
+                                               float acc[4]) {
+    const float w2 = fmaf(l.q, l.q, vf * vf);
+    float fr, fi;
+    if (w2 < kSeriesW2) {
+        const float half = 0.5f * l.apb;
+        fr = half * (1.f - l.q * l.q * (1.f / 3.f) - vf * vf * (1.f / 6.f));
+        fi = -half * l.q * vf * (1.f / 3.f);
+    } else {
+        const float inv = __fdividef(0.5f, w2);
+        fr = fmaf(vf * l.apb, sv, -l.qbma * cv) * inv;
+        fi = -fmaf(vf * l.bma, cv, l.qapb * sv) * inv;
+    }
+    const float pr = fmaf(fr, cp, -fi * sp);
+    const float pi = fmaf(fr, sp, fi * cp);
+    acc[0] = fmaf(l.csr, pr, fmaf(-l.csi, pi, acc[0]));
+    acc[1] = fmaf(l.csr, pi, fmaf(l.csi, pr, acc[1]));
+    acc[2] = fmaf(l.cpr, pr, fmaf(-l.cpi, pi, acc[2]));
+    acc[3] = fmaf(l.cpr, pi, fmaf(l.cpi, pr, acc[3]));
+}
+
 struct CohArgs {
     const int64_t *row_off;
     const double *E, *dom;
@@ -142,7 +188,7 @@ struct CohArgs {
     float *partial;  // [n_item_max][4][n_E]
 };
 
-__global__ void __launch_bounds__(kThreads, 4) coh_field_kernel(const CohArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a) {
     __shared__ CohLine sm[kStage];
     const int64_t item = blockIdx.x;
     const int64_t n_item = a.item_off[a.n_row];
@@ -172,6 +218,31 @@ __global__ void __launch_bounds__(kThreads, 4) coh_field_kernel(const CohArgs a)
 #pragma unroll
     for (int m = 0; m < kEPT; ++m) acc[m][0] = acc[m][1] = acc[m][2] = acc[m][3] = 0.f;
 
+    // largest |E| and |delta_omega| of this CTA's energies (for the fast-path check)
+    __shared__ double red[2][kThreads / 32];
+    double em = 0.0, dm = 0.0;
+#pragma unroll
+    for (int m = 0; m < kEPT; ++m) {
+        em = fmax(em, fabs(E[m]));
+        dm = fmax(dm, fabs(D[m]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        em = fmax(em, __shfl_xor_sync(0xffffffffu, em, o));
+        dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+    }
+    if ((tid & 31) == 0) {
+        red[0][tid >> 5] = em;
+        red[1][tid >> 5] = dm;
+    }
+    __syncthreads();
+    double Emax = 0.0, Dmax = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        Emax = fmax(Emax, red[0][w]);
+        Dmax = fmax(Dmax, red[1][w]);
+    }
+
     for (int64_t s0 = j0; s0 < j1; s0 += kStage) {
         const int n = (int)imin(kStage, j1 - s0);
         __syncthreads();  // the previous stage has been read
@@ -180,14 +251,19 @@ __global__ void __launch_bounds__(kThreads, 4) coh_field_kernel(const CohArgs a)
             CohLine l;
             l.ps_t = a.ps[j] * kInv2Pi;
             l.L_t = a.L[j] * kInv2Pi;
-            l.Ev = a.E_vac[j];
-            const double gt = a.gp[j] * kInv2Pi;
-            l.gp_frac = (float)(gt - ((gt + kRound64) - kRound64));
-            l.a = a.a_vac[j];
-            l.h = a.h[j];
+            l.a_t = a.a_vac[j] * kInv2Pi;
+            l.h_t = a.h[j] * kInv2Pi;
+            const double gt = a.gp[j] * kInv2Pi, Ev = a.E_vac[j];
+            const double phase_span = fabs(l.ps_t) * Emax + fabs(gt) + fabs(l.L_t) * Dmax;
+            const double v_span = fabs(l.a_t) * (Emax + fabs(Ev)) + fabs(l.h_t) * Dmax;
+            l.fast = phase_span < kFastLimit && v_span < kFastLimit;  // false for NaN too
+            l.Gx = l.fast ? kTurnBase - gt : gt;
+            l.Vx = l.fast ? kTurnBase - l.a_t * Ev : Ev;
             l.apb = (float)a.apb[j];
             l.bma = (float)a.bma[j];
             l.q = (float)a.q[j];
+            l.qapb = l.q * l.apb;
+            l.qbma = l.q * l.bma;
             l.csr = (float)a.csr[j];
             l.csi = (float)a.csi[j];
             l.cpr = (float)a.cpr[j];
@@ -198,42 +274,30 @@ __global__ void __launch_bounds__(kThreads, 4) coh_field_kernel(const CohArgs a)
         __syncthreads();
         for (int i = 0; i < n; ++i) {
             const CohLine l = sm[i];
+            if (l.fast) {  // uniform over the block: one line at a time
 #pragma unroll
-            for (int m = 0; m < kEPT; ++m) {
-                // formation factor of the absorbed piece (_formation.py:84-110)
-                const double v = fma(l.a, E[m] - l.Ev, -l.h * D[m]);
-                const float vf = (float)v;
-                if (a.cutoff > 0.f && fabsf(vf) > a.cutoff) continue;
-                const float w2 = fmaf(l.q, l.q, vf * vf);
-                float fr, fi;
-                if (w2 < kSeriesW2) {
-                    const float half = 0.5f * l.apb;
-                    fr = half * (1.f - l.q * l.q * (1.f / 3.f) - vf * vf * (1.f / 6.f));
-                    fi = -half * l.q * vf * (1.f / 3.f);
-                } else {
-                    float sv, cv;
-                    if (fabsf(vf) <= 1.f) {
-                        sincos_taylor(vf, sv, cv);
-                    } else {
-                        const double tv = v * kInv2Pi;
-                        __sincosf((float)(tv - ((tv + kRound64) - kRound64)) * kTwoPiF, &sv, &cv);
-                    }
-                    const float inv = __fdividef(1.f, 2.f * w2);
-                    fr = (vf * l.apb * sv - l.q * l.bma * cv) * inv;
-                    fi = -(vf * l.bma * cv + l.q * l.apb * sv) * inv;
+                for (int m = 0; m < kEPT; ++m) {
+                    const double vx = fma(l.a_t, E[m], fma(-l.h_t, D[m], l.Vx));
+                    const float vf = (float)(vx - kTurnBase) * kTwoPiF;
+                    if (a.cutoff > 0.f && fabsf(vf) > a.cutoff) continue;
+                    float sv, cv, sp, cp;
+                    if (fabsf(vf) <= 1.f) sincos_taylor(vf, sv, cv);
+                    else sincos_turns_offset(vx, sv, cv);
+                    sincos_turns_offset(fma(l.ps_t, E[m], fma(-l.L_t, D[m], l.Gx)), sp, cp);
+                    add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
                 }
-                // propagation phase (_batched_finalize.py:213-215), in turns
-                const double t = fma(l.ps_t, E[m], -l.L_t * D[m]);
-                float x = (float)(t - ((t + kRound64) - kRound64)) - l.gp_frac;
-                x -= (x + kRound32) - kRound32;
-                float sp, cp;
-                __sincosf(x * kTwoPiF, &sp, &cp);
-                const float pr = fr * cp - fi * sp;
-                const float pi = fr * sp + fi * cp;
-                acc[m][0] += l.csr * pr - l.csi * pi;
-                acc[m][1] += l.csr * pi + l.csi * pr;
-                acc[m][2] += l.cpr * pr - l.cpi * pi;
-                acc[m][3] += l.cpr * pi + l.cpi * pr;
+            } else {
+#pragma unroll
+                for (int m = 0; m < kEPT; ++m) {
+                    const double vt = fma(l.a_t, E[m] - l.Vx, -l.h_t * D[m]);
+                    const float vf = (float)vt * kTwoPiF;
+                    if (a.cutoff > 0.f && fabsf(vf) > a.cutoff) continue;
+                    float sv, cv, sp, cp;
+                    if (fabsf(vf) <= 1.f) sincos_taylor(vf, sv, cv);
+                    else sincos_turns(vt, sv, cv);
+                    sincos_turns(fma(l.ps_t, E[m], -fma(l.L_t, D[m], l.Gx)), sp, cp);
+                    add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
+                }
             }
         }
     }

@@ -131,47 +131,81 @@ def _taylor_sincos(v):
     return (v * z * ps + v).astype(f32), (z * pc + f32(1)).astype(f32)
 
 
-def kernel_emulation(rec, cnt, w, E, dom, Ne):
-    """The field kernel's arithmetic with float32 numpy: the formation
-    argument and the propagation phase formed and reduced to one turn in
-    float64, everything else float32, float32 sums per work item, float64
-    across items (SFU errors not modelled)."""
+TURN_BASE = 805306368.0  # 1.5 * 2^29
+FAST_LIMIT = 2.0 ** 27
+INV2PI = 0.15915494309189535
+
+
+def _fma(a, b, c):
+    """Fused multiply-add in float64, emulated through the x87 extended type."""
+    ld = np.longdouble
+    return (np.asarray(a, dtype=ld) * np.asarray(b, dtype=ld) + np.asarray(c, dtype=ld)).astype(np.float64)
+
+
+def turn_fraction_offset(x):
+    """pb_coherent.cu sincos_turns_offset: f - 1/2 from the low 23 mantissa bits of x in [2^29, 2^30)."""
+    bits = np.asarray(x, dtype=np.float64).view(np.uint64) & np.uint64(0x7FFFFF)
+    return (np.float32(1.0) + (bits.astype(np.float64) / 2.0 ** 23).astype(np.float32)) - np.float32(1.5)
+
+
+def kernel_emulation(rec, cnt, w, E, dom, Ne, tile=1024):
+    """The field kernel's arithmetic with numpy: per line and energy tile the
+    offset-binade FP64 path (or the plain FP64 reduction when a line's terms
+    could leave the binade), FP32 formation factor, rotation and per-item
+    sums, FP64 across items (SFU errors not modelled)."""
     f32 = np.float32
     E = np.asarray(E, dtype=np.float64)
     spec = np.zeros(E.size)
     K = _chunk_lines(int(np.sum(cnt)), E.size)
     off = np.concatenate([[0], np.cumsum(cnt)])
-    inv2pi = 0.15915494309189535
+    two_pi = f32(2 * np.pi)
+    Emax = np.zeros(E.size)
+    Dmax = np.zeros(E.size)
+    for t0 in range(0, E.size, tile):
+        Emax[t0:t0 + tile] = np.max(np.abs(E[t0:t0 + tile]))
+        Dmax[t0:t0 + tile] = np.max(np.abs(dom[t0:t0 + tile]))
     for r in range(len(cnt)):
         F = np.zeros((4, E.size))
         for j0 in range(off[r], off[r + 1], K):
             acc = np.zeros((4, E.size), dtype=f32)
             for j in range(j0, min(j0 + K, off[r + 1])):
-                v = rec["a_vac"][j] * (E - rec["E_vac"][j]) - rec["half_dL"][j] * dom
-                vf = v.astype(f32)
-                tv = v * inv2pi
-                vr = ((tv - np.rint(tv)).astype(f32) * f32(2 * np.pi)).astype(f32)
-                q, apb, bma = f32(rec["q"][j]), f32(rec["apb"][j]), f32(rec["bma"][j])
-                w2 = (q.astype(np.float64) * q + (vf * vf).astype(np.float64)).astype(f32)
+                ps_t, L_t = rec["phase_slope"][j] * INV2PI, rec["L_esc"][j] * INV2PI
+                a_t, h_t = rec["a_vac"][j] * INV2PI, rec["half_dL"][j] * INV2PI
+                gt, Ev = rec["g_phase"][j] * INV2PI, rec["E_vac"][j]
+                fast = ((abs(ps_t) * Emax + abs(gt) + abs(L_t) * Dmax < FAST_LIMIT)
+                        & (abs(a_t) * (Emax + abs(Ev)) + abs(h_t) * Dmax < FAST_LIMIT))
+                # fast: offset sums, fraction from the mantissa; sin/cos negated back
+                vx = _fma(a_t, E, _fma(-h_t, dom, TURN_BASE - a_t * Ev))
+                px = _fma(ps_t, E, _fma(-L_t, dom, TURN_BASE - gt))
+                vf_fast = ((vx - TURN_BASE).astype(f32) * two_pi).astype(f32)
+                gv, gp = turn_fraction_offset(vx), turn_fraction_offset(px)
+                sv_f = -np.sin((gv * two_pi).astype(f32)).astype(f32)
+                cv_f = -np.cos((gv * two_pi).astype(f32)).astype(f32)
+                sp_f = -np.sin((gp * two_pi).astype(f32)).astype(f32)
+                cp_f = -np.cos((gp * two_pi).astype(f32)).astype(f32)
+                # plain: turns reduced in FP64
+                vt = _fma(a_t, E - Ev, -h_t * dom)
+                vf_slow = (vt.astype(f32) * two_pi).astype(f32)
+                xv = ((vt - np.rint(vt)).astype(f32) * two_pi).astype(f32)
+                pt = _fma(ps_t, E, -_fma(L_t, dom, gt))
+                xp = ((pt - np.rint(pt)).astype(f32) * two_pi).astype(f32)
+                vf = np.where(fast, vf_fast, vf_slow)
                 st, ct = _taylor_sincos(vf)
                 near = np.abs(vf) <= 1
-                sv = np.where(near, st, np.sin(vr).astype(f32))
-                cv = np.where(near, ct, np.cos(vr).astype(f32))
-                with np.errstate(divide="ignore", over="ignore"):
-                    inv = (f32(1.0) / (f32(2.0) * w2)).astype(f32)
-                fr = (vf * apb * sv - q * bma * cv) * inv
-                fi = -(vf * bma * cv + q * apb * sv) * inv
+                sv = np.where(near, st, np.where(fast, sv_f, np.sin(xv).astype(f32)))
+                cv = np.where(near, ct, np.where(fast, cv_f, np.cos(xv).astype(f32)))
+                sp = np.where(fast, sp_f, np.sin(xp).astype(f32))
+                cp = np.where(fast, cp_f, np.cos(xp).astype(f32))
+                q, apb, bma = f32(rec["q"][j]), f32(rec["apb"][j]), f32(rec["bma"][j])
+                w2 = (q.astype(np.float64) * q + (vf * vf).astype(np.float64)).astype(f32)
+                with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+                    inv = (f32(0.5) / w2).astype(f32)
+                fr = ((vf * apb).astype(np.float64) * sv - (q * bma * cv).astype(np.float64)).astype(f32) * inv
+                fi = -((vf * bma).astype(np.float64) * cv + (q * apb * sv).astype(np.float64)).astype(f32) * inv
                 series = w2 < f32(1e-6)
                 half = f32(0.5) * apb
                 fr = np.where(series, half * (f32(1) - q * q * f32(1 / 3) - vf * vf * f32(1 / 6)), fr)
                 fi = np.where(series, -half * q * vf * f32(1 / 3), fi)
-                gt = rec["g_phase"][j] * inv2pi
-                gp_frac = f32(gt - np.rint(gt))
-                t = (rec["phase_slope"][j] * inv2pi) * E - (rec["L_esc"][j] * inv2pi) * dom
-                x = (t - np.rint(t)).astype(f32) - gp_frac
-                x = x - np.rint(x)
-                rp = (x * f32(2 * np.pi)).astype(f32)
-                sp, cp = np.sin(rp).astype(f32), np.cos(rp).astype(f32)
                 pr, pi = fr * cp - fi * sp, fr * sp + fi * cp
                 csr, csi, cpr, cpi = (f32(rec[k][j]) for k in ("cs_re", "cs_im", "cp_re", "cp_im"))
                 acc[0] += csr * pr - csi * pi
@@ -181,6 +215,39 @@ def kernel_emulation(rec, cnt, w, E, dom, Ne):
             F += acc.astype(np.float64)
         spec += w[r] * np.sum(F * F, axis=0)
     return spec / Ne
+
+
+def _whole_turns_added(rec, every=2, turns=1e9):
+    """Every other line's g_phase moved by a whole number of turns: the same
+    physics, but beyond the offset binade, so those lines take the plain path."""
+    out = dict(rec)
+    gp = rec["g_phase"].copy()
+    gp[::every] += 2.0 * np.pi * turns
+    out["g_phase"] = gp
+    return out
+
+
+def test_float_plan_mixes_both_phase_paths():
+    rec, cnt, w, E, dom, Ne, spec = _golden("hopg20")
+    moved = _whole_turns_added(rec)
+    gt = moved["g_phase"] * INV2PI
+    assert np.count_nonzero(np.abs(gt) > FAST_LIMIT) * 3 > rec["g_phase"].size
+    _assert_close(kernel_emulation(moved, cnt, w, E, dom, Ne), spec, PEAK_TOL / 4, REL_TOL / 4)
+
+
+def test_turn_fraction_from_the_offset_binade():
+    """x = 1.5 * 2^29 + t in [2^29, 2^30): the low 23 mantissa bits are t's
+    fractional turn to 2^-23; the extracted f - 1/2 matches it."""
+    rng = np.random.default_rng(2)
+    t = np.concatenate([rng.uniform(-2.0 ** 27, 2.0 ** 27, 100000), rng.uniform(-3, 3, 1000), [0.0, 0.25, -0.5]])
+    x = TURN_BASE + t
+    assert np.all((x >= 2.0 ** 29) & (x < 2.0 ** 30))
+    g = turn_fraction_offset(x).astype(np.float64)
+    frac = (x - TURN_BASE) - np.floor(x - TURN_BASE)  # exact: x - base is exact (Sterbenz)
+    d = (g + 0.5) - frac
+    d -= np.rint(d)
+    assert np.max(np.abs(d)) == 0.0
+    assert np.max(np.abs(((x - TURN_BASE) - t))) <= 2.0 ** -24 + 1e-30
 
 
 def test_taylor_sincos_accuracy():
@@ -272,6 +339,16 @@ def _random_rows(rng, n_rows, n_per_row, E_lo, E_hi):
         half_dL=rng.uniform(-1e5, 1e5, n), apb=a + b, bma=b - a, q=q,
     )
     return rec, np.full(n_rows, n_per_row), rng.uniform(0.1, 1.0, n_rows)
+
+
+@pytest.mark.gpu
+def test_gpu_coherent_both_phase_paths_agree():
+    """Whole turns added to half the lines' g_phase (plain FP64 path) leave
+    the reference spectrum unchanged."""
+    from pyrite_b200.coherent import coherent_spectrum
+
+    rec, cnt, w, E, dom, Ne, spec = _golden("hopg20")
+    _assert_close(coherent_spectrum(_whole_turns_added(rec), cnt, w, E, dom, Ne), spec)
 
 
 @pytest.mark.gpu
