@@ -311,6 +311,123 @@ def run_sweep(args, torch):
     print(json.dumps(line), flush=True)
 
 
+# Issued thread-instructions per (line, energy) pair of coh_field_kernel, from its ncu
+# capture (profiles/coh_field_kernel_8rows_1M_lines_2048E.md); with 4 warp issue slots per SM
+# per cycle this sets the kernel's issue ceiling in pairs/s.
+COH_INSTR_PER_PAIR = 65.5
+
+
+def coherent_records(rng, n_rows, per_row, E_lo, E_hi):
+    """Seeded line records with the ranges of the reference's coherent fixtures:
+    phases to 6e7 rad, formation widths 0.5-60 per eV, escape optical depths to 12."""
+    n = n_rows * per_row
+    tau_s = rng.uniform(0.0, 6.0, n)
+    tau_e = tau_s + rng.uniform(-tau_s, 6.0, n)
+    a, b = np.exp(-0.5 * tau_s), np.exp(-0.5 * tau_e)
+    rec = dict(E_vac=rng.uniform(E_lo, E_hi, n), a_vac=rng.uniform(0.5, 60.0, n),
+               phase_slope=rng.uniform(-3000.0, 3000.0, n), g_phase=rng.uniform(-6e7, 6e7, n),
+               cs_re=rng.normal(0, 1e-4, n), cs_im=rng.normal(0, 1e-5, n), cp_re=rng.normal(0, 1e-4, n),
+               cp_im=rng.normal(0, 1e-5, n), L_esc=rng.uniform(0.0, 2e5, n), half_dL=rng.uniform(-1e5, 1e5, n),
+               apb=a + b, bma=b - a, q=0.25 * (tau_e - tau_s))
+    return rec, np.full(n_rows, per_row, dtype=np.int64), rng.uniform(0.1, 1.0, n_rows)
+
+
+def run_coherent(args, torch):
+    """The coherent (field-sum) CXR reduction: 8 rows (reflection x mosaic
+    node) x 125,000 line records x 2048 energies (1-61 keV) per step, i.e.
+    2.048e9 line-energy pairs. ``value``: records resident on the device,
+    raw C-ABI calls; ``e2e``: the public host API from host records each
+    step, spectrum read back; ``cpu_baseline``: the numpy FP64 oracle on one
+    row of 4,000 lines over the same energies."""
+    import ctypes as C
+
+    from oracle import coherent as oc
+    from pyrite_b200 import _lib as L
+    from pyrite_b200.coherent import RECORD_FIELDS, coherent_reduce
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(3)
+    n_rows, per_row = 8, 125_000
+    rec, cnt, w = coherent_records(rng, n_rows, per_row, 2000.0, 60000.0)
+    E = np.linspace(1000.0, 61000.0, 2048)
+    dom = 2.3e-4 * (1e4 / (E + 500.0)) ** 2 * E / 1973.27
+    n_line = int(cnt.sum())
+    pairs = n_line * E.size
+    lib = L.load()
+    drec = {k: torch.as_tensor(rec[k], device=dev) for k in RECORD_FIELDS}
+    row_off = torch.as_tensor(np.concatenate([[0], np.cumsum(cnt)]), dtype=torch.int64, device=dev)
+    wt, Et, Dt = (torch.as_tensor(x, device=dev) for x in (w, E, dom))
+    spec = torch.zeros(E.size, dtype=torch.float64, device=dev)
+    nb = C.c_uint64()
+    L.check(lib.pb_coherent_work_size(n_rows, n_line, E.size, C.byref(nb)), "pb_coherent_work_size")
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    a = L.PbCoherentArgs()
+    a.n_row, a.n_E, a.n_line = n_rows, E.size, n_line
+    a.row_off, a.row_weight, a.E, a.delta_omega = (t.data_ptr() for t in (row_off, wt, Et, Dt))
+    for k in RECORD_FIELDS:
+        setattr(a, k, drec[k].data_ptr())
+    a.scale, a.spec, a.work, a.work_bytes = 1.0, spec.data_ptr(), work.data_ptr(), nb.value
+    stream = torch.cuda.current_stream()
+
+    def call():
+        L.check(lib.pb_coherent_reduce(C.byref(a), stream.cuda_stream), "pb_coherent_reduce")
+
+    for _ in range(max(args.warmup, 3)):
+        call()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as sampler:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            call()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    clocks = sampler.summary()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    value = pairs / (ms * 1e-3)
+    # e2e: the host API from host (pinned) records, spectrum read back every step
+    host = {k: torch.as_tensor(rec[k]).pin_memory() for k in RECORD_FIELDS}
+    coherent_reduce(host, cnt, w, E, dom, device=dev).cpu()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = coherent_reduce(host, cnt, w, E, dom, device=dev).cpu().numpy()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    h2d = 8 * (len(RECORD_FIELDS) * n_line + 2 * E.size + n_rows + n_rows + 1)
+    # parity on every 64th energy against the FP64 oracle
+    sub = np.arange(0, E.size, 64)
+    ref = oc.coherent_spectrum(rec, cnt, w, E[sub], dom[sub])
+    parity = float(np.max(np.abs(out[sub] - ref)) / np.max(ref))
+    # CPU baseline: the numpy oracle on one row of 4,000 lines, all energies
+    n_cpu = 4000
+    sample = {k: v[:n_cpu] for k, v in rec.items()}
+    t0 = time.perf_counter()
+    oc.coherent_spectrum(sample, [n_cpu], [1.0], E, dom)
+    cpu_rate = n_cpu * E.size / (time.perf_counter() - t0)
+    peak_pairs = 148 * (clocks.get("sm_mhz") or 1965) * 1e6 * 128 / COH_INSTR_PER_PAIR
+    line = {
+        "metric": "coherent CXR reduction line-energy pairs/s on 1 B200", "value": value, "unit": "pairs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 phases, f32 trig",
+        "data": "synthetic",
+        "config": {"workload": "8 rows x 125,000 line records x 2048 energies (1-61 keV), records resident "
+                               "(104 MB) above L2 between steps", "pairs_per_step": pairs},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "issue", "achieved": value, "peak": peak_pairs, "unit": "pairs/s",
+                     "frac": value / peak_pairs, "traffic": None,
+                     "note": "issue ceiling 148 SM x clock x 128 thread-instr per cycle / %.1f instr per pair "
+                             "(ncu); no HBM or tensor roofline applies" % COH_INSTR_PER_PAIR},
+        "e2e": {"value": pairs / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 8 * E.size},
+        "cpu_baseline": {"value": cpu_rate, "unit": "pairs/s", "cores": 1, "kind": "port",
+                         "sample": "numpy FP64 oracle, 1 row x 4,000 lines x 2048 energies"},
+        "parity_vs_oracle_max_rel_to_peak": parity,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,10 +448,11 @@ def main():
     ap.add_argument("--train-domain", default="case", choices=["case", "uniform"],
                     help="surrogate training segments: the case's transport, or spread over the whole input "
                          "domain (5-100 MeV, +-5 mrad, every depth; adds a 1e5-segment held-out audit)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "sweep", "stack"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "sweep", "stack", "coherent"],
                     help="c2: the headline step (default); sweep: the 256-configuration design sweep, "
                          "one graph replay against sequential plain launches; stack: the 10 MeV HOPG / Si / W "
-                         "stack with four detectors (each its own JSON line)")
+                         "stack with four detectors; coherent: the coherent CXR field-sum reduction "
+                         "(each its own JSON line)")
     ap.add_argument("--sweep-scale", type=float, default=1.0, help="scale of every sweep case's histories")
     ap.add_argument("--sweep-streams", type=int, default=8, help="concurrent case streams of the tuned sweep")
     args = ap.parse_args()
@@ -366,6 +484,10 @@ def main():
     if args.workload == "stack":
         if rank == 0:
             run_stack(args, torch)
+        return
+    if args.workload == "coherent":
+        if rank == 0:
+            run_coherent(args, torch)
         return
 
     dist = None
