@@ -193,6 +193,11 @@ def _declare(L):
         C.POINTER(_CxrTables), C.POINTER(_CxrGeom), C.c_int64, _D, _D, _D, _D, _I64, C.c_int64,
         _D, _D, _D, _U8, C.c_int,
     ]
+    L.or_cxr_coherent_records.restype = None
+    L.or_cxr_coherent_records.argtypes = [
+        C.POINTER(_CxrTables), C.POINTER(_CxrGeom), C.c_int64, _D, _D, _D, _D, _D, _I64, C.c_int64,
+        C.POINTER(_D), _U8,
+    ]
     L.or_reduce_node.restype = None
     L.or_reduce_node.argtypes = [C.c_int64, _D, _D, _D, C.c_int64, _D, _D, C.c_int]
     L.or_reduce_binmean.restype = None
@@ -387,6 +392,42 @@ def cxr_lines(tables: dict, n_hat, thickness, seg: dict, Ne, layers: LayerEscape
         _p(eid, _I64), int(Ne), _p(E_res, _D), _p(aw, _D), _p(w, _D), _p(good, _U8), 1,
     )
     return E_res, aw, w, good.astype(bool)
+
+
+def cxr_coherent_records(tables: dict, n_hat, thickness, seg: dict, Ne):
+    """Coherent route line records per (segment, row), segment-major, single
+    slab: ``({field: [n_seg*n_g]}, good)`` with the fields of
+    ``oracle.coherent.FIELDS``; ``seg`` may carry ``t_ang`` (start ages)."""
+    from .coherent import FIELDS
+
+    G = _f64(tables["G"])
+    ES, EP, WM = _f64(tables["ES"]), _f64(tables["EP"]), _f64(tables["WM"])
+    row_table = np.ascontiguousarray(tables["row_table"], dtype=np.int32)
+    E_tab = _f64(tables["E_tab"])
+    chi_re, chi_im = _f64(tables["chi_re"]), _f64(tables["chi_im"])
+    u_re, u_im = _f64(tables["u_re"]), _f64(tables["u_im"])
+    log_mu = _f64(np.atleast_2d(tables["log_mu"]))
+    delta = _f64(tables["delta"])
+    t = _CxrTables(
+        int(G.shape[0]), _p(G, _D), _p(ES, _D), _p(EP, _D), _p(WM, _D), _p(row_table, _I32),
+        int(E_tab.size), _p(E_tab, _D), _p(chi_re, _D), _p(chi_im, _D), _p(u_re, _D),
+        _p(u_im, _D), int(log_mu.shape[0]), _p(log_mu, _D), _p(delta, _D),
+        float(tables["lo_keep"]), float(tables["hi_keep"]),
+    )
+    geo = _CxrGeom((C.c_double * 3)(*[float(v) for v in n_hat]), float(thickness), None)
+    v_hat, E, L, r = (_f64(seg[k]) for k in ("v_hat", "E_keV", "L_ang", "r_mid"))
+    t_ang = _f64(seg["t_ang"]) if seg.get("t_ang") is not None else None
+    eid = np.ascontiguousarray(seg["elec_id"], dtype=np.int64)
+    n = int(E.size)
+    m = n * int(G.shape[0])
+    out = {k: np.empty(m) for k in FIELDS}
+    ptrs = (_D * len(FIELDS))(*[_p(out[k], _D) for k in FIELDS])
+    good = np.empty(m, dtype=np.uint8)
+    lib().or_cxr_coherent_records(
+        C.byref(t), C.byref(geo), n, _p(v_hat, _D), _p(E, _D), _p(L, _D), _p(r, _D),
+        None if t_ang is None else _p(t_ang, _D), _p(eid, _I64), int(Ne), ptrs, _p(good, _U8),
+    )
+    return out, good.astype(bool)
 
 
 def reduce_node(E_res, a_width, weight, E_grid):

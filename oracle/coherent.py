@@ -78,6 +78,17 @@ def coherent_spectrum(rec, row_count, row_weight, E, delta_omega, Ne=1):
     return spec / Ne
 
 
+def rows_from_pairs(pairs, good, n_g):
+    """Per-row record layout of the reference's block loop (cxr/_batched.py:640-660
+    flattens g-major and keeps ``good``): row r holds its good pairs in
+    segment order. ``pairs`` maps FIELDS to segment-major [n_seg*n_g] arrays.
+    Returns ``(records, row_count)``."""
+    good = np.asarray(good, dtype=bool).reshape(-1, n_g)
+    keep_t = good.T.reshape(-1)
+    rec = {k: np.asarray(pairs[k]).reshape(-1, n_g).T.reshape(-1)[keep_t] for k in FIELDS}
+    return rec, good.sum(axis=0).astype(np.int64)
+
+
 def load_golden(path):
     """``(records, row_count, row_weight, E, delta_omega, Ne, spec)`` of a coherent fixture."""
     z = np.load(path)

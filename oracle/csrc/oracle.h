@@ -148,6 +148,18 @@ void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
                   const double *r_mid, const int64_t *elec_id, int64_t Ne, double *E_res,
                   double *a_width, double *weight, uint8_t *good, int n_threads);
 
+/* Coherent route line records per (segment, row), single slab, one escape
+ * piece per segment (cxr/_batched.py:561-660 on the rows of _batched_block,
+ * cxr/_batched.py:479-559): rec[k][s*n_g + g] for the 13 fields
+ * E_vac, a_vac, phase_slope, g_phase, cs_re, cs_im, cp_re, cp_im, L_esc,
+ * half_dL, apb, bma, q; good = 0 where the reference drops the pair.
+ * t_ang: segment start ages [Angstrom] (NULL = 0). */
+#define OR_COH_FIELDS 13
+void or_cxr_coherent_records(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
+                             const double *v_hat, const double *E_keV, const double *L_ang,
+                             const double *r_mid, const double *t_ang, const int64_t *elec_id,
+                             int64_t Ne, double *const rec[OR_COH_FIELDS], uint8_t *good);
+
 /* spec[e] += sum_j w_j sinc^2(a_j (E_e - E_j)/pi) (cxr/_cpu_reduce.py:26-50) */
 void or_reduce_node(int64_t n_lines, const double *E_res, const double *a_width,
                     const double *weight, int64_t n_e, const double *E_grid, double *spec,

@@ -323,6 +323,162 @@ void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
     }
 }
 
+/* cxr/_formation.py:58-81 (formation_coefficients) */
+static void formation_coefficients(double tau_start, double tau_end, double *apb, double *bma, double *q) {
+    const double qq = 0.25 * (tau_end - tau_start);
+    if (fabs(qq) < 0.5) { /* FORMATION_SMALL_Q */
+        const double c0 = exp(-0.25 * (tau_start + tau_end));
+        *apb = 2.0 * c0 * cosh(qq);
+        *bma = -2.0 * c0 * sinh(qq);
+    } else {
+        const double a = exp(-0.5 * tau_start), b = exp(-0.5 * tau_end);
+        *apb = a + b;
+        *bma = b - a;
+    }
+    *q = qq;
+}
+
+void or_cxr_coherent_records(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
+                             const double *v_hat, const double *E_keV, const double *L_ang,
+                             const double *r_mid, const double *t_ang, const int64_t *elec_id,
+                             int64_t Ne, double *const rec[OR_COH_FIELDS], uint8_t *good_out) {
+    const double nx = geo->n_hat[0], ny = geo->n_hat[1], nz = geo->n_hat[2];
+    const double T = geo->thickness;
+    const double h = HBARC_EV_ANG / M_E_EV;                    /* cxr/_recoil.py:27-32 */
+    const double pref_c1 = 4.0 * (M_PI * M_PI) * HBARC_EV_ANG; /* cxr/_kernels.py:325 */
+    const double mec2_kev = M_E_EV / 1e3;
+    for (int64_t s = 0; s < n_seg; ++s) {
+        const double E = E_keV[s];
+        const double vhx = v_hat[3 * s], vhy = v_hat[3 * s + 1], vhz = v_hat[3 * s + 2];
+        const double beta = or_beta_from_keV(E);
+        const double vx = beta * vhx, vy = beta * vhy, vz = beta * vhz;
+        /* cxr/_kernels.py:678-699 (_vacuum_doppler) */
+        const double gamma = 1.0 + E / mec2_kev;
+        const double one_minus_beta = 1.0 / (gamma * gamma * (1.0 + beta));
+        const double dvx = vhx - nx, dvy = vhy - ny, dvz = vhz - nz;
+        const double omc = 0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
+        const double denom_row = one_minus_beta + beta * omc;
+        /* coherent rows keep their own length and unit piece fraction (cxr/_setup.py:1001-1005) */
+        const double t_L = L_ang[s] / beta;
+        /* escape distance at the piece ends, ordered along travel (cxr/_formation.py:168-200) */
+        const double half = 0.5 * L_ang[s];
+        const double z_mid = r_mid[3 * s + 2];
+        const double L_start = slab_path(z_mid - half * vhz, T, nz);
+        const double L_end = slab_path(z_mid + half * vhz, T, nz);
+        double gx = -0.0 / nz, gy = -0.0 / nz, gz = -1.0 / nz;
+        if (z_mid < 0.0 || z_mid > T) { gx = 0.0; gy = 0.0; gz = 0.0; }
+        const double grad2 = gx * gx + gy * gy + gz * gz;
+        const double v_dot_grad = vx * gx + vy * gy + vz * gz;
+        const int cxr_electron = elec_id[s] < Ne;
+        const double inv_E = HBARC_EV_ANG / (gamma * M_E_EV);
+        /* cxr/_setup.py:1023-1026: midpoint age and retardation d = t_mid - n.r */
+        const double t_mid = (t_ang ? t_ang[s] : 0.0) + 0.5 * t_L;
+        const double rx = r_mid[3 * s], ry = r_mid[3 * s + 1], rz = r_mid[3 * s + 2];
+        const double d_geom = t_mid - (rx * nx + ry * ny + rz * nz);
+        for (int g = 0; g < t->n_g; ++g) {
+            const int64_t o = s * t->n_g + g;
+            const double Gx = t->G[3 * g], Gy = t->G[3 * g + 1], Gz = t->G[3 * g + 2];
+            const double g2 = Gx * Gx + Gy * Gy + Gz * Gz;
+            const double n_dot_g = Gx * nx + Gy * ny + Gz * nz;
+            const double r_num = 0.5 * g2 * inv_E;
+            const double r_den = n_dot_g * inv_E;
+            const double v_dot_g_exact = (vx * Gx + vy * Gy + vz * Gz) - r_num;
+            const double denom_vac = denom_row + r_den;
+            double denom = denom_vac, previous = denom, delta = NAN;
+            for (int pass = 0; pass < 3; ++pass) {  /* cxr/_kernels.py:702-765 */
+                double Er = HBARC_EV_ANG * (v_dot_g_exact / denom);
+                int ix, bl, ab;
+                double fr;
+                interp_index(Er, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+                delta = gather1(t->delta, t->n_tab, ix, fr, bl, ab);
+                previous = denom;
+                denom = denom_vac - delta * v_dot_grad;
+            }
+            int settled = fabs(denom - previous) <= RESONANCE_ROOT_RTOL * fabs(denom);
+            settled = settled && (2.0 * fabs(delta) * grad2 < 1.0);
+            if (!settled) denom = NAN;
+            const double n_dot_g_blk = n_dot_g + delta * (gx * Gx + gy * Gy + gz * Gz);
+            const double v_dot_g = vx * Gx + vy * Gy + vz * Gz;
+            const double omega = (v_dot_g - r_num) / denom;
+            const double k_dot_v = omega * ((1.0 - denom) + r_den);
+            const double k_dot_g = omega * n_dot_g_blk;
+            const double detuning = g2 + 2.0 * k_dot_g;
+            const double k_mag =
+                omega * sqrt(grad2 == 0.0 ? 1.0 : 1.0 - 2.0 * delta + delta * delta * grad2);
+            const double E_res = HBARC_EV_ANG * omega;
+            int keep = cxr_electron && (E_res > t->lo_keep) && (E_res > 10.0) && (E_res < t->hi_keep);
+            int ix, bl, ab;
+            double fr;
+            interp_index(E_res, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+            const double lfr = log_interp_fraction(E_res, t->E_tab, ix);
+            keep = keep && (denom > 0) && (omega * inv_E <= 1.0 - 1.0 / gamma);
+            const int row = t->row_table[g];
+            const double chi_re = gather1(t->chi_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+            const double chi_im = gather1(t->chi_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+            const double u_re = gather1(t->u_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+            const double u_im = gather1(t->u_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+            double mu = 0.0;
+            for (int el = 0; el < t->n_mu; ++el) {
+                const double *lm = t->log_mu + (int64_t)el * t->n_tab;
+                double f0 = lm[ix - 1];
+                double v = exp(f0 + lfr * (lm[ix] - f0));
+                if (bl) v = exp(lm[0]);
+                if (ab) v = exp(lm[t->n_tab - 1]);
+                mu += v;
+            }
+            /* complex PXR + CBS amplitude per polarization (cxr/_batched.py:600-625) */
+            double A_re[2], A_im[2];
+            for (int pol = 0; pol < 2; ++pol) {
+                const double *Ev = pol == 0 ? t->ES + 3 * g : t->EP + 3 * g;
+                const double ex = Ev[0], ey = Ev[1], ez = Ev[2];
+                const double g_dot_e = Gx * ex + Gy * ey + Gz * ez;
+                const double v_dot_e = vx * ex + vy * ey + vz * ez;
+                const double k_dot_e = omega * delta * (gx * ex + gy * ey + gz * ez);
+                double pxr_num, f_cbs;
+                or_quantum_line_factors(h, gamma, v_dot_g, k_dot_v, k_dot_g, g2, k_mag * k_mag,
+                                        v_dot_e, g_dot_e, k_dot_e, &pxr_num, &f_cbs);
+                const double f_pxr = pxr_num / detuning;
+                A_re[pol] = chi_re * f_pxr + u_re * f_cbs;
+                A_im[pol] = chi_im * f_pxr + u_im * f_cbs;
+            }
+            /* formation factor constants of the piece (cxr/_batched.py:627-633) */
+            double apb, bma, q;
+            formation_coefficients(L_start * mu, L_end * mu, &apb, &bma, &q);
+            /* exact vacuum centre / width and recoil phase over the age (cxr/_recoil.py:118-147),
+             * with the vacuum denominator and n.g of the batched tables */
+            const double numerator = v_dot_g - r_num;
+            const double den = denom_row + r_den;
+            const double E_c = HBARC_EV_ANG * numerator / den;
+            const double x = numerator / den * inv_E;
+            const double kappa = 1.0 / (1.0 - x);
+            const double a_vac = kappa * den * t_L / (2.0 * HBARC_EV_ANG);
+            const double d_shift = kappa * (x * denom_row + r_den) * t_mid;
+            const double g_shift = kappa * (x * v_dot_g - r_num) * t_mid;
+            const double amp = sqrt(ALPHA_FS * omega / pref_c1);
+            int good = keep && isfinite(amp) && (amp > 0) && (t_L > 0) && isfinite(apb) && (apb > 0) &&
+                       isfinite(bma);
+            const double cs_re = amp * t_L * A_re[0], cs_im = amp * t_L * A_im[0];
+            const double cp_re = amp * t_L * A_re[1], cp_im = amp * t_L * A_im[1];
+            good = good && isfinite(cs_re) && isfinite(cs_im) && isfinite(cp_re) && isfinite(cp_im);
+            /* record fields (cxr/_batched.py:646-660) */
+            rec[0][o] = E_c;
+            rec[1][o] = a_vac;
+            rec[2][o] = (d_geom + d_shift) / HBARC_EV_ANG;
+            rec[3][o] = rx * Gx + ry * Gy + rz * Gz + g_shift;
+            rec[4][o] = cs_re;
+            rec[5][o] = cs_im;
+            rec[6][o] = cp_re;
+            rec[7][o] = cp_im;
+            rec[8][o] = 0.5 * (L_start + L_end);
+            rec[9][o] = 0.5 * (L_end - L_start);
+            rec[10][o] = apb;
+            rec[11][o] = bma;
+            rec[12][o] = q;
+            good_out[o] = (uint8_t)good;
+        }
+    }
+}
+
 /* ---- line reductions ---------------------------------------------------- */
 
 void or_reduce_node(int64_t n_lines, const double *E_res, const double *a_width,

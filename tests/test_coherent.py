@@ -50,6 +50,49 @@ def test_oracle_matches_reference_coherent_spectrum(name):
     assert np.max(np.abs(got - spec)) <= 1e-12 * np.max(spec)
 
 
+COHERENT_ELECTRONS = {"hopg20": 8, "si50": 6}
+
+
+def _oracle_records(name):
+    """The oracle's coherent records from the fixture's segments and tables."""
+    import oracle
+
+    c = np.load(GOLDEN / f"cxr_{name}.npz")
+    tr = np.load(GOLDEN / f"transport_{c['transport']}.npz")
+    n_elec = COHERENT_ELECTRONS[name]
+    sel = tr["elec_id"] < n_elec
+    seg = dict(v_hat=tr["v_hat"][sel], E_keV=tr["E_repr_keV"][sel], L_ang=tr["L_ang"][sel],
+               r_mid=tr["r_mid"][sel], elec_id=tr["elec_id"][sel], t_ang=tr["t_ang"][sel])
+    t = {k: c[k] for k in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re", "u_im",
+                           "log_mu", "delta")}
+    pad = 0.2 * (c["E_grid"][-1] - c["E_grid"][0])
+    t["lo_keep"], t["hi_keep"] = c["E_grid"][0] - pad, c["E_grid"][-1] + pad
+    pairs, good = oracle.cxr_coherent_records(t, c["n_hat"], c["thickness"], seg, n_elec)
+    return oc.rows_from_pairs(pairs, good, c["G"].shape[0])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_coherent_records_match_reference(name):
+    """Segments + line tables -> the reference's per-row line records: the same
+    pairs kept, in the same order, every field to 1e-10."""
+    rec, cnt = _oracle_records(name)
+    z = np.load(GOLDEN / f"coherent_{name}.npz")
+    assert np.array_equal(cnt, z["row_count"])
+    for f in oc.FIELDS:
+        np.testing.assert_allclose(rec[f], z[f], rtol=1e-10, atol=0, err_msg=f)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_coherent_route_end_to_end(name):
+    """Segments -> records -> spectrum, all in the oracle, against the
+    reference's coherent spectrum. Phases of 1e8 rad carry 1e-8 rad of FP64
+    rounding from the record differences, hence 1e-8 of the peak."""
+    rec, cnt = _oracle_records(name)
+    _, _, w, E, dom, Ne, spec = _golden(name)
+    got = oc.coherent_spectrum(rec, cnt, w, E, dom, Ne)
+    assert np.max(np.abs(got - spec)) <= 1e-8 * np.max(spec)
+
+
 def test_golden_records_exercise_the_hard_cases():
     """Phases near 1e8 rad, formation arguments far from resonance, heavy
     absorption (apb underflowing FP32) and several rows with weights."""
