@@ -78,6 +78,53 @@ def coherent_spectrum(rec, row_count, row_weight, E, delta_omega, Ne=1):
     return spec / Ne
 
 
+def decoherence_factor(A_pop, xy0_pop, g_vec, omega):
+    """Row factor F(E) = |<exp(i (omega A_e - g_perp . xy0_e))>_e|^2 over the
+    sampled population, A_e = t0_e - n_perp . xy0_e (``cxr/_per_hkl.py:121-160``,
+    ``cxr/_setup.py:745-760``)."""
+    A_pop = np.asarray(A_pop, dtype=np.float64)
+    B = np.asarray(xy0_pop, dtype=np.float64) @ np.asarray(g_vec, dtype=np.float64)[:2]
+    chi = np.exp(1j * (np.asarray(omega)[None, :] * A_pop[:, None] - B[:, None])).sum(axis=0) / A_pop.size
+    return chi.real ** 2 + chi.imag ** 2
+
+
+def grouped_row(rec, lo, hi, elec_id, E, delta_omega):
+    """sum_e (|F_sigma,e|^2 + |F_pi,e|^2): each electron's lines of the row
+    summed as a field, squared, then summed over electrons
+    (``cxr/_per_hkl.py:457-500``)."""
+    total = np.zeros(E.size)
+    eid = np.asarray(elec_id[lo:hi])
+    for e in np.unique(eid):
+        idx = lo + np.flatnonzero(eid == e)
+        sub = {k: rec[k][idx] for k in FIELDS}
+        f_s, f_p = row_field(sub, 0, idx.size, E, delta_omega)
+        total += np.abs(f_s) ** 2 + np.abs(f_p) ** 2
+    return total
+
+
+def coherent_spectrum_decoherent(rec, elec_id, row_count, row_weight, G, A_pop, xy0_pop, E, delta_omega, omega,
+                                 Ne):
+    """The sampled-bunch blend per row, (1 - F) grouped + F flat, weighted and
+    summed over rows, divided by ``Ne`` (``cxr/_batched_finalize.py:163-243``,
+    ``spectrum/coherent_population.py:83-96`` without a physical population).
+    Records are offset-free (``cxr/_setup.py:637-642``)."""
+    E = np.asarray(E, dtype=np.float64)
+    delta_omega = np.asarray(delta_omega, dtype=np.float64)
+    rec = {k: np.asarray(rec[k], dtype=np.float64) for k in FIELDS}
+    spec = np.zeros(E.size)
+    off = np.concatenate([[0], np.cumsum(np.asarray(row_count, dtype=np.int64))])
+    for r in range(len(row_count)):
+        lo, hi = int(off[r]), int(off[r + 1])
+        if hi == lo:
+            continue
+        F = decoherence_factor(A_pop, xy0_pop, G[r], omega)
+        f_s, f_p = row_field(rec, lo, hi, E, delta_omega)
+        flat = np.abs(f_s) ** 2 + np.abs(f_p) ** 2
+        grouped = grouped_row(rec, lo, hi, elec_id, E, delta_omega)
+        spec += ((1.0 - F) * grouped + F * flat) * float(row_weight[r])
+    return spec / Ne
+
+
 def rows_from_pairs(pairs, good, n_g):
     """Per-row record layout of the reference's block loop (cxr/_batched.py:640-660
     flattens g-major and keeps ``good``): row r holds its good pairs in

@@ -846,6 +846,109 @@ def gen_coherent():
         )
 
 
+def gen_coherent_decoherence():
+    """Coherent route with sampled beam offsets on the infinite slab: the
+    inter-electron decoherence blend of cxr/_batched_finalize.py:163-243.
+
+    The first 8 electrons of the HOPG 20 MeV case get their transport entry
+    points as face offsets (``initial_r_ang``) and seeded arrival offsets
+    (``initial_t0_ang``, 0.3 Angstrom RMS of c t), so the route builds
+    offset-free records (cxr/_setup.py:637-642), a per-row factor
+    F = |<exp(i(omega A_e - g.xy0_e))>|^2 (cxr/_per_hkl.py:121-160), the
+    per-electron sum of squared fields (cxr/_per_hkl.py:457-500) and the blend
+    (1 - F) grouped + F flat (spectrum/coherent_population.py:83-96). Saves the
+    records with their electron ids, the population offsets, each row's
+    reciprocal vector, F and grouped term, and the spectrum.
+    """
+    from pyrite.materials.crystal import CRYSTALS, reciprocal_g_vector
+    from pyrite.montecarlo.spectrum.cxr import _batched, _batched_finalize, _setup
+    from pyrite.montecarlo.spectrum.cxr._spectrum import mc_cxr_spectrum
+
+    name, n_elec = "hopg20", 8
+    case = CXR_CASES[name]
+    tr = np.load(OUT / f"transport_{case['transport']}.npz")
+    sel = tr["elec_id"] < n_elec
+    seg = {k: tr[k][sel] for k in ("r_mid", "v_hat", "L_ang", "E_keV", "E_repr_keV", "elec_id", "t_ang")}
+    rng = np.random.default_rng(17)
+    r0 = np.array(tr["initial_r"][:n_elec], dtype=float)
+    t0 = rng.normal(0.0, 0.3, n_elec)
+    seg.update(Ne=n_elec, thickness_ang=float(tr["z_bot"][-1]), initial_r_ang=r0, initial_t0_ang=t0)
+    info = CRYSTALS[case["crystal"]]
+    hkl = case["hkl"]
+    g_mags = np.array([reciprocal_g_vector(h, info["lattice"])[1] for h in hkl])
+    E_grid = case["E_grid"]
+    E_tab = synthetic_E_tab(E_grid)
+    tables = synthetic_couplings(g_mags, E_tab)
+    cap = {"F": {}, "grouped": []}
+    orig_fin = _batched._batched_coherent_finalize
+    orig_F = _batched_finalize._row_decoherence_factor
+    orig_grp = _batched_finalize._coherent_electron_grouped_row
+
+    def capture(st, bt, coh_blocks, coh_counts, *a, _orig=orig_fin, **k):
+        cap.update(st=st, bt=bt, blocks=[[np.array(f) for f in b] for b in coh_blocks],
+                   counts=[np.array(c) for c in coh_counts])
+        return _orig(st, bt, coh_blocks, coh_counts, *a, **k)
+
+    def capture_F(st, g_vec, _orig=orig_F):
+        out = _orig(st, g_vec)
+        cap["F"][tuple(np.asarray(g_vec, dtype=float))] = np.array(out)
+        return out
+
+    def capture_grp(*a, _orig=orig_grp, **k):
+        out = _orig(*a, **k)
+        cap["grouped"].append(np.array(out))
+        return out
+
+    patches = [
+        (_setup, "_line_tabulation_grid", lambda *a, **k: E_tab),
+        (_setup, "_elemental_log_mu_table", lambda c, E: synthetic_log_mu(c, E)),
+        (_setup, "refractive_index", lambda cr, E, uh=True: (1.0 - synthetic_delta(E)) + 0j),
+        (_batched, "_reflection_tables", lambda *a, **k: tuple(np.array(t) for t in tables)),
+        (_batched, "_batched_coherent_finalize", capture),
+        (_batched_finalize, "_row_decoherence_factor", capture_F),
+        (_batched_finalize, "_coherent_electron_grouped_row", capture_grp),
+    ]
+    saved = [(m, n, getattr(m, n)) for m, n, _ in patches]
+    for m, n, f in patches:
+        setattr(m, n, f)
+    try:
+        spec = np.asarray(mc_cxr_spectrum(
+            seg, E_grid, crystal=case["crystal"], hkl_list=[tuple(h) for h in hkl],
+            B_ang2=float(info.get("B_ang2", 0.0) or 0.0), absorber_element=case["absorber"],
+            n_hat=tr["n_hat"], surface_hkl=case["surface_hkl"],
+            mosaic_fwhm_rad=np.deg2rad(case["mosaic_fwhm_deg"]), mosaic_nodes=case["mosaic_nodes"],
+            node_support_cutoff=None, coherent=True))
+    finally:
+        for m, n, f in saved:
+            setattr(m, n, f)
+    st, bt = cap["st"], cap["bt"]
+    if not st.decoherence_active or st.analytic_offsets:
+        raise RuntimeError("decoherence fixture expects the sampled (empirical) blend")
+    counts = np.stack(cap["counts"])
+    starts = np.concatenate([np.zeros((counts.shape[0], 1), counts.dtype), np.cumsum(counts, axis=1)], axis=1)
+    rows = {f: [] for f in COHERENT_FIELDS}
+    for i_row in range(int(bt.N_g)):
+        for b, flat in enumerate(cap["blocks"]):
+            for f, arr in zip(COHERENT_FIELDS, flat, strict=True):
+                rows[f].append(arr[int(starts[b, i_row]):int(starts[b, i_row + 1])])
+    row_count = counts.sum(axis=0).astype(np.int64)
+    G = np.asarray(bt.G, dtype=float)
+    active = np.flatnonzero(row_count > 0)
+    F_rows = np.stack([cap["F"][tuple(G[r])] for r in active])
+    if len(cap["grouped"]) != active.size:
+        raise RuntimeError("expected one grouped term per row with lines")
+    _save(
+        "coherent_decoherence_hopg20",
+        transport=case["transport"], n_elec=n_elec, Ne=n_elec, E_grid=np.asarray(st.E_grid),
+        delta_omega=np.asarray(st.delta_omega_grid), omega=np.asarray(st.omega_grid),
+        row_weight=np.asarray(bt.wm_rows, dtype=float).reshape(-1), row_count=row_count, G=G,
+        n_hat=np.asarray(tr["n_hat"], dtype=float), initial_r_ang=r0, initial_t0_ang=t0,
+        A_pop=np.asarray(st.decoherence_A_pop), xy0_pop=np.asarray(st.xy0_pop),
+        active_rows=active, F_rows=F_rows, grouped_rows=np.stack(cap["grouped"]), spec=spec,
+        **{f: np.concatenate(rows[f]) for f in COHERENT_FIELDS},
+    )
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
@@ -857,6 +960,7 @@ GENERATORS = {
     "char": gen_char,
     "layered": gen_layered,
     "coherent": gen_coherent,
+    "coherent_decoherence": gen_coherent_decoherence,
 }
 
 

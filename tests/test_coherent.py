@@ -93,6 +93,52 @@ def test_oracle_coherent_route_end_to_end(name):
     assert np.max(np.abs(got - spec)) <= 1e-8 * np.max(spec)
 
 
+def test_oracle_decoherence_blend_matches_reference():
+    """Sampled beam offsets on the infinite slab: the row factor F, each
+    row's per-electron sum of squared fields and the blended spectrum."""
+    z = np.load(GOLDEN / "coherent_decoherence_hopg20.npz")
+    rec = {k: z[k] for k in oc.FIELDS}
+    cnt, w, G, E, dom = z["row_count"], z["row_weight"], z["G"], z["E_grid"], z["delta_omega"]
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    assert 0.0 < z["F_rows"].min() < 1e-3 and z["F_rows"].max() > 0.5  # a real blend
+    for i, r in enumerate(z["active_rows"]):
+        F = oc.decoherence_factor(z["A_pop"], z["xy0_pop"], G[r], z["omega"])
+        np.testing.assert_allclose(F, z["F_rows"][i], rtol=1e-12, atol=1e-15)
+        if i % 8 == 0:
+            g = oc.grouped_row(rec, off[r], off[r + 1], z["elec_id"], E, dom)
+            assert np.max(np.abs(g - z["grouped_rows"][i])) <= 1e-12 * np.max(z["grouped_rows"][i])
+    spec = oc.coherent_spectrum_decoherent(rec, z["elec_id"], cnt, w, G, z["A_pop"], z["xy0_pop"], E, dom,
+                                           z["omega"], int(z["Ne"]))
+    assert np.max(np.abs(spec - z["spec"])) <= 1e-12 * np.max(z["spec"])
+
+
+def test_oracle_offset_free_records_match_reference():
+    """With each electron's face offset removed from the midpoints
+    (cxr/_setup.py:637-642) the record prologue gives the reference's
+    offset-free records."""
+    import oracle
+
+    z = np.load(GOLDEN / "coherent_decoherence_hopg20.npz")
+    c = np.load(GOLDEN / "cxr_hopg20.npz")
+    tr = np.load(GOLDEN / f"transport_{c['transport']}.npz")
+    n = int(z["n_elec"])
+    sel = tr["elec_id"] < n
+    eid = tr["elec_id"][sel]
+    r_geom = tr["r_mid"][sel].copy()
+    r_geom[:, :2] -= z["xy0_pop"][np.clip(eid, 0, n - 1)]
+    seg = dict(v_hat=tr["v_hat"][sel], E_keV=tr["E_repr_keV"][sel], L_ang=tr["L_ang"][sel], r_mid=r_geom,
+               elec_id=eid, t_ang=tr["t_ang"][sel])
+    t = {k: c[k] for k in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re", "u_im",
+                           "log_mu", "delta")}
+    pad = 0.2 * (c["E_grid"][-1] - c["E_grid"][0])
+    t["lo_keep"], t["hi_keep"] = c["E_grid"][0] - pad, c["E_grid"][-1] + pad
+    pairs, good = oracle.cxr_coherent_records(t, c["n_hat"], c["thickness"], seg, n)
+    rec, cnt = oc.rows_from_pairs(pairs, good, c["G"].shape[0])
+    assert np.array_equal(cnt, z["row_count"])
+    for f in oc.FIELDS:
+        np.testing.assert_allclose(rec[f], z[f], rtol=1e-10, atol=0, err_msg=f)
+
+
 def test_golden_records_exercise_the_hard_cases():
     """Phases near 1e8 rad, formation arguments far from resonance, heavy
     absorption (apb underflowing FP32) and several rows with weights."""
