@@ -49,6 +49,23 @@ MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_t
     if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
 
 
+def spectrum_error_stats(got, ref):
+    """Max and RMS error of per-tile spectra ``got`` against ``ref`` (both
+    [tiles][bins]), each tile relative to its own peak, and of the
+    tile-summed detector spectrum relative to its peak."""
+    got = np.asarray(got, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    peak = np.max(np.abs(ref), axis=1)
+    peak = np.where(peak > 0, peak, np.inf)
+    d = got - ref
+    tot_ref, tot_d = ref.sum(0), d.sum(0)
+    tot_peak = float(np.max(np.abs(tot_ref))) or float("inf")
+    return {"max_over_tiles": float(np.max(np.max(np.abs(d), axis=1) / peak)),
+            "rms_over_tiles": float(np.max(np.sqrt(np.mean(d * d, axis=1)) / peak)),
+            "detector_total_max": float(np.max(np.abs(tot_d)) / tot_peak),
+            "detector_total_rms": float(np.sqrt(np.mean(tot_d * tot_d)) / tot_peak)}
+
+
 def workload_config(args, n_dir, n_g, n_bins):
     return {
         "workload": "50 MeV e- on 500 um Si (220) at 10 deg; 238 reflections |g|<8/A; "
@@ -566,6 +583,7 @@ def main():
                "coarse_bins": int(model.n_out),
                "spectrum_error": {"reference": "exact mixed-precision scorer on the same histories, coarse bins",
                                   "max_over_tiles_rel_to_tile_peak": e_tile, "detector_total_rel_to_peak": e_tot,
+                                  "max_and_rms": spectrum_error_stats(hyb, exact_c),
                                   "surrogate_alone": dict(zip(("max_over_tiles", "detector_total"), errs(pure)))},
                "gate": 0.01, "passed": bool(e_tile <= 0.01)}
         if args.train_domain == "uniform":
@@ -654,6 +672,7 @@ def main():
         line["mixed_exact"]["spectrum_error_vs_fp64"] = {
             "note": "different history batches (statistical): tile-summed exact CXR spectra, mixed vs FP64",
             "max_rel_to_peak": float(np.max(np.abs(a.sum(0) - b.sum(0))) / peak) if peak > 0 else None,
+            "rms_rel_to_peak": float(np.sqrt(np.mean((a.sum(0) - b.sum(0)) ** 2)) / peak) if peak > 0 else None,
         }
     # e2e through the public API with host buffers.
     line["e2e"] = e2e_measure(spec, args, torch, rank, world, dist,
