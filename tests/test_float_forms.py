@@ -102,3 +102,34 @@ def test_escape_forms():
                 scale = max(ref, 1e-30)
                 worst = max(worst, abs(got - ref) / scale)
     assert worst < 1e-4, worst
+
+
+def test_float32_doppler_factor_at_tens_of_mev():
+    """The mixed CXR scorer's FP32 Doppler factor (pb_cxr.cu seg_precompute:
+    gamma = 1 + E/mc^2, 1 - beta v.n = 1/(gamma^2 (1 + beta)) + beta |v - n|^2/2)
+    within the reference's float32 bounds (4 ulp gamma, 16 ulp denominator;
+    tests/montecarlo/spectrum/test_line_kinematics_precision.py:56-66) at
+    30 and 100 MeV, forward (1 mrad, 1/gamma scale) and backward; beta
+    carries up to 3 ulp of the rsqrt-based square root."""
+    f32 = np.float32
+    eps = float(np.finfo(f32).eps)
+    angles = np.array([1e-3, 5e-3, 0.3, 2.0])
+    for E in (3.0e4, 1.0e5):
+        gamma_ref = 1.0 + E / MC2
+        omb_ref = 1.0 / (gamma_ref * gamma_ref * (1.0 + np.sqrt(1.0 - 1.0 / gamma_ref ** 2)))
+        denom_ref = omb_ref + (1.0 - omb_ref) * 2.0 * np.sin(angles / 2.0) ** 2
+        Ef = f32(E)
+        g0 = f32(1) + Ef / f32(510.99895)
+        beta0 = np.sqrt(f32(1) - f32(1) / (g0 * g0)).astype(f32)
+        gamma = f32(1) + Ef / f32(MC2)
+        assert abs(float(gamma) / gamma_ref - 1.0) < 4 * eps
+        vh = np.array([0.0, 0.0, 1.0], dtype=f32)
+        for k in range(-3, 4):
+            beta = f32(beta0 + f32(k) * np.spacing(beta0))
+            omb = f32(1) / (gamma * gamma * (f32(1) + beta))
+            for a, ref in zip(angles, denom_ref):
+                n = np.array([np.sin(a), 0.0, np.cos(a)], dtype=f32)
+                d = vh - n
+                omc = f32(0.5) * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+                denom = omb + beta * omc
+                assert abs(float(denom) / ref - 1.0) < 16 * eps, (E, a, k)
