@@ -139,6 +139,46 @@ def test_oracle_offset_free_records_match_reference():
         np.testing.assert_allclose(rec[f], z[f], rtol=1e-10, atol=0, err_msg=f)
 
 
+@pytest.mark.parametrize("pieces", [2, 4])
+def test_oracle_coherent_sum_is_invariant_under_segment_splitting(pieces):
+    """A straight segment and its collinear pieces (own midpoints, lengths and
+    start ages advanced by the flight time) radiate the same coherent field
+    (cxr/_formation.py:26-36; the reference's segment-escape split
+    invariance, tests/montecarlo/spectrum/test_segment_escape.py:75-86, in its
+    coherent form). Pieces buried under optical depths that underflow drop out
+    with no effect on the spectrum."""
+    import oracle
+
+    c = np.load(GOLDEN / "cxr_hopg20.npz")
+    z = np.load(GOLDEN / "coherent_hopg20.npz")
+    tr = np.load(GOLDEN / f"transport_{c['transport']}.npz")
+    sel = tr["elec_id"] < 1
+    seg = dict(v_hat=tr["v_hat"][sel], E_keV=tr["E_repr_keV"][sel], L_ang=tr["L_ang"][sel],
+               r_mid=tr["r_mid"][sel], elec_id=tr["elec_id"][sel], t_ang=tr["t_ang"][sel])
+    t = {k: c[k] for k in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re", "u_im",
+                           "log_mu", "delta")}
+    pad = 0.2 * (c["E_grid"][-1] - c["E_grid"][0])
+    t["lo_keep"], t["hi_keep"] = c["E_grid"][0] - pad, c["E_grid"][-1] + pad
+
+    def spectrum(sg):
+        pairs, good = oracle.cxr_coherent_records(t, c["n_hat"], c["thickness"], sg, 1)
+        rec, cnt = oc.rows_from_pairs(pairs, good, c["G"].shape[0])
+        return oc.coherent_spectrum(rec, cnt, z["row_weight"], z["E_grid"], z["delta_omega"], 1)
+
+    n = seg["L_ang"].size
+    frac = (np.arange(pieces) + 0.5) / pieces - 0.5
+    L = np.repeat(seg["L_ang"], pieces) / pieces
+    E = np.repeat(seg["E_keV"], pieces)
+    gam = 1.0 + E / 510.99895
+    beta = np.sqrt(1.0 - 1.0 / (gam * gam))
+    v = np.repeat(seg["v_hat"], pieces, axis=0)
+    split = dict(v_hat=v, E_keV=E, L_ang=L, elec_id=np.repeat(seg["elec_id"], pieces),
+                 r_mid=np.repeat(seg["r_mid"], pieces, axis=0) + (np.tile(frac, n) * np.repeat(seg["L_ang"], pieces))[:, None] * v,
+                 t_ang=np.repeat(seg["t_ang"], pieces) + np.tile(np.arange(pieces), n) * L / beta)
+    whole = spectrum(seg)
+    assert np.max(np.abs(spectrum(split) - whole)) <= 1e-8 * np.max(whole)
+
+
 def test_golden_records_exercise_the_hard_cases():
     """Phases near 1e8 rad, formation arguments far from resonance, heavy
     absorption (apb underflowing FP32) and several rows with weights."""

@@ -62,3 +62,21 @@ def test_classical_limit_is_the_braced_form():
         pxr0 = (vdg + kv) * (g @ e + k @ e) - (k @ k) * ve
         cbs0 = -((g @ e - vdg * ve) + ve * (kg - kv * vdg) / vdg) / (gamma * vdg)
         np.testing.assert_allclose(_factors(0.0, gamma, v, g, k, e), [pxr0, cbs0], rtol=1e-12)
+
+
+def test_segment_mean_transmission_against_quadrature():
+    """Segment mean of exp(-tau) for tau linear along the segment, against
+    adaptive quadrature at the reference's own test points, including the
+    equal-depth and near-equal limits and a tau of 800
+    (tests/montecarlo/spectrum/test_segment_escape.py:54-72)."""
+    from scipy.integrate import quad
+
+    tau0 = [0.0, 0.3, 2.0, 5.0, 40.0, 1.0]
+    tau1 = [0.0, 0.3 + 1e-6, 0.5, 9.0, 800.0, 1.0 + 3e-5]
+    for a, b in zip(tau0, tau1):
+        ref = quad(lambda s: np.exp(-(a + (b - a) * s)), 0.0, 1.0, epsabs=0.0, epsrel=1e-13)[0]
+        got = oracle.mean_transmission(a, b)
+        assert abs(got - ref) <= 1e-9 * ref
+        assert oracle.mean_transmission(b, a) == got
+        assert got <= np.exp(-min(a, b))
+    assert oracle.mean_transmission(0.0, 0.0) == 1.0
