@@ -80,3 +80,19 @@ def test_segment_mean_transmission_against_quadrature():
         assert oracle.mean_transmission(b, a) == got
         assert got <= np.exp(-min(a, b))
     assert oracle.mean_transmission(0.0, 0.0) == 1.0
+
+
+def test_node_reducer_matches_the_dense_sinc_squared_contraction():
+    """spec += sum_j w_j sinc^2(a_j (E - E_j)) against the dense matrix form,
+    with an exact resonance on a node (the x = 0 guard) and empty input
+    leaving the spectrum unchanged (tests/montecarlo/transport/test_cxr_cpu_reduce.py)."""
+    rng = np.random.default_rng(7)
+    E_grid = np.linspace(1000.0, 20000.0, 97)
+    E_r = rng.uniform(900.0, 20100.0, 513)
+    E_r[0] = E_grid[11]
+    a = rng.uniform(1.0e-3, 0.5, E_r.size)
+    w = rng.random(E_r.size)
+    x = a[:, None] * (E_grid[None, :] - E_r[:, None])
+    S = np.where(x == 0.0, 1.0, np.sin(np.where(x == 0.0, 1.0, x)) / np.where(x == 0.0, 1.0, x)) ** 2
+    np.testing.assert_allclose(oracle.reduce_node(E_r, a, w, E_grid), w @ S, rtol=1e-12, atol=0.0)
+    assert np.array_equal(oracle.reduce_node(np.empty(0), np.empty(0), np.empty(0), E_grid), np.zeros(E_grid.size))
