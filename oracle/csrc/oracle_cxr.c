@@ -172,150 +172,187 @@ static double exact_mu(const or_layer_escape *ly, int k, double E) {
     return mu;
 }
 
+/* Per-segment quantities every row shares (cxr/_setup.py:945-1005). */
+typedef struct {
+    double vhz, beta, vx, vy, vz, gamma, denom_row, inv_E;
+    double gx, gy, gz, grad2, v_dot_grad;
+    int cxr_electron;
+} seg_state;
+
+static void seg_setup(const double *n_hat, double thickness, double E, const double *vh, double z_mid,
+                      int cxr_electron, seg_state *q) {
+    const double mec2_kev = M_E_EV / 1e3;
+    q->vhz = vh[2];
+    q->beta = or_beta_from_keV(E);
+    q->vx = q->beta * vh[0];
+    q->vy = q->beta * vh[1];
+    q->vz = q->beta * vh[2];
+    /* cxr/_kernels.py:678-699 (_vacuum_doppler) */
+    q->gamma = 1.0 + E / mec2_kev;
+    const double one_minus_beta = 1.0 / (q->gamma * q->gamma * (1.0 + q->beta));
+    const double dvx = vh[0] - n_hat[0], dvy = vh[1] - n_hat[1], dvz = vh[2] - n_hat[2];
+    const double omc = 0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
+    q->denom_row = one_minus_beta + q->beta * omc;
+    /* segment_escape.py:95-131: grad L = -z_hat / (z_hat . n), zero outside */
+    const double nz = n_hat[2];
+    q->gx = -0.0 / nz;
+    q->gy = -0.0 / nz;
+    q->gz = -1.0 / nz;
+    if (z_mid < 0.0 || z_mid > thickness) { q->gx = 0.0; q->gy = 0.0; q->gz = 0.0; }
+    q->grad2 = q->gx * q->gx + q->gy * q->gy + q->gz * q->gz;
+    q->v_dot_grad = q->vx * q->gx + q->vy * q->gy + q->vz * q->gz;
+    q->cxr_electron = cxr_electron;
+    q->inv_E = HBARC_EV_ANG / (q->gamma * M_E_EV); /* cxr/_recoil.py:19-24 */
+}
+
+/* One (segment, row) pair up to the complex amplitudes of both
+ * polarisations: cxr/_batched.py:461-559 and 600-625. */
+typedef struct {
+    double G[3], g2, n_dot_g, r_num, r_den, v_dot_g;
+    double omega, E_res, slope, mu;
+    double A_re[2], A_im[2];
+    int keep;
+} pair_state;
+
+static void pair_chain(const or_cxr_tables *t, const double *n_hat, const seg_state *q, int g, pair_state *p) {
+    const double h = HBARC_EV_ANG / M_E_EV; /* cxr/_recoil.py:27-32 */
+    const double Gx = t->G[3 * g], Gy = t->G[3 * g + 1], Gz = t->G[3 * g + 2];
+    const double vx = q->vx, vy = q->vy, vz = q->vz, gx = q->gx, gy = q->gy, gz = q->gz;
+    p->G[0] = Gx;
+    p->G[1] = Gy;
+    p->G[2] = Gz;
+    const double g2 = Gx * Gx + Gy * Gy + Gz * Gz;
+    const double n_dot_g = Gx * n_hat[0] + Gy * n_hat[1] + Gz * n_hat[2];
+    /* cxr/_block_prologue.py:18-38 + cxr/_recoil.py:79-97 */
+    const double r_num = 0.5 * g2 * q->inv_E;
+    const double r_den = n_dot_g * q->inv_E;
+    const double v_dot_g_exact = (vx * Gx + vy * Gy + vz * Gz) - r_num;
+    const double denom_vac = q->denom_row + r_den;
+    /* cxr/_kernels.py:702-765: three fixed-point Snell passes */
+    double denom = denom_vac, previous = denom, delta = NAN;
+    for (int pass = 0; pass < 3; ++pass) {
+        double Er = HBARC_EV_ANG * (v_dot_g_exact / denom);
+        int ix, bl, ab;
+        double fr;
+        interp_index(Er, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+        delta = gather1(t->delta, t->n_tab, ix, fr, bl, ab);
+        previous = denom;
+        denom = denom_vac - delta * q->v_dot_grad;
+    }
+    int settled = fabs(denom - previous) <= RESONANCE_ROOT_RTOL * fabs(denom);
+    settled = settled && (2.0 * fabs(delta) * q->grad2 < 1.0);
+    if (!settled) denom = NAN;
+    /* cxr/_block_prologue.py:41-50 */
+    const double n_dot_g_blk = n_dot_g + delta * (gx * Gx + gy * Gy + gz * Gz);
+    /* cxr/_kernels.py:624-655 (_cxr_kin_core) */
+    const double v_dot_g = vx * Gx + vy * Gy + vz * Gz;
+    const double omega = (v_dot_g - r_num) / denom;
+    const double k_dot_v = omega * ((1.0 - denom) + r_den);
+    const double k_dot_g = omega * n_dot_g_blk;
+    const double detuning = g2 + 2.0 * k_dot_g;
+    /* cxr/_batched.py:435-458 (_line_bracket) */
+    const double k_mag = omega * sqrt(q->grad2 == 0.0 ? 1.0 : 1.0 - 2.0 * delta + delta * delta * q->grad2);
+    const double E_res = HBARC_EV_ANG * omega;
+    int keep = q->cxr_electron && (E_res > t->lo_keep) && (E_res > 10.0) && (E_res < t->hi_keep);
+    int ix, bl, ab;
+    double fr;
+    interp_index(E_res, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
+    const double lfr = log_interp_fraction(E_res, t->E_tab, ix);
+    /* cxr/_block_prologue.py:53-62 + cxr/_recoil.py:100-118 */
+    p->slope = denom * (1.0 / (1.0 - omega * q->inv_E));
+    keep = keep && (denom > 0) && (omega * q->inv_E <= 1.0 - 1.0 / q->gamma);
+    /* cxr/_kernels.py:482-506,369-388: couplings and attenuation */
+    const int row = t->row_table[g];
+    const double chi_re = gather1(t->chi_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+    const double chi_im = gather1(t->chi_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+    const double u_re = gather1(t->u_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+    const double u_im = gather1(t->u_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
+    double mu = 0.0;
+    for (int el = 0; el < t->n_mu; ++el) {
+        const double *lm = t->log_mu + (int64_t)el * t->n_tab;
+        double f0 = lm[ix - 1];
+        double v = exp(f0 + lfr * (lm[ix] - f0));
+        if (bl) v = exp(lm[0]);
+        if (ab) v = exp(lm[t->n_tab - 1]);
+        mu += v;
+    }
+    /* cxr/_batched.py:789-826 + cxr/_line_amplitude.py:14-37: PXR + CBS per polarization */
+    for (int pol = 0; pol < 2; ++pol) {
+        const double *Ev = pol == 0 ? t->ES + 3 * g : t->EP + 3 * g;
+        const double ex = Ev[0], ey = Ev[1], ez = Ev[2];
+        const double g_dot_e = Gx * ex + Gy * ey + Gz * ez;
+        const double v_dot_e = vx * ex + vy * ey + vz * ez;
+        const double k_dot_e = omega * delta * (gx * ex + gy * ey + gz * ez);
+        double pxr_num, f_cbs;
+        or_quantum_line_factors(h, q->gamma, v_dot_g, k_dot_v, k_dot_g, g2, k_mag * k_mag, v_dot_e, g_dot_e,
+                                k_dot_e, &pxr_num, &f_cbs);
+        const double f_pxr = pxr_num / detuning;
+        p->A_re[pol] = chi_re * f_pxr + u_re * f_cbs;
+        p->A_im[pol] = chi_im * f_pxr + u_im * f_cbs;
+    }
+    p->g2 = g2;
+    p->n_dot_g = n_dot_g;
+    p->r_num = r_num;
+    p->r_den = r_den;
+    p->v_dot_g = v_dot_g;
+    p->omega = omega;
+    p->E_res = E_res;
+    p->mu = mu;
+    p->keep = keep;
+}
+
 void or_cxr_lines(const or_cxr_tables *t, const or_cxr_geom *geo, int64_t n_seg,
                   const double *v_hat, const double *E_keV, const double *L_ang,
                   const double *r_mid, const int64_t *elec_id, int64_t Ne, double *E_res_out,
                   double *a_width_out, double *weight_out, uint8_t *good_out, int n_threads) {
-    const double nx = geo->n_hat[0], ny = geo->n_hat[1], nz = geo->n_hat[2];
+    const double nz = geo->n_hat[2];
     const double T = geo->thickness;
-    const double h = HBARC_EV_ANG / M_E_EV;              /* cxr/_recoil.py:27-32 */
     const double pref_c1 = 4.0 * (M_PI * M_PI) * HBARC_EV_ANG; /* cxr/_kernels.py:325 */
-    const double mec2_kev = M_E_EV / 1e3;
 #pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads > 0 ? n_threads : 1)
     for (int64_t s = 0; s < n_seg; ++s) {
-        const double E = E_keV[s];
-        const double vhx = v_hat[3 * s], vhy = v_hat[3 * s + 1], vhz = v_hat[3 * s + 2];
-        /* cxr/_setup.py:945-1005 */
-        const double beta = or_beta_from_keV(E);
-        const double vx = beta * vhx, vy = beta * vhy, vz = beta * vhz;
-        /* cxr/_kernels.py:678-699 (_vacuum_doppler) */
-        const double gamma = 1.0 + E / mec2_kev;
-        const double one_minus_beta = 1.0 / (gamma * gamma * (1.0 + beta));
-        const double dvx = vhx - nx, dvy = vhy - ny, dvz = vhz - nz;
-        const double omc = 0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
-        const double denom_row = one_minus_beta + beta * omc;
-        const double t_L = L_ang[s] / beta;
+        seg_state q;
+        const double z_mid = r_mid[3 * s + 2];
+        seg_setup(geo->n_hat, T, E_keV[s], v_hat + 3 * s, z_mid, elec_id[s] < Ne, &q);
+        const double t_L = L_ang[s] / q.beta;
         /* segment_escape.py:239-270 (one linear piece on a single slab) */
         const double half = 0.5 * L_ang[s];
-        const double z_mid = r_mid[3 * s + 2];
-        const double path0 = slab_path(z_mid - half * vhz, T, nz);
-        const double path1 = slab_path(z_mid + half * vhz, T, nz);
+        const double path0 = slab_path(z_mid - half * q.vhz, T, nz);
+        const double path1 = slab_path(z_mid + half * q.vhz, T, nz);
         /* layered absorber: linear escape pieces (cxr/_setup.py:1089) */
         const or_layer_escape *ly = geo->layers;
         double pf[OR_MAX_LAYERS], pp0[OR_MAX_LAYERS * OR_MAX_LAYERS], pp1[OR_MAX_LAYERS * OR_MAX_LAYERS];
         int n_piece = 0;
-        if (ly) n_piece = or_layer_pieces(z_mid - half * vhz, z_mid + half * vhz, ly, nz, pf, pp0, pp1);
-        /* segment_escape.py:95-131: grad L = -z_hat / (z_hat . n), zero outside */
-        double gx = -0.0 / nz, gy = -0.0 / nz, gz = -1.0 / nz;
-        if (z_mid < 0.0 || z_mid > T) { gx = 0.0; gy = 0.0; gz = 0.0; }
-        const double grad2 = gx * gx + gy * gy + gz * gz;
-        const double v_dot_grad = vx * gx + vy * gy + vz * gz;
-        const int cxr_electron = elec_id[s] < Ne;
-        const double inv_E = HBARC_EV_ANG / (gamma * M_E_EV); /* cxr/_recoil.py:19-24 */
+        if (ly) n_piece = or_layer_pieces(z_mid - half * q.vhz, z_mid + half * q.vhz, ly, nz, pf, pp0, pp1);
         for (int g = 0; g < t->n_g; ++g) {
             const int64_t o = s * t->n_g + g;
-            const double Gx = t->G[3 * g], Gy = t->G[3 * g + 1], Gz = t->G[3 * g + 2];
-            const double g2 = Gx * Gx + Gy * Gy + Gz * Gz;
-            const double n_dot_g = Gx * nx + Gy * ny + Gz * nz;
-            /* cxr/_block_prologue.py:18-38 + cxr/_recoil.py:79-97 */
-            const double r_num = 0.5 * g2 * inv_E;
-            const double r_den = n_dot_g * inv_E;
-            const double v_dot_g_exact = (vx * Gx + vy * Gy + vz * Gz) - r_num;
-            const double denom_vac = denom_row + r_den;
-            /* cxr/_kernels.py:702-765: three fixed-point Snell passes */
-            double denom = denom_vac, previous = denom, delta = NAN;
-            for (int pass = 0; pass < 3; ++pass) {
-                double Er = HBARC_EV_ANG * (v_dot_g_exact / denom);
-                int ix, bl, ab;
-                double fr;
-                interp_index(Er, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
-                delta = gather1(t->delta, t->n_tab, ix, fr, bl, ab);
-                previous = denom;
-                denom = denom_vac - delta * v_dot_grad;
-            }
-            int settled = fabs(denom - previous) <= RESONANCE_ROOT_RTOL * fabs(denom);
-            settled = settled && (2.0 * fabs(delta) * grad2 < 1.0);
-            if (!settled) denom = NAN;
-            /* cxr/_block_prologue.py:41-50 */
-            const double n_dot_g_blk = n_dot_g + delta * (gx * Gx + gy * Gy + gz * Gz);
-            /* cxr/_kernels.py:624-655 (_cxr_kin_core) */
-            const double v_dot_g = vx * Gx + vy * Gy + vz * Gz;
-            const double omega = (v_dot_g - r_num) / denom;
-            const double k_dot_v = omega * ((1.0 - denom) + r_den);
-            const double k_dot_g = omega * n_dot_g_blk;
-            const double detuning = g2 + 2.0 * k_dot_g;
-            /* cxr/_batched.py:435-458 (_line_bracket) */
-            const double k_mag =
-                omega * sqrt(grad2 == 0.0 ? 1.0 : 1.0 - 2.0 * delta + delta * delta * grad2);
-            const double E_res = HBARC_EV_ANG * omega;
-            int keep = cxr_electron && (E_res > t->lo_keep) && (E_res > 10.0) && (E_res < t->hi_keep);
-            int ix, bl, ab;
-            double fr;
-            interp_index(E_res, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
-            const double lfr = log_interp_fraction(E_res, t->E_tab, ix);
-            /* cxr/_block_prologue.py:53-62 + cxr/_recoil.py:100-118 */
-            const double slope = denom * (1.0 / (1.0 - omega * inv_E));
-            keep = keep && (denom > 0) && (omega * inv_E <= 1.0 - 1.0 / gamma);
-            /* cxr/_kernels.py:482-506,369-388: couplings and attenuation */
-            const int row = t->row_table[g];
-            const double *cr = t->chi_re + (int64_t)row * t->n_tab;
-            const double *ci = t->chi_im + (int64_t)row * t->n_tab;
-            const double *ur = t->u_re + (int64_t)row * t->n_tab;
-            const double *ui = t->u_im + (int64_t)row * t->n_tab;
-            const double chi_re = gather1(cr, t->n_tab, ix, fr, bl, ab);
-            const double chi_im = gather1(ci, t->n_tab, ix, fr, bl, ab);
-            const double u_re = gather1(ur, t->n_tab, ix, fr, bl, ab);
-            const double u_im = gather1(ui, t->n_tab, ix, fr, bl, ab);
-            double mu = 0.0;
-            for (int el = 0; el < t->n_mu; ++el) {
-                const double *lm = t->log_mu + (int64_t)el * t->n_tab;
-                double f0 = lm[ix - 1];
-                double v = exp(f0 + lfr * (lm[ix] - f0));
-                if (bl) v = exp(lm[0]);
-                if (ab) v = exp(lm[t->n_tab - 1]);
-                mu += v;
-            }
-            /* cxr/_batched.py:789-826 + cxr/_line_amplitude.py:14-37 */
-            double A2 = 0.0;
-            for (int pol = 0; pol < 2; ++pol) {
-                const double *Ev = pol == 0 ? t->ES + 3 * g : t->EP + 3 * g;
-                const double ex = Ev[0], ey = Ev[1], ez = Ev[2];
-                const double g_dot_e = Gx * ex + Gy * ey + Gz * ez;
-                const double v_dot_e = vx * ex + vy * ey + vz * ez;
-                const double k_dot_e = omega * delta * (gx * ex + gy * ey + gz * ez);
-                double pxr_num, f_cbs;
-                or_quantum_line_factors(h, gamma, v_dot_g, k_dot_v, k_dot_g, g2, k_mag * k_mag,
-                                        v_dot_e, g_dot_e, k_dot_e, &pxr_num, &f_cbs);
-                const double f_pxr = pxr_num / detuning;
-                const double re = chi_re * f_pxr + u_re * f_cbs;
-                const double im = chi_im * f_pxr + u_im * f_cbs;
-                const double a2 = re * re + im * im;
-                A2 = pol == 0 ? a2 : A2 + a2;
-            }
+            pair_state p;
+            pair_chain(t, geo->n_hat, &q, g, &p);
+            const double A2 = (p.A_re[0] * p.A_re[0] + p.A_im[0] * p.A_im[0]) +
+                              (p.A_re[1] * p.A_re[1] + p.A_im[1] * p.A_im[1]);
             /* cxr/_batched.py:702-730 + cxr/_kernels.py:658-668 */
             double T_abs;
             if (!ly) {
-                T_abs = or_mean_transmission(path0 * mu, path1 * mu);
+                T_abs = or_mean_transmission(path0 * p.mu, path1 * p.mu);
             } else {
                 /* piece_mean_transmission (segment_escape.py:335-355) with the
                  * exact per-layer mu at E_res (cxr/_batched.py:714-720) */
                 double mu_k[OR_MAX_LAYERS];
-                for (int k = 0; k < ly->n_layer; ++k) mu_k[k] = exact_mu(ly, k, E_res);
+                for (int k = 0; k < ly->n_layer; ++k) mu_k[k] = exact_mu(ly, k, p.E_res);
                 T_abs = 0.0;
-                for (int p = 0; p < n_piece; ++p) {
+                for (int i = 0; i < n_piece; ++i) {
                     double t0 = 0.0, t1 = 0.0;
                     for (int k = 0; k < ly->n_layer; ++k) {
-                        t0 += pp0[p * ly->n_layer + k] * mu_k[k];
-                        t1 += pp1[p * ly->n_layer + k] * mu_k[k];
+                        t0 += pp0[i * ly->n_layer + k] * mu_k[k];
+                        t1 += pp1[i * ly->n_layer + k] * mu_k[k];
                     }
-                    T_abs += pf[p] * or_mean_transmission(t0, t1);
+                    T_abs += pf[i] * or_mean_transmission(t0, t1);
                 }
             }
-            const double pref = ALPHA_FS * omega / pref_c1 * (t_L * t_L) * T_abs;
-            const double a_width = slope * t_L / (2.0 * HBARC_EV_ANG) * 1.0;
+            const double pref = ALPHA_FS * p.omega / pref_c1 * (t_L * t_L) * T_abs;
+            const double a_width = p.slope * t_L / (2.0 * HBARC_EV_ANG) * 1.0;
             const double weight = pref * A2 * t->WM[g];
-            const int good = keep && isfinite(weight) && (weight > 0);
-            E_res_out[o] = E_res;
+            const int good = p.keep && isfinite(weight) && (weight > 0);
+            E_res_out[o] = p.E_res;
             a_width_out[o] = a_width;
             weight_out[o] = weight;
             good_out[o] = (uint8_t)good;
@@ -344,127 +381,49 @@ void or_cxr_coherent_records(const or_cxr_tables *t, const or_cxr_geom *geo, int
                              int64_t Ne, double *const rec[OR_COH_FIELDS], uint8_t *good_out) {
     const double nx = geo->n_hat[0], ny = geo->n_hat[1], nz = geo->n_hat[2];
     const double T = geo->thickness;
-    const double h = HBARC_EV_ANG / M_E_EV;                    /* cxr/_recoil.py:27-32 */
     const double pref_c1 = 4.0 * (M_PI * M_PI) * HBARC_EV_ANG; /* cxr/_kernels.py:325 */
-    const double mec2_kev = M_E_EV / 1e3;
     for (int64_t s = 0; s < n_seg; ++s) {
-        const double E = E_keV[s];
-        const double vhx = v_hat[3 * s], vhy = v_hat[3 * s + 1], vhz = v_hat[3 * s + 2];
-        const double beta = or_beta_from_keV(E);
-        const double vx = beta * vhx, vy = beta * vhy, vz = beta * vhz;
-        /* cxr/_kernels.py:678-699 (_vacuum_doppler) */
-        const double gamma = 1.0 + E / mec2_kev;
-        const double one_minus_beta = 1.0 / (gamma * gamma * (1.0 + beta));
-        const double dvx = vhx - nx, dvy = vhy - ny, dvz = vhz - nz;
-        const double omc = 0.5 * (dvx * dvx + dvy * dvy + dvz * dvz);
-        const double denom_row = one_minus_beta + beta * omc;
+        seg_state q;
+        const double z_mid = r_mid[3 * s + 2];
+        seg_setup(geo->n_hat, T, E_keV[s], v_hat + 3 * s, z_mid, elec_id[s] < Ne, &q);
         /* coherent rows keep their own length and unit piece fraction (cxr/_setup.py:1001-1005) */
-        const double t_L = L_ang[s] / beta;
+        const double t_L = L_ang[s] / q.beta;
         /* escape distance at the piece ends, ordered along travel (cxr/_formation.py:168-200) */
         const double half = 0.5 * L_ang[s];
-        const double z_mid = r_mid[3 * s + 2];
-        const double L_start = slab_path(z_mid - half * vhz, T, nz);
-        const double L_end = slab_path(z_mid + half * vhz, T, nz);
-        double gx = -0.0 / nz, gy = -0.0 / nz, gz = -1.0 / nz;
-        if (z_mid < 0.0 || z_mid > T) { gx = 0.0; gy = 0.0; gz = 0.0; }
-        const double grad2 = gx * gx + gy * gy + gz * gz;
-        const double v_dot_grad = vx * gx + vy * gy + vz * gz;
-        const int cxr_electron = elec_id[s] < Ne;
-        const double inv_E = HBARC_EV_ANG / (gamma * M_E_EV);
+        const double L_start = slab_path(z_mid - half * q.vhz, T, nz);
+        const double L_end = slab_path(z_mid + half * q.vhz, T, nz);
         /* cxr/_setup.py:1023-1026: midpoint age and retardation d = t_mid - n.r */
         const double t_mid = (t_ang ? t_ang[s] : 0.0) + 0.5 * t_L;
         const double rx = r_mid[3 * s], ry = r_mid[3 * s + 1], rz = r_mid[3 * s + 2];
         const double d_geom = t_mid - (rx * nx + ry * ny + rz * nz);
         for (int g = 0; g < t->n_g; ++g) {
             const int64_t o = s * t->n_g + g;
-            const double Gx = t->G[3 * g], Gy = t->G[3 * g + 1], Gz = t->G[3 * g + 2];
-            const double g2 = Gx * Gx + Gy * Gy + Gz * Gz;
-            const double n_dot_g = Gx * nx + Gy * ny + Gz * nz;
-            const double r_num = 0.5 * g2 * inv_E;
-            const double r_den = n_dot_g * inv_E;
-            const double v_dot_g_exact = (vx * Gx + vy * Gy + vz * Gz) - r_num;
-            const double denom_vac = denom_row + r_den;
-            double denom = denom_vac, previous = denom, delta = NAN;
-            for (int pass = 0; pass < 3; ++pass) {  /* cxr/_kernels.py:702-765 */
-                double Er = HBARC_EV_ANG * (v_dot_g_exact / denom);
-                int ix, bl, ab;
-                double fr;
-                interp_index(Er, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
-                delta = gather1(t->delta, t->n_tab, ix, fr, bl, ab);
-                previous = denom;
-                denom = denom_vac - delta * v_dot_grad;
-            }
-            int settled = fabs(denom - previous) <= RESONANCE_ROOT_RTOL * fabs(denom);
-            settled = settled && (2.0 * fabs(delta) * grad2 < 1.0);
-            if (!settled) denom = NAN;
-            const double n_dot_g_blk = n_dot_g + delta * (gx * Gx + gy * Gy + gz * Gz);
-            const double v_dot_g = vx * Gx + vy * Gy + vz * Gz;
-            const double omega = (v_dot_g - r_num) / denom;
-            const double k_dot_v = omega * ((1.0 - denom) + r_den);
-            const double k_dot_g = omega * n_dot_g_blk;
-            const double detuning = g2 + 2.0 * k_dot_g;
-            const double k_mag =
-                omega * sqrt(grad2 == 0.0 ? 1.0 : 1.0 - 2.0 * delta + delta * delta * grad2);
-            const double E_res = HBARC_EV_ANG * omega;
-            int keep = cxr_electron && (E_res > t->lo_keep) && (E_res > 10.0) && (E_res < t->hi_keep);
-            int ix, bl, ab;
-            double fr;
-            interp_index(E_res, t->E_tab, t->n_tab, &ix, &fr, &bl, &ab);
-            const double lfr = log_interp_fraction(E_res, t->E_tab, ix);
-            keep = keep && (denom > 0) && (omega * inv_E <= 1.0 - 1.0 / gamma);
-            const int row = t->row_table[g];
-            const double chi_re = gather1(t->chi_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
-            const double chi_im = gather1(t->chi_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
-            const double u_re = gather1(t->u_re + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
-            const double u_im = gather1(t->u_im + (int64_t)row * t->n_tab, t->n_tab, ix, fr, bl, ab);
-            double mu = 0.0;
-            for (int el = 0; el < t->n_mu; ++el) {
-                const double *lm = t->log_mu + (int64_t)el * t->n_tab;
-                double f0 = lm[ix - 1];
-                double v = exp(f0 + lfr * (lm[ix] - f0));
-                if (bl) v = exp(lm[0]);
-                if (ab) v = exp(lm[t->n_tab - 1]);
-                mu += v;
-            }
-            /* complex PXR + CBS amplitude per polarization (cxr/_batched.py:600-625) */
-            double A_re[2], A_im[2];
-            for (int pol = 0; pol < 2; ++pol) {
-                const double *Ev = pol == 0 ? t->ES + 3 * g : t->EP + 3 * g;
-                const double ex = Ev[0], ey = Ev[1], ez = Ev[2];
-                const double g_dot_e = Gx * ex + Gy * ey + Gz * ez;
-                const double v_dot_e = vx * ex + vy * ey + vz * ez;
-                const double k_dot_e = omega * delta * (gx * ex + gy * ey + gz * ez);
-                double pxr_num, f_cbs;
-                or_quantum_line_factors(h, gamma, v_dot_g, k_dot_v, k_dot_g, g2, k_mag * k_mag,
-                                        v_dot_e, g_dot_e, k_dot_e, &pxr_num, &f_cbs);
-                const double f_pxr = pxr_num / detuning;
-                A_re[pol] = chi_re * f_pxr + u_re * f_cbs;
-                A_im[pol] = chi_im * f_pxr + u_im * f_cbs;
-            }
+            pair_state p;
+            pair_chain(t, geo->n_hat, &q, g, &p);
             /* formation factor constants of the piece (cxr/_batched.py:627-633) */
-            double apb, bma, q;
-            formation_coefficients(L_start * mu, L_end * mu, &apb, &bma, &q);
+            double apb, bma, qq;
+            formation_coefficients(L_start * p.mu, L_end * p.mu, &apb, &bma, &qq);
             /* exact vacuum centre / width and recoil phase over the age (cxr/_recoil.py:118-147),
              * with the vacuum denominator and n.g of the batched tables */
-            const double numerator = v_dot_g - r_num;
-            const double den = denom_row + r_den;
+            const double numerator = p.v_dot_g - p.r_num;
+            const double den = q.denom_row + p.r_den;
             const double E_c = HBARC_EV_ANG * numerator / den;
-            const double x = numerator / den * inv_E;
+            const double x = numerator / den * q.inv_E;
             const double kappa = 1.0 / (1.0 - x);
             const double a_vac = kappa * den * t_L / (2.0 * HBARC_EV_ANG);
-            const double d_shift = kappa * (x * denom_row + r_den) * t_mid;
-            const double g_shift = kappa * (x * v_dot_g - r_num) * t_mid;
-            const double amp = sqrt(ALPHA_FS * omega / pref_c1);
-            int good = keep && isfinite(amp) && (amp > 0) && (t_L > 0) && isfinite(apb) && (apb > 0) &&
+            const double d_shift = kappa * (x * q.denom_row + p.r_den) * t_mid;
+            const double g_shift = kappa * (x * p.v_dot_g - p.r_num) * t_mid;
+            const double amp = sqrt(ALPHA_FS * p.omega / pref_c1);
+            int good = p.keep && isfinite(amp) && (amp > 0) && (t_L > 0) && isfinite(apb) && (apb > 0) &&
                        isfinite(bma);
-            const double cs_re = amp * t_L * A_re[0], cs_im = amp * t_L * A_im[0];
-            const double cp_re = amp * t_L * A_re[1], cp_im = amp * t_L * A_im[1];
+            const double cs_re = amp * t_L * p.A_re[0], cs_im = amp * t_L * p.A_im[0];
+            const double cp_re = amp * t_L * p.A_re[1], cp_im = amp * t_L * p.A_im[1];
             good = good && isfinite(cs_re) && isfinite(cs_im) && isfinite(cp_re) && isfinite(cp_im);
             /* record fields (cxr/_batched.py:646-660) */
             rec[0][o] = E_c;
             rec[1][o] = a_vac;
             rec[2][o] = (d_geom + d_shift) / HBARC_EV_ANG;
-            rec[3][o] = rx * Gx + ry * Gy + rz * Gz + g_shift;
+            rec[3][o] = rx * p.G[0] + ry * p.G[1] + rz * p.G[2] + g_shift;
             rec[4][o] = cs_re;
             rec[5][o] = cs_im;
             rec[6][o] = cp_re;
@@ -473,7 +432,7 @@ void or_cxr_coherent_records(const or_cxr_tables *t, const or_cxr_geom *geo, int
             rec[9][o] = 0.5 * (L_end - L_start);
             rec[10][o] = apb;
             rec[11][o] = bma;
-            rec[12][o] = q;
+            rec[12][o] = qq;
             good_out[o] = (uint8_t)good;
         }
     }
