@@ -143,3 +143,53 @@ def run_coherent_reduction_kernel(E_r, aw, phase_slope, g_phase, c_s_re, c_s_im,
     coherent_reduce(records, [n], [float(mosaic_weight)], E_grid, delta_omega, sinc_cutoff=sinc_cutoff,
                     spec=out, device=out.device)
     return out
+
+
+def assign_rows(row_count, world: int):
+    """Rows to ranks, largest first onto the least loaded rank (lines x
+    energies is the cost, the same on every rank for one row). Returns one
+    ascending array of row indices per rank; deterministic."""
+    row_count = np.asarray(row_count, dtype=np.int64)
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = np.zeros(world, dtype=np.int64)
+    owner = np.empty(row_count.size, dtype=np.int64)
+    for r in np.argsort(-row_count, kind="stable"):
+        k = int(np.argmin(load))
+        owner[r] = k
+        load[k] += row_count[r]
+    return [np.flatnonzero(owner == k) for k in range(world)]
+
+
+def coherent_reduce_sharded(records, row_count, row_weight, E_grid_eV, delta_omega, *, scale=1.0, sinc_cutoff=None,
+                            process_group=None, reduce_fn=None, device=None) -> torch.Tensor:
+    """The coherent reduction with rows spread over the ranks of
+    ``process_group``: rows add incoherently, so each rank reduces whole rows
+    (a row's lines interfere and never split across ranks) and one all-reduce
+    sums the FP64 spectra. Every rank passes the full record set and gets the
+    full spectrum. ``reduce_fn`` (default ``coherent_reduce``) takes the same
+    arguments for one rank's rows and returns a float64 tensor on the
+    process group's device."""
+    import torch.distributed as dist
+
+    reduce_fn = reduce_fn or coherent_reduce
+    world = dist.get_world_size(process_group) if process_group is not None or dist.is_initialized() else 1
+    rank = dist.get_rank(process_group) if world > 1 else 0
+    row_count = np.asarray(row_count, dtype=np.int64)
+    off = np.concatenate([[0], np.cumsum(row_count)])
+    rows = assign_rows(row_count, world)[rank]
+    lines = np.concatenate([np.arange(off[r], off[r + 1]) for r in rows]) if rows.size else np.zeros(0, np.int64)
+    sub = {k: (records[k][torch.as_tensor(lines, device=records[k].device)] if torch.is_tensor(records[k])
+               else np.asarray(records[k])[lines]) for k in RECORD_FIELDS}
+    w = np.asarray(row_weight, dtype=np.float64)
+    kw = dict(scale=scale, sinc_cutoff=sinc_cutoff)
+    if device is not None:
+        kw["device"] = device
+    if rows.size == 0:  # more ranks than rows: one empty row, so the rank still joins the collective
+        counts, weights = np.zeros(1, np.int64), np.zeros(1)
+    else:
+        counts, weights = row_count[rows], w[rows]
+    spec = reduce_fn(sub, counts, weights, E_grid_eV, delta_omega, **kw)
+    if world > 1:
+        dist.all_reduce(spec, op=dist.ReduceOp.SUM, group=process_group)
+    return spec
