@@ -312,10 +312,15 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
 }
 
 // spec[e] += scale * sum_r w_r (|sum_items F_sigma|^2 + |sum_items F_pi|^2).
-__global__ void __launch_bounds__(256) coh_finalize_kernel(int n_row, int n_E, const int64_t *__restrict__ item_off,
-                                                           const double *__restrict__ w_row,
-                                                           const float *__restrict__ partial, double scale,
-                                                           double *__restrict__ spec) {
+// One thread per energy walks every item of every row in order, so the loop
+// is unrolled to keep several partial loads in flight (the adds stay in item
+// order: the result does not change) and blocks are small, spreading the
+// energies over more SMs.
+constexpr int kFinalizeThreads = 64;
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    coh_finalize_kernel(int n_row, int n_E, const int64_t *__restrict__ item_off, const double *__restrict__ w_row,
+                        const float *__restrict__ partial, double scale, double *__restrict__ spec) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_E) return;
     double total = 0.0;
@@ -324,6 +329,7 @@ __global__ void __launch_bounds__(256) coh_finalize_kernel(int n_row, int n_E, c
         const int64_t i1 = item_off[r + 1];
         if (i1 > i0) {
             double f[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
             for (int64_t i = i0; i < i1; ++i) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c) f[c] += (double)partial[((size_t)i * 4 + c) * n_E + e];
@@ -377,8 +383,9 @@ cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
     a.partial = partial;
     dim3 grid((unsigned)n_item_max, (unsigned)n_etiles(p.n_E));
     coh_field_kernel<<<grid, kThreads, 0, s>>>(a);
-    coh_finalize_kernel<<<(p.n_E + 255) / 256, 256, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight, partial,
-                                                            p.scale, p.spec);
+    const unsigned fin_blocks = (unsigned)((p.n_E + kFinalizeThreads - 1) / kFinalizeThreads);
+    coh_finalize_kernel<<<fin_blocks, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight, partial,
+                                                                p.scale, p.spec);
     return cudaGetLastError();
 }
 
