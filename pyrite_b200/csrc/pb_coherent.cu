@@ -6,7 +6,7 @@
 // chunk (cxr/_batched_finalize.py:209-243); its CUDA form gives one block per
 // energy and strides the lines over threads (coherent_jit_kernel.py:118-240).
 // Here the work is a line-chunk x energy-tile grid: a CTA stages up to
-// kStage line records into shared memory (80 bytes each, read back as
+// kStage line records into shared memory (96 bytes each, read back as
 // broadcasts), every thread owns kEPT energies and sums the four field
 // components of both polarisations in registers, and writes them once per
 // work item (row, chunk of lines). A second kernel adds a row's chunks in
