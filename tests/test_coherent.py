@@ -568,3 +568,17 @@ def test_gpu_coherent_bad_row_offsets_are_clamped_and_flagged():
         torch.cuda.synchronize()
         assert int(status.item()) & L.PB_DEV_BAD_INPUT
         assert torch.isfinite(spec).all()
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the behaviour without a GPU")
+def test_no_cpu_fallback_without_a_device():
+    """Without a CUDA device the coherent API refuses instead of computing
+    on the host."""
+    from pyrite_b200 import PyriteB200Error
+    from pyrite_b200.coherent import coherent_reduce, coherent_spectrum
+
+    rec, cnt, w, E, dom, Ne, _ = _golden("hopg20")
+    with pytest.raises(PyriteB200Error, match="CUDA"):
+        coherent_reduce(rec, cnt, w, E, dom)
+    with pytest.raises(PyriteB200Error, match="CUDA"):
+        coherent_spectrum(rec, cnt, w, E, dom, Ne)
