@@ -475,11 +475,15 @@ int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a
  * that loads it, held until the process exits), limited to
  * n_dir * (n_E + 2 far_pad) * 3 <= 262144 FP64 moments; larger requests
  * fail with PB_ERR_CAPACITY. The caller still owns every input and output.
- * The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the one array and clear it on entry: calls that overlap
- * on the GPU (different streams, threads or processes sharing a context)
- * race on it and must be serialised by the caller. */
+ * The arguments are checked as pb_cxr_score checks them (same error codes),
+ * except that far_moments may be NULL.
+ * The first call in a CUDA context resolves the array's device address
+ * (cudaGetSymbolAddress) and caches it under the context's ID, so make that
+ * first call before any stream capture; a context created later (after
+ * cudaDeviceReset, or by the driver API) gets its own lookup on its first
+ * call. All calls share the one array and clear it on entry: calls that
+ * overlap on the GPU (different streams, threads or processes sharing a
+ * context) race on it and must be serialised by the caller. */
 int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream);
 
 /* Coherent (field-sum) CXR reduction of per-row line records: for every row

@@ -12,6 +12,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libpyrite_b200.so"
 
 PB_OK = 0
+PB_ERR_INVALID, PB_ERR_CUDA, PB_ERR_UNSUPPORTED, PB_ERR_CAPACITY = 1, 2, 3, 4
 PB_RNG_SPLITMIX, PB_RNG_PHILOX = 0, 1
 PB_FP64, PB_MIXED = 0, 1
 PB_BEAM_EXPLICIT, PB_BEAM_SPOT, PB_BEAM_TWISS = 0, 1, 2

@@ -3,6 +3,7 @@
 // Every entry point validates its plain-C arguments on the host, launches on
 // the caller's stream and returns a pb_status. Errors carry a message in a
 // thread-local buffer read by pb_last_error(). Nothing here allocates.
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -43,6 +44,42 @@ int device_sms() {
 
 namespace pb {
 void set_last_error(const char *msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+
+int validate_cxr(const pb_cxr_args &a, const char *who, bool own_far_workspace) {
+    if (a.n_seg < 0 || a.n_dir < 1 || a.n_E < 1)
+        return fail(PB_ERR_INVALID, "%s: need n_seg >= 0, n_dir >= 1, n_E >= 1", who);
+    if (a.n_seg == 0) return PB_OK;
+    if (a.precision != PB_FP64 && a.precision != PB_MIXED)
+        return fail(PB_ERR_INVALID, "%s: unknown precision %d", who, a.precision);
+    const pb_cxr_tables &t = a.tables;
+    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4)
+        return fail(PB_ERR_INVALID, "%s: need n_g >= 1, n_tab >= 2, 1 <= n_mu <= 4", who);
+    if (!t.G || !t.ES || !t.EP || !t.WM || !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im ||
+        !t.u_re || !t.u_im || !t.log_mu || !t.delta)
+        return fail(PB_ERR_INVALID, "%s: every table pointer must be set", who);
+    if (!a.n_hat || !a.r_mid || !a.v_hat || !a.L || !a.E_keV || !a.elec_id)
+        return fail(PB_ERR_INVALID, "%s: segment and direction pointers must be set", who);
+    if (a.quadrature == PB_QUAD_BINMEAN) {
+        if (!a.edges || !a.spec) return fail(PB_ERR_INVALID, "%s: bin-mean needs edges and spec", who);
+        if (a.exact_widths > 0.0 && a.far_pad >= 0 && !a.far_moments && !own_far_workspace)
+            return fail(PB_ERR_INVALID, "%s: far field needs the far_moments workspace", who);
+    } else if (a.quadrature == PB_QUAD_NODE) {
+        if (!a.line_E || !a.line_a || !a.line_w || !a.line_dir || !a.line_count)
+            return fail(PB_ERR_INVALID, "%s: node quadrature needs a line buffer", who);
+        if (a.spec && !a.E_grid) return fail(PB_ERR_INVALID, "%s: node spectrum needs E_grid", who);
+    } else {
+        return fail(PB_ERR_INVALID, "%s: unknown quadrature %d", who, a.quadrature);
+    }
+    // A line buffer (bin-mean or node) is written through line_count: all of
+    // its arrays and a positive capacity, or none.
+    if (a.line_E && (!a.line_count || a.line_capacity < 1 || !a.line_a || !a.line_w || !a.line_dir))
+        return fail(PB_ERR_INVALID, "%s: line buffer needs line_E/a/w/dir, a count and a capacity >= 1", who);
+    if (a.n_layer < 0 || a.n_layer > 4)
+        return fail(PB_ERR_UNSUPPORTED, "%s: n_layer = %d outside [0, 4]", who, a.n_layer);
+    if (a.n_layer > 0 && (!a.z_top || !a.z_bot || !a.mu_off || !a.mu_knot || !a.mu_value || !a.mu_slope))
+        return fail(PB_ERR_INVALID, "%s: a layered absorber needs bounds and mu tables", who);
+    return PB_OK;
+}
 }  // namespace pb
 
 extern "C" {
@@ -105,34 +142,8 @@ int pb_transport(const pb_transport_args *a, void *stream) {
 
 int pb_cxr_score(const pb_cxr_args *a, void *stream) {
     if (!a) return fail(PB_ERR_INVALID, "pb_cxr_score: args is NULL");
-    if (a->n_seg < 0 || a->n_dir < 1 || a->n_E < 1)
-        return fail(PB_ERR_INVALID, "pb_cxr_score: need n_seg >= 0, n_dir >= 1, n_E >= 1");
-    if (a->n_seg == 0) return PB_OK;
-    const pb_cxr_tables &t = a->tables;
-    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4)
-        return fail(PB_ERR_INVALID, "pb_cxr_score: need n_g >= 1, n_tab >= 2, 1 <= n_mu <= 4");
-    if (!t.G || !t.ES || !t.EP || !t.WM || !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im ||
-        !t.u_re || !t.u_im || !t.log_mu || !t.delta)
-        return fail(PB_ERR_INVALID, "pb_cxr_score: every table pointer must be set");
-    if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id)
-        return fail(PB_ERR_INVALID, "pb_cxr_score: segment and direction pointers must be set");
-    if (a->quadrature == PB_QUAD_BINMEAN) {
-        if (!a->edges || !a->spec) return fail(PB_ERR_INVALID, "pb_cxr_score: bin-mean needs edges and spec");
-        if (a->exact_widths > 0.0 && a->far_pad >= 0 && !a->far_moments)
-            return fail(PB_ERR_INVALID, "pb_cxr_score: far field needs the far_moments workspace");
-    } else if (a->quadrature == PB_QUAD_NODE) {
-        if (!a->line_E || !a->line_a || !a->line_w || !a->line_dir || !a->line_count)
-            return fail(PB_ERR_INVALID, "pb_cxr_score: node quadrature needs a line buffer");
-        if (a->spec && !a->E_grid) return fail(PB_ERR_INVALID, "pb_cxr_score: node spectrum needs E_grid");
-    } else {
-        return fail(PB_ERR_INVALID, "pb_cxr_score: unknown quadrature %d", a->quadrature);
-    }
-    if (a->line_E && (!a->line_count || a->line_capacity < 1))
-        return fail(PB_ERR_INVALID, "pb_cxr_score: line buffer needs a count and a capacity");
-    if (a->n_layer < 0 || a->n_layer > 4)
-        return fail(PB_ERR_UNSUPPORTED, "pb_cxr_score: n_layer = %d outside [0, 4]", a->n_layer);
-    if (a->n_layer > 0 && (!a->z_top || !a->z_bot || !a->mu_off || !a->mu_knot || !a->mu_value || !a->mu_slope))
-        return fail(PB_ERR_INVALID, "pb_cxr_score: a layered absorber needs bounds and mu tables");
+    const int v = pb::validate_cxr(*a, "pb_cxr_score", false);
+    if (v != PB_OK || a->n_seg == 0) return v;
     cudaError_t e = pb::launch_cxr(*a, (cudaStream_t)stream, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_cxr_score: launch");
     return PB_OK;
@@ -329,10 +340,19 @@ static int coherent_sizes_ok(int32_t n_row, int64_t n_line, int32_t n_E) {
            n_E <= (1 << 24);
 }
 
+// The field kernel's grid has one x-block per work item: at most 2^31 - 1.
+// Every size coherent_sizes_ok accepts stays far below it (items <= n_row +
+// 148 * 3 * 4); the check guards the launch should those limits change.
+static int coherent_grid_ok(int32_t n_row, int64_t n_line, int32_t n_E) {
+    return pb::coherent_items(n_row, n_line, n_E) <= (int64_t)INT32_MAX;
+}
+
 int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes) {
     if (!bytes) return fail(PB_ERR_INVALID, "pb_coherent_work_size: bytes is NULL");
     if (!coherent_sizes_ok(n_row, n_line, n_E))
         return fail(PB_ERR_INVALID, "pb_coherent_work_size: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    if (!coherent_grid_ok(n_row, n_line, n_E))
+        return fail(PB_ERR_UNSUPPORTED, "pb_coherent_work_size: more than 2^31 - 1 work items; split the rows");
     *bytes = pb::coherent_work_bytes(n_row, n_line, n_E);
     return PB_OK;
 }
@@ -341,6 +361,8 @@ int pb_coherent_reduce(const pb_coherent_args *a, void *stream) {
     if (!a) return fail(PB_ERR_INVALID, "pb_coherent_reduce: args is NULL");
     if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
         return fail(PB_ERR_INVALID, "pb_coherent_reduce: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    if (!coherent_grid_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_UNSUPPORTED, "pb_coherent_reduce: more than 2^31 - 1 work items; split the rows");
     if (!a->row_off || !a->row_weight || !a->E || !a->delta_omega || !a->spec || !a->work)
         return fail(PB_ERR_INVALID, "pb_coherent_reduce: row_off, row_weight, E, delta_omega, spec, work must be set");
     if (a->n_line > 0 && (!a->E_vac || !a->a_vac || !a->phase_slope || !a->g_phase || !a->cs_re || !a->cs_im ||

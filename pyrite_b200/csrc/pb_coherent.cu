@@ -349,6 +349,10 @@ uint64_t coherent_work_bytes(int n_row, int64_t n_line, int n_E) {
     return align256((size_t)(n_row + 1) * sizeof(int64_t)) + (size_t)items * 4 * (size_t)n_E * sizeof(float);
 }
 
+int64_t coherent_items(int n_row, int64_t n_line, int n_E) {
+    return max_items(n_row, n_line, chunk_lines(n_line, n_E));
+}
+
 cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
     const int64_t K = chunk_lines(p.n_line, p.n_E);
     const int64_t n_item_max = max_items(p.n_row, p.n_line, K);

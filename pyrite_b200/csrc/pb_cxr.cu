@@ -29,6 +29,7 @@
 #include <type_traits>
 #include <cstdint>
 #include <cstdio>
+#include <cuda.h>
 #include <mutex>
 
 #include "pb_common.cuh"
@@ -1596,14 +1597,59 @@ namespace {
 constexpr size_t kNoAllocFarDoubles = size_t(1) << 18;  // 2 MiB of FP64 moments
 static __device__ __align__(256) double g_noalloc_far[kNoAllocFarDoubles];
 
+// The array's device address differs per CUDA context (a module is loaded
+// once per context), so the resolved address is cached per context: keyed by
+// the driver's context ID, which stays unique for the life of the process --
+// a context re-created after cudaDeviceReset, or one the caller made with the
+// driver API, gets a new ID and so a fresh lookup. The two driver functions
+// are reached through the runtime (cudaGetDriverEntryPoint), so the library
+// does not link the driver library directly.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+struct NoAllocSlot {
+    unsigned long long ctx_id;
+    double *ptr;
+};
+constexpr int kNoAllocSlots = 64;
+
 std::mutex g_noalloc_mu;
-double *g_noalloc_ptr[64] = {};
+NoAllocSlot g_noalloc_cache[kNoAllocSlots] = {};
+int g_noalloc_next = 0;
+bool g_ctx_fns_tried = false;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
 thread_local char g_noalloc_err[256] = "";
 
 int noalloc_fail(int code, const char *msg) {
     snprintf(g_noalloc_err, sizeof(g_noalloc_err), "%s", msg);
     pb::set_last_error(g_noalloc_err);
     return code;
+}
+
+// ID of this thread's current context, making the device's primary context
+// current first if none is (cudaSetDevice initialises it). False when the
+// driver functions are unavailable or the query fails: the caller then
+// resolves the address without the cache.
+bool current_ctx_id(int dev, unsigned long long *id) {
+    if (!g_ctx_fns_tried) {
+        g_ctx_fns_tried = true;
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = q0;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q0 == cudaDriverEntryPointSuccess && q1 == cudaDriverEntryPointSuccess) {
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+            g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+        }
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return false;
+    if (!ctx) {
+        if (cudaSetDevice(dev) != cudaSuccess || g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    }
+    return g_ctx_get_id(ctx, id) == CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -1613,16 +1659,10 @@ extern "C" int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream) {
     if (args->quadrature != PB_QUAD_BINMEAN)
         return noalloc_fail(PB_ERR_UNSUPPORTED,
                             "pb_cxr_score_noalloc: only bin-mean quadrature (node sampling needs a line buffer)");
-    if (args->n_seg < 0 || args->n_dir < 1 || args->n_E < 1)
-        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: need n_seg >= 0, n_dir >= 1, n_E >= 1");
-    if (args->n_seg == 0) return PB_OK;
-    const pb_cxr_tables &t = args->tables;
-    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4 || !t.G || !t.ES || !t.EP || !t.WM ||
-        !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im || !t.u_re || !t.u_im || !t.log_mu || !t.delta)
-        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: incomplete reflection tables");
-    if (!args->n_hat || !args->r_mid || !args->v_hat || !args->L || !args->E_keV || !args->elec_id ||
-        !args->edges || !args->spec)
-        return noalloc_fail(PB_ERR_INVALID, "pb_cxr_score_noalloc: segment, axis and output pointers must be set");
+    // The same argument checks as pb_cxr_score (the far-field workspace is
+    // this file's array, so far_moments may be NULL).
+    const int v = pb::validate_cxr(*args, "pb_cxr_score_noalloc", true);
+    if (v != PB_OK || args->n_seg == 0) return v;
     const bool far = args->exact_widths > 0.0 && args->far_pad >= 0;
     if (far) {
         const size_t need = (size_t)args->n_dir * ((size_t)args->n_E + 2 * (size_t)args->far_pad) * 3;
@@ -1636,14 +1676,20 @@ extern "C" int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream) {
         }
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
         return noalloc_fail(PB_ERR_CUDA, "pb_cxr_score_noalloc: no current CUDA device");
     double *ws = nullptr;
     {
-        // First call on a device: resolve the array's device address (host
+        // First call in a context: resolve the array's device address (host
         // code must not use the symbol itself as a pointer).
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        unsigned long long cid = 0;
+        const bool keyed = current_ctx_id(dev, &cid);
+        if (keyed) {
+            for (const NoAllocSlot &e : g_noalloc_cache)
+                if (e.ptr && e.ctx_id == cid) ws = e.ptr;
+        }
+        if (!ws) {
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_far);
             if (e != cudaSuccess) {
@@ -1651,9 +1697,12 @@ extern "C" int pb_cxr_score_noalloc(const pb_cxr_args *args, void *stream) {
                 snprintf(msg, sizeof(msg), "pb_cxr_score_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
                 return noalloc_fail(PB_ERR_CUDA, msg);
             }
-            g_noalloc_ptr[dev] = static_cast<double *>(p);
+            ws = static_cast<double *>(p);
+            if (keyed) {
+                g_noalloc_cache[g_noalloc_next] = NoAllocSlot{cid, ws};
+                g_noalloc_next = (g_noalloc_next + 1) % kNoAllocSlots;
+            }
         }
-        ws = g_noalloc_ptr[dev];
     }
     pb_cxr_args a = *args;
     a.far_moments = far ? ws : nullptr;

@@ -44,9 +44,16 @@ cudaError_t launch_segments_sample(const pb_segments &src, int64_t stride, const
                                    unsigned int *status, cudaStream_t s, int sms);
 
 uint64_t coherent_work_bytes(int n_row, int64_t n_line, int n_E);
+// Work items (x-blocks of the field kernel) of a coherent reduction.
+int64_t coherent_items(int n_row, int64_t n_line, int n_E);
 cudaError_t launch_coherent(const pb_coherent_args &a, cudaStream_t s);
 
 // Record the message pb_last_error() returns on this thread.
 void set_last_error(const char *msg);
+
+// Host checks of a pb_cxr_args, shared by every scorer entry point: PB_OK, or
+// an error code with pb_last_error() set ("who: ..."). own_far_workspace: the
+// entry point supplies the far-field workspace itself.
+int validate_cxr(const pb_cxr_args &a, const char *who, bool own_far_workspace);
 
 }  // namespace pb

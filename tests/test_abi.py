@@ -67,3 +67,64 @@ def test_errors_are_reported_without_a_device():
     c = L.PbCxrArgs()
     c.n_dir = 0
     assert lib.pb_cxr_score(C.byref(c), None) == 1
+
+
+def _filled_cxr_args():
+    """A bin-mean pb_cxr_args whose pointers are all set (to addresses that are
+    never dereferenced: every call below fails in its host checks)."""
+    c = L.PbCxrArgs()
+    c.n_seg, c.n_dir, c.n_E = 16, 1, 8
+    c.precision, c.quadrature = L.PB_MIXED, L.PB_QUAD_BINMEAN
+    fake = 0x1000
+    for f in ("n_hat", "r_mid", "v_hat", "L", "E_keV", "elec_id", "edges", "spec", "E_grid"):
+        setattr(c, f, fake)
+    t = c.tables
+    t.n_g, t.n_tab, t.n_mu = 4, 8, 1
+    for f in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re", "u_im", "log_mu", "delta"):
+        setattr(t, f, fake)
+    c.tables = t
+    return c
+
+
+@pytest.mark.parametrize("entry", ["pb_cxr_score", "pb_cxr_score_noalloc"])
+def test_cxr_entry_points_share_their_argument_checks(entry):
+    """Both scorer entry points refuse, before any launch, a line buffer
+    without its count (the kernel would add to a NULL counter) and a layered
+    absorber without its tables, with the same code and a message naming
+    the entry point."""
+    lib = L.load()
+    fn = getattr(lib, entry)
+    c = _filled_cxr_args()
+    c.line_E = 0x2000  # line_count left NULL
+    assert fn(C.byref(c), None) == L.PB_ERR_INVALID
+    msg = lib.pb_last_error()
+    assert entry.encode() in msg and b"line buffer" in msg
+    c = _filled_cxr_args()
+    c.n_layer = 2  # no bounds, no mu tables
+    assert fn(C.byref(c), None) == L.PB_ERR_INVALID
+    assert b"layered" in lib.pb_last_error()
+    c = _filled_cxr_args()
+    c.n_layer = 5
+    assert fn(C.byref(c), None) == L.PB_ERR_UNSUPPORTED
+    c = _filled_cxr_args()
+    c.precision = 7
+    assert fn(C.byref(c), None) == L.PB_ERR_INVALID
+
+
+def test_noalloc_far_field_capacity_is_checked_before_any_cuda_call():
+    lib = L.load()
+    c = _filled_cxr_args()
+    c.exact_widths, c.far_pad = 64.0, 10
+    c.n_dir, c.n_E = 64, 4096  # 64 * (4096 + 20) * 3 moments > 262144
+    assert lib.pb_cxr_score_noalloc(C.byref(c), None) == L.PB_ERR_CAPACITY
+    assert b"262144" in lib.pb_last_error()
+
+
+def test_coherent_work_size_at_the_largest_accepted_sizes():
+    """The field kernel's grid stays within 2^31 - 1 x-blocks for every size
+    the entry points accept (items <= n_row + 1776)."""
+    lib = L.load()
+    nb = C.c_uint64()
+    assert lib.pb_coherent_work_size(1 << 24, 1 << 40, 1 << 24, C.byref(nb)) == 0
+    assert lib.pb_coherent_work_size(1 << 24, 1 << 40, 1, C.byref(nb)) == 0
+    assert lib.pb_coherent_work_size((1 << 24) + 1, 10, 10, C.byref(nb)) == L.PB_ERR_INVALID
