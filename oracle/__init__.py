@@ -256,6 +256,65 @@ def philox4x32_10(ctr, key):
     return [int(v) for v in c]
 
 
+def beam_entries(beam, e_start: int, n: int, rng: int = 1):
+    """Entrance states (pos [n,3], dir [n,3], E [n]) of histories
+    [e_start, e_start + n) of a Gaussian-spot or Twiss beam, drawn from the
+    counter-addressed entry stream as the reference samples them:
+    normals z_c = ndtri(u_c) of open uniforms of the stream keyed
+    (beam.root, history) (src/pyrite/montecarlo/transport/kinematics.py:270-311;
+    ``rng`` 1 = Philox4x32-10 with a 52-bit open uniform, 0 = SplitMix64);
+    Twiss phase space x = sqrt(eps beta) z0, x' = sqrt(eps / beta)(z1 - alpha z0)
+    (src/pyrite/montecarlo/transverse.py:177-186); offsets projected onto the
+    tilted entrance face (src/pyrite/montecarlo/geometry.py:374-390); direction
+    (x', y', 1) in the beam frame, normalised
+    (src/pyrite/montecarlo/transport/beam_entry.py:347-359).
+    ``beam`` carries the pb_beam fields (mode 1 spot / 2 Twiss, root,
+    twiss_x/y = (eps [mm rad], beta [mm/rad], alpha), sigma_x/y_ang, tilted,
+    e_x, e_y, beam_dir, basis (row-major 3x3), E0_keV)."""
+    from scipy.special import ndtri
+
+    twiss = int(beam.mode) == 2
+    nz = 4 if twiss else 2
+    z = np.empty((n, nz))
+    for i in range(n):
+        key = stream_key(int(beam.root), e_start + i)
+        for c in range(nz):
+            if rng == 1:
+                w = philox_uniform(key, c)
+                u = (np.floor(w * 4503599627370496.0) + 0.5) * (1.0 / 4503599627370496.0)
+            else:
+                z64 = splitmix64((key + 0x9E3779B97F4A7C15 * (c + 1)) % 2**64)
+                u = ((z64 >> 12) + 0.5) * (1.0 / 4503599627370496.0)
+            z[i, c] = ndtri(u)
+    bd = np.array(beam.beam_dir[:], float)
+    if twiss:
+        ex, bx, ax = beam.twiss_x[:]
+        ey, by, ay = beam.twiss_y[:]
+        u_off = np.sqrt(ex * bx) * z[:, 0] * 1.0e7
+        xp = np.sqrt(ex / bx) * (z[:, 1] - ax * z[:, 0])
+        v_off = np.sqrt(ey * by) * z[:, 2] * 1.0e7
+        yp = np.sqrt(ey / by) * (z[:, 3] - ay * z[:, 2])
+    else:
+        u_off, v_off = z[:, 0] * beam.sigma_x_ang, z[:, 1] * beam.sigma_y_ang
+        xp = yp = np.zeros(n)
+    e_x, e_y = np.array(beam.e_x[:], float), np.array(beam.e_y[:], float)
+    pos = np.zeros((n, 3))
+    if beam.tilted:
+        s_star = -(u_off * e_x[2] + v_off * e_y[2]) / bd[2]
+        pos[:, 0] = (u_off * e_x[0] + v_off * e_y[0]) + s_star * bd[0]
+        pos[:, 1] = (u_off * e_x[1] + v_off * e_y[1]) + s_star * bd[1]
+    else:
+        pos[:, 0], pos[:, 1] = u_off, v_off
+    if twiss:
+        B = np.array(beam.basis[:], float).reshape(3, 3)
+        d = (xp[:, None] * B[:, 0][None, :] + yp[:, None] * B[:, 1][None, :]) + bd[None, :]
+        nrm = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        dirs = d / nrm[:, None]
+    else:
+        dirs = np.tile(bd, (n, 1))
+    return pos, dirs, np.full(n, float(beam.E0_keV))
+
+
 # ---------------------------------------------------------------------------
 # Layer tables (src/pyrite/montecarlo/transport/layer_tables.py:52-114)
 # ---------------------------------------------------------------------------

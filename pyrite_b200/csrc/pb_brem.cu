@@ -31,16 +31,18 @@ constexpr int kBremMaxDir = 16;
 // folds the per-segment ones of its cross-section form (brem_nsig):
 // beta_i holds beta_i / p_i^2 and nL[el] holds n_el L Z_el^2 den_i[el].
 template <class Real>
-struct BremSeg {
+struct alignas(sizeof(Real) == 4 ? 16 : 8) BremSeg {
     Real T;       // keV
     Real p_i;     // momentum / (m c)
     Real beta_i;
     // Escape geometry: FP64 keeps the clipped end depths (e0, e1); the float
     // path keeps the exit-side depth of the shallower end toward the top (e0)
-    // and the bottom (e1) and the depth difference |end1 - end0| (e2).
-    Real e0, e1, e2;
+    // and the bottom (e1), the depth difference |end1 - end0| (e2) and its
+    // reciprocal (inv_e2, infinite for a segment parallel to the faces).
+    Real e0, e1, e2, inv_e2;
     Real nL[kBremMaxEl];     // n_el * 1e24 * L * 1e-8  [1/cm^2]
-    Real den_i[kBremMaxEl];  // 1 - exp(-2 pi Z alpha / beta_i)
+    // 1 - exp(-2 pi Z alpha / beta_i); the float path folds it into nL.
+    Real den_i[sizeof(Real) == 8 ? kBremMaxEl : 1];
 };
 
 __device__ __forceinline__ double b_sqrt(double x) { return sqrt(x); }
@@ -131,19 +133,23 @@ __device__ __forceinline__ void brem_stage(BremSeg<Real> &b, const pb_brem_args 
         b.e0 = d0;
         b.e1 = d1;
         b.e2 = 0;
+        b.inv_e2 = 0;
     } else {
         b.e0 = fmin(d0, d1);
         b.e1 = fmin(T_slab - d0, T_slab - d1);
         b.e2 = fabs(d1 - d0);
+        b.inv_e2 = 1.0f / b.e2;
     }
     const bool rad = a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
     const Real path_cm = (Real)a.L[s] * (Real)1e-8;
     for (int el = 0; el < a.n_el; ++el) {
         b.nL[el] = rad ? (Real)(a.n_ang3[el] * 1e24) * (Real)1 * path_cm : (Real)0;
-        b.den_i[el] = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
+        const Real den_i = (Real)1 - b_exp(-za * (Real)a.Z[el] / b.beta_i);
         if constexpr (sizeof(Real) == 4) {
             const Real Z = (Real)a.Z[el];
-            b.nL[el] *= Z * Z * b.den_i[el];
+            b.nL[el] *= Z * Z * den_i;
+        } else {
+            b.den_i[el] = den_i;
         }
     }
     if constexpr (sizeof(Real) == 4) b.beta_i = b.beta_i / (p_i * p_i);
@@ -197,6 +203,89 @@ __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T
     return nsig;
 }
 
+// ---------------------------------------------------------------------------
+// Direction moments of the segment-mean escape (float path).
+//
+// A segment's escape toward direction d is its mean transmission
+//   Tbar(f) = int_0^1 exp(-(a + b s) f) ds = (exp(-a f) - exp(-c f)) / (b f),
+// a = mu e_lo (optical depth of the shallower end below the exit face, along
+// the face normal), b = mu e2 (depth extent of the segment), c = a + b, and
+// f = 1 / |n_z,d| the direction's path factor. The tiles of one detector
+// leave through the same face with path factors f_d = f_c + delta_d inside a
+// narrow band |delta_d| <= Delta (0.13 % of f_c for 16 tiles of a 2x2 cm^2
+// detector at 1 m). The function g(f) = f Tbar(f) = (exp(-a f) - exp(-c f)) / b
+// is a difference of exponentials, so its Taylor series about f_c,
+//   g(f_c + Delta h) = sum_n h^n P_n / n!,
+//   P_n = (-Delta)^n (a^n exp(-a f_c) - c^n exp(-c f_c)) / b,
+// has coefficients that do not depend on the direction. Their sums over the
+// segments of a chunk, Q_n = sum_seg nsig_seg P_n,seg, are accumulated per
+// photon energy, and every direction is rebuilt once per chunk as
+//   sum_seg nsig Tbar(f_d) = (1 / f_d) sum_n h_d^n Q_n / n!,  h_d = delta_d / Delta.
+// Two exponentials per (segment, energy) replace two per (segment, energy,
+// direction). The P_n follow without cancellation from
+//   P_0 = g(f_c),  P_{n+1} = ah P_n + R_n,  R_0 = Delta exp(-c f_c),
+//   R_{n+1} = ch R_n,  ah = -Delta a,  ch = -Delta c
+// (from a^{n+1} E_a - c^{n+1} E_c = a (a^n E_a - c^n E_c) - b c^n E_c), and
+// P_0 = exp(-a f_c) f_c phi(b f_c), phi(x) = (1 - e^-x)/x, takes the series
+// of phi below x = 0.1 (degree 5, truncation < x^6/5040 < 2e-10) where the
+// difference of the exponentials would cancel.
+// Truncation after order N: the remainder of the Taylor series is at most
+// about rho^(N+1) / sqrt(2 pi (N+1)) of the unattenuated term, rho = Delta /
+// f_min, whatever the optical depths (the attenuation exp(-a f_min) bounds the
+// growth of the derivatives); the host-side choice N = 3 for rho <= 0.01 and
+// N = 7 for rho <= 0.1 keeps it below 3e-9.
+// ---------------------------------------------------------------------------
+struct BremMomentConst {
+    float mu_l2fc;  // mu log2(e) f_c
+    float mu_fc;    // mu f_c
+    float inv_mu;   // 1 / mu
+    float mu_dl;    // mu Delta
+    float f_c, dl;  // f_c, Delta
+};
+
+template <int N>
+__device__ __forceinline__ void brem_moment_chunk(const BremSeg<float> *segs, int nc, bool up, float k,
+                                                  const float *Zs, int n_el, float k_ev, float c0, float za,
+                                                  float mc2, const BremKConst &kk, const float *zl,
+                                                  const BremMomentConst &m, float (&Q)[N + 1]) {
+    for (int j = 0; j < nc; ++j) {
+        const BremSeg<float> &b = segs[j];
+        const float T_f = b.T - k;
+        if (!(T_f > 1e-6f && k > 0.0f)) continue;
+        const float nsig = brem_nsig<float>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
+        const float es = up ? b.e0 : b.e1;
+        const float ef = es + b.e2;
+        const float Ea = ex2_approx(-m.mu_l2fc * es);
+        const float Ec = ex2_approx(-m.mu_l2fc * ef);
+        const float x = m.mu_fc * b.e2;
+        const float phi = fmaf(x, fmaf(x, fmaf(x, fmaf(x, fmaf(x, -1.0f / 720.0f, 1.0f / 120.0f), -1.0f / 24.0f),
+                                                   1.0f / 6.0f), -0.5f), 1.0f);
+        float P = x > 0.1f ? (Ea - Ec) * (m.inv_mu * b.inv_e2) : Ea * m.f_c * phi;
+        Q[0] = fmaf(nsig, P, Q[0]);
+        if constexpr (N > 0) {
+            const float ah = -m.mu_dl * es, ch = -m.mu_dl * ef;
+            float R = m.dl * Ec;
+#pragma unroll
+            for (int n = 1; n <= N; ++n) {
+                P = fmaf(ah, P, R);
+                if (n < N) R *= ch;
+                Q[n] = fmaf(nsig, P, Q[n]);
+            }
+        }
+    }
+}
+
+// sum_n h^n Q_n / n! (Horner).
+template <int N>
+__device__ __forceinline__ float brem_moment_eval(const float (&Q)[N + 1], float h) {
+    constexpr float kInvFact[8] = {1.0f, 1.0f, 0.5f, 1.0f / 6.0f, 1.0f / 24.0f, 1.0f / 120.0f, 1.0f / 720.0f,
+                                   1.0f / 5040.0f};
+    float r = Q[N] * kInvFact[N];
+#pragma unroll
+    for (int n = N - 1; n >= 0; --n) r = fmaf(r, h, Q[n] * kInvFact[n]);
+    return r;
+}
+
 template <class Real>
 __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
@@ -230,28 +319,36 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         inv_f_ln2[threadIdx.x] = (float)(fmax(fabs((double)nz), 1.0e-12) / 0.6931471805599453);
     }
     // Whether every direction of this launch leaves through the same face
-    // (+1 top, -1 bottom, 0 mixed), read from the directions themselves; with
-    // a full set of directions on one side the per-direction factors live in
-    // registers (the fast form of the escape loop below).
+    // (+1 top, -1 bottom, 0 mixed), read from the directions themselves.
     int side_all = 0;
-    float fr[kBremMaxDir];
-    float f_min_ln2 = 3.0e38f;
     {
         int n_up = 0;
         for (int dd = 0; dd < nd; ++dd) n_up += a.n_hat[3 * (d0 + dd) + 2] < 0.0 ? 1 : 0;
         side_all = n_up == nd ? 1 : (n_up == 0 ? -1 : 0);
-#pragma unroll
-        for (int dd = 0; dd < kBremMaxDir; ++dd) {
-            const double nz = dd < nd ? fabs(a.n_hat[3 * (d0 + dd) + 2]) : 1.0;
-            fr[dd] = (float)(1.0 / fmax(nz, 1.0e-12));
-            if (dd < nd) f_min_ln2 = fminf(f_min_ln2, fr[dd] * 0.69314718f);
+    }
+    // Moment form (see brem_moment_chunk): float, one exit face, and the
+    // path factors within rho = Delta / f_min <= 0.1 of their centre.
+    __shared__ float mom_h[kBremMaxDir];     // (f_d - f_c) / Delta
+    __shared__ float mom_invf[kBremMaxDir];  // 1 / f_d
+    int order = -1;
+    double f_c = 1.0, dl = 0.0;
+    if (sizeof(Real) == 4 && side_all != 0) {
+        double f_lo = 1e300, f_hi = 0.0;
+        for (int dd = 0; dd < nd; ++dd) {
+            const double f = 1.0 / fmax(fabs(a.n_hat[3 * (d0 + dd) + 2]), 1.0e-12);
+            f_lo = fmin(f_lo, f);
+            f_hi = fmax(f_hi, f);
+        }
+        f_c = 0.5 * (f_lo + f_hi);
+        dl = 0.5 * (f_hi - f_lo);
+        const double rho = dl / f_lo;
+        order = dl == 0.0 ? 0 : (rho <= 0.01 ? 3 : (rho <= 0.1 ? 7 : -1));
+        if (threadIdx.x < nd) {
+            const double f = 1.0 / fmax(fabs(a.n_hat[3 * (d0 + threadIdx.x) + 2]), 1.0e-12);
+            mom_h[threadIdx.x] = dl > 0.0 ? (float)((f - f_c) / dl) : 0.0f;
+            mom_invf[threadIdx.x] = (float)(1.0 / f);
         }
     }
-    const bool fast = sizeof(Real) == 4 && nd == kBremMaxDir && side_all != 0;
-    // The fast form keeps the 16 direction factors as 8 packed pairs.
-    unsigned long long fr2[kBremMaxDir / 2];
-#pragma unroll
-    for (int i = 0; i < kBremMaxDir / 2; ++i) fr2[i] = f2_pack(fr[2 * i], fr[2 * i + 1]);
     const double k_kev_d = on ? a.E_grid[e] / 1e3 : 1.0;
     const Real k = (Real)k_kev_d;
     const Real mu = on ? (Real)a.mu[e] : (Real)0;
@@ -280,52 +377,30 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         __syncthreads();
         if (!on) continue;
         if constexpr (sizeof(Real) == 4) {
-            if (fast) {
-                // The fast form below (see the scalar form's comment), on
-                // packed direction pairs: per pair of directions the
-                // difference form costs 2 FMUL2, 4 SFU, 2 FFMA2 and the series
-                // form 2 FFMA2, 2 FMUL2, 2 SFU, 1 FFMA2.
-                unsigned long long part2[kBremMaxDir / 2];
-#pragma unroll
-                for (int i = 0; i < kBremMaxDir / 2; ++i) part2[i] = 0ull;
-                const float mu2 = mu * 1.44269504f;
-                for (int j = 0; j < nc; ++j) {
-                    const BremSeg<Real> &b = segs[j];
-                    const Real T_f = b.T - k;
-                    if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-                    const float nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
-                    const float A = mu2 * (side_all > 0 ? b.e0 : b.e1);
-                    const float B = mu2 * b.e2;
-                    if (B * f_min_ln2 > 0.01f) {
-                        const float w = __fdividef(nsig, B);
-                        const unsigned long long nA = f2_pack(-A, -A), nC = f2_pack(-(A + B), -(A + B));
-                        const unsigned long long w2 = f2_pack(w, w), nw2 = f2_pack(-w, -w);
-#pragma unroll
-                        for (int i = 0; i < kBremMaxDir / 2; ++i) {
-                            part2[i] = f2_fma(w2, f2_ex2(f2_mul(nA, fr2[i])), part2[i]);
-                            part2[i] = f2_fma(nw2, f2_ex2(f2_mul(nC, fr2[i])), part2[i]);
-                        }
-                    } else {
-                        const float m0 = nsig * 0.69314718f;
-                        const float Bl = B * 0.69314718f;
-                        const float m1 = -0.5f * m0 * Bl;
-                        const float m2 = m0 * Bl * Bl * (1.0f / 6.0f);
-                        const unsigned long long m0_2 = f2_pack(m0, m0), m1_2 = f2_pack(m1, m1),
-                                                 m2_2 = f2_pack(m2, m2), nA = f2_pack(-A, -A);
-#pragma unroll
-                        for (int i = 0; i < kBremMaxDir / 2; ++i) {
-                            const unsigned long long f = fr2[i];
-                            const unsigned long long t = f2_mul(f2_fma(f, f2_fma(f, m2_2, m1_2), m0_2), f);
-                            part2[i] = f2_fma(t, f2_ex2(f2_mul(nA, f)), part2[i]);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < kBremMaxDir / 2; ++i) {
-                    float lo, hi;
-                    f2_unpack(part2[i], lo, hi);
-                    acc[2 * i][threadIdx.x] += (double)lo * (double)inv_f_ln2[2 * i];
-                    acc[2 * i + 1][threadIdx.x] += (double)hi * (double)inv_f_ln2[2 * i + 1];
+            if (order >= 0) {
+                BremMomentConst m;
+                m.mu_l2fc = (float)((double)mu * 1.4426950408889634 * f_c);
+                m.mu_fc = (float)((double)mu * f_c);
+                m.inv_mu = mu > 0.0f ? 1.0f / mu : 0.0f;
+                m.mu_dl = (float)((double)mu * dl);
+                m.f_c = (float)f_c;
+                m.dl = (float)dl;
+                const bool up_all = side_all > 0;
+                if (order == 0) {
+                    float Q[1] = {0.0f};
+                    brem_moment_chunk<0>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    for (int dd = 0; dd < nd; ++dd)
+                        acc[dd][threadIdx.x] += (double)Q[0] * (double)mom_invf[dd];
+                } else if (order == 3) {
+                    float Q[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                    brem_moment_chunk<3>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    for (int dd = 0; dd < nd; ++dd)
+                        acc[dd][threadIdx.x] += (double)brem_moment_eval<3>(Q, mom_h[dd]) * (double)mom_invf[dd];
+                } else {
+                    float Q[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    brem_moment_chunk<7>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    for (int dd = 0; dd < nd; ++dd)
+                        acc[dd][threadIdx.x] += (double)brem_moment_eval<7>(Q, mom_h[dd]) * (double)mom_invf[dd];
                 }
                 continue;
             }
@@ -355,46 +430,16 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
                 // optical depths A f (lower end) and B f (depth difference),
                 // D = B f ln 2. Sums are kept without the factor 1/(f ln 2),
                 // applied once per chunk:
-                //   D > 0.01 for every direction: [nsig / B] 2^(-A f) (1 - 2^(-B f));
-                //   otherwise:                  nsig 2^(-A f) (1 - D/2 + D^2/6 - D^3/24) f ln 2,
+                //   D > 0.01: [nsig / B] 2^(-A f) (1 - 2^(-B f));
+                //   otherwise: nsig 2^(-A f) (1 - D/2 + D^2/6 - D^3/24) f ln 2,
                 // the series where the difference would cancel (D^4/120 < 1e-10).
-                // The fast form (all 16 tiles on one side, per-thread registers
-                // for f) is instruction-issue bound, so each direction costs six
-                // instructions on either branch: the difference form
-                //   w 2^(-A f) - w 2^(-(A+B) f)          (2 FMUL, 2 SFU, 2 FMA), or
-                // the series folded per (segment, energy) into a polynomial in f,
-                //   f (m0 + f (m1 + f m2)) 2^(-A f),  m0 = nsig ln 2,
-                //   m1 = -m0 Bl / 2, m2 = m0 Bl^2 / 6, Bl = B ln 2
-                // (2 FMA, 2 FMUL, 1 SFU, 1 FMA; the D^3/24 term is below float
-                // rounding for D <= 0.01).
+                // This per-direction form serves directions that leave through
+                // both faces or spread too widely for the moment form.
                 const float mu2 = mu * 1.44269504f;
                 const float A_dn = mu2 * b.e1;
                 const float A_up = mu2 * b.e0;
                 const float B = mu2 * b.e2;
-                if (fast) {
-                    const float A = side_all > 0 ? A_up : A_dn;
-                    if (B * f_min_ln2 > 0.01f) {
-                        const float w = __fdividef(nsig, B);
-                        const float nA = -A, nC = -(A + B);
-#pragma unroll
-                        for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                            part[dd] = fmaf(w, ex2_approx(nA * fr[dd]), part[dd]);
-                            part[dd] = fmaf(-w, ex2_approx(nC * fr[dd]), part[dd]);
-                        }
-                    } else {
-                        const float m0 = nsig * 0.69314718f;
-                        const float Bl = B * 0.69314718f;
-                        const float m1 = -0.5f * m0 * Bl;
-                        const float m2 = m0 * Bl * Bl * (1.0f / 6.0f);
-                        const float nA = -A;
-#pragma unroll
-                        for (int dd = 0; dd < kBremMaxDir; ++dd) {
-                            const float f = fr[dd];
-                            const float t = fmaf(f, fmaf(f, m2, m1), m0) * f;
-                            part[dd] = fmaf(t, ex2_approx(nA * f), part[dd]);
-                        }
-                    }
-                } else {
+                {
                     const float w = B > 0.0f ? __fdividef(nsig, B) : 0.0f;
 #pragma unroll
                     for (int dd = 0; dd < kBremMaxDir; ++dd) {

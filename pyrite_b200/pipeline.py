@@ -274,20 +274,25 @@ class ScoringCase:
                 self.char_profiles.append(h.f64(profiles))
         self.histories = 0
 
-    def _cxr_args(self, rad: Radiator, n_hats, E_grid, cap):
-        """pb_cxr_args of one radiator over the case's segment buffer."""
+    def _cxr_args(self, rad: Radiator, n_hats, E_grid, cap, spec_out=None):
+        """pb_cxr_args of one radiator over the case's segment buffer; with
+        ``spec_out`` a separate argument set for the directions ``n_hats``
+        (a subset of the case's) writing into ``spec_out`` [len(n_hats), n_E]
+        with a far-field workspace of its own."""
         h, spec, st = self.h, self.spec, self.spec.stack
         rows = reflection_rows(rad.crystal, rad.hkl_list, n_hats, surface_hkl=rad.surface_hkl,
                                mosaic_fwhm_rad=rad.mosaic_fwhm_rad, mosaic_nodes=rad.mosaic_nodes,
                                recip_miscut_rad=rad.recip_miscut_rad)
-        self._rows = getattr(self, "_rows", []) + [rows]
+        if spec_out is None:
+            self._rows = getattr(self, "_rows", []) + [rows]
+        n_dir = int(np.atleast_2d(n_hats).shape[0])
         lo_keep, hi_keep = line_keep_window(E_grid)
         edges = energy_bin_edges(E_grid)
         c = L.PbCxrArgs()
         c.precision = self.precision
         c.quadrature = L.PB_QUAD_BINMEAN
-        c.n_dir = self.n_dir
-        c.n_hat = _ptr(self._n_hat_dev)
+        c.n_dir = n_dir
+        c.n_hat = _ptr(self._n_hat_dev) if spec_out is None else _ptr(h.f64(np.atleast_2d(n_hats)))
         c.thickness = st.thickness
         # Every streamed history radiates (elec_id < Ne for all of them).
         c.Ne = 1 << 62
@@ -320,12 +325,15 @@ class ScoringCase:
         if spec.exact_widths and spec.exact_widths > 0 and uniform:
             pad = int(np.ceil(max(edges[0] - lo_keep, hi_keep - edges[-1]) / w[0])) + 2
             c.exact_widths, c.far_pad = float(spec.exact_widths), pad
-            if self.far is None:  # shared by the radiators: each call clears it
-                self.far = h.zeros(self.n_dir * (self.n_E + 2 * pad) * 3, torch.float64)
-            c.far_moments = _ptr(self.far)
+            if spec_out is not None:
+                c.far_moments = _ptr(h.zeros(n_dir * (self.n_E + 2 * pad) * 3, torch.float64))
+            else:
+                if self.far is None:  # shared by the radiators: each call clears it
+                    self.far = h.zeros(self.n_dir * (self.n_E + 2 * pad) * 3, torch.float64)
+                c.far_moments = _ptr(self.far)
         else:
             c.exact_widths, c.far_pad = 0.0, -1
-        c.spec = _ptr(self.spec_cxr)
+        c.spec = _ptr(self.spec_cxr if spec_out is None else spec_out)
         c.status = _ptr(self.status)
         if self.layered:
             c.n_layer = st.n_layers
@@ -336,7 +344,7 @@ class ScoringCase:
         return c
 
     # -- one batch ---------------------------------------------------------
-    def use_surrogate(self, models, exact_stride=20):
+    def use_surrogate(self, models, exact_stride=20, tol=0.01, probe_batches=4):
         """Score PXR+CBS with an ensemble of trained surrogates plus an exact
         control variate, instead of the exact reflection sum on every segment.
 
@@ -348,8 +356,22 @@ class ScoringCase:
             S = S_sur(all) + stride (S_exact(sample) - S_sur(sample))
         is unbiased for the exact spectrum whatever the surrogate's error; the
         surrogate only has to make the sampled difference small. The result
-        lives on the coarse grid of the surrogate (``surrogate_spectrum``).
-        ``exact_stride=0`` uses the surrogate alone."""
+        lives on the coarse grid of the surrogate (``surrogate_spectrum``;
+        ``surrogate_spectrum_fine`` on the case's bins).
+        ``exact_stride=0`` uses the surrogate alone.
+
+        Error gate and fallback: after ``probe_batches`` batches (counted from
+        the last ``reset``) the error of the estimate is estimated per tile
+        from the batch-to-batch scatter of the sub-sample residuals
+        (``surrogate.control_variate_error``: three standard errors, worst
+        bin, relative to the tile's peak). Tiles above ``tol`` are scored by
+        the exact mixed scorer from then on, and the batches already run are
+        replayed (transport again from the same counter-based streams, no
+        tallies) so that those tiles' spectra cover the whole run exactly.
+        The decision stands across ``reset``. ``surrogate_report`` gives the
+        estimate, the fallback tiles and the run's audit: the surrogate alone
+        against the exact sum on the run's sub-sample (histories the training
+        never saw)."""
         from .detector import tile_uv
 
         if self.spec.detector is None or self.spec.angular_shape is None:
@@ -398,6 +420,17 @@ class ScoringCase:
             cs.spec = _ptr(self.spec_sample)
             self.cargs_s = cs
             self.sur_hsum_s, self.sur_lsum_s, self.sur_args_s = infer_set(self.smp, cap_s, self.smp["count"])
+        n_out = self.surrogates[0].n_out
+        self.sur_tol = float(tol)
+        self.sur_probe = max(2, int(probe_batches))
+        self.sur_checked = False
+        self.sur_estimate = None
+        self.sur_fallback = np.zeros(self.n_dir, dtype=bool)
+        self._fb_args = None
+        self._fb_spec = None
+        self._sur_res_prev = torch.zeros(self.n_dir, n_out, device=dev, dtype=torch.float64)
+        self._sur_res_sq = torch.zeros_like(self._sur_res_prev)
+        self._run_batches = []
 
     def _head(self, hsums, lsums):
         out = torch.zeros(self.n_dir, self.surrogates[0].n_out, device=self.device, dtype=torch.float64)
@@ -415,10 +448,96 @@ class ScoringCase:
 
     def surrogate_spectrum(self):
         """Surrogate (+ exact control variate) spectrum [n_dir, n_coarse] so far,
-        per history, in the exact scorer's units."""
+        per history, in the exact scorer's units; fallback tiles carry the
+        exact scorer's spectrum."""
+        s = self._cv_coarse()
+        if self._fb_args is not None:
+            s[self._fb_index] = self.coarse(self._fb_spec)
+        return s.cpu().numpy() / max(self.histories, 1)
+
+    def _cv_coarse(self):
         s = self._head(self.sur_hsum, self.sur_lsum)
         if self.sur_stride > 0:
             s += self.sur_stride * (self.coarse(self.spec_sample) - self._head(self.sur_hsum_s, self.sur_lsum_s))
+        return s
+
+    def surrogate_check(self):
+        """Estimate the control variate's error per tile now and move the
+        tiles above the tolerance to the exact scorer (replaying the batches
+        run since the last reset). Returns the per-tile estimate."""
+        from .surrogate import control_variate_error
+
+        B = len(self._run_batches)
+        est = control_variate_error(self._sur_res_prev.cpu().numpy(), self._sur_res_sq.cpu().numpy(), B,
+                                    self.sur_stride, self._cv_coarse().cpu().numpy())
+        if est is None:
+            return None
+        self.sur_estimate = est
+        self.sur_checked = True
+        new = (est > self.sur_tol) & ~self.sur_fallback
+        if np.any(new):
+            self._enable_fallback(self.sur_fallback | new)
+        return est
+
+    def _enable_fallback(self, flagged):
+        """Exact scoring of the tiles ``flagged`` on every segment from now
+        on, after replaying this run's batches for them."""
+        idx = np.flatnonzero(flagged)
+        n_hats = np.atleast_2d(np.asarray(self.spec.n_hats, dtype=float))[idx]
+        rad = Radiator(-1, self.spec.crystal, self.spec.hkl_list, self.spec.line_tables, self.spec.surface_hkl,
+                       None, self.spec.mosaic_fwhm_rad, self.spec.mosaic_nodes)
+        self._fb_spec = self.h.zeros((idx.size, self.n_E), torch.float64)
+        self._fb_args = self._cxr_args(rad, n_hats, np.asarray(self.spec.E_grid, dtype=np.float64),
+                                       self.seg_capacity, spec_out=self._fb_spec)
+        self._fb_index = torch.as_tensor(idx, device=self.device)
+        self.sur_fallback = np.asarray(flagged, dtype=bool).copy()
+        # Replay: the same histories transported again (counter-based
+        # streams give the same segments), tallies into scratch buffers.
+        ta = L.PbTransportArgs.from_buffer_copy(self.targs)
+        scratch = L.PbTallies.from_buffer_copy(self.targs.tallies)
+        self._replay_tallies = [self.h.zeros(tuple(t.shape), t.dtype) for t in (self.fates, self.exit_E,
+                                                                                self.exit_theta, self.deposit)]
+        scratch.fates, scratch.exit_E, scratch.exit_theta, scratch.deposit = (_ptr(t) for t in self._replay_tallies)
+        ta.tallies = scratch
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        for e_start, n in self._run_batches:
+            self.seg_count.zero_()
+            ta.e_start, ta.n = int(e_start), int(n)
+            L.check(self.lib.pb_transport(C.byref(ta), s), "pb_transport")
+            L.check(self.lib.pb_cxr_score(C.byref(self._fb_args), s), "pb_cxr_score")
+
+    def surrogate_report(self) -> dict:
+        """The run's error estimate per tile, the tiles on the exact
+        fallback, and the audit: the surrogate alone against the exact sum on
+        the run's sub-sample, max |difference| over bins relative to each
+        tile's peak."""
+        ex = self.coarse(self.spec_sample).cpu().numpy() if self.sur_stride > 0 else None
+        audit = None
+        if ex is not None and self.histories > 0:
+            su = self._head(self.sur_hsum_s, self.sur_lsum_s).cpu().numpy()
+            peak = np.max(np.abs(ex), axis=1)
+            audit = (np.max(np.abs(su - ex), axis=1) / np.where(peak > 0, peak, np.inf)).tolist()
+        return {"tolerance": self.sur_tol, "probe_batches": self.sur_probe, "checked": self.sur_checked,
+                "estimate_per_tile": None if self.sur_estimate is None else self.sur_estimate.tolist(),
+                "fallback_tiles": np.flatnonzero(self.sur_fallback).tolist(),
+                "audit_surrogate_alone_per_tile": audit}
+
+    def surrogate_spectrum_fine(self):
+        """Surrogate (+ exact control variate) spectrum on the case's own bins
+        [n_dir, n_E] so far, per history: each coarse surrogate value spread
+        over its fine bins (U), corrected by the exact sub-sample at full
+        resolution,
+            S = U(S_sur(all)) + stride (S_exact(sample) - U(S_sur(sample))),
+        unbiased for the exact fine-bin spectrum whatever U is. Inside a coarse
+        bin its noise is the exact sub-sample's: a segment's lines are much
+        narrower than a fine bin, which no smooth U follows."""
+        rep = self.n_E // self.surrogates[0].n_out
+        s = self._head(self.sur_hsum, self.sur_lsum).repeat_interleave(rep, dim=1)
+        if self.sur_stride > 0:
+            s += self.sur_stride * (self.spec_sample
+                                    - self._head(self.sur_hsum_s, self.sur_lsum_s).repeat_interleave(rep, dim=1))
+        if self._fb_args is not None:
+            s[self._fb_index] = self._fb_spec
         return s.cpu().numpy() / max(self.histories, 1)
 
     def run_batch(self, e_start: int, n: int, stream=None, events=None):
@@ -443,6 +562,14 @@ class ScoringCase:
                 events[4].record()  # exact sub-sample done; the surrogate follows
             for sa in self.sur_args + self.sur_args_s:
                 L.check(self.lib.pb_mlp_infer(C.byref(sa), s), "pb_mlp_infer")
+            if self.sur_stride > 0:
+                # this batch's sub-sample residual r_b = cumulative - previous
+                cur = self.coarse(self.spec_sample) - self._head(self.sur_hsum_s, self.sur_lsum_s)
+                r = cur - self._sur_res_prev
+                self._sur_res_sq.add_(r * r)
+                self._sur_res_prev.copy_(cur)
+            if self._fb_args is not None:
+                L.check(self.lib.pb_cxr_score(C.byref(self._fb_args), s), "pb_cxr_score")
         else:
             for ca in self.cargs_all:
                 L.check(self.lib.pb_cxr_score(C.byref(ca), s), "pb_cxr_score")
@@ -455,6 +582,10 @@ class ScoringCase:
         if events is not None:
             events[3].record()
         self.histories += int(n)
+        if getattr(self, "surrogates", None):
+            self._run_batches.append((int(e_start), int(n)))
+            if not self.sur_checked and self.sur_stride > 0 and len(self._run_batches) >= self.sur_probe:
+                self.surrogate_check()
 
     def kernel_launches_per_batch(self) -> int:
         """This library's kernels launched per batch (transport 1, CXR 2 with
@@ -463,6 +594,9 @@ class ScoringCase:
             n = 1 + len(self.surrogates) * (2 if self.sur_stride > 0 else 1)
             if self.sur_stride > 0:
                 n += 1 + 1 + (1 if self.cargs.exact_widths > 0 else 0)
+                n += len(self.surrogates)  # pb_mlp_head of the sub-sample residual
+            if self._fb_args is not None:
+                n += 1 + (1 if self._fb_args.exact_widths > 0 else 0)
         else:
             n = 1 + sum(1 + (1 if ca.exact_widths > 0 else 0) for ca in self.cargs_all)
         n += len(self.bargs_all) * ((self.n_dir + 15) // 16)
@@ -475,8 +609,10 @@ class ScoringCase:
     def results(self) -> dict:
         """Normalised spectra [photons/eV/sr/electron] and tallies so far."""
         Ne = max(self.histories, 1)
+        sur = getattr(self, "surrogates", None)
         out = {
-            "cxr": self.spec_cxr.cpu().numpy() / Ne,
+            # with the surrogate: its control-variate estimate on the case's bins
+            "cxr": self.surrogate_spectrum_fine() if sur else self.spec_cxr.cpu().numpy() / Ne,
             "fates": self.fates.cpu().numpy(),
             "exit_E": self.exit_E.cpu().numpy(),
             "exit_theta": self.exit_theta.cpu().numpy(),
@@ -517,6 +653,12 @@ class ScoringCase:
             t.zero_()
         if getattr(self, "spec_sample", None) is not None:
             self.spec_sample.zero_()
+        if getattr(self, "surrogates", None):
+            self._sur_res_prev.zero_()
+            self._sur_res_sq.zero_()
+            self._run_batches = []
+            if self._fb_spec is not None:
+                self._fb_spec.zero_()
         if self.bargs is not None:
             self.spec_brem.zero_()
         for y in self.char_yields:

@@ -21,3 +21,11 @@ def test_spectrum_error_stats():
     # an all-zero tile does not divide by zero
     ref2 = np.vstack([ref, np.zeros(4)])
     assert np.isfinite(list(bench.spectrum_error_stats(ref2, ref2).values())).all()
+
+
+def test_sigma_stats():
+    ref = np.array([[1.0, 2.0, 4.0, 1e-6]])
+    sigma = np.array([[0.1, 0.1, 0.2, 1e-9]])
+    got = ref + np.array([[0.05, 0.35, -0.2, 1.0]])  # 0.5, 3.5, 1.0 sigma; the last bin is below the floor
+    s = bench.sigma_stats(got, ref, sigma)
+    assert s["bins"] == 3 and np.isclose(s["max"], 3.5) and np.isclose(s["within_3_sigma"], 2 / 3)

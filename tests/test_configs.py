@@ -47,3 +47,27 @@ def test_sweep_case_spec_matches_its_configuration():
         assert np.isclose(s.beam.tilt_polar_rad, np.deg2rad(cfg.tilt_deg))
         assert s.E_grid.size == 1024 and s.E_grid[0] == 1000.0 and s.E_grid[-1] == 60000.0
         assert s.crystal.name in ("silicon", "hopg")
+
+
+def test_host_beam_entries_have_the_scene_spot_and_divergence():
+    """oracle.beam_entries (the CPU baseline's entrance states) follows the
+    50 MeV Si scene's Twiss beam: spot sigma 1 mm and divergence 0.2 mrad
+    per plane (4,000 histories: within 5 %), on the tilted entrance face."""
+    import oracle
+    from pyrite_b200 import configs
+    from pyrite_b200.api import _fill_beam
+    from pyrite_b200.tables import beam_frame_basis
+
+    spec = configs.c2_si_50mev(seed=3)
+    beam = _fill_beam(None, spec.beam, spec.seed)
+    pos, dirs, E = oracle.beam_entries(beam, 0, 4000, rng=1)
+    assert np.all(pos[:, 2] == 0.0) and np.all(E == spec.beam.E0_keV)
+    np.testing.assert_allclose(np.linalg.norm(dirs, axis=1), 1.0, rtol=1e-15)
+    B = beam_frame_basis(np.asarray(spec.beam.beam_dir, float))
+    xp, yp = dirs @ B[:, 0], dirs @ B[:, 1]
+    assert abs(np.std(xp) / 0.2e-3 - 1.0) < 0.05 and abs(np.std(yp) / 0.2e-3 - 1.0) < 0.05
+    # transverse offsets: the entry points seen along the beam (perpendicular plane)
+    bd = np.asarray(spec.beam.beam_dir, float)
+    perp = pos - np.outer(pos @ bd, bd)
+    assert abs(np.std(perp @ B[:, 0]) / 1.0e7 - 1.0) < 0.05
+    assert abs(np.std(perp @ B[:, 1]) / 1.0e7 - 1.0) < 0.05

@@ -253,3 +253,70 @@ def test_single_tile_inference_variant_matches_torch(cuda_device):
                        cwd=root, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "1 passed" in r.stdout
+
+
+def test_error_gate_falls_back_to_the_exact_scorer(cuda_device):
+    """A barely trained surrogate under a tolerance no control variate can
+    meet (1e-6): after the probe batches every tile moves to the exact
+    scorer, the batches already run are replayed for it, and the run's
+    spectrum equals the exact mixed scorer's on the same histories (1e-12 of
+    the peak: the same kernel, FP64 block sums added in another order); the
+    replay leaves the tallies counted once."""
+    from pyrite_b200 import configs
+    from pyrite_b200 import surrogate as S
+    from pyrite_b200.pipeline import ScoringCase
+
+    spec = configs.c2_si_50mev(seed=7)
+    data = S.make_training_set(spec, n_seg=1024, n_dir=16, dir_chunk=16, seed=3, device=cuda_device)
+    model = S.Surrogate(cuda_device, seed=0)
+    model.train(data, epochs=1, batch=1024)
+    H = 2048
+    ce = ScoringCase(spec, precision="mixed", batch_histories=H, device=cuda_device)
+    cs = ScoringCase(spec, precision="mixed", batch_histories=H, device=cuda_device)
+    cs.use_surrogate([model], exact_stride=8, tol=1e-6, probe_batches=3)
+    for i in range(5):
+        ce.run_batch(i * H, H)
+        cs.run_batch(i * H, H)
+    rep = cs.surrogate_report()
+    assert rep["checked"] and rep["fallback_tiles"] == list(range(cs.n_dir))
+    assert all(e > 1e-6 for e in rep["estimate_per_tile"])
+    got, ref = cs.results(), ce.results()
+    peak = np.max(np.abs(ref["cxr"]))
+    assert peak > 0
+    assert np.max(np.abs(got["cxr"] - ref["cxr"])) <= 1e-12 * peak
+    coarse_ref = ref["cxr"].reshape(cs.n_dir, model.n_out, -1).mean(-1)
+    assert np.max(np.abs(cs.surrogate_spectrum() - coarse_ref)) <= 1e-12 * peak
+    for k in ("fates", "exit_E", "exit_theta"):
+        np.testing.assert_array_equal(got[k], ref[k])
+    assert cs.device_status() == 0
+
+
+def test_error_gate_keeps_a_trained_surrogate(cuda_device):
+    """A briefly trained surrogate (2 epochs on 131k pairs) on 65,536
+    histories under a 5 % tolerance: every tile's estimated error is below
+    it, no tile falls back, and the estimate bounds the actual worst-bin
+    error against the exact scorer on the same histories for most tiles.
+    The run's audit (surrogate alone on the sub-sample) is reported."""
+    from pyrite_b200 import configs
+    from pyrite_b200 import surrogate as S
+    from pyrite_b200.pipeline import ScoringCase
+
+    spec = configs.c2_si_50mev(seed=7)
+    data = S.make_training_set(spec, n_seg=2048, n_dir=64, dir_chunk=64, seed=3, device=cuda_device)
+    model = S.Surrogate(cuda_device, seed=0)
+    model.train(data, epochs=2, batch=4096)
+    H = 16384
+    ce = ScoringCase(spec, precision="mixed", batch_histories=H, device=cuda_device)
+    cs = ScoringCase(spec, precision="mixed", batch_histories=H, device=cuda_device)
+    cs.use_surrogate([model], exact_stride=8, tol=0.05, probe_batches=4)
+    for i in range(4):
+        ce.run_batch(i * H, H)
+        cs.run_batch(i * H, H)
+    rep = cs.surrogate_report()
+    est = np.array(rep["estimate_per_tile"])
+    assert rep["checked"] and rep["fallback_tiles"] == [], est
+    exact = ce.results()["cxr"].reshape(cs.n_dir, model.n_out, -1).mean(-1)
+    actual = np.max(np.abs(cs.surrogate_spectrum() - exact), axis=1) / np.max(np.abs(exact), axis=1)
+    assert np.mean(actual <= est) >= 0.75, (actual, est)
+    audit = np.array(rep["audit_surrogate_alone_per_tile"])
+    assert np.all((audit > 0) & (audit < 1)), audit

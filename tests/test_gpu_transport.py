@@ -112,3 +112,32 @@ def test_mixed_precision_statistics(cuda_device):
     na = np.array([a["n_backscattered"], a["n_transmitted"], a["n_cutoff_stopped"]], float)
     nb = np.array([b["n_backscattered"], b["n_transmitted"], b["n_cutoff_stopped"]], float)
     assert np.all(np.abs(na - nb) < 4 * np.sqrt(na + nb + 1))
+
+
+def test_twiss_entries_match_the_host_restatement(cuda_device):
+    """The device's Twiss entrance sampling (sample_entry) and the oracle's
+    host restatement (oracle.beam_entries, scipy ndtri for CUDA's normcdfinv)
+    give the same first segments for the 50 MeV Si scene's beam: transport
+    from the sampled beam and from the host entries as explicit states agree
+    to 1e-12 on every history's first segment."""
+    import oracle
+    from pyrite_b200 import configs, simulate_trajectories
+    from pyrite_b200.api import _fill_beam
+
+    spec = configs.c2_si_50mev(seed=12345)
+    tw = spec.beam.twiss_x
+    n = 256
+    kw = dict(E0_keV=spec.beam.E0_keV, Ne=n, layers=[(0.0, 5.0e6, [("Si", 0.04994)])], E_cut_keV=5.0,
+              seed=spec.seed, beam_dir=spec.beam.beam_dir, tilt_polar_rad=spec.beam.tilt_polar_rad,
+              rng="philox", lut=True, precision="fp64", device=cuda_device)
+    got = simulate_trajectories(transverse_distribution={"x": tw, "y": tw}, **kw)
+    beam = _fill_beam(None, spec.beam, spec.seed)
+    entry = oracle.beam_entries(beam, 0, n, rng=1)
+    ref = simulate_trajectories(entry=entry, **kw)
+    first_g = {int(e): i for i, e in reversed(list(enumerate(got["elec_id"])))}
+    first_r = {int(e): i for i, e in reversed(list(enumerate(ref["elec_id"])))}
+    assert set(first_g) == set(first_r) == set(range(n))
+    for e in range(n):
+        i, j = first_g[e], first_r[e]
+        np.testing.assert_allclose(got["r_mid"][i], ref["r_mid"][j], rtol=1e-12, atol=1e-6)
+        np.testing.assert_allclose(got["v_hat"][i], ref["v_hat"][j], rtol=1e-12, atol=1e-15)
