@@ -31,12 +31,20 @@ import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-DEFAULT_REFERENCE = Path(os.environ.get("PYRITE_REFERENCE_ROOT", "/root/reference"))
 _NON_P1 = ("gep", "ges", "gese", "gese2")
 
 
-def reference_available(root: Path = DEFAULT_REFERENCE) -> bool:
-    return (root / "src" / "pyrite" / "__init__.py").is_file()
+def _root(root) -> Path | None:
+    """The reference tree: the ``root`` argument, else $PYRITE_REFERENCE_ROOT."""
+    if root is None:
+        env = os.environ.get("PYRITE_REFERENCE_ROOT")
+        return Path(env) if env else None
+    return Path(root)
+
+
+def reference_available(root=None) -> bool:
+    r = _root(root)
+    return r is not None and (r / "src" / "pyrite" / "__init__.py").is_file()
 
 
 def _trimmed_catalog(root: Path) -> Path:
@@ -53,10 +61,13 @@ def _trimmed_catalog(root: Path) -> Path:
     return dst
 
 
-def import_reference(root: Path = DEFAULT_REFERENCE):
-    """Return the reference ``pyrite`` package, imported through the stand-ins."""
+def import_reference(root=None):
+    """Return the reference ``pyrite`` package, imported through the stand-ins.
+    ``root`` is the reference tree (or set $PYRITE_REFERENCE_ROOT)."""
     if not reference_available(root):
-        raise RuntimeError(f"reference tree not found under {root}")
+        raise RuntimeError(f"reference tree not found (root={root!r}, PYRITE_REFERENCE_ROOT="
+                           f"{os.environ.get('PYRITE_REFERENCE_ROOT')!r})")
+    root = _root(root)
     os.environ["PYRITE_MC_BACKEND"] = "cpu"
     os.environ["PYRITE_MATH"] = "reproducible"
     os.environ.setdefault("NUMBA_NUM_THREADS", "1")

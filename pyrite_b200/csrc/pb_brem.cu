@@ -83,6 +83,19 @@ __device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsig
     return d;
 }
 
+// Reciprocal square root and base-2 logarithm on the SFU, denormals
+// flushed (the float path's arguments are normal numbers).
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Reciprocal on the SFU (about 1 ulp), for the float path.
 __device__ __forceinline__ float rcp_approx(float x) {
     float y;
@@ -170,10 +183,12 @@ struct BremKConst {
 //   (p_i^2 - p_f^2 = k (T + T_f + 2 m c^2) / (m c^2)^2, without cancellation),
 // so one (segment, energy) costs five SFU operations (rsqrt, rcp, lg2, and
 // ex2 + rcp per element of the Elwert factor).
-template <class Real>
-__device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T_f, const Real *Zs, int n_el,
+template <class Real, int NEL = 0>
+__device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T_f, const Real *Zs, int n_el_rt,
                                           Real k_ev, Real c0, Real za, Real mc2, const BremKConst &kk,
                                           const float *zl) {
+    // NEL > 0: the element count known at compile time (loops unrolled).
+    const int n_el = NEL > 0 ? NEL : n_el_rt;
     Real nsig = 0;
     if constexpr (sizeof(Real) == 8) {
         const Real p_f = b_sqrt(T_f * (T_f + (Real)2 * mc2)) / mc2;
@@ -188,14 +203,16 @@ __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T
     } else {
         const float inv_mc2 = 1.0f / 510.99895f;
         const float q = T_f * (T_f + 2.0f * mc2);
-        const float rs = rsqrtf(q);
+        const float rs = rsqrt_approx(q);
         const float p_f = q * rs * inv_mc2;
         const float sp = b.p_i + p_f;
         const float dpp = kk.kc * fmaf(2.0f, b.T, kk.c2mk);  // p_i^2 - p_f^2
-        const float lg = __log2f(fmaxf(sp * sp * rcp_approx(fmaxf(dpp, 1e-30f)), 1e-30f));
+        const float lg = lg2_approx(fmaxf(sp * sp * rcp_approx(fmaxf(dpp, 1e-30f)), 1e-30f));
         const float inv_beta_f = fmaf(T_f, inv_mc2, 1.0f) * (rs * mc2);
         const float common = kk.c0k * b.beta_i * lg * inv_beta_f;  // beta_i holds beta_i / p_i^2
-        for (int el = 0; el < n_el; ++el) {
+#pragma unroll
+        for (int el = 0; el < (NEL > 0 ? NEL : kBremMaxEl); ++el) {
+            if (NEL == 0 && el >= n_el) break;
             const float den_f = 1.0f - ex2_approx(-zl[el] * inv_beta_f);
             nsig = fmaf(b.nL[el] * common, rcp_approx(den_f), nsig);  // nL holds n L Z^2 den_i
         }
@@ -232,8 +249,8 @@ __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T
 // Truncation after order N: the remainder of the Taylor series is at most
 // about rho^(N+1) / sqrt(2 pi (N+1)) of the unattenuated term, rho = Delta /
 // f_min, whatever the optical depths (the attenuation exp(-a f_min) bounds the
-// growth of the derivatives); the host-side choice N = 3 for rho <= 0.01 and
-// N = 7 for rho <= 0.1 keeps it below 3e-9.
+// growth of the derivatives); the choice N = 3 for rho <= 0.01 and N = 5 for
+// rho <= 0.05 keeps it below 3e-9.
 // ---------------------------------------------------------------------------
 struct BremMomentConst {
     float mu_l2fc;  // mu log2(e) f_c
@@ -243,7 +260,7 @@ struct BremMomentConst {
     float f_c, dl;  // f_c, Delta
 };
 
-template <int N>
+template <int N, int NEL>
 __device__ __forceinline__ void brem_moment_chunk(const BremSeg<float> *segs, int nc, bool up, float k,
                                                   const float *Zs, int n_el, float k_ev, float c0, float za,
                                                   float mc2, const BremKConst &kk, const float *zl,
@@ -252,7 +269,7 @@ __device__ __forceinline__ void brem_moment_chunk(const BremSeg<float> *segs, in
         const BremSeg<float> &b = segs[j];
         const float T_f = b.T - k;
         if (!(T_f > 1e-6f && k > 0.0f)) continue;
-        const float nsig = brem_nsig<float>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
+        const float nsig = brem_nsig<float, NEL>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
         const float es = up ? b.e0 : b.e1;
         const float ef = es + b.e2;
         const float Ea = ex2_approx(-m.mu_l2fc * es);
@@ -286,7 +303,7 @@ __device__ __forceinline__ float brem_moment_eval(const float (&Q)[N + 1], float
     return r;
 }
 
-template <class Real>
+template <class Real, int NEL>
 __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
     // Segment chunk staged in shared memory (half as many FP64 segments, to
@@ -327,7 +344,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         side_all = n_up == nd ? 1 : (n_up == 0 ? -1 : 0);
     }
     // Moment form (see brem_moment_chunk): float, one exit face, and the
-    // path factors within rho = Delta / f_min <= 0.1 of their centre.
+    // path factors within rho = Delta / f_min <= 0.05 of their centre.
     __shared__ float mom_h[kBremMaxDir];     // (f_d - f_c) / Delta
     __shared__ float mom_invf[kBremMaxDir];  // 1 / f_d
     int order = -1;
@@ -342,7 +359,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         f_c = 0.5 * (f_lo + f_hi);
         dl = 0.5 * (f_hi - f_lo);
         const double rho = dl / f_lo;
-        order = dl == 0.0 ? 0 : (rho <= 0.01 ? 3 : (rho <= 0.1 ? 7 : -1));
+        order = dl == 0.0 ? 0 : (rho <= 0.01 ? 3 : (rho <= 0.05 ? 5 : -1));
         if (threadIdx.x < nd) {
             const double f = 1.0 / fmax(fabs(a.n_hat[3 * (d0 + threadIdx.x) + 2]), 1.0e-12);
             mom_h[threadIdx.x] = dl > 0.0 ? (float)((f - f_c) / dl) : 0.0f;
@@ -364,7 +381,9 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         const int64_t live = (int64_t)*a.n_seg_device;
         if (live < n_seg) n_seg = live;
     }
-    const int64_t per = (a.n_seg + gridDim.y - 1) / gridDim.y;
+    // Slices of the live segments (the count read on the device), so every
+    // block of the wave has work.
+    const int64_t per = (n_seg + gridDim.y - 1) / gridDim.y;
     const int64_t s_begin = per * blockIdx.y;
     int64_t s_end = s_begin + per < n_seg ? s_begin + per : n_seg;
     if (s_end < s_begin) s_end = s_begin;
@@ -388,19 +407,19 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
                 const bool up_all = side_all > 0;
                 if (order == 0) {
                     float Q[1] = {0.0f};
-                    brem_moment_chunk<0>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    brem_moment_chunk<0, NEL>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
                     for (int dd = 0; dd < nd; ++dd)
                         acc[dd][threadIdx.x] += (double)Q[0] * (double)mom_invf[dd];
                 } else if (order == 3) {
                     float Q[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                    brem_moment_chunk<3>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    brem_moment_chunk<3, NEL>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
                     for (int dd = 0; dd < nd; ++dd)
                         acc[dd][threadIdx.x] += (double)brem_moment_eval<3>(Q, mom_h[dd]) * (double)mom_invf[dd];
                 } else {
-                    float Q[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                    brem_moment_chunk<7>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
+                    float Q[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    brem_moment_chunk<5, NEL>(segs, nc, up_all, k, Zs, n_el, k_ev, c0, za, mc2, kk, zl, m, Q);
                     for (int dd = 0; dd < nd; ++dd)
-                        acc[dd][threadIdx.x] += (double)brem_moment_eval<7>(Q, mom_h[dd]) * (double)mom_invf[dd];
+                        acc[dd][threadIdx.x] += (double)brem_moment_eval<5>(Q, mom_h[dd]) * (double)mom_invf[dd];
                 }
                 continue;
             }
@@ -414,7 +433,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
             const BremSeg<Real> &b = segs[j];
             const Real T_f = b.T - k;
             if (!(T_f > (Real)1e-6 && k > (Real)0)) continue;
-            const Real nsig = brem_nsig<Real>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
+            const Real nsig = brem_nsig<Real, NEL>(b, k, T_f, Zs, n_el, k_ev, c0, za, mc2, kk, zl);
             if constexpr (sizeof(Real) == 8) {
 #pragma unroll
                 for (int dd = 0; dd < kBremMaxDir; ++dd) {
@@ -567,7 +586,9 @@ __global__ void __launch_bounds__(kBremThreads) brem_layered_kernel(const pb_bre
         const int64_t live = (int64_t)*a.n_seg_device;
         if (live < n_seg) n_seg = live;
     }
-    const int64_t per = (a.n_seg + gridDim.y - 1) / gridDim.y;
+    // Slices of the live segments (the count read on the device), so every
+    // block of the wave has work.
+    const int64_t per = (n_seg + gridDim.y - 1) / gridDim.y;
     const int64_t s_begin = per * blockIdx.y;
     int64_t s_end = s_begin + per < n_seg ? s_begin + per : n_seg;
     if (s_end < s_begin) s_end = s_begin;
@@ -660,10 +681,20 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     int64_t n_seg = a.n_seg;
     const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
     // One wave: as many segment slices as keep every SM at its resident limit.
+    // The kernel instance for this element count (loops over elements unrolled).
+    using Kern = void (*)(const pb_brem_args, int64_t, int);
+    Kern kern = nullptr;
+    if (a.precision == PB_MIXED) {
+        const Kern t[kBremMaxEl] = {brem_kernel<float, 1>, brem_kernel<float, 2>, brem_kernel<float, 3>,
+                                    brem_kernel<float, 4>};
+        kern = t[a.n_el - 1];
+    } else {
+        const Kern t[kBremMaxEl] = {brem_kernel<double, 1>, brem_kernel<double, 2>, brem_kernel<double, 3>,
+                                    brem_kernel<double, 4>};
+        kern = t[a.n_el - 1];
+    }
     int per_sm = 0;
-    cudaError_t oe = a.precision == PB_MIXED
-                         ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_kernel<float>, kBremThreads, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, brem_kernel<double>, kBremThreads, 0);
+    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBremThreads, 0);
     if (oe != cudaSuccess) return oe;
     if (per_sm < 1) per_sm = 1;
     int64_t gy = (int64_t)sms * per_sm / (int64_t)gx;
@@ -672,8 +703,7 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     if (gy < 1) gy = 1;
     dim3 grid(gx, (unsigned)gy, 1);
     for (int d0 = 0; d0 < a.n_dir; d0 += kBremMaxDir) {
-        if (a.precision == PB_MIXED) brem_kernel<float><<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
-        else brem_kernel<double><<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
+        kern<<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }

@@ -18,6 +18,7 @@ the reference's.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -29,7 +30,10 @@ sys.path.insert(0, str(ROOT))
 
 from oracle.ref_harness import import_reference  # noqa: E402
 
-import_reference()
+# The reference tree this recipe reads: $PYRITE_REFERENCE_ROOT, else the
+# read-only mount of the build container.
+REFERENCE_ROOT = Path(os.environ.get("PYRITE_REFERENCE_ROOT", "/root/reference"))
+import_reference(REFERENCE_ROOT)
 
 from pyrite.montecarlo import geometry as ref_geometry  # noqa: E402
 from pyrite.montecarlo.transport import TransportLUTConfig, _simulate_trajectories  # noqa: E402
@@ -949,6 +953,105 @@ def gen_coherent_decoherence():
     )
 
 
+# ---------------------------------------------------------------------------
+# Full run (statistical pin): the 20 MeV HOPG scene with its Twiss beam through
+# the reference's per-electron core, then PXR/CBS bin means, Bethe-Heitler and
+# the exit / fate / depth-loss summaries, in electron groups so the tests can
+# form the reference's own statistical error (batch means).
+# ---------------------------------------------------------------------------
+FULLRUN = dict(E0_keV=20000.0, Ne=20000, groups=10, seed=11, thickness=1.0e6, n_C=0.1133, tilt_deg=45.0,
+               theta_obs_deg=90.0, sigma_mm=0.5, sigma_prime_rad=0.5e-3,
+               E_grid=np.arange(1000.0, 40000.0 + 1e-6, 50.0), exit_E_bins=64, exit_theta_bins=36,
+               depth_bins=10)
+
+
+def gen_fullrun():
+    from pyrite.materials.crystal import CRYSTALS, reciprocal_g_vector
+    from pyrite.montecarlo import trajectory_summary as ts
+    from pyrite.montecarlo.spectrum import brem as ref_brem
+    from pyrite.montecarlo.spectrum.cxr import _batched, _setup
+    from pyrite.montecarlo.spectrum.cxr._spectrum import mc_cxr_spectrum
+    from dataclasses import asdict
+
+    from pyrite.montecarlo.transverse import TransverseDistribution, resolve_transverse_distribution
+
+    c = FULLRUN
+    E0 = c["E0_keV"]
+    bg = float(np.sqrt((1.0 + E0 / 510.99895) ** 2 - 1.0))
+    eps_n = c["sigma_mm"] * c["sigma_prime_rad"] * bg * 1e3  # mm mrad
+    beta_m = c["sigma_mm"] / c["sigma_prime_rad"] * 1e-3
+    tp = np.deg2rad(c["tilt_deg"])
+    beam_dir, n_hat = ref_geometry.tilted_geometry(np.deg2rad(c["theta_obs_deg"]), tp, 0.0)
+    out = _simulate_trajectories(
+        E0_keV=E0, Ne=c["Ne"], thickness_ang=c["thickness"], composition=[("C", c["n_C"])], seed=c["seed"],
+        elastic_model="sr", transport_core="per-electron", radiative_model="uncoupled", beam_dir=beam_dir,
+        tilt_polar_rad=tp,
+        transverse_distribution=asdict(resolve_transverse_distribution(TransverseDistribution(eps_n, beta_m),
+                                                                       energy_keV=E0)),
+        transport_lut_config=TransportLUTConfig(enabled=True))
+    hkl = [(0, 0, l) for l in range(-8, 9) if l != 0]
+    info = CRYSTALS["hopg"]
+    g_mags = np.array([reciprocal_g_vector(h, info["lattice"])[1] for h in hkl])
+    E_grid = c["E_grid"]
+    E_tab = synthetic_E_tab(E_grid)
+    comp = [("C", c["n_C"])]
+    tables = synthetic_couplings(g_mags, E_tab)
+    mosaic = np.deg2rad(0.4 * 2.3548200450309493)
+    patches = [
+        (_setup, "_line_tabulation_grid", lambda *a, **k: E_tab),
+        (_setup, "_elemental_log_mu_table", lambda cc, E: synthetic_log_mu(cc, E)),
+        (_setup, "refractive_index", lambda cr, E, uh=True: (1.0 - synthetic_delta(E)) + 0j),
+        (_batched, "_reflection_tables", lambda *a, **k: tuple(np.array(t) for t in tables)),
+    ]
+    saved = [(m, n, getattr(m, n)) for m, n, _ in patches]
+    for m, n, f in patches:
+        setattr(m, n, f)
+    saved_mu = ref_brem._mu_total_inv_ang
+    ref_brem._mu_total_inv_ang = lambda cc, E: synthetic_mu_total(cc, np.asarray(E, dtype=float))
+    K, Ne = c["groups"], c["Ne"]
+    per = Ne // K
+    eid = np.asarray(out["elec_id"])
+    E_edges = np.linspace(0.0, E0, c["exit_E_bins"] + 1)
+    th_edges = np.linspace(0.0, np.pi, c["exit_theta_bins"] + 1)
+    depth_edges = np.linspace(0.0, c["thickness"], c["depth_bins"] + 1)
+    cxr, brem, exE, exT, fates, dep = [], [], [], [], [], []
+    try:
+        for g in range(K):
+            m = (eid >= g * per) & (eid < (g + 1) * per)
+            seg = {k: np.asarray(out[k])[m] for k in ("r_mid", "v_hat", "L_ang", "E_keV", "E_repr_keV")}
+            seg["elec_id"] = eid[m] - g * per
+            seg["Ne"], seg["thickness_ang"] = per, c["thickness"]
+            cxr.append(np.asarray(mc_cxr_spectrum(
+                seg, E_grid, crystal="hopg", hkl_list=hkl, B_ang2=float(info.get("B_ang2", 0.0) or 0.0),
+                absorber_element="C", n_hat=n_hat, surface_hkl=(0, 0, 1), mosaic_fwhm_rad=mosaic, mosaic_nodes=3,
+                node_support_cutoff=None, line_quadrature="bin-mean")))
+            brem.append(np.asarray(ref_brem.mc_brem_spectrum(seg, E_grid, composition=comp, n_hat=n_hat,
+                                                             cross_section_model="bethe-heitler")))
+            block = {k: np.asarray(out[k])[m] for k in ("r_mid", "L_ang", "v_hat", "E_start_keV", "E_end_keV",
+                                                        "event_kind", "flight_id", "substep_id", "layer")}
+            block["electron_id"] = eid[m]
+            rows = ts._history_rows(block)
+            names = ("backscattered", "transmitted", "side_exited", "cutoff_stopped")
+            fates.append([sum(1 for r in rows if r[1] == n) for n in names])
+            esc = [r for r in rows if r[1] in names[:3]]
+            exE.append(ts._histogram(np.array([r[4] for r in esc]), E_edges))
+            exT.append(ts._histogram(np.array([r[5] for r in esc]), th_edges))
+            prof = ts.depth_loss_profile(block, depth_edges)
+            dep.append(prof["continuous_loss_keV"].to_numpy() / per)
+    finally:
+        for m_, n_, f_ in saved:
+            setattr(m_, n_, f_)
+        ref_brem._mu_total_inv_ang = saved_mu
+    _save("fullrun_hopg20", E0_keV=E0, Ne=Ne, groups=K, seed=c["seed"], thickness=c["thickness"], n_C=c["n_C"],
+          tilt_deg=c["tilt_deg"], beam_dir=beam_dir, n_hat=n_hat, eps_n_mm_mrad=eps_n, beta_m=beta_m,
+          hkl=np.array(hkl), mosaic_fwhm_rad=mosaic, E_grid=E_grid, E_tab=E_tab, delta=synthetic_delta(E_tab),
+          log_mu=synthetic_log_mu(comp, E_tab), chi_re=tables[0], chi_im=tables[1], u_re=tables[2],
+          u_im=tables[3], mu_grid=synthetic_mu_total(comp, E_grid), E_edges=E_edges, theta_edges=th_edges,
+          depth_edges=depth_edges, cxr=np.array(cxr), brem=np.array(brem), exit_E=np.array(exE),
+          exit_theta=np.array(exT), fates=np.array(fates), depth_loss=np.array(dep),
+          fate_names=np.array(["backscattered", "transmitted", "side_exited", "cutoff_stopped"]))
+
+
 GENERATORS = {
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
@@ -961,6 +1064,7 @@ GENERATORS = {
     "layered": gen_layered,
     "coherent": gen_coherent,
     "coherent_decoherence": gen_coherent_decoherence,
+    "fullrun": gen_fullrun,
 }
 
 

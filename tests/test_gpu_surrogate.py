@@ -259,9 +259,12 @@ def test_error_gate_falls_back_to_the_exact_scorer(cuda_device):
     """A barely trained surrogate under a tolerance no control variate can
     meet (1e-6): after the probe batches every tile moves to the exact
     scorer, the batches already run are replayed for it, and the run's
-    spectrum equals the exact mixed scorer's on the same histories (1e-12 of
-    the peak: the same kernel, FP64 block sums added in another order); the
-    replay leaves the tallies counted once."""
+    spectrum equals the exact mixed scorer's on the same histories, within
+    1e-8 of the peak: the same kernel on the same segments, but the mixed
+    scorer sums FP32 partials with shared-memory atomics and the transport
+    appends segments in warp-atomic order, so the float sums group
+    differently from run to run (measured 1e-9); the replay leaves the
+    tallies counted once."""
     from pyrite_b200 import configs
     from pyrite_b200 import surrogate as S
     from pyrite_b200.pipeline import ScoringCase
@@ -283,9 +286,9 @@ def test_error_gate_falls_back_to_the_exact_scorer(cuda_device):
     got, ref = cs.results(), ce.results()
     peak = np.max(np.abs(ref["cxr"]))
     assert peak > 0
-    assert np.max(np.abs(got["cxr"] - ref["cxr"])) <= 1e-12 * peak
+    assert np.max(np.abs(got["cxr"] - ref["cxr"])) <= 1e-8 * peak
     coarse_ref = ref["cxr"].reshape(cs.n_dir, model.n_out, -1).mean(-1)
-    assert np.max(np.abs(cs.surrogate_spectrum() - coarse_ref)) <= 1e-12 * peak
+    assert np.max(np.abs(cs.surrogate_spectrum() - coarse_ref)) <= 1e-8 * peak
     for k in ("fates", "exit_E", "exit_theta"):
         np.testing.assert_array_equal(got[k], ref[k])
     assert cs.device_status() == 0
