@@ -577,6 +577,7 @@ def main():
         torch.cuda.synchronize()
         out = {"res": case.results(), "status": case.device_status()}
         if getattr(case, "surrogates", None):
+            out["report"] = case.surrogate_report()  # the probe ran on these batches
             out["sur_coarse"] = case.surrogate_spectrum()
             out["sur_fine"] = case.surrogate_spectrum_fine()
             out["sur_alone"] = case._head(case.sur_hsum, case.sur_lsum).cpu().numpy() / max(case.histories, 1)
@@ -616,7 +617,7 @@ def main():
         cs = ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H)
         cs.use_surrogate([model], exact_stride=args.exact_stride)
         compare_pass("surrogate", cs)
-        gate_report = cs.surrogate_report()  # the probe ran inside the comparison pass
+        gate_report = compare["surrogate"]["report"]
         arm("surrogate", cs, args.steps)
         sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
                "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,

@@ -182,7 +182,7 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
                           composition=None, layers=None, beam_fwhm_mm=None, beam_fwhm_y_mm=None,
                           tilt_polar_rad=0.0, tilt_azim_rad=0.0, transverse_distribution=None,
                           *, lut=True, rng="splitmix", precision="fp64", entry=None, cap=None,
-                          device=None, stream=None, block_threads=0):
+                          device=None, stream=None, block_threads=0, tallies=None):
     """Transport ``Ne`` electrons into a slab or layer stack; returns segment rows.
 
     Same contract as the reference's per-electron cores: rows of history i
@@ -191,6 +191,14 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     reference's SplitMix64 counter stream (draw-for-draw compatible) or
     Philox4x32-10; ``precision`` "fp64" or "mixed". ``entry`` replaces the
     sampled entrance state with explicit (pos, dir, E) arrays.
+
+    ``tallies=(n_E, n_theta)`` also returns the kernel's fused summary
+    tallies, the reference's summary tables (trajectory_summary.py:147-260)
+    without materialising rows for them: ``tally_fates`` (counts by exit
+    code), ``tally_exit_E`` (escaped primaries' exit energy on n_E bins over
+    [0, E0] with under- and overflow) and ``tally_exit_theta`` (exit polar
+    angle on n_theta bins over [0, pi]), ``tally_deposit_keV`` (continuous
+    loss per layer, summed over the histories).
     """
     dev = _device(device)
     lib = L.load()
@@ -246,11 +254,17 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     wc = h.zeros(1, torch.int64)
     status = h.zeros(1, torch.int32)
     a.work_counter, a.status = _ptr(wc), _ptr(status)
-    entry_dev = None
-    if entry is None:
-        # Record the sampled entrance state: run a zero-step pass? The
-        # kernel samples on device; callers needing the snapshot pass entry.
-        entry_dev = None
+    tal_t = None
+    if tallies is not None:
+        n_tE, n_tth = (int(x) for x in tallies)
+        tal_t = dict(fates=h.zeros(6, torch.int64), exit_E=h.zeros(n_tE + 2, torch.int64),
+                     exit_theta=h.zeros(n_tth + 2, torch.int64), deposit=h.zeros(stack.n_layers, torch.float64))
+        tal = L.PbTallies()
+        tal.fates, tal.exit_E, tal.exit_theta = (_ptr(tal_t[k]) for k in ("fates", "exit_E", "exit_theta"))
+        tal.n_E, tal.E_lo, tal.E_hi = n_tE, 0.0, float(E0_keV)
+        tal.n_theta, tal.theta_lo, tal.theta_hi = n_tth, 0.0, float(np.pi)
+        tal.deposit = _ptr(tal_t["deposit"])
+        a.tallies = tal
     L.check(lib.pb_transport(C.byref(a), _stream_ptr(stream)), "pb_transport")
     torch.cuda.synchronize(dev)
     st = int(status.item())
@@ -262,7 +276,7 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
             beam_dir, composition, layers, beam_fwhm_mm, beam_fwhm_y_mm, tilt_polar_rad,
             tilt_azim_rad, transverse_distribution, lut=lut, rng=rng, precision=precision,
             entry=entry, cap=int(counts.max()), device=device, stream=stream,
-            block_threads=block_threads)
+            block_threads=block_threads, tallies=tallies)
     mask = (np.arange(cap)[None, :] < counts[:, None]).reshape(-1)
     idx = torch.from_numpy(np.flatnonzero(mask)).to(dev)
     out = {k: v.index_select(0, idx).cpu().numpy() for k, v in rows.items()}
@@ -279,7 +293,9 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     out["exit_code"] = codes
     out["final_E_keV"] = final_E.cpu().numpy()
     out["device_status"] = st
-    del entry_dev
+    if tal_t is not None:
+        for k, v in tal_t.items():
+            out[f"tally_{k}" if k != "deposit" else "tally_deposit_keV"] = v.cpu().numpy()
     return out
 
 

@@ -668,17 +668,20 @@ class ScoringCase:
 
 def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 1, warmup: int = 1,
                        precision="mixed", rng="philox", e_start: int = 0, device=None, surrogates=None,
-                       exact_stride=50) -> dict:
+                       exact_stride=50, tol=0.01, probe_batches=None) -> dict:
     """End-to-end run through host buffers: every step copies the case's input
     tables from pinned host memory to the device, runs one batch, and reads
     the spectra and tallies back to pinned host memory. Returns the rate and
     the bytes moved per step. With ``surrogates`` the PXR+CBS part is the
     surrogate with its exact sub-sample; the per-direction accumulators read
-    back each step are the ones its readout needs."""
+    back each step are the ones its readout needs. The surrogate's error
+    probe runs on the warm-up batches (``probe_batches`` defaults to the
+    warm-up count, at least two)."""
     case = ScoringCase(spec, precision=precision, rng=rng, batch_histories=histories_per_step,
                        device=device)
     if surrogates:
-        case.use_surrogate(surrogates, exact_stride=exact_stride)
+        probe = max(2, int(warmup)) if probe_batches is None else int(probe_batches)
+        case.use_surrogate(surrogates, exact_stride=exact_stride, tol=tol, probe_batches=probe)
     pairs = [(t.cpu().pin_memory(), t) for t in case.h.inputs]
     if surrogates:
         outs = case.sur_hsum + case.sur_lsum + case.sur_hsum_s + case.sur_lsum_s

@@ -954,6 +954,41 @@ def gen_coherent_decoherence():
 
 
 # ---------------------------------------------------------------------------
+# Summary tables (pyrite/montecarlo/trajectory_summary.py:147-260) of the
+# golden transport cases: the reference's own reductions of its own rows.
+# ---------------------------------------------------------------------------
+SUMMARY_BINS = dict(exit_E=64, exit_theta=36, depth=8)
+
+
+def gen_summary():
+    from pyrite.montecarlo import trajectory_summary as ts
+
+    for name, case in TRANSPORT_CASES.items():
+        out, _beam_dir, _n_hat = run_reference_transport(case)
+        block = {k: np.asarray(out[k]) for k in ("r_mid", "L_ang", "v_hat", "E_start_keV", "E_end_keV",
+                                                  "event_kind", "flight_id", "substep_id", "layer")}
+        block["electron_id"] = np.asarray(out["elec_id"])
+        rows = ts._history_rows(block)
+        names = ("backscattered", "transmitted", "side_exited", "cutoff_stopped")
+        fates = np.array([sum(1 for r in rows if r[1] == n) for n in names], dtype=np.int64)
+        esc = [r for r in rows if r[1] in names[:3]]
+        E_edges = np.linspace(0.0, case["E0_keV"], SUMMARY_BINS["exit_E"] + 1)
+        th_edges = np.linspace(0.0, np.pi, SUMMARY_BINS["exit_theta"] + 1)
+        exit_E = ts._histogram(np.array([r[4] for r in esc]), E_edges)
+        exit_theta = ts._histogram(np.array([r[5] for r in esc]), th_edges)
+        layers = case["layers"]
+        edges = np.unique(np.concatenate([np.linspace(a, b, SUMMARY_BINS["depth"] + 1) for a, b, _ in layers]))
+        prof = ts.depth_loss_profile(block, edges)
+        per_layer = prof.groupby("layer")["continuous_loss_keV"].sum()
+        deposit = np.array([float(per_layer.get(k, 0.0)) for k in range(len(layers))])
+        _save(f"summary_{name}", E_edges=E_edges, theta_edges=th_edges, fates=fates, fate_names=np.array(names),
+              exit_E=exit_E, exit_theta=exit_theta, depth_edges=edges,
+              depth_layer=prof["layer"].to_numpy(), depth_low=prof["depth_low_ang"].to_numpy(),
+              depth_loss=prof["continuous_loss_keV"].to_numpy(), deposit_per_layer=deposit,
+              escaped_exit_E=np.array([r[4] for r in esc]), escaped_exit_theta=np.array([r[5] for r in esc]))
+
+
+# ---------------------------------------------------------------------------
 # Full run (statistical pin): the 20 MeV HOPG scene with its Twiss beam through
 # the reference's per-electron core, then PXR/CBS bin means, Bethe-Heitler and
 # the exit / fate / depth-loss summaries, in electron groups so the tests can
@@ -1065,6 +1100,7 @@ GENERATORS = {
     "coherent": gen_coherent,
     "coherent_decoherence": gen_coherent_decoherence,
     "fullrun": gen_fullrun,
+    "summary": gen_summary,
 }
 
 

@@ -11,8 +11,11 @@ SYM = {6.0: "C", 8.0: "O", 14.0: "Si", 74.0: "W"}
 
 
 @pytest.mark.parametrize("case", ["c20", "sio2"])
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 2e-3)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 1e-6)])
 def test_brem_matches_reference(case, precision, tol, cuda_device):
+    """FP64 to 1e-13 of the peak (measured 1.5e-14: the same expression, the
+    kernel's exp/log against numpy's); mixed to 1e-6 of the peak (measured
+    3.5e-7: the float cross-section rewrite and transmission forms)."""
     from pyrite_b200 import mc_brem_spectrum
 
     d = golden(f"brem_{case}")

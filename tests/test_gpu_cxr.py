@@ -1,10 +1,22 @@
 """CUDA PXR + CBS scorer against the oracle and the reference's spectra.
 
-Pairs: every (segment, reflection) line of the FP64 kernel equals the oracle's
-to 1e-9 relative. Spectra: FP64 node and exact bin-mean agree with the
-reference to 1e-8 of the peak; the far-envelope bin-mean and the mixed
-precision kernel stay within 1e-3 and 1e-2 of the peak respectively (the
-accuracy target of the mixed-precision path is 1 % spectrum error).
+Pairs (FP64): every (segment, reflection) line equals the oracle's -- the
+resonance energy and width to 1e-14 relative (measured 1e-15), the weight to
+2e-12 (measured 1.3e-12, median 7e-15: the weight carries the escape
+transmission exp(-mu L) and the squared amplitude, whose exp/log/sqrt differ
+in the last bit between CUDA's libm and glibc, and the detuning divides by a
+difference of terms near 1). Spectra (FP64): node within 2e-10 and exact
+bin-mean within 5e-10 of the reference's peak (measured 9e-11 and 2.5e-10: a
+node samples sinc^2 at a(E - E_r) up to 1e4 rad, where 1e-15 of E_r is
+1e-11 of the phase). The far-envelope bin-mean stays within 1e-3 of the
+peak (the reference's own envelope approximation).
+
+Mixed precision (FP32 lines on FP64 segments): resonance energy and width
+within 1e-6 relative of the FP64 oracle on every pair both keep (measured
+8.8e-7, ~7 float ulp); the weights' total error is small where it matters
+(sum |dw| / sum w), while single pairs whose amplitude nearly cancels carry
+large relative errors; the bin-mean spectrum within 1e-4 of the peak
+(measured 4e-5).
 """
 
 import numpy as np
@@ -53,23 +65,50 @@ def test_pairs_match_oracle(case, cuda_device):
     good = good.astype(bool)
     assert np.mean(good == og) > 0.9999
     both = good & og
-    np.testing.assert_allclose(E[both], oE[both], rtol=1e-9)
-    np.testing.assert_allclose(a[both], oa[both], rtol=1e-9)
-    np.testing.assert_allclose(w[both], ow[both], rtol=1e-8)
+    np.testing.assert_allclose(E[both], oE[both], rtol=1e-14)
+    np.testing.assert_allclose(a[both], oa[both], rtol=1e-14)
+    np.testing.assert_allclose(w[both], ow[both], rtol=2e-12)
+
+
+@pytest.mark.parametrize("case", CXR_CASES)
+def test_mixed_pairs_against_fp64_oracle(case, cuda_device):
+    """The mixed scorer's lines (cxr_kernel<float>) against the FP64 oracle on
+    the same segments: E_r and the width within 1e-6 relative on every pair
+    both keep; at least 80 % of the keep decisions agree (the decisions at the
+    keep window's edges follow float rounding); the weight error summed over
+    the kept pairs within 1e-3 of their summed weight."""
+    d, (spec, pairs) = score(case, cuda_device, line_quadrature="node", return_pairs=True, precision="mixed")
+    E, a, w, good = pairs[0]
+    tr = golden(f"transport_{d['transport']}")
+    seg = dict(v_hat=tr["v_hat"], E_keV=tr["E_repr_keV"], L_ang=tr["L_ang"], r_mid=tr["r_mid"],
+               elec_id=tr["elec_id"])
+    E_grid = d["E_grid"]
+    pad = 0.2 * (E_grid[-1] - E_grid[0])
+    t = {k: d[k] for k in ("G", "ES", "EP", "WM", "row_table", "E_tab", "chi_re", "chi_im", "u_re",
+                            "u_im", "log_mu", "delta")}
+    t["lo_keep"], t["hi_keep"] = E_grid[0] - pad, E_grid[-1] + pad
+    oE, oa, ow, og = oracle.cxr_lines(t, d["n_hat"], d["thickness"], seg, int(d["Ne"]))
+    good = good.astype(bool)
+    assert np.mean(good == og) >= 0.8
+    both = good & og
+    assert both.sum() > 1000
+    np.testing.assert_allclose(E[both], oE[both], rtol=1e-6)
+    np.testing.assert_allclose(a[both], oa[both], rtol=1e-6)
+    assert np.sum(np.abs(w[both] - ow[both])) <= 1e-3 * np.sum(np.abs(ow[both]))
 
 
 @pytest.mark.parametrize("case", CXR_CASES)
 def test_node_spectrum_fp64(case, cuda_device):
     d, spec = score(case, cuda_device, line_quadrature="node")
     peak = np.max(np.abs(d["spec_node"]))
-    assert np.max(np.abs(spec - d["spec_node"])) <= 1e-8 * peak
+    assert np.max(np.abs(spec - d["spec_node"])) <= 2e-10 * peak
 
 
 @pytest.mark.parametrize("case", CXR_CASES)
 def test_binmean_exact_fp64(case, cuda_device):
     d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=None)
     peak = np.max(np.abs(d["spec_binmean"]))
-    assert np.max(np.abs(spec - d["spec_binmean"])) <= 1e-8 * peak
+    assert np.max(np.abs(spec - d["spec_binmean"])) <= 5e-10 * peak
 
 
 @pytest.mark.parametrize("case", CXR_CASES)
@@ -82,12 +121,14 @@ def test_binmean_far_envelope(case, cuda_device):
 
 
 @pytest.mark.parametrize("case", CXR_CASES)
-def test_mixed_precision_within_one_percent(case, cuda_device):
-    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=64.0, precision="mixed")
+def test_mixed_binmean_against_reference(case, cuda_device):
+    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=None, precision="mixed")
     ref = d["spec_binmean"]
     peak = np.max(np.abs(ref))
-    assert np.max(np.abs(spec - ref)) <= 1e-2 * peak
-    assert spec.sum() == pytest.approx(ref.sum(), rel=1e-2)
+    assert np.max(np.abs(spec - ref)) <= 1e-4 * peak
+    assert spec.sum() == pytest.approx(ref.sum(), rel=1e-4)
+    d, spec = score(case, cuda_device, line_quadrature="bin-mean", exact_widths=64.0, precision="mixed")
+    assert np.max(np.abs(spec - ref)) <= 1e-3 * peak
 
 
 def test_general_tabulation_grid_uses_search(cuda_device):

@@ -1,12 +1,15 @@
 """CUDA transport kernel against the oracle / the reference's own rows.
 
 The FP64 exact and LUT kernels with the reference's SplitMix64 stream replay
-the reference histories: every row agrees to 1e-9 relative (CUDA's libm and
-glibc differ in the last bit of log/sin/cos, which a chaotic history can
-amplify, so a small fraction of histories may diverge after many steps; none
-may diverge in its first event). Philox runs are deterministic and
-independent of the launch shape; the mixed-precision kernel agrees with FP64
-statistically.
+the reference histories: every history has the reference's number of rows and
+every row agrees within 1e-10 relative. Measured on B200: every row of the
+20 MeV C, 50 MeV Si and LUT 10 MeV stack / 300 keV SiO2 cases within 1e-12;
+the 30 keV Si case (400-480 rows per history) drifts from ~1e-12 partway
+through 8-10 of its 16 histories to at most 2.3e-11 -- CUDA's and glibc's
+log/exp/sin/cos differ in the last bit, and a history's chain of scattering
+angles carries that rounding forward; no history changes its event sequence.
+Philox runs are deterministic and independent of the launch shape; the
+mixed-precision kernel agrees with FP64 statistically.
 """
 
 import numpy as np
@@ -36,8 +39,9 @@ def run(d, cuda_device, **kw):
                                  device=cuda_device, **kw)
 
 
-def history_agreement(ref, got, rtol=1e-9):
-    """Fraction of histories whose every row matches, and whether all first rows match."""
+def history_agreement(ref, got, rtol=1e-10):
+    """Fraction of histories whose every row matches to ``rtol``, and whether
+    all first rows match."""
     eids = np.unique(ref["elec_id"])
     ok = 0
     first_ok = True
@@ -45,7 +49,7 @@ def history_agreement(ref, got, rtol=1e-9):
         a = ref["elec_id"] == e
         b = got["elec_id"] == e
         if a.sum() == b.sum():
-            same = all(np.allclose(ref[k][a], got[k][b], rtol=rtol, atol=1e-9)
+            same = all(np.allclose(ref[k][a], got[k][b], rtol=rtol, atol=1e-10)
                        for k in ("L_ang", "E_keV", "E_end_keV", "t_end_ang", "r_mid", "v_hat"))
             ok += same
         fa, fb = np.flatnonzero(a)[0], np.flatnonzero(b)[0]
@@ -60,8 +64,8 @@ def test_exact_fp64_replays_reference(case, cuda_device):
     got = run(d, cuda_device, lut=False, entry=(d["initial_r"], d["initial_v"], d["initial_E"]))
     frac, first = history_agreement(d, got)
     assert first
-    assert frac >= 0.9, frac
-    assert got["L_ang"].size == pytest.approx(d["L_ang"].size, rel=0.05)
+    assert frac == 1.0, frac
+    assert got["L_ang"].size == d["L_ang"].size
 
 
 @pytest.mark.parametrize("case", LUT_CASES)
@@ -72,7 +76,8 @@ def test_lut_fp64_replays_reference(case, cuda_device):
     got = run(g, cuda_device, lut=True, entry=(d["initial_r"], d["initial_v"], d["initial_E"]))
     frac, first = history_agreement(ref, got)
     assert first
-    assert frac >= 0.9, frac
+    assert frac == 1.0, frac
+    assert got["L_ang"].size == d["L_ang"].size
 
 
 def test_device_entry_sampling_matches_reference(cuda_device):
