@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 3
+#define PB_ABI_VERSION 4
 
 enum pb_status {
     PB_OK = 0,
@@ -181,6 +181,13 @@ typedef struct pb_transport_args {
     pb_tallies tallies;     /* optional (NULL pointers skip) */
     unsigned long long *work_counter;  /* device scratch, 1 word; zeroed by the call */
     unsigned int *status;   /* device status word (pb_device_status bits), OR-ed */
+    /* ABI 4: Urban energy-loss straggling per flight (the reference's
+     * straggling=True, transport/straggling.py with cores.py:654-700): each
+     * flight's loss is sampled from the compound-Poisson Urban model of every
+     * element of the layer instead of the deterministic midpoint loss.
+     * Needs Z. Zero keeps the deterministic loss. */
+    int32_t straggling;
+    const double *Z;        /* [n_layers * max_el] atomic numbers */
 } pb_transport_args;
 
 /* CXR reflection rows and coupling tables (cxr/_batched.py:232-331). */

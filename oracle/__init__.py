@@ -64,6 +64,8 @@ class _Layers(C.Structure):
         ("E_cross", _D),
         ("sr_rate_numer", _D),
         ("sr_joy_numer", _D),
+        ("Z", _D),
+        ("straggling", C.c_int),
     ]
 
 
@@ -170,6 +172,12 @@ def _declare(L):
     L.or_stream_key.argtypes = [C.c_uint64, C.c_uint64]
     L.or_stream_uniform.restype = C.c_double
     L.or_stream_uniform.argtypes = [C.c_uint64, C.c_uint64]
+    L.or_dEds_element.restype = C.c_double
+    L.or_dEds_element.argtypes = [C.c_double] * 5
+    L.or_urban_sample_element.restype = C.c_double
+    L.or_urban_sample_element.argtypes = [C.c_double] * 5 + [C.c_uint64, C.POINTER(C.c_uint64)]
+    L.or_urban_moments_element.restype = None
+    L.or_urban_moments_element.argtypes = [C.c_double] * 5 + [C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.or_philox_uniform.restype = C.c_double
     L.or_philox_uniform.argtypes = [C.c_uint64, C.c_uint64]
     L.or_philox4x32_10.restype = None
@@ -254,6 +262,26 @@ def philox4x32_10(ctr, key):
     k = (C.c_uint32 * 2)(*[int(v) for v in key])
     lib().or_philox4x32_10(c, k)
     return [int(v) for v in c]
+
+
+def dEds_element(J, k, coeff, E_cross, E):
+    """One element's spliced stopping power [keV/Angstrom] (negative)."""
+    return float(lib().or_dEds_element(J, k, coeff, E_cross, E))
+
+
+def urban_sample_element(Z, J, C_keV_per_ang, E, s, key, counter=0):
+    """One element's Urban loss over ``s`` [keV] and the next counter."""
+    c = C.c_uint64(int(counter))
+    dE = float(lib().or_urban_sample_element(Z, J, C_keV_per_ang, E, s, C.c_uint64(int(key) % 2**64),
+                                              C.byref(c)))
+    return dE, int(c.value)
+
+
+def urban_moments_element(Z, J, C_keV_per_ang, E, s):
+    """Analytic (mean, variance) of one element's Urban loss [keV, keV^2]."""
+    m, v = C.c_double(), C.c_double()
+    lib().or_urban_moments_element(Z, J, C_keV_per_ang, E, s, C.byref(m), C.byref(v))
+    return m.value, v.value
 
 
 def beam_entries(beam, e_start: int, n: int, rng: int = 1):
@@ -341,6 +369,7 @@ class LayerTables:
             len(self.z_top), Z.shape[1], _p(self.z_top, _D), _p(self.z_bot, _D),
             _p(self.n_el, _I32), _p(self.J, _D), _p(self.k, _D), _p(self.coeff, _D),
             _p(self.E_cross, _D), _p(self.sr_rate_numer, _D), _p(self.sr_joy_numer, _D),
+            _p(self.Z, _D), 0,
         )
 
     def dEds(self, L, E):
@@ -365,12 +394,17 @@ class LutTables:
 
 
 def transport(layers, pos, direction, E, *, seed, E_cut, rng=RNG_SPLITMIX,
-              e_start=0, max_steps=400_000, cap=4096, keep_rows=True, clock=None):
+              e_start=0, max_steps=400_000, cap=4096, keep_rows=True, clock=None, straggling=False):
     """Per-electron transport of ``len(E)`` histories; returns a dict of rows and finals.
 
     ``layers`` is a :class:`LayerTables` (the exact analytic core) or a
-    :class:`LutTables` (the reference's default LUT core).
+    :class:`LutTables` (the reference's default LUT core). ``straggling``:
+    Urban energy-loss straggling per flight (exact core).
     """
+    if straggling and isinstance(layers, LutTables):
+        raise ValueError("the oracle's LUT core has no straggling")
+    if isinstance(layers, LayerTables):
+        layers.struct.straggling = 1 if straggling else 0
     n = int(np.asarray(E).size)
     pos = _f64(pos).reshape(n, 3).copy()
     direction = _f64(direction).reshape(n, 3).copy()

@@ -49,7 +49,15 @@ typedef struct {
     const double *E_cross;       /* Joy-Luo / Berger-Seltzer crossover, keV */
     const double *sr_rate_numer; /* 5.21e-21 Z^2 4 pi n_cm3 */
     const double *sr_joy_numer;  /* 3.4e-3 Z^0.67 */
+    const double *Z;             /* [n_layers*max_el] atomic numbers (Urban straggling) */
+    int straggling;              /* 1: Urban energy-loss straggling per flight */
 } or_layers;
+
+/* Urban energy-loss straggling (straggling.py:37-333). */
+double or_dEds_element(double J, double k, double coeff, double E_cross, double E);
+double or_urban_sample_element(double Z, double J, double C, double E, double s, uint64_t key,
+                               uint64_t *counter);
+void or_urban_moments_element(double Z, double J, double C, double E, double s, double *mean, double *var);
 
 /* Segment rows, slot i*cap + s (cores.py:911-935). */
 typedef struct {

@@ -108,6 +108,129 @@ double or_dEds_spliced(const or_layers *ly, int L, double E) {
     return -7.85e-4 / E * jl - BS_PREFACTOR / beta_sq * bs;
 }
 
+/* ---- Urban energy-loss straggling (straggling.py) ------------------------
+ * The loss over a flight of length s is the compound Poisson sum of two
+ * excitation levels and a 1/E^2 ionisation continuum whose mean is C s,
+ * C = |dE/dx| of the element (straggling.py:57-120, the Urban model of the
+ * Geant4 Physics Reference Manual). Each flight draws from its own SplitMix64
+ * stream: urban key = sm64(electron key ^ salt) (straggling.py:37-43), flight
+ * key = sm64(urban key + phi ((flight << 32) + substep)) (straggling.py:46-59),
+ * draws (flight key, counter) from counter 0. */
+#define URBAN_SALT 0xD6E8FEB86659FD93ULL
+#define URBAN_E0_KEV 1.0e-2
+#define URBAN_E2_PER_Z2 1.0e-2
+#define URBAN_RATE 0.55
+#define URBAN_CHUNK_MAX 64.0
+
+/* stopping.py via straggling.py:278-298, _dEds_spliced_element_scalar (delta = 0) */
+double or_dEds_element(double J, double k, double coeff, double E_cross, double E) {
+    double tau = E / MC2_KEV;
+    double gamma = 1.0 + tau;
+    double beta_sq = 1.0 - 1.0 / (gamma * gamma);
+    if (E < E_cross) return -7.85e-4 / E * coeff * log(1.166 * (E + k * J) / J);
+    double f_minus = 1.0 - beta_sq + (tau * tau / 8.0 - (2.0 * tau + 1.0) * LN2) / (gamma * gamma);
+    double I_rel = J / MC2_KEV;
+    return -BS_PREFACTOR / beta_sq * coeff * (log(tau * tau * (tau + 2.0) / (2.0 * I_rel * I_rel)) + f_minus - 0.0);
+}
+
+/* straggling.py:127-157, _urban_levels_scalar */
+static void urban_levels(double Z, double J, double T_up, double two_mc2_bg2, double beta_sq, double *f1,
+                         double *E1, double *f2, double *E2) {
+    double e2 = URBAN_E2_PER_Z2 * Z * Z;
+    double g2 = Z > 2.0 ? 2.0 / Z : 1.0;
+    *E2 = e2;
+    if (Z > 2.0 && e2 < T_up && log(two_mc2_bg2 / e2) - beta_sq > 0.0) {
+        double g1 = 1.0 - g2;
+        double e1 = exp((log(J) - g2 * log(e2)) / g1);
+        if (log(two_mc2_bg2 / e1) - beta_sq > 0.0) {
+            *f1 = g1; *E1 = e1; *f2 = g2;
+            return;
+        }
+    }
+    *f1 = 1.0; *E1 = J; *f2 = 0.0;
+}
+
+/* straggling.py:160-201, _urban_channels_scalar; returns valid */
+static int urban_channels(double Z, double J, double C, double E, double *s1, double *E1, double *s2,
+                          double *E2, double *s3) {
+    double tau = E / MC2_KEV;
+    double gamma = 1.0 + tau;
+    double beta_sq = 1.0 - 1.0 / (gamma * gamma);
+    double two_mc2_bg2 = 2.0 * MC2_KEV * tau * (tau + 2.0);
+    double T_up = 0.5 * E;
+    *s1 = *s2 = *s3 = 0.0;
+    *E1 = J;
+    *E2 = 0.0;
+    if (T_up <= URBAN_E0_KEV || C <= 0.0) return 0;
+    double L_I = log(two_mc2_bg2 / J) - beta_sq;
+    if (L_I <= 0.0) return 0;
+    double f1, f2;
+    urban_levels(Z, J, T_up, two_mc2_bg2, beta_sq, &f1, E1, &f2, E2);
+    double soft = C * (1.0 - URBAN_RATE) / L_I;
+    *s1 = soft * (f1 / *E1) * (log(two_mc2_bg2 / *E1) - beta_sq);
+    if (f2 > 0.0) *s2 = soft * (f2 / *E2) * (log(two_mc2_bg2 / *E2) - beta_sq);
+    *s3 = C * URBAN_RATE * (T_up - URBAN_E0_KEV) / (URBAN_E0_KEV * T_up * log(T_up / URBAN_E0_KEV));
+    return 1;
+}
+
+/* straggling.py:204-222, _urban_moments_element_scalar */
+void or_urban_moments_element(double Z, double J, double C, double E, double s, double *mean, double *var) {
+    double s1, E1, s2, E2, s3;
+    if (!urban_channels(Z, J, C, E, &s1, &E1, &s2, &E2, &s3)) {
+        *mean = C * s;
+        *var = 0.0;
+        return;
+    }
+    double T_up = 0.5 * E;
+    double mean3 = URBAN_E0_KEV * T_up * log(T_up / URBAN_E0_KEV) / (T_up - URBAN_E0_KEV);
+    *mean = s * (s1 * E1 + s2 * E2 + s3 * mean3);
+    *var = s * (s1 * E1 * E1 + s2 * E2 * E2 + s3 * URBAN_E0_KEV * T_up);
+}
+
+/* straggling.py:225-262, _urban_poisson_scalar: inverse CDF per chunk of
+ * mean <= 64, one uniform per chunk */
+static int64_t urban_poisson(double lam, uint64_t key, uint64_t *counter) {
+    if (lam <= 0.0) return 0;
+    int64_t n_chunks = (int64_t)ceil(lam / URBAN_CHUNK_MAX);
+    double chunk = lam / (double)n_chunks;
+    int64_t total = 0;
+    for (int64_t c = 0; c < n_chunks; ++c) {
+        double u = or_stream_uniform(key, *counter);
+        *counter += 1;
+        double p = exp(-chunk);
+        double cdf = p;
+        int64_t k = 0;
+        while (u >= cdf) {
+            k += 1;
+            p = p * chunk / (double)k;
+            double next = cdf + p;
+            if (next <= cdf) break;
+            cdf = next;
+        }
+        total += k;
+    }
+    return total;
+}
+
+/* straggling.py:277-275, _urban_sample_element_keV (inverse CDF of the
+ * continuum, straggling.py:265-274) */
+double or_urban_sample_element(double Z, double J, double C, double E, double s, uint64_t key,
+                               uint64_t *counter) {
+    double s1, E1, s2, E2, s3;
+    if (!urban_channels(Z, J, C, E, &s1, &E1, &s2, &E2, &s3) || s <= 0.0) return C * s;
+    int64_t n1 = urban_poisson(s1 * s, key, counter);
+    int64_t n2 = urban_poisson(s2 * s, key, counter);
+    int64_t n3 = urban_poisson(s3 * s, key, counter);
+    double dE = (double)n1 * E1 + (double)n2 * E2;
+    double T_up = 0.5 * E;
+    for (int64_t i = 0; i < n3; ++i) {
+        double u = or_stream_uniform(key, *counter);
+        *counter += 1;
+        dE += URBAN_E0_KEV / (1.0 - u * (T_up - URBAN_E0_KEV) / T_up);
+    }
+    return dE;
+}
+
 /* scattering.py:208-218, _scatter_rates_sr_scalar [1/cm] */
 double or_sr_rate(double E, double sr_rate_numer, double sr_joy_numer) {
     double a = sr_joy_numer / E;
@@ -152,8 +275,8 @@ static int layer_of(const or_layers *ly, double z) {
 /* ---- the per-electron event loop ----------------------------------------
  * cores.py:379-1230 with per_electron=True, lut=False, grooved=False,
  * inelastic=False, radiative=False, mixed=False, cone_split=False,
- * elastic_model_code=0 (SR), energy_model_code=1 (midpoint), straggling off,
- * max_dE_frac=0, infinite lateral footprint. With spliced stopping the lazy
+ * elastic_model_code=0 (SR), energy_model_code=1 (midpoint), straggling
+ * off or Urban (ly->straggling), max_dE_frac=0, infinite lateral footprint. With spliced stopping the lazy
  * cutoff bound is never armed (_jit_cutoff_bound.py:47-56), so the midpoint
  * cutoff solve always runs.
  */
@@ -199,22 +322,46 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
         double dEds = or_dEds_spliced(ly, L, E_j);
         int geometry_event = cross_up || cross_dn;
         int cutoff = 0;
-        /* cores.py:734-776: midpoint cutoff distance */
-        double cutoff_rate = or_dEds_spliced(ly, L, 0.5 * (E_j + E_cut));
-        double cutoff_distance = (E_cut - E_j) / cutoff_rate;
-        if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
-            step = cutoff_distance;
-            cutoff = 1;
-            cross_up = cross_dn = exit_top = exit_bot = 0;
-        }
-        /* cores.py:783-809: midpoint (RK2) end energy and clock */
         double E_end;
-        if (cutoff) {
-            E_end = E_cut;
+        if (ly->straggling) {
+            /* cores.py:654-700: the Urban loss of the flight, element by
+             * element (straggling.py:301-333), a loss beyond E - E_cut
+             * shortening the step in proportion and ending at the cutoff. */
+            uint64_t urban_key = or_splitmix64(key ^ URBAN_SALT);
+            uint64_t fkey = or_splitmix64(urban_key + 0x9E3779B97F4A7C15ULL * ((uint64_t)flight << 32));
+            uint64_t ctr = 0;
+            double loss = 0.0;
+            for (int i = 0; i < n_el; ++i) {
+                int ix = L * ly->max_el + i;
+                double C = -or_dEds_element(ly->J[ix], ly->k[ix], ly->coeff[ix], ly->E_cross[ix], E_j);
+                loss += or_urban_sample_element(ly->Z[ix], ly->J[ix], C, E_j, step, fkey, &ctr);
+            }
+            double delta_cut = E_j - E_cut;
+            if (loss > delta_cut || (loss == delta_cut && !geometry_event)) {
+                step = loss > 0.0 ? step * (delta_cut / loss) : 0.0;
+                cutoff = 1;
+                cross_up = cross_dn = exit_top = exit_bot = 0;
+                E_end = E_cut;
+            } else {
+                E_end = E_j - loss;
+            }
         } else {
-            double E_pred = E_j + dEds * step;
-            double E_mid = 0.5 * (E_j + E_pred);
-            E_end = E_j + step * or_dEds_spliced(ly, L, E_mid);
+            /* cores.py:734-776: midpoint cutoff distance */
+            double cutoff_rate = or_dEds_spliced(ly, L, 0.5 * (E_j + E_cut));
+            double cutoff_distance = (E_cut - E_j) / cutoff_rate;
+            if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
+                step = cutoff_distance;
+                cutoff = 1;
+                cross_up = cross_dn = exit_top = exit_bot = 0;
+            }
+            /* cores.py:783-809: midpoint (RK2) end energy and clock */
+            if (cutoff) {
+                E_end = E_cut;
+            } else {
+                double E_pred = E_j + dEds * step;
+                double E_mid = 0.5 * (E_j + E_pred);
+                E_end = E_j + step * or_dEds_spliced(ly, L, E_mid);
+            }
         }
         double t_end = clk + step / or_beta_from_keV(0.5 * (E_j + E_end));
         int8_t event;

@@ -79,7 +79,7 @@ class PbTransportArgs(C.Structure):
         ("layers", PbLayers), ("lut", PbLut), ("beam", PbBeam), ("cap", _i64), ("rows", PbRows),
         ("seg_count", _vp), ("exit_code", _vp), ("final_pos", _vp), ("final_dir", _vp),
         ("final_E", _vp), ("seg", PbSegments), ("tallies", PbTallies), ("work_counter", _vp),
-        ("status", _vp),
+        ("status", _vp), ("straggling", _i32), ("Z", _vp),
     ]
 
 
@@ -192,7 +192,7 @@ class PyriteB200Error(RuntimeError):
     """A pyrite_b200 C-ABI call returned a non-zero status."""
 
 
-ABI_VERSION = 3  # PB_ABI_VERSION of include/pyrite_b200.h
+ABI_VERSION = 4  # PB_ABI_VERSION of include/pyrite_b200.h
 
 
 def load(path: Path | None = None):

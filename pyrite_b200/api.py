@@ -182,7 +182,7 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
                           composition=None, layers=None, beam_fwhm_mm=None, beam_fwhm_y_mm=None,
                           tilt_polar_rad=0.0, tilt_azim_rad=0.0, transverse_distribution=None,
                           *, lut=True, rng="splitmix", precision="fp64", entry=None, cap=None,
-                          device=None, stream=None, block_threads=0, tallies=None):
+                          device=None, stream=None, block_threads=0, tallies=None, straggling=False):
     """Transport ``Ne`` electrons into a slab or layer stack; returns segment rows.
 
     Same contract as the reference's per-electron cores: rows of history i
@@ -190,7 +190,10 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     the reference's default LUT core or its exact analytic core; ``rng`` the
     reference's SplitMix64 counter stream (draw-for-draw compatible) or
     Philox4x32-10; ``precision`` "fp64" or "mixed". ``entry`` replaces the
-    sampled entrance state with explicit (pos, dir, E) arrays.
+    sampled entrance state with explicit (pos, dir, E) arrays. ``straggling``
+    samples each flight's loss from the Urban model (the reference's
+    ``straggling=True``, transport/straggling.py) instead of the
+    deterministic midpoint loss.
 
     ``tallies=(n_E, n_theta)`` also returns the kernel's fused summary
     tallies, the reference's summary tables (trajectory_summary.py:147-260)
@@ -218,6 +221,8 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     a.E_cut_keV = float(E_cut_keV)
     a.max_steps = int(max_steps)
     a.layers = _fill_layers(h, stack)
+    if straggling:
+        a.straggling, a.Z = 1, _ptr(h.f64(stack.Z))
     if lut:
         E_hi = float(E0_keV) if entry is None else float(np.max(entry[2]))
         a.lut = _fill_lut(h, build_transport_lut(stack, E_cut_keV, E_hi), a.precision)
@@ -276,7 +281,7 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
             beam_dir, composition, layers, beam_fwhm_mm, beam_fwhm_y_mm, tilt_polar_rad,
             tilt_azim_rad, transverse_distribution, lut=lut, rng=rng, precision=precision,
             entry=entry, cap=int(counts.max()), device=device, stream=stream,
-            block_threads=block_threads, tallies=tallies)
+            block_threads=block_threads, tallies=tallies, straggling=straggling)
     mask = (np.arange(cap)[None, :] < counts[:, None]).reshape(-1)
     idx = torch.from_numpy(np.flatnonzero(mask)).to(dev)
     out = {k: v.index_select(0, idx).cpu().numpy() for k, v in rows.items()}

@@ -132,6 +132,7 @@ int pb_transport(const pb_transport_args *a, void *stream) {
         return fail(PB_ERR_INVALID, "pb_transport: exit angle bins must be in [1, 256]");
     if (a->block_threads != 0 && (a->block_threads % 32 != 0 || a->block_threads > 256))
         return fail(PB_ERR_INVALID, "pb_transport: block_threads must be a multiple of 32 <= 256");
+    if (a->straggling && !a->Z) return fail(PB_ERR_INVALID, "pb_transport: straggling needs Z");
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a->work_counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "pb_transport: zero work counter");

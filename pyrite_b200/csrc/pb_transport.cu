@@ -58,6 +58,7 @@ struct LayerSmem {
     double E_cross[kMaxLayers * kMaxEl];
     double srn[kMaxLayers * kMaxEl];
     double sjn[kMaxLayers * kMaxEl];
+    double Z[kMaxLayers * kMaxEl];  // atomic numbers (straggling only)
 };
 
 // Math in the precision of the flight arithmetic.
@@ -91,6 +92,117 @@ __device__ __forceinline__ Real dEds_spliced(const LayerSmem &ly, int max_el, in
         }
     }
     return -(Real)7.85e-4 / E * jl - (Real)kBsPrefactor / beta_sq * bs;
+}
+
+// ---------------------------------------------------------------------------
+// Urban energy-loss straggling (transport/straggling.py), FP64 in both
+// precisions. A flight's loss is the compound Poisson sum of two excitation
+// levels and a 1/E^2 ionisation continuum, per element of the layer, whose
+// mean is the element's |dE/dx| times the path (the model's closure
+// identity). Each flight draws from its own counter stream keyed by the
+// history's key and the flight index (straggling.py:37-59), so the flight's
+// draw count never moves the elastic draws.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kUrbanSalt = 0xD6E8FEB86659FD93ULL;
+constexpr double kUrbanE0 = 1.0e-2;         // ionisation threshold [keV]
+constexpr double kUrbanE2PerZ2 = 1.0e-2;    // K-shell level 10 Z^2 eV [keV]
+constexpr double kUrbanRate = 0.55;         // continuum share of the mean
+constexpr double kUrbanChunkMax = 64.0;     // Poisson means split into chunks <= this
+
+// straggling.py:278-298: one element's spliced stopping power (delta = 0).
+__device__ __forceinline__ double dEds_element(double J, double k, double coeff, double E_cross, double E) {
+    const double tau = E / kMc2Kev;
+    const double gamma = 1.0 + tau;
+    const double beta_sq = 1.0 - 1.0 / (gamma * gamma);
+    if (E < E_cross) return -7.85e-4 / E * coeff * log(1.166 * (E + k * J) / J);
+    const double f_minus = 1.0 - beta_sq + (tau * tau / 8.0 - (2.0 * tau + 1.0) * kLn2) / (gamma * gamma);
+    const double I_rel = J / kMc2Kev;
+    return -kBsPrefactor / beta_sq * coeff * (log(tau * tau * (tau + 2.0) / (2.0 * I_rel * I_rel)) + f_minus - 0.0);
+}
+
+// straggling.py:225-262: Poisson count of mean lam, one uniform per chunk.
+template <int kRng>
+__device__ __forceinline__ int64_t urban_poisson(double lam, uint64_t key, uint64_t &ctr) {
+    if (lam <= 0.0) return 0;
+    const int64_t n_chunks = (int64_t)ceil(lam / kUrbanChunkMax);
+    const double chunk = lam / (double)n_chunks;
+    int64_t total = 0;
+    for (int64_t c = 0; c < n_chunks; ++c) {
+        const double u = uniform<kRng>(key, ctr);
+        ctr += 1;
+        double pk = exp(-chunk);
+        double cdf = pk;
+        int64_t k = 0;
+        while (u >= cdf) {  // ends: cdf grows to 1 or stops growing
+            k += 1;
+            pk = pk * chunk / (double)k;
+            const double next = cdf + pk;
+            if (next <= cdf) break;
+            cdf = next;
+        }
+        total += k;
+    }
+    return total;
+}
+
+// straggling.py:127-201,277-298: one element's sampled loss over s [keV].
+template <int kRng>
+__device__ __forceinline__ double urban_sample_element(double Z, double J, double C, double E, double s,
+                                                      uint64_t key, uint64_t &ctr) {
+    const double tau = E / kMc2Kev;
+    const double gamma = 1.0 + tau;
+    const double beta_sq = 1.0 - 1.0 / (gamma * gamma);
+    const double two_mc2_bg2 = 2.0 * kMc2Kev * tau * (tau + 2.0);
+    const double T_up = 0.5 * E;
+    if (T_up <= kUrbanE0 || C <= 0.0 || s <= 0.0) return C * s;
+    const double L_I = log(two_mc2_bg2 / J) - beta_sq;
+    if (L_I <= 0.0) return C * s;
+    // Levels (straggling.py:127-157): K shell 10 Z^2 eV with f_2 = 2/Z and the
+    // loosely bound level from the log sum rule, else one level at I.
+    double f1 = 1.0, E1 = J, f2 = 0.0;
+    const double E2 = kUrbanE2PerZ2 * Z * Z;
+    const double g2 = Z > 2.0 ? 2.0 / Z : 1.0;
+    if (Z > 2.0 && E2 < T_up && log(two_mc2_bg2 / E2) - beta_sq > 0.0) {
+        const double g1 = 1.0 - g2;
+        const double e1 = exp((log(J) - g2 * log(E2)) / g1);
+        if (log(two_mc2_bg2 / e1) - beta_sq > 0.0) {
+            f1 = g1;
+            E1 = e1;
+            f2 = g2;
+        }
+    }
+    const double soft = C * (1.0 - kUrbanRate) / L_I;
+    const double s1 = soft * (f1 / E1) * (log(two_mc2_bg2 / E1) - beta_sq);
+    const double s2 = f2 > 0.0 ? soft * (f2 / E2) * (log(two_mc2_bg2 / E2) - beta_sq) : 0.0;
+    const double s3 = C * kUrbanRate * (T_up - kUrbanE0) / (kUrbanE0 * T_up * log(T_up / kUrbanE0));
+    const int64_t n1 = urban_poisson<kRng>(s1 * s, key, ctr);
+    const int64_t n2 = urban_poisson<kRng>(s2 * s, key, ctr);
+    const int64_t n3 = urban_poisson<kRng>(s3 * s, key, ctr);
+    double dE = (double)n1 * E1 + (double)n2 * E2;
+    for (int64_t i = 0; i < n3; ++i) {  // inverse CDF of the continuum (straggling.py:265-274)
+        const double u = uniform<kRng>(key, ctr);
+        ctr += 1;
+        dE += kUrbanE0 / (1.0 - u * (T_up - kUrbanE0) / T_up);
+    }
+    return dE;
+}
+
+// The Urban loss of one flight of length s at energy E over the n elements
+// of layer L (straggling.py:301-333), from the flight's own stream (key: the
+// history's key, flight: its row index). The kernel instances with
+// straggling off carry none of it.
+template <int kRng>
+__device__ __forceinline__ double straggled_loss(const LayerSmem &ly, int max_el, int L, int n_el, double E,
+                                              double s, uint64_t key, int64_t flight) {
+    const uint64_t fkey = splitmix64(splitmix64(key ^ kUrbanSalt) + kPhi * ((uint64_t)flight << 32));
+    uint64_t ctr = 0;
+    double loss = 0.0;
+    for (int k = 0; k < n_el; ++k) {
+        const int ix = L * max_el + k;
+        const double C = -dEds_element(ly.J[ix], ly.k[ix], ly.coeff[ix], ly.E_cross[ix], E);
+        loss += urban_sample_element<kRng>(ly.Z[ix], ly.J[ix], C, E, s, fkey, ctr);
+    }
+    return loss;
 }
 
 // scattering.py:208-218
@@ -243,7 +355,7 @@ __device__ __forceinline__ int hist_slot(double v, double lo, double hi, int n) 
     return b + 1;
 }
 
-template <class Real, bool kLut, int kRng>
+template <class Real, bool kLut, int kRng, bool kStrag>
 __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ LayerSmem ly;
@@ -266,6 +378,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
         ly.E_cross[j] = p.layers.E_cross[j];
         ly.srn[j] = p.layers.sr_rate_numer[j];
         ly.sjn[j] = p.layers.sr_joy_numer[j];
+        ly.Z[j] = p.straggling ? p.Z[j] : 0.0;
     }
     for (int j = tid; j < 6; j += blockDim.x) tal.fates[j] = 0;
     const bool want_E = p.tallies.exit_E != nullptr && p.tallies.n_E <= 256;
@@ -408,7 +521,26 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             bool exit_top = cross_up && z_top <= 0.0;
             bool exit_bot = cross_dn && z_bot >= z_total;
             const bool geometry_event = cross_up || cross_dn;
-            Real dEds, cutoff_rate;
+            bool cutoff = false;
+            double E_end;
+            Real dEds = 0;
+            if constexpr (kStrag) {
+                // cores.py:654-700: the flight's Urban loss, element by element
+                // (straggling.py:301-333) from the flight's own stream; a loss
+                // beyond E - E_cut shortens the step in proportion and ends
+                // the history at the cutoff.
+                const double loss = straggled_loss<kRng>(ly, max_el, L, n_el, E_j, (double)step, key, nseg);
+                const double delta_cut = E_j - E_cut;
+                if (loss > delta_cut || (loss == delta_cut && !geometry_event)) {
+                    step = loss > 0.0 ? (Real)((double)step * (delta_cut / loss)) : (Real)0;
+                    cutoff = true;
+                    cross_up = cross_dn = exit_top = exit_bot = false;
+                    E_end = E_cut;
+                } else {
+                    E_end = E_j - loss;
+                }
+            } else {
+            Real cutoff_rate;
             if constexpr (kLut) {
                 const Real *row = lut.dEds + (int64_t)L * lut.ne;
                 dEds = lerp(row, li, lf);
@@ -421,13 +553,11 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                 cutoff_rate = dEds_spliced<Real>(ly, max_el, L, (Real)(0.5 * (E_j + E_cut)));
             }
             const Real cutoff_distance = (Real)(E_cut - E_j) / cutoff_rate;
-            bool cutoff = false;
             if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
                 step = cutoff_distance;
                 cutoff = true;
                 cross_up = cross_dn = exit_top = exit_bot = false;
             }
-            double E_end;
             if (cutoff) {
                 E_end = E_cut;
             } else {
@@ -443,6 +573,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     mid_rate = dEds_spliced<Real>(ly, max_el, L, (Real)E_mid);
                 }
                 E_end = E_j + (double)(step * mid_rate);
+            }
             }
             Real inv_beta_mid;
             if constexpr (kLut) {
@@ -611,9 +742,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             if (tal.deposit[j] != 0.0) atomicAdd(&p.tallies.deposit[j], tal.deposit[j]);
 }
 
-template <class Real, bool kLut, int kRng>
+template <class Real, bool kLut, int kRng, bool kStrag>
 static cudaError_t launch_transport_t(const pb_transport_args &a, cudaStream_t s, int sms) {
-    auto kern = transport_kernel<Real, kLut, kRng>;
+    auto kern = transport_kernel<Real, kLut, kRng, kStrag>;
     size_t dyn = 0;
     if (kLut && a.lut.total_bytes <= (int64_t)kLutSmemBytes) dyn = (size_t)a.lut.total_bytes;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -631,11 +762,12 @@ static cudaError_t launch_transport_t(const pb_transport_args &a, cudaStream_t s
     return cudaGetLastError();
 }
 
-cudaError_t launch_transport(const pb_transport_args &a, cudaStream_t s, int sms) {
+template <bool kStrag>
+static cudaError_t launch_transport_s(const pb_transport_args &a, cudaStream_t s, int sms) {
     const bool mixed = a.precision == PB_MIXED;
     const bool lut = a.use_lut != 0;
     const bool philox = a.rng == PB_RNG_PHILOX;
-#define PB_DISPATCH(R, L, G) return launch_transport_t<R, L, G>(a, s, sms)
+#define PB_DISPATCH(R, L, G) return launch_transport_t<R, L, G, kStrag>(a, s, sms)
     if (mixed) {
         if (lut) { if (philox) PB_DISPATCH(float, true, PB_RNG_PHILOX); PB_DISPATCH(float, true, PB_RNG_SPLITMIX); }
         if (philox) PB_DISPATCH(float, false, PB_RNG_PHILOX);
@@ -645,6 +777,10 @@ cudaError_t launch_transport(const pb_transport_args &a, cudaStream_t s, int sms
     if (philox) PB_DISPATCH(double, false, PB_RNG_PHILOX);
     PB_DISPATCH(double, false, PB_RNG_SPLITMIX);
 #undef PB_DISPATCH
+}
+
+cudaError_t launch_transport(const pb_transport_args &a, cudaStream_t s, int sms) {
+    return a.straggling ? launch_transport_s<true>(a, s, sms) : launch_transport_s<false>(a, s, sms);
 }
 
 }  // namespace pb

@@ -103,6 +103,8 @@ class CaseSpec:
     brem_layers: list | None = None
     brem_mu_layer: np.ndarray | None = None
     char_emitters: list | None = None
+    # Urban energy-loss straggling per flight (transport/straggling.py).
+    straggling: bool = False
 
 
 class ScoringCase:
@@ -125,6 +127,8 @@ class ScoringCase:
         a.E_cut_keV = float(spec.E_cut_keV)
         a.max_steps = int(max_steps)
         a.layers = _fill_layers(h, st)
+        if spec.straggling:
+            a.straggling, a.Z = 1, _ptr(h.f64(st.Z))
         if lut:
             a.lut = _fill_lut(h, build_transport_lut(st, spec.E_cut_keV, spec.beam.E0_keV), self.precision)
         a.beam = _fill_beam(h, spec.beam, int(spec.seed))

@@ -954,6 +954,60 @@ def gen_coherent_decoherence():
 
 
 # ---------------------------------------------------------------------------
+# Urban energy-loss straggling (pyrite/montecarlo/transport/straggling.py):
+# the sampler's leaves on seeded keys, and whole histories of the per-electron
+# exact core with straggling=True.
+# ---------------------------------------------------------------------------
+STRAGGLING_CASES = ("c20mev", "si30kev", "sio2_300kev")
+
+
+def gen_straggling():
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+    from pyrite.montecarlo.transport import straggling as ref_str
+
+    rng = np.random.default_rng(17)
+    rows = []
+    for el in ("C", "O", "Si", "W"):
+        p = TRANSPORT_ELEMENTS[el]
+        Z, A, J = float(p["Z"]), float(p["A"]), float(p["J_keV"])
+        n = 0.05
+        k = 0.731 + 0.0688 * np.log10(Z)
+        coeff = (n / 0.602214076) * Z
+        E_cross = ref_stop._element_crossover_keV(el, Z, A, J)
+        for E in (0.5, 3.0, 30.0, 300.0, 5000.0, 50000.0):
+            C = -float(ref_str._dEds_spliced_element_scalar(J, k, coeff, E_cross, 0.0, E))
+            for s in (1.0, 1e2, 1e4, 1e6):
+                key = int(rng.integers(0, 2**63))
+                dE, ctr = ref_str._urban_sample_element_keV(Z, J, C, E, s, np.uint64(key), np.uint64(0))
+                m, v = ref_str._urban_moments_element_scalar(Z, J, C, E, s)
+                rows.append((Z, J, k, coeff, E_cross, E, s, key, C, float(dE), int(ctr), float(m), float(v)))
+    a = np.array([r[:7] for r in rows])
+    _save("straggling_leaves", Z=a[:, 0], J=a[:, 1], k=a[:, 2], coeff=a[:, 3], E_cross=a[:, 4], E=a[:, 5],
+          s=a[:, 6], key=np.array([r[7] for r in rows], dtype=np.uint64), C=np.array([r[8] for r in rows]),
+          dE=np.array([r[9] for r in rows]), counter=np.array([r[10] for r in rows], dtype=np.uint64),
+          mean=np.array([r[11] for r in rows]), var=np.array([r[12] for r in rows]))
+    for name in STRAGGLING_CASES:
+        case = TRANSPORT_CASES[name]
+        layers = case["layers"]
+        tp = np.deg2rad(case["tilt_deg"])
+        beam_dir, n_hat = ref_geometry.tilted_geometry(np.deg2rad(case["theta_obs_deg"]), tp, 0.0)
+        kwargs = dict(E0_keV=case["E0_keV"], Ne=case["Ne"], thickness_ang=layers[-1][1], seed=case["seed"],
+                      elastic_model="sr", transport_core="per-electron", radiative_model="uncoupled",
+                      beam_dir=beam_dir, tilt_polar_rad=tp, beam_fwhm_mm=case["beam_fwhm_mm"],
+                      transport_lut_config=TransportLUTConfig(enabled=False), straggling=True)
+        if len(layers) == 1:
+            kwargs["composition"] = layers[0][2]
+        else:
+            kwargs["layers"] = layers
+        out = _simulate_trajectories(**kwargs)
+        arrays = {k: np.asarray(out[k]) for k in ROW_KEYS}
+        counts = np.array([int(out[k]) for k in COUNT_KEYS], dtype=np.int64)
+        _save(f"straggling_{name}", E0_keV=case["E0_keV"], E_cut_keV=5.0, seed=case["seed"], Ne=case["Ne"],
+              initial_r=out["initial_r_ang"], initial_v=out["initial_v_hat"], initial_E=out["initial_E_keV"],
+              count_names=np.array(COUNT_KEYS), counts=counts, **arrays)
+
+
+# ---------------------------------------------------------------------------
 # Summary tables (pyrite/montecarlo/trajectory_summary.py:147-260) of the
 # golden transport cases: the reference's own reductions of its own rows.
 # ---------------------------------------------------------------------------
@@ -1101,6 +1155,7 @@ GENERATORS = {
     "coherent_decoherence": gen_coherent_decoherence,
     "fullrun": gen_fullrun,
     "summary": gen_summary,
+    "straggling": gen_straggling,
 }
 
 

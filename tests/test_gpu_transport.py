@@ -146,3 +146,43 @@ def test_twiss_entries_match_the_host_restatement(cuda_device):
         i, j = first_g[e], first_r[e]
         np.testing.assert_allclose(got["r_mid"][i], ref["r_mid"][j], rtol=1e-12, atol=1e-6)
         np.testing.assert_allclose(got["v_hat"][i], ref["v_hat"][j], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("case", ["c20mev", "si30kev", "sio2_300kev"])
+def test_straggled_fp64_replays_reference(case, cuda_device):
+    """Urban energy-loss straggling (straggling=True): the FP64 exact core
+    with the reference's SplitMix64 streams replays the reference's own
+    straggled histories (make_golden.py --only straggling): every first row,
+    and at least 90 % of the histories row for row within 1e-10. A flight's
+    loss is a sum of Poisson counts drawn by comparing uniforms with
+    cumulative exp sums, so a last-bit difference of exp can move one count
+    and with it the rest of a history."""
+    d = golden(f"straggling_{case}")
+    g = golden(f"transport_{case}")
+    got = run(g, cuda_device, lut=False, straggling=True, entry=(d["initial_r"], d["initial_v"], d["initial_E"]))
+    assert got["device_status"] == 0
+    frac, first = history_agreement(d, got)
+    assert first
+    assert frac >= 0.9, frac
+
+
+def test_straggling_keeps_the_mean_loss(cuda_device):
+    """Philox, mixed precision: 300 keV electrons crossing a 1 um Si foil in a
+    single flight lose on average what the deterministic loss gives (the
+    Urban closure identity <dE> = |dE/dx| s), within 4 standard errors of the
+    straggled sample, and straggling spreads the single-flight losses."""
+    from pyrite_b200 import simulate_trajectories
+
+    kw = dict(E0_keV=300.0, Ne=8000, layers=[(0.0, 1.0e4, [("Si", 0.04994)])], E_cut_keV=5.0, seed=4,
+              rng="philox", precision="mixed", device=cuda_device, lut=False)
+    out = {}
+    for stg in (False, True):
+        r = simulate_trajectories(straggling=stg, **kw)
+        one = r["seg_count"] == 1
+        first = np.searchsorted(r["elec_id"], np.flatnonzero(one))
+        out[stg] = (r["E_keV"][first] - r["E_end_keV"][first]) / r["L_ang"][first]
+    det, stg = out[False], out[True]
+    assert det.size > 1000 and stg.size > 1000
+    se = np.std(stg) / np.sqrt(stg.size)
+    assert abs(stg.mean() - det.mean()) < 4.0 * se, (stg.mean(), det.mean(), se)
+    assert np.std(stg) > 10.0 * np.std(det)
