@@ -472,6 +472,35 @@ int pb_cxr_bin_lines(int64_t n_lines, const double *line_E, const double *line_a
                      const int32_t *line_dir, const int64_t *line_seg, int32_t dir0, int32_t n_dir_chunk,
                      int64_t n_seg, double lo_eV, double width_eV, int32_t n_bins, float *target, void *stream);
 
+/* Coherent route, record prologue: the per-row line records of
+ * pb_coherent_reduce from a segment list, for one detector direction
+ * (cxr.n_dir = 1), FP64, single slab. Replaces the reference's record
+ * building of cxr/_batched.py:561-660 (the complex PXR+CBS amplitude per
+ * polarisation of cxr/_batched.py:600-625, escape-piece ends and formation
+ * coefficients of cxr/_formation.py:58-81 and cxr/_batched.py:627-633, the
+ * exact vacuum centre, width and recoil phase over the electron's age of
+ * cxr/_recoil.py:118-147, the phase terms of cxr/_setup.py:1023-1026). Row g
+ * (a reflection x mosaic orientation, the row of cxr.tables) holds its kept
+ * pairs in segment order; rows follow one another (row_off[g] ..
+ * row_off[g+1], written by the call). Kept pairs past ``capacity`` are
+ * dropped and set PB_DEV_QUEUE_OVERFLOW. ``t_start`` holds each segment's
+ * start age [Angstrom] (NULL = 0). cxr.quadrature, the spectrum and line
+ * buffer fields are not read. */
+typedef struct pb_coherent_records_args {
+    pb_cxr_args cxr;           /* segments, direction, tables (n_dir = 1) */
+    const double *t_start;     /* [n_seg] or NULL */
+    int64_t capacity;          /* records each output array holds */
+    double *E_vac, *a_vac, *phase_slope, *g_phase, *cs_re, *cs_im, *cp_re, *cp_im, *L_esc, *half_dL, *apb,
+        *bma, *q;              /* [capacity] */
+    int64_t *row_off;          /* [n_g + 1] out */
+    void *work;                /* pb_coherent_records_work_size bytes, 256-byte aligned */
+    uint64_t work_bytes;
+    unsigned int *status;      /* device status word, OR-ed (NULL: not reported) */
+} pb_coherent_records_args;
+
+int pb_coherent_records_work_size(int64_t n_seg, int32_t n_g, uint64_t *bytes);
+int pb_coherent_records(const pb_coherent_records_args *args, void *stream);
+
 /* pb_cxr_score without any device allocation, for callers that cannot call
  * cudaMalloc: code running inside an allocator or memory-pool callback, an
  * embedding runtime that owns all device memory, or a deployment that fixes

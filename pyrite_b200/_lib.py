@@ -158,6 +158,15 @@ class PbCoherentArgs(C.Structure):
     ]
 
 
+class PbCoherentRecordsArgs(C.Structure):
+    _fields_ = [
+        ("cxr", PbCxrArgs), ("t_start", _vp), ("capacity", _i64), ("E_vac", _vp), ("a_vac", _vp),
+        ("phase_slope", _vp), ("g_phase", _vp), ("cs_re", _vp), ("cs_im", _vp), ("cp_re", _vp), ("cp_im", _vp),
+        ("L_esc", _vp), ("half_dL", _vp), ("apb", _vp), ("bma", _vp), ("q", _vp), ("row_off", _vp),
+        ("work", _vp), ("work_bytes", _u64), ("status", _vp),
+    ]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -183,6 +192,8 @@ EXPORTS = (
     "pb_cxr_bin_lines",
     "pb_coherent_work_size",
     "pb_coherent_reduce",
+    "pb_coherent_records_work_size",
+    "pb_coherent_records",
 )
 
 _lib = None

@@ -14,7 +14,11 @@ phases, a deterministic FP64 row sum.
 ``coherent_reduce`` takes the records of all rows at once;
 ``run_coherent_reduction_kernel`` keeps the reference's one-row signature
 (vacuum sinc, in-medium phase, formation factor and sinc window as optional
-groups, with the same pairing rules and errors).
+groups, with the same pairing rules and errors). ``coherent_records`` builds
+the records themselves on the device from a segment list
+(``pb_coherent_records``, the reference's record prologue
+``cxr/_batched.py:561-660``), and ``coherent_route_spectrum`` runs the whole
+route, segments to spectrum.
 """
 
 from __future__ import annotations
@@ -94,6 +98,76 @@ def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, s
         for t in h.keep:
             t.record_stream(stream)
     return spec
+
+
+def coherent_records(segments, E_grid_eV, *, tables, rows, n_hat, device=None, stream=None):
+    """The coherent route's per-row line records of one detector direction,
+    built on the device from ``segments`` (the reference's segment dict with
+    ``thickness_ang``, ``Ne`` and optional ``t_ang`` start ages) by
+    ``pb_coherent_records``: ``(records, row_count)``, ``records`` mapping
+    ``RECORD_FIELDS`` to FP64 device tensors laid out row after row (each row
+    its kept pairs in segment order), ``row_count`` a numpy array. ``rows``:
+    ``tables.ReflectionRows`` with one direction; ``tables``: ``LineTables``;
+    ``E_grid_eV`` sets the keep window as the incoherent scorer's."""
+    from .api import _fill_tables, _ptr, _segments_on_device
+    from .tables import line_keep_window
+
+    dev = _device(device)
+    lib = L.load()
+    h = _Holder(dev)
+    seg = _segments_on_device(h, segments)
+    n_g = int(rows.G.shape[0])
+    E_grid = np.asarray(E_grid_eV, dtype=np.float64)
+    lo_keep, hi_keep = line_keep_window(E_grid)
+    a = L.PbCoherentRecordsArgs()
+    c = a.cxr
+    c.precision = L.PB_FP64
+    c.n_dir = 1
+    nh = np.asarray(n_hat, dtype=float).reshape(3)
+    c.n_hat = _ptr(h.f64(nh / np.linalg.norm(nh)))
+    c.thickness = float(segments["thickness_ang"])
+    c.Ne = int(segments["Ne"])
+    c.n_seg = seg["n"]
+    c.r_mid, c.v_hat, c.L = _ptr(seg["r_mid"]), _ptr(seg["v_hat"]), _ptr(seg["L"])
+    c.E_keV, c.elec_id = _ptr(seg["E"]), _ptr(seg["elec_id"])
+    t = _fill_tables(h, rows, tables, lo_keep, hi_keep)
+    t.ES = _ptr(h.f64(np.asarray(rows.ES).reshape(-1, n_g, 3)[0]))
+    t.EP = _ptr(h.f64(np.asarray(rows.EP).reshape(-1, n_g, 3)[0]))
+    c.tables = t
+    a.cxr = c
+    t_ang = segments.get("t_ang")
+    a.t_start = _ptr(h.f64(t_ang)) if t_ang is not None else None
+    cap = max(1, seg["n"] * n_g)
+    a.capacity = cap
+    rec = {k: torch.empty(cap, dtype=torch.float64, device=dev) for k in RECORD_FIELDS}
+    for k in RECORD_FIELDS:
+        setattr(a, k, rec[k].data_ptr())
+    row_off = h.zeros(n_g + 1, torch.int64)
+    a.row_off = row_off.data_ptr()
+    nbytes = C.c_uint64()
+    L.check(lib.pb_coherent_records_work_size(seg["n"], n_g, C.byref(nbytes)), "pb_coherent_records_work_size")
+    work = h.empty((max(int(nbytes.value), 1),), torch.uint8)
+    a.work, a.work_bytes = work.data_ptr(), int(nbytes.value)
+    status = h.zeros(1, torch.int32)
+    a.status = status.data_ptr()
+    L.check(lib.pb_coherent_records(C.byref(a), _stream_ptr(stream)), "pb_coherent_records")
+    off = row_off.cpu().numpy()
+    if int(status.item()) != 0:
+        raise L.PyriteB200Error(f"pb_coherent_records: device status {int(status.item())}")
+    n_line = int(off[-1])
+    return {k: v[:n_line] for k, v in rec.items()}, np.diff(off)
+
+
+def coherent_route_spectrum(segments, E_grid_eV, delta_omega, *, tables, rows, n_hat, sinc_cutoff=None,
+                            device=None) -> np.ndarray:
+    """The coherent route end to end on the device for one direction:
+    records from the segments (``coherent_records``), every row reduced with
+    its mosaic weight (``pb_coherent_reduce``), divided by the electron
+    count -- [photons/eV/sr/electron] as the reference's coherent
+    ``mc_cxr_spectrum`` returns it (``cxr/_spectrum.py:285-318``)."""
+    rec, cnt = coherent_records(segments, E_grid_eV, tables=tables, rows=rows, n_hat=n_hat, device=device)
+    return coherent_spectrum(rec, cnt, np.asarray(rows.WM, dtype=float).reshape(-1), E_grid_eV, delta_omega,
+                             int(segments["Ne"]), sinc_cutoff=sinc_cutoff, device=device)
 
 
 def coherent_spectrum(records, row_count, row_weight, E_grid_eV, delta_omega, Ne, *, sinc_cutoff=None,

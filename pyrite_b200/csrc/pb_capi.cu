@@ -348,6 +348,47 @@ static int coherent_grid_ok(int32_t n_row, int64_t n_line, int32_t n_E) {
     return pb::coherent_items(n_row, n_line, n_E) <= (int64_t)INT32_MAX;
 }
 
+int pb_coherent_records_work_size(int64_t n_seg, int32_t n_g, uint64_t *bytes) {
+    if (!bytes) return fail(PB_ERR_INVALID, "pb_coherent_records_work_size: bytes is NULL");
+    if (n_seg < 0 || n_g < 1 || (n_g > 0 && n_seg > (int64_t)INT32_MAX))
+        return fail(PB_ERR_INVALID, "pb_coherent_records_work_size: need 0 <= n_seg < 2^31, n_g >= 1");
+    *bytes = pb::coherent_records_work_bytes(n_seg, n_g);
+    return PB_OK;
+}
+
+int pb_coherent_records(const pb_coherent_records_args *r, void *stream) {
+    if (!r) return fail(PB_ERR_INVALID, "pb_coherent_records: args is NULL");
+    const pb_cxr_args &a = r->cxr;
+    if (a.n_dir != 1) return fail(PB_ERR_INVALID, "pb_coherent_records: one direction per call (n_dir = 1)");
+    if (a.n_seg < 0 || a.n_seg > (int64_t)INT32_MAX)
+        return fail(PB_ERR_INVALID, "pb_coherent_records: need 0 <= n_seg < 2^31");
+    const pb_cxr_tables &t = a.tables;
+    if (t.n_g < 1 || t.n_tab < 2 || t.n_mu < 1 || t.n_mu > 4 || !t.G || !t.ES || !t.EP || !t.WM ||
+        !t.row_table || !t.E_tab || !t.chi_re || !t.chi_im || !t.u_re || !t.u_im || !t.log_mu || !t.delta)
+        return fail(PB_ERR_INVALID, "pb_coherent_records: incomplete reflection tables");
+    if (a.n_layer != 0) return fail(PB_ERR_UNSUPPORTED, "pb_coherent_records: single slab only (n_layer = 0)");
+    if (!r->row_off) return fail(PB_ERR_INVALID, "pb_coherent_records: row_off must be set");
+    if (a.n_seg == 0) {
+        cudaError_t e = cudaMemsetAsync(r->row_off, 0, sizeof(int64_t) * ((size_t)t.n_g + 1), (cudaStream_t)stream);
+        return e == cudaSuccess ? PB_OK : cuda_fail(e, "pb_coherent_records: zero row_off");
+    }
+    if (!a.n_hat || !a.r_mid || !a.v_hat || !a.L || !a.E_keV || !a.elec_id)
+        return fail(PB_ERR_INVALID, "pb_coherent_records: segment and direction pointers must be set");
+    if (r->capacity < 0 || (r->capacity > 0 && (!r->E_vac || !r->a_vac || !r->phase_slope || !r->g_phase ||
+                                                 !r->cs_re || !r->cs_im || !r->cp_re || !r->cp_im || !r->L_esc ||
+                                                 !r->half_dL || !r->apb || !r->bma || !r->q)))
+        return fail(PB_ERR_INVALID, "pb_coherent_records: every record array must be set for capacity > 0");
+    if (!r->work || reinterpret_cast<uintptr_t>(r->work) % 256 != 0)
+        return fail(PB_ERR_INVALID, "pb_coherent_records: work must be set and 256-byte aligned");
+    const uint64_t need = pb::coherent_records_work_bytes(a.n_seg, t.n_g);
+    if (r->work_bytes < need)
+        return fail(PB_ERR_CAPACITY, "pb_coherent_records: work holds %llu bytes, needs %llu",
+                    (unsigned long long)r->work_bytes, (unsigned long long)need);
+    cudaError_t e = pb::launch_coherent_records(*r, (cudaStream_t)stream, device_sms());
+    if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_records: launch");
+    return PB_OK;
+}
+
 int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes) {
     if (!bytes) return fail(PB_ERR_INVALID, "pb_coherent_work_size: bytes is NULL");
     if (!coherent_sizes_ok(n_row, n_line, n_E))

@@ -328,22 +328,39 @@ __device__ __forceinline__ bool pair_may_keep(const SegPre<Real> &sp, const RowP
     return !(dtail[ix - 1] * r_sqrt(sp.grad2) <= (Real)0.5 * denom_vac);
 }
 
-// The per-pair chain. ``E_tab``/``delta_tab``/``log_mu`` point at the
-// shared-memory staging (or global memory for a large FP64 grid).
+// The per-pair chain up to the complex PXR+CBS amplitude of both
+// polarisations (cxr/_batched.py:461-559 and 789-826): the resonance (three
+// Snell passes), the keep decision, the line's slope, the attenuation at the
+// line energy and the amplitudes. Shared by the incoherent line (pair_line)
+// and the coherent route's records (coh_records_kernel). ``E_tab`` /
+// ``delta_tab`` / ``log_mu`` point at the shared-memory staging (or global
+// memory for a large FP64 grid). The float path stops after the keep
+// decision for dropped pairs.
+template <class Real>
+struct PairAmps {
+    Real omega, E_res, slope, mu, v_dot_g, r_num, r_den;
+    Real A_re[2], A_im[2];
+    bool keep;
+};
+
 template <class Real, bool kLayered>
-__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
-                                const Real *E_tab, const Real *delta_tab, const Real *log_mu,
-                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti,
-                                const EscSeg<Real> *es, const pb_cxr_args &a, const Real *lay_t) {
+__device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                                    const Real *E_tab, const Real *delta_tab, const Real *log_mu,
+                                                    int n_tab, int n_mu, const pb_cxr_tables &t,
+                                                    const TabIndex &ti) {
     const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
     const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
     const Real hbarc = (Real)kHbarcEvAng;
+    PairAmps<Real> o;
     // cxr/_block_prologue.py:18-38, cxr/_recoil.py:79-97
     const Real r_num = (Real)0.5 * g2 * sp.inv_E;
     const Real r_den = n_dot_g * sp.inv_E;
     const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
     const Real v_dot_g_exact = v_dot_g - r_num;
     const Real denom_vac = sp.denom_row + r_den;
+    o.r_num = r_num;
+    o.r_den = r_den;
+    o.v_dot_g = v_dot_g;
     // cxr/_kernels.py:702-765
     Real denom = denom_vac, previous = denom, delta = (Real)NAN;
     for (int pass = 0; pass < 3; ++pass) {
@@ -370,18 +387,17 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
                                                            : (Real)1 - (Real)2 * delta + delta * delta * sp.grad2);
     const Real E_res = hbarc * omega;
     bool keep = sp.radiates && (E_res > (Real)t.lo_keep) && (E_res > (Real)10) && (E_res < (Real)t.hi_keep);
-    Line<Real> out;
-    out.good = false;
-    out.E_res = E_res;
-    out.a_width = (Real)NAN;
-    out.weight = (Real)NAN;
+    o.omega = omega;
+    o.E_res = E_res;
+    o.mu = (Real)0;
     // cxr/_block_prologue.py:53-62, cxr/_recoil.py:100-118
-    const Real slope = denom * rdiv((Real)1, (Real)1 - omega * sp.inv_E);
+    o.slope = denom * rdiv((Real)1, (Real)1 - omega * sp.inv_E);
     keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - rdiv((Real)1, sp.gamma));
+    o.keep = keep;
     if constexpr (sizeof(Real) == 4) {
         // The float path stops here for dropped pairs (FP64 completes every
         // pair so its per-pair output matches the reference's arrays).
-        if (!keep) return out;
+        if (!keep) return o;
     }
     int ix;
     Real fr;
@@ -415,10 +431,10 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
         if (ab) v = r_exp(lm[n_tab - 1]);
         mu += v;
     }
+    o.mu = mu;
     // cxr/_batched.py:789-826, cxr/_line_amplitude.py:14-37
     const Real h = (Real)(kHbarcEvAng / kMeEv);
     const Real k2 = k_mag * k_mag;
-    Real A2 = 0;
 #pragma unroll
     for (int pol = 0; pol < 2; ++pol) {
         const Real *Ev = pol == 0 ? rw.ES : rw.EP;
@@ -429,20 +445,37 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
         quantum_line_factors<Real>(h, sp.gamma, v_dot_g, k_dot_v, k_dot_g, g2, k2, v_dot_e, g_dot_e,
                                    k_dot_e, pxr_num, f_cbs);
         const Real f_pxr = rdiv(pxr_num, detuning);
-        const Real re = chi_re * f_pxr + u_re * f_cbs;
-        const Real im = chi_im * f_pxr + u_im * f_cbs;
-        const Real a2 = re * re + im * im;
-        A2 = pol == 0 ? a2 : A2 + a2;
+        o.A_re[pol] = chi_re * f_pxr + u_re * f_cbs;
+        o.A_im[pol] = chi_im * f_pxr + u_im * f_cbs;
     }
-    // cxr/_batched.py:702-730, cxr/_kernels.py:658-668
+    return o;
+}
+
+// The incoherent line of a pair: resonance, width and weight
+// (cxr/_batched.py:702-730, cxr/_kernels.py:658-668).
+template <class Real, bool kLayered>
+__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                const Real *E_tab, const Real *delta_tab, const Real *log_mu,
+                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti,
+                                const EscSeg<Real> *es, const pb_cxr_args &a, const Real *lay_t) {
+    const PairAmps<Real> p = pair_amps<Real, kLayered>(sp, rw, E_tab, delta_tab, log_mu, n_tab, n_mu, t, ti);
+    Line<Real> out;
+    out.good = false;
+    out.E_res = p.E_res;
+    out.a_width = (Real)NAN;
+    out.weight = (Real)NAN;
+    if constexpr (sizeof(Real) == 4) {
+        if (!p.keep) return out;
+    }
+    const Real A2 = (p.A_re[0] * p.A_re[0] + p.A_im[0] * p.A_im[0]) + (p.A_re[1] * p.A_re[1] + p.A_im[1] * p.A_im[1]);
     Real T_abs;
-    if constexpr (kLayered) T_abs = esc_transmission<Real>(*es, a, lay_t, (double)E_res);
-    else T_abs = mean_transmission<Real>(sp.path0 * mu, sp.path1 * mu);
+    if constexpr (kLayered) T_abs = esc_transmission<Real>(*es, a, lay_t, (double)p.E_res);
+    else T_abs = mean_transmission<Real>(sp.path0 * p.mu, sp.path1 * p.mu);
     const Real pref_c1 = (Real)(4.0 * (kPi * kPi) * kHbarcEvAng);
-    const Real pref = rdiv((Real)kAlphaFs * omega, pref_c1) * (sp.t_L * sp.t_L) * T_abs;
-    out.a_width = rdiv(slope * sp.t_L, (Real)2 * hbarc) * (Real)1;
+    const Real pref = rdiv((Real)kAlphaFs * p.omega, pref_c1) * (sp.t_L * sp.t_L) * T_abs;
+    out.a_width = rdiv(p.slope * sp.t_L, (Real)2 * (Real)kHbarcEvAng) * (Real)1;
     out.weight = pref * A2 * rw.wm;
-    out.good = keep && isfinite(out.weight) && (out.weight > (Real)0);
+    out.good = p.keep && isfinite(out.weight) && (out.weight > (Real)0);
     return out;
 }
 
@@ -1541,6 +1574,216 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
 cudaError_t launch_cxr(const pb_cxr_args &a, cudaStream_t s, int sms) {
     if (a.precision == PB_MIXED) return launch_cxr_t<float>(a, s, sms, a.far_pad);
     return launch_cxr_t<double>(a, s, sms, a.far_pad);
+}
+
+// ---------------------------------------------------------------------------
+// Coherent route: per-row line records from the segment list (FP64).
+//
+// For every (segment, reflection row) pair the chain of pair_amps gives the
+// complex PXR+CBS amplitude of both polarisations; the record adds the
+// segment's escape-piece ends and formation coefficients, the exact vacuum
+// line centre and width with the recoil phase over the electron's age, and
+// the phase terms (cxr/_batched.py:561-660, cxr/_formation.py:58-81,
+// cxr/_recoil.py:118-147, cxr/_setup.py:1023-1026). Rows hold their kept
+// pairs in segment order, row after row (row_off), as the reference's block
+// loop lays them out and pb_coherent_reduce reads them: pass 1 flags the kept
+// pairs [row][segment], pass 2 scans each row, pass 3 writes the records.
+// ---------------------------------------------------------------------------
+struct CohRec {
+    double f[13];  // E_vac, a_vac, phase_slope, g_phase, cs_re, cs_im, cp_re, cp_im, L_esc, half_dL, apb, bma, q
+};
+
+// cxr/_formation.py:58-81
+__device__ __forceinline__ void formation_coefficients(double tau_start, double tau_end, double &apb, double &bma,
+                                                       double &q) {
+    q = 0.25 * (tau_end - tau_start);
+    if (fabs(q) < 0.5) {
+        const double c0 = exp(-0.25 * (tau_start + tau_end));
+        apb = 2.0 * c0 * cosh(q);
+        bma = -2.0 * c0 * sinh(q);
+    } else {
+        const double ea = exp(-0.5 * tau_start), eb = exp(-0.5 * tau_end);
+        apb = ea + eb;
+        bma = eb - ea;
+    }
+}
+
+__device__ bool coh_record(const pb_cxr_args &a, const double *t_start, int64_t s, int g, const TabIndex &ti,
+                           CohRec *rec) {
+    SegPre<double> sp;
+    seg_precompute<double>(sp, a, s, a.n_hat);
+    RowPre<double> rw;
+    const double *nh = a.n_hat;
+    for (int c = 0; c < 3; ++c) {
+        rw.G[c] = a.tables.G[3 * g + c];
+        rw.ES[c] = a.tables.ES[3 * g + c];
+        rw.EP[c] = a.tables.EP[3 * g + c];
+    }
+    rw.g2 = rw.G[0] * rw.G[0] + rw.G[1] * rw.G[1] + rw.G[2] * rw.G[2];
+    rw.n_dot_g = rw.G[0] * nh[0] + rw.G[1] * nh[1] + rw.G[2] * nh[2];
+    rw.g_dot_es = rw.G[0] * rw.ES[0] + rw.G[1] * rw.ES[1] + rw.G[2] * rw.ES[2];
+    rw.g_dot_ep = rw.G[0] * rw.EP[0] + rw.G[1] * rw.EP[1] + rw.G[2] * rw.EP[2];
+    rw.wm = a.tables.WM[g];
+    rw.row = a.tables.row_table[g];
+    const int n_tab = a.tables.n_tab;
+    const PairAmps<double> p = pair_amps<double, false>(sp, rw, a.tables.E_tab, a.tables.delta, a.tables.log_mu,
+                                                        n_tab, a.tables.n_mu, a.tables, ti);
+    double apb, bma, qq;
+    formation_coefficients(sp.path0 * p.mu, sp.path1 * p.mu, apb, bma, qq);
+    // exact vacuum centre / width and recoil phase over the age, with the
+    // vacuum denominator and n.g of the row (cxr/_recoil.py:118-147)
+    const double numerator = p.v_dot_g - p.r_num;
+    const double den = sp.denom_row + p.r_den;
+    const double E_c = kHbarcEvAng * numerator / den;
+    const double x = numerator / den * sp.inv_E;
+    const double kappa = 1.0 / (1.0 - x);
+    const double a_vac = kappa * den * sp.t_L / (2.0 * kHbarcEvAng);
+    const double t_mid = (t_start ? t_start[s] : 0.0) + 0.5 * sp.t_L;
+    const double rx = a.r_mid[3 * s], ry = a.r_mid[3 * s + 1], rz = a.r_mid[3 * s + 2];
+    const double d_geom = t_mid - (rx * nh[0] + ry * nh[1] + rz * nh[2]);
+    const double d_shift = kappa * (x * sp.denom_row + p.r_den) * t_mid;
+    const double g_shift = kappa * (x * p.v_dot_g - p.r_num) * t_mid;
+    const double amp = sqrt(kAlphaFs * p.omega / (4.0 * (kPi * kPi) * kHbarcEvAng));
+    const double cs_re = amp * sp.t_L * p.A_re[0], cs_im = amp * sp.t_L * p.A_im[0];
+    const double cp_re = amp * sp.t_L * p.A_re[1], cp_im = amp * sp.t_L * p.A_im[1];
+    const bool good = p.keep && isfinite(amp) && amp > 0.0 && sp.t_L > 0.0 && isfinite(apb) && apb > 0.0 &&
+                      isfinite(bma) && isfinite(cs_re) && isfinite(cs_im) && isfinite(cp_re) && isfinite(cp_im);
+    if (rec && good) {
+        // record fields (cxr/_batched.py:646-660)
+        rec->f[0] = E_c;
+        rec->f[1] = a_vac;
+        rec->f[2] = (d_geom + d_shift) / kHbarcEvAng;
+        rec->f[3] = rx * rw.G[0] + ry * rw.G[1] + rz * rw.G[2] + g_shift;
+        rec->f[4] = cs_re;
+        rec->f[5] = cs_im;
+        rec->f[6] = cp_re;
+        rec->f[7] = cp_im;
+        rec->f[8] = 0.5 * (sp.path0 + sp.path1);
+        rec->f[9] = 0.5 * (sp.path1 - sp.path0);
+        rec->f[10] = apb;
+        rec->f[11] = bma;
+        rec->f[12] = qq;
+    }
+    return good;
+}
+
+__device__ __forceinline__ TabIndex tab_index_of(const pb_cxr_tables &t) {
+    TabIndex ti{};
+    ti.geometric = t.tab_log_step > 0.0;
+    ti.log0 = t.tab_log0;
+    ti.inv_h = ti.geometric ? 1.0 / t.tab_log_step : 0.0;
+    return ti;
+}
+
+// Pass 1: kept flags, row-major [g][s].
+__global__ void coh_rec_flags_kernel(const pb_cxr_args a, const double *t_start, int64_t n_seg, uint8_t *flags) {
+    const TabIndex ti = tab_index_of(a.tables);
+    const int n_g = a.tables.n_g;
+    const int64_t n = n_seg * (int64_t)n_g;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = q / n_g;
+        const int g = (int)(q - s * n_g);
+        flags[(int64_t)g * n_seg + s] = coh_record(a, t_start, s, g, ti, nullptr) ? 1 : 0;
+    }
+}
+
+// Pass 2: exclusive scan of one row's flags (one block per row) and its count.
+__global__ void __launch_bounds__(1024) coh_rec_scan_kernel(int64_t n_seg, const uint8_t *flags, int32_t *pos,
+                                                           int64_t *count) {
+    __shared__ int64_t warp_sum[32];
+    __shared__ int64_t carry;
+    const int g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint8_t *f = flags + (int64_t)g * n_seg;
+    int32_t *o = pos + (int64_t)g * n_seg;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < n_seg; base += 1024) {
+        const int64_t s = base + tid;
+        const int v = s < n_seg ? f[s] : 0;
+        int incl = v;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        if (lane == 31) warp_sum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int64_t w = warp_sum[lane];
+            int64_t wi = w;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int64_t u = __shfl_up_sync(0xffffffffu, wi, d);
+                if (lane >= d) wi += u;
+            }
+            warp_sum[lane] = wi - w;  // exclusive prefix of the warps
+        }
+        __syncthreads();
+        const int64_t excl = carry + warp_sum[warp] + incl - v;
+        if (s < n_seg) o[s] = (int32_t)excl;
+        __syncthreads();
+        if (tid == 1023) carry = excl + v;
+        __syncthreads();
+    }
+    if (tid == 0) count[g] = carry;
+}
+
+// Row offsets from the counts (one thread: rows are few).
+__global__ void coh_rec_offsets_kernel(int n_g, const int64_t *count, int64_t *row_off) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int64_t run = 0;
+        row_off[0] = 0;
+        for (int g = 0; g < n_g; ++g) {
+            run += count[g];
+            row_off[g + 1] = run;
+        }
+    }
+}
+
+// Pass 3: the records of the kept pairs at their row positions.
+__global__ void coh_rec_write_kernel(const pb_coherent_records_args r, const uint8_t *flags, const int32_t *pos) {
+    const pb_cxr_args &a = r.cxr;
+    const TabIndex ti = tab_index_of(a.tables);
+    const int n_g = a.tables.n_g;
+    const int64_t n_seg = a.n_seg;
+    const int64_t n = n_seg * (int64_t)n_g;
+    double *const out[13] = {r.E_vac, r.a_vac, r.phase_slope, r.g_phase, r.cs_re, r.cs_im, r.cp_re,
+                             r.cp_im, r.L_esc, r.half_dL, r.apb, r.bma, r.q};
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = q / n_g;
+        const int g = (int)(q - s * n_g);
+        const int64_t fi = (int64_t)g * n_seg + s;
+        if (!flags[fi]) continue;
+        CohRec rec;
+        if (!coh_record(a, r.t_start, s, g, ti, &rec)) continue;
+        const int64_t slot = r.row_off[g] + pos[fi];
+        if (slot >= r.capacity) {
+            set_status(r.status, PB_DEV_QUEUE_OVERFLOW);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < 13; ++k) out[k][slot] = rec.f[k];
+    }
+}
+
+uint64_t coherent_records_work_bytes(int64_t n_seg, int n_g) {
+    const uint64_t pairs = (uint64_t)n_seg * (uint64_t)n_g;
+    const auto al = [](uint64_t b) { return (b + 255) / 256 * 256; };
+    return al(pairs) + al(pairs * 4) + al((uint64_t)n_g * 8);
+}
+
+cudaError_t launch_coherent_records(const pb_coherent_records_args &r, cudaStream_t s, int sms) {
+    const int64_t n_seg = r.cxr.n_seg;
+    const int n_g = r.cxr.tables.n_g;
+    const uint64_t pairs = (uint64_t)n_seg * (uint64_t)n_g;
+    const auto al = [](uint64_t b) { return (b + 255) / 256 * 256; };
+    uint8_t *flags = static_cast<uint8_t *>(r.work);
+    int32_t *pos = reinterpret_cast<int32_t *>(static_cast<uint8_t *>(r.work) + al(pairs));
+    int64_t *count = reinterpret_cast<int64_t *>(static_cast<uint8_t *>(r.work) + al(pairs) + al(pairs * 4));
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((int64_t)((pairs + 255) / 256), (int64_t)sms * 8));
+    coh_rec_flags_kernel<<<(unsigned)blocks, 256, 0, s>>>(r.cxr, r.t_start, n_seg, flags);
+    coh_rec_scan_kernel<<<(unsigned)n_g, 1024, 0, s>>>(n_seg, flags, pos, count);
+    coh_rec_offsets_kernel<<<1, 32, 0, s>>>(n_g, count, r.row_off);
+    coh_rec_write_kernel<<<(unsigned)blocks, 256, 0, s>>>(r, flags, pos);
+    return cudaGetLastError();
 }
 
 // Coarse per-pair binning of a line buffer (surrogate training targets).

@@ -48,6 +48,9 @@ uint64_t coherent_work_bytes(int n_row, int64_t n_line, int n_E);
 int64_t coherent_items(int n_row, int64_t n_line, int n_E);
 cudaError_t launch_coherent(const pb_coherent_args &a, cudaStream_t s);
 
+uint64_t coherent_records_work_bytes(int64_t n_seg, int n_g);
+cudaError_t launch_coherent_records(const pb_coherent_records_args &r, cudaStream_t s, int sms);
+
 // Record the message pb_last_error() returns on this thread.
 void set_last_error(const char *msg);
 

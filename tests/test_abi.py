@@ -34,7 +34,7 @@ STRUCTS = {
     "pb_layers": L.PbLayers, "pb_lut": L.PbLut, "pb_beam": L.PbBeam, "pb_rows": L.PbRows,
     "pb_segments": L.PbSegments, "pb_tallies": L.PbTallies, "pb_transport_args": L.PbTransportArgs,
     "pb_cxr_tables": L.PbCxrTables, "pb_cxr_args": L.PbCxrArgs, "pb_brem_args": L.PbBremArgs,
-    "pb_coherent_args": L.PbCoherentArgs,
+    "pb_coherent_args": L.PbCoherentArgs, "pb_coherent_records_args": L.PbCoherentRecordsArgs,
 }
 
 

@@ -453,6 +453,37 @@ def test_gpu_coherent_matches_reference(name):
     _assert_close(got, spec)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_coherent_records_and_route_match_reference(name):
+    """The device record prologue (``pb_coherent_records``) from the fixture's
+    segments (with start ages) and line tables: the reference's per-row line
+    records -- the same pairs kept in the same order (equal row counts), every
+    field within 1e-10 -- and the whole device route, segments -> records ->
+    reduction, the reference's coherent spectrum within the reduction's
+    tolerance (2e-5 of the peak, 1e-4 relative above 1e-3 of it)."""
+    from pyrite_b200 import LineTables
+    from pyrite_b200.coherent import coherent_records, coherent_route_spectrum
+    from pyrite_b200.tables import ReflectionRows
+
+    c = np.load(GOLDEN / f"cxr_{name}.npz")
+    tr = np.load(GOLDEN / f"transport_{c['transport']}.npz")
+    n_elec = COHERENT_ELECTRONS[name]
+    sel = tr["elec_id"] < n_elec
+    seg = dict(v_hat=tr["v_hat"][sel], E_keV=tr["E_repr_keV"][sel], L_ang=tr["L_ang"][sel],
+               r_mid=tr["r_mid"][sel], elec_id=tr["elec_id"][sel], t_ang=tr["t_ang"][sel], Ne=n_elec,
+               thickness_ang=float(c["thickness"]))
+    tables = LineTables(c["E_tab"], c["chi_re"], c["chi_im"], c["u_re"], c["u_im"], c["log_mu"], c["delta"])
+    rows = ReflectionRows(c["G"], c["ES"][None], c["EP"][None], c["WM"], c["row_table"])
+    rec, cnt = coherent_records(seg, c["E_grid"], tables=tables, rows=rows, n_hat=c["n_hat"])
+    z = np.load(GOLDEN / f"coherent_{name}.npz")
+    assert np.array_equal(cnt, z["row_count"])
+    for f in oc.FIELDS:
+        np.testing.assert_allclose(rec[f].cpu().numpy(), z[f], rtol=1e-10, atol=1e-300, err_msg=f)
+    got = coherent_route_spectrum(seg, z["E_grid"], z["delta_omega"], tables=tables, rows=rows, n_hat=c["n_hat"])
+    _assert_close(got, z["spec"])
+
+
 def _random_rows(rng, n_rows, n_per_row, E_lo, E_hi):
     n = n_rows * n_per_row
     E_vac = rng.uniform(E_lo, E_hi, n)
