@@ -34,16 +34,21 @@ sys.path.insert(0, str(ROOT))
 METRIC = "e- histories/s on 1 B200: surrogate+mixed vs plain FP64, at <=1% spectrum error"
 UNIT = "histories/s"
 ALG_FLOPS_PAIR = 300.0   # FP32 census of one (segment, reflection, tile) line: kinematics, amplitudes, escape
+ALG_FLOPS_ITEM = 80.0    # FP32 flops of one (line, bin) item of the bin-mean deposit
 # Surrogate: one (segment, tile) pair through the hidden layers, 2 (6*256 + 3*256*256); the linear
 # output layer is applied once per tile to the length-weighted sums, not per pair.
 ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
-# Bethe-Heitler + Elwert per (segment, tile, energy): ~60 flops of dsigma/dk shared by the 16 tiles plus
-# ~15 of segment-mean escape per tile (transcendental-heavy: the FP32 roofline is a loose bound).
-ALG_FLOPS_BREM = 20.0
+# Bethe-Heitler + Elwert per (segment, energy), all the tiles of one exit face at once (direction
+# moments): the cross section (sqrt, log, reciprocal, and exp + reciprocal of the Elwert factor per
+# element) and the escape at the band centre (two exponentials) are 7 transcendentals on the SFU,
+# beside ~58 FP32 flops (FMA = 2); the tiles are rebuilt from the moments once per 256 segments.
+BREM_SFU_PER_PAIR = 7.0
+ALG_FLOPS_BREM = 58.0
+SFU_OPS_PER_SM_CLOCK = 16.0  # MUFU lanes per SM per cycle
 # DRAM bytes (read + write) per history of the three scorers, from one ncu
 # capture each of a 2,048-history batch of this workload (profiles/*_si50_2048hist.md);
 # a kernel's traffic grows with its segments, so a full launch is this x histories.
-DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 7.0e6 / 2048, "brem_kernel": 5.226752e6 / 2048,
+DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 7.0e6 / 2048, "brem_kernel": 5.259264e6 / 2048,
                           "mlp_infer_kernel": 5.484032e6 / 2048}
 BENCH_SEED = 12345  # seed of the 50 MeV Si scene in every arm
 MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"]) \
@@ -591,7 +596,12 @@ def main():
 
     # 1. exact mixed precision (FP32 flight and lines, FP64 bookkeeping)
     mixed_case = ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H)
+    cxr_counters = torch.zeros(2, dtype=torch.int64, device="cuda")
+    mixed_case.cargs.counters = cxr_counters.data_ptr()  # kept lines, deposit items (comparison pass only)
     compare_pass("mixed", mixed_case)
+    mixed_case.cargs.counters = None
+    cxr_work = {"lines_kept": int(cxr_counters[0].item()), "deposit_items": int(cxr_counters[1].item()),
+                "segments": int(mixed_case.seg_count.item()) * C}  # approximate: last batch's count x C
     arm("mixed", mixed_case, args.steps)
     # 2. surrogate + exact control variate on the same histories
     sur = None
@@ -704,19 +714,38 @@ def main():
     ce = cases["mixed"]
     n_seg = mixed["res"]["segments_last_batch"]
     n_g, n_dir, n_E = int(ce.rows.G.shape[0]), ce.n_dir, ce.n_E
+    n_g_cxr = n_g
     pairs = n_seg * n_g * n_dir
     peak_fp32 = 148 * 128 * 2 * 1.965e9 / 1e12
     cxr_tflops = pairs * ALG_FLOPS_PAIR / (mixed["t_cxr"] / 1e3) / 1e12
-    brem_flops = n_seg * n_dir * n_E * ALG_FLOPS_BREM
-    brem_tflops = brem_flops / (r_head["t_brem"] / 1e3) / 1e12
+    # Second census with the bin-mean deposit: (line, bin) items per pair from
+    # the comparison pass's counters, ~80 FP32 flops each (midpoint series,
+    # closed far form or antiderivative difference).
+    items_per_pair = cxr_work["deposit_items"] / max(1.0, cxr_work["segments"] * n_g_cxr * mixed_case.n_dir)
+    cxr_tflops_dep = pairs * (ALG_FLOPS_PAIR + items_per_pair * ALG_FLOPS_ITEM) / (mixed["t_cxr"] / 1e3) / 1e12
+    brem_pairs_s = n_seg * n_E / (r_head["t_brem"] / 1e3)
+    sm_mhz = (clocks[head].get("sm_mhz") or 1965.0)
+    sfu_ceiling = 148 * sm_mhz * 1e6 * SFU_OPS_PER_SM_CLOCK / BREM_SFU_PER_PAIR
     rooflines = {
         "cxr_kernel": {"bound": "fp32", "kernel": "cxr_kernel<float> (exact PXR+CBS lines + bin-mean deposit)",
                        "achieved": cxr_tflops, "peak": peak_fp32, "unit": "TFLOP/s", "frac": cxr_tflops / peak_fp32,
                        "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
+                       "census": "%g FP32 flops per (segment, reflection, tile) pair" % ALG_FLOPS_PAIR,
+                       "with_deposit": {"achieved": cxr_tflops_dep, "frac": cxr_tflops_dep / peak_fp32,
+                                        "items_per_pair": items_per_pair, "lines_kept": cxr_work["lines_kept"],
+                                        "deposit_items": cxr_work["deposit_items"],
+                                        "census": "%g per pair + %g per (line, bin) item" % (ALG_FLOPS_PAIR,
+                                                                                           ALG_FLOPS_ITEM)},
                        "traffic": DRAM_BYTES_PER_HISTORY["cxr_kernel"] * H},
-        "brem_kernel": {"bound": "fp32", "kernel": "brem_kernel<float> (Bethe-Heitler + Elwert, 16 tiles)",
-                        "achieved": brem_tflops, "peak": peak_fp32, "unit": "TFLOP/s",
-                        "frac": brem_tflops / peak_fp32, "peak_source": "nominal FP32 CUDA-core peak",
+        "brem_kernel": {"bound": "sfu", "kernel": "brem_kernel<float> (Bethe-Heitler + Elwert, 16 tiles by "
+                                                  "direction moments)",
+                        "achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
+                        "frac": brem_pairs_s / sfu_ceiling,
+                        "peak_source": "SFU ceiling: 148 SM x measured SM clock x 16 MUFU lanes / %g "
+                                       "transcendentals per pair" % BREM_SFU_PER_PAIR,
+                        "fp32": {"achieved_tflops": brem_pairs_s * ALG_FLOPS_BREM / 1e12, "peak_tflops": peak_fp32,
+                                 "frac": brem_pairs_s * ALG_FLOPS_BREM / 1e12 / peak_fp32,
+                                 "census": "%g FP32 flops per pair" % ALG_FLOPS_BREM},
                         "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H},
     }
     if sur is not None:

@@ -278,6 +278,9 @@ typedef struct pb_cxr_args {
      * layer equals emit_layer radiate. */
     const int32_t *seg_layer;
     int32_t emit_layer;
+    /* ABI 4, optional (NULL skips): work counters added to by the call,
+     * [0] lines kept, [1] (line, bin) items deposited (bin-mean). */
+    unsigned long long *counters;
 } pb_cxr_args;
 
 typedef struct pb_brem_args {

@@ -104,7 +104,7 @@ class PbCxrArgs(C.Structure):
         ("line_w", _vp), ("line_dir", _vp), ("pair_E", _vp), ("pair_a", _vp), ("pair_w", _vp),
         ("pair_good", _vp), ("status", _vp), ("line_seg", _vp),
         ("n_layer", _i32), ("z_top", _vp), ("z_bot", _vp), ("mu_off", _vp), ("mu_knot", _vp),
-        ("mu_value", _vp), ("mu_slope", _vp), ("seg_layer", _vp), ("emit_layer", _i32),
+        ("mu_value", _vp), ("mu_slope", _vp), ("seg_layer", _vp), ("emit_layer", _i32), ("counters", _vp),
     ]
 
 

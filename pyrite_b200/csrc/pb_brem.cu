@@ -303,6 +303,204 @@ __device__ __forceinline__ float brem_moment_eval(const float (&Q)[N + 1], float
     return r;
 }
 
+// ---------------------------------------------------------------------------
+// Packed moment kernel: the float path for directions on one exit face with
+// rho <= 0.01 (order-3 moments; a single direction is the order-0 case of the
+// same recurrences). Two photon energies per thread on packed FP32x2
+// arithmetic (fma/mul/add.rn.f32x2), so the non-SFU instructions of a
+// (segment, energy) pair are issued once per two pairs; the moments Q_n of
+// both energies are summed in FP64 registers across the chunks and the
+// directions are rebuilt once at the end (the reconstruction is linear in
+// Q_n), so no per-direction accumulators are kept. For relativistic final
+// states (1/beta_f - 1 < 0.01, T_f > ~3 MeV) the Elwert factor's reciprocal
+// 1/(1 - exp(-z/beta_f)) comes from its series in s = z (1/beta_f - 1):
+//   G0 [1 - rho s + (rho/2 + rho^2) s^2 - (rho/6 + rho^2 + rho^3) s^3],
+//   G0 = 1/(1 - e^-z), rho = e^-z G0, z = 2 pi Z alpha,
+// truncation below (rho s)^4 < 1e-8 for Z <= 92; elsewhere the SFU form.
+// ---------------------------------------------------------------------------
+struct F2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float lo, float hi) { return F2{f2_pack(lo, hi)}; }
+__device__ __forceinline__ F2 f2s(float x) { return F2{f2_pack(x, x)}; }
+__device__ __forceinline__ float f2lo(F2 a) { float l, h; f2_unpack(a.v, l, h); return l; }
+__device__ __forceinline__ float f2hi(F2 a) { float l, h; f2_unpack(a.v, l, h); return h; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{f2_mul(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a.v), "l"(b.v));
+    return F2{d};
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2{f2_fma(a.v, b.v, c.v)}; }
+__device__ __forceinline__ F2 neg2(F2 a) { return F2{a.v ^ 0x8000000080000000ull}; }
+__device__ __forceinline__ F2 ex2_2(F2 a) { float l, h; f2_unpack(a.v, l, h); return f2(ex2_approx(l), ex2_approx(h)); }
+__device__ __forceinline__ F2 rcp_2(F2 a) { float l, h; f2_unpack(a.v, l, h); return f2(rcp_approx(l), rcp_approx(h)); }
+__device__ __forceinline__ F2 rsqrt_2(F2 a) {
+    float l, h;
+    f2_unpack(a.v, l, h);
+    return f2(rsqrt_approx(l), rsqrt_approx(h));
+}
+__device__ __forceinline__ F2 lg2_2(F2 a) { float l, h; f2_unpack(a.v, l, h); return f2(lg2_approx(l), lg2_approx(h)); }
+
+constexpr int kBremPackedThreads = 256;  // x 2 energies
+
+// Whether the launch's directions take the packed moment kernel: one exit
+// face and relative spread rho = Delta / f_min <= 0.01 (the same test both
+// brem kernels make, so exactly one of them scores the launch).
+__device__ __forceinline__ bool brem_packed_applies(const pb_brem_args &a, int d0, int nd, double &f_c, double &dl) {
+    int n_up = 0;
+    double f_lo = 1e300, f_hi = 0.0;
+    for (int dd = 0; dd < nd; ++dd) {
+        const double nz = a.n_hat[3 * (d0 + dd) + 2];
+        n_up += nz < 0.0 ? 1 : 0;
+        const double f = 1.0 / fmax(fabs(nz), 1.0e-12);
+        f_lo = fmin(f_lo, f);
+        f_hi = fmax(f_hi, f);
+    }
+    f_c = 0.5 * (f_lo + f_hi);
+    dl = 0.5 * (f_hi - f_lo);
+    return (n_up == nd || n_up == 0) && dl <= 0.01 * f_lo;
+}
+
+template <int NEL>
+__global__ void __launch_bounds__(kBremPackedThreads, 3)
+    brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
+    __shared__ BremSeg<float> segs[kBremChunk];
+    __shared__ double sQ[8][kBremPackedThreads];  // FP64 moment sums: [energy half * 4 + n][thread]
+    const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
+    double f_c_d, dl_d;
+    if (a.precision != PB_MIXED || !brem_packed_applies(a, d0, nd, f_c_d, dl_d)) return;
+    const bool up_all = a.n_hat[3 * d0 + 2] < 0.0;
+    const float T_slab = (float)a.thickness;
+    const float mc2 = 510.99895f, inv_mc2 = 1.0f / 510.99895f;
+    const float za = (float)(2.0 * kPi * kAlphaFs);
+    const int e0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const bool on_a = e0 < a.n_E, on_b = e0 + 1 < a.n_E;
+    // per-energy constants, packed (energy e0 low, e0 + 1 high)
+    double kd[2], mud[2];
+    for (int h = 0; h < 2; ++h) {
+        const int e = e0 + h;
+        const bool on = e < a.n_E;
+        kd[h] = on ? a.E_grid[e] / 1e3 : 0.0;  // k = 0 marks an idle lane: no pair is valid
+        mud[h] = on ? a.mu[e] : 0.0;
+    }
+    const F2 k2 = f2((float)kd[0], (float)kd[1]);
+    const F2 kc = f2((float)(kd[0] / (510.99895 * 510.99895)), (float)(kd[1] / (510.99895 * 510.99895)));
+    const F2 c2mk = f2((float)(2.0 * 510.99895 - kd[0]), (float)(2.0 * 510.99895 - kd[1]));
+    const double c0 = 16.0 / 3.0 * kAlphaFs * kReCm2 * 0.6931471805599453;
+    const F2 c0k = f2((float)(c0 / fmax(kd[0] * 1e3, 1e-30)), (float)(c0 / fmax(kd[1] * 1e3, 1e-30)));
+    const F2 nmu_l2fc = f2((float)(-mud[0] * 1.4426950408889634 * f_c_d), (float)(-mud[1] * 1.4426950408889634 * f_c_d));
+    const F2 mu_fc = f2((float)(mud[0] * f_c_d), (float)(mud[1] * f_c_d));
+    const F2 inv_mu = f2(mud[0] > 0.0 ? (float)(1.0 / mud[0]) : 0.0f, mud[1] > 0.0 ? (float)(1.0 / mud[1]) : 0.0f);
+    const F2 nmu_dl = f2((float)(-mud[0] * dl_d), (float)(-mud[1] * dl_d));
+    const F2 dl2 = f2s((float)dl_d);
+    const float f_c = (float)f_c_d;
+    // Elwert constants per element: z log2(e) for the SFU form; G0 and rho
+    // of the relativistic series.
+    float zl[NEL], zn[NEL], G0[NEL], rh[NEL];
+#pragma unroll
+    for (int el = 0; el < NEL; ++el) {
+        const double z = 2.0 * kPi * kAlphaFs * a.Z[el];
+        const double ez = exp(-z);
+        zl[el] = (float)(z * 1.4426950408889634);
+        zn[el] = (float)z;
+        G0[el] = (float)(1.0 / (1.0 - ez));
+        rh[el] = (float)(ez / (1.0 - ez));
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) sQ[i][threadIdx.x] = 0.0;
+    const bool act_a = kd[0] > 0.0, act_b = kd[1] > 0.0;
+    int64_t live = n_seg;
+    if (a.n_seg_device && (int64_t)*a.n_seg_device < live) live = (int64_t)*a.n_seg_device;
+    const int64_t per = (live + gridDim.y - 1) / gridDim.y;
+    const int64_t s_begin = per * blockIdx.y;
+    int64_t s_end = s_begin + per < live ? s_begin + per : live;
+    if (s_end < s_begin) s_end = s_begin;
+    for (int64_t c0s = s_begin; c0s < s_end; c0s += kBremChunk) {
+        const int nc = (int)((s_end - c0s) < kBremChunk ? (s_end - c0s) : kBremChunk);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) brem_stage<float>(segs[j], a, c0s + j, T_slab, mc2, za);
+        __syncthreads();
+        if (!on_a) continue;
+        F2 Q0 = f2s(0.0f), Q1 = f2s(0.0f), Q2 = f2s(0.0f), Q3 = f2s(0.0f);
+        for (int j = 0; j < nc; ++j) {
+            const BremSeg<float> &b = segs[j];
+            F2 Tf = f2s(b.T) + neg2(k2);
+            const float tfl = f2lo(Tf), tfh = f2hi(Tf);
+            const bool va = tfl > 1e-6f && act_a, vb = tfh > 1e-6f && act_b;
+            if (!va && !vb) continue;
+            Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
+            // cross section (brem_nsig's float form, both energies at once)
+            const F2 q = Tf * (Tf + f2s(2.0f * mc2));
+            const F2 rs = rsqrt_2(q);
+            const F2 p_f = (q * rs) * f2s(inv_mc2);
+            const F2 sp = f2s(b.p_i) + p_f;
+            const F2 dpp = kc * (f2s(2.0f * b.T) + c2mk);
+            const F2 lg = lg2_2((sp * sp) * rcp_2(dpp));
+            const F2 inv_bf = fma2(Tf, f2s(inv_mc2), f2s(1.0f)) * (rs * f2s(mc2));
+            const F2 common = (c0k * f2s(b.beta_i)) * (lg * inv_bf);  // beta_i holds beta_i / p_i^2
+            F2 nsig = f2s(0.0f);
+            const F2 del = inv_bf + f2s(-1.0f);
+            const bool rel = f2lo(del) < 0.01f && f2hi(del) < 0.01f;
+#pragma unroll
+            for (int el = 0; el < NEL; ++el) {
+                F2 ginv;
+                if (rel) {
+                    const F2 sz = del * f2s(zn[el]);
+                    const float r = rh[el], r2 = r * r;
+                    const F2 poly = fma2(sz, fma2(sz, fma2(sz, f2s(-(r / 6.0f + r2 + r2 * r)), f2s(0.5f * r + r2)),
+                                                  f2s(-r)), f2s(1.0f));
+                    ginv = poly * f2s(G0[el]);
+                } else {
+                    ginv = rcp_2(f2s(1.0f) + neg2(ex2_2(neg2(inv_bf * f2s(zl[el])))));
+                }
+                nsig = fma2(f2s(b.nL[el]) * common, ginv, nsig);  // nL holds n L Z^2 den_i
+            }
+            nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
+            // escape moments (brem_moment_chunk, order 3, both energies)
+            const float es = up_all ? b.e0 : b.e1;
+            const float ef = es + b.e2;
+            const F2 Ea = ex2_2(nmu_l2fc * f2s(es));
+            const F2 Ec = ex2_2(nmu_l2fc * f2s(ef));
+            const F2 x = mu_fc * f2s(b.e2);
+            const F2 phi = fma2(x, fma2(x, fma2(x, fma2(x, fma2(x, f2s(-f_c / 720.0f), f2s(f_c / 120.0f)),
+                                                          f2s(-f_c / 24.0f)), f2s(f_c / 6.0f)), f2s(-0.5f * f_c)),
+                                f2s(f_c));
+            const F2 dif = (Ea + neg2(Ec)) * (inv_mu * f2s(b.inv_e2));
+            const F2 ser = Ea * phi;
+            F2 P = f2(f2lo(x) > 0.1f ? f2lo(dif) : f2lo(ser), f2hi(x) > 0.1f ? f2hi(dif) : f2hi(ser));
+            Q0 = fma2(nsig, P, Q0);
+            const F2 ah = nmu_dl * f2s(es), ch = nmu_dl * f2s(ef);
+            F2 R = dl2 * Ec;
+            P = fma2(ah, P, R);
+            R = R * ch;
+            Q1 = fma2(nsig, P, Q1);
+            P = fma2(ah, P, R);
+            R = R * ch;
+            Q2 = fma2(nsig, P, Q2);
+            P = fma2(ah, P, R);
+            Q3 = fma2(nsig, P, Q3);
+        }
+        const int t = threadIdx.x;
+        sQ[0][t] += f2lo(Q0); sQ[4][t] += f2hi(Q0);
+        sQ[1][t] += f2lo(Q1); sQ[5][t] += f2hi(Q1);
+        sQ[2][t] += f2lo(Q2); sQ[6][t] += f2hi(Q2);
+        sQ[3][t] += f2lo(Q3); sQ[7][t] += f2hi(Q3);
+    }
+    // Every direction of the launch from the summed moments: (1/f_d) sum_n h^n Q_n / n!.
+    for (int dd = 0; dd < nd; ++dd) {
+        const double f = 1.0 / fmax(fabs(a.n_hat[3 * (d0 + dd) + 2]), 1.0e-12);
+        const double hh = dl_d > 0.0 ? (f - f_c_d) / dl_d : 0.0;
+        for (int h = 0; h < 2; ++h) {
+            if (!(h == 0 ? on_a : on_b)) continue;
+            const double *Qh[4] = {&sQ[4 * h][threadIdx.x], &sQ[4 * h + 1][threadIdx.x], &sQ[4 * h + 2][threadIdx.x],
+                                   &sQ[4 * h + 3][threadIdx.x]};
+            const double v = (((*Qh[3] * (1.0 / 6.0)) * hh + *Qh[2] * 0.5) * hh + *Qh[1]) * hh + *Qh[0];
+            if (v != 0.0) atomicAdd(&a.spec[(int64_t)(d0 + dd) * a.n_E + e0 + h], v / f);
+        }
+    }
+}
+
 template <class Real, int NEL>
 __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
     brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
@@ -342,6 +540,12 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         int n_up = 0;
         for (int dd = 0; dd < nd; ++dd) n_up += a.n_hat[3 * (d0 + dd) + 2] < 0.0 ? 1 : 0;
         side_all = n_up == nd ? 1 : (n_up == 0 ? -1 : 0);
+    }
+    // Directions on one face within rho <= 0.01: the packed moment kernel
+    // (brem_moment_packed_kernel) scores this launch.
+    if constexpr (sizeof(Real) == 4) {
+        double fc_p, dl_p;
+        if (brem_packed_applies(a, d0, nd, fc_p, dl_p)) return;
     }
     // Moment form (see brem_moment_chunk): float, one exit face, and the
     // path factors within rho = Delta / f_min <= 0.05 of their centre.
@@ -702,7 +906,32 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     if (gy > max_y) gy = max_y;
     if (gy < 1) gy = 1;
     dim3 grid(gx, (unsigned)gy, 1);
+    // Mixed precision: the packed two-energy moment kernel takes the launches
+    // whose directions share an exit face within rho <= 0.01; for the others
+    // it returns at once and brem_kernel scores them (each kernel makes the
+    // same test on the device, so exactly one of the two does the work).
+    Kern packed = nullptr;
+    dim3 pgrid(1, 1, 1);
+    if (a.precision == PB_MIXED) {
+        const Kern t[kBremMaxEl] = {brem_moment_packed_kernel<1>, brem_moment_packed_kernel<2>,
+                                    brem_moment_packed_kernel<3>, brem_moment_packed_kernel<4>};
+        packed = t[a.n_el - 1];
+        int pp = 0;
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pp, packed, kBremPackedThreads, 0);
+        if (oe != cudaSuccess) return oe;
+        if (pp < 1) pp = 1;
+        const unsigned px = (unsigned)((a.n_E + 2 * kBremPackedThreads - 1) / (2 * kBremPackedThreads));
+        int64_t py = (int64_t)sms * pp / (int64_t)px;
+        if (py > max_y) py = max_y;
+        if (py < 1) py = 1;
+        pgrid = dim3(px, (unsigned)py, 1);
+    }
     for (int d0 = 0; d0 < a.n_dir; d0 += kBremMaxDir) {
+        if (packed) {
+            packed<<<pgrid, kBremPackedThreads, 0, s>>>(a, n_seg, d0);
+            cudaError_t err = cudaGetLastError();
+            if (err != cudaSuccess) return err;
+        }
         kern<<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;

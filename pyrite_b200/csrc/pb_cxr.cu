@@ -1321,6 +1321,10 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
                 __syncthreads();
             }
             const int n_items = qStart[nq];
+            if (a.counters && tid == 0) {
+                atomicAdd(&a.counters[0], (unsigned long long)nq);
+                atomicAdd(&a.counters[1], (unsigned long long)n_items);
+            }
             // Each thread walks one contiguous run of (line, bin) items: one
             // line search per pass, line constants held in registers, and
             // consecutive bins of a line share their edge evaluations.
@@ -1448,6 +1452,45 @@ __global__ void far_field_kernel(const double *edges, int n_E, int pad, const do
     spec[(int64_t)d * n_E + b] += acc;
 }
 
+// The same far field as a convolution on the uniform axis: with the centre
+// bin c and the output bin b a distance D = b - c apart, A = (D - 1/2) w and
+// B = (D + 1/2) w, so the three expansion coefficients are
+//   f0 = r / w^2, f1 = 2 D r^2 / w^3, f2 = (3 D^2 + 1/4) r^3 / w^4,
+//   r = 1 / (D^2 - 1/4),
+// and r depends on the integer D alone: one table of r per block replaces a
+// division per (bin, centre) pair. Blocks of 128 output bins of one direction.
+__global__ void __launch_bounds__(128) far_field_conv_kernel(const double *edges, int n_E, int pad,
+                                                             const double *mom, double *spec, int K_far) {
+    extern __shared__ double sR[];  // r(D) for D = -n_mom .. n_mom
+    const int d = blockIdx.y;
+    const int n_mom = n_E + 2 * pad;
+    const double w = (edges[n_E] - edges[0]) / n_E;
+    for (int i = threadIdx.x; i <= 2 * n_mom; i += blockDim.x) {
+        const double D = (double)(i - n_mom);
+        sR[i] = 1.0 / (D * D - 0.25);
+    }
+    __syncthreads();
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n_E) return;
+    const double *m = mom + (int64_t)d * n_mom * 3;
+    const double iw = 1.0 / w;
+    const double iw2 = iw * iw, iw3 = iw2 * iw, iw4 = iw2 * iw2;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int slot = 0; slot < n_mom; ++slot) {
+        const int c = slot - pad;
+        if (c >= b - K_far && c <= b + K_far) continue;
+        const double m0 = m[3 * slot];
+        if (m0 == 0.0) continue;
+        const int D = b - c;
+        const double r = sR[D + n_mom];
+        const double Dd = (double)D;
+        acc0 = fma(m0, r, acc0);
+        acc1 = fma(m[3 * slot + 1], 2.0 * Dd * r * r, acc1);
+        acc2 = fma(m[3 * slot + 2], (3.0 * Dd * Dd + 0.25) * r * r * r, acc2);
+    }
+    spec[(int64_t)d * n_E + b] += acc0 * iw2 + acc1 * iw3 + acc2 * iw4;
+}
+
 // Node reduction of buffered lines: spec[d][e] += sum_j w_j sinc^2(x_je),
 // x = a (E_e - E_j) / pi, with the phase a (E_e - E_j) formed in double.
 template <class Real>
@@ -1558,7 +1601,15 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
     if (err != cudaSuccess) return err;
     if (K_far > 0) {
         dim3 fg((unsigned)((a.n_E + 127) / 128), (unsigned)a.n_dir);
-        far_field_kernel<<<fg, 128, 0, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
+        const size_t tab = sizeof(double) * (2 * ((size_t)a.n_E + 2 * (size_t)far_pad) + 1);
+        if (tab <= 200 * 1024) {
+            // the moments sit on a uniform axis (far moments are enabled on uniform edges only)
+            err = cudaFuncSetAttribute(far_field_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+            if (err != cudaSuccess) return err;
+            far_field_conv_kernel<<<fg, 128, tab, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
+        } else {
+            far_field_kernel<<<fg, 128, 0, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
+        }
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }

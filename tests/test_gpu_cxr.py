@@ -67,7 +67,9 @@ def test_pairs_match_oracle(case, cuda_device):
     both = good & og
     np.testing.assert_allclose(E[both], oE[both], rtol=1e-14)
     np.testing.assert_allclose(a[both], oa[both], rtol=1e-14)
-    np.testing.assert_allclose(w[both], ow[both], rtol=2e-12)
+    # weights reach the subnormal range (1e-300 and below) where relative
+    # differences stop meaning anything
+    np.testing.assert_allclose(w[both], ow[both], rtol=2e-12, atol=1e-290)
 
 
 @pytest.mark.parametrize("case", CXR_CASES)

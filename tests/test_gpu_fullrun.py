@@ -91,7 +91,13 @@ def test_full_run_agrees_with_reference_within_3_sigma(precision, cuda_device):
         report[k] = (n, int(np.sum(np.abs(z) > 3.0)) if n else 0, float(np.max(np.abs(z))) if n else 0.0)
     for k, (n, beyond, zmax) in report.items():
         assert beyond <= 2 + 0.03 * n and zmax <= 6.0, (k, report)
-    # Fates: the scene transmits every electron in both runs.
-    np.testing.assert_array_equal(ref["fates"].mean(0), np.mean(per["fates"], axis=0))
+    # Fates (back, trans, side, cutoff): nearly every electron is transmitted;
+    # a few in 1e5 backscatter. Binomial errors of both runs, 4 sigma plus one
+    # event of the reference's sample.
+    p_ref, p_gpu = ref["fates"].mean(0), np.mean(per["fates"], axis=0)
+    n_ref, n_gpu = Kr * per_ref, B * H
+    p = 0.5 * (p_ref + p_gpu)
+    se = np.sqrt(p * (1.0 - p) * (1.0 / n_ref + 1.0 / n_gpu))
+    assert np.all(np.abs(p_gpu - p_ref) <= 4.0 * se + 1.0 / n_ref), (p_ref, p_gpu)
     # The spectra are not trivially empty.
     assert report["cxr"][0] > 100 and report["brem"][0] > 700

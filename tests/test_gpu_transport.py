@@ -167,13 +167,14 @@ def test_straggled_fp64_replays_reference(case, cuda_device):
 
 
 def test_straggling_keeps_the_mean_loss(cuda_device):
-    """Philox, mixed precision: 300 keV electrons crossing a 1 um Si foil in a
-    single flight lose on average what the deterministic loss gives (the
-    Urban closure identity <dE> = |dE/dx| s), within 4 standard errors of the
-    straggled sample, and straggling spreads the single-flight losses."""
+    """Philox, mixed precision: 300 keV electrons crossing a 0.1 um Si foil
+    (0.4 elastic mean free paths) in a single flight lose on average what the
+    deterministic loss gives (the Urban closure identity <dE> = |dE/dx| s),
+    within 4 standard errors of the straggled sample, and straggling spreads
+    the single-flight losses."""
     from pyrite_b200 import simulate_trajectories
 
-    kw = dict(E0_keV=300.0, Ne=8000, layers=[(0.0, 1.0e4, [("Si", 0.04994)])], E_cut_keV=5.0, seed=4,
+    kw = dict(E0_keV=300.0, Ne=8000, layers=[(0.0, 1.0e3, [("Si", 0.04994)])], E_cut_keV=5.0, seed=4,
               rng="philox", precision="mixed", device=cuda_device, lut=False)
     out = {}
     for stg in (False, True):
