@@ -585,6 +585,7 @@ def main():
             out["report"] = case.surrogate_report()  # the probe ran on these batches
             out["sur_coarse"] = case.surrogate_spectrum()
             out["sur_fine"] = case.surrogate_spectrum_fine()
+            out["sur_fine_uniform"] = case.surrogate_spectrum_fine(shape="uniform")
             out["sur_alone"] = case._head(case.sur_hsum, case.sur_lsum).cpu().numpy() / max(case.histories, 1)
         if timed:
             # the per-batch snapshots sit between the events; each batch is
@@ -681,7 +682,8 @@ def main():
     if sur is not None:
         errors["surrogate_cv"] = {
             "coarse_512": spectrum_error_stats(compare["surrogate"]["sur_coarse"], coarse(ref_cxr)),
-            "fine_2048": spectrum_error_stats(compare["surrogate"]["sur_fine"], ref_cxr)}
+            "fine_2048": spectrum_error_stats(compare["surrogate"]["sur_fine"], ref_cxr),
+            "fine_2048_uniform_shape": spectrum_error_stats(compare["surrogate"]["sur_fine_uniform"], ref_cxr)}
         if sigma is not None:
             errors["surrogate_cv"]["fine_2048_in_fp64_sigma"] = sigma_stats(compare["surrogate"]["sur_fine"], ref_cxr,
                                                                             sigma["cxr"])

@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 4
+#define PB_ABI_VERSION 5
 
 enum pb_status {
     PB_OK = 0,
@@ -567,6 +567,46 @@ typedef struct pb_coherent_args {
 /* Workspace bytes pb_coherent_reduce needs for these sizes. */
 int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes);
 int pb_coherent_reduce(const pb_coherent_args *args, void *stream);
+
+/* The sampled-bunch decoherence factor of every row,
+ *   F[r, k] = |(1/n_pop) sum_p exp(i (omega_k A_p - (G_r,x x0_p + G_r,y y0_p)))|^2,
+ * A_p = t0_p - n_perp . xy0_p the population's emission-time offsets
+ * (Angstrom) and xy0_p its transverse entry offsets, FP64 throughout.
+ * Replaces the reference's row factor, src/pyrite/montecarlo/spectrum/cxr/
+ * _per_hkl.py:121-160 with the population of cxr/_setup.py:745-760. */
+typedef struct pb_decoherence_args {
+    int32_t n_row;
+    int32_t n_pop;
+    int32_t n_E;
+    int32_t pad_;
+    const double *G;         /* [n_row * 3] reciprocal vectors of the rows (x, y used) */
+    const double *A_pop;     /* [n_pop] */
+    const double *xy0_pop;   /* [n_pop * 2] */
+    const double *omega;     /* [n_E] omega(E) = E / (hbar c), 1/Angstrom */
+    double *F;               /* [n_row * n_E], written */
+} pb_decoherence_args;
+
+int pb_decoherence_factor(const pb_decoherence_args *args, void *stream);
+
+/* The coherent reduction with the sampled-bunch decoherence blend: every row
+ * mixes its all-electron field (flat) and the sum over electrons of each
+ * electron's own squared field (grouped) by the row factor F,
+ *   spec[k] += scale * sum_r row_weight[r] (F[r,k] flat_r(E_k)
+ *                                           + (1 - F[r,k]) grouped_r(E_k)).
+ * Replaces src/pyrite/montecarlo/spectrum/cxr/_batched_finalize.py:163-243
+ * (_decoherence_blend with every energy kept) and its per-electron grouped
+ * row (cxr/_per_hkl.py:457-500). A row's lines of one electron must be
+ * contiguous, electrons in nondecreasing id order (the record prologue's
+ * segment order); a decrease sets PB_DEV_BAD_INPUT in base.status. The
+ * flat and grouped sums come out of one pass over the lines. */
+typedef struct pb_coherent_blend_args {
+    pb_coherent_args base;   /* base.work: pb_coherent_blend_work_size bytes */
+    const int64_t *elec_id;  /* [n_line] emitting electron of every line */
+    const double *F_row;     /* [n_row * n_E] row factors (pb_decoherence_factor) */
+} pb_coherent_blend_args;
+
+int pb_coherent_blend_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes);
+int pb_coherent_blend(const pb_coherent_blend_args *args, void *stream);
 
 #ifdef __cplusplus
 }

@@ -167,6 +167,17 @@ class PbCoherentRecordsArgs(C.Structure):
     ]
 
 
+class PbDecoherenceArgs(C.Structure):
+    _fields_ = [
+        ("n_row", _i32), ("n_pop", _i32), ("n_E", _i32), ("pad_", _i32), ("G", _vp), ("A_pop", _vp),
+        ("xy0_pop", _vp), ("omega", _vp), ("F", _vp),
+    ]
+
+
+class PbCoherentBlendArgs(C.Structure):
+    _fields_ = [("base", PbCoherentArgs), ("elec_id", _vp), ("F_row", _vp)]
+
+
 # Exported symbols declared by include/pyrite_b200.h, checked by the tests.
 EXPORTS = (
     "pb_abi_version",
@@ -194,6 +205,9 @@ EXPORTS = (
     "pb_coherent_reduce",
     "pb_coherent_records_work_size",
     "pb_coherent_records",
+    "pb_decoherence_factor",
+    "pb_coherent_blend_work_size",
+    "pb_coherent_blend",
 )
 
 _lib = None
@@ -203,7 +217,7 @@ class PyriteB200Error(RuntimeError):
     """A pyrite_b200 C-ABI call returned a non-zero status."""
 
 
-ABI_VERSION = 4  # PB_ABI_VERSION of include/pyrite_b200.h
+ABI_VERSION = 5  # PB_ABI_VERSION of include/pyrite_b200.h
 
 
 def load(path: Path | None = None):
@@ -245,6 +259,11 @@ def load(path: Path | None = None):
     lib.pb_cxr_bin_lines.argtypes = [_i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _f64, _f64, _i32, _vp, _vp]
     lib.pb_coherent_work_size.argtypes = [_i32, _i64, _i32, C.POINTER(_u64)]
     lib.pb_coherent_reduce.argtypes = [C.POINTER(PbCoherentArgs), _vp]
+    lib.pb_coherent_records_work_size.argtypes = [_i64, _i32, C.POINTER(_u64)]
+    lib.pb_coherent_records.argtypes = [C.POINTER(PbCoherentRecordsArgs), _vp]
+    lib.pb_decoherence_factor.argtypes = [C.POINTER(PbDecoherenceArgs), _vp]
+    lib.pb_coherent_blend_work_size.argtypes = [_i32, _i64, _i32, C.POINTER(_u64)]
+    lib.pb_coherent_blend.argtypes = [C.POINTER(PbCoherentBlendArgs), _vp]
     if path is None:
         _lib = lib
     return lib

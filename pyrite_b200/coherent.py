@@ -37,16 +37,19 @@ RECORD_FIELDS = ("E_vac", "a_vac", "phase_slope", "g_phase", "cs_re", "cs_im", "
                  "L_esc", "half_dL", "apb", "bma", "q")
 
 
-def _work(h: _Holder, n_row: int, n_line: int, n_E: int):
+def _work(h: _Holder, n_row: int, n_line: int, n_E: int, blend: bool = False):
     lib = L.load()
     nbytes = C.c_uint64()
-    L.check(lib.pb_coherent_work_size(n_row, n_line, n_E, C.byref(nbytes)), "pb_coherent_work_size")
+    if blend:
+        L.check(lib.pb_coherent_blend_work_size(n_row, n_line, n_E, C.byref(nbytes)), "pb_coherent_blend_work_size")
+    else:
+        L.check(lib.pb_coherent_work_size(n_row, n_line, n_E, C.byref(nbytes)), "pb_coherent_work_size")
     # torch's caching allocator hands out 512-byte aligned blocks
     return h.empty((max(int(nbytes.value), 1),), torch.uint8), int(nbytes.value)
 
 
 def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, scale=1.0, sinc_cutoff=None,
-                    spec=None, device=None, stream=None, status=None) -> torch.Tensor:
+                    spec=None, device=None, stream=None, status=None, elec_id=None, F_row=None) -> torch.Tensor:
     """``spec += scale * sum_rows w_r (|F_sigma|^2 + |F_pi|^2)`` on the device.
 
     ``records`` maps ``RECORD_FIELDS`` to per-line arrays (numpy or tensors),
@@ -54,6 +57,12 @@ def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, s
     intensity is weighted by ``row_weight[r]``. ``delta_omega`` is
     ``(1 - Re n(E)) omega(E)`` on ``E_grid_eV`` [1/Angstrom]. Returns the FP64
     device spectrum (``spec`` when given, accumulated into).
+
+    With ``elec_id`` (the emitting electron of every line, contiguous and
+    nondecreasing inside a row) and ``F_row`` [n_row, n_E] (the rows'
+    decoherence factors, ``decoherence_factor``), each row is the
+    sampled-bunch blend ``F flat + (1 - F) grouped`` of its all-electron
+    field and its per-electron squared fields (``pb_coherent_blend``).
     """
     dev = _device(device)
     h = _Holder(dev)
@@ -81,7 +90,18 @@ def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, s
         spec = h.zeros((n_E,), torch.float64)
     elif spec.dtype != torch.float64 or spec.device != dev or int(spec.numel()) != n_E or not spec.is_contiguous():
         raise ValueError("spec must be a contiguous float64 tensor on the device with one entry per energy")
-    work, nbytes = _work(h, n_row, n_line, n_E)
+    blend = elec_id is not None or F_row is not None
+    if blend:
+        if elec_id is None or F_row is None:
+            raise ValueError("the decoherence blend needs both elec_id and F_row")
+        eid = h.typed(np.asarray(elec_id, dtype=np.int64).reshape(-1) if not torch.is_tensor(elec_id)
+                      else elec_id.reshape(-1), torch.int64)
+        if int(eid.numel()) != n_line:
+            raise ValueError("elec_id must have one entry per line")
+        F = h.f64(F_row).reshape(-1)
+        if int(F.numel()) != n_row * n_E:
+            raise ValueError("F_row must be [n_row, n_E]")
+    work, nbytes = _work(h, n_row, n_line, n_E, blend)
     a = L.PbCoherentArgs()
     a.n_row, a.n_E, a.n_line = n_row, n_E, n_line
     a.row_off, a.row_weight, a.E, a.delta_omega = (t.data_ptr() for t in (row_off, w, E, dom))
@@ -92,7 +112,13 @@ def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, s
     a.spec = spec.data_ptr()
     a.work, a.work_bytes = work.data_ptr(), nbytes
     a.status = None if status is None else status.data_ptr()
-    L.check(L.load().pb_coherent_reduce(C.byref(a), _stream_ptr(stream)), "pb_coherent_reduce")
+    if blend:
+        b = L.PbCoherentBlendArgs()
+        b.base = a
+        b.elec_id, b.F_row = eid.data_ptr(), F.data_ptr()
+        L.check(L.load().pb_coherent_blend(C.byref(b), _stream_ptr(stream)), "pb_coherent_blend")
+    else:
+        L.check(L.load().pb_coherent_reduce(C.byref(a), _stream_ptr(stream)), "pb_coherent_reduce")
     if stream is not None:
         # freed on torch's current stream: keep the blocks until the call has run
         for t in h.keep:
@@ -178,6 +204,46 @@ def coherent_spectrum(records, row_count, row_weight, E_grid_eV, delta_omega, Ne
         raise ValueError("Ne must be >= 1")
     spec = coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, scale=1.0 / Ne,
                            sinc_cutoff=sinc_cutoff, device=device)
+    return spec.cpu().numpy()
+
+
+def decoherence_factor(G, A_pop, xy0_pop, omega, *, device=None, stream=None) -> torch.Tensor:
+    """Row factors ``F[r, k] = |<exp(i (omega_k A_p - G_r,perp . xy0_p))>_p|^2``
+    over the sampled population (``cxr/_per_hkl.py:121-160``,
+    ``cxr/_setup.py:745-760``), FP64 on the device: [n_row, n_E]."""
+    dev = _device(device)
+    h = _Holder(dev)
+    G = h.f64(G).reshape(-1, 3)
+    A = h.f64(A_pop).reshape(-1)
+    xy = h.f64(xy0_pop).reshape(-1, 2)
+    om = h.f64(omega).reshape(-1)
+    if int(xy.shape[0]) != int(A.numel()):
+        raise ValueError("A_pop and xy0_pop must describe the same population")
+    n_row, n_pop, n_E = int(G.shape[0]), int(A.numel()), int(om.numel())
+    F = torch.empty((n_row, n_E), dtype=torch.float64, device=dev)
+    a = L.PbDecoherenceArgs()
+    a.n_row, a.n_pop, a.n_E = n_row, n_pop, n_E
+    a.G, a.A_pop, a.xy0_pop, a.omega, a.F = (t.data_ptr() for t in (G, A, xy, om, F))
+    L.check(L.load().pb_decoherence_factor(C.byref(a), _stream_ptr(stream)), "pb_decoherence_factor")
+    if stream is not None:
+        for t in h.keep:
+            t.record_stream(stream)
+    return F
+
+
+def coherent_spectrum_decoherent(records, elec_id, row_count, row_weight, G, A_pop, xy0_pop, E_grid_eV,
+                                 delta_omega, omega, Ne, *, sinc_cutoff=None, device=None) -> np.ndarray:
+    """The coherent route with the sampled-bunch decoherence blend, per
+    electron: every row's ``(1 - F) grouped + F flat`` weighted and summed
+    over rows, divided by ``Ne`` (``cxr/_batched_finalize.py:163-243``).
+    ``G`` holds the rows' reciprocal vectors, ``A_pop`` / ``xy0_pop`` the
+    population's emission-time and transverse offsets (records offset-free,
+    ``cxr/_setup.py:637-642``)."""
+    if Ne < 1:
+        raise ValueError("Ne must be >= 1")
+    F = decoherence_factor(G, A_pop, xy0_pop, omega, device=device)
+    spec = coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, scale=1.0 / Ne,
+                           sinc_cutoff=sinc_cutoff, device=device, elec_id=elec_id, F_row=F)
     return spec.cpu().numpy()
 
 

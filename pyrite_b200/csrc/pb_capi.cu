@@ -399,24 +399,68 @@ int pb_coherent_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *
     return PB_OK;
 }
 
+static int coherent_check(const pb_coherent_args *a, const char *who, uint64_t need) {
+    if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_INVALID, "%s: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40", who);
+    if (!coherent_grid_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_UNSUPPORTED, "%s: more than 2^31 - 1 work items; split the rows", who);
+    if (!a->row_off || !a->row_weight || !a->E || !a->delta_omega || !a->spec || !a->work)
+        return fail(PB_ERR_INVALID, "%s: row_off, row_weight, E, delta_omega, spec, work must be set", who);
+    if (a->n_line > 0 && (!a->E_vac || !a->a_vac || !a->phase_slope || !a->g_phase || !a->cs_re || !a->cs_im ||
+                          !a->cp_re || !a->cp_im || !a->L_esc || !a->half_dL || !a->apb || !a->bma || !a->q))
+        return fail(PB_ERR_INVALID, "%s: every line record array must be set", who);
+    if (reinterpret_cast<uintptr_t>(a->work) % 256 != 0)
+        return fail(PB_ERR_INVALID, "%s: work must be 256-byte aligned", who);
+    if (!(a->sinc_cutoff >= 0.0)) return fail(PB_ERR_INVALID, "%s: sinc_cutoff must be >= 0", who);
+    if (a->work_bytes < need)
+        return fail(PB_ERR_CAPACITY, "%s: work holds %llu bytes, needs %llu", who,
+                    (unsigned long long)a->work_bytes, (unsigned long long)need);
+    return PB_OK;
+}
+
+int pb_coherent_blend_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes) {
+    if (!bytes) return fail(PB_ERR_INVALID, "pb_coherent_blend_work_size: bytes is NULL");
+    if (!coherent_sizes_ok(n_row, n_line, n_E))
+        return fail(PB_ERR_INVALID,
+                    "pb_coherent_blend_work_size: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    if (!coherent_grid_ok(n_row, n_line, n_E))
+        return fail(PB_ERR_UNSUPPORTED, "pb_coherent_blend_work_size: more than 2^31 - 1 work items; split the rows");
+    *bytes = pb::coherent_blend_work_bytes(n_row, n_line, n_E);
+    return PB_OK;
+}
+
+int pb_coherent_blend(const pb_coherent_blend_args *b, void *stream) {
+    if (!b) return fail(PB_ERR_INVALID, "pb_coherent_blend: args is NULL");
+    const pb_coherent_args *a = &b->base;
+    if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_INVALID, "pb_coherent_blend: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    const int rc = coherent_check(a, "pb_coherent_blend", pb::coherent_blend_work_bytes(a->n_row, a->n_line, a->n_E));
+    if (rc != PB_OK) return rc;
+    if (!b->F_row || (a->n_line > 0 && !b->elec_id))
+        return fail(PB_ERR_INVALID, "pb_coherent_blend: elec_id and F_row must be set");
+    if (a->n_line == 0) return PB_OK;
+    cudaError_t e = pb::launch_coherent_blend(*b, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_blend: launch");
+    return PB_OK;
+}
+
+int pb_decoherence_factor(const pb_decoherence_args *a, void *stream) {
+    if (!a) return fail(PB_ERR_INVALID, "pb_decoherence_factor: args is NULL");
+    if (a->n_row < 1 || a->n_row > 65535 || a->n_pop < 1 || a->n_E < 1 || a->n_E > (1 << 24))
+        return fail(PB_ERR_INVALID, "pb_decoherence_factor: need 1 <= n_row <= 65535, n_pop >= 1, 1 <= n_E <= 2^24");
+    if (!a->G || !a->A_pop || !a->xy0_pop || !a->omega || !a->F)
+        return fail(PB_ERR_INVALID, "pb_decoherence_factor: G, A_pop, xy0_pop, omega and F must be set");
+    cudaError_t e = pb::launch_decoherence(*a, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_decoherence_factor: launch");
+    return PB_OK;
+}
+
 int pb_coherent_reduce(const pb_coherent_args *a, void *stream) {
     if (!a) return fail(PB_ERR_INVALID, "pb_coherent_reduce: args is NULL");
     if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
         return fail(PB_ERR_INVALID, "pb_coherent_reduce: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
-    if (!coherent_grid_ok(a->n_row, a->n_line, a->n_E))
-        return fail(PB_ERR_UNSUPPORTED, "pb_coherent_reduce: more than 2^31 - 1 work items; split the rows");
-    if (!a->row_off || !a->row_weight || !a->E || !a->delta_omega || !a->spec || !a->work)
-        return fail(PB_ERR_INVALID, "pb_coherent_reduce: row_off, row_weight, E, delta_omega, spec, work must be set");
-    if (a->n_line > 0 && (!a->E_vac || !a->a_vac || !a->phase_slope || !a->g_phase || !a->cs_re || !a->cs_im ||
-                          !a->cp_re || !a->cp_im || !a->L_esc || !a->half_dL || !a->apb || !a->bma || !a->q))
-        return fail(PB_ERR_INVALID, "pb_coherent_reduce: every line record array must be set");
-    if (reinterpret_cast<uintptr_t>(a->work) % 256 != 0)
-        return fail(PB_ERR_INVALID, "pb_coherent_reduce: work must be 256-byte aligned");
-    if (!(a->sinc_cutoff >= 0.0)) return fail(PB_ERR_INVALID, "pb_coherent_reduce: sinc_cutoff must be >= 0");
-    const uint64_t need = pb::coherent_work_bytes(a->n_row, a->n_line, a->n_E);
-    if (a->work_bytes < need)
-        return fail(PB_ERR_CAPACITY, "pb_coherent_reduce: work holds %llu bytes, needs %llu",
-                    (unsigned long long)a->work_bytes, (unsigned long long)need);
+    const int rc = coherent_check(a, "pb_coherent_reduce", pb::coherent_work_bytes(a->n_row, a->n_line, a->n_E));
+    if (rc != PB_OK) return rc;
     if (a->n_line == 0) return PB_OK;  // no line: the spectrum is unchanged
     cudaError_t e = pb::launch_coherent(*a, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_reduce: launch");

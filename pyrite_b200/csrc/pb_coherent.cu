@@ -177,6 +177,18 @@ __device__ __forceinline__ void add_line_field(const CohLine &l, float vf, float
     acc[3] = fmaf(l.cpr, pi, fmaf(l.cpi, pr, acc[3]));
 }
 
+// The same term added to the row's field and to the current electron's.
+__device__ __forceinline__ void add_line_field2(const CohLine &l, float vf, float sv, float cv, float sp, float cp,
+                                                float acc[4], float acc_e[4]) {
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+    add_line_field(l, vf, sv, cv, sp, cp, t);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        acc[c] += t[c];
+        acc_e[c] += t[c];
+    }
+}
+
 struct CohArgs {
     const int64_t *row_off;
     const double *E, *dom;
@@ -186,9 +198,21 @@ struct CohArgs {
     int64_t n_line, K, n_item_max;
     const int64_t *item_off;
     float *partial;  // [n_item_max][4][n_E]
+    // Decoherence blend only: electron of every line (nondecreasing inside a
+    // row), the per-item sum over electrons of each electron's own squared
+    // field [n_item_max][n_E], and the status word for unordered electrons.
+    const int64_t *elec;
+    float *power;
+    unsigned int *status;
 };
 
-__global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a) {
+// kGrouped: items start and end on electron boundaries (the nominal bounds
+// moved forward past lines of the electron that straddles them; adjacent
+// items move a shared bound alike, so the items still partition the row),
+// and besides the row's field the kernel sums every electron's own field,
+// squares it where the electron ends and adds the squares up per item.
+template <bool kGrouped>
+__global__ void __launch_bounds__(kThreads, kGrouped ? 2 : 3) coh_field_kernel(const CohArgs a) {
     __shared__ CohLine sm[kStage];
     const int64_t item = blockIdx.x;
     const int64_t n_item = a.item_off[a.n_row];
@@ -202,8 +226,12 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
     }
     const int64_t rb = imin(imax(a.row_off[lo], 0), a.n_line);
     const int64_t re = imin(imax(a.row_off[lo + 1], rb), a.n_line);
-    const int64_t j0 = rb + (item - a.item_off[lo]) * a.K;
-    const int64_t j1 = imin(j0 + a.K, re);
+    int64_t j0 = imin(rb + (item - a.item_off[lo]) * a.K, re);
+    int64_t j1 = imin(j0 + a.K, re);
+    if constexpr (kGrouped) {
+        while (j0 > rb && j0 < re && a.elec[j0] == a.elec[j0 - 1]) ++j0;
+        while (j1 > rb && j1 < re && a.elec[j1] == a.elec[j1 - 1]) ++j1;
+    }
 
     const int tid = threadIdx.x;
     const int e_base = blockIdx.y * kETile + tid;
@@ -217,6 +245,10 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
     float acc[kEPT][4];
 #pragma unroll
     for (int m = 0; m < kEPT; ++m) acc[m][0] = acc[m][1] = acc[m][2] = acc[m][3] = 0.f;
+    // kGrouped: the current electron's field and the item's sum of squares
+    float acc_e[kGrouped ? kEPT : 1][4], pw[kGrouped ? kEPT : 1];
+#pragma unroll
+    for (int m = 0; m < (kGrouped ? kEPT : 1); ++m) acc_e[m][0] = acc_e[m][1] = acc_e[m][2] = acc_e[m][3] = pw[m] = 0.f;
 
     // largest |E| and |delta_omega| of this CTA's energies (for the fast-path check)
     __shared__ double red[2][kThreads / 32];
@@ -269,11 +301,28 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
             l.cpr = (float)a.cpr[j];
             l.cpi = (float)a.cpi[j];
             l.pad[0] = l.pad[1] = 0.f;
+            if constexpr (kGrouped) {
+                if (j > j0) {
+                    const int64_t ep = a.elec[j - 1], ej = a.elec[j];
+                    l.pad[0] = ej != ep ? 1.f : 0.f;  // an electron starts here
+                    if (ej < ep && a.status) atomicOr(a.status, PB_DEV_BAD_INPUT);
+                }
+            }
             sm[tid] = l;
         }
         __syncthreads();
         for (int i = 0; i < n; ++i) {
             const CohLine l = sm[i];
+            if constexpr (kGrouped) {
+                if (l.pad[0] != 0.f) {  // uniform: close the previous electron
+#pragma unroll
+                    for (int m = 0; m < kEPT; ++m) {
+                        pw[m] += acc_e[m][0] * acc_e[m][0] + acc_e[m][1] * acc_e[m][1] +
+                                 acc_e[m][2] * acc_e[m][2] + acc_e[m][3] * acc_e[m][3];
+                        acc_e[m][0] = acc_e[m][1] = acc_e[m][2] = acc_e[m][3] = 0.f;
+                    }
+                }
+            }
             if (l.fast) {  // uniform over the block: one line at a time
 #pragma unroll
                 for (int m = 0; m < kEPT; ++m) {
@@ -284,7 +333,8 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
                     if (fabsf(vf) <= 1.f) sincos_taylor(vf, sv, cv);
                     else sincos_turns_offset(vx, sv, cv);
                     sincos_turns_offset(fma(l.ps_t, E[m], fma(-l.L_t, D[m], l.Gx)), sp, cp);
-                    add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
+                    if constexpr (kGrouped) add_line_field2(l, vf, sv, cv, sp, cp, acc[m], acc_e[m]);
+                    else add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
                 }
             } else {
 #pragma unroll
@@ -296,7 +346,8 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
                     if (fabsf(vf) <= 1.f) sincos_taylor(vf, sv, cv);
                     else sincos_turns(vt, sv, cv);
                     sincos_turns(fma(l.ps_t, E[m], -fma(l.L_t, D[m], l.Gx)), sp, cp);
-                    add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
+                    if constexpr (kGrouped) add_line_field2(l, vf, sv, cv, sp, cp, acc[m], acc_e[m]);
+                    else add_line_field(l, vf, sv, cv, sp, cp, acc[m]);
                 }
             }
         }
@@ -307,6 +358,9 @@ __global__ void __launch_bounds__(kThreads, 3) coh_field_kernel(const CohArgs a)
         if (e < a.n_E) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) a.partial[((size_t)item * 4 + c) * a.n_E + e] = acc[m][c];
+            if constexpr (kGrouped)
+                a.power[(size_t)item * a.n_E + e] = pw[m] + acc_e[m][0] * acc_e[m][0] + acc_e[m][1] * acc_e[m][1] +
+                                                    acc_e[m][2] * acc_e[m][2] + acc_e[m][3] * acc_e[m][3];
         }
     }
 }
@@ -341,7 +395,88 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     spec[e] += scale * total;
 }
 
+// The sampled-bunch blend (_batched_finalize.py:163-243):
+// spec[e] += scale * sum_r w_r (F_r(e) |sum_items F|^2 + (1 - F_r(e)) sum_items power),
+// rows and items in order, as coh_finalize_kernel.
+__global__ void __launch_bounds__(kFinalizeThreads)
+    coh_finalize_blend_kernel(int n_row, int n_E, const int64_t *__restrict__ item_off,
+                              const double *__restrict__ w_row, const double *__restrict__ F_row,
+                              const float *__restrict__ partial, const float *__restrict__ power, double scale,
+                              double *__restrict__ spec) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_E) return;
+    double total = 0.0;
+    int64_t i0 = item_off[0];
+    for (int r = 0; r < n_row; ++r) {
+        const int64_t i1 = item_off[r + 1];
+        if (i1 > i0) {
+            double f[4] = {0.0, 0.0, 0.0, 0.0}, g = 0.0;
+#pragma unroll 4
+            for (int64_t i = i0; i < i1; ++i) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) f[c] += (double)partial[((size_t)i * 4 + c) * n_E + e];
+                g += (double)power[(size_t)i * n_E + e];
+            }
+            const double F = F_row[(size_t)r * n_E + e];
+            const double flat = f[0] * f[0] + f[1] * f[1] + f[2] * f[2] + f[3] * f[3];
+            total += w_row[r] * (F * flat + (1.0 - F) * g);
+        }
+        i0 = i1;
+    }
+    spec[e] += scale * total;
+}
+
+// F_r(e) = |(1/N) sum_p exp(i (omega_e A_p - g_r,perp . xy0_p))|^2
+// (cxr/_per_hkl.py:121-160, cxr/_setup.py:745-760), FP64 throughout: one
+// thread per (row, energy), the population staged in shared memory.
+constexpr int kDecohThreads = 256;
+constexpr int kDecohStage = 512;
+
+__global__ void __launch_bounds__(kDecohThreads)
+    decoherence_kernel(int n_row, int n_pop, int n_E, const double *__restrict__ G, const double *__restrict__ A,
+                       const double *__restrict__ xy0, const double *__restrict__ omega, double *__restrict__ F) {
+    __shared__ double sA[kDecohStage], sB[kDecohStage];
+    const int r = blockIdx.y;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const double gx = G[3 * r], gy = G[3 * r + 1];
+    const double w = e < n_E ? omega[e] : 0.0;
+    double cr = 0.0, ci = 0.0;
+    for (int p0 = 0; p0 < n_pop; p0 += kDecohStage) {
+        const int n = min(kDecohStage, n_pop - p0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            sA[k] = A[p0 + k];
+            sB[k] = __dadd_rn(__dmul_rn(xy0[2 * (p0 + k)], gx), __dmul_rn(xy0[2 * (p0 + k) + 1], gy));
+        }
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            double sn, cs;
+            sincos(__dsub_rn(__dmul_rn(w, sA[k]), sB[k]), &sn, &cs);
+            cr += cs;
+            ci += sn;
+        }
+    }
+    if (e < n_E) {
+        cr /= n_pop;
+        ci /= n_pop;
+        F[(size_t)r * n_E + e] = cr * cr + ci * ci;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_decoherence(const pb_decoherence_args &p, cudaStream_t s) {
+    dim3 grid((unsigned)((p.n_E + kDecohThreads - 1) / kDecohThreads), (unsigned)p.n_row);
+    decoherence_kernel<<<grid, kDecohThreads, 0, s>>>(p.n_row, p.n_pop, p.n_E, p.G, p.A_pop, p.xy0_pop, p.omega,
+                                                      p.F);
+    return cudaGetLastError();
+}
+
+uint64_t coherent_blend_work_bytes(int n_row, int64_t n_line, int n_E) {
+    const int64_t K = chunk_lines(n_line, n_E);
+    const int64_t items = max_items(n_row, n_line, K);
+    return coherent_work_bytes(n_row, n_line, n_E) + align256((size_t)items * (size_t)n_E * sizeof(float));
+}
 
 uint64_t coherent_work_bytes(int n_row, int64_t n_line, int n_E) {
     const int64_t K = chunk_lines(n_line, n_E);
@@ -353,7 +488,8 @@ int64_t coherent_items(int n_row, int64_t n_line, int n_E) {
     return max_items(n_row, n_line, chunk_lines(n_line, n_E));
 }
 
-cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
+cudaError_t launch_coherent_impl(const pb_coherent_args &p, const int64_t *elec, const double *F_row,
+                                 cudaStream_t s) {
     const int64_t K = chunk_lines(p.n_line, p.n_E);
     const int64_t n_item_max = max_items(p.n_row, p.n_line, K);
     auto *item_off = static_cast<int64_t *>(p.work);
@@ -385,12 +521,31 @@ cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
     a.n_item_max = n_item_max;
     a.item_off = item_off;
     a.partial = partial;
+    a.elec = elec;
+    a.power = elec ? reinterpret_cast<float *>(reinterpret_cast<char *>(partial) +
+                                               (size_t)n_item_max * 4 * (size_t)p.n_E * sizeof(float))
+                   : nullptr;
+    a.status = p.status;
     dim3 grid((unsigned)n_item_max, (unsigned)n_etiles(p.n_E));
-    coh_field_kernel<<<grid, kThreads, 0, s>>>(a);
     const unsigned fin_blocks = (unsigned)((p.n_E + kFinalizeThreads - 1) / kFinalizeThreads);
-    coh_finalize_kernel<<<fin_blocks, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight, partial,
-                                                                p.scale, p.spec);
+    if (elec) {
+        coh_field_kernel<true><<<grid, kThreads, 0, s>>>(a);
+        coh_finalize_blend_kernel<<<fin_blocks, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight,
+                                                                          F_row, partial, a.power, p.scale, p.spec);
+    } else {
+        coh_field_kernel<false><<<grid, kThreads, 0, s>>>(a);
+        coh_finalize_kernel<<<fin_blocks, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight, partial,
+                                                                    p.scale, p.spec);
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
+    return launch_coherent_impl(p, nullptr, nullptr, s);
+}
+
+cudaError_t launch_coherent_blend(const pb_coherent_blend_args &p, cudaStream_t s) {
+    return launch_coherent_impl(p.base, p.elec_id, p.F_row, s);
 }
 
 }  // namespace pb

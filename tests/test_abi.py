@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(L.EXPORTS)
     for name in names:
         assert hasattr(lib, name), name
-    assert lib.pb_abi_version() == L.ABI_VERSION == 4
+    assert lib.pb_abi_version() == L.ABI_VERSION == 5
 
 
 STRUCTS = {
@@ -35,6 +35,7 @@ STRUCTS = {
     "pb_segments": L.PbSegments, "pb_tallies": L.PbTallies, "pb_transport_args": L.PbTransportArgs,
     "pb_cxr_tables": L.PbCxrTables, "pb_cxr_args": L.PbCxrArgs, "pb_brem_args": L.PbBremArgs,
     "pb_coherent_args": L.PbCoherentArgs, "pb_coherent_records_args": L.PbCoherentRecordsArgs,
+    "pb_decoherence_args": L.PbDecoherenceArgs, "pb_coherent_blend_args": L.PbCoherentBlendArgs,
 }
 
 
@@ -128,3 +129,35 @@ def test_coherent_work_size_at_the_largest_accepted_sizes():
     assert lib.pb_coherent_work_size(1 << 24, 1 << 40, 1 << 24, C.byref(nb)) == 0
     assert lib.pb_coherent_work_size(1 << 24, 1 << 40, 1, C.byref(nb)) == 0
     assert lib.pb_coherent_work_size((1 << 24) + 1, 10, 10, C.byref(nb)) == L.PB_ERR_INVALID
+
+
+def test_blend_and_decoherence_checks_without_a_device():
+    """The blend needs its electron ids and row factors, the decoherence
+    factor its population; both refuse before any CUDA call."""
+    lib = L.load()
+    nb = C.c_uint64()
+    assert lib.pb_coherent_blend_work_size(4, 1000, 64, C.byref(nb)) == 0
+    plain = C.c_uint64()
+    assert lib.pb_coherent_work_size(4, 1000, 64, C.byref(plain)) == 0
+    assert nb.value > plain.value
+    b = L.PbCoherentBlendArgs()
+    a = b.base
+    a.n_row, a.n_E, a.n_line = 4, 64, 1000
+    fake = 0x1000
+    for f in ("row_off", "row_weight", "E", "delta_omega", "spec") + tuple(
+            n for n, _ in L.PbCoherentArgs._fields_[7:20]):
+        setattr(a, f, fake)
+    a.work, a.work_bytes = 0x100000, nb.value
+    b.base = a
+    assert lib.pb_coherent_blend(C.byref(b), None) == L.PB_ERR_INVALID
+    assert b"elec_id and F_row" in lib.pb_last_error()
+    a.work_bytes = plain.value
+    b.base = a
+    b.elec_id, b.F_row = fake, fake
+    assert lib.pb_coherent_blend(C.byref(b), None) == L.PB_ERR_CAPACITY
+    d = L.PbDecoherenceArgs()
+    d.n_row, d.n_pop, d.n_E = 3, 0, 16
+    assert lib.pb_decoherence_factor(C.byref(d), None) == L.PB_ERR_INVALID
+    d.n_pop = 8
+    assert lib.pb_decoherence_factor(C.byref(d), None) == L.PB_ERR_INVALID
+    assert b"must be set" in lib.pb_last_error()

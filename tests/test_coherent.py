@@ -613,3 +613,77 @@ def test_no_cpu_fallback_without_a_device():
         coherent_reduce(rec, cnt, w, E, dom)
     with pytest.raises(PyriteB200Error, match="CUDA"):
         coherent_spectrum(rec, cnt, w, E, dom, Ne)
+
+
+@pytest.mark.gpu
+def test_gpu_decoherence_blend_matches_reference():
+    """The sampled-bunch blend on the device: the row factors F against the
+    reference's (FP64, 1e-12), and the blended spectrum -- flat and
+    per-electron fields from one pass, mixed by F -- against the reference's
+    within the reduction's tolerance."""
+    from pyrite_b200.coherent import coherent_spectrum_decoherent, decoherence_factor
+
+    z = np.load(GOLDEN / "coherent_decoherence_hopg20.npz")
+    rec = {k: z[k] for k in oc.FIELDS}
+    F = decoherence_factor(z["G"], z["A_pop"], z["xy0_pop"], z["omega"]).cpu().numpy()
+    np.testing.assert_allclose(F[z["active_rows"]], z["F_rows"], rtol=1e-12, atol=1e-15)
+    spec = coherent_spectrum_decoherent(rec, z["elec_id"], z["row_count"], z["row_weight"], z["G"], z["A_pop"],
+                                        z["xy0_pop"], z["E_grid"], z["delta_omega"], z["omega"], int(z["Ne"]))
+    _assert_close(spec, z["spec"])
+
+
+@pytest.mark.gpu
+def test_gpu_blend_limits_and_long_electrons():
+    """Random rows whose electrons hold 1 to 40 lines, one of them 700 (longer
+    than a work item, so item bounds move to electron ends): F = 1 gives the
+    plain reduction, F = 0 the oracle's per-electron sum on every 16th
+    energy; repeated calls are bit-identical."""
+    import torch
+
+    from pyrite_b200.coherent import coherent_reduce
+
+    rng = np.random.default_rng(17)
+    n_rows, n_per_row = 3, 6000
+    rec, cnt, w = _random_rows(rng, n_rows, n_per_row, 2000.0, 40000.0)
+    eid = []
+    for r in range(n_rows):
+        ids, e = [], 1000 * r
+        while len(ids) < n_per_row:
+            k = 700 if (r == 1 and e == 1003) else int(rng.integers(1, 41))
+            ids += [e] * k
+            e += 1
+        eid.append(np.asarray(ids[:n_per_row], dtype=np.int64))
+    eid = np.concatenate(eid)
+    E = np.linspace(1000.0, 41000.0, 2048)
+    dom = 2.3e-4 * (1e4 / (E + 500.0)) ** 2 * E / 1973.27
+    ones, zeros = np.ones((n_rows, E.size)), np.zeros((n_rows, E.size))
+    plain = coherent_reduce(rec, cnt, w, E, dom).cpu().numpy()
+    flat = coherent_reduce(rec, cnt, w, E, dom, elec_id=eid, F_row=ones).cpu().numpy()
+    _assert_close(flat, plain)
+    grouped = coherent_reduce(rec, cnt, w, E, dom, elec_id=eid, F_row=zeros).cpu().numpy()
+    again = coherent_reduce(rec, cnt, w, E, dom, elec_id=eid, F_row=zeros).cpu().numpy()
+    assert np.array_equal(grouped, again)
+    sub = np.arange(0, E.size, 16)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    rec64 = {k: np.asarray(rec[k], dtype=np.float64) for k in oc.FIELDS}
+    ref = sum(w[r] * oc.grouped_row(rec64, off[r], off[r + 1], eid, E[sub], dom[sub]) for r in range(n_rows))
+    _assert_close(grouped[sub], ref)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_gpu_blend_flags_unordered_electrons():
+    """Electron ids that decrease inside a row set PB_DEV_BAD_INPUT."""
+    import torch
+
+    from pyrite_b200 import _lib as L
+    from pyrite_b200.coherent import coherent_reduce
+
+    rng = np.random.default_rng(23)
+    rec, cnt, w = _random_rows(rng, 1, 600, 2000.0, 40000.0)
+    eid = np.repeat(np.arange(60, dtype=np.int64), 10)[::-1].copy()
+    E = np.linspace(1000.0, 41000.0, 256)
+    dom = np.zeros_like(E)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    coherent_reduce(rec, cnt, w, E, dom, elec_id=eid, F_row=np.zeros((1, E.size)), status=status)
+    assert int(status.item()) & L.PB_DEV_BAD_INPUT
