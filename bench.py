@@ -567,10 +567,14 @@ def main():
         case.reset()
         torch.cuda.synchronize()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(C + 1)]
-        per_batch, prev = [], None
+        per_batch, prev, fine_by_batch = [], None, []
         for i in range(C):
             ev[i].record()
             case.run_batch(cmp_base + i * H, H)
+            if getattr(case, "surrogates", None):
+                # the cumulative surrogate+CV fine spectrum after every batch
+                # (the arm is not timed): its error trajectory against FP64
+                fine_by_batch.append(case.surrogate_spectrum_fine())
             if timed:
                 cur = {k: v.detach().clone() for k, v in (("cxr", case.spec_cxr), ("brem", case.spec_brem))}
                 if prev is not None:
@@ -585,7 +589,7 @@ def main():
             out["report"] = case.surrogate_report()  # the probe ran on these batches
             out["sur_coarse"] = case.surrogate_spectrum()
             out["sur_fine"] = case.surrogate_spectrum_fine()
-            out["sur_fine_uniform"] = case.surrogate_spectrum_fine(shape="uniform")
+            out["sur_fine_by_batch"] = fine_by_batch
             out["sur_alone"] = case._head(case.sur_hsum, case.sur_lsum).cpu().numpy() / max(case.histories, 1)
         if timed:
             # the per-batch snapshots sit between the events; each batch is
@@ -682,11 +686,34 @@ def main():
     if sur is not None:
         errors["surrogate_cv"] = {
             "coarse_512": spectrum_error_stats(compare["surrogate"]["sur_coarse"], coarse(ref_cxr)),
-            "fine_2048": spectrum_error_stats(compare["surrogate"]["sur_fine"], ref_cxr),
-            "fine_2048_uniform_shape": spectrum_error_stats(compare["surrogate"]["sur_fine_uniform"], ref_cxr)}
+            "fine_2048": spectrum_error_stats(compare["surrogate"]["sur_fine"], ref_cxr)}
         if sigma is not None:
             errors["surrogate_cv"]["fine_2048_in_fp64_sigma"] = sigma_stats(compare["surrogate"]["sur_fine"], ref_cxr,
                                                                             sigma["cxr"])
+        if ref_name == "fp64":
+            # The fine-bin error is the exact sub-sample's sampling noise: it
+            # falls as 1 / sqrt(histories). Its trajectory over the comparison
+            # batches (cumulative estimates against the cumulative FP64
+            # spectra), the fitted exponent, and the value it extrapolates to
+            # at the configuration's 1e8 histories.
+            pb = compare["fp64"]["per_batch"]
+            traj = []
+            for k in range(1, C + 1):
+                ref_k = np.mean(np.stack([b["cxr"] for b in pb[:k]]), axis=0)
+                traj.append(spectrum_error_stats(compare["surrogate"]["sur_fine_by_batch"][k - 1], ref_k))
+            ks = np.arange(1, C + 1, dtype=float)
+            rms = np.array([t["rms_over_tiles"] for t in traj])
+            slope = float(np.polyfit(np.log(ks), np.log(np.maximum(rms, 1e-300)), 1)[0]) if C >= 2 else float("nan")
+            scale = np.sqrt(C * H / 1.0e8)
+            errors["surrogate_cv"]["fine_2048_by_batches"] = {
+                "histories": [int(k * H) for k in ks],
+                "max_over_tiles": [t["max_over_tiles"] for t in traj],
+                "rms_over_tiles": [t["rms_over_tiles"] for t in traj],
+                "rms_exponent_vs_histories": slope,
+                "projected_at_1e8_histories": {
+                    "max_over_tiles": traj[-1]["max_over_tiles"] * scale,
+                    "rms_over_tiles": traj[-1]["rms_over_tiles"] * scale,
+                    "rule": "measured at %d histories x sqrt(%d / 1e8)" % (C * H, C * H)}}
         # the surrogate alone (no control variate), coarse: what the network
         # gains over the exact sub-sample alone is the gap between the two
         errors["surrogate_alone_coarse_512"] = spectrum_error_stats(compare["surrogate"]["sur_alone"],

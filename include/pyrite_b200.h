@@ -67,6 +67,7 @@ enum pb_rng { PB_RNG_SPLITMIX = 0, PB_RNG_PHILOX = 1 };
 enum pb_precision { PB_FP64 = 0, PB_MIXED = 1 };
 enum pb_beam_mode { PB_BEAM_EXPLICIT = 0, PB_BEAM_SPOT = 1, PB_BEAM_TWISS = 2 };
 enum pb_quadrature { PB_QUAD_NODE = 0, PB_QUAD_BINMEAN = 1 };
+enum pb_elastic { PB_ELASTIC_SR = 0, PB_ELASTIC_ELSEPA = 2 };  /* the reference's elastic_model_code */
 
 /* Exact analytic physics, padded per-layer element rows
  * (transport/batching.py:33-105). Device pointers. */
@@ -157,6 +158,29 @@ typedef struct pb_tallies {
     double *deposit;             /* [n_layers] keV lost continuously, per layer */
 } pb_tallies;
 
+/* ELSEPA tabulated elastic scattering (ABI 5), the reference's packed group
+ * of src/pyrite/montecarlo/transport/scattering.py:398-490
+ * (pack_elsepa_tables): every (layer, element) slot owns ``length`` energy
+ * rows from ``start``; a row holds ln E, the log of the macroscopic rate
+ * n sigma [1/cm], the piecewise-linear angular density in
+ * mu = (1 - cos theta) / 2 on the shared grid ``mu``, its CDF and a guide
+ * table of ``cells + 1`` panel bounds (cells a power of two). The rate is
+ * interpolated log-log in energy (_elsepa_rate_scalar, :539-546) and a polar
+ * cosine comes from one uniform inverted on both bracketing rows
+ * (_sample_cos_theta_elsepa, :616-640). */
+typedef struct pb_elsepa {
+    int32_t n_mu;
+    int32_t cells;
+    const int64_t *start;      /* [n_layers * max_el] */
+    const int64_t *length;     /* [n_layers * max_el], >= 2 for every element */
+    const double *logE;        /* [rows] ln(E / eV), increasing within a slot */
+    const double *log_rate;    /* [rows] */
+    const double *cdf;         /* [rows * n_mu] */
+    const double *pdf;         /* [rows * n_mu] */
+    const double *mu;          /* [n_mu] */
+    const int32_t *guide;      /* [rows * (cells + 1)] */
+} pb_elsepa;
+
 typedef struct pb_transport_args {
     int32_t rng;        /* pb_rng */
     int32_t precision;  /* pb_precision */
@@ -188,6 +212,12 @@ typedef struct pb_transport_args {
      * Needs Z. Zero keeps the deterministic loss. */
     int32_t straggling;
     const double *Z;        /* [n_layers * max_el] atomic numbers */
+    /* ABI 5: the elastic model, PB_ELASTIC_SR (the screened-Rutherford rates
+     * and angles of pb_layers) or PB_ELASTIC_ELSEPA (the tables below; the
+     * exact core only: use_lut must be 0, as the reference bypasses its LUT
+     * for tabulated elastic scattering). */
+    int32_t elastic_model;
+    pb_elsepa elsepa;
 } pb_transport_args;
 
 /* CXR reflection rows and coupling tables (cxr/_batched.py:232-331). */

@@ -51,6 +51,21 @@ _I8 = C.POINTER(C.c_int8)
 _U8 = C.POINTER(C.c_uint8)
 
 
+class _Elsepa(C.Structure):
+    _fields_ = [
+        ("n_mu", C.c_int),
+        ("cells", C.c_int),
+        ("start", C.POINTER(C.c_int64)),
+        ("length", C.POINTER(C.c_int64)),
+        ("logE", _D),
+        ("log_rate", _D),
+        ("cdf", _D),
+        ("pdf", _D),
+        ("mu", _D),
+        ("guide", C.POINTER(C.c_int32)),
+    ]
+
+
 class _Layers(C.Structure):
     _fields_ = [
         ("n_layers", C.c_int),
@@ -66,6 +81,7 @@ class _Layers(C.Structure):
         ("sr_joy_numer", _D),
         ("Z", _D),
         ("straggling", C.c_int),
+        ("elsepa", C.POINTER(_Elsepa)),
     ]
 
 
@@ -184,6 +200,10 @@ def _declare(L):
     L.or_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.or_dEds_spliced.restype = C.c_double
     L.or_dEds_spliced.argtypes = [C.POINTER(_Layers), C.c_int, C.c_double]
+    L.or_elsepa_rate.restype = C.c_double
+    L.or_elsepa_rate.argtypes = [C.POINTER(_Elsepa), C.c_int64, C.c_int64, C.c_double]
+    L.or_elsepa_cos_theta.restype = C.c_double
+    L.or_elsepa_cos_theta.argtypes = [C.POINTER(_Elsepa), C.c_int64, C.c_int64, C.c_double, C.c_double]
     L.or_sr_rate.restype = C.c_double
     L.or_sr_rate.argtypes = [C.c_double, C.c_double, C.c_double]
     L.or_transport.restype = None
@@ -369,11 +389,48 @@ class LayerTables:
             len(self.z_top), Z.shape[1], _p(self.z_top, _D), _p(self.z_bot, _D),
             _p(self.n_el, _I32), _p(self.J, _D), _p(self.k, _D), _p(self.coeff, _D),
             _p(self.E_cross, _D), _p(self.sr_rate_numer, _D), _p(self.sr_joy_numer, _D),
-            _p(self.Z, _D), 0,
+            _p(self.Z, _D), 0, None,
         )
+        self.elsepa = None
+
+    def use_elsepa(self, tables: "ElsepaTables | None"):
+        """Sample elastic events from ELSEPA tables (None: screened Rutherford)."""
+        self.elsepa = tables
+        self.struct.elsepa = C.pointer(tables.struct) if tables is not None else None
+        return self
 
     def dEds(self, L, E):
         return float(lib().or_dEds_spliced(C.byref(self.struct), int(L), float(E)))
+
+
+class ElsepaTables:
+    """A packed ELSEPA group in the layout of ``pack_elsepa_tables``
+    (``scattering.py:398-490``): ``start``/``length`` [n_layers, max_el], the
+    flat ``logE``/``log_rate`` rows, ``cdf``/``pdf`` [rows, n_mu], ``mu``
+    [n_mu] and ``guide`` [rows, cells + 1]."""
+
+    def __init__(self, start, length, logE, log_rate, cdf, pdf, mu, guide):
+        self.start = np.ascontiguousarray(start, dtype=np.int64)
+        self.length = np.ascontiguousarray(length, dtype=np.int64)
+        self.logE, self.log_rate = _f64(logE), _f64(log_rate)
+        self.cdf, self.pdf, self.mu = _f64(cdf), _f64(pdf), _f64(mu)
+        self.guide = np.ascontiguousarray(guide, dtype=np.int32)
+        self.struct = _Elsepa(
+            int(self.mu.size), int(self.guide.shape[1] - 1), self.start.ctypes.data_as(C.POINTER(C.c_int64)),
+            self.length.ctypes.data_as(C.POINTER(C.c_int64)), _p(self.logE, _D), _p(self.log_rate, _D),
+            _p(self.cdf, _D), _p(self.pdf, _D), _p(self.mu, _D), self.guide.ctypes.data_as(C.POINTER(C.c_int32)),
+        )
+
+    def slot(self, L, k):
+        return int(self.start[L, k]), int(self.length[L, k])
+
+    def rate(self, L, k, E_keV):
+        """Macroscopic elastic rate [1/cm] of element ``k`` of layer ``L``."""
+        return float(lib().or_elsepa_rate(C.byref(self.struct), *self.slot(L, k), float(E_keV)))
+
+    def cos_theta(self, L, k, E_keV, xi):
+        """Polar deflection cosine for the uniform ``xi``."""
+        return float(lib().or_elsepa_cos_theta(C.byref(self.struct), *self.slot(L, k), float(E_keV), float(xi)))
 
 
 class LutTables:

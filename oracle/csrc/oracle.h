@@ -36,6 +36,25 @@ enum {
     OR_EVENT_CUTOFF = 7
 };
 
+/* ELSEPA tabulated elastic group (scattering.py:398-490, pack_elsepa_tables):
+ * per (layer, element) a run of energy rows, each an angular density on the
+ * shared mu grid with its CDF and guide table. */
+typedef struct {
+    int n_mu;
+    int cells;                   /* guide cells (a power of two) */
+    const int64_t *start;        /* [n_layers*max_el] first row */
+    const int64_t *length;       /* [n_layers*max_el] rows */
+    const double *logE;          /* [rows] ln(E / eV) */
+    const double *log_rate;      /* [rows] ln(n sigma / cm^-1) */
+    const double *cdf;           /* [rows*n_mu] */
+    const double *pdf;           /* [rows*n_mu] */
+    const double *mu;            /* [n_mu] */
+    const int32_t *guide;        /* [rows*(cells+1)] */
+} or_elsepa;
+
+double or_elsepa_rate(const or_elsepa *t, int64_t start, int64_t length, double E_keV);
+double or_elsepa_cos_theta(const or_elsepa *t, int64_t start, int64_t length, double E_keV, double xi);
+
 /* Padded per-layer element tables: batching.py:33-105 (pack_layer_tables). */
 typedef struct {
     int n_layers;
@@ -51,6 +70,7 @@ typedef struct {
     const double *sr_joy_numer;  /* 3.4e-3 Z^0.67 */
     const double *Z;             /* [n_layers*max_el] atomic numbers (Urban straggling) */
     int straggling;              /* 1: Urban energy-loss straggling per flight */
+    const or_elsepa *elsepa;     /* non-NULL: ELSEPA elastic model (elastic_model_code 2) */
 } or_layers;
 
 /* Urban energy-loss straggling (straggling.py:37-333). */

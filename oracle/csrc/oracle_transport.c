@@ -243,6 +243,86 @@ double or_sr_rate(double E, double sr_rate_numer, double sr_joy_numer) {
 /* scattering.py:234-236 */
 double or_cos_theta_sr(double alpha, double R) { return 1.0 - 2.0 * alpha * R / (1.0 + alpha - R); }
 
+/* ---- ELSEPA tabulated elastic scattering (scattering.py:516-640) -------- */
+
+/* _elsepa_bracket: grid interval and fraction of logE, clamped to the ends */
+static void elsepa_bracket(const or_elsepa *t, double logE, int64_t start, int64_t length, int64_t *row,
+                           double *f) {
+    int64_t first = start, last = start + length - 1;
+    if (logE <= t->logE[first]) { *row = first; *f = 0.0; return; }
+    if (logE >= t->logE[last]) { *row = last - 1; *f = 1.0; return; }
+    int64_t lo = first, hi = last;
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) / 2;
+        if (t->logE[mid] <= logE) lo = mid; else hi = mid;
+    }
+    *row = lo;
+    *f = (logE - t->logE[lo]) / (t->logE[hi] - t->logE[lo]);
+}
+
+/* _elsepa_rate_scalar: macroscopic elastic rate [1/cm], log-log in energy */
+double or_elsepa_rate(const or_elsepa *t, int64_t start, int64_t length, double E_keV) {
+    int64_t row;
+    double f;
+    elsepa_bracket(t, log(E_keV * 1e3), start, length, &row, &f);
+    return exp(t->log_rate[row] + f * (t->log_rate[row + 1] - t->log_rate[row]));
+}
+
+/* _elsepa_panel: last panel k with cdf[row, k] <= xi, bisection inside the
+ * guide window of xi's cell */
+static int64_t elsepa_panel(const or_elsepa *t, int64_t row, double xi) {
+    int cells = t->cells;
+    double scaled = xi * cells;
+    int cell;
+    if (scaled >= cells) cell = cells - 1;
+    else if (scaled > 0.0) cell = (int)scaled;
+    else cell = 0;
+    const int32_t *g = t->guide + row * (int64_t)(cells + 1);
+    int64_t lo = g[cell], hi = (int64_t)g[cell + 1] + 1;
+    const double *cdf = t->cdf + row * (int64_t)t->n_mu;
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) / 2;
+        if (cdf[mid] <= xi) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+/* _elsepa_invert_row: the quadratic CDF of the linear panel density solved
+ * in its cancellation-free form, t clamped to [0, 1] */
+static double elsepa_invert_row(const or_elsepa *t, int64_t row, double xi) {
+    int64_t lo = elsepa_panel(t, row, xi);
+    const double *cdf = t->cdf + row * (int64_t)t->n_mu;
+    const double *pdf = t->pdf + row * (int64_t)t->n_mu;
+    double dmu = t->mu[lo + 1] - t->mu[lo];
+    double p0 = pdf[lo], p1 = pdf[lo + 1];
+    double r = xi - cdf[lo];
+    double b = dmu * p0;
+    double disc = b * b + 2.0 * dmu * (p1 - p0) * r;
+    if (disc < 0.0) disc = 0.0;
+    double denom = b + sqrt(disc);
+    double tt = denom > 0.0 ? 2.0 * r / denom : 0.0;
+    if (tt < 0.0) tt = 0.0;
+    else if (tt > 1.0) tt = 1.0;
+    return t->mu[lo] + tt * dmu;
+}
+
+/* _sample_cos_theta_elsepa: one xi inverted on both bracketing energy rows,
+ * quantiles interpolated linearly in ln E */
+double or_elsepa_cos_theta(const or_elsepa *t, int64_t start, int64_t length, double E_keV, double xi) {
+    int64_t row;
+    double f;
+    elsepa_bracket(t, log(E_keV * 1e3), start, length, &row, &f);
+    double mu0 = elsepa_invert_row(t, row, xi);
+    double mu1 = elsepa_invert_row(t, row + 1, xi);
+    return 1.0 - 2.0 * ((1.0 - f) * mu0 + f * mu1);
+}
+
+/* the elastic rate of element slot ix at E: ELSEPA or screened Rutherford */
+static double elastic_rate(const or_layers *ly, int ix, double E) {
+    if (ly->elsepa) return or_elsepa_rate(ly->elsepa, ly->elsepa->start[ix], ly->elsepa->length[ix], E);
+    return or_sr_rate(E, ly->sr_rate_numer[ix], ly->sr_joy_numer[ix]);
+}
+
 /* core_geometry.py:16-35, _rotate_direction_scalar */
 void or_rotate(double *dx, double *dy, double *dz, double cos_t, double phi) {
     double st2 = 1.0 - cos_t * cos_t;
@@ -275,7 +355,7 @@ static int layer_of(const or_layers *ly, double z) {
 /* ---- the per-electron event loop ----------------------------------------
  * cores.py:379-1230 with per_electron=True, lut=False, grooved=False,
  * inelastic=False, radiative=False, mixed=False, cone_split=False,
- * elastic_model_code=0 (SR), energy_model_code=1 (midpoint), straggling
+ * elastic_model_code=0 (SR) or 2 (ELSEPA, ly->elsepa), energy_model_code=1 (midpoint), straggling
  * off or Urban (ly->straggling), max_dE_frac=0, infinite lateral footprint. With spliced stopping the lazy
  * cutoff bound is never armed (_jit_cutoff_bound.py:47-56), so the midpoint
  * cutoff solve always runs.
@@ -301,7 +381,7 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
         double total_rate = 0.0;
         for (int i = 0; i < n_el; ++i) {
             int ix = L * ly->max_el + i;
-            total_rate += or_sr_rate(E_j, ly->sr_rate_numer[ix], ly->sr_joy_numer[ix]);
+            total_rate += elastic_rate(ly, ix, E_j);
         }
         double lam = 1e8 / total_rate;
         if (tau_left < 0.0) {
@@ -415,16 +495,19 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
             i_el = n_el - 1;
             for (int k = 0; k < n_el; ++k) {
                 int ix = L * ly->max_el + k;
-                cum += or_sr_rate(E_j, ly->sr_rate_numer[ix], ly->sr_joy_numer[ix]);
+                cum += elastic_rate(ly, ix, E_j);
                 if (cum > u) { i_el = k; break; }
             }
         }
-        double alpha = ly->sr_joy_numer[L * ly->max_el + i_el] / E;
+        const int ix_el = L * ly->max_el + i_el;
         double cos_u = draw_uniform(rng_kind, key, draws);
         draws += 1;
         double phi_u = draw_uniform(rng_kind, key, draws);
         draws += 1;
-        double cos_t = or_cos_theta_sr(alpha, cos_u);
+        /* cores.py:1158-1188: ELSEPA tables at the post-step energy, else SR */
+        double cos_t = ly->elsepa ? or_elsepa_cos_theta(ly->elsepa, ly->elsepa->start[ix_el],
+                                                        ly->elsepa->length[ix_el], E, cos_u)
+                                  : or_cos_theta_sr(ly->sr_joy_numer[ix_el] / E, cos_u);
         or_rotate(&dx, &dy, &dz, cos_t, 2.0 * M_PI * phi_u);
         steps += 1;
     }

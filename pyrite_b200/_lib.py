@@ -19,6 +19,7 @@ PB_BEAM_EXPLICIT, PB_BEAM_SPOT, PB_BEAM_TWISS = 0, 1, 2
 PB_QUAD_NODE, PB_QUAD_BINMEAN = 0, 1
 PB_DEV_STEP_LIMIT, PB_DEV_ROW_OVERFLOW, PB_DEV_QUEUE_OVERFLOW = 1, 2, 4
 PB_DEV_WAIT_TIMEOUT, PB_DEV_BAD_INPUT = 8, 16
+PB_ELASTIC_SR, PB_ELASTIC_ELSEPA = 0, 2
 
 _vp = C.c_void_p
 _i32, _i64, _u64, _f64 = C.c_int32, C.c_int64, C.c_uint64, C.c_double
@@ -72,6 +73,13 @@ class PbTallies(C.Structure):
     ]
 
 
+class PbElsepa(C.Structure):
+    _fields_ = [
+        ("n_mu", _i32), ("cells", _i32), ("start", _vp), ("length", _vp), ("logE", _vp), ("log_rate", _vp),
+        ("cdf", _vp), ("pdf", _vp), ("mu", _vp), ("guide", _vp),
+    ]
+
+
 class PbTransportArgs(C.Structure):
     _fields_ = [
         ("rng", _i32), ("precision", _i32), ("use_lut", _i32), ("block_threads", _i32),
@@ -79,7 +87,7 @@ class PbTransportArgs(C.Structure):
         ("layers", PbLayers), ("lut", PbLut), ("beam", PbBeam), ("cap", _i64), ("rows", PbRows),
         ("seg_count", _vp), ("exit_code", _vp), ("final_pos", _vp), ("final_dir", _vp),
         ("final_E", _vp), ("seg", PbSegments), ("tallies", PbTallies), ("work_counter", _vp),
-        ("status", _vp), ("straggling", _i32), ("Z", _vp),
+        ("status", _vp), ("straggling", _i32), ("Z", _vp), ("elastic_model", _i32), ("elsepa", PbElsepa),
     ]
 
 

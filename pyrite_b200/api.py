@@ -20,7 +20,10 @@ import torch
 from . import _lib as L
 from .tables import (
     CRYSTALS,
+    ElsepaGroup,
     LayerStack,
+    check_elsepa_range,
+    pack_elsepa,
     beam_entry_basis,
     beam_frame_basis,
     build_transport_lut,
@@ -177,12 +180,24 @@ _RNG = {"splitmix": L.PB_RNG_SPLITMIX, "philox": L.PB_RNG_PHILOX}
 _PREC = {"fp64": L.PB_FP64, "mixed": L.PB_MIXED}
 
 
+def _fill_elsepa(h: "_Holder", g: ElsepaGroup) -> "L.PbElsepa":
+    t = L.PbElsepa()
+    t.n_mu, t.cells = int(g.mu.size), int(g.guide.shape[1] - 1)
+    t.start = _ptr(h.typed(np.asarray(g.start, dtype=np.int64).reshape(-1), torch.int64))
+    t.length = _ptr(h.typed(np.asarray(g.length, dtype=np.int64).reshape(-1), torch.int64))
+    t.logE, t.log_rate = _ptr(h.f64(g.logE)), _ptr(h.f64(g.log_rate))
+    t.cdf, t.pdf, t.mu = _ptr(h.f64(g.cdf)), _ptr(h.f64(g.pdf)), _ptr(h.f64(g.mu))
+    t.guide = _ptr(h.typed(np.asarray(g.guide, dtype=np.int32), torch.int32))
+    return t
+
+
 def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_per_ang3=None,
                           E_cut_keV=5.0, seed=0, max_steps=400_000, beam_dir=None,
                           composition=None, layers=None, beam_fwhm_mm=None, beam_fwhm_y_mm=None,
                           tilt_polar_rad=0.0, tilt_azim_rad=0.0, transverse_distribution=None,
                           *, lut=True, rng="splitmix", precision="fp64", entry=None, cap=None,
-                          device=None, stream=None, block_threads=0, tallies=None, straggling=False):
+                          device=None, stream=None, block_threads=0, tallies=None, straggling=False,
+                          elastic_model="sr", elastic_tables=None):
     """Transport ``Ne`` electrons into a slab or layer stack; returns segment rows.
 
     Same contract as the reference's per-electron cores: rows of history i
@@ -195,6 +210,16 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     ``straggling=True``, transport/straggling.py) instead of the
     deterministic midpoint loss.
 
+    ``elastic_model="elsepa"`` samples elastic events from tabulated ELSEPA
+    cross sections and angular distributions (the reference's default model,
+    scattering.py:330-640): ``elastic_tables`` is either the reference's
+    ``elastic_tables`` argument (one list per layer of one mapping per
+    element with ``energy_eV``, ``total_elastic_cm2``, ``mu``,
+    ``dcs_cm2_sr``) or an already packed ``tables.ElsepaGroup``. As in the
+    reference the exact core runs (``lut`` is ignored) and energies outside
+    the tables are refused. ``"sr"`` (the default here, since the production
+    ELSEPA tables are not shipped) is the analytic screened-Rutherford model.
+
     ``tallies=(n_E, n_theta)`` also returns the kernel's fused summary
     tallies, the reference's summary tables (trajectory_summary.py:147-260)
     without materialising rows for them: ``tally_fates`` (counts by exit
@@ -203,12 +228,22 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     angle on n_theta bins over [0, pi]), ``tally_deposit_keV`` (continuous
     loss per layer, summed over the histories).
     """
-    dev = _device(device)
     lib = L.load()
     if layers is None:
         comp = composition if composition is not None else [(element, n_atoms_per_ang3)]
         layers = [(0.0, float(thickness_ang), list(comp))]
     stack = LayerStack([(float(a), float(b), list(c)) for a, b, c in layers])
+    group = None
+    if elastic_model == "elsepa":
+        if elastic_tables is None:
+            raise ValueError("elastic_model='elsepa' needs elastic_tables (the production tables are not shipped)")
+        group = elastic_tables if isinstance(elastic_tables, ElsepaGroup) else pack_elsepa(stack, elastic_tables)
+        E_hi = float(E0_keV) if entry is None else float(np.max(entry[2]))
+        check_elsepa_range(group, stack, float(E_cut_keV), E_hi)
+        lut = False  # the exact core, as the reference bypasses its LUT for tabulated elastic scattering
+    elif elastic_model != "sr":
+        raise ValueError(f"elastic_model must be 'sr' or 'elsepa', not {elastic_model!r}")
+    dev = _device(device)
     h = _Holder(dev)
     a = L.PbTransportArgs()
     a.rng = _RNG[rng]
@@ -223,6 +258,9 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     a.layers = _fill_layers(h, stack)
     if straggling:
         a.straggling, a.Z = 1, _ptr(h.f64(stack.Z))
+    if group is not None:
+        a.elastic_model = L.PB_ELASTIC_ELSEPA
+        a.elsepa = _fill_elsepa(h, group)
     if lut:
         E_hi = float(E0_keV) if entry is None else float(np.max(entry[2]))
         a.lut = _fill_lut(h, build_transport_lut(stack, E_cut_keV, E_hi), a.precision)

@@ -133,6 +133,16 @@ int pb_transport(const pb_transport_args *a, void *stream) {
     if (a->block_threads != 0 && (a->block_threads % 32 != 0 || a->block_threads > 256))
         return fail(PB_ERR_INVALID, "pb_transport: block_threads must be a multiple of 32 <= 256");
     if (a->straggling && !a->Z) return fail(PB_ERR_INVALID, "pb_transport: straggling needs Z");
+    if (a->elastic_model != PB_ELASTIC_SR && a->elastic_model != PB_ELASTIC_ELSEPA)
+        return fail(PB_ERR_INVALID, "pb_transport: elastic_model = %d", a->elastic_model);
+    if (a->elastic_model == PB_ELASTIC_ELSEPA) {
+        const pb_elsepa &t = a->elsepa;
+        if (a->use_lut) return fail(PB_ERR_UNSUPPORTED, "pb_transport: ELSEPA elastic runs on the exact core only");
+        if (t.n_mu < 2 || t.cells < 1 || (t.cells & (t.cells - 1)))
+            return fail(PB_ERR_INVALID, "pb_transport: ELSEPA needs n_mu >= 2 and a power-of-two cell count");
+        if (!t.start || !t.length || !t.logE || !t.log_rate || !t.cdf || !t.pdf || !t.mu || !t.guide)
+            return fail(PB_ERR_INVALID, "pb_transport: every ELSEPA table pointer must be set");
+    }
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a->work_counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "pb_transport: zero work counter");

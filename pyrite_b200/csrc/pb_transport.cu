@@ -213,6 +213,74 @@ __device__ __forceinline__ Real sr_rate(Real E, Real srn, Real sjn) {
     return srn / (E * E) / (a * ((Real)1 + a)) * (r * r);
 }
 
+// ---- ELSEPA tabulated elastic scattering (scattering.py:516-640) ----------
+// The tables stay in global memory: a case's rows (tens of energies x a few
+// hundred mu nodes per element) are L2-resident, and one event reads two
+// short guide windows and four table entries, so staging them would cost
+// more shared memory than the reads it saves. FP64 throughout: the exact
+// core replays the reference's draws.
+
+// _elsepa_bracket: energy row and fraction of lnE within one slot, clamped.
+__device__ __forceinline__ int64_t elsepa_bracket(const pb_elsepa &t, double lnE, int64_t start, int64_t len,
+                                                  double &f) {
+    const int64_t first = start, last = start + len - 1;
+    if (lnE <= t.logE[first]) { f = 0.0; return first; }
+    if (lnE >= t.logE[last]) { f = 1.0; return last - 1; }
+    int64_t lo = first, hi = last;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (t.logE[mid] <= lnE) lo = mid;
+        else hi = mid;
+    }
+    f = (lnE - t.logE[lo]) / (t.logE[hi] - t.logE[lo]);
+    return lo;
+}
+
+// _elsepa_rate_scalar: n sigma [1/cm] of one element, log-log in energy.
+__device__ __forceinline__ double elsepa_rate(const pb_elsepa &t, int ix, double E_keV) {
+    double f;
+    const int64_t r = elsepa_bracket(t, log(E_keV * 1e3), t.start[ix], t.length[ix], f);
+    return exp(t.log_rate[r] + f * (t.log_rate[r + 1] - t.log_rate[r]));
+}
+
+// _elsepa_panel + _elsepa_invert_row: the panel k whose CDF bracket holds
+// xi, found by bisection inside the guide window of xi's cell, then the
+// linear-density panel's quadratic CDF solved in its cancellation-free form.
+__device__ __forceinline__ double elsepa_invert(const pb_elsepa &t, int64_t row, double xi) {
+    const int cells = t.cells;
+    const double scaled = xi * (double)cells;
+    const int cell = scaled >= (double)cells ? cells - 1 : scaled > 0.0 ? (int)scaled : 0;
+    const int32_t *g = t.guide + row * (int64_t)(cells + 1);
+    const double *cdf = t.cdf + row * (int64_t)t.n_mu;
+    int64_t lo = g[cell], hi = (int64_t)g[cell + 1] + 1;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (cdf[mid] <= xi) lo = mid;
+        else hi = mid;
+    }
+    const double *pdf = t.pdf + row * (int64_t)t.n_mu;
+    const double dmu = t.mu[lo + 1] - t.mu[lo];
+    const double p0 = pdf[lo], p1 = pdf[lo + 1];
+    const double r = xi - cdf[lo];
+    const double b = dmu * p0;
+    double disc = b * b + 2.0 * dmu * (p1 - p0) * r;
+    if (disc < 0.0) disc = 0.0;
+    const double denom = b + sqrt(disc);
+    double u = denom > 0.0 ? 2.0 * r / denom : 0.0;
+    u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+    return t.mu[lo] + u * dmu;
+}
+
+// _sample_cos_theta_elsepa: one uniform on both bracketing energy rows, the
+// quantiles interpolated linearly in ln E.
+__device__ __forceinline__ double elsepa_cos_theta(const pb_elsepa &t, int ix, double E_keV, double xi) {
+    double f;
+    const int64_t r = elsepa_bracket(t, log(E_keV * 1e3), t.start[ix], t.length[ix], f);
+    const double mu0 = elsepa_invert(t, r, xi);
+    const double mu1 = elsepa_invert(t, r + 1, xi);
+    return 1.0 - 2.0 * ((1.0 - f) * mu0 + f * mu1);
+}
+
 // kinematics.py:162-166
 template <class Real>
 __device__ __forceinline__ Real beta_from_keV(Real E) {
@@ -355,7 +423,8 @@ __device__ __forceinline__ int hist_slot(double v, double lo, double hi, int n) 
     return b + 1;
 }
 
-template <class Real, bool kLut, int kRng, bool kStrag>
+// kEls: ELSEPA elastic rates and angles (the exact core only, kLut false).
+template <class Real, bool kLut, int kRng, bool kStrag, bool kEls>
 __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ LayerSmem ly;
@@ -501,7 +570,8 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             } else {
                 for (int k = 0; k < n_el; ++k) {
                     const int ix = L * max_el + k;
-                    total_rate += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
+                    if constexpr (kEls) total_rate += (Real)elsepa_rate(p.elsepa, ix, E_j);
+                    else total_rate += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
                 }
             }
             const Real lam = (Real)1e8 / total_rate;
@@ -668,25 +738,29 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                         Real cum = 0;
                         for (int k = 0; k < n_el; ++k) {
                             const int ix = L * max_el + k;
-                            cum += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
+                            if constexpr (kEls) cum += (Real)elsepa_rate(p.elsepa, ix, E_j);
+                            else cum += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
                             if (cum > target) { i_el = k; break; }
                         }
                     }
                 }
-                Real alpha;
+                Real alpha = 0;
                 if constexpr (kLut) {
                     int ai;
                     Real af;
                     lut_index(lut, E, ai, af);
                     alpha = lerp(lut.alpha + ((int64_t)L * max_el + i_el) * lut.ne, ai, af);
-                } else {
+                } else if constexpr (!kEls) {
                     alpha = (Real)ly.sjn[L * max_el + i_el] / (Real)E;
                 }
-                const Real cos_u = (Real)uniform<kRng>(key, draws);
+                const double cos_ud = uniform<kRng>(key, draws);
+                const Real cos_u = (Real)cos_ud;
                 draws += 1;
                 const Real phi_u = (Real)uniform<kRng>(key, draws);
                 draws += 1;
-                const Real cos_t = (Real)1 - (Real)2 * alpha * cos_u / ((Real)1 + alpha - cos_u);
+                Real cos_t;
+                if constexpr (kEls) cos_t = (Real)elsepa_cos_theta(p.elsepa, L * max_el + i_el, E, cos_ud);
+                else cos_t = (Real)1 - (Real)2 * alpha * cos_u / ((Real)1 + alpha - cos_u);
                 rotate<Real>(dx, dy, dz, cos_t, (Real)(2.0 * kPi) * phi_u);
                 steps += 1;
             }
@@ -742,9 +816,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             if (tal.deposit[j] != 0.0) atomicAdd(&p.tallies.deposit[j], tal.deposit[j]);
 }
 
-template <class Real, bool kLut, int kRng, bool kStrag>
+template <class Real, bool kLut, int kRng, bool kStrag, bool kEls = false>
 static cudaError_t launch_transport_t(const pb_transport_args &a, cudaStream_t s, int sms) {
-    auto kern = transport_kernel<Real, kLut, kRng, kStrag>;
+    auto kern = transport_kernel<Real, kLut, kRng, kStrag, kEls>;
     size_t dyn = 0;
     if (kLut && a.lut.total_bytes <= (int64_t)kLutSmemBytes) dyn = (size_t)a.lut.total_bytes;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -767,6 +841,14 @@ static cudaError_t launch_transport_s(const pb_transport_args &a, cudaStream_t s
     const bool mixed = a.precision == PB_MIXED;
     const bool lut = a.use_lut != 0;
     const bool philox = a.rng == PB_RNG_PHILOX;
+    if (a.elastic_model == PB_ELASTIC_ELSEPA) {  // exact core only (checked by the caller)
+        if (mixed) {
+            if (philox) return launch_transport_t<float, false, PB_RNG_PHILOX, kStrag, true>(a, s, sms);
+            return launch_transport_t<float, false, PB_RNG_SPLITMIX, kStrag, true>(a, s, sms);
+        }
+        if (philox) return launch_transport_t<double, false, PB_RNG_PHILOX, kStrag, true>(a, s, sms);
+        return launch_transport_t<double, false, PB_RNG_SPLITMIX, kStrag, true>(a, s, sms);
+    }
 #define PB_DISPATCH(R, L, G) return launch_transport_t<R, L, G, kStrag>(a, s, sms)
     if (mixed) {
         if (lut) { if (philox) PB_DISPATCH(float, true, PB_RNG_PHILOX); PB_DISPATCH(float, true, PB_RNG_SPLITMIX); }

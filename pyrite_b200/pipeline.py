@@ -526,36 +526,23 @@ class ScoringCase:
                 "fallback_tiles": np.flatnonzero(self.sur_fallback).tolist(),
                 "audit_surrogate_alone_per_tile": audit}
 
-    def surrogate_spectrum_fine(self, shape: str = "sample"):
+    def surrogate_spectrum_fine(self):
         """Surrogate (+ exact control variate) spectrum on the case's own bins
-        [n_dir, n_E] so far, per history.
-
-        ``shape="sample"`` (the default): each coarse bin's control-variate
-        total C(c) is spread over its fine bins in the proportions of the
-        exact sub-sample,
-            S(j) = C(c) * E_s(j) / mean_{j' in c} E_s(j'),
-        a ratio estimator (consistent, bias of order 1 / sub-sample size): a
-        segment's lines are much narrower than a coarse bin, so the fine
-        shape inside a coarse bin is the lines' own, which the sub-sample
-        measures with far less scatter than its absolute level. Coarse bins
-        the sub-sample left empty are spread evenly.
-
-        ``shape="uniform"``: each coarse surrogate value spread evenly (U),
-        corrected by the exact sub-sample at full resolution,
+        [n_dir, n_E] so far, per history: each coarse surrogate value spread
+        over its fine bins (U), corrected by the exact sub-sample at full
+        resolution,
             S = U(S_sur(all)) + stride (S_exact(sample) - U(S_sur(sample))),
-        unbiased whatever U is, but inside a coarse bin its noise is the exact
-        sub-sample's whole noise."""
-        from .surrogate import sample_shaped
+        unbiased for the exact fine-bin spectrum whatever U is. Inside a coarse
+        bin its noise is the exact sub-sample's: a segment's lines are much
+        narrower than a fine bin, which no smooth U follows, so the fine-bin
+        error falls as 1 / sqrt(histories). (Shaping each coarse total by the
+        sub-sample's own fine proportions instead was measured no better: the
+        proportions carry the same sampling noise.)"""
         rep = self.n_E // self.surrogates[0].n_out
-        if self.sur_stride > 0 and shape == "sample":
-            s = sample_shaped(self._cv_coarse(), self.spec_sample)
-        elif shape in ("sample", "uniform"):
-            s = self._head(self.sur_hsum, self.sur_lsum).repeat_interleave(rep, dim=1)
-            if self.sur_stride > 0:
-                s += self.sur_stride * (self.spec_sample
-                                        - self._head(self.sur_hsum_s, self.sur_lsum_s).repeat_interleave(rep, dim=1))
-        else:
-            raise ValueError("shape must be 'sample' or 'uniform'")
+        s = self._head(self.sur_hsum, self.sur_lsum).repeat_interleave(rep, dim=1)
+        if self.sur_stride > 0:
+            s += self.sur_stride * (self.spec_sample
+                                    - self._head(self.sur_hsum_s, self.sur_lsum_s).repeat_interleave(rep, dim=1))
         if self._fb_args is not None:
             s[self._fb_index] = self._fb_spec
         return s.cpu().numpy() / max(self.histories, 1)

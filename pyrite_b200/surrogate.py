@@ -612,22 +612,6 @@ def train_ensemble(spec, *, k=4, n_seg=16384, n_dir=1024, epochs=10, lr=2e-3, se
     return models
 
 
-def sample_shaped(cv_coarse, sample_fine):
-    """Spread coarse control-variate totals over the fine bins in the exact
-    sub-sample's proportions: S(j) = C(c) * E_s(j) / mean_{j' in c} E_s(j')
-    for the fine bins j of coarse bin c; coarse bins the sub-sample left
-    empty are spread evenly. Both inputs in per-fine-bin units (a coarse
-    value is the mean of its fine bins); works on any device.
-
-    cv_coarse [n_dir, n_coarse], sample_fine [n_dir, n_fine] -> [n_dir, n_fine]."""
-    rep = sample_fine.shape[1] // cv_coarse.shape[1]
-    m = sample_fine.reshape(sample_fine.shape[0], cv_coarse.shape[1], rep).mean(-1)
-    has = m > 0
-    ratio = torch.where(has, cv_coarse / torch.where(has, m, torch.ones_like(m)), torch.zeros_like(m))
-    even = torch.where(has, torch.zeros_like(cv_coarse), cv_coarse)
-    return sample_fine * ratio.repeat_interleave(rep, dim=1) + even.repeat_interleave(rep, dim=1)
-
-
 def control_variate_error(res_sum, res_sq, n_batches, stride, spectrum, n_sigma=3.0, window=9):
     """Estimated error of the control-variate spectrum per detector tile.
 

@@ -176,6 +176,114 @@ class LayerStack:
 
 
 # ---------------------------------------------------------------------------
+# ELSEPA tabulated elastic scattering (transport/scattering.py:330-490).
+# ---------------------------------------------------------------------------
+ELSEPA_GUIDE_CELLS = 1024  # a power of two: xi * cells and the cell bounds j / cells are exact
+
+
+@dataclass
+class ElsepaGroup:
+    """Packed ELSEPA tables in the reference's layout (``pack_elsepa_tables``):
+    ``start``/``length`` [n_layers, max_el] energy rows of every element slot,
+    the flat rows' ``logE`` (ln eV) and ``log_rate`` (ln of n sigma in 1/cm),
+    ``pdf``/``cdf`` [rows, n_mu] on the shared ``mu`` grid, ``guide``
+    [rows, cells + 1]."""
+
+    start: np.ndarray
+    length: np.ndarray
+    logE: np.ndarray
+    log_rate: np.ndarray
+    cdf: np.ndarray
+    pdf: np.ndarray
+    mu: np.ndarray
+    guide: np.ndarray
+
+
+def elsepa_density(mu, dcs):
+    """Angular densities p(mu) of DCS rows, mu = (1 - cos theta) / 2, each row
+    normalised by its trapezoid integral, and the CDFs (exact integrals of the
+    piecewise-linear densities, last node 1): scattering.py:330-356."""
+    mu = np.asarray(mu, dtype=np.float64)
+    dcs = np.atleast_2d(np.asarray(dcs, dtype=np.float64))
+    panel = 0.5 * (dcs[:, :-1] + dcs[:, 1:]) * np.diff(mu)
+    total = panel.sum(axis=1)
+    if not np.all(np.isfinite(total)) or np.any(total <= 0.0):
+        raise ValueError("every ELSEPA DCS row needs a positive finite integral")
+    cdf = np.zeros_like(dcs)
+    cdf[:, 1:] = np.cumsum(panel, axis=1) / total[:, None]
+    cdf[:, -1] = 1.0
+    return dcs / total[:, None], cdf
+
+
+def elsepa_guide(cdf, cells=ELSEPA_GUIDE_CELLS):
+    """Guide table of each CDF row (scattering.py:366-396): entry j is the last
+    panel k <= n_mu - 2 with cdf[k] <= j / cells, so the panel of any xi in
+    cell j lies between entries j and j + 1 and a bisection there finds the
+    same panel as one over the whole row."""
+    cdf = np.atleast_2d(np.asarray(cdf, dtype=np.float64))
+    if cells < 1 or cells & (cells - 1):
+        raise ValueError("the guide cell count must be a positive power of two")
+    n_mu = cdf.shape[1]
+    head = cdf[:, : n_mu - 1]
+    if np.any(np.diff(head, axis=1) < 0.0):
+        raise ValueError("ELSEPA CDF rows must be nondecreasing")
+    edges = np.arange(cells + 1, dtype=np.float64) / cells
+    guide = np.stack([np.searchsorted(row, edges, side="right") - 1 for row in head]).astype(np.int32)
+    np.clip(guide, 0, n_mu - 2, out=guide)
+    guide[:, 0] = 0
+    guide[:, -1] = n_mu - 2
+    return guide
+
+
+def pack_elsepa(stack: "LayerStack", elastic_tables, cells=ELSEPA_GUIDE_CELLS) -> ElsepaGroup:
+    """Pack ``elastic_tables`` (one list per layer of one mapping per element,
+    in composition order, with ``energy_eV``, ``total_elastic_cm2``, ``mu``,
+    ``dcs_cm2_sr`` on one shared mu grid: the reference's ``elastic_tables``
+    argument) for the transport kernel (scattering.py:398-490)."""
+    if len(elastic_tables) != stack.n_layers:
+        raise ValueError("elastic_tables needs one entry per layer")
+    start = np.zeros((stack.n_layers, stack.max_el), dtype=np.int64)
+    length = np.zeros_like(start)
+    logE, log_rate, pdf, cdf = [], [], [], []
+    mu_ref = None
+    row = 0
+    for L, layer in enumerate(elastic_tables):
+        if len(layer) != int(stack.n_el[L]):
+            raise ValueError(f"elastic_tables layer {L} needs one table per element")
+        for k, t in enumerate(layer):
+            E = np.asarray(t["energy_eV"], dtype=np.float64)
+            sigma = np.asarray(t["total_elastic_cm2"], dtype=np.float64)
+            mu = np.asarray(t["mu"], dtype=np.float64)
+            if mu_ref is None:
+                mu_ref = mu
+            elif not np.array_equal(mu, mu_ref):
+                raise ValueError("every ELSEPA table must share one mu grid")
+            if E.size < 2 or np.any(np.diff(E) <= 0.0) or np.any(sigma <= 0.0):
+                raise ValueError("ELSEPA tables need >= 2 increasing energies and positive cross sections")
+            p, c = elsepa_density(mu, t["dcs_cm2_sr"])
+            start[L, k], length[L, k] = row, E.size
+            logE.append(np.log(E))
+            log_rate.append(np.log(float(stack.N[L, k]) * 1e24 * sigma))
+            pdf.append(p)
+            cdf.append(c)
+            row += E.size
+    cdf = np.vstack(cdf)
+    return ElsepaGroup(start, length, np.concatenate(logE), np.concatenate(log_rate), cdf, np.vstack(pdf),
+                       np.ascontiguousarray(mu_ref), elsepa_guide(cdf, cells))
+
+
+def check_elsepa_range(group: ElsepaGroup, stack: "LayerStack", E_min_keV: float, E_max_keV: float):
+    """Refuse a transport energy range outside any element's table: the
+    tables are never extrapolated (scattering.py:493-505)."""
+    for L in range(stack.n_layers):
+        for k in range(int(stack.n_el[L])):
+            s, n = int(group.start[L, k]), int(group.length[L, k])
+            lo, hi = np.exp(group.logE[s]) / 1e3, np.exp(group.logE[s + n - 1]) / 1e3
+            if E_min_keV < lo * (1 - 1e-12) or E_max_keV > hi * (1 + 1e-12):
+                raise ValueError(f"transport energy range must be within the ELSEPA table [{lo:g}, {hi:g}] keV")
+
+
+# ---------------------------------------------------------------------------
 # Transport LUT (transport/lut.py:64-283): uniform in log kinetic energy.
 # ---------------------------------------------------------------------------
 @dataclass

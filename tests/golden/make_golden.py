@@ -1008,6 +1008,83 @@ def gen_straggling():
 
 
 # ---------------------------------------------------------------------------
+# ELSEPA tabulated elastic scattering (transport/scattering.py:330-640,
+# cores.py:425-440 and 1120-1180) with synthetic tables passed through the
+# reference's public ``elastic_tables`` argument: smooth total cross sections
+# and angular densities on a shared mu grid, shaped like screened Rutherford
+# with a mild modulation so neither the rates nor the inversion are the
+# analytic model's.
+# ---------------------------------------------------------------------------
+ELSEPA_CASES = ("si30kev", "sio2_300kev", "c20mev")
+
+
+def synthetic_elsepa_table(symbol):
+    """One element's table in the reference's ``elastic_tables`` layout."""
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+
+    Z = float(TRANSPORT_ELEMENTS[symbol]["Z"])
+    energy_eV = np.geomspace(1.0e3, 1.0e8, 48)
+    E = energy_eV / 1e3
+    a = 3.4e-3 * Z ** 0.67 / E
+    r = (E + 511.0) / (E + 1024.0)
+    sigma = 5.21e-21 * Z * Z * 4.0 * np.pi / (E * E) / (a * (1.0 + a)) * r * r
+    sigma = sigma * (1.0 + 0.15 * np.sin(np.log(energy_eV)))
+    mu = np.concatenate([[0.0], np.geomspace(1.0e-9, 1.0, 199)])
+    dcs = (1.0 + 0.4 * mu[None, :]) / (mu[None, :] + a[:, None]) ** 2
+    dcs = dcs * (1.0 + 0.05 * np.cos(7.0 * mu[None, :] + np.log(E)[:, None]))
+    return dict(energy_eV=energy_eV, total_elastic_cm2=sigma, mu=mu, dcs_cm2_sr=dcs)
+
+
+def gen_elsepa():
+    rng = np.random.default_rng(29)
+    for name in ELSEPA_CASES:
+        case = TRANSPORT_CASES[name]
+        layers = case["layers"]
+        tables = [[synthetic_elsepa_table(el) for el, _n in layer[2]] for layer in layers]
+        L_ncm3 = [np.array([n * 1e24 for _el, n in layer[2]]) for layer in layers]
+        has, start, length, logE, log_rate, cdf, pdf, mu, guide = ref_scat.pack_elsepa_tables(tables, L_ncm3)
+        tp = np.deg2rad(case["tilt_deg"])
+        beam_dir, n_hat = ref_geometry.tilted_geometry(np.deg2rad(case["theta_obs_deg"]), tp, 0.0)
+        kwargs = dict(E0_keV=case["E0_keV"], Ne=case["Ne"], thickness_ang=layers[-1][1], seed=case["seed"],
+                      elastic_model="elsepa", elastic_tables=tables, transport_core="per-electron",
+                      radiative_model="uncoupled", beam_dir=beam_dir, tilt_polar_rad=tp,
+                      beam_fwhm_mm=case["beam_fwhm_mm"], transport_lut_config=TransportLUTConfig(enabled=False))
+        if len(layers) == 1:
+            kwargs["composition"] = layers[0][2]
+        else:
+            kwargs["layers"] = layers
+        out = _simulate_trajectories(**kwargs)
+        arrays = {k: np.asarray(out[k]) for k in ROW_KEYS}
+        counts = np.array([int(out[k]) for k in COUNT_KEYS], dtype=np.int64)
+        # leaves: rates and polar cosines at seeded (E, xi) of every element
+        n_leaf = 64
+        leaf_E = np.exp(rng.uniform(np.log(1.0), np.log(1.0e5), n_leaf))
+        leaf_E[:4] = (1.0, 1.0e5, 30.0, 0.5)  # both table ends, a mid value, below the table
+        leaf_xi = rng.uniform(0.0, 1.0, n_leaf)
+        leaf_xi[4:8] = (0.0, 1.0, 0.5, 1.0 - 2.0 ** -40)
+        leaf_rate = np.zeros((len(layers), has.shape[1], n_leaf))
+        leaf_cos = np.zeros_like(leaf_rate)
+        for L in range(len(layers)):
+            for k in range(len(layers[L][2])):
+                for j in range(n_leaf):
+                    E = float(leaf_E[j])  # below the table the bracket clamps to its first node
+                    leaf_rate[L, k, j] = ref_scat._elsepa_rate_scalar(E, logE, log_rate, start[L, k], length[L, k])
+                    leaf_cos[L, k, j] = ref_scat._sample_cos_theta_elsepa(E, leaf_xi[j], logE, cdf, pdf, mu, guide,
+                                                                          start[L, k], length[L, k])
+        raw = {}
+        for L, layer in enumerate(tables):
+            for k, t in enumerate(layer):
+                for f in ("energy_eV", "total_elastic_cm2", "dcs_cm2_sr"):
+                    raw[f"raw_{L}_{k}_{f}"] = t[f]
+        _save(f"elsepa_{name}", E0_keV=case["E0_keV"], E_cut_keV=5.0, seed=case["seed"], Ne=case["Ne"],
+              initial_r=out["initial_r_ang"], initial_v=out["initial_v_hat"], initial_E=out["initial_E_keV"],
+              count_names=np.array(COUNT_KEYS), counts=counts,
+              el_has=has, el_start=start, el_length=length, el_logE=logE, el_log_rate=log_rate, el_cdf=cdf,
+              el_pdf=pdf, el_mu=mu, el_guide=guide, leaf_E=leaf_E, leaf_xi=leaf_xi, leaf_rate=leaf_rate,
+              leaf_cos=leaf_cos, **raw, **arrays)
+
+
+# ---------------------------------------------------------------------------
 # Summary tables (pyrite/montecarlo/trajectory_summary.py:147-260) of the
 # golden transport cases: the reference's own reductions of its own rows.
 # ---------------------------------------------------------------------------
@@ -1142,6 +1219,7 @@ def gen_fullrun():
 
 
 GENERATORS = {
+    "elsepa": gen_elsepa,
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
     "transport": gen_transport,

@@ -51,26 +51,3 @@ def test_estimate_needs_two_batches_and_flags_a_poor_surrogate():
     z = control_variate_error(*_run(rng, 4, sigma, 10), 4, 10, np.array([np.ones(64), np.zeros(64)]))
     assert z[1] == 0.0
 
-
-def test_sample_shaped_spread_keeps_totals_and_follows_the_sample():
-    """``surrogate.sample_shaped``: each coarse total is kept, the fine bins
-    follow the sub-sample's shape exactly when the sub-sample has the true
-    shape, and coarse bins the sub-sample left empty are spread evenly."""
-    import torch
-
-    from pyrite_b200.surrogate import sample_shaped
-
-    rng = np.random.default_rng(3)
-    n_dir, n_coarse, rep = 3, 16, 4
-    truth = rng.gamma(0.3, 1.0, (n_dir, n_coarse * rep))
-    truth[1, 8:12] = 0.0  # an empty coarse bin in the sub-sample
-    coarse = truth.reshape(n_dir, n_coarse, rep).mean(-1)
-    cv = coarse.copy()
-    cv[1, 2] = 0.7  # a total the sample does not see
-    sample = 0.01 * truth  # the sub-sample: 1 % of the histories, true shape
-    out = sample_shaped(torch.tensor(cv), torch.tensor(sample)).numpy()
-    np.testing.assert_allclose(out.reshape(n_dir, n_coarse, rep).mean(-1), cv, rtol=1e-14, atol=1e-15)
-    mask = np.ones_like(truth, dtype=bool)
-    mask[1, 8:12] = False
-    np.testing.assert_allclose(out[mask], truth[mask], rtol=1e-13, atol=1e-15)
-    np.testing.assert_allclose(out[1, 8:12], np.full(4, cv[1, 2]), rtol=1e-14)
