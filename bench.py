@@ -719,17 +719,27 @@ def main():
         errors["surrogate_alone_coarse_512"] = spectrum_error_stats(compare["surrogate"]["sur_alone"],
                                                                     coarse(ref_cxr))
         # The gate: the headline variant's PXR+CBS on the surrogate's grid
-        # and its bremsstrahlung on the case's grid, worst tile, against the
-        # reference arm on the same histories.
-        e_gate = max(errors["surrogate_cv"]["coarse_512"]["max_over_tiles"],
-                     errors.get("brem_mixed", {}).get("fine_2048", {}).get("max_over_tiles", 0.0))
+        # and its bremsstrahlung on the case's grid as measured, and its
+        # PXR+CBS on the case's 2048 bins at the configuration's 1e8
+        # histories (the measured fine-bin error scaled by its 1/sqrt(N)
+        # law, whose exponent the trajectory above reports), worst tile,
+        # against the reference arm on the same histories.
+        fine_proj = (errors["surrogate_cv"].get("fine_2048_by_batches", {})
+                     .get("projected_at_1e8_histories", {}).get("max_over_tiles", 0.0))
+        parts = [errors["surrogate_cv"]["coarse_512"]["max_over_tiles"],
+                 errors.get("brem_mixed", {}).get("fine_2048", {}).get("max_over_tiles", 0.0), fine_proj]
+        t = torch.tensor(parts, device="cuda", dtype=torch.float64)
         if dist is not None:
-            t = torch.tensor([e_gate], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_gate = float(t.item())
+        parts = [float(x) for x in t.cpu()]
+        e_gate = max(parts)
         sur["gate"] = {"bound": 0.01, "error": e_gate,
-                       "measured_on": "surrogate+CV PXR/CBS (512 bins) and mixed brem (2048 bins), worst tile "
-                                      "relative to the tile peak, against the %s on the same histories" % errors["reference"]}
+                       "parts": {"pxr_cbs_512_measured": parts[0], "brem_2048_measured": parts[1],
+                                 "pxr_cbs_2048_projected_1e8": parts[2]},
+                       "measured_on": "worst tile relative to the tile peak, against the %s on the same "
+                                      "histories: surrogate+CV PXR/CBS on 512 bins and mixed brem on 2048 "
+                                      "bins as measured; surrogate+CV PXR/CBS on 2048 bins projected to 1e8 "
+                                      "histories" % errors["reference"]}
         sur["passed"] = bool(e_gate <= 0.01)
 
     def rate(name):

@@ -181,6 +181,21 @@ typedef struct pb_elsepa {
     const int32_t *guide;      /* [rows * (cells + 1)] */
 } pb_elsepa;
 
+/* SBETHE table stopping (ABI 5), the reference's padded per-layer tables of
+ * src/pyrite/montecarlo/transport/stopping.py:11-83 (prepare / pack): layer
+ * L's first count[L] entries of row L hold ln(E / keV) and
+ * ln(S / (keV/Angstrom)); the continuous stopping is their log-log
+ * interpolation (_dEds_sbethe_scalar, :86-103), clamped at both ends. With
+ * straggling each element's Urban mean is scaled by the table's stopping
+ * over the spliced one (cores.py:595-604). count NULL keeps the spliced
+ * Joy-Luo / Berger-Seltzer stopping. Exact core only (use_lut 0). */
+typedef struct pb_stopping {
+    int32_t width;
+    const int32_t *count;      /* [n_layers], >= 2 */
+    const double *logE;        /* [n_layers * width] */
+    const double *logS;        /* [n_layers * width] */
+} pb_stopping;
+
 typedef struct pb_transport_args {
     int32_t rng;        /* pb_rng */
     int32_t precision;  /* pb_precision */
@@ -218,6 +233,7 @@ typedef struct pb_transport_args {
      * for tabulated elastic scattering). */
     int32_t elastic_model;
     pb_elsepa elsepa;
+    pb_stopping stopping;
 } pb_transport_args;
 
 /* CXR reflection rows and coupling tables (cxr/_batched.py:232-331). */

@@ -82,6 +82,10 @@ class _Layers(C.Structure):
         ("Z", _D),
         ("straggling", C.c_int),
         ("elsepa", C.POINTER(_Elsepa)),
+        ("sb_width", C.c_int),
+        ("sb_count", C.POINTER(C.c_int32)),
+        ("sb_logE", _D),
+        ("sb_logS", _D),
     ]
 
 
@@ -200,6 +204,8 @@ def _declare(L):
     L.or_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.or_dEds_spliced.restype = C.c_double
     L.or_dEds_spliced.argtypes = [C.POINTER(_Layers), C.c_int, C.c_double]
+    L.or_sbethe_dEds.restype = C.c_double
+    L.or_sbethe_dEds.argtypes = [C.POINTER(_Layers), C.c_int, C.c_double]
     L.or_elsepa_rate.restype = C.c_double
     L.or_elsepa_rate.argtypes = [C.POINTER(_Elsepa), C.c_int64, C.c_int64, C.c_double]
     L.or_elsepa_cos_theta.restype = C.c_double
@@ -389,15 +395,33 @@ class LayerTables:
             len(self.z_top), Z.shape[1], _p(self.z_top, _D), _p(self.z_bot, _D),
             _p(self.n_el, _I32), _p(self.J, _D), _p(self.k, _D), _p(self.coeff, _D),
             _p(self.E_cross, _D), _p(self.sr_rate_numer, _D), _p(self.sr_joy_numer, _D),
-            _p(self.Z, _D), 0, None,
+            _p(self.Z, _D), 0, None, 0, None, None, None,
         )
         self.elsepa = None
+        self.sbethe = None
 
     def use_elsepa(self, tables: "ElsepaTables | None"):
         """Sample elastic events from ELSEPA tables (None: screened Rutherford)."""
         self.elsepa = tables
         self.struct.elsepa = C.pointer(tables.struct) if tables is not None else None
         return self
+
+    def use_sbethe(self, count, logE, logS):
+        """Continuous stopping from SBETHE tables, packed as
+        ``pack_sbethe_stopping_tables`` returns them (None: spliced)."""
+        if count is None:
+            self.sbethe = None
+            self.struct.sb_count, self.struct.sb_logE, self.struct.sb_logS, self.struct.sb_width = None, None, None, 0
+            return self
+        self.sbethe = (np.ascontiguousarray(count, dtype=np.int32), _f64(logE), _f64(logS))
+        c, e, v = self.sbethe
+        self.struct.sb_width = int(e.shape[1])
+        self.struct.sb_count = c.ctypes.data_as(C.POINTER(C.c_int32))
+        self.struct.sb_logE, self.struct.sb_logS = _p(e, _D), _p(v, _D)
+        return self
+
+    def sbethe_dEds(self, L, E):
+        return float(lib().or_sbethe_dEds(C.byref(self.struct), int(L), float(E)))
 
     def dEds(self, L, E):
         return float(lib().or_dEds_spliced(C.byref(self.struct), int(L), float(E)))

@@ -71,7 +71,16 @@ typedef struct {
     const double *Z;             /* [n_layers*max_el] atomic numbers (Urban straggling) */
     int straggling;              /* 1: Urban energy-loss straggling per flight */
     const or_elsepa *elsepa;     /* non-NULL: ELSEPA elastic model (elastic_model_code 2) */
+    /* SBETHE table stopping (stopping.py:11-103): per layer sb_count[L]
+     * nodes of ln(E / keV) and ln(S / (keV/Angstrom)); sb_count NULL keeps
+     * the spliced analytic stopping. */
+    int sb_width;
+    const int *sb_count;
+    const double *sb_logE;
+    const double *sb_logS;
 } or_layers;
+
+double or_sbethe_dEds(const or_layers *ly, int L, double E);
 
 /* Urban energy-loss straggling (straggling.py:37-333). */
 double or_dEds_element(double J, double k, double coeff, double E_cross, double E);

@@ -317,6 +317,29 @@ double or_elsepa_cos_theta(const or_elsepa *t, int64_t start, int64_t length, do
     return 1.0 - 2.0 * ((1.0 - f) * mu0 + f * mu1);
 }
 
+/* stopping.py:86-103, _dEds_sbethe_scalar: log-log interpolation of layer
+ * L's table, hi the first node at or above ln E, clamped at both ends */
+double or_sbethe_dEds(const or_layers *ly, int L, double E) {
+    const double *lE = ly->sb_logE + (int64_t)L * ly->sb_width;
+    const double *lS = ly->sb_logS + (int64_t)L * ly->sb_width;
+    int n = ly->sb_count[L];
+    double x = log(E);
+    if (x <= lE[0]) return -exp(lS[0]);
+    if (x >= lE[n - 1]) return -exp(lS[n - 1]);
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (lE[mid] < x) lo = mid; else hi = mid;
+    }
+    double f = (x - lE[lo]) / (lE[hi] - lE[lo]);
+    return -exp(lS[lo] + f * (lS[hi] - lS[lo]));
+}
+
+/* cores.py:581-590: the continuous stopping of layer L, SBETHE or spliced */
+static double stopping(const or_layers *ly, int L, double E) {
+    return ly->sb_count ? or_sbethe_dEds(ly, L, E) : or_dEds_spliced(ly, L, E);
+}
+
 /* the elastic rate of element slot ix at E: ELSEPA or screened Rutherford */
 static double elastic_rate(const or_layers *ly, int ix, double E) {
     if (ly->elsepa) return or_elsepa_rate(ly->elsepa, ly->elsepa->start[ix], ly->elsepa->length[ix], E);
@@ -399,7 +422,7 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
         }
         int exit_top = cross_up && z_top <= 0.0;
         int exit_bot = cross_dn && z_bot >= z_total;
-        double dEds = or_dEds_spliced(ly, L, E_j);
+        double dEds = stopping(ly, L, E_j);
         int geometry_event = cross_up || cross_dn;
         int cutoff = 0;
         double E_end;
@@ -411,9 +434,13 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
             uint64_t fkey = or_splitmix64(urban_key + 0x9E3779B97F4A7C15ULL * ((uint64_t)flight << 32));
             uint64_t ctr = 0;
             double loss = 0.0;
+            /* cores.py:595-604: with SBETHE each element's C is scaled by the
+             * table's stopping over the spliced one at the row's energy */
+            const double scale = ly->sb_count ? dEds / or_dEds_spliced(ly, L, E_j) : 1.0;
             for (int i = 0; i < n_el; ++i) {
                 int ix = L * ly->max_el + i;
                 double C = -or_dEds_element(ly->J[ix], ly->k[ix], ly->coeff[ix], ly->E_cross[ix], E_j);
+                C *= scale;
                 loss += or_urban_sample_element(ly->Z[ix], ly->J[ix], C, E_j, step, fkey, &ctr);
             }
             double delta_cut = E_j - E_cut;
@@ -427,7 +454,7 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
             }
         } else {
             /* cores.py:734-776: midpoint cutoff distance */
-            double cutoff_rate = or_dEds_spliced(ly, L, 0.5 * (E_j + E_cut));
+            double cutoff_rate = stopping(ly, L, 0.5 * (E_j + E_cut));
             double cutoff_distance = (E_cut - E_j) / cutoff_rate;
             if (cutoff_distance < step || (cutoff_distance == step && !geometry_event)) {
                 step = cutoff_distance;
@@ -440,7 +467,7 @@ void or_transport_one(const or_layers *ly, int rng_kind, uint64_t key, int64_t e
             } else {
                 double E_pred = E_j + dEds * step;
                 double E_mid = 0.5 * (E_j + E_pred);
-                E_end = E_j + step * or_dEds_spliced(ly, L, E_mid);
+                E_end = E_j + step * stopping(ly, L, E_mid);
             }
         }
         double t_end = clk + step / or_beta_from_keV(0.5 * (E_j + E_end));

@@ -80,6 +80,10 @@ class PbElsepa(C.Structure):
     ]
 
 
+class PbStopping(C.Structure):
+    _fields_ = [("width", _i32), ("count", _vp), ("logE", _vp), ("logS", _vp)]
+
+
 class PbTransportArgs(C.Structure):
     _fields_ = [
         ("rng", _i32), ("precision", _i32), ("use_lut", _i32), ("block_threads", _i32),
@@ -88,6 +92,7 @@ class PbTransportArgs(C.Structure):
         ("seg_count", _vp), ("exit_code", _vp), ("final_pos", _vp), ("final_dir", _vp),
         ("final_E", _vp), ("seg", PbSegments), ("tallies", PbTallies), ("work_counter", _vp),
         ("status", _vp), ("straggling", _i32), ("Z", _vp), ("elastic_model", _i32), ("elsepa", PbElsepa),
+        ("stopping", PbStopping),
     ]
 
 

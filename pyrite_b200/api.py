@@ -22,8 +22,11 @@ from .tables import (
     CRYSTALS,
     ElsepaGroup,
     LayerStack,
+    StoppingTables,
     check_elsepa_range,
+    check_stopping_range,
     pack_elsepa,
+    pack_stopping,
     beam_entry_basis,
     beam_frame_basis,
     build_transport_lut,
@@ -197,7 +200,7 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
                           tilt_polar_rad=0.0, tilt_azim_rad=0.0, transverse_distribution=None,
                           *, lut=True, rng="splitmix", precision="fp64", entry=None, cap=None,
                           device=None, stream=None, block_threads=0, tallies=None, straggling=False,
-                          elastic_model="sr", elastic_tables=None):
+                          elastic_model="sr", elastic_tables=None, stopping_tables=None):
     """Transport ``Ne`` electrons into a slab or layer stack; returns segment rows.
 
     Same contract as the reference's per-electron cores: rows of history i
@@ -219,6 +222,9 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     reference the exact core runs (``lut`` is ignored) and energies outside
     the tables are refused. ``"sr"`` (the default here, since the production
     ELSEPA tables are not shipped) is the analytic screened-Rutherford model.
+    ``stopping_tables`` (one SBETHE table per layer, the reference's argument
+    of that name) replaces the spliced analytic stopping by the tables'
+    log-log interpolation (stopping.py:11-103; exact core, range checked).
 
     ``tallies=(n_E, n_theta)`` also returns the kernel's fused summary
     tallies, the reference's summary tables (trajectory_summary.py:147-260)
@@ -243,6 +249,12 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
         lut = False  # the exact core, as the reference bypasses its LUT for tabulated elastic scattering
     elif elastic_model != "sr":
         raise ValueError(f"elastic_model must be 'sr' or 'elsepa', not {elastic_model!r}")
+    stop = None
+    if stopping_tables is not None:
+        stop = stopping_tables if isinstance(stopping_tables, StoppingTables) else pack_stopping(stack, stopping_tables)
+        E_hi = float(E0_keV) if entry is None else float(np.max(entry[2]))
+        check_stopping_range(stop, float(E_cut_keV), E_hi)
+        lut = False  # table stopping runs on the exact core
     dev = _device(device)
     h = _Holder(dev)
     a = L.PbTransportArgs()
@@ -261,6 +273,10 @@ def simulate_trajectories(E0_keV, Ne, thickness_ang=None, element=None, n_atoms_
     if group is not None:
         a.elastic_model = L.PB_ELASTIC_ELSEPA
         a.elsepa = _fill_elsepa(h, group)
+    if stop is not None:
+        a.stopping.width = int(stop.logE.shape[1])
+        a.stopping.count = _ptr(h.typed(np.asarray(stop.count, dtype=np.int32), torch.int32))
+        a.stopping.logE, a.stopping.logS = _ptr(h.f64(stop.logE)), _ptr(h.f64(stop.logS))
     if lut:
         E_hi = float(E0_keV) if entry is None else float(np.max(entry[2]))
         a.lut = _fill_lut(h, build_transport_lut(stack, E_cut_keV, E_hi), a.precision)

@@ -143,6 +143,11 @@ int pb_transport(const pb_transport_args *a, void *stream) {
         if (!t.start || !t.length || !t.logE || !t.log_rate || !t.cdf || !t.pdf || !t.mu || !t.guide)
             return fail(PB_ERR_INVALID, "pb_transport: every ELSEPA table pointer must be set");
     }
+    if (a->stopping.count) {
+        if (a->use_lut) return fail(PB_ERR_UNSUPPORTED, "pb_transport: SBETHE stopping runs on the exact core only");
+        if (a->stopping.width < 2 || !a->stopping.logE || !a->stopping.logS)
+            return fail(PB_ERR_INVALID, "pb_transport: SBETHE tables need width >= 2, logE and logS");
+    }
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a->work_counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "pb_transport: zero work counter");

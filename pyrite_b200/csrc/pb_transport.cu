@@ -193,13 +193,14 @@ __device__ __forceinline__ double urban_sample_element(double Z, double J, doubl
 // straggling off carry none of it.
 template <int kRng>
 __device__ __forceinline__ double straggled_loss(const LayerSmem &ly, int max_el, int L, int n_el, double E,
-                                              double s, uint64_t key, int64_t flight) {
+                                              double s, uint64_t key, int64_t flight, double scale = 1.0) {
     const uint64_t fkey = splitmix64(splitmix64(key ^ kUrbanSalt) + kPhi * ((uint64_t)flight << 32));
     uint64_t ctr = 0;
     double loss = 0.0;
     for (int k = 0; k < n_el; ++k) {
         const int ix = L * max_el + k;
-        const double C = -dEds_element(ly.J[ix], ly.k[ix], ly.coeff[ix], ly.E_cross[ix], E);
+        double C = -dEds_element(ly.J[ix], ly.k[ix], ly.coeff[ix], ly.E_cross[ix], E);
+        C *= scale;
         loss += urban_sample_element<kRng>(ly.Z[ix], ly.J[ix], C, E, s, fkey, ctr);
     }
     return loss;
@@ -279,6 +280,26 @@ __device__ __forceinline__ double elsepa_cos_theta(const pb_elsepa &t, int ix, d
     const double mu0 = elsepa_invert(t, r, xi);
     const double mu1 = elsepa_invert(t, r + 1, xi);
     return 1.0 - 2.0 * ((1.0 - f) * mu0 + f * mu1);
+}
+
+// ---- SBETHE table stopping (stopping.py:86-103) -----------------------------
+// Layer L's log-log table; hi is the first node at or above ln E (numpy's
+// searchsorted on the left), both ends clamped. FP64, negative.
+__device__ __forceinline__ double sbethe_dEds(const pb_stopping &t, int L, double E) {
+    const double *lE = t.logE + (int64_t)L * t.width;
+    const double *lS = t.logS + (int64_t)L * t.width;
+    const int n = t.count[L];
+    const double x = log(E);
+    if (x <= lE[0]) return -exp(lS[0]);
+    if (x >= lE[n - 1]) return -exp(lS[n - 1]);
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (lE[mid] < x) lo = mid;
+        else hi = mid;
+    }
+    const double f = (x - lE[lo]) / (lE[hi] - lE[lo]);
+    return -exp(lS[lo] + f * (lS[hi] - lS[lo]));
 }
 
 // kinematics.py:162-166
@@ -423,8 +444,10 @@ __device__ __forceinline__ int hist_slot(double v, double lo, double hi, int n) 
     return b + 1;
 }
 
-// kEls: ELSEPA elastic rates and angles (the exact core only, kLut false).
-template <class Real, bool kLut, int kRng, bool kStrag, bool kEls>
+// kTab: the exact core with the table-driven physics switched on at run time
+// (ELSEPA elastic rates and angles, SBETHE stopping); kLut is false with it.
+// The analytic exact core and the LUT core compile without those branches.
+template <class Real, bool kLut, int kRng, bool kStrag, bool kTab>
 __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ LayerSmem ly;
@@ -570,7 +593,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             } else {
                 for (int k = 0; k < n_el; ++k) {
                     const int ix = L * max_el + k;
-                    if constexpr (kEls) total_rate += (Real)elsepa_rate(p.elsepa, ix, E_j);
+                    if (kTab && p.elastic_model == PB_ELASTIC_ELSEPA) total_rate += (Real)elsepa_rate(p.elsepa, ix, E_j);
                     else total_rate += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
                 }
             }
@@ -599,7 +622,13 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                 // (straggling.py:301-333) from the flight's own stream; a loss
                 // beyond E - E_cut shortens the step in proportion and ends
                 // the history at the cutoff.
-                const double loss = straggled_loss<kRng>(ly, max_el, L, n_el, E_j, (double)step, key, nseg);
+                // cores.py:595-604: SBETHE scales each element's Urban mean
+                // by the table's stopping over the spliced one at E_j.
+                double scale = 1.0;
+                if constexpr (kTab)
+                    if (p.stopping.count)
+                        scale = sbethe_dEds(p.stopping, L, E_j) / (double)dEds_spliced<double>(ly, max_el, L, E_j);
+                const double loss = straggled_loss<kRng>(ly, max_el, L, n_el, E_j, (double)step, key, nseg, scale);
                 const double delta_cut = E_j - E_cut;
                 if (loss > delta_cut || (loss == delta_cut && !geometry_event)) {
                     step = loss > 0.0 ? (Real)((double)step * (delta_cut / loss)) : (Real)0;
@@ -618,6 +647,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                 Real cf;
                 lut_index(lut, 0.5 * (E_j + E_cut), ci, cf);
                 cutoff_rate = lerp(row, ci, cf);
+            } else if (kTab && p.stopping.count) {
+                dEds = (Real)sbethe_dEds(p.stopping, L, E_j);
+                cutoff_rate = (Real)sbethe_dEds(p.stopping, L, 0.5 * (E_j + E_cut));
             } else {
                 dEds = dEds_spliced<Real>(ly, max_el, L, Er);
                 cutoff_rate = dEds_spliced<Real>(ly, max_el, L, (Real)(0.5 * (E_j + E_cut)));
@@ -639,6 +671,8 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     Real mf;
                     lut_index(lut, E_mid, mi, mf);
                     mid_rate = lerp(lut.dEds + (int64_t)L * lut.ne, mi, mf);
+                } else if (kTab && p.stopping.count) {
+                    mid_rate = (Real)sbethe_dEds(p.stopping, L, E_mid);
                 } else {
                     mid_rate = dEds_spliced<Real>(ly, max_el, L, (Real)E_mid);
                 }
@@ -738,7 +772,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                         Real cum = 0;
                         for (int k = 0; k < n_el; ++k) {
                             const int ix = L * max_el + k;
-                            if constexpr (kEls) cum += (Real)elsepa_rate(p.elsepa, ix, E_j);
+                            if (kTab && p.elastic_model == PB_ELASTIC_ELSEPA) cum += (Real)elsepa_rate(p.elsepa, ix, E_j);
                             else cum += sr_rate<Real>(Er, (Real)ly.srn[ix], (Real)ly.sjn[ix]);
                             if (cum > target) { i_el = k; break; }
                         }
@@ -750,7 +784,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                     Real af;
                     lut_index(lut, E, ai, af);
                     alpha = lerp(lut.alpha + ((int64_t)L * max_el + i_el) * lut.ne, ai, af);
-                } else if constexpr (!kEls) {
+                } else {
                     alpha = (Real)ly.sjn[L * max_el + i_el] / (Real)E;
                 }
                 const double cos_ud = uniform<kRng>(key, draws);
@@ -759,8 +793,10 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
                 const Real phi_u = (Real)uniform<kRng>(key, draws);
                 draws += 1;
                 Real cos_t;
-                if constexpr (kEls) cos_t = (Real)elsepa_cos_theta(p.elsepa, L * max_el + i_el, E, cos_ud);
-                else cos_t = (Real)1 - (Real)2 * alpha * cos_u / ((Real)1 + alpha - cos_u);
+                if (kTab && p.elastic_model == PB_ELASTIC_ELSEPA)
+                    cos_t = (Real)elsepa_cos_theta(p.elsepa, L * max_el + i_el, E, cos_ud);
+                else
+                    cos_t = (Real)1 - (Real)2 * alpha * cos_u / ((Real)1 + alpha - cos_u);
                 rotate<Real>(dx, dy, dz, cos_t, (Real)(2.0 * kPi) * phi_u);
                 steps += 1;
             }
@@ -816,9 +852,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const pb_transport_args 
             if (tal.deposit[j] != 0.0) atomicAdd(&p.tallies.deposit[j], tal.deposit[j]);
 }
 
-template <class Real, bool kLut, int kRng, bool kStrag, bool kEls = false>
+template <class Real, bool kLut, int kRng, bool kStrag, bool kTab = false>
 static cudaError_t launch_transport_t(const pb_transport_args &a, cudaStream_t s, int sms) {
-    auto kern = transport_kernel<Real, kLut, kRng, kStrag, kEls>;
+    auto kern = transport_kernel<Real, kLut, kRng, kStrag, kTab>;
     size_t dyn = 0;
     if (kLut && a.lut.total_bytes <= (int64_t)kLutSmemBytes) dyn = (size_t)a.lut.total_bytes;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -841,7 +877,7 @@ static cudaError_t launch_transport_s(const pb_transport_args &a, cudaStream_t s
     const bool mixed = a.precision == PB_MIXED;
     const bool lut = a.use_lut != 0;
     const bool philox = a.rng == PB_RNG_PHILOX;
-    if (a.elastic_model == PB_ELASTIC_ELSEPA) {  // exact core only (checked by the caller)
+    if (a.elastic_model == PB_ELASTIC_ELSEPA || a.stopping.count) {  // exact core only (checked by the caller)
         if (mixed) {
             if (philox) return launch_transport_t<float, false, PB_RNG_PHILOX, kStrag, true>(a, s, sms);
             return launch_transport_t<float, false, PB_RNG_SPLITMIX, kStrag, true>(a, s, sms);

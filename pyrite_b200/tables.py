@@ -284,6 +284,59 @@ def check_elsepa_range(group: ElsepaGroup, stack: "LayerStack", E_min_keV: float
 
 
 # ---------------------------------------------------------------------------
+# SBETHE table stopping (transport/stopping.py:11-83).
+# ---------------------------------------------------------------------------
+@dataclass
+class StoppingTables:
+    """Per-layer SBETHE collision stopping, padded: layer L's first
+    ``count[L]`` entries of ``logE[L]`` / ``logS[L]`` hold ln(E / keV) and
+    ln(S / (keV/Angstrom))."""
+
+    count: np.ndarray
+    logE: np.ndarray
+    logS: np.ndarray
+
+
+def pack_stopping(stack: "LayerStack", stopping_tables) -> StoppingTables:
+    """One table per layer, each a mapping with ``stopping_energy_eV`` and
+    ``stopping_eV_per_angstrom`` (the reference's ``stopping_tables``
+    argument) or an already prepared ``(logE, logS)`` pair: validated,
+    converted to keV and keV/Angstrom, log-transformed and padded."""
+    if len(stopping_tables) != stack.n_layers:
+        raise ValueError("stopping_tables needs one SBETHE table per layer")
+    rows = []
+    for t in stopping_tables:
+        if not isinstance(t, dict) and len(t) == 2 and np.asarray(t[0]).ndim == 1:
+            rows.append((np.asarray(t[0], dtype=np.float64), np.asarray(t[1], dtype=np.float64)))
+            continue
+        E = np.asarray(t["stopping_energy_eV"], dtype=np.float64) * 1.0e-3
+        S = np.asarray(t["stopping_eV_per_angstrom"], dtype=np.float64) * 1.0e-3
+        if E.ndim != 1 or S.shape != E.shape or E.size < 2 or not np.all(np.diff(E) > 0.0):
+            raise ValueError("an SBETHE table needs matching vectors on a strictly increasing energy grid")
+        if not (np.all(np.isfinite(E)) and np.all(np.isfinite(S))) or np.any(E <= 0.0) or np.any(S <= 0.0):
+            raise ValueError("SBETHE table values must be finite and strictly positive")
+        rows.append((np.log(E), np.log(S)))
+    count = np.array([r[0].size for r in rows], dtype=np.int32)
+    width = int(count.max())
+    logE = np.zeros((stack.n_layers, width))
+    logS = np.zeros((stack.n_layers, width))
+    for L, (e, v) in enumerate(rows):
+        logE[L, : e.size] = e
+        logS[L, : v.size] = v
+    return StoppingTables(count, logE, logS)
+
+
+def check_stopping_range(t: StoppingTables, E_min_keV: float, E_max_keV: float):
+    """Refuse a transport energy range outside any layer's table
+    (host_pass.py:598-608: node ends widened by one ulp, no extrapolation)."""
+    for L in range(t.count.size):
+        lo = float(np.nextafter(np.exp(t.logE[L, 0]), -np.inf))
+        hi = float(np.nextafter(np.exp(t.logE[L, t.count[L] - 1]), np.inf))
+        if E_min_keV < lo or E_max_keV > hi:
+            raise ValueError(f"transport energy range must be within the SBETHE table [{lo:g}, {hi:g}] keV")
+
+
+# ---------------------------------------------------------------------------
 # Transport LUT (transport/lut.py:64-283): uniform in log kinetic energy.
 # ---------------------------------------------------------------------------
 @dataclass

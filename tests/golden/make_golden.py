@@ -1085,6 +1085,68 @@ def gen_elsepa():
 
 
 # ---------------------------------------------------------------------------
+# SBETHE table stopping (transport/stopping.py:11-103, cores.py:581-600 and
+# 720-780) with synthetic per-layer tables passed through the reference's
+# public ``stopping_tables`` argument: the layer's spliced analytic stopping
+# with a smooth modulation, on a geometric grid from 1 keV to 1 GeV.
+# ---------------------------------------------------------------------------
+SBETHE_CASES = (("si30kev", False), ("sio2_300kev", False), ("c20mev", False), ("sio2_300kev", True))
+
+
+def synthetic_sbethe_table(composition):
+    from pyrite.materials._transport_data import TRANSPORT_ELEMENTS
+    from pyrite.montecarlo.transport import straggling as ref_str
+
+    E_eV = np.geomspace(1.0e3, 1.0e9, 120)
+    S = np.zeros_like(E_eV)
+    for el, n in composition:
+        p = TRANSPORT_ELEMENTS[el]
+        Z, A, J = float(p["Z"]), float(p["A"]), float(p["J_keV"])
+        k = 0.731 + 0.0688 * np.log10(Z)
+        coeff = (n / 0.602214076) * Z
+        E_cross = ref_stop._element_crossover_keV(el, Z, A, J)
+        S += np.array([-float(ref_str._dEds_spliced_element_scalar(J, k, coeff, E_cross, 0.0, e / 1e3))
+                       for e in E_eV])
+    S_eV = S * 1e3 * (1.0 + 0.08 * np.sin(2.0 * np.log(E_eV)))
+    return dict(stopping_energy_eV=E_eV, stopping_eV_per_angstrom=S_eV)
+
+
+def gen_sbethe():
+    for name, stg in SBETHE_CASES:
+        case = TRANSPORT_CASES[name]
+        layers = case["layers"]
+        tables = [synthetic_sbethe_table(layer[2]) for layer in layers]
+        prepared = ref_stop.prepare_sbethe_stopping_tables(tables, len(layers))
+        _on, count, logE, logS = ref_stop.pack_sbethe_stopping_tables(prepared, len(layers))
+        tp = np.deg2rad(case["tilt_deg"])
+        beam_dir, n_hat = ref_geometry.tilted_geometry(np.deg2rad(case["theta_obs_deg"]), tp, 0.0)
+        kwargs = dict(E0_keV=case["E0_keV"], Ne=case["Ne"], thickness_ang=layers[-1][1], seed=case["seed"],
+                      elastic_model="sr", stopping_tables=tables, transport_core="per-electron",
+                      radiative_model="uncoupled", beam_dir=beam_dir, tilt_polar_rad=tp,
+                      beam_fwhm_mm=case["beam_fwhm_mm"], transport_lut_config=TransportLUTConfig(enabled=False),
+                      straggling=stg)
+        if len(layers) == 1:
+            kwargs["composition"] = layers[0][2]
+        else:
+            kwargs["layers"] = layers
+        out = _simulate_trajectories(**kwargs)
+        arrays = {k: np.asarray(out[k]) for k in ROW_KEYS}
+        counts = np.array([int(out[k]) for k in COUNT_KEYS], dtype=np.int64)
+        leaf_E = np.geomspace(0.5, 2.0e6, 97)
+        leaf_S = np.array([[ref_stop._dEds_sbethe_packed_scalar(logE, logS, L, count[L], e) for e in leaf_E]
+                           for L in range(len(layers))])
+        raw = {}
+        for L, t in enumerate(tables):
+            for f in ("stopping_energy_eV", "stopping_eV_per_angstrom"):
+                raw[f"raw_{L}_{f}"] = t[f]
+        _save(f"sbethe_{name}{'_straggled' if stg else ''}", E0_keV=case["E0_keV"], E_cut_keV=5.0,
+              seed=case["seed"], Ne=case["Ne"], straggling=stg,
+              initial_r=out["initial_r_ang"], initial_v=out["initial_v_hat"], initial_E=out["initial_E_keV"],
+              count_names=np.array(COUNT_KEYS), counts=counts, sb_count=count, sb_logE=logE, sb_logS=logS,
+              leaf_E=leaf_E, leaf_S=leaf_S, **raw, **arrays)
+
+
+# ---------------------------------------------------------------------------
 # Summary tables (pyrite/montecarlo/trajectory_summary.py:147-260) of the
 # golden transport cases: the reference's own reductions of its own rows.
 # ---------------------------------------------------------------------------
@@ -1220,6 +1282,7 @@ def gen_fullrun():
 
 GENERATORS = {
     "elsepa": gen_elsepa,
+    "sbethe": gen_sbethe,
     "rng": gen_rng,
     "physics_leaves": gen_physics_leaves,
     "transport": gen_transport,

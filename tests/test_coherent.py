@@ -458,10 +458,17 @@ def test_gpu_coherent_matches_reference(name):
 def test_gpu_coherent_records_and_route_match_reference(name):
     """The device record prologue (``pb_coherent_records``) from the fixture's
     segments (with start ages) and line tables: the reference's per-row line
-    records -- the same pairs kept in the same order (equal row counts), every
-    field within 1e-10 -- and the whole device route, segments -> records ->
-    reduction, the reference's coherent spectrum within the reduction's
-    tolerance (2e-5 of the peak, 1e-4 relative above 1e-3 of it)."""
+    records -- the same pairs kept in the same order, every field within
+    1e-10 -- and the whole device route, segments -> records -> reduction,
+    the reference's coherent spectrum within the reduction's tolerance (2e-5
+    of the peak, 1e-4 relative above 1e-3 of it).
+
+    One exception is allowed and checked: a pair whose escape optical depth
+    puts its formation coefficient apb = exp(-tau_s/2) + exp(-tau_e/2) at the
+    last subnormal (the reference keeps apb = 5e-324 when glibc's exp rounds
+    up to it, CUDA's exp may round to 0 and drop the pair). Such a record
+    adds nothing to any field; records with apb below 1e-300 are compared
+    as absent."""
     from pyrite_b200 import LineTables
     from pyrite_b200.coherent import coherent_records, coherent_route_spectrum
     from pyrite_b200.tables import ReflectionRows
@@ -477,9 +484,15 @@ def test_gpu_coherent_records_and_route_match_reference(name):
     rows = ReflectionRows(c["G"], c["ES"][None], c["EP"][None], c["WM"], c["row_table"])
     rec, cnt = coherent_records(seg, c["E_grid"], tables=tables, rows=rows, n_hat=c["n_hat"])
     z = np.load(GOLDEN / f"coherent_{name}.npz")
-    assert np.array_equal(cnt, z["row_count"])
+    got_rec = {f: rec[f].cpu().numpy() for f in oc.FIELDS}
+    live_got, live_ref = got_rec["apb"] > 1e-300, z["apb"] > 1e-300
+    row_got = np.repeat(np.arange(cnt.size), cnt)
+    row_ref = np.repeat(np.arange(z["row_count"].size), z["row_count"])
+    assert np.array_equal(np.bincount(row_got[live_got], minlength=cnt.size),
+                          np.bincount(row_ref[live_ref], minlength=cnt.size))
+    assert abs(int(cnt.sum()) - int(z["row_count"].sum())) <= int((~live_ref).sum()) + int((~live_got).sum())
     for f in oc.FIELDS:
-        np.testing.assert_allclose(rec[f].cpu().numpy(), z[f], rtol=1e-10, atol=1e-300, err_msg=f)
+        np.testing.assert_allclose(got_rec[f][live_got], z[f][live_ref], rtol=1e-10, atol=1e-300, err_msg=f)
     got = coherent_route_spectrum(seg, z["E_grid"], z["delta_omega"], tables=tables, rows=rows, n_hat=c["n_hat"])
     _assert_close(got, z["spec"])
 
