@@ -485,6 +485,11 @@ def main():
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
     ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--surrogate-form", default="pairwise", choices=["pairwise", "tiles"],
+                    help="pairwise: the direction is an input and every (segment, tile) pair runs the network; "
+                         "tiles: one head per detector tile on shared segment features (one pass per segment)")
+    ap.add_argument("--tile-segments", type=int, default=262144, help="training segments of the tiles form")
+    ap.add_argument("--tile-epochs", type=int, default=40, help="training epochs of the tiles form")
     ap.add_argument("--train-domain", default="case", choices=["case", "uniform"],
                     help="surrogate training segments: the case's transport, or spread over the whole input "
                          "domain (5-100 MeV, +-5 mrad, every depth; adds a 1e5-segment held-out audit)")
@@ -617,13 +622,21 @@ def main():
         t0 = time.perf_counter()
         # Data-parallel on N > 1 GPUs: each rank builds 1/N of the segments of
         # the training set (its own seed) and the gradients are averaged.
-        n_seg_rank = max(1024, args.train_segments // world)
         pg = dist.group.WORLD if dist is not None else None
-        data = S.make_training_set(spec, n_seg=n_seg_rank, n_dir=args.train_dirs,
-                                   dir_chunk=max(1, 2 ** 20 // n_seg_rank), seed=1000 + rank, device="cuda",
-                                   process_group=pg, domain=args.train_domain)
-        model = S.Surrogate("cuda", seed=0)
-        losses = model.train(data, epochs=args.train_epochs, lr=2e-3, lr_final=2e-5, process_group=pg)
+        if args.surrogate_form == "tiles":
+            n_seg_rank = max(8192, args.tile_segments // world)
+            data = S.make_tile_training_set(spec, n_seg=n_seg_rank, seed=1000 + rank, device="cuda",
+                                            process_group=pg)
+            model = S.Surrogate("cuda", seed=0, n_tiles=int(data["n_tiles"]))
+            epochs = args.tile_epochs
+        else:
+            n_seg_rank = max(1024, args.train_segments // world)
+            data = S.make_training_set(spec, n_seg=n_seg_rank, n_dir=args.train_dirs,
+                                       dir_chunk=max(1, 2 ** 20 // n_seg_rank), seed=1000 + rank, device="cuda",
+                                       process_group=pg, domain=args.train_domain)
+            model = S.Surrogate("cuda", seed=0)
+            epochs = args.train_epochs
+        losses = model.train(data, epochs=epochs, lr=2e-3, lr_final=2e-5, process_group=pg)
         n_pairs = int(data["X"].shape[0]) * world
         n_dropped = int(data.get("nonfinite_pairs_dropped", 0))
         del data
@@ -634,12 +647,16 @@ def main():
         compare_pass("surrogate", cs)
         gate_report = compare["surrogate"]["report"]
         arm("surrogate", cs, args.steps)
-        sur = {"model": "MLP 6 -> 4x256 SiLU -> 512 bins, bf16 weights and activations, FP32 accumulate (tcgen05)",
-               "train_s": train_s, "train_pairs": n_pairs, "epochs": args.train_epochs,
+        form = ("MLP 6 -> 4x256 SiLU -> 512 bins per (segment, tile) pair" if model.n_tiles == 1 else
+                "MLP 4 segment features -> 4x256 SiLU -> %d tile heads x 512 bins (one pass per segment)"
+                % model.n_tiles)
+        sur = {"model": form + ", bf16 weights and activations, FP32 accumulate (tcgen05)",
+               "form": args.surrogate_form,
+               "train_s": train_s, "train_pairs": n_pairs, "epochs": epochs,
                "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
                "diverged_epochs_redone": int(model.retries), "nonfinite_pairs_dropped": n_dropped,
                "train_domain": args.train_domain, "exact_stride": args.exact_stride,
-               "coarse_bins": int(model.n_out),
+               "coarse_bins": int(model.n_bins),
                "error_estimate": {"what": "the product path's own per-tile estimate after its probe batches "
                                           "(3 standard errors of the control-variate correction, worst bin, "
                                           "relative to the tile peak), the tiles moved to the exact scorer, and "
@@ -789,22 +806,30 @@ def main():
     }
     if sur is not None:
         t_sample, t_inf = cases["surrogate"].t_split
-        inf_pairs = n_seg * n_dir * (1.0 + 1.0 / max(args.exact_stride, 1))
+        tiles_form = sur["form"] == "tiles"
+        # network rows per step: every (segment, tile) pair, or every segment once (tiles form)
+        inf_pairs = n_seg * (1 if tiles_form else n_dir) * (1.0 + 1.0 / max(args.exact_stride, 1))
         inf_tflops = inf_pairs * ALG_FLOPS_INFER / (t_inf / 1e3) / 1e12
         rooflines["mlp_infer_kernel"] = {
-            "bound": "tensor", "kernel": "mlp_infer_kernel (tcgen05 BF16, 4 hidden layers per segment x tile)",
+            "bound": "tensor",
+            "kernel": "mlp_infer_kernel (tcgen05 BF16, 4 hidden layers per %s)"
+                      % ("segment; tile heads at readout" if tiles_form else "segment x tile"),
             "achieved": inf_tflops, "peak": MEASURED_BF16_SUSTAINED, "unit": "TFLOP/s",
             "frac": inf_tflops / MEASURED_BF16_SUSTAINED,
             "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
-            "traffic": DRAM_BYTES_PER_HISTORY["mlp_infer_kernel"] * H}
+            "traffic": None if tiles_form else DRAM_BYTES_PER_HISTORY["mlp_infer_kernel"] * H}
         sur["kernel_ms"] = {"transport": results["surrogate"]["t_tr"], "exact_subsample": t_sample,
                             "surrogate_infer": t_inf, "brem": results["surrogate"]["t_brem"]}
         sur["value"], sur["ms_per_step"] = rate("surrogate")
         # Training is outside the timed step: its cost spread over a C2-size
         # run of 1e8 histories.
         sur["amortised_rate_1e8_histories_with_training"] = 1e8 / (1e8 / sur["value"] + train_s)
-    dominant = max(("brem_kernel", r_head["t_brem"]), ("cxr_kernel" if head == "mixed" else "mlp_infer_kernel",
-                   r_head["t_cxr"] if head == "mixed" else cases["surrogate"].t_split[1]), key=lambda kv: kv[1])[0]
+    if head == "mixed":
+        cands = [("brem_kernel", r_head["t_brem"]), ("cxr_kernel", r_head["t_cxr"])]
+    else:
+        t_sample, t_inf = cases["surrogate"].t_split
+        cands = [("brem_kernel", r_head["t_brem"]), ("mlp_infer_kernel", t_inf), ("cxr_kernel", t_sample)]
+    dominant = max(cands, key=lambda kv: kv[1])[0]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

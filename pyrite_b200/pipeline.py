@@ -382,18 +382,29 @@ class ScoringCase:
             raise ValueError("the surrogate needs the case's detector tiling")
         if len(self.cargs_all) != 1 or self.layered:
             raise ValueError("the surrogate covers a single-crystal slab; a stack scores its layers exactly")
-        n_out = models[0].n_out
-        if self.n_E % n_out != 0:
+        n_bins = models[0].n_bins
+        if self.n_E % n_bins != 0:
             raise ValueError("the case's bins must split evenly into the surrogate's coarse bins")
+        tiles = {int(m.n_tiles) for m in models}
+        if len(tiles) != 1 or {m.n_bins for m in models} != {n_bins}:
+            raise ValueError("an ensemble needs one form and one coarse grid")
+        self.sur_factored = tiles.pop() > 1
+        if self.sur_factored and models[0].n_tiles != self.n_dir:
+            raise ValueError("a tile-factored surrogate needs one head per direction of the case")
         self.surrogates = list(models)
         self.sur_stride = int(exact_stride)
         dev, h = self.device, self.h
-        self.sur_uv = torch.as_tensor(tile_uv(self.spec.detector, self.spec.angular_shape), dtype=torch.float32,
-                                      device=dev)
+        if self.sur_factored:
+            # one feature direction: the tile heads are applied at readout
+            self.sur_uv = torch.zeros(1, 2, dtype=torch.float32, device=dev)
+        else:
+            self.sur_uv = torch.as_tensor(tile_uv(self.spec.detector, self.spec.angular_shape),
+                                          dtype=torch.float32, device=dev)
+        n_feat_dir = int(self.sur_uv.shape[0])
 
         def infer_set(seg, cap, count):
-            hs = [torch.zeros(self.n_dir, 256, device=dev, dtype=torch.float64) for _ in self.surrogates]
-            ls = [torch.zeros(self.n_dir, device=dev, dtype=torch.float64) for _ in self.surrogates]
+            hs = [torch.zeros(n_feat_dir, 256, device=dev, dtype=torch.float64) for _ in self.surrogates]
+            ls = [torch.zeros(n_feat_dir, device=dev, dtype=torch.float64) for _ in self.surrogates]
             args = [m.infer_args(self.spec, seg, cap, self.sur_uv, a, b, n_seg_device=count, status=self.status)
                     for m, a, b in zip(self.surrogates, hs, ls)]
             return hs, ls, args
@@ -424,7 +435,7 @@ class ScoringCase:
             cs.spec = _ptr(self.spec_sample)
             self.cargs_s = cs
             self.sur_hsum_s, self.sur_lsum_s, self.sur_args_s = infer_set(self.smp, cap_s, self.smp["count"])
-        n_out = self.surrogates[0].n_out
+        n_out = self.surrogates[0].n_bins
         self.sur_tol = float(tol)
         self.sur_probe = max(2, int(probe_batches))
         self.sur_checked = False
@@ -437,18 +448,22 @@ class ScoringCase:
         self._run_batches = []
 
     def _head(self, hsums, lsums):
-        out = torch.zeros(self.n_dir, self.surrogates[0].n_out, device=self.device, dtype=torch.float64)
+        """The surrogate spectrum [n_dir, n_bins] from the summed last-layer
+        activations: per direction (pairwise form), or every tile's head on
+        the one shared sum (tile-factored form)."""
+        n_feat_dir = int(self.sur_uv.shape[0])
+        out = torch.zeros(n_feat_dir, self.surrogates[0].n_out, device=self.device, dtype=torch.float64)
         k = len(self.surrogates)
         for m, hs, ls in zip(self.surrogates, hsums, lsums):
-            L.check(self.lib.pb_mlp_head(self.n_dir, m.n_out, m.W5r.data_ptr(), m.p["b5"].data_ptr(),
+            L.check(self.lib.pb_mlp_head(n_feat_dir, m.n_out, m.W5r.data_ptr(), m.p["b5"].data_ptr(),
                                          hs.data_ptr(), ls.data_ptr(), float(m.t_scale) / k, out.data_ptr(),
                                          torch.cuda.current_stream().cuda_stream), "pb_mlp_head")
-        return out
+        return out.view(self.n_dir, self.surrogates[0].n_bins)
 
     def coarse(self, spec_fine):
-        """Mean of each run of n_E / n_out fine bins: the surrogate's coarse bins."""
-        n_out = self.surrogates[0].n_out
-        return spec_fine.view(spec_fine.shape[0], n_out, -1).mean(-1)
+        """Mean of each run of n_E / n_bins fine bins: the surrogate's coarse bins."""
+        n_bins = self.surrogates[0].n_bins
+        return spec_fine.view(spec_fine.shape[0], n_bins, -1).mean(-1)
 
     def surrogate_spectrum(self):
         """Surrogate (+ exact control variate) spectrum [n_dir, n_coarse] so far,
@@ -538,7 +553,7 @@ class ScoringCase:
         error falls as 1 / sqrt(histories). (Shaping each coarse total by the
         sub-sample's own fine proportions instead was measured no better: the
         proportions carry the same sampling noise.)"""
-        rep = self.n_E // self.surrogates[0].n_out
+        rep = self.n_E // self.surrogates[0].n_bins
         s = self._head(self.sur_hsum, self.sur_lsum).repeat_interleave(rep, dim=1)
         if self.sur_stride > 0:
             s += self.sur_stride * (self.spec_sample

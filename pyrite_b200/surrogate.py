@@ -79,9 +79,16 @@ def _beam_axes(spec):
 class Surrogate:
     """Parameters, optimiser state and the packed weight copies of the MLP."""
 
-    def __init__(self, device, n_out=512, seed=0):
+    def __init__(self, device, n_out=512, seed=0, n_tiles=1):
+        """``n_out`` coarse bins per output spectrum. ``n_tiles`` > 1 builds
+        the tile-factored form: the hidden layers see the segment alone (the
+        direction features are zero) and the output layer holds one linear
+        head of ``n_out`` bins per detector tile, so a segment's hidden
+        activations are computed once for all tiles."""
         self.device = torch.device(device)
-        self.n_out = int(n_out)
+        self.n_tiles = int(n_tiles)
+        self.n_bins = int(n_out)
+        self.n_out = self.n_bins * self.n_tiles
         shapes = [("W1", (HIDDEN, K_IN)), ("b1", (HIDDEN,)), ("W2", (HIDDEN, HIDDEN)), ("b2", (HIDDEN,)),
                   ("W3", (HIDDEN, HIDDEN)), ("b3", (HIDDEN,)), ("W4", (HIDDEN, HIDDEN)), ("b4", (HIDDEN,)),
                   ("W5", (self.n_out, HIDDEN)), ("b5", (self.n_out,))]
@@ -496,6 +503,64 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
         Lrow = Lrow[perm].contiguous()
     return {"X": X, "Xt": X.t().contiguous(), "T": T, "L": Lrow, "t_scale": t_scale, "grid": grid,
             "n_seg": n_seg, "n_dir": n_dir, "nonfinite_pairs_dropped": n_bad}
+
+
+def make_tile_training_set(spec, *, n_seg=65536, n_hist=None, seg_chunk=4096, seed=101, device=None, grid=None,
+                           log=None, shuffle=True, process_group=None):
+    """Training rows of the tile-factored surrogate: one row per segment of the
+    case's own transport, its features without a direction (the tile
+    features are zero), its targets the exact coarse spectra per unit length
+    towards every one of the case's directions ``spec.n_hats``, concatenated
+    tile after tile: T [n_seg, n_tiles * n_bins]. Returns the same dict as
+    ``make_training_set`` (``n_dir`` = 1 feature direction, ``n_tiles``)."""
+    device = torch.device(device or "cuda")
+    grid = grid or CoarseGrid.of(spec.E_grid)
+    n_hats = np.atleast_2d(np.asarray(spec.n_hats, dtype=float))
+    n_tiles = n_hats.shape[0]
+    n_hist = n_hist or max(4096, n_seg // 8)
+    all_seg, _n_all = transported_segments(spec, n_hist, seed, device)
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    cand = torch.nonzero(all_seg["L"] > 0.0).flatten().cpu()
+    pick = cand[torch.randperm(cand.numel(), generator=gen)[:n_seg]].to(device)
+    seg = {k: v[pick].contiguous() for k, v in all_seg.items()}
+    n_seg = int(pick.numel())
+    X = torch.empty(n_seg, K_IN, device=device, dtype=torch.bfloat16)
+    T = torch.empty(n_seg, n_tiles * grid.n_bins, device=device, dtype=torch.bfloat16)
+    t_scale = None
+    for s0 in range(0, n_seg, seg_chunk):
+        ns = min(seg_chunk, n_seg - s0)
+        sub = {k: v[s0:s0 + ns] for k, v in seg.items()}
+        lines, n_lines = _cxr_lines(spec, sub, ns, n_hats, device)
+        tgt = torch.zeros(n_tiles * ns, grid.n_bins, device=device, dtype=torch.float32)
+        _bin(lines, n_lines, 0, n_tiles, ns, grid, tgt)
+        tgt = tgt.view(n_tiles, ns, grid.n_bins).permute(1, 0, 2).reshape(ns, n_tiles * grid.n_bins)
+        tgt.mul_((1.0 / sub["L"]).to(torch.float32)[:, None])
+        if t_scale is None:
+            ms = tgt.square().mean().double().reshape(1)
+            if process_group is not None:
+                import torch.distributed as dist
+
+                dist.all_reduce(ms, group=process_group)
+                ms /= dist.get_world_size(process_group)
+            t_scale = float(ms.sqrt().item()) or 1.0
+        T[s0:s0 + ns] = (tgt / t_scale).to(torch.bfloat16)
+        del lines, tgt
+        if log and (s0 // seg_chunk) % 8 == 0:
+            log(f"tile targets: {s0 + ns}/{n_seg} segments")
+    a = _feature_args(spec, seg, n_seg, torch.zeros(1, 2, dtype=torch.float32, device=device))
+    L.check(L.load().pb_mlp_features(C.byref(a), X.data_ptr(), None, _stream()), "pb_mlp_features")
+    Lrow = seg["L"].to(torch.float32)
+    good = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
+    n_bad = int((~good).sum().item())
+    if n_bad:
+        keep = torch.nonzero(good).flatten()
+        X, T, Lrow = X[keep], T[keep], Lrow[keep]
+        n_seg = int(keep.numel())
+    if shuffle:
+        perm = torch.randperm(n_seg, generator=gen).to(device)
+        X, T, Lrow = X[perm].contiguous(), T[perm].contiguous(), Lrow[perm].contiguous()
+    return {"X": X, "Xt": X.t().contiguous(), "T": T, "L": Lrow, "t_scale": t_scale, "grid": grid,
+            "n_seg": n_seg, "n_dir": 1, "n_tiles": n_tiles, "nonfinite_pairs_dropped": n_bad}
 
 
 def _feature_args(spec, seg, n_seg, dir_uv_t):

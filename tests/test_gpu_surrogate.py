@@ -327,3 +327,60 @@ def test_error_gate_keeps_a_trained_surrogate(cuda_device):
     assert 0.5 <= np.median(ratio) <= 2.0 and np.all((ratio > 0.25) & (ratio < 4.0)), (actual, est)
     audit = np.array(rep["audit_surrogate_alone_per_tile"])
     assert np.all((audit > 0) & (audit < 1)), audit
+
+
+def test_tile_factored_form_heads_and_gradients(cuda_device):
+    """The tile-factored surrogate (one 512-bin head per tile on shared
+    segment features): one inference pass over the segments (direction
+    features zero) and every tile's head on the one activation sum equals
+    the torch forward of the same bf16 model per tile; its training step's
+    output-layer gradient (N = tiles x 512) matches autograd."""
+    from pyrite_b200.surrogate import HIDDEN, Surrogate
+
+    n_tiles = 4
+    model = Surrogate(cuda_device, seed=11, n_tiles=n_tiles)
+    assert model.n_out == n_tiles * 512 and model.n_bins == 512
+    with torch.no_grad():
+        for k in ("b1", "b2", "b3", "b4", "b5"):
+            model.p[k].normal_(0.0, 0.1)
+    model.repack()
+    n = 1000
+    seg = _segments(n, cuda_device, seed=2)
+    uv = torch.zeros(1, 2, device=cuda_device)
+    hsum = torch.zeros(1, HIDDEN, device=cuda_device, dtype=torch.float64)
+    lsum = torch.zeros(1, device=cuda_device, dtype=torch.float64)
+    status = torch.zeros(1, device=cuda_device, dtype=torch.int32)
+    spec = torch.zeros(1, model.n_out, device=cuda_device, dtype=torch.float64)
+    a = model.infer_args(_Spec, seg, n, uv, hsum, lsum, status=status)
+    model.score(a, spec, hsum, lsum)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    ref_h = _torch_forward_hsum(model, _torch_features(seg, uv, _Spec)[0], seg["L"].float())
+    assert float((hsum[0].float() - ref_h).abs().max()) <= 3e-2 * float(ref_h.abs().max())
+    tiles = spec.view(n_tiles, 512).float()
+    for t in range(n_tiles):
+        W = model.W5r[t * 512:(t + 1) * 512]
+        head = W @ hsum[0].float() + model.p["b5"][t * 512:(t + 1) * 512] * float(lsum[0])
+        assert torch.allclose(tiles[t], head, rtol=1e-4, atol=1e-4 * float(head.abs().max()))
+    # one training step: the output layer's gradient against autograd
+    B = 1024
+    g = torch.Generator(device=cuda_device).manual_seed(13)
+    X = torch.zeros(B, 16, device=cuda_device)
+    X[:, :4] = torch.rand(B, 4, device=cuda_device, generator=g) * 2 - 1
+    Xb = X.to(torch.bfloat16)
+    T = (0.5 * torch.randn(B, model.n_out, device=cuda_device, generator=g)).to(torch.bfloat16)
+    ws = model._workspace(B)
+    P = {k: v.clone().requires_grad_(True) for k, v in model.p.items()}
+    model.train_step(Xb, Xb.t().contiguous(), T, ws, lr=0.0)
+    torch.cuda.synchronize()
+    assert int(ws["status"].item()) == 0
+    h = Xb.float()
+    for Wn, bn in (("W1", "b1"), ("W2", "b2"), ("W3", "b3"), ("W4", "b4")):
+        h = torch.nn.functional.silu(h @ P[Wn].to(torch.bfloat16).float().t() + P[bn])
+        h = h.to(torch.bfloat16).float()
+    Y = h @ P["W5"].to(torch.bfloat16).float().t() + P["b5"]
+    loss = ((Y - T.float()) ** 2).mean()
+    loss.backward()
+    gW5 = model.g["W5"]
+    rel = float((gW5 - P["W5"].grad).norm() / P["W5"].grad.norm())
+    assert rel < 2e-2, rel
