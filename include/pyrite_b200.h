@@ -470,6 +470,31 @@ int pb_char_yields(const pb_char_args *args, void *stream);
 int pb_char_spectrum(int32_t n_dir, int32_t n_line, int32_t n_E, const double *line_yield,
                      const double *profiles, double *spec, void *stream);
 
+/* One whole pass of the hot path (ABI 5): zero the segment stream's count,
+ * transport histories [transport.e_start, transport.e_start + transport.n)
+ * into it, then score the stream with every CXR, bremsstrahlung and
+ * characteristic argument set in order, all on ``stream`` -- the C form of
+ * the reference's transport pass followed by its emission adapters
+ * (montecarlo/transport/batching.py:547-554, then
+ * montecarlo/runner/emission_adapters.py:53-112 per emission), which a
+ * binding calls once per batch. The scorer sets read the segments through
+ * their own pointers (normally transport.seg's arrays, with n_seg_device at
+ * transport.seg.count). Every set is checked as its own entry point checks
+ * it before anything is launched, so an argument error enqueues nothing; a
+ * launch error part way returns with the earlier launches enqueued. */
+typedef struct pb_transport_score_args {
+    pb_transport_args transport;  /* transport.seg must be set */
+    int32_t n_cxr;
+    int32_t n_brem;
+    int32_t n_char;
+    int32_t pad_;
+    const pb_cxr_args *cxr;       /* [n_cxr], host array */
+    const pb_brem_args *brem;     /* [n_brem] */
+    const pb_char_args *chars;    /* [n_char] */
+} pb_transport_score_args;
+
+int pb_transport_score(const pb_transport_score_args *args, void *stream);
+
 /* Surrogate training: GEMM + fused epilogue (above). */
 int pb_mlp_gemm(const pb_mlp_gemm_args *args, void *stream);
 /* dY = g_scale (Y - t_scale T) (bf16, row-major [rows][cols] and transposed

@@ -180,6 +180,13 @@ class PbCoherentRecordsArgs(C.Structure):
     ]
 
 
+class PbTransportScoreArgs(C.Structure):
+    _fields_ = [
+        ("transport", PbTransportArgs), ("n_cxr", _i32), ("n_brem", _i32), ("n_char", _i32), ("pad_", _i32),
+        ("cxr", C.POINTER(PbCxrArgs)), ("brem", C.POINTER(PbBremArgs)), ("chars", C.POINTER(PbCharArgs)),
+    ]
+
+
 class PbDecoherenceArgs(C.Structure):
     _fields_ = [
         ("n_row", _i32), ("n_pop", _i32), ("n_E", _i32), ("pad_", _i32), ("G", _vp), ("A_pop", _vp),
@@ -219,6 +226,7 @@ EXPORTS = (
     "pb_coherent_records_work_size",
     "pb_coherent_records",
     "pb_decoherence_factor",
+    "pb_transport_score",
     "pb_coherent_blend_work_size",
     "pb_coherent_blend",
 )
@@ -275,6 +283,7 @@ def load(path: Path | None = None):
     lib.pb_coherent_records_work_size.argtypes = [_i64, _i32, C.POINTER(_u64)]
     lib.pb_coherent_records.argtypes = [C.POINTER(PbCoherentRecordsArgs), _vp]
     lib.pb_decoherence_factor.argtypes = [C.POINTER(PbDecoherenceArgs), _vp]
+    lib.pb_transport_score.argtypes = [C.POINTER(PbTransportScoreArgs), _vp]
     lib.pb_coherent_blend_work_size.argtypes = [_i32, _i64, _i32, C.POINTER(_u64)]
     lib.pb_coherent_blend.argtypes = [C.POINTER(PbCoherentBlendArgs), _vp]
     if path is None:

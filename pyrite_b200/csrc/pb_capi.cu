@@ -95,7 +95,8 @@ int pb_device_count(int *count) {
     return PB_OK;
 }
 
-int pb_transport(const pb_transport_args *a, void *stream) {
+// Argument checks of pb_transport (no CUDA call); n == 0 passes.
+static int check_transport(const pb_transport_args *a) {
     if (!a) return fail(PB_ERR_INVALID, "pb_transport: args is NULL");
     if (a->n < 0) return fail(PB_ERR_INVALID, "pb_transport: n = %lld < 0", (long long)a->n);
     if (a->n == 0) return PB_OK;
@@ -148,12 +149,21 @@ int pb_transport(const pb_transport_args *a, void *stream) {
         if (a->stopping.width < 2 || !a->stopping.logE || !a->stopping.logS)
             return fail(PB_ERR_INVALID, "pb_transport: SBETHE tables need width >= 2, logE and logS");
     }
-    cudaStream_t s = (cudaStream_t)stream;
+    return PB_OK;
+}
+
+static int run_transport(const pb_transport_args *a, cudaStream_t s) {
+    if (a->n == 0) return PB_OK;
     cudaError_t e = cudaMemsetAsync(a->work_counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_fail(e, "pb_transport: zero work counter");
     e = pb::launch_transport(*a, s, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_transport: launch");
     return PB_OK;
+}
+
+int pb_transport(const pb_transport_args *a, void *stream) {
+    const int v = check_transport(a);
+    return v != PB_OK ? v : run_transport(a, (cudaStream_t)stream);
 }
 
 int pb_cxr_score(const pb_cxr_args *a, void *stream) {
@@ -165,7 +175,7 @@ int pb_cxr_score(const pb_cxr_args *a, void *stream) {
     return PB_OK;
 }
 
-int pb_brem_score(const pb_brem_args *a, void *stream) {
+static int check_brem(const pb_brem_args *a) {
     if (!a) return fail(PB_ERR_INVALID, "pb_brem_score: args is NULL");
     if (a->n_seg < 0 || a->n_dir < 1 || a->n_E < 1)
         return fail(PB_ERR_INVALID, "pb_brem_score: need n_seg >= 0, n_dir >= 1, n_E >= 1");
@@ -178,12 +188,22 @@ int pb_brem_score(const pb_brem_args *a, void *stream) {
     if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->Z ||
         !a->n_ang3 || !a->E_grid || (!a->mu && a->n_layer == 0) || !a->spec)
         return fail(PB_ERR_INVALID, "pb_brem_score: every pointer must be set");
-    cudaError_t e = pb::launch_brem(*a, (cudaStream_t)stream, device_sms());
+    return PB_OK;
+}
+
+static int run_brem(const pb_brem_args *a, cudaStream_t s) {
+    if (a->n_seg == 0) return PB_OK;
+    cudaError_t e = pb::launch_brem(*a, s, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_brem_score: launch");
     return PB_OK;
 }
 
-int pb_char_yields(const pb_char_args *a, void *stream) {
+int pb_brem_score(const pb_brem_args *a, void *stream) {
+    const int v = check_brem(a);
+    return v != PB_OK ? v : run_brem(a, (cudaStream_t)stream);
+}
+
+static int check_char(const pb_char_args *a) {
     if (!a) return fail(PB_ERR_INVALID, "pb_char_yields: args is NULL");
     if (a->n_seg < 0 || a->n_dir < 1 || a->n_line < 1 || a->n_shell < 1)
         return fail(PB_ERR_INVALID, "pb_char_yields: need n_seg >= 0, n_dir >= 1, n_line >= 1, n_shell >= 1");
@@ -201,8 +221,47 @@ int pb_char_yields(const pb_char_args *a, void *stream) {
         return fail(PB_ERR_INVALID, "pb_char_yields: layer bounds missing");
     if (a->n_layer == 0 && !(a->thickness > 0.0))
         return fail(PB_ERR_INVALID, "pb_char_yields: single slab needs thickness > 0");
-    cudaError_t e = pb::launch_char(*a, (cudaStream_t)stream, device_sms());
+    return PB_OK;
+}
+
+static int run_char(const pb_char_args *a, cudaStream_t s) {
+    if (a->n_seg == 0) return PB_OK;
+    cudaError_t e = pb::launch_char(*a, s, device_sms());
     if (e != cudaSuccess) return cuda_fail(e, "pb_char_yields: launch");
+    return PB_OK;
+}
+
+int pb_char_yields(const pb_char_args *a, void *stream) {
+    const int v = check_char(a);
+    return v != PB_OK ? v : run_char(a, (cudaStream_t)stream);
+}
+
+int pb_transport_score(const pb_transport_score_args *p, void *stream) {
+    if (!p) return fail(PB_ERR_INVALID, "pb_transport_score: args is NULL");
+    if (p->n_cxr < 0 || p->n_brem < 0 || p->n_char < 0 || (p->n_cxr && !p->cxr) || (p->n_brem && !p->brem) ||
+        (p->n_char && !p->chars))
+        return fail(PB_ERR_INVALID, "pb_transport_score: scorer counts and arrays disagree");
+    if (!p->transport.seg.L || !p->transport.seg.count)
+        return fail(PB_ERR_INVALID, "pb_transport_score: the transport needs its segment stream");
+    // every check before any launch
+    int v = check_transport(&p->transport);
+    for (int i = 0; v == PB_OK && i < p->n_cxr; ++i) v = pb::validate_cxr(p->cxr[i], "pb_transport_score (cxr)", false);
+    for (int i = 0; v == PB_OK && i < p->n_brem; ++i) v = check_brem(&p->brem[i]);
+    for (int i = 0; v == PB_OK && i < p->n_char; ++i) v = check_char(&p->chars[i]);
+    if (v != PB_OK) return v;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(p->transport.seg.count, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_transport_score: zero the segment count");
+    if ((v = run_transport(&p->transport, s)) != PB_OK) return v;
+    for (int i = 0; i < p->n_cxr; ++i) {
+        if (p->cxr[i].n_seg == 0) continue;
+        e = pb::launch_cxr(p->cxr[i], s, device_sms());
+        if (e != cudaSuccess) return cuda_fail(e, "pb_transport_score: cxr launch");
+    }
+    for (int i = 0; i < p->n_brem; ++i)
+        if ((v = run_brem(&p->brem[i], s)) != PB_OK) return v;
+    for (int i = 0; i < p->n_char; ++i)
+        if ((v = run_char(&p->chars[i], s)) != PB_OK) return v;
     return PB_OK;
 }
 

@@ -567,9 +567,21 @@ class ScoringCase:
         if n > self.batch:
             raise ValueError("batch larger than the case's segment buffer was sized for")
         s = (stream or torch.cuda.current_stream()).cuda_stream
-        self.seg_count.zero_()
         a = self.targs
         a.e_start, a.n = int(e_start), int(n)
+        if events is None and not getattr(self, "surrogates", None):
+            # the whole exact pass in one C call: transport, then every scorer
+            p = L.PbTransportScoreArgs()
+            p.transport = a
+            p.n_cxr, p.n_brem, p.n_char = len(self.cargs_all), len(self.bargs_all), len(self.chargs_all)
+            keep = ((L.PbCxrArgs * max(p.n_cxr, 1))(*self.cargs_all), (L.PbBremArgs * max(p.n_brem, 1))(*self.bargs_all),
+                    (L.PbCharArgs * max(p.n_char, 1))(*self.chargs_all))
+            p.cxr, p.brem, p.chars = (C.cast(k, C.POINTER(t)) for k, t in
+                                      zip(keep, (L.PbCxrArgs, L.PbBremArgs, L.PbCharArgs)))
+            L.check(self.lib.pb_transport_score(C.byref(p), s), "pb_transport_score")
+            self.histories += int(n)
+            return
+        self.seg_count.zero_()
         if events is not None:
             events[0].record()
         L.check(self.lib.pb_transport(C.byref(a), s), "pb_transport")

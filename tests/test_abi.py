@@ -35,7 +35,8 @@ STRUCTS = {
     "pb_segments": L.PbSegments, "pb_tallies": L.PbTallies, "pb_transport_args": L.PbTransportArgs,
     "pb_cxr_tables": L.PbCxrTables, "pb_cxr_args": L.PbCxrArgs, "pb_brem_args": L.PbBremArgs,
     "pb_coherent_args": L.PbCoherentArgs, "pb_coherent_records_args": L.PbCoherentRecordsArgs,
-    "pb_decoherence_args": L.PbDecoherenceArgs, "pb_elsepa": L.PbElsepa, "pb_stopping": L.PbStopping, "pb_coherent_blend_args": L.PbCoherentBlendArgs,
+    "pb_decoherence_args": L.PbDecoherenceArgs, "pb_elsepa": L.PbElsepa, "pb_stopping": L.PbStopping,
+    "pb_transport_score_args": L.PbTransportScoreArgs, "pb_coherent_blend_args": L.PbCoherentBlendArgs,
 }
 
 
