@@ -570,6 +570,8 @@ typedef struct pb_coherent_records_args {
     void *work;                /* pb_coherent_records_work_size bytes, 256-byte aligned */
     uint64_t work_bytes;
     unsigned int *status;      /* device status word, OR-ed (NULL: not reported) */
+    int64_t *elec_out;         /* ABI 5, optional [capacity]: each record's electron (the
+                                  segment's elec_id), for the decoherence blend */
 } pb_coherent_records_args;
 
 int pb_coherent_records_work_size(int64_t n_seg, int32_t n_g, uint64_t *bytes);
@@ -678,6 +680,31 @@ typedef struct pb_coherent_blend_args {
 
 int pb_coherent_blend_work_size(int32_t n_row, int64_t n_line, int32_t n_E, uint64_t *bytes);
 int pb_coherent_blend(const pb_coherent_blend_args *args, void *stream);
+
+/* Streamed coherent reduction (ABI 5), the reference's field-plane route
+ * (src/pyrite/montecarlo/spectrum/coherent_stream_jit_kernel.py): a row's
+ * complex field must be summed over every segment before it is squared, so
+ * block after block of records (pb_coherent_records of one segment block)
+ * is folded into persistent FP64 field planes fields[n_row][4][n_E]
+ * (sigma re, sigma im, pi re, pi im), and with elec_id the per-electron
+ * squared fields into power[n_row][n_E] (a block must then end on an
+ * electron boundary). pb_coherent_finalize squares and weights them:
+ *   spec[k] += scale * sum_r row_weight[r] (F[r,k] |field_r(E_k)|^2
+ *                                           + (1 - F[r,k]) power_r(E_k)),
+ * F = 1 (no power needed) when F_row is NULL. base.spec is unused by the
+ * accumulation; base.work is pb_coherent_blend_work_size bytes with elec_id,
+ * pb_coherent_work_size bytes without. Each cell has one writer per launch:
+ * no atomics, results independent of the launch. */
+typedef struct pb_coherent_stream_args {
+    pb_coherent_args base;
+    const int64_t *elec_id;  /* optional [n_line] */
+    double *fields;          /* [n_row * 4 * n_E], accumulated */
+    double *power;           /* [n_row * n_E], accumulated when elec_id is set */
+} pb_coherent_stream_args;
+
+int pb_coherent_accumulate(const pb_coherent_stream_args *args, void *stream);
+int pb_coherent_finalize(int32_t n_row, int32_t n_E, const double *row_weight, const double *fields,
+                         const double *power, const double *F_row, double scale, double *spec, void *stream);
 
 #ifdef __cplusplus
 }

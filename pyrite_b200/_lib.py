@@ -176,7 +176,7 @@ class PbCoherentRecordsArgs(C.Structure):
         ("cxr", PbCxrArgs), ("t_start", _vp), ("capacity", _i64), ("E_vac", _vp), ("a_vac", _vp),
         ("phase_slope", _vp), ("g_phase", _vp), ("cs_re", _vp), ("cs_im", _vp), ("cp_re", _vp), ("cp_im", _vp),
         ("L_esc", _vp), ("half_dL", _vp), ("apb", _vp), ("bma", _vp), ("q", _vp), ("row_off", _vp),
-        ("work", _vp), ("work_bytes", _u64), ("status", _vp),
+        ("work", _vp), ("work_bytes", _u64), ("status", _vp), ("elec_out", _vp),
     ]
 
 
@@ -185,6 +185,10 @@ class PbTransportScoreArgs(C.Structure):
         ("transport", PbTransportArgs), ("n_cxr", _i32), ("n_brem", _i32), ("n_char", _i32), ("pad_", _i32),
         ("cxr", C.POINTER(PbCxrArgs)), ("brem", C.POINTER(PbBremArgs)), ("chars", C.POINTER(PbCharArgs)),
     ]
+
+
+class PbCoherentStreamArgs(C.Structure):
+    _fields_ = [("base", PbCoherentArgs), ("elec_id", _vp), ("fields", _vp), ("power", _vp)]
 
 
 class PbDecoherenceArgs(C.Structure):
@@ -227,6 +231,8 @@ EXPORTS = (
     "pb_coherent_records",
     "pb_decoherence_factor",
     "pb_transport_score",
+    "pb_coherent_accumulate",
+    "pb_coherent_finalize",
     "pb_coherent_blend_work_size",
     "pb_coherent_blend",
 )
@@ -284,6 +290,8 @@ def load(path: Path | None = None):
     lib.pb_coherent_records.argtypes = [C.POINTER(PbCoherentRecordsArgs), _vp]
     lib.pb_decoherence_factor.argtypes = [C.POINTER(PbDecoherenceArgs), _vp]
     lib.pb_transport_score.argtypes = [C.POINTER(PbTransportScoreArgs), _vp]
+    lib.pb_coherent_accumulate.argtypes = [C.POINTER(PbCoherentStreamArgs), _vp]
+    lib.pb_coherent_finalize.argtypes = [_i32, _i32, _vp, _vp, _vp, _vp, _f64, _vp, _vp]
     lib.pb_coherent_blend_work_size.argtypes = [_i32, _i64, _i32, C.POINTER(_u64)]
     lib.pb_coherent_blend.argtypes = [C.POINTER(PbCoherentBlendArgs), _vp]
     if path is None:

@@ -126,7 +126,7 @@ def coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, *, s
     return spec
 
 
-def coherent_records(segments, E_grid_eV, *, tables, rows, n_hat, device=None, stream=None):
+def coherent_records(segments, E_grid_eV, *, tables, rows, n_hat, device=None, stream=None, with_electrons=False):
     """The coherent route's per-row line records of one detector direction,
     built on the device from ``segments`` (the reference's segment dict with
     ``thickness_ang``, ``Ne`` and optional ``t_ang`` start ages) by
@@ -134,7 +134,8 @@ def coherent_records(segments, E_grid_eV, *, tables, rows, n_hat, device=None, s
     ``RECORD_FIELDS`` to FP64 device tensors laid out row after row (each row
     its kept pairs in segment order), ``row_count`` a numpy array. ``rows``:
     ``tables.ReflectionRows`` with one direction; ``tables``: ``LineTables``;
-    ``E_grid_eV`` sets the keep window as the incoherent scorer's."""
+    ``E_grid_eV`` sets the keep window as the incoherent scorer's.
+    ``with_electrons`` adds ``records["elec_id"]``, each record's electron."""
     from .api import _fill_tables, _ptr, _segments_on_device
     from .tables import line_keep_window
 
@@ -168,6 +169,9 @@ def coherent_records(segments, E_grid_eV, *, tables, rows, n_hat, device=None, s
     rec = {k: torch.empty(cap, dtype=torch.float64, device=dev) for k in RECORD_FIELDS}
     for k in RECORD_FIELDS:
         setattr(a, k, rec[k].data_ptr())
+    if with_electrons:
+        rec["elec_id"] = torch.empty(cap, dtype=torch.int64, device=dev)
+        a.elec_out = rec["elec_id"].data_ptr()
     row_off = h.zeros(n_g + 1, torch.int64)
     a.row_off = row_off.data_ptr()
     nbytes = C.c_uint64()
@@ -204,6 +208,75 @@ def coherent_spectrum(records, row_count, row_weight, E_grid_eV, delta_omega, Ne
         raise ValueError("Ne must be >= 1")
     spec = coherent_reduce(records, row_count, row_weight, E_grid_eV, delta_omega, scale=1.0 / Ne,
                            sinc_cutoff=sinc_cutoff, device=device)
+    return spec.cpu().numpy()
+
+
+def coherent_route_spectrum_streamed(segments, E_grid_eV, delta_omega, *, tables, rows, n_hat,
+                                    block_segments=1 << 16, sinc_cutoff=None, decoherence=None,
+                                    device=None) -> np.ndarray:
+    """The coherent route over segment blocks, as the reference's streamed
+    field-plane route does (``coherent_stream_jit_kernel.py``): each block's
+    records (``coherent_records``) are folded into persistent FP64 field
+    planes per row (``pb_coherent_accumulate``), which are squared and
+    weighted once at the end (``pb_coherent_finalize``), so memory holds one
+    block's records, not the whole run's. Blocks end on electron boundaries
+    (the segments must be in electron order). ``decoherence`` =
+    ``dict(A_pop=, xy0_pop=, omega=)`` applies the sampled-bunch blend with
+    the rows' factors, the per-electron fields accumulated beside the flat
+    ones. Per electron, as ``coherent_route_spectrum``."""
+    dev = _device(device)
+    lib = L.load()
+    h = _Holder(dev)
+    eid = np.asarray(segments["elec_id"]).reshape(-1)
+    n = int(eid.size)
+    if np.any(np.diff(eid) < 0):
+        raise ValueError("the streamed route needs the segments in electron order")
+    starts = [0]
+    while starts[-1] < n:
+        b = min(starts[-1] + int(block_segments), n)
+        while 0 < b < n and eid[b] == eid[b - 1]:
+            b += 1
+        starts.append(b)
+    E = h.f64(E_grid_eV)
+    dom = h.f64(delta_omega)
+    n_E, n_row = int(E.numel()), int(np.asarray(rows.G).reshape(-1, 3).shape[0])
+    w = h.f64(np.asarray(rows.WM, dtype=float).reshape(-1))
+    fields = h.zeros((n_row * 4 * n_E,), torch.float64)
+    power = h.zeros((n_row * n_E,), torch.float64) if decoherence is not None else None
+    arrays = {k: v for k, v in segments.items() if k not in ("Ne", "thickness_ang")}
+    for s0, s1 in zip(starts[:-1], starts[1:]):
+        sub = {k: np.asarray(v)[s0:s1] for k, v in arrays.items()}
+        sub["Ne"], sub["thickness_ang"] = segments["Ne"], segments["thickness_ang"]
+        rec, cnt = coherent_records(sub, E_grid_eV, tables=tables, rows=rows, n_hat=n_hat, device=dev,
+                                    with_electrons=decoherence is not None)
+        n_line = int(cnt.sum())
+        if n_line == 0:
+            continue
+        a = L.PbCoherentStreamArgs()
+        b = a.base
+        b.n_row, b.n_E, b.n_line = n_row, n_E, n_line
+        row_off = h.typed(np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64), torch.int64)
+        b.row_off, b.row_weight, b.E, b.delta_omega = (t.data_ptr() for t in (row_off, w, E, dom))
+        for k in RECORD_FIELDS:
+            setattr(b, k, rec[k].data_ptr())
+        b.scale = 1.0
+        b.sinc_cutoff = 0.0 if sinc_cutoff is None else float(sinc_cutoff)
+        work, nbytes = _work(h, n_row, n_line, n_E, decoherence is not None)
+        b.work, b.work_bytes = work.data_ptr(), nbytes
+        a.base = b
+        a.fields = fields.data_ptr()
+        if decoherence is not None:
+            a.elec_id, a.power = rec["elec_id"].data_ptr(), power.data_ptr()
+        L.check(lib.pb_coherent_accumulate(C.byref(a), _stream_ptr(None)), "pb_coherent_accumulate")
+    F = None
+    if decoherence is not None:
+        F = decoherence_factor(rows.G, decoherence["A_pop"], decoherence["xy0_pop"], decoherence["omega"],
+                               device=dev)
+    spec = h.zeros((n_E,), torch.float64)
+    L.check(lib.pb_coherent_finalize(n_row, n_E, w.data_ptr(), fields.data_ptr(),
+                                     power.data_ptr() if power is not None else None,
+                                     F.data_ptr() if F is not None else None, 1.0 / int(segments["Ne"]),
+                                     spec.data_ptr(), _stream_ptr(None)), "pb_coherent_finalize")
     return spec.cpu().numpy()
 
 

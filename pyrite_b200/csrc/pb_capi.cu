@@ -518,6 +518,37 @@ int pb_coherent_blend(const pb_coherent_blend_args *b, void *stream) {
     return PB_OK;
 }
 
+int pb_coherent_accumulate(const pb_coherent_stream_args *b, void *stream) {
+    if (!b) return fail(PB_ERR_INVALID, "pb_coherent_accumulate: args is NULL");
+    const pb_coherent_args *a = &b->base;
+    if (!coherent_sizes_ok(a->n_row, a->n_line, a->n_E))
+        return fail(PB_ERR_INVALID, "pb_coherent_accumulate: need 1 <= n_row, n_E <= 2^24 and 0 <= n_line <= 2^40");
+    const uint64_t need = b->elec_id ? pb::coherent_blend_work_bytes(a->n_row, a->n_line, a->n_E)
+                                     : pb::coherent_work_bytes(a->n_row, a->n_line, a->n_E);
+    pb_coherent_args chk = *a;
+    double dummy_spec = 0.0;
+    if (!chk.spec) chk.spec = &dummy_spec;  // the accumulation writes no spectrum
+    const int rc = coherent_check(&chk, "pb_coherent_accumulate", need);
+    if (rc != PB_OK) return rc;
+    if (!b->fields || (b->elec_id && !b->power))
+        return fail(PB_ERR_INVALID, "pb_coherent_accumulate: fields (and power with elec_id) must be set");
+    if (a->n_line == 0) return PB_OK;
+    cudaError_t e = pb::launch_coherent_accumulate(*b, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_accumulate: launch");
+    return PB_OK;
+}
+
+int pb_coherent_finalize(int32_t n_row, int32_t n_E, const double *row_weight, const double *fields,
+                         const double *power, const double *F_row, double scale, double *spec, void *stream) {
+    if (n_row < 1 || n_E < 1 || n_E > (1 << 24) || !row_weight || !fields || !spec || (F_row && !power))
+        return fail(PB_ERR_INVALID, "pb_coherent_finalize: need n_row, n_E >= 1, row_weight, fields, spec "
+                                    "(and power with F_row)");
+    cudaError_t e = pb::launch_coherent_stream_finalize(n_row, n_E, row_weight, fields, power, F_row, scale, spec,
+                                                        (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pb_coherent_finalize: launch");
+    return PB_OK;
+}
+
 int pb_decoherence_factor(const pb_decoherence_args *a, void *stream) {
     if (!a) return fail(PB_ERR_INVALID, "pb_decoherence_factor: args is NULL");
     if (a->n_row < 1 || a->n_row > 65535 || a->n_pop < 1 || a->n_E < 1 || a->n_E > (1 << 24))

@@ -426,6 +426,52 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     spec[e] += scale * total;
 }
 
+// Streamed route: fold this call's item partials into the persistent FP64
+// field planes of every row (and the per-electron power planes), one thread
+// per (row, energy), items in order -- one writer per cell, no atomics.
+__global__ void coh_fold_kernel(int n_row, int n_E, const int64_t *__restrict__ item_off,
+                                const float *__restrict__ partial, const float *__restrict__ power,
+                                double *__restrict__ fields, double *__restrict__ pw_planes) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_E) return;
+    for (int r = blockIdx.y; r < n_row; r += gridDim.y) {  // grid.y <= 65535 rows at a time
+        const int64_t i0 = item_off[r], i1 = item_off[r + 1];
+        if (i1 <= i0) continue;
+        double f[4] = {0.0, 0.0, 0.0, 0.0}, g = 0.0;
+        for (int64_t i = i0; i < i1; ++i) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) f[c] += (double)partial[((size_t)i * 4 + c) * n_E + e];
+            if (power) g += (double)power[(size_t)i * n_E + e];
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) fields[((size_t)r * 4 + c) * n_E + e] += f[c];
+        if (power) pw_planes[(size_t)r * n_E + e] += g;
+    }
+}
+
+// spec[e] += scale sum_r w_r (F |field|^2 + (1 - F) power), F = 1 without
+// row factors; rows in order.
+__global__ void coh_stream_finalize_kernel(int n_row, int n_E, const double *__restrict__ w_row,
+                                           const double *__restrict__ fields, const double *__restrict__ pw_planes,
+                                           const double *__restrict__ F_row, double scale,
+                                           double *__restrict__ spec) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_E) return;
+    double total = 0.0;
+    for (int r = 0; r < n_row; ++r) {
+        const double *f = fields + (size_t)r * 4 * n_E + e;
+        const double flat = f[0] * f[0] + f[(size_t)n_E] * f[(size_t)n_E] + f[2 * (size_t)n_E] * f[2 * (size_t)n_E] +
+                            f[3 * (size_t)n_E] * f[3 * (size_t)n_E];
+        if (F_row) {
+            const double F = F_row[(size_t)r * n_E + e];
+            total += w_row[r] * (F * flat + (1.0 - F) * pw_planes[(size_t)r * n_E + e]);
+        } else {
+            total += w_row[r] * flat;
+        }
+    }
+    spec[e] += scale * total;
+}
+
 // F_r(e) = |(1/N) sum_p exp(i (omega_e A_p - g_r,perp . xy0_p))|^2
 // (cxr/_per_hkl.py:121-160, cxr/_setup.py:745-760), FP64 throughout: one
 // thread per (row, energy), the population staged in shared memory.
@@ -489,7 +535,7 @@ int64_t coherent_items(int n_row, int64_t n_line, int n_E) {
 }
 
 cudaError_t launch_coherent_impl(const pb_coherent_args &p, const int64_t *elec, const double *F_row,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, double *fields = nullptr, double *pw_planes = nullptr) {
     const int64_t K = chunk_lines(p.n_line, p.n_E);
     const int64_t n_item_max = max_items(p.n_row, p.n_line, K);
     auto *item_off = static_cast<int64_t *>(p.work);
@@ -528,7 +574,14 @@ cudaError_t launch_coherent_impl(const pb_coherent_args &p, const int64_t *elec,
     a.status = p.status;
     dim3 grid((unsigned)n_item_max, (unsigned)n_etiles(p.n_E));
     const unsigned fin_blocks = (unsigned)((p.n_E + kFinalizeThreads - 1) / kFinalizeThreads);
-    if (elec) {
+    if (fields) {  // streamed: fold into the persistent planes, no squaring yet
+        if (elec) coh_field_kernel<true><<<grid, kThreads, 0, s>>>(a);
+        else coh_field_kernel<false><<<grid, kThreads, 0, s>>>(a);
+        dim3 fgrid((unsigned)((p.n_E + kFinalizeThreads - 1) / kFinalizeThreads),
+                   (unsigned)(p.n_row < 65535 ? p.n_row : 65535));
+        coh_fold_kernel<<<fgrid, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, partial, elec ? a.power : nullptr,
+                                                           fields, pw_planes);
+    } else if (elec) {
         coh_field_kernel<true><<<grid, kThreads, 0, s>>>(a);
         coh_finalize_blend_kernel<<<fin_blocks, kFinalizeThreads, 0, s>>>(p.n_row, p.n_E, item_off, p.row_weight,
                                                                           F_row, partial, a.power, p.scale, p.spec);
@@ -546,6 +599,18 @@ cudaError_t launch_coherent(const pb_coherent_args &p, cudaStream_t s) {
 
 cudaError_t launch_coherent_blend(const pb_coherent_blend_args &p, cudaStream_t s) {
     return launch_coherent_impl(p.base, p.elec_id, p.F_row, s);
+}
+
+cudaError_t launch_coherent_accumulate(const pb_coherent_stream_args &p, cudaStream_t s) {
+    return launch_coherent_impl(p.base, p.elec_id, nullptr, s, p.fields, p.power);
+}
+
+cudaError_t launch_coherent_stream_finalize(int n_row, int n_E, const double *w_row, const double *fields,
+                                            const double *power, const double *F_row, double scale, double *spec,
+                                            cudaStream_t s) {
+    coh_stream_finalize_kernel<<<(unsigned)((n_E + kFinalizeThreads - 1) / kFinalizeThreads), kFinalizeThreads, 0,
+                                 s>>>(n_row, n_E, w_row, fields, power, F_row, scale, spec);
+    return cudaGetLastError();
 }
 
 }  // namespace pb

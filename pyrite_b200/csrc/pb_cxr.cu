@@ -1812,6 +1812,7 @@ __global__ void coh_rec_write_kernel(const pb_coherent_records_args r, const uin
         }
 #pragma unroll
         for (int k = 0; k < 13; ++k) out[k][slot] = rec.f[k];
+        if (r.elec_out) r.elec_out[slot] = a.elec_id[s];
     }
 }
 

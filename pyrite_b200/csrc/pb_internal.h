@@ -50,6 +50,10 @@ cudaError_t launch_coherent(const pb_coherent_args &a, cudaStream_t s);
 uint64_t coherent_blend_work_bytes(int n_row, int64_t n_line, int n_E);
 cudaError_t launch_coherent_blend(const pb_coherent_blend_args &a, cudaStream_t s);
 cudaError_t launch_decoherence(const pb_decoherence_args &a, cudaStream_t s);
+cudaError_t launch_coherent_accumulate(const pb_coherent_stream_args &a, cudaStream_t s);
+cudaError_t launch_coherent_stream_finalize(int n_row, int n_E, const double *w_row, const double *fields,
+                                            const double *power, const double *F_row, double scale, double *spec,
+                                            cudaStream_t s);
 
 uint64_t coherent_records_work_bytes(int64_t n_seg, int n_g);
 cudaError_t launch_coherent_records(const pb_coherent_records_args &r, cudaStream_t s, int sms);

@@ -491,7 +491,10 @@ def make_training_set(spec, *, n_seg=8192, n_dir=2048, dir_chunk=64, n_hist=None
     good = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
     n_bad = int((~good).sum().item())
     if n_bad:
+        # (a multiple of 64 rows keeps the transposed features' row stride
+        # a multiple of 8, as the GEMMs want)
         keep = torch.nonzero(good).flatten()
+        keep = keep[: keep.numel() // 64 * 64]
         X, T, Lrow = X[keep], T[keep], Lrow[keep]
         N = int(keep.numel())
         if log:
@@ -552,8 +555,11 @@ def make_tile_training_set(spec, *, n_seg=65536, n_hist=None, seg_chunk=4096, se
     Lrow = seg["L"].to(torch.float32)
     good = torch.isfinite(T).all(dim=1) & torch.isfinite(X).all(dim=1)
     n_bad = int((~good).sum().item())
-    if n_bad:
-        keep = torch.nonzero(good).flatten()
+    # the GEMMs want the transposed features' row stride a multiple of 8:
+    # keep a multiple of 64 rows
+    keep = torch.nonzero(good).flatten()
+    keep = keep[: keep.numel() // 64 * 64]
+    if int(keep.numel()) != n_seg:
         X, T, Lrow = X[keep], T[keep], Lrow[keep]
         n_seg = int(keep.numel())
     if shuffle:

@@ -36,7 +36,7 @@ STRUCTS = {
     "pb_cxr_tables": L.PbCxrTables, "pb_cxr_args": L.PbCxrArgs, "pb_brem_args": L.PbBremArgs,
     "pb_coherent_args": L.PbCoherentArgs, "pb_coherent_records_args": L.PbCoherentRecordsArgs,
     "pb_decoherence_args": L.PbDecoherenceArgs, "pb_elsepa": L.PbElsepa, "pb_stopping": L.PbStopping,
-    "pb_transport_score_args": L.PbTransportScoreArgs, "pb_coherent_blend_args": L.PbCoherentBlendArgs,
+    "pb_transport_score_args": L.PbTransportScoreArgs, "pb_coherent_stream_args": L.PbCoherentStreamArgs, "pb_coherent_blend_args": L.PbCoherentBlendArgs,
 }
 
 
