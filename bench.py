@@ -485,7 +485,7 @@ def main():
     ap.add_argument("--train-segments", type=int, default=16384)
     ap.add_argument("--train-dirs", type=int, default=512)
     ap.add_argument("--train-epochs", type=int, default=6)
-    ap.add_argument("--surrogate-form", default="pairwise", choices=["pairwise", "tiles"],
+    ap.add_argument("--surrogate-form", default="tiles", choices=["pairwise", "tiles"],
                     help="pairwise: the direction is an input and every (segment, tile) pair runs the network; "
                          "tiles: one head per detector tile on shared segment features (one pass per segment)")
     ap.add_argument("--tile-segments", type=int, default=262144, help="training segments of the tiles form")

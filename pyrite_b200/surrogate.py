@@ -1,14 +1,20 @@
 """BF16 MLP surrogate of the per-segment PXR+CBS spectrum, trained and run on tcgen05.
 
-Model: 6 inputs -> 4 hidden layers of 256 SiLU units -> 512 linear outputs,
+Model: 6 inputs -> 4 hidden layers of 256 SiLU units -> linear outputs,
 bf16 weights and activations, FP32 accumulation (``pb_mlp_*`` kernels). The
-inputs of a (segment, detector direction) pair are the kernel's feature map
-(``pb_mlp_infer_args``): log energy, the two transverse angles of the
-segment direction, depth, and the direction's detector coordinates. The
-output is the segment's line spectrum per unit path length on a coarse
-uniform grid of 512 bins spanning the case's bins (each coarse bin = 4 fine
-bins of the 2048-bin grid), in units of the exact scorer's spectrum times
-``t_scale``.
+inputs are the kernel's feature map (``pb_mlp_infer_args``): log energy, the
+two transverse angles of the segment direction, depth, and a direction's
+detector coordinates. The outputs are the segment's line spectrum per unit
+path length on a coarse uniform grid of 512 bins spanning the case's bins
+(each coarse bin = 4 fine bins of the 2048-bin grid), in units of the exact
+scorer's spectrum times ``t_scale``. Two forms:
+
+- pairwise (``Surrogate()``): one (segment, direction) pair per row, 512
+  outputs; any direction of the detector plane;
+- tile-factored (``Surrogate(n_tiles=T)``): the direction inputs are zero
+  and the output layer holds one 512-bin head per tile of the case
+  (T x 512 outputs); the network then runs once per segment and the heads
+  apply to the one summed activation (``make_tile_training_set``).
 
 Training pairs come from the exact FP64 reflection sum (``pb_cxr_score``
 with its line buffer, ``pb_cxr_bin_lines``): segments of the case's own
