@@ -344,6 +344,46 @@ __device__ __forceinline__ F2 lg2_2(F2 a) { float l, h; f2_unpack(a.v, l, h); re
 
 constexpr int kBremPackedThreads = 256;  // x 2 energies
 
+// The packed form's cross section per element without the segment factor
+// n L Z^2 den_i and the photon factor c0 ln2 / k:
+//   J_el(T) = (beta_i / p_i^2) log2((p_i + p_f)^2 / dpp) / beta_f / (1 - exp(-z / beta_f)),
+// for both energies at electron energy T (p_i, bp = beta_i / p_i^2 of T
+// given); the Elwert reciprocal from its relativistic series where
+// 1/beta_f - 1 < 0.01 in both lanes, else the SFU form. Tf must be > 0.
+// With kSum the elements are summed at once, weighted by w (the segment's
+// n L Z^2 den_i), into J[0].
+template <int NEL, bool kSum = false>
+__device__ __forceinline__ void brem_J2(F2 Tf, float T, float p_i, float bp, F2 kc, F2 c2mk, float mc2, float inv_mc2,
+                                        const float (&zl)[NEL], const float (&zn)[NEL], const float (&G0)[NEL],
+                                        const float (&rh)[NEL], F2 (&J)[NEL], const float *w = nullptr) {
+    const F2 q = Tf * (Tf + f2s(2.0f * mc2));
+    const F2 rs = rsqrt_2(q);
+    const F2 p_f = (q * rs) * f2s(inv_mc2);
+    const F2 sp = f2s(p_i) + p_f;
+    const F2 dpp = kc * (f2s(2.0f * T) + c2mk);
+    const F2 lg = lg2_2((sp * sp) * rcp_2(dpp));
+    const F2 inv_bf = fma2(Tf, f2s(inv_mc2), f2s(1.0f)) * (rs * f2s(mc2));
+    const F2 base = f2s(bp) * (lg * inv_bf);
+    const F2 del = inv_bf + f2s(-1.0f);
+    const bool rel = f2lo(del) < 0.01f && f2hi(del) < 0.01f;
+#pragma unroll
+    for (int el = 0; el < NEL; ++el) {
+        F2 ginv;
+        if (rel) {
+            const F2 sz = del * f2s(zn[el]);
+            const float r = rh[el], r2 = r * r;
+            const F2 poly = fma2(sz, fma2(sz, fma2(sz, f2s(-(r / 6.0f + r2 + r2 * r)), f2s(0.5f * r + r2)),
+                                          f2s(-r)), f2s(1.0f));
+            ginv = poly * f2s(G0[el]);
+        } else {
+            ginv = rcp_2(f2s(1.0f) + neg2(ex2_2(neg2(inv_bf * f2s(zl[el])))));
+        }
+        if constexpr (kSum) J[0] = fma2(f2s(w[el]) * base, ginv, el == 0 ? f2s(0.0f) : J[0]);
+        else J[el] = base * ginv;
+    }
+}
+
+
 // Whether the launch's directions take the packed moment kernel: one exit
 // face and relative spread rho = Delta / f_min <= 0.01 (the same test both
 // brem kernels make, so exactly one of them scores the launch).
@@ -367,6 +407,7 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
     __shared__ BremSeg<float> segs[kBremChunk];
     __shared__ double sQ[8][kBremPackedThreads];  // FP64 moment sums: [energy half * 4 + n][thread]
+    __shared__ float sT[2][kBremPackedThreads / 32];  // the chunk's electron energy range, per warp
     const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
     double f_c_d, dl_d;
     if (a.precision != PB_MIXED || !brem_packed_applies(a, d0, nd, f_c_d, dl_d)) return;
@@ -419,44 +460,114 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     for (int64_t c0s = s_begin; c0s < s_end; c0s += kBremChunk) {
         const int nc = (int)((s_end - c0s) < kBremChunk ? (s_end - c0s) : kBremChunk);
         __syncthreads();
-        for (int j = threadIdx.x; j < nc; j += blockDim.x) brem_stage<float>(segs[j], a, c0s + j, T_slab, mc2, za);
+        float tlo = 3.4e38f, thi = -3.4e38f;
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            brem_stage<float>(segs[j], a, c0s + j, T_slab, mc2, za);
+            tlo = fminf(tlo, segs[j].T);
+            thi = fmaxf(thi, segs[j].T);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            tlo = fminf(tlo, __shfl_xor_sync(0xffffffffu, tlo, o));
+            thi = fmaxf(thi, __shfl_xor_sync(0xffffffffu, thi, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            sT[0][threadIdx.x >> 5] = tlo;
+            sT[1][threadIdx.x >> 5] = thi;
+        }
         __syncthreads();
         if (!on_a) continue;
+        tlo = sT[0][0];
+        thi = sT[1][0];
+#pragma unroll
+        for (int w = 1; w < kBremPackedThreads / 32; ++w) {
+            tlo = fminf(tlo, sT[0][w]);
+            thi = fmaxf(thi, sT[1][w]);
+        }
+        // The chunk's electrons span [tlo, thi]. Where that range is narrow
+        // (at most 10 % of tlo) and clear of the spectrum's tip, J_el(T) of
+        // this thread's two energies is the cubic through four Chebyshev
+        // nodes of the range, accepted only if it matches J at both ends and
+        // the middle to 1e-6: the pair loop then costs a cubic per element
+        // instead of five SFU operations.
+        // Chebyshev nodes cos((2j + 1) pi / 8)
+        constexpr float kCheb4[4] = {0.92387953251128676f, 0.38268343236508977f, -0.38268343236508977f,
+                                     -0.92387953251128676f};
+        const float t_c = 0.5f * (tlo + thi), t_h = 0.5f * (thi - tlo);
+        // (single-element targets: more elements would spill the coefficients)
+        bool cub = NEL == 1 && t_h <= 0.05f * tlo && tlo - fmaxf(f2lo(k2), f2hi(k2)) > 0.01f * tlo;
+        F2 A0[NEL], A1[NEL], A2[NEL], A3[NEL];
+        if (NEL == 1 && cub) {
+            F2 fj[4][NEL];
+#pragma unroll
+            for (int jn = 0; jn < 4; ++jn) {
+                const float T = fmaf(t_h, kCheb4[jn], t_c);
+                const float p_i = sqrtf(T * (T + 2.0f * mc2)) * inv_mc2;
+                const float bi = p_i / (1.0f + T * inv_mc2);
+                brem_J2<NEL>(f2s(T) + neg2(k2), T, p_i, bi / (p_i * p_i), kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh,
+                             fj[jn]);
+            }
+#pragma unroll
+            for (int el = 0; el < NEL; ++el) {
+                // Chebyshev coefficients c_m = (2 / 4) sum_j f_j T_m(x_j), c_0 halved,
+                // then the monomial form in u: a0 = c0 - c2, a1 = c1 - 3 c3, a2 = 2 c2, a3 = 4 c3.
+                F2 c[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    F2 acc = f2s(0.0f);
+#pragma unroll
+                    for (int jn = 0; jn < 4; ++jn) {
+                        const float x = kCheb4[jn];
+                        const float Tm = m == 0 ? 1.0f : m == 1 ? x : m == 2 ? 2.0f * x * x - 1.0f : x * (4.0f * x * x - 3.0f);
+                        acc = fma2(fj[jn][el], f2s(Tm), acc);
+                    }
+                    c[m] = acc * f2s(m == 0 ? 0.25f : 0.5f);
+                }
+                A0[el] = c[0] + neg2(c[2]);
+                A1[el] = c[1] + neg2(c[3] * f2s(3.0f));
+                A2[el] = c[2] * f2s(2.0f);
+                A3[el] = c[3] * f2s(4.0f);
+            }
+#pragma unroll
+            for (int jc = 0; jc < 3; ++jc) {
+                const float u = jc == 0 ? -1.0f : jc == 1 ? 0.0f : 1.0f;
+                const float T = fmaf(t_h, u, t_c);
+                const float p_i = sqrtf(T * (T + 2.0f * mc2)) * inv_mc2;
+                const float bi = p_i / (1.0f + T * inv_mc2);
+                F2 ex[NEL];
+                brem_J2<NEL>(f2s(T) + neg2(k2), T, p_i, bi / (p_i * p_i), kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, ex);
+#pragma unroll
+                for (int el = 0; el < NEL; ++el) {
+                    const F2 pv = fma2(fma2(fma2(A3[el], f2s(u), A2[el]), f2s(u), A1[el]), f2s(u), A0[el]);
+                    const F2 d = pv + neg2(ex[el]);
+                    cub = cub && fabsf(f2lo(d)) <= 1e-6f * fabsf(f2lo(ex[el])) &&
+                          fabsf(f2hi(d)) <= 1e-6f * fabsf(f2hi(ex[el]));
+                }
+            }
+        }
+        const float inv_th = t_h > 0.0f ? 1.0f / t_h : 0.0f;
         F2 Q0 = f2s(0.0f), Q1 = f2s(0.0f), Q2 = f2s(0.0f), Q3 = f2s(0.0f);
         for (int j = 0; j < nc; ++j) {
             const BremSeg<float> &b = segs[j];
-            F2 Tf = f2s(b.T) + neg2(k2);
-            const float tfl = f2lo(Tf), tfh = f2hi(Tf);
-            const bool va = tfl > 1e-6f && act_a, vb = tfh > 1e-6f && act_b;
-            if (!va && !vb) continue;
-            Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
-            // cross section (brem_nsig's float form, both energies at once)
-            const F2 q = Tf * (Tf + f2s(2.0f * mc2));
-            const F2 rs = rsqrt_2(q);
-            const F2 p_f = (q * rs) * f2s(inv_mc2);
-            const F2 sp = f2s(b.p_i) + p_f;
-            const F2 dpp = kc * (f2s(2.0f * b.T) + c2mk);
-            const F2 lg = lg2_2((sp * sp) * rcp_2(dpp));
-            const F2 inv_bf = fma2(Tf, f2s(inv_mc2), f2s(1.0f)) * (rs * f2s(mc2));
-            const F2 common = (c0k * f2s(b.beta_i)) * (lg * inv_bf);  // beta_i holds beta_i / p_i^2
             F2 nsig = f2s(0.0f);
-            const F2 del = inv_bf + f2s(-1.0f);
-            const bool rel = f2lo(del) < 0.01f && f2hi(del) < 0.01f;
+            if (NEL == 1 && cub) {  // uniform over the thread's chunk
+                const F2 u = f2s((b.T - t_c) * inv_th);
 #pragma unroll
-            for (int el = 0; el < NEL; ++el) {
-                F2 ginv;
-                if (rel) {
-                    const F2 sz = del * f2s(zn[el]);
-                    const float r = rh[el], r2 = r * r;
-                    const F2 poly = fma2(sz, fma2(sz, fma2(sz, f2s(-(r / 6.0f + r2 + r2 * r)), f2s(0.5f * r + r2)),
-                                                  f2s(-r)), f2s(1.0f));
-                    ginv = poly * f2s(G0[el]);
-                } else {
-                    ginv = rcp_2(f2s(1.0f) + neg2(ex2_2(neg2(inv_bf * f2s(zl[el])))));
-                }
-                nsig = fma2(f2s(b.nL[el]) * common, ginv, nsig);  // nL holds n L Z^2 den_i
+                for (int el = 0; el < NEL; ++el)
+                    nsig = fma2(f2s(b.nL[el]), fma2(fma2(fma2(A3[el], u, A2[el]), u, A1[el]), u, A0[el]), nsig);
+                nsig = nsig * c0k;
+            } else {
+                F2 Tf = f2s(b.T) + neg2(k2);
+                const float tfl = f2lo(Tf), tfh = f2hi(Tf);
+                const bool va = tfl > 1e-6f && act_a, vb = tfh > 1e-6f && act_b;
+                if (!va && !vb) continue;
+                Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
+                F2 J[NEL];
+                // beta_i holds beta_i / p_i^2, nL holds n L Z^2 den_i
+                brem_J2<NEL, true>(Tf, b.T, b.p_i, b.beta_i, kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, J, b.nL);
+                nsig = J[0] * c0k;
+                nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
             }
-            nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
             // escape moments (brem_moment_chunk, order 3, both energies)
             const float es = up_all ? b.e0 : b.e1;
             const float ef = es + b.e2;
