@@ -871,26 +871,7 @@ __device__ __forceinline__ double bin_exact(const LineDep &L, int b, const LineW
 struct EdgeCacheF {
     bool valid, has_r;
     float x, q, r;  // q = Q(2 pi |x|) of the far form, r = R(x)
-    // far form on a uniform axis: sin and cos of 2 pi |x| at the cached edge,
-    // and of 2 pi dx (one bin), so the next edge's phase is one rotation
-    bool has_sc, has_rot;
-    float sn, cs, sd, cd;
 };
-
-// Q(2 pi |x|) of q_osc_x_f32 from sin and cos of 2 pi |x| already known.
-__device__ __forceinline__ float q_osc_sc_f32(float x, float sn, float cs) {
-    const float u = 6.28318530717958648f * fabsf(x);
-    const float inv_u = __frcp_rn(u);
-    const float yf = inv_u * inv_u;
-    const float p1 = yf * (2.0f + yf * (-24.0f + yf * (720.0f + yf * (-40320.0f + yf * 3628800.0f))));
-    const float p2 = 1.0f + yf * (-6.0f + yf * (120.0f + yf * (-5040.0f + yf * 362880.0f)));
-    return cs * p1 * inv_u - sn * p2 * yf;
-}
-
-__device__ __forceinline__ void sincos_turns_f32(float x, float &sn, float &cs) {
-    const float ax = fabsf(x);
-    __sincosf(6.28318530717958648f * (ax - rintf(ax)), &sn, &cs);
-}
 
 // R(x) = F(x) - sign(x)/2 of sincsq_tail in float:
 // Si(t) - pi/2 = -f(t) cos t - g(t) sin t with t = 2 pi |x| and the rational
@@ -993,31 +974,12 @@ __device__ __forceinline__ int bin_fast_f32(float E_r, float s, float scale, int
             const float r_hi = sincsq_tail_f32(x_hi);
             ec.valid = true;
             ec.has_r = true;
-            ec.has_sc = false;
             ec.x = x_hi;
             ec.r = r_hi;
             mass = r_hi - r_lo + ((x_lo < 0.0f && x_hi >= 0.0f) ? 1.0f : 0.0f);
         } else {
             const float q_lo = (cached && !ec.has_r) ? ec.q : q_osc_x_f32(x_lo);
-            float q_hi;
-            if (uniform && cached && !ec.has_r && ec.has_sc) {
-                // the next edge one bin further: rotate the cached phase by
-                // +-2 pi dx (|x| grows above the line, shrinks below it)
-                if (!ec.has_rot) {
-                    sincos_turns_f32(dxw, ec.sd, ec.cd);
-                    ec.has_rot = true;
-                }
-                const float sd = x_lo > 0.0f ? ec.sd : -ec.sd;
-                const float sn = fmaf(ec.sn, ec.cd, ec.cs * sd);
-                const float cs = fmaf(ec.cs, ec.cd, -ec.sn * sd);
-                ec.sn = sn;
-                ec.cs = cs;
-                q_hi = q_osc_sc_f32(x_hi, sn, cs);
-            } else {
-                sincos_turns_f32(x_hi, ec.sn, ec.cs);
-                ec.has_sc = true;
-                q_hi = q_osc_sc_f32(x_hi, ec.sn, ec.cs);
-            }
+            const float q_hi = q_osc_x_f32(x_hi);
             ec.valid = true;
             ec.has_r = false;
             ec.x = x_hi;
@@ -1387,8 +1349,6 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
                 ec.valid = false;
                 EdgeCacheF ecf;
                 ecf.valid = false;
-                ecf.has_sc = false;
-                ecf.has_rot = false;
                 for (int item = i_begin; item < i_end; ++item) {
                     if (item >= next) {
                         do {
@@ -1408,8 +1368,6 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
                         }
                         ec.valid = false;
                         ecf.valid = false;
-                        ecf.has_sc = false;
-                        ecf.has_rot = false;
                     }
                     const int b = lw.b0 + (item - start);
                     if constexpr (kMixed) {
