@@ -871,7 +871,30 @@ __device__ __forceinline__ double bin_exact(const LineDep &L, int b, const LineW
 struct EdgeCacheF {
     bool valid, has_r;
     float x, q, r;  // q = Q(2 pi |x|) of the far form, r = R(x)
+    float iu;       // far form: 1 / (2 pi |x|) of the cached edge
+    float ia;       // far correction: 1 / (s (edge - E_c)) of the cached edge (0: unset)
 };
+
+// Reciprocal on the SFU alone (rcp.approx, about 1 ulp): the mixed path's
+// bin forms carry float rounding far below their tolerance.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Q(2 pi |x|) of q_osc_x_f32 with its reciprocal 1 / (2 pi |x|) returned in iu.
+__device__ __forceinline__ float q_osc_iu_f32(float x, float &iu) {
+    const float ax = fabsf(x);
+    const float inv_u = rcp_fast(6.28318530717958648f * ax);
+    iu = inv_u;
+    const float yf = inv_u * inv_u;
+    const float p1 = yf * (2.0f + yf * (-24.0f + yf * (720.0f + yf * (-40320.0f + yf * 3628800.0f))));
+    const float p2 = 1.0f + yf * (-6.0f + yf * (120.0f + yf * (-5040.0f + yf * 362880.0f)));
+    float sn, cs;
+    __sincosf(6.28318530717958648f * (ax - rintf(ax)), &sn, &cs);
+    return cs * p1 * inv_u - sn * p2 * yf;
+}
 
 // R(x) = F(x) - sign(x)/2 of sincsq_tail in float:
 // Si(t) - pi/2 = -f(t) cos t - g(t) sin t with t = 2 pi |x| and the rational
@@ -960,6 +983,7 @@ __device__ __forceinline__ int bin_fast_f32(float E_r, float s, float scale, int
     const float dxw = s * (e1 - e0);
     const float xc = 0.5f * (x_lo + x_hi);
     const float w = scale * s;
+    const bool consec = ec.valid && ec.x == x_lo;  // the previous bin of this line, cached
     if (dxw <= 0.1f && fabsf(xc) >= 2.0f) {
         ec.valid = false;
         v = w * sincsq_midpoint_mean_f32(xc, dxw);
@@ -978,28 +1002,40 @@ __device__ __forceinline__ int bin_fast_f32(float E_r, float s, float scale, int
             ec.r = r_hi;
             mass = r_hi - r_lo + ((x_lo < 0.0f && x_hi >= 0.0f) ? 1.0f : 0.0f);
         } else {
-            const float q_lo = (cached && !ec.has_r) ? ec.q : q_osc_x_f32(x_lo);
-            const float q_hi = q_osc_x_f32(x_hi);
+            // Far closed form: the envelope (1/lo - 1/hi) / (2 pi^2) from the
+            // edges' reciprocals 1/(2 pi |x|), which the phase terms need
+            // anyway, plus the oscillation (Q(hi) - Q(lo)) / pi.
+            const bool reuse = cached && !ec.has_r;
+            float iu_lo, iu_hi;
+            const float q_lo = reuse ? ec.q : q_osc_iu_f32(x_lo, iu_lo);
+            if (reuse) iu_lo = ec.iu;
+            const float q_hi = q_osc_iu_f32(x_hi, iu_hi);
             ec.valid = true;
             ec.has_r = false;
             ec.x = x_hi;
             ec.q = q_hi;
+            ec.iu = iu_hi;
             const bool pos = x_lo > 0.0f;
-            const float lo = pos ? x_lo : -x_hi;
-            const float hi = pos ? x_hi : -x_lo;
-            const float env = __fdividef((hi - lo) * (float)kInv2Pi2, lo * hi);
+            const float env = (pos ? (iu_lo - iu_hi) : (iu_hi - iu_lo)) * (float)kInvPi;
             const float osc = pos ? (q_hi - q_lo) : (q_lo - q_hi);
             mass = env + osc * (float)kInvPi;
         }
         v = mass * scale * (uniform ? inv_w : __frcp_rn(e1 - e0));
     }
     if (c != INT_MIN && (b - c > K_far || c - b > K_far)) {
-        const float A = s * (e0 - E_c), B = s * (e1 - E_c), d = s * (E_r - E_c);
-        const float AB = A * B;
-        const float r = __frcp_rn(AB);
-        const float f1 = (A + B) * r * r;
-        const float f2 = (A * A + AB + B * B) * r * r * r;
+        // The envelope the moments spread here: with ra = 1/A, rb = 1/B,
+        // A = s (e0 - E_c), B = s (e1 - E_c), r = ra rb:
+        // r + d (r (ra + rb) + d r (ra^2 + ra rb + rb^2)), d = s (E_r - E_c).
+        const float ra = (consec && ec.ia != 0.0f) ? ec.ia : rcp_fast(s * (e0 - E_c));
+        const float rb = rcp_fast(s * (e1 - E_c));
+        ec.ia = rb;
+        const float d = s * (E_r - E_c);
+        const float r = ra * rb;
+        const float f1 = r * (ra + rb);
+        const float f2 = r * fmaf(ra, ra + rb, rb * rb);
         v -= w * (float)kInv2Pi2 * (r + d * (f1 + d * f2));
+    } else {
+        ec.ia = 0.0f;
     }
     return kBinDone;
 }
