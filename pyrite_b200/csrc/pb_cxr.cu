@@ -1499,10 +1499,18 @@ __global__ void far_field_kernel(const double *edges, int n_E, int pad, const do
 //   f0 = r / w^2, f1 = 2 D r^2 / w^3, f2 = (3 D^2 + 1/4) r^3 / w^4,
 //   r = 1 / (D^2 - 1/4),
 // and r depends on the integer D alone: one table of r per block replaces a
-// division per (bin, centre) pair. Blocks of 128 output bins of one direction.
-__global__ void __launch_bounds__(128) far_field_conv_kernel(const double *edges, int n_E, int pad,
-                                                             const double *mom, double *spec, int K_far) {
+// division per (bin, centre) pair. A block takes 32 output bins of one
+// direction; its 8 warps split the centre bins into 8 contiguous slices (a
+// warp's lanes read the same centre bin: broadcast loads) and the slices'
+// sums are added in slice order, so the result does not depend on the launch.
+constexpr int kFarBins = 32;
+constexpr int kFarSlices = 8;
+
+__global__ void __launch_bounds__(kFarBins * kFarSlices) far_field_conv_kernel(const double *edges, int n_E, int pad,
+                                                                               const double *mom, double *spec,
+                                                                               int K_far) {
     extern __shared__ double sR[];  // r(D) for D = -n_mom .. n_mom
+    __shared__ double part[3][kFarSlices][kFarBins];
     const int d = blockIdx.y;
     const int n_mom = n_E + 2 * pad;
     const double w = (edges[n_E] - edges[0]) / n_E;
@@ -1511,25 +1519,42 @@ __global__ void __launch_bounds__(128) far_field_conv_kernel(const double *edges
         sR[i] = 1.0 / (D * D - 0.25);
     }
     __syncthreads();
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n_E) return;
+    const int lane = threadIdx.x % kFarBins, slice = threadIdx.x / kFarBins;
+    const int b = blockIdx.x * kFarBins + lane;
     const double *m = mom + (int64_t)d * n_mom * 3;
-    const double iw = 1.0 / w;
-    const double iw2 = iw * iw, iw3 = iw2 * iw, iw4 = iw2 * iw2;
+    const int per = (n_mom + kFarSlices - 1) / kFarSlices;
+    const int s0 = slice * per, s1 = min(s0 + per, n_mom);
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    for (int slot = 0; slot < n_mom; ++slot) {
-        const int c = slot - pad;
-        if (c >= b - K_far && c <= b + K_far) continue;
-        const double m0 = m[3 * slot];
-        if (m0 == 0.0) continue;
-        const int D = b - c;
-        const double r = sR[D + n_mom];
-        const double Dd = (double)D;
-        acc0 = fma(m0, r, acc0);
-        acc1 = fma(m[3 * slot + 1], 2.0 * Dd * r * r, acc1);
-        acc2 = fma(m[3 * slot + 2], (3.0 * Dd * Dd + 0.25) * r * r * r, acc2);
+    if (b < n_E) {
+        for (int slot = s0; slot < s1; ++slot) {
+            const int c = slot - pad;
+            if (c >= b - K_far && c <= b + K_far) continue;
+            const double m0 = m[3 * slot];
+            if (m0 == 0.0) continue;
+            const int D = b - c;
+            const double r = sR[D + n_mom];
+            const double Dd = (double)D;
+            acc0 = fma(m0, r, acc0);
+            acc1 = fma(m[3 * slot + 1], 2.0 * Dd * r * r, acc1);
+            acc2 = fma(m[3 * slot + 2], (3.0 * Dd * Dd + 0.25) * r * r * r, acc2);
+        }
     }
-    spec[(int64_t)d * n_E + b] += acc0 * iw2 + acc1 * iw3 + acc2 * iw4;
+    part[0][slice][lane] = acc0;
+    part[1][slice][lane] = acc1;
+    part[2][slice][lane] = acc2;
+    __syncthreads();
+    if (slice == 0 && b < n_E) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < kFarSlices; ++k) {
+            t0 += part[0][k][lane];
+            t1 += part[1][k][lane];
+            t2 += part[2][k][lane];
+        }
+        const double iw = 1.0 / w;
+        const double iw2 = iw * iw, iw3 = iw2 * iw, iw4 = iw2 * iw2;
+        spec[(int64_t)d * n_E + b] += t0 * iw2 + t1 * iw3 + t2 * iw4;
+    }
 }
 
 // Node reduction of buffered lines: spec[d][e] += sum_j w_j sinc^2(x_je),
@@ -1647,7 +1672,9 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
             // the moments sit on a uniform axis (far moments are enabled on uniform edges only)
             err = cudaFuncSetAttribute(far_field_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
             if (err != cudaSuccess) return err;
-            far_field_conv_kernel<<<fg, 128, tab, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
+            dim3 cg((unsigned)((a.n_E + kFarBins - 1) / kFarBins), (unsigned)a.n_dir);
+            far_field_conv_kernel<<<cg, kFarBins * kFarSlices, tab, s>>>(a.edges, a.n_E, far_pad, a.far_moments,
+                                                                         a.spec, K_far);
         } else {
             far_field_kernel<<<fg, 128, 0, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
         }
