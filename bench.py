@@ -48,7 +48,7 @@ SFU_OPS_PER_SM_CLOCK = 16.0  # MUFU lanes per SM per cycle
 # DRAM bytes (read + write) per history of the three scorers, from one ncu
 # capture each of a 2,048-history batch of this workload (profiles/*_si50_2048hist.md);
 # a kernel's traffic grows with its segments, so a full launch is this x histories.
-DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 7.0e6 / 2048, "brem_kernel": 5.239552e6 / 2048,
+DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 6.868736e6 / 2048, "brem_kernel": 5.239552e6 / 2048,
                           "mlp_infer_kernel": 5.484032e6 / 2048}
 BENCH_SEED = 12345  # seed of the 50 MeV Si scene in every arm
 MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"]) \
