@@ -488,6 +488,9 @@ def main():
     ap.add_argument("--surrogate-form", default="tiles", choices=["pairwise", "tiles"],
                     help="pairwise: the direction is an input and every (segment, tile) pair runs the network; "
                          "tiles: one head per detector tile on shared segment features (one pass per segment)")
+    ap.add_argument("--cv-exact-widths", type=float, default=16.0,
+                    help="exact bin-mean window of the control variate's sub-sample scorer, in first-zero widths "
+                         "(the exact arms keep the reference's 64)")
     ap.add_argument("--tile-segments", type=int, default=262144, help="training segments of the tiles form")
     ap.add_argument("--tile-epochs", type=int, default=40, help="training epochs of the tiles form")
     ap.add_argument("--train-domain", default="case", choices=["case", "uniform"],
@@ -643,7 +646,7 @@ def main():
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
         cs = ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H)
-        cs.use_surrogate([model], exact_stride=args.exact_stride)
+        cs.use_surrogate([model], exact_stride=args.exact_stride, sample_exact_widths=args.cv_exact_widths)
         compare_pass("surrogate", cs)
         gate_report = compare["surrogate"]["report"]
         arm("surrogate", cs, args.steps)
@@ -656,6 +659,7 @@ def main():
                "final_mse": losses[-1], "epoch_mse": [float(x) for x in losses],
                "diverged_epochs_redone": int(model.retries), "nonfinite_pairs_dropped": n_dropped,
                "train_domain": args.train_domain, "exact_stride": args.exact_stride,
+               "cv_exact_widths": args.cv_exact_widths,
                "coarse_bins": int(model.n_bins),
                "error_estimate": {"what": "the product path's own per-tile estimate after its probe batches "
                                           "(3 standard errors of the control-variate correction, worst bin, "
@@ -893,7 +897,8 @@ def e2e_measure(spec, args, torch, rank, world, dist, surrogates=None):
     steps = max(1, args.steps // 2)
     res = simulate_case_host(spec, args.histories, steps=steps, warmup=args.warmup, precision="mixed",
                              e_start=10_000_000 + rank * 10_000_000, surrogates=surrogates,
-                             exact_stride=args.exact_stride)
+                             exact_stride=args.exact_stride,
+                             sample_exact_widths=args.cv_exact_widths if surrogates else None)
     ms = float(res["ms_per_step"])
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
