@@ -574,16 +574,12 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
             const F2 Ea = ex2_2(nmu_l2fc * f2s(es));
             const F2 Ec = ex2_2(nmu_l2fc * f2s(ef));
             const F2 x = mu_fc * f2s(b.e2);
+            const F2 phi = fma2(x, fma2(x, fma2(x, fma2(x, fma2(x, f2s(-f_c / 720.0f), f2s(f_c / 120.0f)),
+                                                          f2s(-f_c / 24.0f)), f2s(f_c / 6.0f)), f2s(-0.5f * f_c)),
+                                f2s(f_c));
             const F2 dif = (Ea + neg2(Ec)) * (inv_mu * f2s(b.inv_e2));
-            F2 P = dif;
-            if (!(f2lo(x) > 0.1f && f2hi(x) > 0.1f)) {  // a thin segment in either lane: the series
-                const F2 phi = fma2(x, fma2(x, fma2(x, fma2(x, fma2(x, f2s(-f_c / 720.0f), f2s(f_c / 120.0f)),
-                                                              f2s(-f_c / 24.0f)), f2s(f_c / 6.0f)),
-                                            f2s(-0.5f * f_c)),
-                                    f2s(f_c));
-                const F2 ser = Ea * phi;
-                P = f2(f2lo(x) > 0.1f ? f2lo(dif) : f2lo(ser), f2hi(x) > 0.1f ? f2hi(dif) : f2hi(ser));
-            }
+            const F2 ser = Ea * phi;
+            F2 P = f2(f2lo(x) > 0.1f ? f2lo(dif) : f2lo(ser), f2hi(x) > 0.1f ? f2hi(dif) : f2hi(ser));
             Q0 = fma2(nsig, P, Q0);
             const F2 ah = nmu_dl * f2s(es), ch = nmu_dl * f2s(ef);
             F2 R = dl2 * Ec;
