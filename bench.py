@@ -39,11 +39,13 @@ ALG_FLOPS_ITEM = 80.0    # FP32 flops of one (line, bin) item of the bin-mean de
 # output layer is applied once per tile to the length-weighted sums, not per pair.
 ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
 # Bethe-Heitler + Elwert per (segment, energy), all the tiles of one exit face at once (direction
-# moments): the cross section (sqrt, log, reciprocal, and exp + reciprocal of the Elwert factor per
-# element) and the escape at the band centre (two exponentials) are 7 transcendentals on the SFU,
-# beside ~58 FP32 flops (FMA = 2); the tiles are rebuilt from the moments once per 256 segments.
-BREM_SFU_PER_PAIR = 7.0
-ALG_FLOPS_BREM = 58.0
+# moments), on the path this scene takes (one element, each 256-segment chunk within a narrow energy
+# range): the cross section is a cubic in the electron energy (3 FMA), the escape at the band centre
+# two exponentials, then the thin-segment series and four moment updates -- ~45 FP32 flops (FMA = 2)
+# and 2 SFU operations per pair, plus seven exact cross-section evaluations (3 SFU each) per energy
+# and chunk for the fit (0.08 per pair); the tiles are rebuilt from the moments once per launch.
+BREM_SFU_PER_PAIR = 2.0 + 7 * 3 / 256.0
+ALG_FLOPS_BREM = 45.0
 SFU_OPS_PER_SM_CLOCK = 16.0  # MUFU lanes per SM per cycle
 # DRAM bytes (read + write) per history of the three scorers, from one ncu
 # capture each of a 2,048-history batch of this workload (profiles/*_si50_2048hist.md);
@@ -797,15 +799,17 @@ def main():
                                         "census": "%g per pair + %g per (line, bin) item" % (ALG_FLOPS_PAIR,
                                                                                            ALG_FLOPS_ITEM)},
                        "traffic": DRAM_BYTES_PER_HISTORY["cxr_kernel"] * H},
-        "brem_kernel": {"bound": "sfu", "kernel": "brem_moment_packed_kernel (Bethe-Heitler + Elwert, 16 "
-                                                  "tiles by direction moments, FP32x2)",
-                        "achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
-                        "frac": brem_pairs_s / sfu_ceiling,
-                        "peak_source": "SFU ceiling: 148 SM x measured SM clock x 16 MUFU lanes / %g "
-                                       "transcendentals per pair" % BREM_SFU_PER_PAIR,
-                        "fp32": {"achieved_tflops": brem_pairs_s * ALG_FLOPS_BREM / 1e12, "peak_tflops": peak_fp32,
-                                 "frac": brem_pairs_s * ALG_FLOPS_BREM / 1e12 / peak_fp32,
-                                 "census": "%g FP32 flops per pair" % ALG_FLOPS_BREM},
+        "brem_kernel": {"bound": "fp32", "kernel": "brem_moment_packed_kernel (Bethe-Heitler + Elwert, 16 "
+                                                   "tiles by direction moments, FP32x2, cubic cross section)",
+                        "achieved": brem_pairs_s * ALG_FLOPS_BREM / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
+                        "frac": brem_pairs_s * ALG_FLOPS_BREM / 1e12 / peak_fp32,
+                        "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
+                        "census": "%g FP32 flops per (segment, energy) pair" % ALG_FLOPS_BREM,
+                        "pairs_per_s": brem_pairs_s,
+                        "sfu": {"achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
+                                "frac": brem_pairs_s / sfu_ceiling,
+                                "peak_source": "148 SM x measured SM clock x 16 MUFU lanes / %.2f SFU operations "
+                                               "per pair" % BREM_SFU_PER_PAIR},
                         "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H},
     }
     if sur is not None:
