@@ -518,7 +518,10 @@ def main():
             "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "50 MeV e- on 500 um Si (220), 16 tiles, 2048 bins (CPU oracle port)"},
+            "config": dict(workload_config(args, 16, 238, 2048),
+                           precision="FP64 (the CPU oracle port of the reference's algorithm)",
+                           transport="exact SR core, the same Twiss entrance states",
+                           l2="n/a (host cores)"),
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
