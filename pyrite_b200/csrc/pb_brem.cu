@@ -408,6 +408,12 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     __shared__ BremSeg<float> segs[kBremChunk];
     __shared__ double sQ[8][kBremPackedThreads];  // FP64 moment sums: [energy half * 4 + n][thread]
     __shared__ float sT[2][kBremPackedThreads / 32];  // the chunk's electron energy range, per warp
+    // the chunk's per-segment operands already packed for the FP32x2 pair
+    // loop (each half holds the same value), so the loop issues no packing
+    struct Pk {
+        F2 u, nl, es, ef, e2, ie2;
+    };
+    __shared__ Pk pk[kBremChunk];
     const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
     double f_c_d, dl_d;
     if (a.precision != PB_MIXED || !brem_packed_applies(a, d0, nd, f_c_d, dl_d)) return;
@@ -476,7 +482,6 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
             sT[1][threadIdx.x >> 5] = thi;
         }
         __syncthreads();
-        if (!on_a) continue;
         tlo = sT[0][0];
         thi = sT[1][0];
 #pragma unroll
@@ -484,6 +489,17 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
             tlo = fminf(tlo, sT[0][w]);
             thi = fmaxf(thi, sT[1][w]);
         }
+        {
+            const float tc = 0.5f * (tlo + thi), th = 0.5f * (thi - tlo);
+            const float ith = th > 0.0f ? 1.0f / th : 0.0f;
+            for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+                const BremSeg<float> &b = segs[j];
+                const float es = up_all ? b.e0 : b.e1;
+                pk[j] = Pk{f2s((b.T - tc) * ith), f2s(b.nL[0]), f2s(es), f2s(es + b.e2), f2s(b.e2), f2s(b.inv_e2)};
+            }
+        }
+        __syncthreads();
+        if (!on_a) continue;
         // The chunk's electrons span [tlo, thi]. Where that range is narrow
         // (at most 10 % of tlo) and clear of the spectrum's tip, J_el(T) of
         // this thread's two energies is the cubic through four Chebyshev
@@ -550,12 +566,9 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
         for (int j = 0; j < nc; ++j) {
             const BremSeg<float> &b = segs[j];
             F2 nsig = f2s(0.0f);
+            const Pk &q = pk[j];
             if (NEL == 1 && cub) {  // uniform over the thread's chunk
-                const F2 u = f2s((b.T - t_c) * inv_th);
-#pragma unroll
-                for (int el = 0; el < NEL; ++el)
-                    nsig = fma2(f2s(b.nL[el]), fma2(fma2(fma2(A3[el], u, A2[el]), u, A1[el]), u, A0[el]), nsig);
-                nsig = nsig * c0k;
+                nsig = (q.nl * fma2(fma2(fma2(A3[0], q.u, A2[0]), q.u, A1[0]), q.u, A0[0])) * c0k;
             } else {
                 F2 Tf = f2s(b.T) + neg2(k2);
                 const float tfl = f2lo(Tf), tfh = f2hi(Tf);
@@ -569,19 +582,17 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
                 nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
             }
             // escape moments (brem_moment_chunk, order 3, both energies)
-            const float es = up_all ? b.e0 : b.e1;
-            const float ef = es + b.e2;
-            const F2 Ea = ex2_2(nmu_l2fc * f2s(es));
-            const F2 Ec = ex2_2(nmu_l2fc * f2s(ef));
-            const F2 x = mu_fc * f2s(b.e2);
+            const F2 Ea = ex2_2(nmu_l2fc * q.es);
+            const F2 Ec = ex2_2(nmu_l2fc * q.ef);
+            const F2 x = mu_fc * q.e2;
             const F2 phi = fma2(x, fma2(x, fma2(x, fma2(x, fma2(x, f2s(-f_c / 720.0f), f2s(f_c / 120.0f)),
                                                           f2s(-f_c / 24.0f)), f2s(f_c / 6.0f)), f2s(-0.5f * f_c)),
                                 f2s(f_c));
-            const F2 dif = (Ea + neg2(Ec)) * (inv_mu * f2s(b.inv_e2));
+            const F2 dif = (Ea + neg2(Ec)) * (inv_mu * q.ie2);
             const F2 ser = Ea * phi;
             F2 P = f2(f2lo(x) > 0.1f ? f2lo(dif) : f2lo(ser), f2hi(x) > 0.1f ? f2hi(dif) : f2hi(ser));
             Q0 = fma2(nsig, P, Q0);
-            const F2 ah = nmu_dl * f2s(es), ch = nmu_dl * f2s(ef);
+            const F2 ah = nmu_dl * q.es, ch = nmu_dl * q.ef;
             F2 R = dl2 * Ec;
             P = fma2(ah, P, R);
             R = R * ch;
