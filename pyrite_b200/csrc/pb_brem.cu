@@ -250,7 +250,8 @@ __device__ __forceinline__ Real brem_nsig(const BremSeg<Real> &b, Real k, Real T
 // about rho^(N+1) / sqrt(2 pi (N+1)) of the unattenuated term, rho = Delta /
 // f_min, whatever the optical depths (the attenuation exp(-a f_min) bounds the
 // growth of the derivatives); the choice N = 3 for rho <= 0.01 and N = 5 for
-// rho <= 0.05 keeps it below 3e-9.
+// rho <= 0.05 keeps it below 3e-9, and so does N = 2 for rho <= 0.002 (the
+// packed kernel's order there).
 // ---------------------------------------------------------------------------
 struct BremMomentConst {
     float mu_l2fc;  // mu log2(e) f_c
@@ -402,6 +403,11 @@ __device__ __forceinline__ bool brem_packed_applies(const pb_brem_args &a, int d
     return (n_up == nd || n_up == 0) && dl <= 0.01 * f_lo;
 }
 
+template <int N>
+struct MomentOrder {
+    static constexpr int value = N;
+};
+
 template <int NEL>
 __global__ void __launch_bounds__(kBremPackedThreads, 3)
     brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
@@ -418,6 +424,9 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     double f_c_d, dl_d;
     if (a.precision != PB_MIXED || !brem_packed_applies(a, d0, nd, f_c_d, dl_d)) return;
     const bool up_all = a.n_hat[3 * d0 + 2] < 0.0;
+    // Moment order: 2 where rho = Delta / f_min <= 0.002 (truncation below
+    // rho^3 / sqrt(6 pi) < 2e-9 of the unattenuated term), else 3.
+    const bool order3 = dl_d > 0.002 * (f_c_d - dl_d);
     const float T_slab = (float)a.thickness;
     const float mc2 = 510.99895f, inv_mc2 = 1.0f / 510.99895f;
     const float za = (float)(2.0 * kPi * kAlphaFs);
@@ -437,11 +446,21 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     const double c0 = 16.0 / 3.0 * kAlphaFs * kReCm2 * 0.6931471805599453;
     const F2 c0k = f2((float)(c0 / fmax(kd[0] * 1e3, 1e-30)), (float)(c0 / fmax(kd[1] * 1e3, 1e-30)));
     const F2 nmu_l2fc = f2((float)(-mud[0] * 1.4426950408889634 * f_c_d), (float)(-mud[1] * 1.4426950408889634 * f_c_d));
-    const F2 mu_fc = f2((float)(mud[0] * f_c_d), (float)(mud[1] * f_c_d));
     const F2 inv_mu = f2(mud[0] > 0.0 ? (float)(1.0 / mud[0]) : 0.0f, mud[1] > 0.0 ? (float)(1.0 / mud[1]) : 0.0f);
     const F2 nmu_dl = f2((float)(-mud[0] * dl_d), (float)(-mud[1] * dl_d));
     const F2 dl2 = f2s((float)dl_d);
-    const float f_c = (float)f_c_d;
+    const F2 nmu_fc = f2((float)(-mud[0] * f_c_d), (float)(-mud[1] * f_c_d));
+    const F2 fc2 = f2s((float)f_c_d);
+    // Depth extent below which x = mu f_c e2 <= 0.1 in every lane of this
+    // warp (the largest mu of its 64 energies): the pair loop's branch on it
+    // is warp-uniform, since all lanes take the same segment.
+    float e2_series;
+    {
+        float mm = (float)(fmax(mud[0], mud[1]) * f_c_d);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+        e2_series = mm > 0.0f ? 0.1f / mm : 3.4e38f;
+    }
     // Elwert constants per element: z log2(e) for the SFU form; G0 and rho
     // of the relativistic series.
     float zl[NEL], zn[NEL], G0[NEL], rh[NEL];
@@ -561,48 +580,63 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
                 }
             }
         }
-        const float inv_th = t_h > 0.0f ? 1.0f / t_h : 0.0f;
         F2 Q0 = f2s(0.0f), Q1 = f2s(0.0f), Q2 = f2s(0.0f), Q3 = f2s(0.0f);
-        for (int j = 0; j < nc; ++j) {
-            const BremSeg<float> &b = segs[j];
-            F2 nsig = f2s(0.0f);
-            const Pk &q = pk[j];
-            if (NEL == 1 && cub) {  // uniform over the thread's chunk
-                nsig = (q.nl * fma2(fma2(fma2(A3[0], q.u, A2[0]), q.u, A1[0]), q.u, A0[0])) * c0k;
-            } else {
-                F2 Tf = f2s(b.T) + neg2(k2);
-                const float tfl = f2lo(Tf), tfh = f2hi(Tf);
-                const bool va = tfl > 1e-6f && act_a, vb = tfh > 1e-6f && act_b;
-                if (!va && !vb) continue;
-                Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
-                F2 J[NEL];
-                // beta_i holds beta_i / p_i^2, nL holds n L Z^2 den_i
-                brem_J2<NEL, true>(Tf, b.T, b.p_i, b.beta_i, kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, J, b.nL);
-                nsig = J[0] * c0k;
-                nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
+        // The pair loop for moment order 2 or 3 (the order is uniform over the launch).
+        auto pairs = [&](auto order) {
+            constexpr int kOrd = decltype(order)::value;
+            for (int j = 0; j < nc; ++j) {
+                const BremSeg<float> &b = segs[j];
+                F2 nsig = f2s(0.0f);
+                const Pk &q = pk[j];
+                if (NEL == 1 && cub) {  // uniform over the thread's chunk
+                    nsig = (q.nl * fma2(fma2(fma2(A3[0], q.u, A2[0]), q.u, A1[0]), q.u, A0[0])) * c0k;
+                } else {
+                    F2 Tf = f2s(b.T) + neg2(k2);
+                    const float tfl = f2lo(Tf), tfh = f2hi(Tf);
+                    const bool va = tfl > 1e-6f && act_a, vb = tfh > 1e-6f && act_b;
+                    if (!va && !vb) continue;
+                    Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
+                    F2 J[NEL];
+                    // beta_i holds beta_i / p_i^2, nL holds n L Z^2 den_i
+                    brem_J2<NEL, true>(Tf, b.T, b.p_i, b.beta_i, kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, J, b.nL);
+                    nsig = J[0] * c0k;
+                    nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
+                }
+                // escape moments (brem_moment_chunk, order kOrd, both energies)
+                const F2 Ea = ex2_2(nmu_l2fc * q.es);
+                // y = -x = -mu f_c e2; phi(x) = (1 - e^-x)/x = sum_n y^n / (n + 1)!
+                const F2 y = nmu_fc * q.e2;
+                const F2 phi = fma2(y, fma2(y, fma2(y, fma2(y, fma2(y, f2s(1.0f / 720.0f), f2s(1.0f / 120.0f)),
+                                                              f2s(1.0f / 24.0f)), f2s(1.0f / 6.0f)), f2s(0.5f)),
+                                    f2s(1.0f));
+                const F2 A = Ea * phi;
+                F2 P = A * fc2, Ec;
+                if (f2lo(q.e2) <= e2_series) {
+                    // x <= 0.1 in both lanes: P_0 = E_a f_c phi(x) from the series,
+                    // and E_c = E_a e^-x = E_a (1 - x phi(x)) (no second exponential).
+                    Ec = fma2(A, y, Ea);
+                } else {
+                    Ec = ex2_2(nmu_l2fc * q.ef);
+                    const F2 dif = (Ea + neg2(Ec)) * (inv_mu * q.ie2);
+                    P = f2(f2lo(y) < -0.1f ? f2lo(dif) : f2lo(P), f2hi(y) < -0.1f ? f2hi(dif) : f2hi(P));
+                }
+                Q0 = fma2(nsig, P, Q0);
+                const F2 ah = nmu_dl * q.es, ch = nmu_dl * q.ef;
+                F2 R = dl2 * Ec;
+                P = fma2(ah, P, R);
+                R = R * ch;
+                Q1 = fma2(nsig, P, Q1);
+                P = fma2(ah, P, R);
+                Q2 = fma2(nsig, P, Q2);
+                if constexpr (kOrd >= 3) {
+                    R = R * ch;
+                    P = fma2(ah, P, R);
+                    Q3 = fma2(nsig, P, Q3);
+                }
             }
-            // escape moments (brem_moment_chunk, order 3, both energies)
-            const F2 Ea = ex2_2(nmu_l2fc * q.es);
-            const F2 Ec = ex2_2(nmu_l2fc * q.ef);
-            const F2 x = mu_fc * q.e2;
-            const F2 phi = fma2(x, fma2(x, fma2(x, fma2(x, fma2(x, f2s(-f_c / 720.0f), f2s(f_c / 120.0f)),
-                                                          f2s(-f_c / 24.0f)), f2s(f_c / 6.0f)), f2s(-0.5f * f_c)),
-                                f2s(f_c));
-            const F2 dif = (Ea + neg2(Ec)) * (inv_mu * q.ie2);
-            const F2 ser = Ea * phi;
-            F2 P = f2(f2lo(x) > 0.1f ? f2lo(dif) : f2lo(ser), f2hi(x) > 0.1f ? f2hi(dif) : f2hi(ser));
-            Q0 = fma2(nsig, P, Q0);
-            const F2 ah = nmu_dl * q.es, ch = nmu_dl * q.ef;
-            F2 R = dl2 * Ec;
-            P = fma2(ah, P, R);
-            R = R * ch;
-            Q1 = fma2(nsig, P, Q1);
-            P = fma2(ah, P, R);
-            R = R * ch;
-            Q2 = fma2(nsig, P, Q2);
-            P = fma2(ah, P, R);
-            Q3 = fma2(nsig, P, Q3);
-        }
+        };
+        if (order3) pairs(MomentOrder<3>{});
+        else pairs(MomentOrder<2>{});
         const int t = threadIdx.x;
         sQ[0][t] += f2lo(Q0); sQ[4][t] += f2hi(Q0);
         sQ[1][t] += f2lo(Q1); sQ[5][t] += f2hi(Q1);
