@@ -39,13 +39,16 @@ ALG_FLOPS_ITEM = 80.0    # FP32 flops of one (line, bin) item of the bin-mean de
 # output layer is applied once per tile to the length-weighted sums, not per pair.
 ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
 # Bethe-Heitler + Elwert per (segment, energy), all the tiles of one exit face at once (direction
-# moments), on the path this scene takes (one element, each 256-segment chunk within a narrow energy
-# range): the cross section is a cubic in the electron energy (3 FMA), the escape at the band centre
-# two exponentials, then the thin-segment series and four moment updates -- ~45 FP32 flops (FMA = 2)
-# and 2 SFU operations per pair, plus seven exact cross-section evaluations (3 SFU each) per energy
-# and chunk for the fit (0.08 per pair); the tiles are rebuilt from the moments once per launch.
-BREM_SFU_PER_PAIR = 2.0 + 7 * 3 / 256.0
-ALG_FLOPS_BREM = 45.0
+# moments, order 2 for this detector's spread), on the path this scene takes (one element, each
+# 256-segment chunk within a narrow energy range): the cross section is a cubic in the electron
+# energy (3 FMA), the escape at the band centre one exponential and the thin-segment series, then
+# three moment updates -- 38 FP32 flops (FMA = 2) and 1 SFU operation per pair where the warp's
+# segment is optically thin (x = mu f_c e2 <= 0.1 for all its 64 energies), 2 more flops and a
+# second exponential elsewhere; plus seven exact cross-section evaluations (3 SFU each) per energy
+# and chunk for the fit (0.08 per pair). The thin share is counted from the last batch's segments
+# (brem_thin_fraction); the tiles are rebuilt from the moments once per launch.
+ALG_FLOPS_BREM_THIN, ALG_FLOPS_BREM_THICK = 38.0, 40.0
+BREM_FIT_SFU_PER_PAIR = 7 * 3 / 256.0
 SFU_OPS_PER_SM_CLOCK = 16.0  # MUFU lanes per SM per cycle
 # DRAM bytes (read + write) per history of the three scorers, from one ncu
 # capture each of a 2,048-history batch of this workload (profiles/*_si50_2048hist.md);
@@ -86,6 +89,28 @@ def sigma_stats(got, ref, sigma, floor=1e-3):
         return {"max": None, "within_3_sigma": None, "bins": 0}
     z = np.abs(got - ref)[m] / sigma[m]
     return {"max": float(z.max()), "within_3_sigma": float(np.mean(z <= 3.0)), "bins": int(m.sum())}
+
+
+def brem_thin_fraction(case, spec, n_seg, torch):
+    """Share of the (segment, energy) pairs that brem_moment_packed_kernel scores on its
+    thin-segment path: the segment's depth extent e2 in the slab is at most 0.1 / (mu f_c) for
+    the largest attenuation mu of the 64 energies a warp holds (f_c the centre path factor of
+    the tiles). Counted on the device from the last batch's segments."""
+    z = case.seg_r[:3 * n_seg].view(-1, 3)[:, 2]
+    vz = case.seg_v[:3 * n_seg].view(-1, 3)[:, 2]
+    half = 0.5 * case.seg_L[:n_seg]
+    T = float(case.bargs.thickness)
+    e2 = ((z + half * vz).clamp(0.0, T) - (z - half * vz).clamp(0.0, T)).abs()
+    f = 1.0 / np.maximum(np.abs(np.asarray(spec.n_hats)[:case.n_dir, 2]), 1e-12)
+    f_c = 0.5 * (f.min() + f.max())
+    mu = np.asarray(spec.brem_mu, dtype=np.float64)
+    n_E = mu.size
+    thin = 0.0
+    for g0 in range(0, n_E, 64):
+        m = mu[g0:g0 + 64].max() * f_c
+        lim = 0.1 / m if m > 0 else np.inf
+        thin += (mu[g0:g0 + 64].size) * float((e2 <= lim).sum().item())
+    return thin / max(1.0, float(n_seg) * n_E)
 
 
 def workload_config(args, n_dir, n_g, n_bins):
@@ -789,8 +814,11 @@ def main():
     items_per_pair = cxr_work["deposit_items"] / max(1.0, cxr_work["segments"] * n_g_cxr * mixed_case.n_dir)
     cxr_tflops_dep = pairs * (ALG_FLOPS_PAIR + items_per_pair * ALG_FLOPS_ITEM) / (mixed["t_cxr"] / 1e3) / 1e12
     brem_pairs_s = n_seg * n_E / (r_head["t_brem"] / 1e3)
+    thin = brem_thin_fraction(ce, spec, n_seg, torch)
+    flops_brem = thin * ALG_FLOPS_BREM_THIN + (1.0 - thin) * ALG_FLOPS_BREM_THICK
+    sfu_brem = thin * 1.0 + (1.0 - thin) * 2.0 + BREM_FIT_SFU_PER_PAIR
     sm_mhz = (clocks[head].get("sm_mhz") or 1965.0)
-    sfu_ceiling = 148 * sm_mhz * 1e6 * SFU_OPS_PER_SM_CLOCK / BREM_SFU_PER_PAIR
+    sfu_ceiling = 148 * sm_mhz * 1e6 * SFU_OPS_PER_SM_CLOCK / sfu_brem
     rooflines = {
         "cxr_kernel": {"bound": "fp32", "kernel": "cxr_kernel<float> (exact PXR+CBS lines + bin-mean deposit)",
                        "achieved": cxr_tflops, "peak": peak_fp32, "unit": "TFLOP/s", "frac": cxr_tflops / peak_fp32,
@@ -803,16 +831,20 @@ def main():
                                                                                            ALG_FLOPS_ITEM)},
                        "traffic": DRAM_BYTES_PER_HISTORY["cxr_kernel"] * H},
         "brem_kernel": {"bound": "fp32", "kernel": "brem_moment_packed_kernel (Bethe-Heitler + Elwert, 16 "
-                                                   "tiles by direction moments, FP32x2, cubic cross section)",
-                        "achieved": brem_pairs_s * ALG_FLOPS_BREM / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
-                        "frac": brem_pairs_s * ALG_FLOPS_BREM / 1e12 / peak_fp32,
+                                                   "tiles by direction moments, FP32x2, cubic cross section, "
+                                                   "thin-segment escape series)",
+                        "achieved": brem_pairs_s * flops_brem / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
+                        "frac": brem_pairs_s * flops_brem / 1e12 / peak_fp32,
                         "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
-                        "census": "%g FP32 flops per (segment, energy) pair" % ALG_FLOPS_BREM,
+                        "census": "%.2f FP32 flops per (segment, energy) pair (%g thin-segment, %g otherwise; "
+                                  "%.3f of the pairs thin)" % (flops_brem, ALG_FLOPS_BREM_THIN,
+                                                               ALG_FLOPS_BREM_THICK, thin),
+                        "thin_fraction": thin,
                         "pairs_per_s": brem_pairs_s,
                         "sfu": {"achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
                                 "frac": brem_pairs_s / sfu_ceiling,
                                 "peak_source": "148 SM x measured SM clock x 16 MUFU lanes / %.2f SFU operations "
-                                               "per pair" % BREM_SFU_PER_PAIR},
+                                               "per pair" % sfu_brem},
                         "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H},
     }
     if sur is not None:
