@@ -41,13 +41,14 @@ ALG_FLOPS_INFER = 2.0 * (6 * 256 + 3 * 256 * 256)
 # Bethe-Heitler + Elwert per (segment, energy), all the tiles of one exit face at once (direction
 # moments, order 2 for this detector's spread), on the path this scene takes (one element, each
 # 256-segment chunk within a narrow energy range): the cross section is a cubic in the electron
-# energy (3 FMA), the escape at the band centre one exponential and the thin-segment series, then
-# three moment updates -- 38 FP32 flops (FMA = 2) and 1 SFU operation per pair where the warp's
-# segment is optically thin (x = mu f_c e2 <= 0.1 for all its 64 energies), 2 more flops and a
-# second exponential elsewhere; plus seven exact cross-section evaluations (3 SFU each) per energy
-# and chunk for the fit (0.08 per pair). The thin share is counted from the last batch's segments
-# (brem_thin_fraction); the tiles are rebuilt from the moments once per launch.
-ALG_FLOPS_BREM_THIN, ALG_FLOPS_BREM_THICK = 38.0, 40.0
+# energy (3 FMA), the escape at the band centre one exponential (its exponent carries the segment
+# factor) and the thin-segment series, then three moment updates -- 36 FP32 flops (FMA = 2) and
+# 1 SFU operation per pair where the warp's segment is optically thin (x = mu f_c e2 <= 0.1 for
+# all its 64 energies), 3 more flops and a second exponential elsewhere; plus seven exact
+# cross-section evaluations (3 SFU each) per energy and chunk for the fit (0.08 per pair). The
+# thin share is counted from the last batch's segments (brem_thin_fraction); the tiles are rebuilt
+# from the moments once per launch.
+ALG_FLOPS_BREM_THIN, ALG_FLOPS_BREM_THICK = 36.0, 39.0
 BREM_FIT_SFU_PER_PAIR = 7 * 3 / 256.0
 SFU_OPS_PER_SM_CLOCK = 16.0  # MUFU lanes per SM per cycle
 # DRAM bytes (read + write) per history of the three scorers, from one ncu
@@ -96,9 +97,9 @@ def brem_thin_fraction(case, spec, n_seg, torch):
     thin-segment path: the segment's depth extent e2 in the slab is at most 0.1 / (mu f_c) for
     the largest attenuation mu of the 64 energies a warp holds (f_c the centre path factor of
     the tiles). Counted on the device from the last batch's segments."""
-    z = case.seg_r[:3 * n_seg].view(-1, 3)[:, 2]
-    vz = case.seg_v[:3 * n_seg].view(-1, 3)[:, 2]
-    half = 0.5 * case.seg_L[:n_seg]
+    z = case.seg_r.reshape(-1)[:3 * n_seg].view(-1, 3)[:, 2]
+    vz = case.seg_v.reshape(-1)[:3 * n_seg].view(-1, 3)[:, 2]
+    half = 0.5 * case.seg_L.reshape(-1)[:n_seg]
     T = float(case.bargs.thickness)
     e2 = ((z + half * vz).clamp(0.0, T) - (z - half * vz).clamp(0.0, T)).abs()
     f = 1.0 / np.maximum(np.abs(np.asarray(spec.n_hats)[:case.n_dir, 2]), 1e-12)

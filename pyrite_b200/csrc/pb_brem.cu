@@ -306,13 +306,17 @@ __device__ __forceinline__ float brem_moment_eval(const float (&Q)[N + 1], float
 
 // ---------------------------------------------------------------------------
 // Packed moment kernel: the float path for directions on one exit face with
-// rho <= 0.01 (order-3 moments; a single direction is the order-0 case of the
-// same recurrences). Two photon energies per thread on packed FP32x2
-// arithmetic (fma/mul/add.rn.f32x2), so the non-SFU instructions of a
-// (segment, energy) pair are issued once per two pairs; the moments Q_n of
-// both energies are summed in FP64 registers across the chunks and the
-// directions are rebuilt once at the end (the reconstruction is linear in
-// Q_n), so no per-direction accumulators are kept. For relativistic final
+// rho <= 0.01 (order-3 moments, order 2 for rho <= 0.002; a single direction
+// is the order-0 case of the same recurrences). Two photon energies per
+// thread on packed FP32x2 arithmetic (fma/mul/add.rn.f32x2), so the non-SFU
+// instructions of a (segment, energy) pair are issued once per two pairs; the
+// moments are summed per chunk in float and then in FP64 shared memory, and
+// the directions are rebuilt once at the end (the reconstruction is linear in
+// the moments), so no per-direction accumulators are kept. The pair loop
+// carries the moments divided by Delta^n (Q_n / Delta^n, rebuilt with
+// (f_d - f_c)^n) and, for one element, without the segment factor and c0 / k:
+// the segment factor enters the escape exponent as log2 of its ratio to the
+// chunk's 2^ref, and c0 2^ref / k scales the chunk's sums. For relativistic final
 // states (1/beta_f - 1 < 0.01, T_f > ~3 MeV) the Elwert factor's reciprocal
 // 1/(1 - exp(-z/beta_f)) comes from its series in s = z (1/beta_f - 1):
 //   G0 [1 - rho s + (rho/2 + rho^2) s^2 - (rho/6 + rho^2 + rho^3) s^3],
@@ -413,11 +417,11 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
     __shared__ BremSeg<float> segs[kBremChunk];
     __shared__ double sQ[8][kBremPackedThreads];  // FP64 moment sums: [energy half * 4 + n][thread]
-    __shared__ float sT[2][kBremPackedThreads / 32];  // the chunk's electron energy range, per warp
+    __shared__ float sT[3][kBremPackedThreads / 32];  // the chunk's electron energy range, per warp
     // the chunk's per-segment operands already packed for the FP32x2 pair
     // loop (each half holds the same value), so the loop issues no packing
     struct Pk {
-        F2 u, nl, es, ef, e2, ie2;
+        F2 u, lnl, es, ef, e2;
     };
     __shared__ Pk pk[kBremChunk];
     const int nd = (a.n_dir - d0) < kBremMaxDir ? (a.n_dir - d0) : kBremMaxDir;
@@ -444,11 +448,9 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     const F2 kc = f2((float)(kd[0] / (510.99895 * 510.99895)), (float)(kd[1] / (510.99895 * 510.99895)));
     const F2 c2mk = f2((float)(2.0 * 510.99895 - kd[0]), (float)(2.0 * 510.99895 - kd[1]));
     const double c0 = 16.0 / 3.0 * kAlphaFs * kReCm2 * 0.6931471805599453;
-    const F2 c0k = f2((float)(c0 / fmax(kd[0] * 1e3, 1e-30)), (float)(c0 / fmax(kd[1] * 1e3, 1e-30)));
     const F2 nmu_l2fc = f2((float)(-mud[0] * 1.4426950408889634 * f_c_d), (float)(-mud[1] * 1.4426950408889634 * f_c_d));
     const F2 inv_mu = f2(mud[0] > 0.0 ? (float)(1.0 / mud[0]) : 0.0f, mud[1] > 0.0 ? (float)(1.0 / mud[1]) : 0.0f);
-    const F2 nmu_dl = f2((float)(-mud[0] * dl_d), (float)(-mud[1] * dl_d));
-    const F2 dl2 = f2s((float)dl_d);
+    const F2 nmu = f2((float)-mud[0], (float)-mud[1]);
     const F2 nmu_fc = f2((float)(-mud[0] * f_c_d), (float)(-mud[1] * f_c_d));
     const F2 fc2 = f2s((float)f_c_d);
     // Depth extent below which x = mu f_c e2 <= 0.1 in every lane of this
@@ -485,36 +487,48 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     for (int64_t c0s = s_begin; c0s < s_end; c0s += kBremChunk) {
         const int nc = (int)((s_end - c0s) < kBremChunk ? (s_end - c0s) : kBremChunk);
         __syncthreads();
-        float tlo = 3.4e38f, thi = -3.4e38f;
+        float tlo = 3.4e38f, thi = -3.4e38f, nmax = 0.0f;
         for (int j = threadIdx.x; j < nc; j += blockDim.x) {
             brem_stage<float>(segs[j], a, c0s + j, T_slab, mc2, za);
             tlo = fminf(tlo, segs[j].T);
             thi = fmaxf(thi, segs[j].T);
+            nmax = fmaxf(nmax, segs[j].nL[0]);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             tlo = fminf(tlo, __shfl_xor_sync(0xffffffffu, tlo, o));
             thi = fmaxf(thi, __shfl_xor_sync(0xffffffffu, thi, o));
+            nmax = fmaxf(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
         }
         if ((threadIdx.x & 31) == 0) {
             sT[0][threadIdx.x >> 5] = tlo;
             sT[1][threadIdx.x >> 5] = thi;
+            sT[2][threadIdx.x >> 5] = nmax;
         }
         __syncthreads();
         tlo = sT[0][0];
         thi = sT[1][0];
+        nmax = sT[2][0];
 #pragma unroll
         for (int w = 1; w < kBremPackedThreads / 32; ++w) {
             tlo = fminf(tlo, sT[0][w]);
             thi = fmaxf(thi, sT[1][w]);
+            nmax = fmaxf(nmax, sT[2][w]);
         }
+        // One element: the segment factor n L Z^2 den_i rides in the escape
+        // exponent as log2 of its ratio to 2^ref (ref the chunk's largest,
+        // rounded down), so the pair loop multiplies by neither it nor c0 / k;
+        // both come back once per chunk. Several elements weight the cross
+        // section itself (ref = 0, exponent offset 0).
+        const int ref = (NEL == 1 && nmax > 0.0f) ? (int)floorf(log2f(nmax)) : 0;
         {
             const float tc = 0.5f * (tlo + thi), th = 0.5f * (thi - tlo);
             const float ith = th > 0.0f ? 1.0f / th : 0.0f;
             for (int j = threadIdx.x; j < nc; j += blockDim.x) {
                 const BremSeg<float> &b = segs[j];
                 const float es = up_all ? b.e0 : b.e1;
-                pk[j] = Pk{f2s((b.T - tc) * ith), f2s(b.nL[0]), f2s(es), f2s(es + b.e2), f2s(b.e2), f2s(b.inv_e2)};
+                const float lnl = NEL == 1 ? log2f(b.nL[0]) - (float)ref : 0.0f;  // log2(0) = -inf: no emission
+                pk[j] = Pk{f2s((b.T - tc) * ith), f2s(lnl), f2s(es), f2s(es + b.e2), f2s(b.e2)};
             }
         }
         __syncthreads();
@@ -589,7 +603,7 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
                 F2 nsig = f2s(0.0f);
                 const Pk &q = pk[j];
                 if (NEL == 1 && cub) {  // uniform over the thread's chunk
-                    nsig = (q.nl * fma2(fma2(fma2(A3[0], q.u, A2[0]), q.u, A1[0]), q.u, A0[0])) * c0k;
+                    nsig = fma2(fma2(fma2(A3[0], q.u, A2[0]), q.u, A1[0]), q.u, A0[0]);
                 } else {
                     F2 Tf = f2s(b.T) + neg2(k2);
                     const float tfl = f2lo(Tf), tfh = f2hi(Tf);
@@ -598,12 +612,14 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
                     Tf = f2(va ? tfl : 1.0f, vb ? tfh : 1.0f);  // keep idle halves finite
                     F2 J[NEL];
                     // beta_i holds beta_i / p_i^2, nL holds n L Z^2 den_i
-                    brem_J2<NEL, true>(Tf, b.T, b.p_i, b.beta_i, kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, J, b.nL);
-                    nsig = J[0] * c0k;
+                    const float one[1] = {1.0f};
+                    brem_J2<NEL, true>(Tf, b.T, b.p_i, b.beta_i, kc, c2mk, mc2, inv_mc2, zl, zn, G0, rh, J,
+                                       NEL == 1 ? one : b.nL);
+                    nsig = J[0];
                     nsig = f2(va ? f2lo(nsig) : 0.0f, vb ? f2hi(nsig) : 0.0f);
                 }
                 // escape moments (brem_moment_chunk, order kOrd, both energies)
-                const F2 Ea = ex2_2(nmu_l2fc * q.es);
+                const F2 Ea = ex2_2(fma2(nmu_l2fc, q.es, q.lnl));
                 // y = -x = -mu f_c e2; phi(x) = (1 - e^-x)/x = sum_n y^n / (n + 1)!
                 const F2 y = nmu_fc * q.e2;
                 const F2 phi = fma2(y, fma2(y, fma2(y, fma2(y, fma2(y, f2s(1.0f / 720.0f), f2s(1.0f / 120.0f)),
@@ -616,16 +632,17 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
                     // and E_c = E_a e^-x = E_a (1 - x phi(x)) (no second exponential).
                     Ec = fma2(A, y, Ea);
                 } else {
-                    Ec = ex2_2(nmu_l2fc * q.ef);
-                    const F2 dif = (Ea + neg2(Ec)) * (inv_mu * q.ie2);
+                    Ec = ex2_2(fma2(nmu_l2fc, q.ef, q.lnl));
+                    const F2 dif = (Ea + neg2(Ec)) * (inv_mu * f2s(b.inv_e2));
                     P = f2(f2lo(y) < -0.1f ? f2lo(dif) : f2lo(P), f2hi(y) < -0.1f ? f2hi(dif) : f2hi(P));
                 }
                 Q0 = fma2(nsig, P, Q0);
-                const F2 ah = nmu_dl * q.es, ch = nmu_dl * q.ef;
-                F2 R = dl2 * Ec;
-                P = fma2(ah, P, R);
-                R = R * ch;
+                // P_n / Delta^n: the recurrence without Delta (it returns as
+                // (f - f_c)^n at the reconstruction)
+                const F2 ah = nmu * q.es, ch = nmu * q.ef;
+                P = fma2(ah, P, Ec);
                 Q1 = fma2(nsig, P, Q1);
+                F2 R = Ec * ch;
                 P = fma2(ah, P, R);
                 Q2 = fma2(nsig, P, Q2);
                 if constexpr (kOrd >= 3) {
@@ -638,15 +655,18 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
         if (order3) pairs(MomentOrder<3>{});
         else pairs(MomentOrder<2>{});
         const int t = threadIdx.x;
-        sQ[0][t] += f2lo(Q0); sQ[4][t] += f2hi(Q0);
-        sQ[1][t] += f2lo(Q1); sQ[5][t] += f2hi(Q1);
-        sQ[2][t] += f2lo(Q2); sQ[6][t] += f2hi(Q2);
-        sQ[3][t] += f2lo(Q3); sQ[7][t] += f2hi(Q3);
+        const double sc = ldexp(c0, ref);
+        const double s_lo = sc / fmax(a.E_grid[e0], 1e-30), s_hi = on_b ? sc / fmax(a.E_grid[e0 + 1], 1e-30) : 0.0;
+        sQ[0][t] += f2lo(Q0) * s_lo; sQ[4][t] += f2hi(Q0) * s_hi;
+        sQ[1][t] += f2lo(Q1) * s_lo; sQ[5][t] += f2hi(Q1) * s_hi;
+        sQ[2][t] += f2lo(Q2) * s_lo; sQ[6][t] += f2hi(Q2) * s_hi;
+        sQ[3][t] += f2lo(Q3) * s_lo; sQ[7][t] += f2hi(Q3) * s_hi;
     }
-    // Every direction of the launch from the summed moments: (1/f_d) sum_n h^n Q_n / n!.
+    // Every direction of the launch from the summed moments:
+    // (1/f_d) sum_n (f_d - f_c)^n (Q_n / Delta^n) / n!.
     for (int dd = 0; dd < nd; ++dd) {
         const double f = 1.0 / fmax(fabs(a.n_hat[3 * (d0 + dd) + 2]), 1.0e-12);
-        const double hh = dl_d > 0.0 ? (f - f_c_d) / dl_d : 0.0;
+        const double hh = f - f_c_d;
         for (int h = 0; h < 2; ++h) {
             if (!(h == 0 ? on_a : on_b)) continue;
             const double *Qh[4] = {&sQ[4 * h][threadIdx.x], &sQ[4 * h + 1][threadIdx.x], &sQ[4 * h + 2][threadIdx.x],
