@@ -59,6 +59,11 @@ DRAM_BYTES_PER_HISTORY = {"cxr_kernel": 6.868736e6 / 2048, "brem_kernel": 5.2395
 BENCH_SEED = 12345  # seed of the 50 MeV Si scene in every arm
 MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops_sustained"]) \
     if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
+MEASURED_HBM_GBS = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]) \
+    if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+# Depth-node bremsstrahlung: the segment fields its passes read per segment (electron energy,
+# length, z of the midpoint, v_z, electron id: 5 x 8 B); nothing per (segment, energy).
+NODE_BYTES_PER_SEGMENT = 40.0
 
 
 def spectrum_error_stats(got, ref):
@@ -831,23 +836,36 @@ def main():
                                         "census": "%g per pair + %g per (line, bin) item" % (ALG_FLOPS_PAIR,
                                                                                            ALG_FLOPS_ITEM)},
                        "traffic": DRAM_BYTES_PER_HISTORY["cxr_kernel"] * H},
-        "brem_kernel": {"bound": "fp32", "kernel": "brem_moment_packed_kernel (Bethe-Heitler + Elwert, 16 "
-                                                   "tiles by direction moments, FP32x2, cubic cross section, "
-                                                   "thin-segment escape series)",
-                        "achieved": brem_pairs_s * flops_brem / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
-                        "frac": brem_pairs_s * flops_brem / 1e12 / peak_fp32,
-                        "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
-                        "census": "%.2f FP32 flops per (segment, energy) pair (%g thin-segment, %g otherwise; "
-                                  "%.3f of the pairs thin)" % (flops_brem, ALG_FLOPS_BREM_THIN,
-                                                               ALG_FLOPS_BREM_THICK, thin),
-                        "thin_fraction": thin,
-                        "pairs_per_s": brem_pairs_s,
-                        "sfu": {"achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
-                                "frac": brem_pairs_s / sfu_ceiling,
-                                "peak_source": "148 SM x measured SM clock x 16 MUFU lanes / %.2f SFU operations "
-                                               "per pair" % sfu_brem},
-                        "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H},
     }
+    node_state = cases[head].brem_node_state()
+    if node_state and node_state[0]["ok"]:
+        # the depth-node form scored the step: an HBM census of what it reads
+        gbs = NODE_BYTES_PER_SEGMENT * n_seg / (r_head["t_brem"] / 1e3) / 1e9
+        rooflines["brem_kernel"] = {
+            "bound": "hbm", "kernel": "brem_node_* (depth-node form: energy window and depth grid, moment pass "
+                                      "on the FP64 tensor cores, one contraction block per photon energy)",
+            "achieved": gbs, "peak": MEASURED_HBM_GBS, "unit": "GB/s", "frac": gbs / MEASURED_HBM_GBS,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "census": "%g B per segment (energy, length, z, v_z, electron id); the five launches and the "
+                      "left-out segments' per-pair launches all inside the timed brem span" % NODE_BYTES_PER_SEGMENT,
+            "node": node_state[0], "segments": n_seg,
+            "traffic": None}
+    else:
+        rooflines["brem_kernel"] = {
+            "bound": "fp32", "kernel": "brem_moment_packed_kernel (Bethe-Heitler + Elwert, 16 tiles by direction "
+                                       "moments, FP32x2, cubic cross section, thin-segment escape series)",
+            "achieved": brem_pairs_s * flops_brem / 1e12, "peak": peak_fp32, "unit": "TFLOP/s",
+            "frac": brem_pairs_s * flops_brem / 1e12 / peak_fp32,
+            "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
+            "census": "%.2f FP32 flops per (segment, energy) pair (%g thin-segment, %g otherwise; %.3f of the "
+                      "pairs thin)" % (flops_brem, ALG_FLOPS_BREM_THIN, ALG_FLOPS_BREM_THICK, thin),
+            "thin_fraction": thin,
+            "pairs_per_s": brem_pairs_s,
+            "sfu": {"achieved": brem_pairs_s, "peak": sfu_ceiling, "unit": "(segment, energy) pairs/s",
+                    "frac": brem_pairs_s / sfu_ceiling,
+                    "peak_source": "148 SM x measured SM clock x 16 MUFU lanes / %.2f SFU operations per pair"
+                                   % sfu_brem},
+            "traffic": DRAM_BYTES_PER_HISTORY["brem_kernel"] * H}
     if sur is not None:
         t_sample, t_inf = cases["surrogate"].t_split
         tiles_form = sur["form"] == "tiles"

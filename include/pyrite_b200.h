@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define PB_ABI_VERSION 5
+#define PB_ABI_VERSION 6
 
 enum pb_status {
     PB_OK = 0,
@@ -361,6 +361,15 @@ typedef struct pb_brem_args {
      * segments whose layer equals emit_layer radiate. */
     const int32_t *seg_layer;
     int32_t emit_layer;
+    /* Optional device workspace of the mixed single-slab path (bytes from
+     * pb_brem_work_size; 16-byte aligned). With it the segments whose
+     * electron energy lies in a narrow window below the batch's highest are
+     * scored in the depth-node form (per-segment depth moments, then one
+     * contraction per photon energy); the rest, or all of them where the
+     * form does not apply, take the per-(segment, energy) form. NULL keeps
+     * the per-(segment, energy) form throughout. */
+    void *work;
+    int64_t work_bytes;
 } pb_brem_args;
 
 /* Characteristic lines of one emitting element: per-segment shell
@@ -460,6 +469,11 @@ int pb_cxr_score(const pb_cxr_args *args, void *stream);
 
 /* Bethe-Heitler + Elwert track-length bremsstrahlung of a segment list. */
 int pb_brem_score(const pb_brem_args *args, void *stream);
+
+/* Workspace bytes the depth-node form of pb_brem_score needs for these
+ * arguments (precision, n_el, n_E, n_seg, n_layer): 0 where the form does
+ * not apply (FP64, layered absorbers, more than two elements). */
+int pb_brem_work_size(const pb_brem_args *args, int64_t *bytes);
 
 /* Characteristic line yields of a segment list (accumulated). */
 int pb_char_yields(const pb_char_args *args, void *stream);

@@ -128,7 +128,7 @@ class PbBremArgs(C.Structure):
         ("elec_id", _vp), ("n_seg_device", _vp), ("n_el", _i32), ("Z", _vp), ("n_ang3", _vp),
         ("n_E", _i32), ("E_grid", _vp), ("mu", _vp), ("spec", _vp), ("status", _vp),
         ("n_layer", _i32), ("z_top", _vp), ("z_bot", _vp), ("mu_layer", _vp), ("seg_layer", _vp),
-        ("emit_layer", _i32),
+        ("emit_layer", _i32), ("work", _vp), ("work_bytes", _i64),
     ]
 
 
@@ -210,6 +210,7 @@ EXPORTS = (
     "pb_transport",
     "pb_cxr_score",
     "pb_brem_score",
+    "pb_brem_work_size",
     "pb_cxr_score_noalloc",
     "pb_char_yields",
     "pb_char_spectrum",
@@ -244,7 +245,7 @@ class PyriteB200Error(RuntimeError):
     """A pyrite_b200 C-ABI call returned a non-zero status."""
 
 
-ABI_VERSION = 5  # PB_ABI_VERSION of include/pyrite_b200.h
+ABI_VERSION = 6  # PB_ABI_VERSION of include/pyrite_b200.h
 
 
 def load(path: Path | None = None):
@@ -268,6 +269,7 @@ def load(path: Path | None = None):
     lib.pb_transport.argtypes = [C.POINTER(PbTransportArgs), _vp]
     lib.pb_cxr_score.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_brem_score.argtypes = [C.POINTER(PbBremArgs), _vp]
+    lib.pb_brem_work_size.argtypes = [C.POINTER(PbBremArgs), C.POINTER(_i64)]
     lib.pb_cxr_score_noalloc.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_char_yields.argtypes = [C.POINTER(PbCharArgs), _vp]
     lib.pb_char_spectrum.argtypes = [_i32, _i32, _i32, _vp, _vp, _vp, _vp]

@@ -573,7 +573,7 @@ def mc_cxr_spectrum(segments, E_grid_eV, crystal, hkl_list, *, tables: LineTable
 
 
 def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu=None, precision="fp64",
-                     layers=None, mu_layer=None, emit_layer=None, device=None, stream=None):
+                     layers=None, mu_layer=None, emit_layer=None, device=None, stream=None, depth_nodes=True):
     """Bethe-Heitler + Elwert continuum density [photons/eV/sr/electron].
 
     ``mu`` is the absorber's total attenuation [1/Angstrom] on ``E_grid_eV``
@@ -583,6 +583,11 @@ def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu=None, precis
     absorber (brem.py:978-1005); ``composition`` is then the emitting layer's
     and ``emit_layer`` keeps only that layer's segments radiating
     (runner/emission.py:155-172).
+
+    ``depth_nodes`` (mixed precision, single slab, one or two elements) lets
+    the scorer take the segments of the batch's top electron-energy window
+    in the depth-node form; False keeps the per-(segment, energy) form for
+    every segment.
     """
     from .tables import ELEMENTS
 
@@ -627,6 +632,11 @@ def mc_brem_spectrum(segments, E_grid_eV, *, composition, n_hat, mu=None, precis
     spec = h.zeros((n_dir, n_E), torch.float64)
     a.spec = _ptr(spec)
     a.status = _ptr(h.zeros(1, torch.int32))
+    if depth_nodes:
+        nb = C.c_int64(0)
+        L.check(lib.pb_brem_work_size(C.byref(a), C.byref(nb)), "pb_brem_work_size")
+        if nb.value > 0:
+            a.work, a.work_bytes = _ptr(h.empty(int(nb.value), torch.uint8)), int(nb.value)
     L.check(lib.pb_brem_score(C.byref(a), _stream_ptr(stream)), "pb_brem_score")
     torch.cuda.synchronize(dev)
     out = spec.cpu().numpy() / (4.0 * np.pi) / int(segments["Ne"])

@@ -29,7 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 PER_FILE = {
     "pb_transport.cu": ["-fmad=false"],
 }
-SOURCES = ["pb_capi.cu", "pb_transport.cu", "pb_cxr.cu", "pb_brem.cu", "pb_char.cu", "pb_mlp.cu", "pb_coherent.cu"]
+SOURCES = ["pb_capi.cu", "pb_transport.cu", "pb_cxr.cu", "pb_brem.cu", "pb_brem_node.cu", "pb_char.cu", "pb_mlp.cu", "pb_coherent.cu"]
 
 
 def nvcc() -> str:

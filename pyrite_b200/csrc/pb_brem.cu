@@ -16,6 +16,7 @@
 // reference's direct difference.
 #include <cstdint>
 
+#include "pb_brem_node.cuh"
 #include "pb_common.cuh"
 #include "pb_internal.h"
 #include "pb_layers.cuh"
@@ -414,7 +415,8 @@ struct MomentOrder {
 
 template <int NEL>
 __global__ void __launch_bounds__(kBremPackedThreads, 3)
-    brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
+    brem_moment_packed_kernel(const pb_brem_args a, int64_t n_seg, int d0, const BremNodeHdr *nh,
+                              const int64_t *nidx) {
     __shared__ BremSeg<float> segs[kBremChunk];
     __shared__ double sQ[8][kBremPackedThreads];  // FP64 moment sums: [energy half * 4 + n][thread]
     __shared__ float sT[3][kBremPackedThreads / 32];  // the chunk's electron energy range, per warp
@@ -480,6 +482,12 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
     const bool act_a = kd[0] > 0.0, act_b = kd[1] > 0.0;
     int64_t live = n_seg;
     if (a.n_seg_device && (int64_t)*a.n_seg_device < live) live = (int64_t)*a.n_seg_device;
+    // With the depth-node form active, only the segments it left out.
+    const int64_t *sidx = nullptr;
+    if (nh != nullptr && nh->ok) {
+        live = (int64_t)nh->n_out;
+        sidx = nidx;
+    }
     const int64_t per = (live + gridDim.y - 1) / gridDim.y;
     const int64_t s_begin = per * blockIdx.y;
     int64_t s_end = s_begin + per < live ? s_begin + per : live;
@@ -489,7 +497,7 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
         __syncthreads();
         float tlo = 3.4e38f, thi = -3.4e38f, nmax = 0.0f;
         for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-            brem_stage<float>(segs[j], a, c0s + j, T_slab, mc2, za);
+            brem_stage<float>(segs[j], a, sidx ? sidx[c0s + j] : c0s + j, T_slab, mc2, za);
             tlo = fminf(tlo, segs[j].T);
             thi = fmaxf(thi, segs[j].T);
             nmax = fmaxf(nmax, segs[j].nL[0]);
@@ -679,7 +687,7 @@ __global__ void __launch_bounds__(kBremPackedThreads, 3)
 
 template <class Real, int NEL>
 __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
-    brem_kernel(const pb_brem_args a, int64_t n_seg, int d0) {
+    brem_kernel(const pb_brem_args a, int64_t n_seg, int d0, const BremNodeHdr *nh, const int64_t *nidx) {
     // Segment chunk staged in shared memory (half as many FP64 segments, to
     // stay within the static shared-memory limit next to the accumulators).
     constexpr int kChunk = sizeof(Real) == 4 ? kBremChunk : kBremChunk / 2;
@@ -761,6 +769,12 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         const int64_t live = (int64_t)*a.n_seg_device;
         if (live < n_seg) n_seg = live;
     }
+    // With the depth-node form active, only the segments it left out.
+    const int64_t *sidx = nullptr;
+    if (nh != nullptr && nh->ok) {
+        n_seg = (int64_t)nh->n_out;
+        sidx = nidx;
+    }
     // Slices of the live segments (the count read on the device), so every
     // block of the wave has work.
     const int64_t per = (n_seg + gridDim.y - 1) / gridDim.y;
@@ -771,7 +785,7 @@ __global__ void __launch_bounds__(kBremThreads, sizeof(Real) == 4 ? 4 : 2)
         const int nc = (int)((s_end - c0s) < kChunk ? (s_end - c0s) : kChunk);
         __syncthreads();
         for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-            brem_stage<Real>(segs[j], a, c0s + j, T_slab, mc2, za);
+            brem_stage<Real>(segs[j], a, sidx ? sidx[c0s + j] : c0s + j, T_slab, mc2, za);
         }
         __syncthreads();
         if (!on) continue;
@@ -1059,10 +1073,19 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
         return cudaSuccess;
     }
     int64_t n_seg = a.n_seg;
+    // Mixed precision with a workspace: the depth-node form first; the
+    // per-(segment, energy) kernels below then take only the segments it left
+    // out (all of them where it does not apply on the device).
+    const BremNodeHdr *nh = nullptr;
+    const int64_t *nidx = nullptr;
+    if (a.precision == PB_MIXED) {
+        const cudaError_t ne = launch_brem_node(a, s, sms, &nh, &nidx);
+        if (ne != cudaSuccess) return ne;
+    }
     const unsigned gx = (unsigned)((a.n_E + kBremThreads - 1) / kBremThreads);
     // One wave: as many segment slices as keep every SM at its resident limit.
     // The kernel instance for this element count (loops over elements unrolled).
-    using Kern = void (*)(const pb_brem_args, int64_t, int);
+    using Kern = void (*)(const pb_brem_args, int64_t, int, const BremNodeHdr *, const int64_t *);
     Kern kern = nullptr;
     if (a.precision == PB_MIXED) {
         const Kern t[kBremMaxEl] = {brem_kernel<float, 1>, brem_kernel<float, 2>, brem_kernel<float, 3>,
@@ -1104,11 +1127,11 @@ cudaError_t launch_brem(const pb_brem_args &a, cudaStream_t s, int sms) {
     }
     for (int d0 = 0; d0 < a.n_dir; d0 += kBremMaxDir) {
         if (packed) {
-            packed<<<pgrid, kBremPackedThreads, 0, s>>>(a, n_seg, d0);
+            packed<<<pgrid, kBremPackedThreads, 0, s>>>(a, n_seg, d0, nh, nidx);
             cudaError_t err = cudaGetLastError();
             if (err != cudaSuccess) return err;
         }
-        kern<<<grid, kBremThreads, 0, s>>>(a, n_seg, d0);
+        kern<<<grid, kBremThreads, 0, s>>>(a, n_seg, d0, nh, nidx);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "pb_brem_node.cuh"
 #include "pb_internal.h"
 
 namespace {
@@ -188,6 +189,21 @@ static int check_brem(const pb_brem_args *a) {
     if (!a->n_hat || !a->r_mid || !a->v_hat || !a->L || !a->E_keV || !a->elec_id || !a->Z ||
         !a->n_ang3 || !a->E_grid || (!a->mu && a->n_layer == 0) || !a->spec)
         return fail(PB_ERR_INVALID, "pb_brem_score: every pointer must be set");
+    if (a->work != nullptr && pb::brem_node_applies(*a)) {
+        const int64_t need = (int64_t)pb::brem_node_layout(*a).total;
+        if (a->work_bytes < need)
+            return fail(PB_ERR_INVALID, "pb_brem_score: work_bytes %lld below the %lld pb_brem_work_size gives",
+                        (long long)a->work_bytes, (long long)need);
+        if (((uintptr_t)a->work & 15u) != 0) return fail(PB_ERR_INVALID, "pb_brem_score: work is not 16-byte aligned");
+    }
+    return PB_OK;
+}
+
+int pb_brem_work_size(const pb_brem_args *a, int64_t *bytes) {
+    if (!a || !bytes) return fail(PB_ERR_INVALID, "pb_brem_work_size: args or bytes is NULL");
+    if (a->n_seg < 0 || a->n_E < 1 || a->n_el < 1 || a->n_el > 4)
+        return fail(PB_ERR_INVALID, "pb_brem_work_size: need n_seg >= 0, n_E >= 1, 1 <= n_el <= 4");
+    *bytes = pb::brem_node_applies(*a) ? (int64_t)pb::brem_node_layout(*a).total : 0;
     return PB_OK;
 }
 

@@ -192,6 +192,7 @@ class ScoringCase:
         # ---- brem scorer (one argument set per emitting layer) ----
         self.bargs = None
         self.bargs_all = []
+        self.brem_work = []  # depth-node workspaces of the mixed single-slab brem scorer
         brem_sets = []
         if spec.brem_layers:
             brem_sets = [(k, comp) for k, comp in enumerate(spec.brem_layers) if comp]
@@ -229,6 +230,13 @@ class ScoringCase:
                     b.seg_layer, b.emit_layer = _ptr(self.seg_layer), int(k)
                 b.spec = _ptr(self.spec_brem)
                 b.status = _ptr(self.status)
+                # workspace of the depth-node form (mixed single slab; 0 bytes elsewhere)
+                nb = C.c_int64(0)
+                L.check(self.lib.pb_brem_work_size(C.byref(b), C.byref(nb)), "pb_brem_work_size")
+                if nb.value > 0:
+                    wk = h.empty(int(nb.value), torch.uint8)
+                    b.work, b.work_bytes = _ptr(wk), int(nb.value)
+                    self.brem_work.append(wk)
                 self.bargs_all.append(b)
             self.bargs = self.bargs_all[0]
         # ---- characteristic lines (one argument set per emitter) ----
@@ -635,7 +643,9 @@ class ScoringCase:
 
     def kernel_launches_per_batch(self) -> int:
         """This library's kernels launched per batch (transport 1, CXR 2 with
-        the far-field finalize, brem one per 16 directions)."""
+        the far-field finalize; brem: FP64 one per 16 directions, mixed two per
+        16 directions plus the depth-node form's five where it has a
+        workspace)."""
         if getattr(self, "surrogates", None):
             n = 1 + len(self.surrogates) * (2 if self.sur_stride > 0 else 1)
             if self.sur_stride > 0:
@@ -645,9 +655,26 @@ class ScoringCase:
                 n += 1 + (1 if self._fb_args.exact_widths > 0 else 0)
         else:
             n = 1 + sum(1 + (1 if ca.exact_widths > 0 else 0) for ca in self.cargs_all)
-        n += len(self.bargs_all) * ((self.n_dir + 15) // 16)
+        per_group = 2 if self.precision == L.PB_MIXED else 1
+        n += len(self.bargs_all) * per_group * ((self.n_dir + 15) // 16) + 5 * len(self.brem_work)
         n += len(self.chargs_all)
         return n
+
+    def brem_node_state(self) -> list:
+        """Launch state of the depth-node bremsstrahlung form after the last
+        batch, per workspace: whether it scored the batch (``ok``), how many
+        radiating segments it left to the per-(segment, energy) form
+        (``left_out``), its depth cells and its electron-energy window [keV]
+        (the header ``BremNodeHdr`` at the start of the workspace)."""
+        out = []
+        for wk in self.brem_work:
+            raw = wk[:88].cpu().numpy()
+            u64 = raw[:24].view(np.uint64)
+            u32 = raw[24:40].view(np.uint32)
+            f64 = raw[40:88].view(np.float64)
+            out.append({"ok": bool(u32[0]), "left_out": int(u64[2]), "faces": int(u32[1]),
+                        "n_cells": int(u32[2]), "T_lo_keV": float(f64[0]), "T_hi_keV": float(f64[1])})
+        return out
 
     def device_status(self) -> int:
         return int(self.status.item())

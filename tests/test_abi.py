@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(L.EXPORTS)
     for name in names:
         assert hasattr(lib, name), name
-    assert lib.pb_abi_version() == L.ABI_VERSION == 5
+    assert lib.pb_abi_version() == L.ABI_VERSION == 6
 
 
 STRUCTS = {
