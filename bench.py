@@ -61,6 +61,10 @@ MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_t
     if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
 MEASURED_HBM_GBS = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]) \
     if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+# cxr_kernel<float> at the size of the control variate's sub-sample (4 exact widths, 14,395 segments,
+# everything L2-resident): DRAM bytes (read + write) per segment from one ncu capture
+# (profiles/cxr_kernel_subsample_si50_437hist.md): 2.857 MB per launch.
+DRAM_BYTES_PER_SUBSAMPLE_SEGMENT = 2.857e6 / 14395
 # Depth-node bremsstrahlung: the segment fields its passes read per segment (electron energy,
 # length, z of the midpoint, v_z, electron id: 5 x 8 B); nothing per (segment, energy).
 NODE_BYTES_PER_SEGMENT = 40.0
@@ -683,7 +687,12 @@ def main():
         train_s = time.perf_counter() - t0
         cs = ScoringCase(spec, precision="mixed", rng="philox", lut=True, batch_histories=H)
         cs.use_surrogate([model], exact_stride=args.exact_stride, sample_exact_widths=args.cv_exact_widths)
+        sub_counters = torch.zeros(2, dtype=torch.int64, device="cuda")
+        cs.cargs_s.counters = sub_counters.data_ptr()  # the sub-sample scorer's lines and items (comparison pass)
         compare_pass("surrogate", cs)
+        cs.cargs_s.counters = None
+        sub_work = {"lines_kept": int(sub_counters[0].item()), "deposit_items": int(sub_counters[1].item()),
+                    "segments": int(cs.smp["count"].item()) * C}  # approximate: last batch's count x C
         gate_report = compare["surrogate"]["report"]
         arm("surrogate", cs, args.steps)
         form = ("MLP 6 -> 4x256 SiLU -> 512 bins per (segment, tile) pair" if model.n_tiles == 1 else
@@ -880,6 +889,28 @@ def main():
             "frac": inf_tflops / MEASURED_BF16_SUSTAINED,
             "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
             "traffic": None if tiles_form else DRAM_BYTES_PER_HISTORY["mlp_infer_kernel"] * H}
+        # The exact control variate as it runs in the step: every exact_stride-th
+        # segment through cxr_kernel<float> with the narrow exact window, plus
+        # the segment sampler and the far-field convolution, all inside t_sample.
+        n_sub = int(cases["surrogate"].smp["count"].item())
+        sub_pairs = n_sub * n_g * n_dir
+        sub_tflops = sub_pairs * ALG_FLOPS_PAIR / (t_sample / 1e3) / 1e12
+        sub_items = sub_work["deposit_items"] / max(1.0, sub_work["segments"] * n_g * n_dir)
+        sub_tflops_dep = sub_pairs * (ALG_FLOPS_PAIR + sub_items * ALG_FLOPS_ITEM) / (t_sample / 1e3) / 1e12
+        rooflines["cxr_subsample"] = {
+            "bound": "fp32",
+            "kernel": "cxr_kernel<float> on the exact sub-sample (every %d-th segment, %g first-zero widths of "
+                      "exact bin means) with the segment sampler and the far-field convolution"
+                      % (args.exact_stride, args.cv_exact_widths),
+            "achieved": sub_tflops, "peak": peak_fp32, "unit": "TFLOP/s", "frac": sub_tflops / peak_fp32,
+            "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 lanes x 2 x 1.965 GHz)",
+            "census": "%g FP32 flops per (segment, reflection, tile) pair" % ALG_FLOPS_PAIR,
+            "pairs_per_step": sub_pairs,
+            "with_deposit": {"achieved": sub_tflops_dep, "frac": sub_tflops_dep / peak_fp32,
+                             "items_per_pair": sub_items, "lines_kept": sub_work["lines_kept"],
+                             "deposit_items": sub_work["deposit_items"],
+                             "census": "%g per pair + %g per (line, bin) item" % (ALG_FLOPS_PAIR, ALG_FLOPS_ITEM)},
+            "traffic": (DRAM_BYTES_PER_SUBSAMPLE_SEGMENT * n_sub if DRAM_BYTES_PER_SUBSAMPLE_SEGMENT else None)}
         sur["kernel_ms"] = {"transport": results["surrogate"]["t_tr"], "exact_subsample": t_sample,
                             "surrogate_infer": t_inf, "brem": results["surrogate"]["t_brem"]}
         sur["value"], sur["ms_per_step"] = rate("surrogate")
@@ -890,7 +921,7 @@ def main():
         cands = [("brem_kernel", r_head["t_brem"]), ("cxr_kernel", r_head["t_cxr"])]
     else:
         t_sample, t_inf = cases["surrogate"].t_split
-        cands = [("brem_kernel", r_head["t_brem"]), ("mlp_infer_kernel", t_inf), ("cxr_kernel", t_sample)]
+        cands = [("brem_kernel", r_head["t_brem"]), ("mlp_infer_kernel", t_inf), ("cxr_subsample", t_sample)]
     dominant = max(cands, key=lambda kv: kv[1])[0]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
