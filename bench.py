@@ -61,10 +61,10 @@ MEASURED_BF16_SUSTAINED = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_t
     if (ROOT / "MEASURED_PEAKS.json").exists() else 1400.0
 MEASURED_HBM_GBS = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]) \
     if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
-# cxr_kernel<float> at the size of the control variate's sub-sample (4 exact widths, 14,395 segments,
-# everything L2-resident): DRAM bytes (read + write) per segment from one ncu capture
-# (profiles/cxr_kernel_subsample_si50_437hist.md): 2.857 MB per launch.
-DRAM_BYTES_PER_SUBSAMPLE_SEGMENT = 2.857e6 / 14395
+# cxr_kernel<float> on the control variate's sub-sample (4 exact widths, ~14,560 segments, L2-resident):
+# DRAM bytes (read + write) per sampled segment from the one-pass ncu capture of the bench's own
+# sub-sample launches (profiles/cxr_kernel_subsample_si50_65536hist.md): 2.80-2.98 MB per launch.
+DRAM_BYTES_PER_SUBSAMPLE_SEGMENT = 2.9e6 / 14560
 # Depth-node bremsstrahlung: the segment fields its passes read per segment (electron energy,
 # length, z of the midpoint, v_z, electron id: 5 x 8 B); nothing per (segment, energy).
 NODE_BYTES_PER_SEGMENT = 40.0
