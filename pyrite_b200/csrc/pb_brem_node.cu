@@ -47,6 +47,7 @@ namespace {
 constexpr double kNodeMc2 = 510.99895;
 constexpr int kNodeThreads = 256;
 constexpr int kContractThreads = 128;
+constexpr int kNodeTile = 1024;  // segments a block orders by depth cell at a time
 
 __device__ __forceinline__ bool node_radiates(const pb_brem_args &a, int64_t s) {
     return a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
@@ -293,6 +294,10 @@ __global__ void __launch_bounds__(kNodeThreads, 2) brem_node_accum_kernel(const 
     float *Ss = reinterpret_cast<float *>(node_smem + sizeof(double) * kWarps * (NEL + 1) * 32 * kNodeRow);
     __shared__ double zb_s[kNodeMaxCells + 1];
     __shared__ double mid_s[kNodeMaxCells], ihw_s[kNodeMaxCells];  // cell centre and 2 / width
+    __shared__ unsigned short ord_s[kNodeTile];   // the tile's window segments in cell order
+    __shared__ unsigned char key_s[kNodeTile];    // start cell per segment (kNodeMaxCells: not in the window)
+    __shared__ int cnt_s[kNodeMaxCells + 1];
+    __shared__ int n_in_s;
     __shared__ double prm[6];
     __shared__ int go_s, nc_s;
     __shared__ unsigned int faces_s;
@@ -326,123 +331,171 @@ __global__ void __launch_bounds__(kNodeThreads, 2) brem_node_accum_kernel(const 
     const unsigned int lane = tid & 31;
     const int warp = tid >> 5;
     const int grow = (int)(lane >> 2), gcol = (int)(lane & 3);  // tile row / column group of this lane
-    const int64_t n_groups = (live + 31) / 32;
-    const int64_t wstride = (int64_t)gridDim.x * kWarps;
-    for (int64_t g = (int64_t)blockIdx.x * kWarps + warp; g < n_groups; g += wstride) {
-        const int64_t s = g * 32 + lane;
-        const bool rad = s < live && node_radiates(a, s);
-        const double T = rad ? a.E_keV[s] : 0.0;
-        const bool in_win = rad && T >= T_lo && T <= T_hi;
-        const bool left = rad && !in_win;
-        const unsigned int lm = __ballot_sync(0xffffffffu, left);
-        if (lm) {
-            const int ld = __ffs(lm) - 1;
-            unsigned long long q0 = 0ULL;
-            if ((int)lane == ld) q0 = atomicAdd(&h->n_out, (unsigned long long)__popc(lm));
-            q0 = __shfl_sync(0xffffffffu, q0, ld);
-            if (left) {
-                const unsigned long long q = q0 + (unsigned long long)__popc(lm & ((1u << lane) - 1u));
-                if (q < (unsigned long long)cap) idx[q] = s;
-                else atomicExch(&h->ok, 0u);  // list full: the per-pair form takes every segment
-            }
-        }
-        double lo = 0.0, hi = 0.0;
-        if (in_win) {
-            const double u = (T - Tc) * inv_Th;
-            const double p_i = sqrt(T * (T + 2.0 * kNodeMc2)) / kNodeMc2;
-            const double b_i = p_i / (1.0 + T / kNodeMc2);
-            const double Lc = a.L[s];
-#pragma unroll
-            for (int el = 0; el < NEL; ++el) {
-                const double Z = a.Z[el];
-                double wp = a.n_ang3[el] * 1e24 * (Lc * 1e-8) * (Z * Z) * (1.0 - exp(-za * Z / b_i));
-#pragma unroll
-                for (int p = 0; p < kNodePts; ++p) {
-                    sW[warp][el][lane][p] = p < kNodeTDeg ? wp : 0.0;
-                    wp *= u;
+    // Tiles of kNodeTile consecutive segments, ordered by the depth cell of
+    // their start on the first face in use (a counting sort in shared
+    // memory), so that the 32 segments a warp takes share their cells and a
+    // round of pieces needs one or two tensor-core products.
+    const int f0 = (faces & 1u) ? 0 : 1;
+    const int64_t n_tiles = (live + kNodeTile - 1) / kNodeTile;
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int64_t t0 = tile * kNodeTile;
+        for (int q = tid; q <= kNodeMaxCells; q += blockDim.x) cnt_s[q] = 0;
+        __syncthreads();
+#pragma unroll 1
+        for (int k = 0; k < kNodeTile / kNodeThreads; ++k) {
+            const int li = k * kNodeThreads + tid;
+            const int64_t s = t0 + li;
+            const bool rad = s < live && node_radiates(a, s);
+            const double T = rad ? a.E_keV[s] : 0.0;
+            const bool in_win = rad && T >= T_lo && T <= T_hi;
+            const bool left = rad && !in_win;
+            const unsigned int lm = __ballot_sync(0xffffffffu, left);
+            if (lm) {
+                const int ld = __ffs(lm) - 1;
+                unsigned long long q0 = 0ULL;
+                if ((int)lane == ld) q0 = atomicAdd(&h->n_out, (unsigned long long)__popc(lm));
+                q0 = __shfl_sync(0xffffffffu, q0, ld);
+                if (left) {
+                    const unsigned long long q = q0 + (unsigned long long)__popc(lm & ((1u << lane) - 1u));
+                    if (q < (unsigned long long)cap) idx[q] = s;
+                    else atomicExch(&h->ok, 0u);  // list full: the per-pair form takes every segment
                 }
             }
-            const double half = 0.5 * Lc;
-            const double zm = a.r_mid[3 * s + 2], vz = a.v_hat[3 * s + 2];
-            const double d0 = fmin(fmax(zm - half * vz, 0.0), T_slab);
-            const double d1 = fmin(fmax(zm + half * vz, 0.0), T_slab);
-            lo = fmin(d0, d1);
-            hi = fmax(d0, d1);
-        }
-#pragma unroll
-        for (int f = 0; f < 2; ++f) {
-            if (!((faces >> f) & 1u)) continue;
-            const double za_ = f == 0 ? lo : T_slab - hi;
-            const double zb_ = f == 0 ? hi : T_slab - lo;
-            int c = 0, cend = -1;
-            bool point = false;
-            double inv_len = 0.0;
+            int key = kNodeMaxCells;  // outside the window: after every cell
             if (in_win) {
-                c = node_cell(zb_s, nc, h_min, z_g, za_);
-                point = !(zb_ - za_ > 1e-9 * (zb_s[c + 1] - zb_s[c]));
-                cend = point ? c : node_cell(zb_s, nc, h_min, z_g, zb_);
-                inv_len = point ? 0.0 : 1.0 / (zb_ - za_);
+                const double half = 0.5 * a.L[s];
+                const double zm = a.r_mid[3 * s + 2], vz = a.v_hat[3 * s + 2];
+                const double d0 = fmin(fmax(zm - half * vz, 0.0), T_slab);
+                const double d1 = fmin(fmax(zm + half * vz, 0.0), T_slab);
+                const double zs = f0 == 0 ? fmin(d0, d1) : T_slab - fmax(d0, d1);
+                key = node_cell(zb_s, nc, h_min, z_g, zs);
             }
-            while (__any_sync(0xffffffffu, c <= cend)) {
-                const bool have = c <= cend;
-                double M[kNodePts];
-#pragma unroll
-                for (int j = 0; j < kNodePts; ++j) M[j] = 0.0;
-                if (have) {
-                    const double mid = mid_s[c], ihw = ihw_s[c];
-                    if (point) {
-                        const double t = fmin(fmax((za_ - mid) * ihw, -1.0), 1.0);
-                        M[0] = 1.0;
-#pragma unroll
-                        for (int j = 1; j < kNodePts; ++j) M[j] = M[j - 1] * t;
-                    } else {
-                        const double oa = fmax(za_, zb_s[c]), ob = fmin(zb_, zb_s[c + 1]);
-                        if (ob > oa) {
-                            const double ta = fmin(fmax((oa - mid) * ihw, -1.0), 1.0);
-                            const double tb = fmin(fmax((ob - mid) * ihw, -1.0), 1.0);
-                            const double frac = (ob - oa) * inv_len;
-                            // D_1 = 1, D_{n+1} = t_b D_n + t_a^n; mean of t^j = frac D_{j+1} / (j + 1)
-                            double D = 1.0, tan = ta;
-                            M[0] = frac;
-#pragma unroll
-                            for (int j = 1; j < kNodePts; ++j) {
-                                D = fma(tb, D, tan);
-                                tan *= ta;
-                                M[j] = frac * D / (double)(j + 1);
+            key_s[li] = (unsigned char)key;
+            atomicAdd(&cnt_s[key], 1);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int run = 0;
+            for (int c = 0; c <= kNodeMaxCells; ++c) {
+                const int v = cnt_s[c];
+                cnt_s[c] = run;
+                run += v;
+            }
+            n_in_s = cnt_s[kNodeMaxCells];
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int k = 0; k < kNodeTile / kNodeThreads; ++k) {
+            const int li = k * kNodeThreads + tid;
+            const int pos = atomicAdd(&cnt_s[key_s[li]], 1);
+            ord_s[pos] = (unsigned short)li;
+        }
+        __syncthreads();
+        const int n_in = n_in_s;
+        for (int g = warp; g * 32 < n_in; g += kWarps) {
+            const int pos = g * 32 + (int)lane;
+            const bool in_win = pos < n_in;
+            const int64_t s = in_win ? t0 + ord_s[pos] : 0;
+            const double T = in_win ? a.E_keV[s] : 0.0;
+            double lo = 0.0, hi = 0.0;
+            if (in_win) {
+                const double u = (T - Tc) * inv_Th;
+                const double p_i = sqrt(T * (T + 2.0 * kNodeMc2)) / kNodeMc2;
+                const double b_i = p_i / (1.0 + T / kNodeMc2);
+                const double Lc = a.L[s];
+    #pragma unroll
+                for (int el = 0; el < NEL; ++el) {
+                    const double Z = a.Z[el];
+                    double wp = a.n_ang3[el] * 1e24 * (Lc * 1e-8) * (Z * Z) * (1.0 - exp(-za * Z / b_i));
+    #pragma unroll
+                    for (int p = 0; p < kNodePts; ++p) {
+                        sW[warp][el][lane][p] = p < kNodeTDeg ? wp : 0.0;
+                        wp *= u;
+                    }
+                }
+                const double half = 0.5 * Lc;
+                const double zm = a.r_mid[3 * s + 2], vz = a.v_hat[3 * s + 2];
+                const double d0 = fmin(fmax(zm - half * vz, 0.0), T_slab);
+                const double d1 = fmin(fmax(zm + half * vz, 0.0), T_slab);
+                lo = fmin(d0, d1);
+                hi = fmax(d0, d1);
+            }
+    #pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                if (!((faces >> f) & 1u)) continue;
+                const double za_ = f == 0 ? lo : T_slab - hi;
+                const double zb_ = f == 0 ? hi : T_slab - lo;
+                int c = 0, cend = -1;
+                bool point = false;
+                double inv_len = 0.0;
+                if (in_win) {
+                    c = node_cell(zb_s, nc, h_min, z_g, za_);
+                    point = !(zb_ - za_ > 1e-9 * (zb_s[c + 1] - zb_s[c]));
+                    cend = point ? c : node_cell(zb_s, nc, h_min, z_g, zb_);
+                    inv_len = point ? 0.0 : 1.0 / (zb_ - za_);
+                }
+                while (__any_sync(0xffffffffu, c <= cend)) {
+                    const bool have = c <= cend;
+                    double M[kNodePts];
+    #pragma unroll
+                    for (int j = 0; j < kNodePts; ++j) M[j] = 0.0;
+                    if (have) {
+                        const double mid = mid_s[c], ihw = ihw_s[c];
+                        if (point) {
+                            const double t = fmin(fmax((za_ - mid) * ihw, -1.0), 1.0);
+                            M[0] = 1.0;
+    #pragma unroll
+                            for (int j = 1; j < kNodePts; ++j) M[j] = M[j - 1] * t;
+                        } else {
+                            const double oa = fmax(za_, zb_s[c]), ob = fmin(zb_, zb_s[c + 1]);
+                            if (ob > oa) {
+                                const double ta = fmin(fmax((oa - mid) * ihw, -1.0), 1.0);
+                                const double tb = fmin(fmax((ob - mid) * ihw, -1.0), 1.0);
+                                const double frac = (ob - oa) * inv_len;
+                                // D_1 = 1, D_{n+1} = t_b D_n + t_a^n; mean of t^j = frac D_{j+1} / (j + 1)
+                                double D = 1.0, tan = ta;
+                                M[0] = frac;
+    #pragma unroll
+                                for (int j = 1; j < kNodePts; ++j) {
+                                    D = fma(tb, D, tan);
+                                    tan *= ta;
+                                    M[j] = frac * D / (double)(j + 1);
+                                }
                             }
                         }
                     }
-                }
-#pragma unroll
-                for (int j = 0; j < kNodePts; ++j) sM[warp][lane][j] = M[j];
-                __syncwarp();
-                const int key = have ? c : -1;
-                unsigned int pending = __ballot_sync(0xffffffffu, have);
-                while (pending) {
-                    const int ld = __ffs(pending) - 1;
-                    const int K = __shfl_sync(0xffffffffu, key, ld);
-                    const unsigned int grp = __ballot_sync(0xffffffffu, have && key == K);
-                    pending &= ~grp;
-#pragma unroll
-                    for (int el = 0; el < NEL; ++el) {
-                        double d0 = 0.0, d1 = 0.0;
-#pragma unroll
-                        for (int st = 0; st < 8; ++st) {
-                            const int l = 4 * st + gcol;
-                            const double av = ((grp >> l) & 1u) ? sW[warp][el][l][grow] : 0.0;
-                            dmma_884(d0, d1, av, sM[warp][l][grow]);
-                        }
-                        if (grow < kNodeTDeg) {
-                            float *row = Ss + ((el * 2 + f) * kNodeMaxCells + K) * kNodePJ + grow * kNodePts + 2 * gcol;
-                            if (d0 != 0.0) atomicAdd(row, (float)d0);
-                            if (d1 != 0.0) atomicAdd(row + 1, (float)d1);
+    #pragma unroll
+                    for (int j = 0; j < kNodePts; ++j) sM[warp][lane][j] = M[j];
+                    __syncwarp();
+                    const int key = have ? c : -1;
+                    unsigned int pending = __ballot_sync(0xffffffffu, have);
+                    while (pending) {
+                        const int ld = __ffs(pending) - 1;
+                        const int K = __shfl_sync(0xffffffffu, key, ld);
+                        const unsigned int grp = __ballot_sync(0xffffffffu, have && key == K);
+                        pending &= ~grp;
+    #pragma unroll
+                        for (int el = 0; el < NEL; ++el) {
+                            double d0 = 0.0, d1 = 0.0;
+    #pragma unroll
+                            for (int st = 0; st < 8; ++st) {
+                                const int l = 4 * st + gcol;
+                                const double av = ((grp >> l) & 1u) ? sW[warp][el][l][grow] : 0.0;
+                                dmma_884(d0, d1, av, sM[warp][l][grow]);
+                            }
+                            if (grow < kNodeTDeg) {
+                                float *row = Ss + ((el * 2 + f) * kNodeMaxCells + K) * kNodePJ + grow * kNodePts + 2 * gcol;
+                                if (d0 != 0.0) atomicAdd(row, (float)d0);
+                                if (d1 != 0.0) atomicAdd(row + 1, (float)d1);
+                            }
                         }
                     }
+                    __syncwarp();
+                    ++c;
                 }
-                __syncwarp();
-                ++c;
             }
         }
+        __syncthreads();  // the next tile reuses the order
     }
     __syncthreads();
     const int per = nc * kNodePJ;
