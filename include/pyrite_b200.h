@@ -539,6 +539,13 @@ int pb_mlp_pack(int32_t rows, int32_t cols, const float *W, void *Wb, int32_t ld
 int pb_segments_sample(const pb_segments *src, int64_t stride, const pb_segments *dst, unsigned int *status,
                        void *stream);
 
+/* Copy n device byte ranges in one launch: desc (device memory) holds n
+ * triples (source address, destination address, bytes) as int64. Ranges must
+ * not overlap. The host API moves a step's scattered inputs and outputs
+ * through one staging buffer each with it, so a step crosses the host link
+ * in one copy each way. */
+int pb_copy_segments(int32_t n, const int64_t *desc, void *stream);
+
 /* Surrogate inference (above). */
 int pb_mlp_infer(const pb_mlp_infer_args *args, void *stream);
 /* The inference kernel's inputs as a matrix, for training: X bf16

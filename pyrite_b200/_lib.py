@@ -211,6 +211,7 @@ EXPORTS = (
     "pb_cxr_score",
     "pb_brem_score",
     "pb_brem_work_size",
+    "pb_copy_segments",
     "pb_cxr_score_noalloc",
     "pb_char_yields",
     "pb_char_spectrum",
@@ -270,6 +271,7 @@ def load(path: Path | None = None):
     lib.pb_cxr_score.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_brem_score.argtypes = [C.POINTER(PbBremArgs), _vp]
     lib.pb_brem_work_size.argtypes = [C.POINTER(PbBremArgs), C.POINTER(_i64)]
+    lib.pb_copy_segments.argtypes = [_i32, _vp, _vp]
     lib.pb_cxr_score_noalloc.argtypes = [C.POINTER(PbCxrArgs), _vp]
     lib.pb_char_yields.argtypes = [C.POINTER(PbCharArgs), _vp]
     lib.pb_char_spectrum.argtypes = [_i32, _i32, _i32, _vp, _vp, _vp, _vp]

@@ -366,6 +366,36 @@ int pb_segments_sample(const pb_segments *src, int64_t stride, const pb_segments
     return PB_OK;
 }
 
+namespace {
+// One block per range (grid-strided): 16-byte moves where both ends and the
+// length allow, bytes otherwise.
+__global__ void __launch_bounds__(256) copy_segments_kernel(int n, const int64_t *desc) {
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(desc[3 * k]);
+        unsigned char *dst = reinterpret_cast<unsigned char *>(desc[3 * k + 1]);
+        const int64_t nb = desc[3 * k + 2];
+        int64_t done = 0;
+        if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
+            const int64_t n16 = nb >> 4;
+            for (int64_t i = threadIdx.x; i < n16; i += blockDim.x)
+                reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+            done = n16 << 4;
+        }
+        for (int64_t i = done + threadIdx.x; i < nb; i += blockDim.x) dst[i] = src[i];
+    }
+}
+}  // namespace
+
+int pb_copy_segments(int32_t n, const int64_t *desc, void *stream) {
+    if (n < 0 || (n > 0 && !desc)) return fail(PB_ERR_INVALID, "pb_copy_segments: need n >= 0 and desc");
+    if (n == 0) return PB_OK;
+    const int grid = n < 4 * device_sms() ? n : 4 * device_sms();
+    copy_segments_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, desc);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "pb_copy_segments: launch");
+    return PB_OK;
+}
+
 int pb_mlp_infer(const pb_mlp_infer_args *a, void *stream) {
     if (!a) return fail(PB_ERR_INVALID, "pb_mlp_infer: args is NULL");
     if (a->n_seg < 0 || a->n_dir < 1) return fail(PB_ERR_INVALID, "pb_mlp_infer: need n_seg >= 0, n_dir >= 1");

@@ -744,8 +744,12 @@ def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 
                        exact_stride=50, tol=0.01, probe_batches=None, sample_exact_widths=None) -> dict:
     """End-to-end run through host buffers: every step copies the case's input
     tables from pinned host memory to the device, runs one batch, and reads
-    the spectra and tallies back to pinned host memory. Returns the rate and
-    the bytes moved per step. With ``surrogates`` the PXR+CBS part is the
+    the spectra and tallies back to pinned host memory -- one copy each way
+    through a pinned staging buffer (``pb_copy_segments`` scatters and gathers
+    the case's tensors on the device), double-buffered on two copy streams so
+    that the next step's inputs and this step's results cross the host link
+    while the GPU computes. Returns the rate, the bytes moved per step and the
+    last step's read-back. With ``surrogates`` the PXR+CBS part is the
     surrogate with its exact sub-sample; the per-direction accumulators read
     back each step are the ones its readout needs. The surrogate's error
     probe runs on the warm-up batches (``probe_batches`` defaults to the
@@ -756,7 +760,7 @@ def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 
         probe = max(2, int(warmup)) if probe_batches is None else int(probe_batches)
         case.use_surrogate(surrogates, exact_stride=exact_stride, tol=tol, probe_batches=probe,
                            sample_exact_widths=sample_exact_widths)
-    pairs = [(t.cpu().pin_memory(), t) for t in case.h.inputs]
+    ins = list(case.h.inputs)
     if surrogates:
         outs = case.sur_hsum + case.sur_lsum + case.sur_hsum_s + case.sur_lsum_s
         outs += [case.spec_sample] if case.sur_stride > 0 else []
@@ -766,28 +770,90 @@ def simulate_case_host(spec: CaseSpec, histories_per_step: int, *, steps: int = 
     if case.bargs is not None:
         outs.append(case.spec_brem)
     outs += case.char_yields
-    host_out = [torch.empty_like(t, device="cpu").pin_memory() for t in outs]
-    h2d = sum(h.numel() * h.element_size() for h, _ in pairs)
+    h2d = sum(t.numel() * t.element_size() for t in ins)
     d2h = sum(t.numel() * t.element_size() for t in outs)
 
+    # One pinned host staging buffer per direction, 16-byte aligned slots: a
+    # step crosses the host link in one copy each way, and pb_copy_segments
+    # moves the slots to and from the case's tensors on the device. The device
+    # staging buffers are double-buffered, so the next step's inputs cross on
+    # a copy stream while this step computes, and its results leave on another.
+    def layout(tensors):
+        offs, o = [], 0
+        for t in tensors:
+            offs.append(o)
+            o += (t.numel() * t.element_size() + 15) & ~15
+        return offs, max(o, 16)
+
+    in_offs, in_total = layout(ins)
+    out_offs, out_total = layout(outs)
+    dev = case.device
+    stage_h = torch.empty(in_total, dtype=torch.uint8).pin_memory()
+    for t, off in zip(ins, in_offs):
+        nb = t.numel() * t.element_size()
+        stage_h[off:off + nb].copy_(t.detach().reshape(-1).view(torch.uint8).cpu())
+    stage_d = [torch.empty(in_total, dtype=torch.uint8, device=dev) for _ in range(2)]
+    ostage_d = [torch.empty(out_total, dtype=torch.uint8, device=dev) for _ in range(2)]
+    ostage_h = [torch.empty(out_total, dtype=torch.uint8).pin_memory() for _ in range(2)]
+
+    def descriptors(triples):
+        rows = []
+        for src, dst, nb in triples:  # pieces of at most 256 KB spread a large table over blocks
+            for o in range(0, nb, 1 << 18):
+                rows += [src + o, dst + o, min(1 << 18, nb - o)]
+        return torch.tensor(rows, dtype=torch.int64, device=dev).reshape(-1, 3)
+
+    d_in = [descriptors([(stage_d[k].data_ptr() + off, t.data_ptr(), t.numel() * t.element_size())
+                         for t, off in zip(ins, in_offs)]) for k in range(2)]
+    d_out = [descriptors([(t.data_ptr(), ostage_d[k].data_ptr() + off, t.numel() * t.element_size())
+                          for t, off in zip(outs, out_offs)]) for k in range(2)]
+    lib = case.lib
+    main = torch.cuda.current_stream(dev)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    ev = {name: [torch.cuda.Event() for _ in range(2)] for name in ("h2d", "used", "out", "d2h")}
+    for k in range(2):
+        ev["used"][k].record(main)
+        ev["d2h"][k].record(main)
+
     def step(i):
-        for hsrc, dst in pairs:
-            dst.copy_(hsrc, non_blocking=True)
-        case.run_batch(e_start + i * histories_per_step, histories_per_step)
-        for src, hdst in zip(outs, host_out):
-            hdst.copy_(src, non_blocking=True)
+        k = i & 1
+        up.wait_event(ev["used"][k])  # the scatter two steps back has read this buffer
+        with torch.cuda.stream(up):
+            stage_d[k].copy_(stage_h, non_blocking=True)
+        ev["h2d"][k].record(up)
+        main.wait_event(ev["h2d"][k])
+        L.check(lib.pb_copy_segments(int(d_in[k].shape[0]), d_in[k].data_ptr(), main.cuda_stream),
+                "pb_copy_segments")
+        ev["used"][k].record(main)
+        case.run_batch(e_start + i * histories_per_step, histories_per_step, stream=main)
+        main.wait_event(ev["d2h"][k])  # the read-back two steps back has left this buffer
+        L.check(lib.pb_copy_segments(int(d_out[k].shape[0]), d_out[k].data_ptr(), main.cuda_stream),
+                "pb_copy_segments")
+        ev["out"][k].record(main)
+        down.wait_event(ev["out"][k])
+        with torch.cuda.stream(down):
+            ostage_h[k].copy_(ostage_d[k], non_blocking=True)
+        ev["d2h"][k].record(down)
 
     for i in range(warmup):
         step(i)
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
+    t0.record(main)
+    up.wait_event(t0)
     for i in range(steps):
         step(warmup + i)
-    t1.record()
+    for k in range(2):
+        main.wait_event(ev["d2h"][k])
+    t1.record(main)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1) / steps
+    last = ostage_h[(warmup + steps - 1) & 1]
+    result = []
+    for t, off in zip(outs, out_offs):
+        nb = t.numel() * t.element_size()
+        result.append(last[off:off + nb].view(t.dtype).reshape(t.shape).numpy().copy())
     return {"histories_per_s": histories_per_step / (ms / 1e3), "ms_per_step": ms,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "result": [h.numpy().copy() for h in host_out]}
+            "result": result}
