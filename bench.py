@@ -525,7 +525,7 @@ def main():
     ap.add_argument("--surrogate-form", default="tiles", choices=["pairwise", "tiles"],
                     help="pairwise: the direction is an input and every (segment, tile) pair runs the network; "
                          "tiles: one head per detector tile on shared segment features (one pass per segment)")
-    ap.add_argument("--cv-exact-widths", type=float, default=4.0,
+    ap.add_argument("--cv-exact-widths", type=float, default=2.0,
                     help="exact bin-mean window of the control variate's sub-sample scorer, in first-zero widths "
                          "(the exact arms keep the reference's 64)")
     ap.add_argument("--tile-segments", type=int, default=262144, help="training segments of the tiles form")

@@ -390,10 +390,10 @@ class ScoringCase:
         reference's 64). Beyond the window a line's bins take the far-field
         envelope through the moments, which omits only the sinc^2
         oscillation averaged over a bin: on the 50 MeV Si scene the spectrum
-        with 4 widths differs from the one with 64 by 7e-7 of the tile peak
-        (2 widths: 8e-7, 16 widths: 4e-7), against the estimator's per-mille
-        sampling noise, and the sub-sample's scorer takes half the time. The
-        estimate is then unbiased for that scorer's spectrum."""
+        with 2 widths differs from the one with 64 by 8e-7 of the tile peak
+        (4 widths: 7e-7, 16 widths: 4e-7), against the estimator's per-mille
+        sampling noise, and the sub-sample's scorer takes 40 % of the time.
+        The estimate is then unbiased for that scorer's spectrum."""
         from .detector import tile_uv
 
         if self.spec.detector is None or self.spec.angular_shape is None:
