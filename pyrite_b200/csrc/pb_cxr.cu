@@ -349,24 +349,28 @@ struct PairAmps {
     bool keep;
 };
 
-template <class Real, bool kLayered>
-__device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, const RowPre<Real> &rw,
-                                                    const Real *E_tab, const Real *delta_tab, const Real *log_mu,
-                                                    int n_tab, int n_mu, const pb_cxr_tables &t,
-                                                    const TabIndex &ti) {
+// The resonance of a pair: three Snell passes for the refraction at the line
+// energy and the keep decision (delta and denom carry what the amplitude part
+// needs; denom is NaN when the passes did not settle).
+template <class Real>
+struct Resonance {
+    Real delta, denom;
+    bool keep;
+};
+
+template <class Real>
+__device__ __forceinline__ Resonance<Real> pair_resonance(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                                          const Real *E_tab, const Real *delta_tab, int n_tab,
+                                                          const pb_cxr_tables &t, const TabIndex &ti) {
     const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
     const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
     const Real hbarc = (Real)kHbarcEvAng;
-    PairAmps<Real> o;
     // cxr/_block_prologue.py:18-38, cxr/_recoil.py:79-97
     const Real r_num = (Real)0.5 * g2 * sp.inv_E;
     const Real r_den = n_dot_g * sp.inv_E;
     const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
     const Real v_dot_g_exact = v_dot_g - r_num;
     const Real denom_vac = sp.denom_row + r_den;
-    o.r_num = r_num;
-    o.r_den = r_den;
-    o.v_dot_g = v_dot_g;
     // cxr/_kernels.py:702-765
     Real denom = denom_vac, previous = denom, delta = (Real)NAN;
     for (int pass = 0; pass < 3; ++pass) {
@@ -382,6 +386,33 @@ __device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, cons
     bool settled = fabs(denom - previous) <= (Real)1e-3 * fabs(denom);
     settled = settled && ((Real)2 * fabs(delta) * sp.grad2 < (Real)1);
     if (!settled) denom = (Real)NAN;
+    const Real omega = rdiv(v_dot_g - r_num, denom);
+    const Real E_res = hbarc * omega;
+    bool keep = sp.radiates && (E_res > (Real)t.lo_keep) && (E_res > (Real)10) && (E_res < (Real)t.hi_keep);
+    keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - rdiv((Real)1, sp.gamma));
+    return Resonance<Real>{delta, denom, keep};
+}
+
+// The rest of the chain from the resonance: the line's slope, the attenuation
+// at the line energy and the complex amplitudes. The float path stops after
+// the resonance for dropped pairs; FP64 completes every pair so its per-pair
+// output matches the reference's arrays.
+template <class Real, bool kLayered>
+__device__ __forceinline__ PairAmps<Real> pair_amps_from(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                                         const Resonance<Real> &res, const Real *E_tab,
+                                                         const Real *log_mu, int n_tab, int n_mu,
+                                                         const pb_cxr_tables &t, const TabIndex &ti) {
+    const Real Gx = rw.G[0], Gy = rw.G[1], Gz = rw.G[2];
+    const Real g2 = rw.g2, n_dot_g = rw.n_dot_g;
+    const Real hbarc = (Real)kHbarcEvAng;
+    PairAmps<Real> o;
+    const Real r_num = (Real)0.5 * g2 * sp.inv_E;
+    const Real r_den = n_dot_g * sp.inv_E;
+    const Real v_dot_g = sp.vx * Gx + sp.vy * Gy + sp.vz * Gz;
+    o.r_num = r_num;
+    o.r_den = r_den;
+    o.v_dot_g = v_dot_g;
+    const Real delta = res.delta, denom = res.denom;
     const Real n_dot_g_blk = n_dot_g + delta * (sp.gx * Gx + sp.gy * Gy + sp.gz * Gz);
     // cxr/_kernels.py:624-655
     const Real omega = rdiv(v_dot_g - r_num, denom);
@@ -392,18 +423,14 @@ __device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, cons
     const Real k_mag = omega * r_sqrt(sp.grad2 == (Real)0 ? (Real)1
                                                            : (Real)1 - (Real)2 * delta + delta * delta * sp.grad2);
     const Real E_res = hbarc * omega;
-    bool keep = sp.radiates && (E_res > (Real)t.lo_keep) && (E_res > (Real)10) && (E_res < (Real)t.hi_keep);
     o.omega = omega;
     o.E_res = E_res;
     o.mu = (Real)0;
     // cxr/_block_prologue.py:53-62, cxr/_recoil.py:100-118
     o.slope = denom * rdiv((Real)1, (Real)1 - omega * sp.inv_E);
-    keep = keep && (denom > (Real)0) && (omega * sp.inv_E <= (Real)1 - rdiv((Real)1, sp.gamma));
-    o.keep = keep;
+    o.keep = res.keep;
     if constexpr (sizeof(Real) == 4) {
-        // The float path stops here for dropped pairs (FP64 completes every
-        // pair so its per-pair output matches the reference's arrays).
-        if (!keep) return o;
+        if (!res.keep) return o;
     }
     int ix;
     Real fr;
@@ -457,14 +484,23 @@ __device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, cons
     return o;
 }
 
+template <class Real, bool kLayered>
+__device__ __forceinline__ PairAmps<Real> pair_amps(const SegPre<Real> &sp, const RowPre<Real> &rw,
+                                                    const Real *E_tab, const Real *delta_tab, const Real *log_mu,
+                                                    int n_tab, int n_mu, const pb_cxr_tables &t,
+                                                    const TabIndex &ti) {
+    const Resonance<Real> res = pair_resonance<Real>(sp, rw, E_tab, delta_tab, n_tab, t, ti);
+    return pair_amps_from<Real, kLayered>(sp, rw, res, E_tab, log_mu, n_tab, n_mu, t, ti);
+}
+
 // The incoherent line of a pair: resonance, width and weight
 // (cxr/_batched.py:702-730, cxr/_kernels.py:658-668).
 template <class Real, bool kLayered>
-__device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
-                                const Real *E_tab, const Real *delta_tab, const Real *log_mu,
-                                int n_tab, int n_mu, const pb_cxr_tables &t, const TabIndex &ti,
-                                const EscSeg<Real> *es, const pb_cxr_args &a, const Real *lay_t) {
-    const PairAmps<Real> p = pair_amps<Real, kLayered>(sp, rw, E_tab, delta_tab, log_mu, n_tab, n_mu, t, ti);
+__device__ Line<Real> pair_line_from(const SegPre<Real> &sp, const RowPre<Real> &rw, const Resonance<Real> &res,
+                                     const Real *E_tab, const Real *log_mu, int n_tab, int n_mu,
+                                     const pb_cxr_tables &t, const TabIndex &ti, const EscSeg<Real> *es,
+                                     const pb_cxr_args &a, const Real *lay_t) {
+    const PairAmps<Real> p = pair_amps_from<Real, kLayered>(sp, rw, res, E_tab, log_mu, n_tab, n_mu, t, ti);
     Line<Real> out;
     out.good = false;
     out.E_res = p.E_res;
@@ -483,6 +519,15 @@ __device__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw,
     out.weight = pref * A2 * rw.wm;
     out.good = p.keep && isfinite(out.weight) && (out.weight > (Real)0);
     return out;
+}
+
+template <class Real, bool kLayered>
+__device__ __forceinline__ Line<Real> pair_line(const SegPre<Real> &sp, const RowPre<Real> &rw, const Real *E_tab,
+                                                const Real *delta_tab, const Real *log_mu, int n_tab, int n_mu,
+                                                const pb_cxr_tables &t, const TabIndex &ti, const EscSeg<Real> *es,
+                                                const pb_cxr_args &a, const Real *lay_t) {
+    const Resonance<Real> res = pair_resonance<Real>(sp, rw, E_tab, delta_tab, n_tab, t, ti);
+    return pair_line_from<Real, kLayered>(sp, rw, res, E_tab, log_mu, n_tab, n_mu, t, ti, es, a, lay_t);
 }
 
 // ---- sine integral and the sinc^2 antiderivative --------------------------
