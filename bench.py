@@ -983,7 +983,7 @@ def e2e_measure(spec, args, torch, rank, world, dist, surrogates=None):
     """
     from pyrite_b200.pipeline import simulate_case_host
 
-    steps = max(1, args.steps // 2)
+    steps = max(1, args.steps)
     res = simulate_case_host(spec, args.histories, steps=steps, warmup=args.warmup, precision="mixed",
                              e_start=10_000_000 + rank * 10_000_000, surrogates=surrogates,
                              exact_stride=args.exact_stride,
