@@ -162,3 +162,50 @@ def test_blend_and_decoherence_checks_without_a_device():
     d.n_pop = 8
     assert lib.pb_decoherence_factor(C.byref(d), None) == L.PB_ERR_INVALID
     assert b"must be set" in lib.pb_last_error()
+
+
+def _filled_brem_args(precision=None):
+    """A single-slab pb_brem_args with every pointer set (never dereferenced:
+    the calls below stop in the host checks)."""
+    b = L.PbBremArgs()
+    b.precision = L.PB_MIXED if precision is None else precision
+    b.n_dir, b.n_seg, b.n_el, b.n_E, b.Ne = 16, 1000, 1, 2048, 1 << 20
+    b.thickness = 5e6
+    fake = 0x1000
+    for f in ("n_hat", "r_mid", "v_hat", "L", "E_keV", "elec_id", "Z", "n_ang3", "E_grid", "mu", "spec"):
+        setattr(b, f, fake)
+    return b
+
+
+def test_brem_work_size_and_workspace_checks_without_a_device():
+    lib = L.load()
+    nb = C.c_int64(-1)
+    b = _filled_brem_args()
+    assert lib.pb_brem_work_size(C.byref(b), C.byref(nb)) == 0
+    need = nb.value
+    assert need > 0  # mixed, single slab, one element: the depth-node form applies
+    # the workspace grows with the segment capacity (the left-out list)
+    b.n_seg = 100_000
+    nb2 = C.c_int64(0)
+    assert lib.pb_brem_work_size(C.byref(b), C.byref(nb2)) == 0 and nb2.value > need
+    for prec, layers, n_el in ((L.PB_FP64, 0, 1), (L.PB_MIXED, 2, 1), (L.PB_MIXED, 0, 3)):
+        c = _filled_brem_args(prec)
+        c.n_layer, c.n_el = layers, n_el
+        z = C.c_int64(-1)
+        assert lib.pb_brem_work_size(C.byref(c), C.byref(z)) == 0
+        assert z.value == 0, (prec, layers, n_el)  # the form does not apply: no workspace
+    # a workspace below the size, or misaligned, is refused before any launch
+    b = _filled_brem_args()
+    b.work, b.work_bytes = 0x2000, need - 8
+    assert lib.pb_brem_score(C.byref(b), None) == 1
+    assert b"work_bytes" in lib.pb_last_error()
+    b.work, b.work_bytes = 0x2008, need
+    assert lib.pb_brem_score(C.byref(b), None) == 1
+    assert b"aligned" in lib.pb_last_error()
+
+
+def test_copy_segments_checks_without_a_device():
+    lib = L.load()
+    assert lib.pb_copy_segments(-1, None, None) == 1
+    assert lib.pb_copy_segments(3, None, None) == 1
+    assert lib.pb_copy_segments(0, None, None) == 0  # nothing to copy: no launch
