@@ -331,6 +331,7 @@ __global__ void __launch_bounds__(kNodeThreads, 2) brem_node_accum_kernel(const 
     const unsigned int lane = tid & 31;
     const int warp = tid >> 5;
     const int grow = (int)(lane >> 2), gcol = (int)(lane & 3);  // tile row / column group of this lane
+    constexpr double kInvJ1[kNodePts] = {1.0, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8};
     // Tiles of kNodeTile consecutive segments, ordered by the depth cell of
     // their start on the first face in use (a counting sort in shared
     // memory), so that the 32 segments a warp takes share their cells and a
@@ -400,13 +401,13 @@ __global__ void __launch_bounds__(kNodeThreads, 2) brem_node_accum_kernel(const 
             double lo = 0.0, hi = 0.0;
             if (in_win) {
                 const double u = (T - Tc) * inv_Th;
-                const double p_i = sqrt(T * (T + 2.0 * kNodeMc2)) / kNodeMc2;
-                const double b_i = p_i / (1.0 + T / kNodeMc2);
+                // 1 / beta_i = (T + m c^2) / sqrt(T (T + 2 m c^2))
+                const double inv_bi = (T + kNodeMc2) / sqrt(T * (T + 2.0 * kNodeMc2));
                 const double Lc = a.L[s];
     #pragma unroll
                 for (int el = 0; el < NEL; ++el) {
                     const double Z = a.Z[el];
-                    double wp = a.n_ang3[el] * 1e24 * (Lc * 1e-8) * (Z * Z) * (1.0 - exp(-za * Z / b_i));
+                    double wp = a.n_ang3[el] * 1e24 * (Lc * 1e-8) * (Z * Z) * (1.0 - exp(-za * Z * inv_bi));
     #pragma unroll
                     for (int p = 0; p < kNodePts; ++p) {
                         sW[warp][el][lane][p] = p < kNodeTDeg ? wp : 0.0;
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(kNodeThreads, 2) brem_node_accum_kernel(const 
                                 for (int j = 1; j < kNodePts; ++j) {
                                     D = fma(tb, D, tan);
                                     tan *= ta;
-                                    M[j] = frac * D / (double)(j + 1);
+                                    M[j] = frac * D * kInvJ1[j];
                                 }
                             }
                         }
