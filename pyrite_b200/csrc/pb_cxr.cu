@@ -1560,17 +1560,23 @@ __global__ void far_field_kernel(const double *edges, int n_E, int pad, const do
 constexpr int kFarBins = 32;
 constexpr int kFarSlices = 8;
 
+// Acc is the accumulation type: double on the FP64 path, float on the mixed
+// one (a bin's far field is a sum of positive envelope terms and two small
+// corrections, well inside float over 2,100 centres; the slices' partial sums
+// and the spectrum stay FP64).
+template <class Acc>
 __global__ void __launch_bounds__(kFarBins * kFarSlices) far_field_conv_kernel(const double *edges, int n_E, int pad,
                                                                                const double *mom, double *spec,
                                                                                int K_far) {
-    extern __shared__ double sR[];  // r(D) for D = -n_mom .. n_mom
+    extern __shared__ __align__(16) unsigned char far_smem[];
+    Acc *sR = reinterpret_cast<Acc *>(far_smem);  // r(D) for D = -n_mom .. n_mom
     __shared__ double part[3][kFarSlices][kFarBins];
     const int d = blockIdx.y;
     const int n_mom = n_E + 2 * pad;
     const double w = (edges[n_E] - edges[0]) / n_E;
     for (int i = threadIdx.x; i <= 2 * n_mom; i += blockDim.x) {
         const double D = (double)(i - n_mom);
-        sR[i] = 1.0 / (D * D - 0.25);
+        sR[i] = (Acc)(1.0 / (D * D - 0.25));
     }
     __syncthreads();
     const int lane = threadIdx.x % kFarBins, slice = threadIdx.x / kFarBins;
@@ -1578,7 +1584,7 @@ __global__ void __launch_bounds__(kFarBins * kFarSlices) far_field_conv_kernel(c
     const double *m = mom + (int64_t)d * n_mom * 3;
     const int per = (n_mom + kFarSlices - 1) / kFarSlices;
     const int s0 = slice * per, s1 = min(s0 + per, n_mom);
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    Acc acc0 = 0, acc1 = 0, acc2 = 0;
     if (b < n_E) {
         for (int slot = s0; slot < s1; ++slot) {
             const int c = slot - pad;
@@ -1586,16 +1592,16 @@ __global__ void __launch_bounds__(kFarBins * kFarSlices) far_field_conv_kernel(c
             const double m0 = m[3 * slot];
             if (m0 == 0.0) continue;
             const int D = b - c;
-            const double r = sR[D + n_mom];
-            const double Dd = (double)D;
-            acc0 = fma(m0, r, acc0);
-            acc1 = fma(m[3 * slot + 1], 2.0 * Dd * r * r, acc1);
-            acc2 = fma(m[3 * slot + 2], (3.0 * Dd * Dd + 0.25) * r * r * r, acc2);
+            const Acc r = sR[D + n_mom];
+            const Acc Dd = (Acc)D;
+            acc0 = fma((Acc)m0, r, acc0);
+            acc1 = fma((Acc)m[3 * slot + 1], (Acc)2 * Dd * r * r, acc1);
+            acc2 = fma((Acc)m[3 * slot + 2], ((Acc)3 * Dd * Dd + (Acc)0.25) * r * r * r, acc2);
         }
     }
-    part[0][slice][lane] = acc0;
-    part[1][slice][lane] = acc1;
-    part[2][slice][lane] = acc2;
+    part[0][slice][lane] = (double)acc0;
+    part[1][slice][lane] = (double)acc1;
+    part[2][slice][lane] = (double)acc2;
     __syncthreads();
     if (slice == 0 && b < n_E) {
         double t0 = 0.0, t1 = 0.0, t2 = 0.0;
@@ -1723,14 +1729,14 @@ static cudaError_t launch_cxr_t(const pb_cxr_args &a, cudaStream_t s, int sms, i
     if (err != cudaSuccess) return err;
     if (K_far > 0) {
         dim3 fg((unsigned)((a.n_E + 127) / 128), (unsigned)a.n_dir);
-        const size_t tab = sizeof(double) * (2 * ((size_t)a.n_E + 2 * (size_t)far_pad) + 1);
+        const size_t tab = sizeof(Real) * (2 * ((size_t)a.n_E + 2 * (size_t)far_pad) + 1);
         if (tab <= 200 * 1024) {
             // the moments sit on a uniform axis (far moments are enabled on uniform edges only)
-            err = cudaFuncSetAttribute(far_field_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+            auto conv = far_field_conv_kernel<Real>;
+            err = cudaFuncSetAttribute(conv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
             if (err != cudaSuccess) return err;
             dim3 cg((unsigned)((a.n_E + kFarBins - 1) / kFarBins), (unsigned)a.n_dir);
-            far_field_conv_kernel<<<cg, kFarBins * kFarSlices, tab, s>>>(a.edges, a.n_E, far_pad, a.far_moments,
-                                                                         a.spec, K_far);
+            conv<<<cg, kFarBins * kFarSlices, tab, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
         } else {
             far_field_kernel<<<fg, 128, 0, s>>>(a.edges, a.n_E, far_pad, a.far_moments, a.spec, K_far);
         }
