@@ -200,7 +200,7 @@ typedef struct pb_transport_args {
     int32_t rng;        /* pb_rng */
     int32_t precision;  /* pb_precision */
     int32_t use_lut;
-    int32_t block_threads;  /* 0 = tuned default */
+    int32_t block_threads;  /* 0 = the default (256) */
     uint64_t seed;
     int64_t e_start;    /* first global history index */
     int64_t n;          /* histories */
