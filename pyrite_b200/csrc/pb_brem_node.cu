@@ -47,7 +47,7 @@ namespace {
 constexpr double kNodeMc2 = 510.99895;
 constexpr int kNodeThreads = 256;
 constexpr int kContractThreads = 128;
-constexpr int kNodeTile = 1024;  // segments a block orders by depth cell at a time
+constexpr int kNodeTile = 2048;  // segments a block orders by depth cell at a time (1024: 7 % slower, 4096: 3 %)
 
 __device__ __forceinline__ bool node_radiates(const pb_brem_args &a, int64_t s) {
     return a.elec_id[s] < a.Ne && (a.seg_layer == nullptr || a.seg_layer[s] == a.emit_layer);
