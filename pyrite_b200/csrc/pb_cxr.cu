@@ -1277,6 +1277,11 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
         }
         for (int g0 = 0; g0 < n_g; g0 += kRowChunk) {
             const int ng = (n_g - g0) < kRowChunk ? (n_g - g0) : kRowChunk;
+            // q / ng for the pass's pair ids q < kSegTile * ng by a multiply-high:
+            // magic = floor((2^32 - 1) / ng) + 1 is at least 2^32 / ng and
+            // exceeds it by under one, so q magic / 2^32 lies in
+            // [q / ng, q / ng + q / 2^32) and its floor is exact for q < 2^32 / ng.
+            const unsigned ng_magic = (unsigned)(0xFFFFFFFFull / (unsigned)ng) + 1u;
             __syncthreads();
             for (int j = tid; j < ng; j += blockDim.x) {
                 const int g = g0 + j;
@@ -1306,7 +1311,7 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
                     const int q = it * blockDim.x + tid;
                     bool ok = false;
                     if (q < n_pairs) {
-                        const int si = q / ng;
+                        const int si = (int)__umulhi((unsigned)q, ng_magic);
                         ok = pair_may_keep<Real>(segs[si], rows[q - si * ng], E_tab, dtail, n_tab, a.tables, ti);
                     }
                     const unsigned mask = __ballot_sync(0xffffffffu, ok);
@@ -1328,7 +1333,7 @@ __global__ void __launch_bounds__(kCxrThreads, 2) cxr_kernel(const pb_cxr_args a
                 ln.good = false;
                 if (k < n_surv) {
                     const int q = dtail != nullptr ? pq[k] : k;
-                    const int si = q / ng;
+                    const int si = (int)__umulhi((unsigned)q, ng_magic);
                     const int gi = q - si * ng;
                     ln = pair_line<Real, kLayered>(segs[si], rows[gi], E_tab, delta_tab, log_mu, n_tab, n_mu,
                                                    a.tables, ti, esc + si, a, lay_t);
